@@ -1,0 +1,209 @@
+/*
+ * rrg_gpu.h — C ABI of the B200 gzip/DEFLATE decoder.
+ *
+ * This is the drop-in boundary for rusty_rapidgzip's streaming decode path:
+ *
+ *   pub fn read_gz(path, sink: Sender<Arc<Vec<u8>>>, config: Config)
+ *       -> Result<DecodeStats, Error>                (crates/rusty-rapidgzip/src/lib.rs:366-370)
+ *
+ * Every entry point takes plain pointers and sizes. Device pointers are
+ * ordinary CUDA global-memory addresses on the context's device; host
+ * pointers are ordinary process memory. No entry point takes a torch or any
+ * other framework type.
+ *
+ * Threading: a context runs one decode at a time (calls on one context must
+ * not overlap); independent contexts are fully independent. The sink callback
+ * runs on the calling thread, in stream order.
+ */
+#ifndef RRG_GPU_H
+#define RRG_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. 1..9 mirror the reference's error enums:
+ *   Error::Io                       (lib.rs:111-118)            -> RRG_ERR_IO
+ *   GzipError::BadMagic             (gzip.rs:26-61)             -> RRG_ERR_BAD_MAGIC
+ *   GzipError::UnsupportedMethod(u8)                            -> RRG_ERR_UNSUPPORTED_METHOD
+ *   GzipError::ReservedFlags(u8)                                -> RRG_ERR_RESERVED_FLAGS
+ *   GzipError::Truncated                                        -> RRG_ERR_TRUNCATED
+ *   GzipError::CrcMismatch{..}                                  -> RRG_ERR_CRC_MISMATCH
+ *   GzipError::IsizeMismatch{..}                                -> RRG_ERR_ISIZE_MISMATCH
+ *   DeflateError::UnexpectedEof     (deflate/mod.rs:23-28)      -> RRG_ERR_DEFLATE_EOF
+ *   DeflateError::Invalid(&str)                                 -> RRG_ERR_DEFLATE_INVALID
+ * 20.. are conditions of the device path that the CPU reference cannot hit. */
+enum rrg_status {
+    RRG_OK = 0,
+    RRG_ERR_IO = 1,
+    RRG_ERR_BAD_MAGIC = 2,
+    RRG_ERR_UNSUPPORTED_METHOD = 3,
+    RRG_ERR_RESERVED_FLAGS = 4,
+    RRG_ERR_TRUNCATED = 5,
+    RRG_ERR_CRC_MISMATCH = 6,
+    RRG_ERR_ISIZE_MISMATCH = 7,
+    RRG_ERR_DEFLATE_EOF = 8,
+    RRG_ERR_DEFLATE_INVALID = 9,
+    RRG_ERR_CUDA = 20,             /* a CUDA runtime call failed (message holds the CUDA error string) */
+    RRG_ERR_OUT_OF_MEMORY = 21,    /* device allocation or HBM budget exceeded */
+    RRG_ERR_INVALID_ARGUMENT = 22, /* bad pointer/size/flag passed to the ABI */
+    RRG_ERR_TIMEOUT = 23,          /* a bounded device-side wait gave up */
+    RRG_ERR_CAPACITY = 24          /* caller-provided output buffer too small */
+};
+
+/* Error detail; fields follow GzipError::CrcMismatch / IsizeMismatch (gzip.rs:36-58). */
+typedef struct rrg_error {
+    int32_t code;          /* enum rrg_status */
+    uint32_t member;       /* 0-based member index (CRC/ISIZE errors) */
+    uint32_t expected;     /* trailer CRC32 or ISIZE; method/flag byte for codes 3/4 */
+    uint32_t got_crc;      /* computed CRC32 (CRC errors) */
+    uint64_t got;          /* computed uncompressed length (ISIZE errors) */
+    uint64_t uncompressed; /* member's uncompressed bytes */
+    uint64_t trailer_byte; /* byte offset of the member's trailer in the input file */
+    char message[160];     /* human-readable; DeflateError::Invalid's text for code 9 */
+} rrg_error;
+
+/* Mirrors Config (lib.rs:50-100). */
+typedef struct rrg_config {
+    uint32_t num_threads;        /* host threads for sink delivery/IO; 0 = all cores (Config::num_threads) */
+    uint64_t chunk_size_bytes;   /* sink delivery granularity in compressed bytes; 0 = 4 MiB (Config::chunk_size_bytes) */
+    int32_t verbose;             /* 0 = Verbosity::Off, 1 = Verbosity::On (stderr lines) */
+    int32_t device;              /* CUDA device ordinal; -1 = current device */
+    uint64_t gpu_chunk_bytes;    /* speculative sub-chunk size on the GPU; 0 = autotuned */
+    uint64_t finder_tile_bits;   /* block-finder tile width in bits; 0 = autotuned */
+    int32_t warps_per_stream;    /* 0 = autotuned; 1 or 2 (decoder warp + copy warp) */
+    int32_t reserved0;
+    uint64_t hbm_budget_bytes;   /* serving admission budget; 0 = 120 GB */
+} rrg_config;
+
+/* Mirrors DecodeStats (lib.rs:103-108), plus device-path counters. */
+typedef struct rrg_stats {
+    uint64_t compressed_bytes;
+    uint64_t uncompressed_bytes;
+    uint64_t chunks_decoded;       /* sink pieces delivered */
+    uint64_t speculation_failures; /* chunks re-decoded because a guessed start was false */
+    uint64_t gpu_chunks;           /* speculative sub-chunks decoded on the device */
+    uint64_t markers;              /* unresolved back-reference cells resolved by the marker kernel */
+    uint64_t members;              /* gzip members verified */
+    uint64_t kernel_launches;      /* kernels launched by this call */
+    double finder_ms, inflate_ms, resolve_ms, crc_ms, h2d_ms, d2h_ms, total_ms;
+} rrg_stats;
+
+/* Sink: called in stream order with consecutive pieces of decompressed output.
+ * The pointer is valid only for the duration of the call. Return 0 to continue,
+ * non-zero to close the sink (decoding stops early and the call returns RRG_OK,
+ * like a disconnected Sender in pipeline.rs:1028-1030). */
+typedef int (*rrg_sink_fn)(void* user, const uint8_t* data, size_t len);
+
+typedef struct rrg_ctx rrg_ctx;
+
+/* Context lifetime. Allocates the device workspace lazily on first use.
+ * Replaces constructing Config + the worker pools (pipeline.rs:580-625). */
+rrg_ctx* rrg_gpu_create(const rrg_config* cfg, rrg_error* err);
+void rrg_gpu_destroy(rrg_ctx* ctx);
+
+/* Drop-in for read_gz (lib.rs:366-496): open `path`, route BGZF vs plain member
+ * decode (lib.rs:463), decode on the GPU, verify CRC32/ISIZE per member and
+ * stream the bytes to `sink` in order. A zero-byte file is RRG_ERR_TRUNCATED. */
+int rrg_gpu_read_gz(rrg_ctx* ctx, const char* path, rrg_sink_fn sink, void* user,
+                    rrg_stats* stats, rrg_error* err);
+
+/* Same as rrg_gpu_read_gz for a gzip file already in host memory (`data` may be
+ * pageable or pinned). Replaces read_gz's mmap'd InputBytes (pipeline.rs:47-50). */
+int rrg_gpu_decode_host(rrg_ctx* ctx, const uint8_t* data, size_t len, rrg_sink_fn sink,
+                        void* user, rrg_stats* stats, rrg_error* err);
+
+/* Device-resident decode: `d_in` (device, `len` bytes) is a whole gzip file;
+ * the decompressed stream is written contiguously to `d_out` (device, capacity
+ * `out_cap`). Returns RRG_ERR_CAPACITY with *out_len = the required size when
+ * `out_cap` is too small. All work is ordered on `stream` (a cudaStream_t, or
+ * NULL for the context's own stream); the call returns after the stream's work
+ * for this decode has completed. Covers parallel_decode_member (pipeline.rs:468)
+ * and parallel_decode_bgzf (pipeline.rs:1357) without any host round trip of
+ * the payload. */
+int rrg_gpu_decode_device(rrg_ctx* ctx, const uint8_t* d_in, size_t len, uint8_t* d_out,
+                          size_t out_cap, size_t* out_len, void* stream, rrg_stats* stats,
+                          rrg_error* err);
+
+/* Batched decode of `n` independent gzip files/members already on the device
+ * (one persistent-kernel launch over a device work queue; see the BGZF batch
+ * path pipeline.rs:1357-1636 and decode_gzip_member libdeflate_ffi.rs:137-176).
+ * Input i is d_in[in_off[i] .. in_off[i]+in_len[i]); its output goes to
+ * d_out[out_off[i] ..] with room for out_cap[i] bytes; out_len[i] and status[i]
+ * (enum rrg_status) are written to host arrays. in_off/in_len/out_off/out_cap
+ * are host arrays. Returns the first failing status (RRG_OK if all passed). */
+int rrg_gpu_decode_batch(rrg_ctx* ctx, const uint8_t* d_in, const uint64_t* in_off,
+                         const uint64_t* in_len, uint8_t* d_out, const uint64_t* out_off,
+                         const uint64_t* out_cap, uint64_t* out_len, int32_t* status, size_t n,
+                         void* stream, rrg_stats* stats, rrg_error* err);
+
+/* ---- kernel-level entry points (each replaces one reference function) ---- */
+
+/* Block finder over a raw DEFLATE body on the device. For each target bit
+ * offset targets[i] (host array), writes to found[i] (host array) the first
+ * bit offset >= targets[i] and < limits[i] that find_next_dynamic_block
+ * (deflate/block_finder.rs:109-141) would return with until_bit = limits[i],
+ * or UINT64_MAX if none. */
+int rrg_gpu_find_blocks(rrg_ctx* ctx, const uint8_t* d_body, size_t body_len,
+                        const uint64_t* targets, const uint64_t* limits, uint64_t* found,
+                        size_t n, rrg_error* err);
+
+/* CRC32 (IEEE, as crc32fast::hash) of a device buffer; replaces the crc32fast
+ * pieces + combine of pipeline.rs:712-732 and :885-916. */
+int rrg_gpu_crc32(rrg_ctx* ctx, const uint8_t* d_data, size_t len, uint32_t* crc_out,
+                  rrg_error* err);
+
+/* Marker resolution (deflate/speculative.rs:175-213): for each marker
+ * (out_pos[i], prefix_offset[i]) set d_bytes[out_pos[i]] =
+ * d_tail[tail_len - 1 - prefix_offset[i]]. All arrays are on the device. Fails
+ * with RRG_ERR_DEFLATE_INVALID if any prefix_offset >= tail_len. */
+int rrg_gpu_resolve_markers(rrg_ctx* ctx, uint8_t* d_bytes, size_t n_bytes,
+                            const uint32_t* d_out_pos, const uint16_t* d_prefix_offset,
+                            size_t n_markers, const uint8_t* d_tail, size_t tail_len,
+                            rrg_error* err);
+
+/* Speculative decode of one chunk of a raw DEFLATE body on the device, with
+ * the output contract of decode_one_chunk + decode_until_u16 (pipeline.rs:1080-1185,
+ * deflate/fast_inflate.rs:1794-1888): host receives the chunk's bytes (marker
+ * bytes = 0), its markers sorted by out_pos, and the bit offset where decoding
+ * stopped. `*n_bytes`/`*n_markers` are in: capacity, out: count. */
+int rrg_gpu_decode_chunk(rrg_ctx* ctx, const uint8_t* d_body, size_t body_len,
+                         uint64_t start_bit, uint64_t end_bit_hint, uint8_t* bytes,
+                         size_t* n_bytes, uint32_t* marker_pos, uint16_t* marker_off,
+                         size_t* n_markers, uint64_t* actual_end_bit, int32_t* final_block,
+                         rrg_error* err);
+
+/* ---- serving loop (continuous batching under an HBM budget) ---- */
+
+/* Submit a whole gzip file held in host memory (copied at submit). Returns a
+ * request id >= 0, or -1 on error. Requests are admitted to the GPU as slots
+ * and HBM budget free up; admitted requests' work overlaps on the device. */
+int64_t rrg_gpu_submit(rrg_ctx* ctx, const uint8_t* data, size_t len, rrg_error* err);
+
+/* Drive the serving loop once and collect one finished request if any.
+ * Returns 1 and fills the outputs when a request finished, 0 if none finished
+ * within `timeout_ms`, or a negative rrg_status on failure. `*out` is a
+ * malloc'd buffer the caller frees with rrg_gpu_free; `*latency_ms` is
+ * submit-to-finish wall time. A request that failed returns 1 with
+ * *status != RRG_OK and *out == NULL. */
+int rrg_gpu_poll(rrg_ctx* ctx, int64_t* request_id, uint8_t** out, size_t* out_len,
+                 int32_t* status, double* latency_ms, int32_t timeout_ms, rrg_error* err);
+
+/* Number of requests submitted but not yet returned by rrg_gpu_poll. */
+int64_t rrg_gpu_pending(rrg_ctx* ctx);
+
+void rrg_gpu_free(void* p);
+
+/* Library version string and the number of kernels this library has launched
+ * in this process (for launch accounting). */
+const char* rrg_gpu_version(void);
+uint64_t rrg_gpu_kernel_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RRG_GPU_H */
