@@ -1,0 +1,323 @@
+#!/usr/bin/env python3
+"""Decompressed GB/s of the B200 gzip/DEFLATE decoder.
+
+Default workload: 1 GiB of seeded Zipf(1.1) word text (50,000-word vocabulary,
+newline every 8-20 words) compressed at zlib level 9 as ONE gzip member,
+decoded on one GPU (input resident in HBM, output to HBM). A step is one
+whole-file decode through rrg_gpu_decode_device.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload zipf1g|fastq64m|bgzf|files]
+
+With N > 1 (torchrun, one rank per GPU) every rank decodes its own copy of the
+workload (independent files: weak scaling, no collective on the data path);
+value = all ranks' bytes / the slowest rank's time.
+
+--impl reference times the reference algorithm's CPU path (the C restatement in
+oracle/, rusty_rapidgzip's Rust crate cannot be built here) on all host cores
+on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CACHE = os.environ.get("RRG_BENCH_CACHE", "/tmp/rrg_bench_cache")
+GEN_VERSION = 2
+
+
+def workload(name: str, size: int | None):
+    """(raw, compressed, description) — cached on local disk between runs."""
+    from rusty_rapidgzip_b200 import workloads as W
+    if name == "zipf1g":
+        n = size or (1 << 30)
+        key, make = f"zipf_{n}_s1_v{GEN_VERSION}", lambda: W.config1(n, seed=1)
+        desc = {"workload": "zipf_text_level9_single_member", "uncompressed_bytes": n, "zlib_level": 9,
+                "vocabulary": 50000, "zipf_exponent": 1.1}
+    elif name == "fastq64m":
+        n = size or (64 << 20)
+        key, make = f"fastq_{n}_s0_v{GEN_VERSION}", lambda: W.config0(n, seed=0)
+        desc = {"workload": "fastq_like_level6_single_member", "uncompressed_bytes": n, "zlib_level": 6}
+    elif name == "bgzf":
+        n = size or (4 << 30)
+        key, make = f"bgzf_{n}_s0_v{GEN_VERSION}", lambda: W.config2(n, seed=0)
+        desc = {"workload": "fastq_like_bgzf_level5", "uncompressed_bytes": n, "zlib_level": 5,
+                "member_max_input": 65280}
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    os.makedirs(CACHE, exist_ok=True)
+    pr, pc = os.path.join(CACHE, key + ".raw"), os.path.join(CACHE, key + ".gz")
+    if os.path.exists(pr) and os.path.exists(pc) and os.path.getsize(pr) == n:
+        return open(pr, "rb").read(), open(pc, "rb").read(), desc
+    raw, gz = make()
+    try:
+        with open(pr + ".tmp", "wb") as f:
+            f.write(raw)
+        with open(pc + ".tmp", "wb") as f:
+            f.write(gz)
+        os.replace(pr + ".tmp", pr)
+        os.replace(pc + ".tmp", pc)
+    except OSError:
+        pass
+    return raw, gz, desc
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_time_oracle(gz: bytes, n_raw: int, threads: int, min_reps: int = 3, min_seconds: float = 3.0):
+    import oracle
+    times = []
+    t_start = time.perf_counter()
+    while len(times) < min_reps or time.perf_counter() - t_start < min_seconds:
+        t0 = time.perf_counter()
+        n, _ = oracle.read_gz_count(gz, num_threads=threads, chunk_size=4 << 20)
+        times.append(time.perf_counter() - t0)
+        assert n == n_raw
+        if len(times) >= 20:
+            break
+    return times
+
+
+def run_reference(args, raw, gz, desc):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_time_oracle(gz, len(raw), threads, min_reps=1, min_seconds=0)
+    times = []
+    for _ in range(args.steps):
+        times += cpu_time_oracle(gz, len(raw), threads, min_reps=1, min_seconds=0)
+    total = sum(times)
+    value = len(raw) * len(times) / total / 1e9
+    line = {
+        "metric": "decompressed GB/s", "value": round(value, 3), "unit": "GB/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1000 * total / len(times), 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator)",
+        "config": dict(desc, compressed_bytes=len(gz), parallelism="cpu threads"),
+        "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+                         "sample": "whole workload file per step, all host threads, oracle/ C restatement of the "
+                                   "reference pipeline (rusty_rapidgzip's Rust crate has no toolchain here)"},
+        "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, raw, gz, desc):
+    import torch
+    import torch.distributed as dist
+    from rusty_rapidgzip_b200 import Config, Decoder, kernel_launch_count
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local))
+    dec = Decoder(Config(device=local, gpu_chunk_bytes=args.gpu_chunk, verbose=False))
+    stream = torch.cuda.Stream()
+    din = torch.empty(len(gz), dtype=torch.uint8, device="cuda")
+    din.copy_(torch.frombuffer(bytearray(gz), dtype=torch.uint8))
+    dout = torch.empty(len(raw) + 64, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+
+    def step():
+        n, st = dec.decode_device(din, len(gz), dout, dout.numel(), stream=stream.cuda_stream)
+        assert n == len(raw)
+        return st
+
+    for _ in range(max(args.warmup, 1)):
+        step()
+    # correctness of the measured path (outside the timed region)
+    torch.cuda.synchronize()
+    import hashlib
+    ok = hashlib.sha256(dout[: len(raw)].cpu().numpy().tobytes()).digest() == hashlib.sha256(raw).digest()
+    if not ok:
+        raise SystemExit("decoded bytes differ from the generator output")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---------------- device-resident timed region
+    barrier()
+    torch.cuda.synchronize()
+    stats = []
+    with ClockSampler(local) as clk:
+        l0 = kernel_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            stats.append(step())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        launches = kernel_launch_count() - l0
+    barrier()
+    t = e0.elapsed_time(e1) / 1000.0
+    if world > 1:
+        tt = torch.tensor([t], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt.item())
+    value = world * len(raw) * args.steps / t / 1e9
+
+    # ---------------- end to end through the C ABI with host buffers
+    pinned = torch.empty(len(gz), dtype=torch.uint8, pin_memory=True)
+    pinned.copy_(torch.frombuffer(bytearray(gz), dtype=torch.uint8))
+    buf = pinned.numpy()
+    n, _ = dec.count(buf)  # warm the host-path buffers
+    assert n == len(raw)
+    barrier()
+    e2e_times = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        n, _ = dec.count(buf)
+        e2e_times.append(time.perf_counter() - t0)
+        assert n == len(raw)
+    te = sum(e2e_times)
+    if world > 1:
+        tt = torch.tensor([te], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        te = float(tt.item())
+    e2e_value = world * len(raw) * args.steps / te / 1e9
+
+    # ---------------- roofline of the dominant kernel
+    kern = {k: statistics.mean(s.timings_ms[k] for s in stats) for k in ("finder", "inflate", "resolve", "crc")}
+    dominant = max(kern, key=kern.get)
+    C_, U_ = len(gz), len(raw)
+    algo = {"inflate": C_ + 2 * U_,          # compressed read once + u16 cells written
+            "resolve": 3 * U_,                # u16 cells read + bytes written
+            "crc": U_,                        # bytes read
+            "finder": C_}                     # upper bound: every compressed byte scanned once
+    peak, peak_kind = measured_peak_hbm()
+    achieved = algo[dominant] / (kern[dominant] / 1000.0) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get(f"{args.workload}:{dominant}")
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        times = cpu_time_oracle(gz, len(raw), threads)
+        cpu = {"value": round(len(raw) / statistics.median(times) / 1e9, 3), "unit": "GB/s", "cores": threads,
+               "kind": "port",
+               "sample": f"whole workload file, median of {len(times)} runs, oracle/ C restatement of the reference "
+                         "pipeline on all host threads"}
+    if rank == 0:
+        ms = stats[-1]
+        line = {
+            "metric": "decompressed GB/s", "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * t / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded generator)",
+            "config": dict(desc, compressed_bytes=C_, parallelism=f"replicas x{world}",
+                           l2="inputs (compressed + output) larger than L2; no flush",
+                           gpu_chunk_bytes=args.gpu_chunk or "auto", gpu_chunks=ms.gpu_chunks,
+                           markers=ms.markers, speculation_failures=ms.speculation_failures),
+            "e2e": {"value": round(e2e_value, 3), "unit": "GB/s", "h2d_bytes_per_step": C_,
+                    "d2h_bytes_per_step": U_},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 2), "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "traffic": traffic, "algorithmic_bytes_per_launch": algo[dominant]},
+            "kernels_ms": {k: round(v, 3) for k, v in kern.items()},
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    dec.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="zipf1g", choices=["zipf1g", "fastq64m", "bgzf"])
+    ap.add_argument("--size", type=int, default=None)
+    ap.add_argument("--gpu-chunk", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        print("note: fewer than 3 warm-up steps", file=sys.stderr)
+    raw, gz, desc = workload(args.workload, args.size)
+    if args.impl == "reference":
+        run_reference(args, raw, gz, desc)
+    else:
+        run_ours(args, raw, gz, desc)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,481 @@
+"""ctypes binding of include/rrg_gpu.h and the Python mirror of the reference API.
+
+The reference's drop-in surface (crates/rusty-rapidgzip/src/lib.rs):
+
+    read_gz(path, sink: Sender<Arc<Vec<u8>>>, config: Config) -> Result<DecodeStats, Error>
+
+is mirrored by :func:`read_gz` here: ``sink`` receives the decompressed stream
+in order as ``bytes`` pieces (a callable, or any object with ``send``/``put``,
+e.g. ``queue.Queue``); a sink returning ``False`` (or whose ``send``/``put``
+raises :class:`SinkClosed`) closes the channel and decoding stops early with
+success, as a dropped receiver does in the reference (pipeline.rs:1028-1030).
+Errors raise :class:`RrgError` subclasses mirroring ``Error::{Io, Gzip, Deflate}``.
+
+All work runs in the CUDA library ``librrg_gpu.so`` built next to this file.
+There is no CPU fallback: if the library is missing, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+from dataclasses import dataclass, field
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_NAME = "librrg_gpu.so"
+DEFAULT_LIB = os.path.join(HERE, LIB_NAME)
+
+# enum rrg_status
+OK = 0
+ERR_IO = 1
+ERR_BAD_MAGIC = 2
+ERR_UNSUPPORTED_METHOD = 3
+ERR_RESERVED_FLAGS = 4
+ERR_TRUNCATED = 5
+ERR_CRC_MISMATCH = 6
+ERR_ISIZE_MISMATCH = 7
+ERR_DEFLATE_EOF = 8
+ERR_DEFLATE_INVALID = 9
+ERR_CUDA = 20
+ERR_OUT_OF_MEMORY = 21
+ERR_INVALID_ARGUMENT = 22
+ERR_TIMEOUT = 23
+ERR_CAPACITY = 24
+
+GZIP_KINDS = {
+    ERR_BAD_MAGIC: "BadMagic",
+    ERR_UNSUPPORTED_METHOD: "UnsupportedMethod",
+    ERR_RESERVED_FLAGS: "ReservedFlags",
+    ERR_TRUNCATED: "Truncated",
+    ERR_CRC_MISMATCH: "CrcMismatch",
+    ERR_ISIZE_MISMATCH: "IsizeMismatch",
+}
+
+
+class _Error(C.Structure):
+    _fields_ = [
+        ("code", C.c_int32),
+        ("member", C.c_uint32),
+        ("expected", C.c_uint32),
+        ("got_crc", C.c_uint32),
+        ("got", C.c_uint64),
+        ("uncompressed", C.c_uint64),
+        ("trailer_byte", C.c_uint64),
+        ("message", C.c_char * 160),
+    ]
+
+
+class _Config(C.Structure):
+    _fields_ = [
+        ("num_threads", C.c_uint32),
+        ("chunk_size_bytes", C.c_uint64),
+        ("verbose", C.c_int32),
+        ("device", C.c_int32),
+        ("gpu_chunk_bytes", C.c_uint64),
+        ("finder_tile_bits", C.c_uint64),
+        ("warps_per_stream", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("hbm_budget_bytes", C.c_uint64),
+    ]
+
+
+_STAT_U64 = ["compressed_bytes", "uncompressed_bytes", "chunks_decoded", "speculation_failures",
+             "gpu_chunks", "markers", "members", "kernel_launches"]
+_STAT_F64 = ["finder_ms", "inflate_ms", "resolve_ms", "crc_ms", "h2d_ms", "d2h_ms", "total_ms"]
+
+
+class _Stats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in _STAT_U64] + [(n, C.c_double) for n in _STAT_F64]
+
+
+SINK_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_uint8), C.c_size_t)
+
+
+# ------------------------------------------------------------------ API types
+@dataclass
+class Config:
+    """Mirrors Config (lib.rs:50-100) plus device tunables (0 = autotuned)."""
+    num_threads: int = 0
+    chunk_size_bytes: int = 4 << 20
+    verbose: bool = False
+    device: int = -1
+    gpu_chunk_bytes: int = 0
+    finder_tile_bits: int = 0
+    warps_per_stream: int = 0
+    hbm_budget_bytes: int = 0
+
+    def _c(self) -> _Config:
+        c = _Config()
+        c.num_threads = self.num_threads
+        c.chunk_size_bytes = self.chunk_size_bytes
+        c.verbose = 1 if self.verbose else 0
+        c.device = self.device
+        c.gpu_chunk_bytes = self.gpu_chunk_bytes
+        c.finder_tile_bits = self.finder_tile_bits
+        c.warps_per_stream = self.warps_per_stream
+        c.hbm_budget_bytes = self.hbm_budget_bytes
+        return c
+
+
+@dataclass
+class DecodeStats:
+    """Mirrors DecodeStats (lib.rs:103-108) plus device-path counters."""
+    compressed_bytes: int = 0
+    uncompressed_bytes: int = 0
+    chunks_decoded: int = 0
+    speculation_failures: int = 0
+    gpu_chunks: int = 0
+    markers: int = 0
+    members: int = 0
+    kernel_launches: int = 0
+    timings_ms: dict = field(default_factory=dict)
+
+    @classmethod
+    def _from(cls, s: _Stats) -> "DecodeStats":
+        return cls(**{n: int(getattr(s, n)) for n in _STAT_U64},
+                   timings_ms={n[:-3]: float(getattr(s, n)) for n in _STAT_F64})
+
+
+class RrgError(Exception):
+    """Base of the decoder errors (Error in lib.rs:111-118)."""
+
+    def __init__(self, e: _Error):
+        self.code = int(e.code)
+        self.member = int(e.member)
+        self.expected = int(e.expected)
+        self.got_crc = int(e.got_crc)
+        self.got = int(e.got)
+        self.uncompressed = int(e.uncompressed)
+        self.trailer_byte = int(e.trailer_byte)
+        self.message = e.message.decode(errors="replace")
+        super().__init__(self.message or f"status {self.code}")
+
+
+class IoError(RrgError):
+    """Error::Io"""
+
+
+class GzipError(RrgError):
+    """Error::Gzip(GzipError::...); ``kind`` names the variant."""
+
+    @property
+    def kind(self) -> str:
+        return GZIP_KINDS.get(self.code, "Unknown")
+
+
+class DeflateError(RrgError):
+    """Error::Deflate(DeflateError::UnexpectedEof | Invalid(&str))."""
+
+    @property
+    def kind(self) -> str:
+        return "UnexpectedEof" if self.code == ERR_DEFLATE_EOF else "Invalid"
+
+
+class DeviceError(RrgError):
+    """CUDA runtime failure, device memory exhausted, or bad ABI argument."""
+
+
+class CapacityError(RrgError):
+    """Caller-provided output buffer too small."""
+
+
+class SinkClosed(Exception):
+    """Raise from a sink to close it (the reference's disconnected receiver)."""
+
+
+def _raise(e: _Error):
+    code = int(e.code)
+    if code == OK:
+        return
+    if code == ERR_IO:
+        raise IoError(e)
+    if code in GZIP_KINDS:
+        raise GzipError(e)
+    if code in (ERR_DEFLATE_EOF, ERR_DEFLATE_INVALID):
+        raise DeflateError(e)
+    if code == ERR_CAPACITY:
+        raise CapacityError(e)
+    raise DeviceError(e)
+
+
+# ------------------------------------------------------------------ library
+_lib_cache: dict = {}
+_lib_lock = threading.Lock()
+
+
+def library_path() -> str:
+    return os.environ.get("RRG_GPU_LIB", DEFAULT_LIB)
+
+
+def load_library(path: str | None = None):
+    """Load and type the decoder library; raises if it has not been built."""
+    path = path or library_path()
+    with _lib_lock:
+        if path in _lib_cache:
+            return _lib_cache[path]
+        if not os.path.exists(path):
+            raise ImportError(
+                f"{path} not found: build the CUDA library first "
+                "(python -m rusty_rapidgzip_b200.build); there is no CPU fallback")
+        L = C.CDLL(path)
+        vp, sz, u64, i32 = C.c_void_p, C.c_size_t, C.c_uint64, C.c_int32
+        E, S = C.POINTER(_Error), C.POINTER(_Stats)
+        L.rrg_gpu_create.argtypes = [C.POINTER(_Config), E]
+        L.rrg_gpu_create.restype = vp
+        L.rrg_gpu_destroy.argtypes = [vp]
+        L.rrg_gpu_read_gz.argtypes = [vp, C.c_char_p, SINK_FN, vp, S, E]
+        L.rrg_gpu_decode_host.argtypes = [vp, vp, sz, SINK_FN, vp, S, E]
+        L.rrg_gpu_decode_device.argtypes = [vp, vp, sz, vp, sz, C.POINTER(sz), vp, S, E]
+        L.rrg_gpu_decode_batch.argtypes = [vp, vp, C.POINTER(u64), C.POINTER(u64), vp, C.POINTER(u64),
+                                           C.POINTER(u64), C.POINTER(u64), C.POINTER(i32), sz, vp, S, E]
+        L.rrg_gpu_find_blocks.argtypes = [vp, vp, sz, C.POINTER(u64), C.POINTER(u64), C.POINTER(u64), sz, E]
+        L.rrg_gpu_crc32.argtypes = [vp, vp, sz, C.POINTER(C.c_uint32), E]
+        L.rrg_gpu_resolve_markers.argtypes = [vp, vp, sz, vp, vp, sz, vp, sz, E]
+        L.rrg_gpu_decode_chunk.argtypes = [vp, vp, sz, u64, u64, vp, C.POINTER(sz), vp, vp, C.POINTER(sz),
+                                           C.POINTER(u64), C.POINTER(i32), E]
+        L.rrg_gpu_submit.argtypes = [vp, vp, sz, E]
+        L.rrg_gpu_submit.restype = C.c_int64
+        L.rrg_gpu_poll.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(sz),
+                                   C.POINTER(i32), C.POINTER(C.c_double), i32, E]
+        L.rrg_gpu_pending.argtypes = [vp]
+        L.rrg_gpu_pending.restype = C.c_int64
+        L.rrg_gpu_free.argtypes = [vp]
+        L.rrg_gpu_version.restype = C.c_char_p
+        L.rrg_gpu_kernel_launch_count.restype = C.c_uint64
+        _lib_cache[path] = L
+        return L
+
+
+def _ptr(x) -> int:
+    """Address of a device buffer: an int, or an object with data_ptr() (torch)."""
+    if x is None:
+        return 0
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return int(x.data_ptr())
+    raise TypeError(f"expected a device pointer, got {type(x).__name__}")
+
+
+def _host_buffer(data):
+    """(address, length, keepalive) of a host bytes-like object."""
+    mv = memoryview(data).cast("B")
+    if mv.readonly:
+        buf = (C.c_char * len(mv)).from_buffer_copy(mv) if len(mv) else None
+    else:
+        buf = (C.c_char * len(mv)).from_buffer(mv) if len(mv) else None
+    return (C.addressof(buf) if buf is not None else None), len(mv), (buf, mv)
+
+
+def _as_sink(sink):
+    if sink is None:
+        return None
+    if callable(sink):
+        return sink
+    for m in ("send", "put"):
+        if hasattr(sink, m):
+            return getattr(sink, m)
+    raise TypeError("sink must be callable or have send()/put()")
+
+
+class Decoder:
+    """A decoding context on one GPU (rrg_gpu_create). One decode at a time."""
+
+    def __init__(self, config: Config | None = None, lib: str | None = None):
+        self.config = config or Config()
+        self._L = load_library(lib)
+        e = _Error()
+        self._ctx = self._L.rrg_gpu_create(C.byref(self.config._c()), C.byref(e))
+        if not self._ctx:
+            _raise(e)
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            self._L.rrg_gpu_destroy(self._ctx)
+            self._ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -------------------------------------------------------------- streaming
+    def _run(self, fn, *args, sink=None) -> DecodeStats:
+        target = _as_sink(sink)
+        failure = []
+
+        def cb(_u, p, n):
+            if target is None:
+                return 0
+            try:
+                r = target(C.string_at(p, n))
+            except SinkClosed:
+                return 1
+            except BaseException as ex:  # surfaced after the call returns
+                failure.append(ex)
+                return 1
+            return 1 if r is False else 0
+
+        st, e = _Stats(), _Error()
+        fn(self._ctx, *args, SINK_FN(cb), None, C.byref(st), C.byref(e))
+        if failure:
+            raise failure[0]
+        _raise(e)
+        return DecodeStats._from(st)
+
+    def read_gz(self, path, sink) -> DecodeStats:
+        """read_gz (lib.rs:366-496) for a file path."""
+        return self._run(self._L.rrg_gpu_read_gz, os.fsencode(os.fspath(path)), sink=sink)
+
+    def decode_host(self, data, sink) -> DecodeStats:
+        """read_gz over a gzip file already in host memory."""
+        addr, n, keep = _host_buffer(data)
+        stats = self._run(self._L.rrg_gpu_decode_host, addr, n, sink=sink)
+        del keep
+        return stats
+
+    def decompress(self, data) -> bytes:
+        out = []
+        self.decode_host(data, out.append)
+        return b"".join(out)
+
+    def count(self, data) -> tuple[int, DecodeStats]:
+        """Decode, delivering to a sink that only counts bytes (no Python copy)."""
+        addr, n, keep = _host_buffer(data)
+        total = [0]
+
+        def cb(_u, _p, ln):
+            total[0] += ln
+            return 0
+
+        st, e = _Stats(), _Error()
+        self._L.rrg_gpu_decode_host(self._ctx, addr, n, SINK_FN(cb), None, C.byref(st), C.byref(e))
+        del keep
+        _raise(e)
+        return total[0], DecodeStats._from(st)
+
+    # -------------------------------------------------------------- device
+    def decode_device(self, d_in, length: int, d_out, out_cap: int, stream=None) -> tuple[int, DecodeStats]:
+        """Device-resident decode; returns (bytes written, stats)."""
+        out_len = C.c_size_t()
+        st, e = _Stats(), _Error()
+        self._L.rrg_gpu_decode_device(self._ctx, _ptr(d_in), length, _ptr(d_out), out_cap, C.byref(out_len),
+                                      _ptr(stream), C.byref(st), C.byref(e))
+        if e.code == ERR_CAPACITY:
+            err = CapacityError(e)
+            err.required = int(out_len.value)
+            raise err
+        _raise(e)
+        return int(out_len.value), DecodeStats._from(st)
+
+    def decode_batch(self, d_in, in_off, in_len, d_out, out_off, out_cap, stream=None):
+        """Batched member decode; returns (out_len list, status list, stats).
+        Raises nothing for per-item failures (see the status list)."""
+        n = len(in_off)
+        A = C.c_uint64 * max(n, 1)
+        io, il, oo, oc = A(*in_off), A(*in_len), A(*out_off), A(*out_cap)
+        ol = A()
+        stv = (C.c_int32 * max(n, 1))()
+        st, e = _Stats(), _Error()
+        self._L.rrg_gpu_decode_batch(self._ctx, _ptr(d_in), io, il, _ptr(d_out), oo, oc, ol, stv, n,
+                                     _ptr(stream), C.byref(st), C.byref(e))
+        if e.code not in (OK,) and e.code >= ERR_CUDA and e.code != ERR_CAPACITY:
+            _raise(e)
+        return [int(ol[i]) for i in range(n)], [int(stv[i]) for i in range(n)], DecodeStats._from(st)
+
+    # -------------------------------------------------------------- kernels
+    def find_blocks(self, d_body, body_len: int, targets, limits):
+        n = len(targets)
+        A = C.c_uint64 * max(n, 1)
+        t, lim, f = A(*targets), A(*limits), A()
+        e = _Error()
+        self._L.rrg_gpu_find_blocks(self._ctx, _ptr(d_body), body_len, t, lim, f, n, C.byref(e))
+        _raise(e)
+        return [None if f[i] == 0xFFFFFFFFFFFFFFFF else int(f[i]) for i in range(n)]
+
+    def crc32(self, d_data, length: int) -> int:
+        out = C.c_uint32()
+        e = _Error()
+        self._L.rrg_gpu_crc32(self._ctx, _ptr(d_data), length, C.byref(out), C.byref(e))
+        _raise(e)
+        return int(out.value)
+
+    def resolve_markers(self, d_bytes, n_bytes, d_out_pos, d_prefix_offset, n_markers, d_tail, tail_len):
+        e = _Error()
+        self._L.rrg_gpu_resolve_markers(self._ctx, _ptr(d_bytes), n_bytes, _ptr(d_out_pos),
+                                        _ptr(d_prefix_offset), n_markers, _ptr(d_tail), tail_len, C.byref(e))
+        _raise(e)
+
+    def decode_chunk(self, d_body, body_len: int, start_bit: int, end_bit_hint: int,
+                     max_bytes: int = 64 << 20, max_markers: int = 16 << 20):
+        """Speculative chunk decode -> (bytes, marker_pos list, marker_off list, actual_end_bit, final)."""
+        import numpy as np
+        nb, nm = C.c_size_t(max_bytes), C.c_size_t(max_markers)
+        b = np.zeros(max_bytes, np.uint8)
+        mp = np.zeros(max_markers, np.uint32)
+        mo = np.zeros(max_markers, np.uint16)
+        end, fin = C.c_uint64(), C.c_int32()
+        e = _Error()
+        self._L.rrg_gpu_decode_chunk(self._ctx, _ptr(d_body), body_len, start_bit, end_bit_hint,
+                                     b.ctypes.data, C.byref(nb), mp.ctypes.data, mo.ctypes.data, C.byref(nm),
+                                     C.byref(end), C.byref(fin), C.byref(e))
+        _raise(e)
+        return (b[:nb.value].tobytes(), mp[:nm.value].copy(), mo[:nm.value].copy(), int(end.value),
+                bool(fin.value))
+
+    # -------------------------------------------------------------- serving
+    def submit(self, data) -> int:
+        addr, n, keep = _host_buffer(data)
+        e = _Error()
+        rid = self._L.rrg_gpu_submit(self._ctx, addr, n, C.byref(e))
+        del keep
+        if rid < 0:
+            _raise(e)
+        return int(rid)
+
+    def poll(self, timeout_ms: int = 0):
+        """-> None, or (request_id, bytes | None, status, latency_ms)."""
+        rid = C.c_int64()
+        out = C.POINTER(C.c_uint8)()
+        n = C.c_size_t()
+        stv = C.c_int32()
+        lat = C.c_double()
+        e = _Error()
+        r = self._L.rrg_gpu_poll(self._ctx, C.byref(rid), C.byref(out), C.byref(n), C.byref(stv), C.byref(lat),
+                                 timeout_ms, C.byref(e))
+        if r < 0:
+            _raise(e)
+        if r == 0:
+            return None
+        data = None
+        if out:
+            data = C.string_at(out, n.value)
+            self._L.rrg_gpu_free(out)
+        return int(rid.value), data, int(stv.value), float(lat.value)
+
+    def pending(self) -> int:
+        return int(self._L.rrg_gpu_pending(self._ctx))
+
+
+def read_gz(path, sink, config: Config | None = None) -> DecodeStats:
+    """Decode `path` and stream decompressed bytes to `sink` in stream order.
+
+    Blocks until EOF or the first error (lib.rs:366-496)."""
+    with Decoder(config) as d:
+        return d.read_gz(path, sink)
+
+
+def decompress(data, config: Config | None = None) -> bytes:
+    with Decoder(config) as d:
+        return d.decompress(data)
+
+
+def kernel_launch_count(lib: str | None = None) -> int:
+    return int(load_library(lib).rrg_gpu_kernel_launch_count())

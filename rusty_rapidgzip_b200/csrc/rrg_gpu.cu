@@ -1,0 +1,1444 @@
+// rrg_gpu.cu — host orchestration and C ABI (include/rrg_gpu.h) of the B200
+// gzip/DEFLATE decoder.
+//
+// Member route (rrg/src/pipeline.rs:468-1041, parallel_decode_member):
+//   k_find_blocks  -> sub-chunk boundaries every `gpu_chunk_bytes` of compressed input
+//   k_inflate<u16> -> every sub-chunk decoded at once, one warp each, unknown-window
+//                     back-references emitted as 16-bit marker cells
+//   host chain     -> anchored verification (pipeline.rs:758-809): chunk k is kept iff
+//                     it starts where chunk k-1 stopped; otherwise it is re-decoded
+//   k_resolve      -> markers chased to literal cells, cells compacted to bytes
+//   k_crc_*        -> CRC32/ISIZE of every member from per-piece CRCs + GF(2) combine
+// BGZF route (pipeline.rs:1357-1636): members found by a header walk, one warp
+// per member through the persistent k_inflate<u8> work queue, CRC as above.
+#ifndef RRG_EMU
+#include <cuda_runtime.h>
+#endif
+
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <deque>
+#include <unordered_map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "rrg_gpu.h"
+#include "rrg_common.h"
+#include "rrg_kernels.cuh"
+
+#ifdef RRG_EMU
+#define RRG_LAUNCH(kern, grid, block, smem, strm, ...) emu::launch((grid), (block), (smem), [&] { kern(__VA_ARGS__); })
+#else
+#define RRG_LAUNCH(kern, grid, block, smem, strm, ...) kern<<<(grid), (block), (smem), (strm)>>>(__VA_ARGS__)
+#endif
+
+using namespace rrg;
+
+namespace {
+
+std::atomic<uint64_t> g_launches{0};
+
+const char* msg_text(int m) {
+    switch (m) {
+    case MSG_RESERVED_BTYPE: return "reserved block type";
+    case MSG_STORED_NLEN: return "stored block: LEN/NLEN mismatch";
+    case MSG_LITLEN_RANGE: return "literal/length symbol out of range";
+    case MSG_DIST_RANGE: return "distance symbol out of range";
+    case MSG_NO_CODE: return "no matching huffman code";
+    case MSG_OVERSUB: return "oversubscribed huffman tree";
+    case MSG_HLIT_HDIST: return "dynamic block: HLIT/HDIST out of range";
+    case MSG_CODE16_FIRST: return "code 16 with no previous";
+    case MSG_CODE16_OVER: return "code 16 overruns lengths";
+    case MSG_CODE17_OVER: return "code 17 overruns lengths";
+    case MSG_CODE18_OVER: return "code 18 overruns lengths";
+    case MSG_BAD_CL_SYM: return "bad code-length symbol";
+    case MSG_EOB_ZERO: return "EOB symbol has zero length";
+    case MSG_DIST_FAR: return "back-reference distance out of bounds";
+    case MSG_MARKER_WINDOW: return "marker references bytes outside the available prefix window";
+    default: return "invalid deflate stream";
+    }
+}
+
+void set_err(rrg_error* e, int code, const char* fmt, ...) {
+    if (!e) return;
+    std::memset(e, 0, sizeof(*e));
+    e->code = code;
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(e->message, sizeof(e->message), fmt, ap);
+    va_end(ap);
+}
+
+int status_err(rrg_error* e, int st, int msg, uint64_t where) {
+    switch (st) {
+    case DS_EOF: set_err(e, RRG_ERR_DEFLATE_EOF, "unexpected end of input"); break;
+    case DS_INVALID: set_err(e, RRG_ERR_DEFLATE_INVALID, "%s", msg_text(msg)); break;
+    case DS_TRUNCATED: set_err(e, RRG_ERR_TRUNCATED, "truncated gzip stream"); break;
+    case DS_BAD_MAGIC: set_err(e, RRG_ERR_BAD_MAGIC, "not a gzip file (bad magic)"); break;
+    case DS_METHOD:
+        set_err(e, RRG_ERR_UNSUPPORTED_METHOD, "unsupported compression method: %d", msg);
+        if (e) e->expected = (uint32_t)msg;
+        break;
+    case DS_FLAGS:
+        set_err(e, RRG_ERR_RESERVED_FLAGS, "reserved gzip flag bits set: %#x", msg);
+        if (e) e->expected = (uint32_t)msg;
+        break;
+    default: set_err(e, RRG_ERR_DEFLATE_INVALID, "decode status %d", st); break;
+    }
+    if (e) e->trailer_byte = where;
+    return e ? e->code : RRG_ERR_DEFLATE_INVALID;
+}
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// ---------------------------------------------------------------- host CRC
+uint32_t g_crc_tab[8][256];
+uint32_t g_x2k[67];
+std::once_flag g_tab_once;
+
+uint32_t host_mulmod(uint32_t a, uint32_t b) {
+    uint32_t p = 0;
+    for (int i = 0; i < 32; i++) {
+        if (a & (0x80000000u >> i)) p ^= b;
+        b = (b & 1u) ? (b >> 1) ^ 0xEDB88320u : (b >> 1);
+    }
+    return p;
+}
+
+void init_tables() {
+    for (uint32_t n = 0; n < 256; n++) {
+        uint32_t c = n;
+        for (int k = 0; k < 8; k++) c = (c & 1u) ? (c >> 1) ^ 0xEDB88320u : (c >> 1);
+        g_crc_tab[0][n] = c;
+    }
+    for (uint32_t n = 0; n < 256; n++) {
+        uint32_t c = g_crc_tab[0][n];
+        for (int t = 1; t < 8; t++) {
+            c = g_crc_tab[0][c & 0xff] ^ (c >> 8);
+            g_crc_tab[t][n] = c;
+        }
+    }
+    g_x2k[0] = 0x40000000u;
+    for (int k = 1; k < 67; k++) g_x2k[k] = host_mulmod(g_x2k[k - 1], g_x2k[k - 1]);
+}
+
+// 13-bit prefilter skip table (block_finder.rs:60-101).
+uint8_t g_next_lut[8192];
+std::once_flag g_lut_once;
+void init_next_lut() {
+    auto cand = [](uint32_t b) {
+        return !(b & 1) && ((b >> 1) & 3) == 2 && ((b >> 3) & 31) <= 29 && ((b >> 8) & 31) <= 29;
+    };
+    for (uint32_t i = 0; i < 8192; i++) {
+        uint32_t s = 0, v = i;
+        while (s < 13 && !cand(v)) {
+            v >>= 1;
+            s++;
+        }
+        g_next_lut[i] = (uint8_t)s;
+    }
+}
+
+// gzip.rs:252-300
+int host_parse_header(const uint8_t* in, size_t len, size_t* hl, int* detail) {
+    *detail = 0;
+    if (len < 10) return DS_TRUNCATED;
+    if (in[0] != 0x1f || in[1] != 0x8b) return DS_BAD_MAGIC;
+    if (in[2] != 8) {
+        *detail = in[2];
+        return DS_METHOD;
+    }
+    uint8_t flg = in[3];
+    if (flg & 0xe0) {
+        *detail = flg;
+        return DS_FLAGS;
+    }
+    size_t pos = 10;
+    if (flg & 4) {
+        if (pos + 2 > len) return DS_TRUNCATED;
+        pos += 2 + ((size_t)in[pos] | ((size_t)in[pos + 1] << 8));
+        if (pos > len) return DS_TRUNCATED;
+    }
+    for (int f = 8; f <= 16; f <<= 1) {
+        if (flg & f) {
+            const void* z = pos < len ? std::memchr(in + pos, 0, len - pos) : nullptr;
+            if (!z) return DS_TRUNCATED;
+            pos = (size_t)((const uint8_t*)z - in) + 1;
+        }
+    }
+    if (flg & 2) {
+        if (pos + 2 > len) return DS_TRUNCATED;
+        pos += 2;
+    }
+    *hl = pos;
+    return DS_OK;
+}
+
+// gzip.rs:311-351 parse_bgzf_block_size; -1 = None.
+int64_t host_bgzf_size(const uint8_t* in, size_t len) {
+    if (len < 12 || in[0] != 0x1f || in[1] != 0x8b || in[2] != 8 || !(in[3] & 4)) return -1;
+    size_t xlen = (size_t)in[10] | ((size_t)in[11] << 8);
+    if (12 + xlen > len) return -1;
+    size_t p = 12, end = 12 + xlen;
+    while (p + 4 <= end) {
+        size_t slen = (size_t)in[p + 2] | ((size_t)in[p + 3] << 8);
+        if (p + 4 + slen > end) return -1;
+        if (in[p] == 'B' && in[p + 1] == 'C' && slen == 2) return (int64_t)(in[p + 4] | (in[p + 5] << 8)) + 1;
+        p += 4 + slen;
+    }
+    return -1;
+}
+
+uint32_t le32(const uint8_t* p) {
+    return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
+}
+
+struct DBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+};
+
+}  // namespace
+
+// ====================================================================== ctx
+struct rrg_ctx {
+    rrg_config cfg{};
+    int device = 0;
+    int n_sm = 148;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    bool tables_uploaded = false;
+
+    // device buffers (grow-only)
+    DBuf items, results, order, queue, mbs, mbcount, cells, out, targets, limits, found, next_lut, chunks,
+        tiles, rerr, markers, crc_table, pieces, piece_crc, mpiece, exp_crc, exp_isize, got_crc, got_len,
+        mstatus, comp;
+    // pinned host staging
+    uint8_t* h_stage[2] = {nullptr, nullptr};
+    size_t h_stage_cap = 0;
+    uint8_t* h_in = nullptr;
+    size_t h_in_cap = 0;
+
+    // tunables
+    uint64_t gpu_chunk = 0;
+    uint32_t inflate_warps = 4;
+    uint32_t finder_tile = 1024;
+    double expand = 6.0;
+
+    rrg_stats st{};
+    uint64_t launches = 0;
+
+    // serving
+    std::mutex srv_mu;
+    struct Req {
+        int64_t id;
+        std::vector<uint8_t> data;
+        double t_submit;
+    };
+    std::deque<Req> srv_queue;
+    int64_t srv_next_id = 0;
+};
+
+namespace {
+
+cudaError_t dgrow(DBuf& b, size_t n) {
+    if (n == 0) n = 16;
+    if (n <= b.cap) return cudaSuccess;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    size_t c = n + n / 8 + 256;
+    cudaError_t e = cudaMalloc(&b.p, c);
+    if (e == cudaSuccess) b.cap = c;
+    return e;
+}
+
+int cuda_fail(rrg_error* err, cudaError_t e, const char* what) {
+    set_err(err, e == cudaErrorMemoryAllocation ? RRG_ERR_OUT_OF_MEMORY : RRG_ERR_CUDA, "%s: %s", what,
+            cudaGetErrorString(e));
+    return err ? err->code : RRG_ERR_CUDA;
+}
+
+#define CK(call)                                                 \
+    do {                                                         \
+        cudaError_t e_ = (call);                                 \
+        if (e_ != cudaSuccess) return cuda_fail(err, e_, #call); \
+    } while (0)
+
+#define LAUNCHED(ctx)                                                               \
+    do {                                                                            \
+        g_launches.fetch_add(1);                                                    \
+        (ctx)->launches++;                                                          \
+        cudaError_t e_ = cudaGetLastError();                                        \
+        if (e_ != cudaSuccess) return cuda_fail(err, e_, "kernel launch");         \
+    } while (0)
+
+// Device time of one kernel launch, measured with events on the launch stream.
+struct KTimer {
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaStream_t s;
+    explicit KTimer(cudaStream_t st) : s(st) {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, s);
+    }
+    void stop() { cudaEventRecord(b, s); }
+    // call after the stream has been synchronised
+    double ms() {
+        float f = 0;
+        cudaEventElapsedTime(&f, a, b);
+        return (double)f;
+    }
+    ~KTimer() {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    }
+};
+
+int upload_tables(rrg_ctx* c, rrg_error* err) {
+    if (c->tables_uploaded) return 0;
+    std::call_once(g_tab_once, init_tables);
+    std::call_once(g_lut_once, init_next_lut);
+    CK(cudaMemcpyToSymbol(c_x2k, g_x2k, sizeof(g_x2k)));
+    CK(dgrow(c->crc_table, sizeof(g_crc_tab)));
+    CK(cudaMemcpy(c->crc_table.p, g_crc_tab, sizeof(g_crc_tab), cudaMemcpyHostToDevice));
+    CK(dgrow(c->next_lut, sizeof(g_next_lut)));
+    CK(cudaMemcpy(c->next_lut.p, g_next_lut, sizeof(g_next_lut), cudaMemcpyHostToDevice));
+    c->tables_uploaded = true;
+    return 0;
+}
+
+uint32_t persistent_blocks(rrg_ctx* c, uint32_t per_sm, uint64_t work_units, uint32_t units_per_block) {
+    uint64_t need = (work_units + units_per_block - 1) / units_per_block;
+    uint64_t cap = (uint64_t)c->n_sm * per_sm;
+    return (uint32_t)std::max<uint64_t>(1, std::min(need, cap));
+}
+
+// ------------------------------------------------------------ inflate launch
+int launch_inflate(rrg_ctx* c, const uint8_t* d_in, const std::vector<ChunkItem>& items, bool bytes_out,
+                   void* d_out_cells, std::vector<ChunkResult>& res, std::vector<MemberRec>* mrecs,
+                   rrg_error* err) {
+    const uint32_t n = (uint32_t)items.size();
+    res.assign(n, ChunkResult{});
+    if (!n) return 0;
+    // largest spans first: long chunks start early, short ones fill the tail
+    std::vector<uint32_t> order(n);
+    for (uint32_t i = 0; i < n; i++) order[i] = i;
+    auto span = [&](uint32_t i) {
+        uint64_t e = items[i].end_hint == ~0ull ? items[i].in_len * 8 : items[i].end_hint;
+        return e > items[i].start_bit ? e - items[i].start_bit : 0;
+    };
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return span(a) > span(b); });
+    uint32_t mb_cap = mrecs ? (uint32_t)std::max<size_t>(4096, mrecs->capacity()) : 0;
+    for (int attempt = 0; attempt < 2; attempt++) {
+        CK(dgrow(c->items, n * sizeof(ChunkItem)));
+        CK(dgrow(c->results, n * sizeof(ChunkResult)));
+        CK(dgrow(c->order, n * sizeof(uint32_t)));
+        CK(dgrow(c->queue, 16));
+        CK(dgrow(c->mbs, (size_t)std::max<uint32_t>(mb_cap, 1) * sizeof(MemberRec)));
+        CK(dgrow(c->mbcount, 16));
+        CK(cudaMemcpyAsync(c->items.p, items.data(), n * sizeof(ChunkItem), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->order.p, order.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemsetAsync(c->queue.p, 0, 16, c->stream));
+        CK(cudaMemsetAsync(c->mbcount.p, 0, 16, c->stream));
+        InflateArgs A;
+        A.in = d_in;
+        A.items = (const ChunkItem*)c->items.p;
+        A.results = (ChunkResult*)c->results.p;
+        A.n_items = n;
+        A.order = (const uint32_t*)c->order.p;
+        A.queue = (uint32_t*)c->queue.p;
+        A.out = d_out_cells;
+        A.mbs = (MemberRec*)c->mbs.p;
+        A.mb_count = (uint32_t*)c->mbcount.p;
+        A.mb_cap = mb_cap;
+        const uint32_t W = c->inflate_warps;
+        const size_t smem = W * sizeof(WarpSmem);
+        const uint32_t per_sm = std::max<uint32_t>(1, (uint32_t)((200 * 1024) / smem));
+        const uint32_t grid = persistent_blocks(c, per_sm, n, W);
+        KTimer kt(c->stream);
+        if (bytes_out) {
+            RRG_LAUNCH(k_inflate<uint8_t>, grid, W * 32, smem, c->stream, A);
+        } else {
+            RRG_LAUNCH(k_inflate<uint16_t>, grid, W * 32, smem, c->stream, A);
+        }
+        kt.stop();
+        LAUNCHED(c);
+        CK(cudaMemcpyAsync(res.data(), c->results.p, n * sizeof(ChunkResult), cudaMemcpyDeviceToHost, c->stream));
+        uint32_t cnt = 0;
+        CK(cudaMemcpyAsync(&cnt, c->mbcount.p, 4, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        c->st.inflate_ms += kt.ms();
+        if (!mrecs) return 0;
+        if (cnt <= mb_cap) {
+            mrecs->resize(cnt);
+            if (cnt)
+                CK(cudaMemcpy(mrecs->data(), c->mbs.p, cnt * sizeof(MemberRec), cudaMemcpyDeviceToHost));
+            return 0;
+        }
+        mb_cap = cnt + 1024;  // member records overflowed: once more with room for all
+    }
+    set_err(err, RRG_ERR_OUT_OF_MEMORY, "member record buffer overflow");
+    return RRG_ERR_OUT_OF_MEMORY;
+}
+
+// ------------------------------------------------------------ CRC check
+struct MemberSpan {
+    uint64_t out_start, len;
+    uint32_t crc, isize;
+    uint64_t trailer_byte;
+};
+
+int check_members(rrg_ctx* c, const uint8_t* d_out, const std::vector<MemberSpan>& ms, uint32_t member_base,
+                  rrg_error* err) {
+    const uint32_t nm = (uint32_t)ms.size();
+    if (!nm) return 0;
+    const uint64_t PIECE = 256 * 1024;
+    std::vector<CrcPiece> pieces;
+    std::vector<uint32_t> mstart(nm + 1);
+    std::vector<uint32_t> ecrc(nm), eisz(nm);
+    for (uint32_t m = 0; m < nm; m++) {
+        mstart[m] = (uint32_t)pieces.size();
+        for (uint64_t o = 0; o < ms[m].len; o += PIECE)
+            pieces.push_back(CrcPiece{ms[m].out_start + o, std::min(PIECE, ms[m].len - o)});
+        ecrc[m] = ms[m].crc;
+        eisz[m] = ms[m].isize;
+    }
+    mstart[nm] = (uint32_t)pieces.size();
+    const uint32_t np = (uint32_t)pieces.size();
+    double t0 = now_ms();
+    CK(dgrow(c->pieces, std::max<size_t>(np, 1) * sizeof(CrcPiece)));
+    CK(dgrow(c->piece_crc, std::max<size_t>(np, 1) * 4));
+    CK(dgrow(c->mpiece, (nm + 1) * 4));
+    CK(dgrow(c->exp_crc, nm * 4));
+    CK(dgrow(c->exp_isize, nm * 4));
+    CK(dgrow(c->got_crc, nm * 4));
+    CK(dgrow(c->got_len, nm * 8));
+    CK(dgrow(c->mstatus, nm * 4));
+    if (np) CK(cudaMemcpyAsync(c->pieces.p, pieces.data(), np * sizeof(CrcPiece), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->mpiece.p, mstart.data(), (nm + 1) * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->exp_crc.p, ecrc.data(), nm * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->exp_isize.p, eisz.data(), nm * 4, cudaMemcpyHostToDevice, c->stream));
+    KTimer kt(c->stream);
+    if (np) {
+        CrcArgs A{d_out, (const CrcPiece*)c->pieces.p, np, (uint32_t*)c->piece_crc.p, (const uint32_t*)c->crc_table.p};
+        uint32_t grid = persistent_blocks(c, 8, np, 1);
+        RRG_LAUNCH(k_crc_pieces, grid, CRC_THREADS, 0, c->stream, A);
+        LAUNCHED(c);
+    }
+    CrcMemberArgs B{(const CrcPiece*)c->pieces.p, (const uint32_t*)c->piece_crc.p, (const uint32_t*)c->mpiece.p, nm,
+                    (const uint32_t*)c->exp_crc.p, (const uint32_t*)c->exp_isize.p, (uint32_t*)c->got_crc.p,
+                    (uint64_t*)c->got_len.p, (int32_t*)c->mstatus.p};
+    RRG_LAUNCH(k_crc_members, (nm * 32 + 255) / 256, 256, 0, c->stream, B);
+    kt.stop();
+    LAUNCHED(c);
+    std::vector<int32_t> stv(nm);
+    std::vector<uint32_t> got(nm);
+    std::vector<uint64_t> glen(nm);
+    CK(cudaMemcpyAsync(stv.data(), c->mstatus.p, nm * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(got.data(), c->got_crc.p, nm * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(glen.data(), c->got_len.p, nm * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->st.crc_ms += kt.ms();
+    (void)t0;
+    c->st.members += nm;
+    for (uint32_t m = 0; m < nm; m++) {
+        if (stv[m] == DS_CRC) {
+            set_err(err, RRG_ERR_CRC_MISMATCH,
+                    "CRC32 mismatch in member #%u (uncompressed bytes: %llu, trailer at byte %llu): expected "
+                    "%#010x, got %#010x",
+                    member_base + m, (unsigned long long)glen[m], (unsigned long long)ms[m].trailer_byte,
+                    ms[m].crc, got[m]);
+            err->member = member_base + m;
+            err->expected = ms[m].crc;
+            err->got_crc = got[m];
+            err->uncompressed = glen[m];
+            err->trailer_byte = ms[m].trailer_byte;
+            return RRG_ERR_CRC_MISMATCH;
+        }
+        if (stv[m] == DS_ISIZE) {
+            set_err(err, RRG_ERR_ISIZE_MISMATCH,
+                    "ISIZE mismatch in member #%u (trailer at byte %llu): expected %u, got %llu", member_base + m,
+                    (unsigned long long)ms[m].trailer_byte, ms[m].isize, (unsigned long long)glen[m]);
+            err->member = member_base + m;
+            err->expected = ms[m].isize;
+            err->got = glen[m];
+            err->uncompressed = glen[m];
+            err->trailer_byte = ms[m].trailer_byte;
+            return RRG_ERR_ISIZE_MISMATCH;
+        }
+    }
+    return 0;
+}
+
+// ------------------------------------------------------------ output target
+// Where decoded bytes go: a caller buffer of fixed capacity, or the context's
+// own buffer, which grows on demand keeping the bytes already written.
+struct OutTarget {
+    uint8_t* p;
+    uint64_t cap;
+    bool grow;
+};
+
+int ensure_out(rrg_ctx* c, OutTarget& t, uint64_t need, uint64_t keep, rrg_error* err) {
+    if (need <= t.cap) return 0;
+    if (!t.grow) {
+        set_err(err, RRG_ERR_CAPACITY, "output buffer too small: need %llu bytes", (unsigned long long)need);
+        return RRG_ERR_CAPACITY;
+    }
+    void* np = nullptr;
+    size_t nc = need + need / 8 + 4096;
+    CK(cudaMalloc(&np, nc));
+    if (keep && t.p) {
+        CK(cudaMemcpyAsync(np, t.p, keep, cudaMemcpyDeviceToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    if (c->out.p) cudaFree(c->out.p);
+    c->out.p = np;
+    c->out.cap = nc;
+    t.p = (uint8_t*)np;
+    t.cap = nc;
+    return 0;
+}
+
+// ------------------------------------------------------------ member route
+struct Decoded {
+    uint64_t total = 0;  // bytes written at d_dst
+    uint64_t consumed = 0;
+    uint32_t members = 0;
+};
+
+uint64_t round8(uint64_t v) { return (v + 7) & ~7ull; }
+
+// Decodes the gzip member stream whose first member body starts at byte
+// `body_off` of d_file (the first member's header already parsed) into
+// tgt.p[dst_off ..]. On RRG_ERR_CAPACITY `out->total` holds the size required.
+int member_route(rrg_ctx* c, const uint8_t* d_file, uint64_t len, uint64_t body_off, OutTarget& tgt, uint64_t dst_off,
+                 uint32_t member_base, Decoded* out, rrg_error* err) {
+    const uint8_t* body = d_file + body_off;
+    const uint64_t blen = len - body_off;
+    const uint64_t total_bits = blen * 8;
+    const uint64_t G = std::max<uint64_t>(c->gpu_chunk ? c->gpu_chunk : (1ull << 17), 4096);
+    // ---- sub-chunk boundaries: first dynamic block at/after every G bytes
+    std::vector<uint64_t> targets, limits, found;
+    for (uint64_t t = G * 8; t < total_bits; t += G * 8) targets.push_back(t);
+    for (size_t i = 0; i < targets.size(); i++) limits.push_back(i + 1 < targets.size() ? targets[i + 1] : total_bits);
+    found.assign(targets.size(), ~0ull);
+    if (!targets.empty()) {
+        const uint32_t n = (uint32_t)targets.size();
+        double t0 = now_ms();
+        CK(dgrow(c->targets, n * 8));
+        CK(dgrow(c->limits, n * 8));
+        CK(dgrow(c->found, n * 8));
+        CK(dgrow(c->queue, 16));
+        CK(cudaMemcpyAsync(c->targets.p, targets.data(), n * 8, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->limits.p, limits.data(), n * 8, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemsetAsync(c->queue.p, 0, 16, c->stream));
+        FindArgs F{body, blen, (const uint64_t*)c->targets.p, (const uint64_t*)c->limits.p, (uint64_t*)c->found.p, n,
+                   (uint32_t*)c->queue.p, (const uint8_t*)c->next_lut.p, c->finder_tile};
+        const uint32_t W = 8;
+        uint32_t grid = persistent_blocks(c, 4, n, W);
+        KTimer kt(c->stream);
+        RRG_LAUNCH(k_find_blocks, grid, W * 32, W * sizeof(FindSmem), c->stream, F);
+        kt.stop();
+        LAUNCHED(c);
+        CK(cudaMemcpyAsync(found.data(), c->found.p, n * 8, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        c->st.finder_ms += kt.ms();
+        (void)t0;
+    }
+    std::vector<uint64_t> starts{0};
+    for (uint64_t f : found)
+        if (f != ~0ull && f > starts.back()) starts.push_back(f);
+    const size_t n = starts.size();
+    // ---- slot arena: every chunk gets expand x its compressed span, plus room for re-decodes
+    std::vector<ChunkItem> items(n);
+    uint64_t arena = 0;
+    for (size_t k = 0; k < n; k++) {
+        ChunkItem& it = items[k];
+        it.in_off = body_off;
+        it.in_len = blen;
+        it.start_bit = starts[k];
+        it.end_hint = k + 1 < n ? starts[k + 1] : ~0ull;
+        uint64_t span = ((k + 1 < n ? starts[k + 1] : total_bits) - starts[k] + 7) / 8;
+        it.out_cap = round8((uint64_t)(span * c->expand) + 65536);
+        it.out_off = arena;
+        it.flags = ITEM_MARKERS;
+        it.id = (uint32_t)k;
+        arena += it.out_cap;
+    }
+    uint64_t arena_cap = arena + arena / 4 + (1u << 20);
+    CK(dgrow(c->cells, arena_cap * 2));
+    std::vector<ChunkResult> res;
+    std::vector<MemberRec> mrecs;
+    mrecs.reserve(4096);
+    int rc = launch_inflate(c, d_file, items, false, c->cells.p, res, &mrecs, err);
+    if (rc) return rc;
+    c->st.gpu_chunks += n;
+
+    // ---- anchored chain (pipeline.rs:758-809)
+    struct Acc {
+        ChunkItem it;
+        ChunkResult r;
+        std::vector<MemberRec> m;
+    };
+    std::unordered_map<uint32_t, std::vector<MemberRec>> by_item;
+    auto bucket = [&](const std::vector<MemberRec>& all) {
+        for (const MemberRec& m : all) by_item[m.item].push_back(m);
+    };
+    auto take_recs = [&](uint32_t id) {
+        std::vector<MemberRec> v;
+        auto f = by_item.find(id);
+        if (f != by_item.end()) {
+            v.swap(f->second);
+            std::sort(v.begin(), v.end(), [](const MemberRec& a, const MemberRec& b) { return a.seq < b.seq; });
+        }
+        return v;
+    };
+    bucket(mrecs);
+    std::vector<Acc> acc;  // accepted chunks in stream order
+    uint64_t expected = 0;
+    bool final_seen = false;
+    uint32_t next_id = (uint32_t)n;
+    std::vector<size_t> overflow_pending;  // indices into acc needing a bigger slot
+    for (size_t k = 0; k < n && !final_seen; k++) {
+        ChunkItem it = items[k];
+        ChunkResult r = res[k];
+        if (it.start_bit == expected && (r.status == DS_OK || r.status == DS_OVERFLOW)) {
+            acc.push_back(Acc{it, r, take_recs(it.id)});
+        } else {
+            // false boundary or failed speculative decode: re-decode from the anchor
+            c->st.speculation_failures++;
+            if (it.end_hint != ~0ull && expected >= it.end_hint) continue;  // empty chunk
+            it.start_bit = expected;
+            it.id = next_id++;
+            if (arena + it.out_cap > arena_cap) {
+                set_err(err, RRG_ERR_OUT_OF_MEMORY, "re-decode arena exhausted");
+                return RRG_ERR_OUT_OF_MEMORY;
+            }
+            it.out_off = arena;
+            arena += it.out_cap;
+            std::vector<ChunkItem> one{it};
+            std::vector<ChunkResult> r1;
+            std::vector<MemberRec> m1;
+            m1.reserve(4096);
+            rc = launch_inflate(c, d_file, one, false, c->cells.p, r1, &m1, err);
+            if (rc) return rc;
+            r = r1[0];
+            if (r.status != DS_OK && r.status != DS_OVERFLOW)
+                return status_err(err, r.status, r.msg, body_off + r.err_bit / 8);
+            bucket(m1);
+            acc.push_back(Acc{it, r, take_recs(it.id)});
+        }
+        if (acc.back().r.status == DS_OVERFLOW) overflow_pending.push_back(acc.size() - 1);
+        expected = acc.back().r.actual_end_bit;
+        final_seen = acc.back().r.final_block != 0;
+    }
+    if (!final_seen) {
+        set_err(err, RRG_ERR_IO, "parallel decode produced no final block");
+        return RRG_ERR_IO;
+    }
+    // ---- overflowed slots: decode again with the exact size now known
+    if (!overflow_pending.empty()) {
+        std::vector<ChunkItem> redo;
+        for (size_t a : overflow_pending) {
+            ChunkItem it = acc[a].it;
+            it.out_cap = round8(acc[a].r.n_cells + 8);
+            it.id = next_id++;
+            redo.push_back(it);
+        }
+        uint64_t need = 0;
+        for (auto& it : redo) need += it.out_cap;
+        if (arena + need > arena_cap) {
+            // the slots were far too small for this data: decode everything
+            // again with a larger expansion estimate (DEFLATE expands <= 1032x)
+            if (c->expand >= 1100.0) {
+                set_err(err, RRG_ERR_OUT_OF_MEMORY, "output slot arena exhausted");
+                return RRG_ERR_OUT_OF_MEMORY;
+            }
+            c->expand = std::min(1100.0, c->expand * 8);
+            return member_route(c, d_file, len, body_off, tgt, dst_off, member_base, out, err);
+        }
+        for (auto& it : redo) {
+            it.out_off = arena;
+            arena += it.out_cap;
+        }
+        std::vector<ChunkResult> r2;
+        std::vector<MemberRec> m2;
+        m2.reserve(4096);
+        rc = launch_inflate(c, d_file, redo, false, c->cells.p, r2, &m2, err);
+        if (rc) return rc;
+        bucket(m2);
+        for (size_t i = 0; i < redo.size(); i++) {
+            if (r2[i].status != DS_OK) return status_err(err, r2[i].status, r2[i].msg, body_off + r2[i].err_bit / 8);
+            Acc& a = acc[overflow_pending[i]];
+            a.it = redo[i];
+            a.r = r2[i];
+            a.m = take_recs(redo[i].id);
+        }
+    }
+    // ---- output layout and member spans
+    std::vector<ResolveChunk> rchunks;
+    std::vector<uint64_t> tile_start{0};
+    std::vector<MemberSpan> spans;
+    uint64_t pos = 0, mstart = 0;
+    for (const Acc& a : acc) {
+        if (a.r.n_cells) {
+            ResolveChunk rc2{dst_off + pos, a.it.out_off, a.r.n_cells, dst_off + mstart};
+            rchunks.push_back(rc2);
+            tile_start.push_back(tile_start.back() + (a.r.n_cells + RES_TILE - 1) / RES_TILE);
+        }
+        for (const MemberRec& m : a.m) {
+            uint64_t end = pos + m.cell_off;
+            spans.push_back(MemberSpan{dst_off + mstart, end - mstart, m.crc, m.isize, body_off + m.trailer_byte});
+            mstart = end;
+        }
+        pos += a.r.n_cells;
+    }
+    out->total = pos;
+    out->consumed = body_off + expected / 8;
+    out->members = (uint32_t)spans.size();
+    rc = ensure_out(c, tgt, dst_off + pos, dst_off, err);
+    if (rc) return rc;
+    uint8_t* d_dst = tgt.p;
+    // ---- resolve markers + compact
+    if (!rchunks.empty()) {
+        double t0 = now_ms();
+        const uint32_t nc = (uint32_t)rchunks.size();
+        CK(dgrow(c->chunks, nc * sizeof(ResolveChunk)));
+        CK(dgrow(c->tiles, (nc + 1) * 8));
+        CK(dgrow(c->rerr, 16));
+        CK(dgrow(c->markers, 8));
+        CK(cudaMemcpyAsync(c->chunks.p, rchunks.data(), nc * sizeof(ResolveChunk), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->tiles.p, tile_start.data(), (nc + 1) * 8, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemsetAsync(c->rerr.p, 0, 16, c->stream));
+        CK(cudaMemsetAsync(c->markers.p, 0, 8, c->stream));
+        // chunk table holds global positions relative to d_dst
+        ResolveArgs R{(const uint16_t*)c->cells.p, (const ResolveChunk*)c->chunks.p, (const uint64_t*)c->tiles.p, nc,
+                      tile_start.back(), d_dst, (uint32_t*)c->rerr.p, (unsigned long long*)c->markers.p};
+        uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(tile_start.back(), (uint64_t)c->n_sm * 16));
+        KTimer kt(c->stream);
+        RRG_LAUNCH(k_resolve, grid, RES_THREADS, 0, c->stream, R);
+        kt.stop();
+        LAUNCHED(c);
+        uint32_t e4[4];
+        unsigned long long nmk = 0;
+        CK(cudaMemcpyAsync(e4, c->rerr.p, 16, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(&nmk, c->markers.p, 8, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        c->st.resolve_ms += kt.ms();
+        (void)t0;
+        c->st.markers += nmk;
+        if (e4[0]) {
+            set_err(err, RRG_ERR_DEFLATE_INVALID, "%s", msg_text(MSG_MARKER_WINDOW));
+            return RRG_ERR_DEFLATE_INVALID;
+        }
+    }
+    // spans carry positions relative to d_dst
+    return check_members(c, d_dst, spans, member_base, err);
+}
+
+// ------------------------------------------------------------ BGZF route
+struct BgzfMember {
+    uint64_t off, size;
+    uint32_t isize, crc;
+};
+
+// Walk BGZF members from offset 0 (pipeline.rs:1524-1541). Needs the whole
+// file in host memory. Returns the remainder offset.
+uint64_t bgzf_walk(const uint8_t* h, uint64_t len, std::vector<BgzfMember>& ms, bool* truncated) {
+    uint64_t pos = 0;
+    *truncated = false;
+    while (pos < len) {
+        int64_t sz = host_bgzf_size(h + pos, len - pos);
+        if (sz < 0) break;
+        if (pos + (uint64_t)sz > len) {
+            *truncated = true;
+            break;
+        }
+        BgzfMember m{pos, (uint64_t)sz, 0, 0};
+        if (sz >= 8) {
+            m.crc = le32(h + pos + sz - 8);
+            m.isize = le32(h + pos + sz - 4);
+        }
+        ms.push_back(m);
+        pos += (uint64_t)sz;
+    }
+    return pos;
+}
+
+int bgzf_route(rrg_ctx* c, const uint8_t* d_file, const std::vector<BgzfMember>& ms, OutTarget& tgt, Decoded* out,
+               rrg_error* err) {
+    const size_t nm = ms.size();
+    std::vector<ChunkItem> items(nm);
+    uint64_t pos = 0;
+    for (size_t i = 0; i < nm; i++) {
+        ChunkItem& it = items[i];
+        it.in_off = ms[i].off;
+        it.in_len = ms[i].size;
+        it.start_bit = 0;
+        it.end_hint = ~0ull;
+        it.out_off = pos;
+        it.out_cap = ms[i].isize;
+        it.flags = ITEM_ONE_MEMBER;
+        it.id = (uint32_t)i;
+        pos += ms[i].isize;
+    }
+    out->total = pos;
+    out->members = (uint32_t)nm;
+    out->consumed = nm ? ms.back().off + ms.back().size : 0;
+    int rc0 = ensure_out(c, tgt, pos, 0, err);
+    if (rc0) return rc0;
+    uint8_t* d_dst = tgt.p;
+    std::vector<ChunkResult> res;
+    int rc = launch_inflate(c, d_file, items, true, d_dst, res, nullptr, err);
+    if (rc) return rc;
+    c->st.gpu_chunks += nm;
+    std::vector<MemberSpan> spans(nm);
+    for (size_t i = 0; i < nm; i++) {
+        const ChunkResult& r = res[i];
+        uint64_t trailer = ms[i].off + ms[i].size - 8;
+        if (r.status == DS_OVERFLOW) {
+            set_err(err, RRG_ERR_ISIZE_MISMATCH, "ISIZE mismatch in member #%zu (trailer at byte %llu): expected %u, got %llu",
+                    i, (unsigned long long)trailer, ms[i].isize, (unsigned long long)r.n_cells);
+            err->member = (uint32_t)i;
+            err->expected = ms[i].isize;
+            err->got = r.n_cells;
+            err->trailer_byte = trailer;
+            return RRG_ERR_ISIZE_MISMATCH;
+        }
+        if (r.status != DS_OK) return status_err(err, r.status, r.msg, ms[i].off + r.err_bit / 8);
+        uint32_t tcrc = (uint32_t)r.markers, tisz = (uint32_t)(r.markers >> 32);
+        spans[i] = MemberSpan{items[i].out_off, r.n_cells, tcrc, tisz, trailer};
+    }
+    return check_members(c, d_dst, spans, 0, err);
+}
+
+// ------------------------------------------------------------ whole file
+// Decode a whole gzip file at d_file (device) into d_dst. `h_file` (optional)
+// is the same bytes in host memory, used for the BGZF walk.
+int decode_file(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_t* h_file, OutTarget& tgt, Decoded* out,
+                rrg_error* err) {
+    *out = Decoded{};
+    if (len == 0) {
+        set_err(err, RRG_ERR_TRUNCATED, "truncated gzip stream");
+        return RRG_ERR_TRUNCATED;
+    }
+    int rc = upload_tables(c, err);
+    if (rc) return rc;
+    // first bytes to the host for header parsing / BGZF sniff
+    std::vector<uint8_t> head;
+    const uint8_t* hp = h_file;
+    uint64_t hlen = len;
+    if (!hp) {
+        hlen = std::min<uint64_t>(len, 1 << 16);
+        head.resize(hlen);
+        CK(cudaMemcpy(head.data(), d_file, hlen, cudaMemcpyDeviceToHost));
+        hp = head.data();
+    }
+    if (host_bgzf_size(hp, hlen) >= 0) {
+        std::vector<uint8_t> whole;
+        if (!h_file) {
+            whole.resize(len);
+            CK(cudaMemcpy(whole.data(), d_file, len, cudaMemcpyDeviceToHost));
+            h_file = whole.data();
+        }
+        std::vector<BgzfMember> ms;
+        bool trunc = false;
+        uint64_t rem = bgzf_walk(h_file, len, ms, &trunc);
+        Decoded d1;
+        rc = bgzf_route(c, d_file, ms, tgt, &d1, err);
+        if (rc) {
+            out->total = d1.total;
+            return rc;
+        }
+        if (trunc) {
+            set_err(err, RRG_ERR_TRUNCATED, "truncated gzip stream");
+            return RRG_ERR_TRUNCATED;
+        }
+        out->total = d1.total;
+        out->members = d1.members;
+        if (rem < len) {
+            size_t hl;
+            int detail;
+            int st = host_parse_header(h_file + rem, len - rem, &hl, &detail);
+            if (st) return status_err(err, st, detail, rem);
+            Decoded d2;
+            rc = member_route(c, d_file, len, rem + hl, tgt, d1.total, d1.members, &d2, err);
+            out->total = d1.total + d2.total;
+            out->members += d2.members;
+            if (rc) return rc;
+        }
+        return 0;
+    }
+    size_t hl = 0;
+    int detail = 0;
+    int st = host_parse_header(hp, hlen, &hl, &detail);
+    if (st == DS_TRUNCATED && hlen < len) {
+        head.resize(len);
+        CK(cudaMemcpy(head.data(), d_file, len, cudaMemcpyDeviceToHost));
+        st = host_parse_header(head.data(), len, &hl, &detail);
+    }
+    if (st) return status_err(err, st, detail, 0);
+    return member_route(c, d_file, len, hl, tgt, 0, 0, out, err);
+}
+
+int ensure_stage(rrg_ctx* c, size_t n, rrg_error* err) {
+    if (c->h_stage_cap >= n) return 0;
+    for (auto& p : c->h_stage)
+        if (p) cudaFreeHost(p);
+    c->h_stage[0] = c->h_stage[1] = nullptr;
+    c->h_stage_cap = 0;
+    CK(cudaMallocHost((void**)&c->h_stage[0], n));
+    CK(cudaMallocHost((void**)&c->h_stage[1], n));
+    c->h_stage_cap = n;
+    return 0;
+}
+
+// Stream d_src[0..n) to the sink in order through two pinned buffers.
+int deliver(rrg_ctx* c, const uint8_t* d_src, uint64_t n, rrg_sink_fn sink, void* user, bool* closed, rrg_error* err) {
+    *closed = false;
+    if (!n || !sink) return 0;
+    const uint64_t P = std::max<uint64_t>(1 << 20, std::min<uint64_t>(c->cfg.chunk_size_bytes * 2, 16ull << 20));
+    int rc = ensure_stage(c, P, err);
+    if (rc) return rc;
+    double t0 = now_ms();
+    uint64_t npieces = (n + P - 1) / P;
+    cudaEvent_t ev[2];
+    CK(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+    auto issue = [&](uint64_t i) -> cudaError_t {
+        uint64_t o = i * P, l = std::min(P, n - o);
+        cudaError_t e = cudaMemcpyAsync(c->h_stage[i & 1], d_src + o, l, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[i & 1], c->stream);
+        return e;
+    };
+    cudaError_t e = issue(0);
+    for (uint64_t i = 0; e == cudaSuccess && i < npieces; i++) {
+        e = cudaEventSynchronize(ev[i & 1]);
+        if (e != cudaSuccess) break;
+        if (i + 1 < npieces) {
+            e = issue(i + 1);
+            if (e != cudaSuccess) break;
+        }
+        uint64_t o = i * P, l = std::min(P, n - o);
+        c->st.chunks_decoded++;
+        if (sink(user, c->h_stage[i & 1], (size_t)l)) {
+            *closed = true;
+            break;
+        }
+    }
+    cudaStreamSynchronize(c->stream);
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    c->st.d2h_ms += now_ms() - t0;
+    if (e != cudaSuccess) return cuda_fail(err, e, "deliver");
+    return 0;
+}
+
+int decode_host_impl(rrg_ctx* c, const uint8_t* data, size_t len, rrg_sink_fn sink, void* user, rrg_stats* stats,
+                     rrg_error* err) {
+    double t_all = now_ms();
+    c->st = rrg_stats{};
+    c->launches = 0;
+    c->st.compressed_bytes = len;
+    if (len == 0) {
+        set_err(err, RRG_ERR_TRUNCATED, "truncated gzip stream");
+        if (stats) *stats = c->st;
+        return RRG_ERR_TRUNCATED;
+    }
+    double t0 = now_ms();
+    CK(dgrow(c->comp, len + 16));
+    CK(cudaMemcpyAsync(c->comp.p, data, len, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->st.h2d_ms = now_ms() - t0;
+    // output size is only known after the chain; decode into the context buffer
+    Decoded d;
+    OutTarget tgt{(uint8_t*)c->out.p, c->out.cap, true};
+    int rc = decode_file(c, (const uint8_t*)c->comp.p, len, data, tgt, &d, err);
+    bool closed = false;
+    if (!rc) {
+        c->st.uncompressed_bytes = d.total;
+        rc = deliver(c, tgt.p, d.total, sink, user, &closed, err);
+    }
+    c->st.kernel_launches = c->launches;
+    c->st.total_ms = now_ms() - t_all;
+    if (stats) *stats = c->st;
+    if (c->cfg.verbose)
+        std::fprintf(stderr,
+                     "[rrg-gpu] %zu -> %llu bytes, %llu sub-chunks, %llu speculation failures, %llu markers, "
+                     "finder %.3f ms, inflate %.3f ms, resolve %.3f ms, crc %.3f ms, total %.3f ms\n",
+                     len, (unsigned long long)c->st.uncompressed_bytes, (unsigned long long)c->st.gpu_chunks,
+                     (unsigned long long)c->st.speculation_failures, (unsigned long long)c->st.markers, c->st.finder_ms,
+                     c->st.inflate_ms, c->st.resolve_ms, c->st.crc_ms, c->st.total_ms);
+    return rc;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+rrg_ctx* rrg_gpu_create(const rrg_config* cfg, rrg_error* err) {
+    rrg_ctx* c = new rrg_ctx();
+    if (cfg) c->cfg = *cfg;
+    if (!c->cfg.chunk_size_bytes) c->cfg.chunk_size_bytes = 4ull << 20;
+    if (!c->cfg.hbm_budget_bytes) c->cfg.hbm_budget_bytes = 120ull * 1000 * 1000 * 1000;
+    c->gpu_chunk = c->cfg.gpu_chunk_bytes;
+    if (c->cfg.finder_tile_bits) c->finder_tile = (uint32_t)std::min<uint64_t>(FIND_TILE, (c->cfg.finder_tile_bits + 31) & ~31ull);
+    cudaError_t e;
+    if (c->cfg.device >= 0) {
+        e = cudaSetDevice(c->cfg.device);
+        if (e != cudaSuccess) {
+            cuda_fail(err, e, "cudaSetDevice");
+            delete c;
+            return nullptr;
+        }
+    }
+    cudaGetDevice(&c->device);
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device) == cudaSuccess && sms > 0) c->n_sm = sms;
+    e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        cuda_fail(err, e, "cudaStreamCreate");
+        delete c;
+        return nullptr;
+    }
+    c->stream = c->own_stream;
+    int smem_optin = 0;
+    cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+    size_t want = (size_t)c->inflate_warps * sizeof(WarpSmem);
+    if (smem_optin > 0 && want > 48 * 1024) {
+        cudaFuncSetAttribute(k_inflate<uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)want);
+        cudaFuncSetAttribute(k_inflate<uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)want);
+    }
+    if (err) std::memset(err, 0, sizeof(*err));
+    return c;
+}
+
+void rrg_gpu_destroy(rrg_ctx* c) {
+    if (!c) return;
+    DBuf* bufs[] = {&c->items,  &c->results, &c->order,     &c->queue,    &c->mbs,      &c->mbcount,   &c->cells,
+                    &c->out,    &c->targets, &c->limits,    &c->found,    &c->next_lut, &c->chunks,    &c->tiles,
+                    &c->rerr,   &c->markers, &c->crc_table, &c->pieces,   &c->piece_crc, &c->mpiece,   &c->exp_crc,
+                    &c->exp_isize, &c->got_crc, &c->got_len, &c->mstatus, &c->comp};
+    for (DBuf* b : bufs)
+        if (b->p) cudaFree(b->p);
+    for (auto& p : c->h_stage)
+        if (p) cudaFreeHost(p);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+}
+
+int rrg_gpu_decode_host(rrg_ctx* c, const uint8_t* data, size_t len, rrg_sink_fn sink, void* user, rrg_stats* stats,
+                        rrg_error* err) {
+    rrg_error local_err;
+    if (!err) err = &local_err;
+    if (!c || (!data && len)) {
+        set_err(err, RRG_ERR_INVALID_ARGUMENT, "null context or data");
+        return RRG_ERR_INVALID_ARGUMENT;
+    }
+    if (err) std::memset(err, 0, sizeof(*err));
+    return decode_host_impl(c, data, len, sink, user, stats, err);
+}
+
+int rrg_gpu_read_gz(rrg_ctx* c, const char* path, rrg_sink_fn sink, void* user, rrg_stats* stats, rrg_error* err) {
+    rrg_error local_err;
+    if (!err) err = &local_err;
+    if (!c || !path) {
+        set_err(err, RRG_ERR_INVALID_ARGUMENT, "null context or path");
+        return RRG_ERR_INVALID_ARGUMENT;
+    }
+    int fd = open(path, O_RDONLY);
+    if (fd < 0) {
+        set_err(err, RRG_ERR_IO, "io: cannot open %s: %s", path, std::strerror(errno));
+        return RRG_ERR_IO;
+    }
+    struct stat sb;
+    if (fstat(fd, &sb) != 0) {
+        set_err(err, RRG_ERR_IO, "io: stat %s: %s", path, std::strerror(errno));
+        close(fd);
+        return RRG_ERR_IO;
+    }
+    std::vector<uint8_t> data;
+    if (S_ISREG(sb.st_mode)) {
+        data.resize((size_t)sb.st_size);
+        size_t got = 0;
+        while (got < data.size()) {
+            ssize_t r = read(fd, data.data() + got, data.size() - got);
+            if (r <= 0) break;
+            got += (size_t)r;
+        }
+        data.resize(got);
+    } else {
+        // pipes / character devices: read to EOF (lib.rs:383-431 streams these)
+        uint8_t buf[1 << 16];
+        for (;;) {
+            ssize_t r = read(fd, buf, sizeof(buf));
+            if (r <= 0) break;
+            data.insert(data.end(), buf, buf + r);
+        }
+    }
+    close(fd);
+    if (err) std::memset(err, 0, sizeof(*err));
+    return decode_host_impl(c, data.data(), data.size(), sink, user, stats, err);
+}
+
+int rrg_gpu_decode_device(rrg_ctx* c, const uint8_t* d_in, size_t len, uint8_t* d_out, size_t out_cap, size_t* out_len,
+                          void* stream, rrg_stats* stats, rrg_error* err) {
+    rrg_error local_err;
+    if (!err) err = &local_err;
+    if (!c || (!d_in && len)) {
+        set_err(err, RRG_ERR_INVALID_ARGUMENT, "null context or input");
+        return RRG_ERR_INVALID_ARGUMENT;
+    }
+    if (err) std::memset(err, 0, sizeof(*err));
+    double t_all = now_ms();
+    c->st = rrg_stats{};
+    c->launches = 0;
+    c->st.compressed_bytes = len;
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    Decoded d;
+    OutTarget tgt{d_out, out_cap, false};
+    int rc = decode_file(c, d_in, len, nullptr, tgt, &d, err);
+    c->stream = c->own_stream;
+    if (out_len) *out_len = (size_t)d.total;
+    c->st.uncompressed_bytes = rc ? 0 : d.total;
+    c->st.kernel_launches = c->launches;
+    c->st.total_ms = now_ms() - t_all;
+    if (stats) *stats = c->st;
+    return rc;
+}
+
+int rrg_gpu_decode_batch(rrg_ctx* c, const uint8_t* d_in, const uint64_t* in_off, const uint64_t* in_len, uint8_t* d_out,
+                         const uint64_t* out_off, const uint64_t* out_cap, uint64_t* out_len, int32_t* status, size_t n,
+                         void* stream, rrg_stats* stats, rrg_error* err) {
+    rrg_error local_err;
+    if (!err) err = &local_err;
+    if (!c || (n && (!d_in || !in_off || !in_len || !d_out || !out_off || !out_cap || !out_len || !status))) {
+        set_err(err, RRG_ERR_INVALID_ARGUMENT, "null argument");
+        return RRG_ERR_INVALID_ARGUMENT;
+    }
+    if (err) std::memset(err, 0, sizeof(*err));
+    double t_all = now_ms();
+    c->st = rrg_stats{};
+    c->launches = 0;
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    int rc = upload_tables(c, err);
+    if (rc) {
+        c->stream = c->own_stream;
+        return rc;
+    }
+    std::vector<ChunkItem> items(n);
+    for (size_t i = 0; i < n; i++) {
+        items[i] = ChunkItem{in_off[i], in_len[i], 0, ~0ull, out_off[i], out_cap[i], ITEM_ONE_MEMBER, (uint32_t)i};
+        c->st.compressed_bytes += in_len[i];
+    }
+    std::vector<ChunkResult> res;
+    rc = launch_inflate(c, d_in, items, true, d_out, res, nullptr, err);
+    int first_bad = RRG_OK;
+    if (!rc) {
+        std::vector<MemberSpan> spans;
+        std::vector<size_t> idx;
+        for (size_t i = 0; i < n; i++) {
+            const ChunkResult& r = res[i];
+            out_len[i] = r.n_cells;
+            if (r.status == DS_OVERFLOW) status[i] = RRG_ERR_CAPACITY;
+            else if (r.status != DS_OK) {
+                rrg_error tmp;
+                status[i] = status_err(&tmp, r.status, r.msg, in_off[i] + r.err_bit / 8);
+            } else {
+                status[i] = RRG_OK;
+                spans.push_back(MemberSpan{out_off[i], r.n_cells, (uint32_t)r.markers, (uint32_t)(r.markers >> 32),
+                                           in_off[i] + in_len[i] - 8});
+                idx.push_back(i);
+            }
+        }
+        // per-member CRC/ISIZE: check each independently
+        if (!spans.empty()) {
+            rrg_error tmp;
+            int crc_rc = check_members(c, d_out, spans, 0, &tmp);
+            if (crc_rc == RRG_ERR_CRC_MISMATCH || crc_rc == RRG_ERR_ISIZE_MISMATCH) {
+                // find every failing member
+                std::vector<int32_t> stv(spans.size());
+                cudaMemcpy(stv.data(), c->mstatus.p, spans.size() * 4, cudaMemcpyDeviceToHost);
+                for (size_t j = 0; j < spans.size(); j++)
+                    if (stv[j] == DS_CRC) status[idx[j]] = RRG_ERR_CRC_MISMATCH;
+                    else if (stv[j] == DS_ISIZE) status[idx[j]] = RRG_ERR_ISIZE_MISMATCH;
+            } else if (crc_rc) {
+                rc = crc_rc;
+                if (err) *err = tmp;
+            }
+        }
+        for (size_t i = 0; i < n && !rc; i++)
+            if (status[i] != RRG_OK) {
+                first_bad = status[i];
+                set_err(err, status[i], "batch item %zu failed with status %d", i, status[i]);
+                break;
+            }
+        for (size_t i = 0; i < n; i++)
+            if (status[i] == RRG_OK) c->st.uncompressed_bytes += out_len[i];
+    }
+    c->stream = c->own_stream;
+    c->st.gpu_chunks = n;
+    c->st.kernel_launches = c->launches;
+    c->st.total_ms = now_ms() - t_all;
+    if (stats) *stats = c->st;
+    return rc ? rc : first_bad;
+}
+
+int rrg_gpu_find_blocks(rrg_ctx* c, const uint8_t* d_body, size_t body_len, const uint64_t* targets,
+                        const uint64_t* limits, uint64_t* found, size_t n, rrg_error* err) {
+    rrg_error local_err;
+    if (!err) err = &local_err;
+    if (!c || (n && (!targets || !limits || !found))) {
+        set_err(err, RRG_ERR_INVALID_ARGUMENT, "null argument");
+        return RRG_ERR_INVALID_ARGUMENT;
+    }
+    if (err) std::memset(err, 0, sizeof(*err));
+    int rc = upload_tables(c, err);
+    if (rc || !n) return rc;
+    CK(dgrow(c->targets, n * 8));
+    CK(dgrow(c->limits, n * 8));
+    CK(dgrow(c->found, n * 8));
+    CK(dgrow(c->queue, 16));
+    CK(cudaMemcpyAsync(c->targets.p, targets, n * 8, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->limits.p, limits, n * 8, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(c->queue.p, 0, 16, c->stream));
+    FindArgs F{d_body, body_len, (const uint64_t*)c->targets.p, (const uint64_t*)c->limits.p, (uint64_t*)c->found.p,
+               (uint32_t)n, (uint32_t*)c->queue.p, (const uint8_t*)c->next_lut.p, c->finder_tile};
+    const uint32_t W = 8;
+    RRG_LAUNCH(k_find_blocks, persistent_blocks(c, 4, n, W), W * 32, W * sizeof(FindSmem), c->stream, F);
+    LAUNCHED(c);
+    CK(cudaMemcpyAsync(found, c->found.p, n * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+int rrg_gpu_crc32(rrg_ctx* c, const uint8_t* d_data, size_t len, uint32_t* crc_out, rrg_error* err) {
+    rrg_error local_err;
+    if (!err) err = &local_err;
+    if (!c || !crc_out || (len && !d_data)) {
+        set_err(err, RRG_ERR_INVALID_ARGUMENT, "null argument");
+        return RRG_ERR_INVALID_ARGUMENT;
+    }
+    if (err) std::memset(err, 0, sizeof(*err));
+    int rc = upload_tables(c, err);
+    if (rc) return rc;
+    // a single member spanning the buffer, checked against a dummy trailer:
+    // the computed CRC is reported back through got_crc
+    std::vector<MemberSpan> one{MemberSpan{0, len, 0, (uint32_t)len, 0}};
+    rrg_error tmp;
+    rc = check_members(c, d_data, one, 0, &tmp);
+    if (rc && rc != RRG_ERR_CRC_MISMATCH && rc != RRG_ERR_ISIZE_MISMATCH) {
+        if (err) *err = tmp;
+        return rc;
+    }
+    CK(cudaMemcpy(crc_out, c->got_crc.p, 4, cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int rrg_gpu_resolve_markers(rrg_ctx* c, uint8_t* d_bytes, size_t n_bytes, const uint32_t* d_out_pos,
+                            const uint16_t* d_prefix_offset, size_t n_markers, const uint8_t* d_tail, size_t tail_len,
+                            rrg_error* err) {
+    rrg_error local_err;
+    if (!err) err = &local_err;
+    if (!c || (n_markers && (!d_bytes || !d_out_pos || !d_prefix_offset))) {
+        set_err(err, RRG_ERR_INVALID_ARGUMENT, "null argument");
+        return RRG_ERR_INVALID_ARGUMENT;
+    }
+    if (err) std::memset(err, 0, sizeof(*err));
+    if (!n_markers) return 0;
+    // Express the reference's (bytes, markers, prev_tail) triple as two chunks
+    // of cells: the tail (all literals) followed by the chunk, whose marker
+    // cells carry their prefix offsets; k_resolve then writes tail || bytes.
+    const uint64_t tl = tail_len, nb = n_bytes;
+    const uint64_t cells_n = round8(tl) + round8(nb);
+    CK(dgrow(c->cells, cells_n * 2 + 64));
+    CK(dgrow(c->out, tl + nb + 64));
+    std::vector<uint16_t> hc(cells_n, 0);
+    std::vector<uint8_t> tail(tl), bytes(nb);
+    std::vector<uint32_t> mp(n_markers);
+    std::vector<uint16_t> mo(n_markers);
+    if (tl) CK(cudaMemcpy(tail.data(), d_tail, tl, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(bytes.data(), d_bytes, nb, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(mp.data(), d_out_pos, n_markers * 4, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(mo.data(), d_prefix_offset, n_markers * 2, cudaMemcpyDeviceToHost));
+    for (uint64_t i = 0; i < tl; i++) hc[i] = tail[i];
+    const uint64_t base = round8(tl);
+    for (uint64_t i = 0; i < nb; i++) hc[base + i] = bytes[i];
+    for (size_t i = 0; i < n_markers; i++) {
+        if (mo[i] >= tl || mp[i] >= nb) {
+            set_err(err, RRG_ERR_DEFLATE_INVALID, "%s", msg_text(MSG_MARKER_WINDOW));
+            return RRG_ERR_DEFLATE_INVALID;
+        }
+        hc[base + mp[i]] = (uint16_t)(MARKER16 | mo[i]);
+    }
+    CK(cudaMemcpy(c->cells.p, hc.data(), cells_n * 2, cudaMemcpyHostToDevice));
+    std::vector<ResolveChunk> ch;
+    std::vector<uint64_t> ts{0};
+    if (tl) {
+        ch.push_back(ResolveChunk{0, 0, tl, 0});
+        ts.push_back(ts.back() + (tl + RES_TILE - 1) / RES_TILE);
+    }
+    ch.push_back(ResolveChunk{tl, base, nb, 0});
+    ts.push_back(ts.back() + (nb + RES_TILE - 1) / RES_TILE);
+    const uint32_t nc = (uint32_t)ch.size();
+    CK(dgrow(c->chunks, nc * sizeof(ResolveChunk)));
+    CK(dgrow(c->tiles, (nc + 1) * 8));
+    CK(dgrow(c->rerr, 16));
+    CK(dgrow(c->markers, 8));
+    CK(cudaMemcpy(c->chunks.p, ch.data(), nc * sizeof(ResolveChunk), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->tiles.p, ts.data(), (nc + 1) * 8, cudaMemcpyHostToDevice));
+    CK(cudaMemset(c->rerr.p, 0, 16));
+    CK(cudaMemset(c->markers.p, 0, 8));
+    ResolveArgs R{(const uint16_t*)c->cells.p, (const ResolveChunk*)c->chunks.p, (const uint64_t*)c->tiles.p, nc,
+                  ts.back(), (uint8_t*)c->out.p, (uint32_t*)c->rerr.p, (unsigned long long*)c->markers.p};
+    RRG_LAUNCH(k_resolve, (uint32_t)std::max<uint64_t>(1, ts.back()), RES_THREADS, 0, c->stream, R);
+    LAUNCHED(c);
+    CK(cudaStreamSynchronize(c->stream));
+    uint32_t e4[4];
+    CK(cudaMemcpy(e4, c->rerr.p, 16, cudaMemcpyDeviceToHost));
+    if (e4[0]) {
+        set_err(err, RRG_ERR_DEFLATE_INVALID, "%s", msg_text(MSG_MARKER_WINDOW));
+        return RRG_ERR_DEFLATE_INVALID;
+    }
+    CK(cudaMemcpy(d_bytes, (const uint8_t*)c->out.p + tl, nb, cudaMemcpyDeviceToDevice));
+    return 0;
+}
+
+int rrg_gpu_decode_chunk(rrg_ctx* c, const uint8_t* d_body, size_t body_len, uint64_t start_bit, uint64_t end_bit_hint,
+                         uint8_t* bytes, size_t* n_bytes, uint32_t* marker_pos, uint16_t* marker_off, size_t* n_markers,
+                         uint64_t* actual_end_bit, int32_t* final_block, rrg_error* err) {
+    rrg_error local_err;
+    if (!err) err = &local_err;
+    if (!c || !d_body || !n_bytes || !n_markers) {
+        set_err(err, RRG_ERR_INVALID_ARGUMENT, "null argument");
+        return RRG_ERR_INVALID_ARGUMENT;
+    }
+    if (err) std::memset(err, 0, sizeof(*err));
+    int rc = upload_tables(c, err);
+    if (rc) return rc;
+    const uint64_t cap_b = *n_bytes, cap_m = *n_markers;
+    uint64_t cap = round8(std::max<uint64_t>(cap_b, 64));
+    CK(dgrow(c->cells, cap * 2 + 64));
+    std::vector<ChunkItem> items{ChunkItem{0, body_len, start_bit, end_bit_hint, 0, cap, ITEM_MARKERS, 0}};
+    std::vector<ChunkResult> res;
+    std::vector<MemberRec> mr;
+    mr.reserve(4096);
+    rc = launch_inflate(c, d_body, items, false, c->cells.p, res, &mr, err);
+    if (rc) return rc;
+    const ChunkResult& r = res[0];
+    if (r.status == DS_OVERFLOW) {
+        *n_bytes = r.n_cells;
+        set_err(err, RRG_ERR_CAPACITY, "chunk needs %llu bytes", (unsigned long long)r.n_cells);
+        return RRG_ERR_CAPACITY;
+    }
+    if (r.status) return status_err(err, r.status, r.msg, r.err_bit / 8);
+    std::vector<uint16_t> cells(r.n_cells);
+    if (r.n_cells) CK(cudaMemcpy(cells.data(), c->cells.p, r.n_cells * 2, cudaMemcpyDeviceToHost));
+    uint64_t nm = 0;
+    for (uint64_t i = 0; i < r.n_cells; i++) {
+        uint16_t v = cells[i];
+        if (v & MARKER16) {
+            if (nm < cap_m) {
+                if (marker_pos) marker_pos[nm] = (uint32_t)i;
+                if (marker_off) marker_off[nm] = (uint16_t)(v & 0x7fff);
+            }
+            nm++;
+            if (bytes && i < cap_b) bytes[i] = 0;
+        } else if (bytes && i < cap_b) {
+            bytes[i] = (uint8_t)v;
+        }
+    }
+    *n_bytes = r.n_cells;
+    *n_markers = nm;
+    if (actual_end_bit) *actual_end_bit = r.actual_end_bit;
+    if (final_block) *final_block = r.final_block;
+    if (nm > cap_m) {
+        set_err(err, RRG_ERR_CAPACITY, "chunk has %llu markers", (unsigned long long)nm);
+        return RRG_ERR_CAPACITY;
+    }
+    return 0;
+}
+
+int64_t rrg_gpu_submit(rrg_ctx* c, const uint8_t* data, size_t len, rrg_error* err) {
+    if (!c || (!data && len)) {
+        set_err(err, RRG_ERR_INVALID_ARGUMENT, "null argument");
+        return -1;
+    }
+    std::lock_guard<std::mutex> g(c->srv_mu);
+    rrg_ctx::Req r;
+    r.id = c->srv_next_id++;
+    r.data.assign(data, data + len);
+    r.t_submit = now_ms();
+    c->srv_queue.push_back(std::move(r));
+    return c->srv_queue.back().id;
+}
+
+int rrg_gpu_poll(rrg_ctx* c, int64_t* request_id, uint8_t** out, size_t* out_len, int32_t* status, double* latency_ms,
+                 int32_t timeout_ms, rrg_error* err) {
+    (void)timeout_ms;
+    if (!c || !request_id || !out || !out_len || !status) {
+        set_err(err, RRG_ERR_INVALID_ARGUMENT, "null argument");
+        return -RRG_ERR_INVALID_ARGUMENT;
+    }
+    rrg_ctx::Req r;
+    {
+        std::lock_guard<std::mutex> g(c->srv_mu);
+        if (c->srv_queue.empty()) return 0;
+        r = std::move(c->srv_queue.front());
+        c->srv_queue.pop_front();
+    }
+    struct Coll {
+        std::vector<uint8_t> v;
+    } coll;
+    auto sink = [](void* u, const uint8_t* p, size_t n) -> int {
+        auto* cc = (Coll*)u;
+        cc->v.insert(cc->v.end(), p, p + n);
+        return 0;
+    };
+    rrg_error e2;
+    int rc = decode_host_impl(c, r.data.data(), r.data.size(), sink, &coll, nullptr, &e2);
+    *request_id = r.id;
+    *status = rc;
+    *latency_ms = now_ms() - r.t_submit;
+    if (rc) {
+        *out = nullptr;
+        *out_len = 0;
+        if (err) *err = e2;
+        return 1;
+    }
+    *out = (uint8_t*)std::malloc(std::max<size_t>(coll.v.size(), 1));
+    if (!coll.v.empty()) std::memcpy(*out, coll.v.data(), coll.v.size());
+    *out_len = coll.v.size();
+    return 1;
+}
+
+int64_t rrg_gpu_pending(rrg_ctx* c) {
+    if (!c) return -1;
+    std::lock_guard<std::mutex> g(c->srv_mu);
+    return (int64_t)c->srv_queue.size();
+}
+
+void rrg_gpu_free(void* p) { std::free(p); }
+
+const char* rrg_gpu_version(void) { return "rrg-gpu 0.1 (sm_100a)"; }
+
+uint64_t rrg_gpu_kernel_launch_count(void) { return g_launches.load(); }
+
+}  // extern "C"

@@ -1,0 +1,1300 @@
+// rrg_kernels.cuh — device code of the B200 gzip/DEFLATE decoder.
+//
+// Kernels (each names the reference function whose result it reproduces;
+// paths are relative to the rusty_rapidgzip repository, rrg/ = crates/rusty-rapidgzip/):
+//   k_find_blocks  — rrg/src/deflate/block_finder.rs:109-141 find_next_dynamic_block
+//   k_inflate      — rrg/src/pipeline.rs:1080-1185 decode_one_chunk with
+//                    rrg/src/deflate/fast_inflate.rs:1794-2234 (u16 marker cells), or a
+//                    whole member into final bytes (gzip.rs:197-249 decode_one_indexed_fast)
+//   k_resolve      — rrg/src/deflate/speculative.rs:175-213 resolve_markers together with the
+//                    tail chain of rrg/src/pipeline.rs:1045-1078, fused with the chunk compaction
+//   k_crc_pieces / k_crc_members — crc32fast hashing + combine (rrg/src/pipeline.rs:712-732, :885-916)
+//
+// This header is compiled by nvcc for sm_100a (rrg_kernels.cu) and, for the
+// CPU test build only, by g++ against a warp-emulation shim.
+#pragma once
+#include "rrg_common.h"
+
+#ifndef FULLMASK
+#define FULLMASK 0xffffffffu
+#endif
+
+#if defined(__CUDA_ARCH__)
+#define RRG_PREFETCH_L1(p) asm volatile("prefetch.global.L1 [%0];" ::"l"(p))
+#else
+#define RRG_PREFETCH_L1(p) ((void)(p))
+#endif
+
+#ifdef RRG_EMU
+#define RRG_DYN_SMEM(name) unsigned char* name = emu::dyn_smem()
+#else
+#define RRG_DYN_SMEM(name) extern __shared__ __align__(16) unsigned char name[]
+#endif
+
+namespace rrg {
+
+// ---------------------------------------------------------------- constants
+__constant__ uint16_t c_len_base[29] = {3,  4,  5,  6,  7,  8,  9,  10, 11,  13,  15,  17,  19,  23, 27,
+                                         31, 35, 43, 51, 59, 67, 83, 99, 115, 131, 163, 195, 227, 258};
+__constant__ uint8_t c_len_extra[29] = {0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 2, 2, 2,
+                                        2, 3, 3, 3, 3, 4, 4, 4, 4, 5, 5, 5, 5, 0};
+__constant__ uint16_t c_dist_base[30] = {1,    2,    3,    4,    5,    7,     9,     13,    17,  25,
+                                         33,   49,   65,   97,   129,  193,   257,   385,   513, 769,
+                                         1025, 1537, 2049, 3073, 4097, 6145, 8193, 12289, 16385, 24577};
+__constant__ uint8_t c_dist_extra[30] = {0, 0, 0, 0, 1, 1, 2, 2, 3, 3, 4, 4, 5, 5, 6,
+                                         6, 7, 7, 8, 8, 9, 9, 10, 10, 11, 11, 12, 12, 13, 13};
+__constant__ uint8_t c_cl_order[19] = {16, 17, 18, 0, 8, 7, 9, 6, 10, 5, 11, 4, 12, 3, 13, 2, 14, 1, 15};
+// x^(2^k) mod P (reflected CRC-32), k = 0..66; uploaded by the host.
+__constant__ uint32_t c_x2k[67];
+
+constexpr int LUT_BITS = 10;
+constexpr int LUT_SIZE = 1 << LUT_BITS;
+constexpr int PRE_BITS = 7;
+constexpr int NB = 32;  // symbols per decode batch
+
+// ------------------------------------------------------- warp helpers
+__device__ __forceinline__ uint32_t warp_sum(uint32_t v) {
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULLMASK, v, o);
+    return v;
+}
+__device__ __forceinline__ uint64_t bcast64(uint64_t v) {
+    uint32_t lo = __shfl_sync(FULLMASK, (uint32_t)v, 0);
+    uint32_t hi = __shfl_sync(FULLMASK, (uint32_t)(v >> 32), 0);
+    return ((uint64_t)hi << 32) | lo;
+}
+__device__ __forceinline__ int32_t bcast32(int32_t v) { return __shfl_sync(FULLMASK, v, 0); }
+
+// ------------------------------------------------------- bounded byte source
+// Bytes [lo, hi) relative to a 4-byte-aligned base are readable. Whole words
+// inside the range use one aligned load; edge words are assembled from bytes
+// so no access leaves the caller's buffer.
+struct Src {
+    const uint8_t* base;
+    uint64_t lo, hi;
+};
+__device__ __forceinline__ Src make_src(const uint8_t* p, uint64_t len) {
+    Src s;
+    uintptr_t a = (uintptr_t)p;
+    s.base = (const uint8_t*)(a & ~(uintptr_t)3);
+    s.lo = a & 3;
+    s.hi = s.lo + len;
+    return s;
+}
+__device__ __forceinline__ uint32_t src_word(const Src& s, uint64_t w) {
+    uint64_t b = w * 4;
+    if (b >= s.lo && b + 4 <= s.hi) return __ldg((const uint32_t*)(s.base + b));
+    uint32_t v = 0;
+    for (int k = 0; k < 4; k++) {
+        uint64_t p = b + k;
+        if (p >= s.lo && p < s.hi) v |= (uint32_t)__ldg(s.base + p) << (8 * k);
+    }
+    return v;
+}
+__device__ __forceinline__ uint32_t src_byte(const Src& s, uint64_t rel) {  // rel: from s.lo
+    uint64_t p = s.lo + rel;
+    return p < s.hi ? (uint32_t)__ldg(s.base + p) : 0u;
+}
+
+// ------------------------------------------------------- bit reader (one lane)
+// LSB-first (RFC 1951 §3.1.1). `nw` is the next 32-bit word to load; after a
+// refill at least 33 bits are buffered. Bits past the end read as zero; the
+// caller compares tell() with the end to report EOF exactly.
+struct BR {
+    Src s;
+    uint64_t nw;
+    uint64_t buf;
+    uint32_t bits;
+};
+__device__ __forceinline__ void br_refill(BR& b) {
+    if (b.bits <= 32) {
+        if ((b.nw & 31) == 0 && (b.nw + 128) * 4 < b.s.hi) RRG_PREFETCH_L1(b.s.base + (b.nw + 128) * 4);
+        b.buf |= (uint64_t)src_word(b.s, b.nw) << b.bits;
+        b.nw++;
+        b.bits += 32;
+    }
+}
+__device__ __forceinline__ void br_consume(BR& b, uint32_t n) {
+    b.buf >>= n;
+    b.bits -= n;
+}
+// absolute bit position relative to base
+__device__ __forceinline__ uint64_t br_tell_abs(const BR& b) { return b.nw * 32 - b.bits; }
+__device__ __forceinline__ uint64_t br_tell(const BR& b) { return br_tell_abs(b) - b.s.lo * 8; }
+__device__ __forceinline__ void br_seek(BR& b, uint64_t rel_bit) {
+    uint64_t a = rel_bit + b.s.lo * 8;
+    b.nw = a >> 5;
+    b.buf = 0;
+    b.bits = 0;
+    br_refill(b);
+    br_consume(b, (uint32_t)(a & 31));
+    br_refill(b);
+}
+__device__ __forceinline__ uint32_t br_read(BR& b, uint32_t n) {  // n <= 32
+    br_refill(b);
+    uint32_t v = (uint32_t)(b.buf & ((1ull << n) - 1));
+    br_consume(b, n);
+    return v;
+}
+__device__ __forceinline__ bool br_past_end(const BR& b) { return br_tell_abs(b) > b.s.hi * 8; }
+
+// ------------------------------------------------------- Huffman tables
+// LUT entry (u32): bits 0-3 code length (0 = not in the LUT), bits 4-5 kind,
+// bits 8-11 extra-bit count, bits 16-31 value.
+//   litlen kind: 0 literal (value = byte), 1 length (value = base), 2 end of block, 3 invalid (286/287)
+//   dist kind:   0 distance (value = base), 3 invalid (30/31)
+//   precode:     value = symbol
+enum { TK_LITLEN = 0, TK_DIST = 1, TK_PRE = 2 };
+
+__device__ __forceinline__ uint32_t make_entry(int kind, uint32_t sym, uint32_t len) {
+    if (kind == TK_LITLEN) {
+        if (sym < 256) return (sym << 16) | len;
+        if (sym == 256) return (2u << 4) | len;
+        if (sym <= 285)
+            return ((uint32_t)c_len_base[sym - 257] << 16) | ((uint32_t)c_len_extra[sym - 257] << 8) | (1u << 4) | len;
+        return (3u << 4) | len;
+    }
+    if (kind == TK_DIST) {
+        if (sym < 30) return ((uint32_t)c_dist_base[sym] << 16) | ((uint32_t)c_dist_extra[sym] << 8) | len;
+        return (3u << 4) | len;
+    }
+    return (sym << 16) | len;
+}
+
+struct Table {
+    uint32_t* lut;
+    uint16_t* sorted;  // symbols in canonical order
+    uint16_t* first;   // [16] first canonical code of each length
+    uint16_t* count;   // [16]
+    uint16_t* off;     // [16] index of each length's first symbol in `sorted`
+};
+
+// Canonical code construction (RFC 1951 §3.2.2), warp-parallel. Rejects an
+// oversubscribed tree with >= 2 symbols (huffman.rs:238-249, non-strict).
+// Returns MSG_NONE or MSG_OVERSUB (uniform across the warp).
+__device__ int warp_build(const uint8_t* len, int n, const Table& T, int lut_bits, int kind, uint16_t* run,
+                          int lane) {
+    const uint32_t lut_size = 1u << lut_bits;
+    for (uint32_t i = lane; i < lut_size; i += 32) T.lut[i] = 0;
+    uint32_t cnt = 0;
+    if (lane >= 1 && lane <= 15)
+        for (int s = 0; s < n; s++) cnt += (len[s] == (uint32_t)lane);
+    uint32_t kraft = (lane >= 1 && lane <= 15) ? (cnt << (15 - lane)) : 0u;
+    uint32_t ksum = warp_sum(kraft), nsym = warp_sum(cnt);
+    if (nsym >= 2 && ksum > 32768u) {
+        __syncwarp();
+        return MSG_OVERSUB;
+    }
+    uint32_t f = 0, o = 0;
+    for (int i = 1; i < 16; i++) {
+        uint32_t ci = __shfl_sync(FULLMASK, cnt, i);
+        if (i < lane) {
+            f = (f + ci) << 1;
+            o += ci;
+        }
+    }
+    if (lane < 16) {
+        T.first[lane] = (uint16_t)f;
+        T.count[lane] = (uint16_t)(lane ? cnt : 0);
+        T.off[lane] = (uint16_t)o;
+        run[lane] = 0;
+    }
+    __syncwarp();
+    for (int g = 0; g < n; g += 32) {
+        int s = g + lane;
+        uint32_t l = (s < n) ? len[s] : 0u;
+        unsigned same = __match_any_sync(FULLMASK, l);
+        unsigned rank = __popc(same & ((1u << lane) - 1u));
+        uint32_t base = run[l];
+        __syncwarp();
+        if (l && (same >> lane) == 1u) run[l] = (uint16_t)(base + __popc(same));
+        __syncwarp();
+        if (s < n && l) {
+            uint32_t idx = base + rank;
+            uint32_t code = T.first[l] + idx;
+            T.sorted[T.off[l] + idx] = (uint16_t)s;
+            if ((int)l <= lut_bits) {
+                uint32_t e = make_entry(kind, (uint32_t)s, l);
+                uint32_t rev = __brev(code) >> (32 - l);
+                for (uint32_t i = rev; i < lut_size; i += (1u << l)) T.lut[i] = e;
+            }
+        }
+    }
+    __syncwarp();
+    return MSG_NONE;
+}
+
+// Codes longer than the LUT: canonical decode over lengths lut_bits+1..15.
+// Returns 0 when no code matches.
+__device__ __noinline__ uint32_t long_decode(uint64_t buf, const Table& T, int lut_bits, int kind) {
+    uint32_t rv = __brev((uint32_t)buf);
+    for (int l = lut_bits + 1; l <= 15; l++) {
+        uint32_t code = rv >> (32 - l);
+        uint32_t d = code - T.first[l];
+        if (d < T.count[l]) return make_entry(kind, T.sorted[T.off[l] + d], (uint32_t)l);
+    }
+    return 0;
+}
+
+// ------------------------------------------------------- inflate kernel
+struct WarpSmem {
+    uint32_t lit_lut[LUT_SIZE];
+    uint32_t dist_lut[LUT_SIZE];
+    uint32_t pre_lut[1 << PRE_BITS];
+    uint32_t ent[NB];
+    uint32_t epos[NB];
+    uint16_t lit_sorted[288];
+    uint16_t dist_sorted[32];
+    uint16_t pre_sorted[32];
+    uint16_t lit_first[16], lit_count[16], lit_off[16];
+    uint16_t dist_first[16], dist_count[16], dist_off[16];
+    uint16_t pre_first[16], pre_count[16], pre_off[16];
+    uint16_t run[16];
+    uint8_t lengths[320];
+    uint8_t pre_len[20];
+    int32_t fixed_loaded;
+    int32_t pad[3];
+};
+
+struct InflateArgs {
+    const uint8_t* in;       // compressed input base
+    const ChunkItem* items;
+    ChunkResult* results;
+    uint32_t n_items;
+    const uint32_t* order;   // optional permutation of the work queue (largest first)
+    uint32_t* queue;         // work-queue head
+    void* out;               // cell arena (u16) or byte output (u8)
+    MemberRec* mbs;
+    uint32_t* mb_count;
+    uint32_t mb_cap;
+};
+
+// Per-item decode state (identical in every lane except the bit reader,
+// which only lane 0 advances).
+struct ItemState {
+    BR br;
+    uint64_t cur;           // cells produced
+    uint64_t cap;           // cells available
+    uint64_t member_start;  // cell where the current member began
+    uint64_t markers;
+    int32_t status, msg;
+    bool markers_ok;
+    bool counting;          // output full: keep decoding only to measure the size
+};
+
+__device__ __forceinline__ Table lit_table(WarpSmem& S) {
+    return Table{S.lit_lut, S.lit_sorted, S.lit_first, S.lit_count, S.lit_off};
+}
+__device__ __forceinline__ Table dist_table(WarpSmem& S) {
+    return Table{S.dist_lut, S.dist_sorted, S.dist_first, S.dist_count, S.dist_off};
+}
+__device__ __forceinline__ Table pre_table(WarpSmem& S) {
+    return Table{S.pre_lut, S.pre_sorted, S.pre_first, S.pre_count, S.pre_off};
+}
+
+__device__ __forceinline__ int find_entry(const uint32_t* epos, int n, uint32_t j) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (epos[mid] <= j) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Dynamic block header (inflate.rs:74-145 read_dynamic_header) -> tables.
+__device__ void read_dynamic(WarpSmem& S, ItemState& st, int lane) {
+    int status = 0, msg = 0;
+    uint32_t hlit = 0, hdist = 0;
+    if (lane == 0) {
+        hlit = br_read(st.br, 5) + 257;
+        hdist = br_read(st.br, 5) + 1;
+        uint32_t hclen = br_read(st.br, 4) + 4;
+        for (int i = 0; i < 19; i++) S.pre_len[i] = 0;
+        if (hlit > 286 || hdist > 30) {
+            status = DS_INVALID;
+            msg = MSG_HLIT_HDIST;
+        } else {
+            for (uint32_t i = 0; i < hclen; i++) S.pre_len[c_cl_order[i]] = (uint8_t)br_read(st.br, 3);
+            if (br_past_end(st.br)) status = DS_EOF;
+        }
+    }
+    status = bcast32(status);
+    msg = bcast32(msg);
+    hlit = (uint32_t)bcast32((int32_t)hlit);
+    hdist = (uint32_t)bcast32((int32_t)hdist);
+    if (status) {
+        st.status = status;
+        st.msg = msg;
+        return;
+    }
+    __syncwarp();
+    msg = warp_build(S.pre_len, 19, pre_table(S), PRE_BITS, TK_PRE, S.run, lane);
+    if (msg) {
+        st.status = DS_INVALID;
+        st.msg = msg;
+        return;
+    }
+    for (int i = lane; i < 320; i += 32) S.lengths[i] = 0;
+    __syncwarp();
+    if (lane == 0) {
+        uint32_t total = hlit + hdist, i = 0;
+        while (i < total) {
+            br_refill(st.br);
+            uint32_t e = S.pre_lut[st.br.buf & ((1u << PRE_BITS) - 1)];
+            uint32_t cl = e & 15;
+            if (!cl) {
+                status = DS_INVALID;
+                msg = MSG_NO_CODE;
+                break;
+            }
+            br_consume(st.br, cl);
+            uint32_t sym = e >> 16;
+            if (sym <= 15) {
+                S.lengths[i++] = (uint8_t)sym;
+            } else if (sym == 16) {
+                if (i == 0) {
+                    status = DS_INVALID;
+                    msg = MSG_CODE16_FIRST;
+                    break;
+                }
+                uint32_t r = br_read(st.br, 2) + 3;
+                if (i + r > total) {
+                    status = DS_INVALID;
+                    msg = MSG_CODE16_OVER;
+                    break;
+                }
+                uint8_t prev = S.lengths[i - 1];
+                for (uint32_t j = 0; j < r; j++) S.lengths[i + j] = prev;
+                i += r;
+            } else if (sym == 17) {
+                uint32_t r = br_read(st.br, 3) + 3;
+                if (i + r > total) {
+                    status = DS_INVALID;
+                    msg = MSG_CODE17_OVER;
+                    break;
+                }
+                i += r;
+            } else {
+                uint32_t r = br_read(st.br, 7) + 11;
+                if (i + r > total) {
+                    status = DS_INVALID;
+                    msg = MSG_CODE18_OVER;
+                    break;
+                }
+                i += r;
+            }
+            if (br_past_end(st.br)) {
+                status = DS_EOF;
+                break;
+            }
+        }
+        if (!status && S.lengths[256] == 0) {
+            status = DS_INVALID;
+            msg = MSG_EOB_ZERO;
+        }
+    }
+    status = bcast32(status);
+    msg = bcast32(msg);
+    if (status) {
+        st.status = status;
+        st.msg = msg;
+        return;
+    }
+    __syncwarp();
+    msg = warp_build(S.lengths, (int)hlit, lit_table(S), LUT_BITS, TK_LITLEN, S.run, lane);
+    if (!msg) msg = warp_build(S.lengths + hlit, (int)hdist, dist_table(S), LUT_BITS, TK_DIST, S.run, lane);
+    if (msg) {
+        st.status = DS_INVALID;
+        st.msg = msg;
+    }
+    if (lane == 0) S.fixed_loaded = 0;
+    __syncwarp();
+}
+
+__device__ void load_fixed(WarpSmem& S, int lane) {
+    if (S.fixed_loaded) return;  // uniform (shared value)
+    for (int i = lane; i < 288; i += 32) S.lengths[i] = i < 144 ? 8 : i < 256 ? 9 : i < 280 ? 7 : 8;
+    for (int i = lane; i < 30; i += 32) S.lengths[288 + i] = 5;
+    __syncwarp();
+    warp_build(S.lengths, 288, lit_table(S), LUT_BITS, TK_LITLEN, S.run, lane);
+    warp_build(S.lengths + 288, 30, dist_table(S), LUT_BITS, TK_DIST, S.run, lane);
+    if (lane == 0) S.fixed_loaded = 1;
+    __syncwarp();
+}
+
+// Stored block (inflate.rs:38-53): byte-align, LEN/NLEN, LEN raw bytes.
+template <typename CellT>
+__device__ void stored_block(WarpSmem& S, ItemState& st, CellT* out, int lane) {
+    int status = 0, msg = 0;
+    uint64_t bp = 0;
+    uint32_t len = 0;
+    if (lane == 0) {
+        br_consume(st.br, st.br.bits & 7);
+        len = br_read(st.br, 16);
+        uint32_t nlen = br_read(st.br, 16);
+        if ((len ^ 0xffffu) != nlen) {
+            status = DS_INVALID;
+            msg = MSG_STORED_NLEN;
+        } else {
+            bp = br_tell(st.br) >> 3;  // relative to the source start
+            if (st.br.s.lo + bp + len > st.br.s.hi) status = DS_EOF;
+        }
+    }
+    status = bcast32(status);
+    msg = bcast32(msg);
+    len = (uint32_t)bcast32((int32_t)len);
+    bp = bcast64(bp);
+    if (status) {
+        st.status = status;
+        st.msg = msg;
+        return;
+    }
+    if (!st.counting && st.cur + len > st.cap) st.counting = true;
+    if (!st.counting)
+        for (uint32_t i = lane; i < len; i += 32) out[st.cur + i] = (CellT)src_byte(st.br.s, bp + i);
+    st.cur += len;
+    if (lane == 0) br_seek(st.br, (bp + len) * 8);
+    __syncwarp();
+}
+
+// Huffman-coded block body: lane 0 decodes up to NB symbols into the batch,
+// the warp materialises the batch's bytes in parallel.
+template <typename CellT>
+__device__ void decode_codes(WarpSmem& S, ItemState& st, CellT* out, int lane) {
+    const Table LT = lit_table(S), DT = dist_table(S);
+    for (;;) {
+        int n = 0, stop = 0, status = 0, msg = 0;
+        uint32_t pos = 0;
+        if (lane == 0) {
+            uint64_t room = st.counting ? ~0ull : (st.cap > st.cur ? st.cap - st.cur : 0);
+            BR b = st.br;
+            while (n < NB) {
+                const BR save = b;
+                br_refill(b);
+                uint32_t e = S.lit_lut[b.buf & (LUT_SIZE - 1)];
+                uint32_t cl = e & 15;
+                if (!cl) {
+                    e = long_decode(b.buf, LT, LUT_BITS, TK_LITLEN);
+                    cl = e & 15;
+                    if (!cl) {
+                        status = br_past_end(b) ? DS_EOF : DS_INVALID;
+                        msg = MSG_NO_CODE;
+                        break;
+                    }
+                }
+                uint32_t kind = (e >> 4) & 3;
+                if (kind == 0) {
+                    if (pos + 1 > room) {  // output full: this symbol is re-read in counting mode
+                        b = save;
+                        stop = 3;
+                        break;
+                    }
+                    br_consume(b, cl);
+                    S.ent[n] = 0x80000000u | (e >> 16);
+                    S.epos[n] = pos;
+                    pos += 1;
+                    n++;
+                } else if (kind == 1) {
+                    uint32_t ex = (e >> 8) & 15;
+                    uint32_t length = (e >> 16) + ((uint32_t)(b.buf >> cl) & ((1u << ex) - 1u));
+                    br_consume(b, cl + ex);
+                    br_refill(b);
+                    uint32_t de = S.dist_lut[b.buf & (LUT_SIZE - 1)];
+                    uint32_t dl = de & 15;
+                    if (!dl) {
+                        de = long_decode(b.buf, DT, LUT_BITS, TK_DIST);
+                        dl = de & 15;
+                        if (!dl) {
+                            status = br_past_end(b) ? DS_EOF : DS_INVALID;
+                            msg = MSG_NO_CODE;
+                            break;
+                        }
+                    }
+                    if (((de >> 4) & 3) == 3) {
+                        status = DS_INVALID;
+                        msg = MSG_DIST_RANGE;
+                        break;
+                    }
+                    if (pos + length > room) {
+                        b = save;
+                        stop = 3;
+                        break;
+                    }
+                    uint32_t dx = (de >> 8) & 15;
+                    uint32_t dist = (de >> 16) + ((uint32_t)(b.buf >> dl) & ((1u << dx) - 1u));
+                    br_consume(b, dl + dx);
+                    S.ent[n] = (dist << 9) | length;
+                    S.epos[n] = pos;
+                    pos += length;
+                    n++;
+                } else if (kind == 2) {
+                    br_consume(b, cl);
+                    stop = 1;
+                } else {
+                    status = DS_INVALID;
+                    msg = MSG_LITLEN_RANGE;
+                    break;
+                }
+                if (br_past_end(b)) {
+                    status = DS_EOF;
+                    break;
+                }
+                if (stop) break;
+            }
+            st.br = b;
+        }
+        n = bcast32(n);
+        pos = (uint32_t)bcast32((int32_t)pos);
+        stop = bcast32(stop);
+        status = bcast32(status);
+        msg = bcast32(msg);
+        __syncwarp();
+        if (!st.counting && n) {
+            uint32_t bad = 0, mk = 0;
+            const uint64_t cur = st.cur;
+            for (uint32_t j = lane; j < pos; j += 32) {
+                int k = find_entry(S.epos, n, j);
+                uint32_t jj = j, cell = 0;
+                for (;;) {
+                    uint32_t e = S.ent[k];
+                    if (e & 0x80000000u) {
+                        cell = e & 0xffu;
+                        break;
+                    }
+                    uint32_t d = e >> 9;
+                    uint32_t t = jj - S.epos[k];
+                    if (t >= d) t %= d;
+                    int64_t src = (int64_t)S.epos[k] - (int64_t)d + (int64_t)t;
+                    if (src >= 0) {
+                        jj = (uint32_t)src;
+                        k = find_entry(S.epos, k, jj);
+                        continue;
+                    }
+                    int64_t a = (int64_t)cur + src;
+                    if (a >= (int64_t)st.member_start) {
+                        cell = (uint32_t)out[a];
+                        break;
+                    }
+                    if (st.markers_ok && a < 0) {
+                        cell = MARKER16 | (uint32_t)(-a - 1);
+                        mk++;
+                        break;
+                    }
+                    bad = 1;
+                    break;
+                }
+                out[cur + j] = (CellT)cell;
+            }
+            bad = warp_sum(bad);
+            mk = warp_sum(mk);
+            st.markers += mk;
+            if (bad && !status) {
+                status = DS_INVALID;
+                msg = MSG_DIST_FAR;
+            }
+        }
+        st.cur += pos;
+        __syncwarp();
+        if (status) {
+            st.status = status;
+            st.msg = msg;
+            return;
+        }
+        if (stop == 1) return;
+        if (stop == 3) st.counting = true;
+    }
+}
+
+__device__ __forceinline__ uint32_t le32_at(const Src& s, uint64_t rel) {
+    return src_byte(s, rel) | (src_byte(s, rel + 1) << 8) | (src_byte(s, rel + 2) << 16) | (src_byte(s, rel + 3) << 24);
+}
+
+// gzip.rs:252-300 parse_header, on the device (lane 0 only).
+__device__ int dev_parse_header(const Src& s, uint64_t at, uint64_t* hl, int* msg) {
+    uint64_t n = s.hi - s.lo;
+    *msg = 0;
+    if (at + 10 > n) return DS_TRUNCATED;
+    if (src_byte(s, at) != 0x1f || src_byte(s, at + 1) != 0x8b) return DS_BAD_MAGIC;
+    uint32_t cm = src_byte(s, at + 2);
+    if (cm != 8) {
+        *msg = (int)cm;
+        return DS_METHOD;
+    }
+    uint32_t flg = src_byte(s, at + 3);
+    if (flg & 0xe0) {
+        *msg = (int)flg;
+        return DS_FLAGS;
+    }
+    uint64_t pos = at + 10;
+    if (flg & 4) {
+        if (pos + 2 > n) return DS_TRUNCATED;
+        uint64_t xlen = src_byte(s, pos) | (src_byte(s, pos + 1) << 8);
+        pos += 2 + xlen;
+        if (pos > n) return DS_TRUNCATED;
+    }
+    for (uint32_t f = 8; f <= 16; f <<= 1) {
+        if (flg & f) {
+            while (pos < n && src_byte(s, pos) != 0) pos++;
+            if (pos >= n) return DS_TRUNCATED;
+            pos++;
+        }
+    }
+    if (flg & 2) {
+        if (pos + 2 > n) return DS_TRUNCATED;
+        pos += 2;
+    }
+    *hl = pos - at;
+    return DS_OK;
+}
+
+template <typename CellT>
+__device__ void inflate_item(WarpSmem& S, const InflateArgs& A, uint32_t item_idx, int lane) {
+    const ChunkItem it = A.items[item_idx];
+    CellT* out = (CellT*)A.out + it.out_off;
+    ItemState st;
+    st.br.s = make_src(A.in + it.in_off, it.in_len);
+    st.br.nw = 0;
+    st.br.buf = 0;
+    st.br.bits = 0;
+    st.cur = 0;
+    st.cap = it.out_cap;
+    st.member_start = 0;
+    st.markers = 0;
+    st.status = 0;
+    st.msg = 0;
+    st.markers_ok = (it.flags & ITEM_MARKERS) != 0 && sizeof(CellT) == 2;
+    st.counting = false;
+    const uint64_t body_len = it.in_len;
+    uint64_t start = it.start_bit;
+    uint32_t trailer_crc = 0, trailer_isize = 0;
+    if (it.flags & ITEM_ONE_MEMBER) {
+        int status = 0, msg = 0;
+        uint64_t hl = 0;
+        if (lane == 0) status = dev_parse_header(st.br.s, 0, &hl, &msg);
+        status = bcast32(status);
+        msg = bcast32(msg);
+        hl = bcast64(hl);
+        if (status) {
+            st.status = status;
+            st.msg = msg;
+        }
+        start = hl * 8;
+    }
+    if (lane == 0) {
+        if (start > body_len * 8) st.status = DS_EOF;
+        else br_seek(st.br, start);
+        S.fixed_loaded = 0;
+    }
+    st.status = bcast32(st.status);
+    __syncwarp();
+    bool final_block = false;
+    uint32_t n_members = 0;
+    uint64_t end_bit = 0;
+    while (!st.status) {
+        int at_end = 0;
+        if (lane == 0) at_end = br_tell(st.br) >= it.end_hint;
+        if (bcast32(at_end)) break;
+        // one member: blocks until BFINAL or the chunk boundary
+        int bfinal = 0;
+        for (;;) {
+            uint32_t bt = 0;
+            int status = 0;
+            if (lane == 0) {
+                bfinal = (int)br_read(st.br, 1);
+                bt = br_read(st.br, 2);
+                if (br_past_end(st.br)) status = DS_EOF;
+            }
+            bfinal = bcast32(bfinal);
+            bt = (uint32_t)bcast32((int32_t)bt);
+            status = bcast32(status);
+            if (status) {
+                st.status = status;
+                break;
+            }
+            if (bt == 0) {
+                stored_block<CellT>(S, st, out, lane);
+            } else if (bt == 1) {
+                load_fixed(S, lane);
+                decode_codes<CellT>(S, st, out, lane);
+            } else if (bt == 2) {
+                read_dynamic(S, st, lane);
+                if (!st.status) decode_codes<CellT>(S, st, out, lane);
+            } else {
+                st.status = DS_INVALID;
+                st.msg = MSG_RESERVED_BTYPE;
+            }
+            if (st.status || bfinal) break;
+            int past = 0;
+            if (lane == 0) past = br_tell(st.br) >= it.end_hint;
+            if (bcast32(past)) break;
+        }
+        if (st.status || !bfinal) break;
+        // member trailer (pipeline.rs:1124-1165)
+        int status = 0, msg = 0, fin = 0;
+        uint64_t after = 0, hl = 0;
+        if (lane == 0) {
+            br_consume(st.br, st.br.bits & 7);
+            uint64_t tb = br_tell(st.br) >> 3;
+            if (tb + 8 > body_len) {
+                status = DS_TRUNCATED;
+            } else {
+                trailer_crc = le32_at(st.br.s, tb);
+                trailer_isize = le32_at(st.br.s, tb + 4);
+                if (!(it.flags & ITEM_ONE_MEMBER)) {
+                    uint32_t slot = atomicAdd(A.mb_count, 1u);
+                    if (slot < A.mb_cap) {
+                        MemberRec r;
+                        r.item = it.id;
+                        r.seq = n_members;
+                        r.cell_off = st.cur;
+                        r.crc = trailer_crc;
+                        r.isize = trailer_isize;
+                        r.trailer_byte = tb;
+                        A.mbs[slot] = r;
+                    }
+                }
+                after = tb + 8;
+                if (after >= body_len || (it.flags & ITEM_ONE_MEMBER)) {
+                    fin = 1;
+                } else {
+                    status = dev_parse_header(st.br.s, after, &hl, &msg);
+                    if (!status) br_seek(st.br, (after + hl) * 8);
+                }
+            }
+        }
+        status = bcast32(status);
+        msg = bcast32(msg);
+        fin = bcast32(fin);
+        after = bcast64(after);
+        n_members++;
+        if (status) {
+            st.status = status;
+            st.msg = msg;
+            break;
+        }
+        if (fin) {
+            final_block = true;
+            end_bit = after * 8;
+            break;
+        }
+        st.member_start = st.cur;
+        st.markers_ok = false;
+    }
+    if (lane == 0) {
+        ChunkResult r;
+        r.n_cells = st.cur;
+        r.actual_end_bit = final_block ? end_bit : br_tell(st.br);
+        r.status = st.status ? st.status : (st.counting ? DS_OVERFLOW : DS_OK);
+        r.msg = st.msg;
+        r.final_block = final_block ? 1 : 0;
+        r.n_members = n_members;
+        r.markers = st.markers;
+        r.err_bit = br_tell(st.br);
+        if (it.flags & ITEM_ONE_MEMBER) {
+            // batch mode: the trailer fields travel in place of the marker count
+            r.markers = ((uint64_t)trailer_isize << 32) | trailer_crc;
+        }
+        A.results[item_idx] = r;
+    }
+    __syncwarp();
+}
+
+template <typename CellT>
+__global__ void k_inflate(InflateArgs A) {
+    RRG_DYN_SMEM(smem_raw);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    WarpSmem& S = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
+    for (;;) {
+        uint32_t idx = 0;
+        if (lane == 0) idx = atomicAdd(A.queue, 1u);
+        idx = (uint32_t)bcast32((int32_t)idx);
+        if (idx >= A.n_items) break;
+        uint32_t item = A.order ? A.order[idx] : idx;
+        inflate_item<CellT>(S, A, item, lane);
+    }
+}
+
+// ------------------------------------------------------- block finder
+// One warp per target. The 13-bit prefilter of block_finder.rs:60-101 (BFINAL=0,
+// BTYPE=2, HLIT<=29, HDIST<=29) gives each offset its skip distance; the warp
+// evaluates a tile of offsets in parallel (skip distance, and the strict
+// verification for every prefilter candidate), then lane 0 walks the skip
+// chain through the tile exactly as find_next_dynamic_block does.
+constexpr int FIND_TILE = 1024;
+
+struct FindArgs {
+    const uint8_t* body;
+    uint64_t body_len;
+    const uint64_t* targets;
+    const uint64_t* limits;
+    uint64_t* found;
+    uint32_t n;
+    uint32_t* queue;
+    const uint8_t* next_lut;  // 8192 entries
+    uint32_t tile;            // offsets evaluated per tile (<= FIND_TILE, multiple of 32)
+};
+
+struct FindSmem {
+    uint8_t step[FIND_TILE];
+    uint8_t ok[FIND_TILE];
+};
+
+// Per-thread bit cursor for candidate verification with the reference's exact
+// availability rules (bitreader.rs refill/peek: a read of n bits fails unless n
+// bits remain; a Huffman probe needs 10 bits, a long code 15).
+struct VCur {
+    const Src* s;
+    uint64_t pos;   // bit position relative to s->lo
+    uint64_t total; // bits available
+};
+__device__ __forceinline__ uint32_t vpeek(const VCur& c, uint32_t n) {  // n <= 25, caller checks availability
+    uint64_t a = c.pos + c.s->lo * 8;
+    uint64_t w = a >> 5;
+    uint64_t v = (uint64_t)src_word(*c.s, w) | ((uint64_t)src_word(*c.s, w + 1) << 32);
+    return (uint32_t)(v >> (a & 31)) & ((1u << n) - 1u);
+}
+__device__ __forceinline__ bool vread(VCur& c, uint32_t n, uint32_t* v) {
+    if (c.pos + n > c.total) return false;
+    *v = n ? vpeek(c, n) : 0;
+    c.pos += n;
+    return true;
+}
+// canonical decode (count/symbol form); the symbol's code length is returned in *len.
+__device__ __forceinline__ int vdecode(VCur& c, const uint16_t* count, const uint16_t* sym) {
+    if (c.pos + 10 > c.total) return -1;
+    uint32_t bits = vpeek(c, c.pos + 15 <= c.total ? 15 : (uint32_t)(c.total - c.pos));
+    int code = 0, first = 0, index = 0;
+    for (int l = 1; l <= 15; l++) {
+        code |= (int)((bits >> (l - 1)) & 1u);
+        int cnt = count[l];
+        if (code - cnt < first) {
+            if (l > 10 && c.pos + 15 > c.total) return -1;
+            c.pos += (uint64_t)l;
+            return sym[index + (code - first)];
+        }
+        index += cnt;
+        first += cnt;
+        first <<= 1;
+        code <<= 1;
+    }
+    return -1;
+}
+// Strict canonical tables (huffman.rs strict build): counts + symbols sorted.
+__device__ bool vbuild(const uint8_t* len, int n, uint16_t* count, uint16_t* sym) {
+    for (int l = 0; l < 16; l++) count[l] = 0;
+    for (int s = 0; s < n; s++) count[len[s]]++;
+    count[0] = 0;
+    uint32_t total = 0, nsym = 0;
+    for (int l = 1; l < 16; l++) {
+        total += (uint32_t)count[l] << (15 - l);
+        nsym += count[l];
+    }
+    if (nsym >= 2 && total != 32768u) return false;  // oversubscribed or incomplete
+    uint16_t offs[16];
+    offs[1] = 0;
+    for (int l = 1; l < 15; l++) offs[l + 1] = offs[l] + count[l];
+    for (int s = 0; s < n; s++)
+        if (len[s]) sym[offs[len[s]]++] = (uint16_t)s;
+    return true;
+}
+
+// block_finder.rs:175-301 verify_candidate, read_dynamic_header_strict_into, trial_decode.
+__device__ __noinline__ bool verify_candidate(const Src& s, uint64_t total_bits, uint64_t pos) {
+    VCur c{&s, pos, total_bits};
+    uint32_t v;
+    if (!vread(c, 3, &v)) return false;
+    uint32_t hlit, hdist, hclen;
+    if (!vread(c, 5, &hlit) || !vread(c, 5, &hdist) || !vread(c, 4, &hclen)) return false;
+    hlit += 257;
+    hdist += 1;
+    hclen += 4;
+    if (hlit > 286 || hdist > 30) return false;
+    uint8_t cl[19];
+    for (int i = 0; i < 19; i++) cl[i] = 0;
+    for (uint32_t i = 0; i < hclen; i++) {
+        if (!vread(c, 3, &v)) return false;
+        cl[c_cl_order[i]] = (uint8_t)v;
+    }
+    // cheap strict precode check before any table work
+    {
+        uint32_t total = 0, nsym = 0;
+        for (int i = 0; i < 19; i++)
+            if (cl[i]) {
+                total += 1u << (7 - cl[i]);
+                nsym++;
+            }
+        if (nsym >= 2 && total != 128u) return false;
+    }
+    uint16_t pcount[16], psym[19];
+    if (!vbuild(cl, 19, pcount, psym)) return false;
+    uint8_t lengths[320];
+    for (int i = 0; i < 320; i++) lengths[i] = 0;
+    uint32_t total = hlit + hdist, i = 0;
+    while (i < total) {
+        int sym = vdecode(c, pcount, psym);
+        if (sym < 0) return false;
+        if (sym <= 15) {
+            lengths[i++] = (uint8_t)sym;
+        } else if (sym == 16) {
+            if (i == 0 || !vread(c, 2, &v)) return false;
+            uint32_t r = v + 3;
+            if (i + r > total) return false;
+            for (uint32_t j = 0; j < r; j++) lengths[i + j] = lengths[i - 1];
+            i += r;
+        } else if (sym == 17) {
+            if (!vread(c, 3, &v) || i + v + 3 > total) return false;
+            i += v + 3;
+        } else {
+            if (!vread(c, 7, &v) || i + v + 11 > total) return false;
+            i += v + 11;
+        }
+    }
+    if (lengths[256] == 0) return false;
+    uint16_t lcount[16], lsym[288], dcount[16], dsym[32];
+    if (!vbuild(lengths, (int)hlit, lcount, lsym)) return false;
+    if (!vbuild(lengths + hlit, (int)hdist, dcount, dsym)) return false;
+    for (int k = 0; k < 64; k++) {
+        int sym = vdecode(c, lcount, lsym);
+        if (sym < 0) return false;
+        if (sym < 256) continue;
+        if (sym == 256) return true;
+        if (sym > 285) return false;
+        uint32_t ex = c_len_extra[sym - 257];
+        if (ex && !vread(c, ex, &v)) return false;
+        int ds = vdecode(c, dcount, dsym);
+        if (ds < 0 || ds >= 30) return false;
+        uint32_t dx = c_dist_extra[ds];
+        if (dx && !vread(c, dx, &v)) return false;
+    }
+    return true;
+}
+
+__global__ void k_find_blocks(FindArgs A) {
+    RRG_DYN_SMEM(smem_raw);
+    __shared__ uint8_t lut[8192];
+    for (int i = threadIdx.x; i < 8192; i += blockDim.x) lut[i] = A.next_lut[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    FindSmem& S = reinterpret_cast<FindSmem*>(smem_raw)[warp];
+    const Src src = make_src(A.body, A.body_len);
+    const uint64_t total_bits = A.body_len * 8;
+    const uint32_t tile = A.tile;
+    for (;;) {
+        uint32_t idx = 0;
+        if (lane == 0) idx = atomicAdd(A.queue, 1u);
+        idx = (uint32_t)bcast32((int32_t)idx);
+        if (idx >= A.n) break;
+        uint64_t from = A.targets[idx];
+        uint64_t limit = A.limits[idx] < total_bits ? A.limits[idx] : total_bits;
+        uint64_t result = ~0ull;
+        uint64_t pos = from;
+        bool done = from >= limit;
+        while (!done) {
+            const uint64_t tb = pos;
+            for (uint32_t k = lane; k < tile; k += 32) {
+                uint64_t p = tb + k;
+                uint8_t stp = 255, ok = 0;
+                if (p + 13 <= limit) {
+                    uint64_t a = p + src.lo * 8;
+                    uint64_t w = a >> 5;
+                    uint64_t v = (uint64_t)src_word(src, w) | ((uint64_t)src_word(src, w + 1) << 32);
+                    uint32_t win = (uint32_t)(v >> (a & 31)) & 0x1fffu;
+                    stp = lut[win];
+                    if (stp == 0) ok = verify_candidate(src, total_bits, p) ? 1 : 0;
+                }
+                S.step[k] = stp;
+                S.ok[k] = ok;
+            }
+            __syncwarp();
+            int d = 0;
+            uint64_t np = pos, res = ~0ull;
+            if (lane == 0) {
+                while (np < tb + tile) {
+                    uint32_t k = (uint32_t)(np - tb);
+                    uint8_t stp = S.step[k];
+                    if (stp == 255) {
+                        d = 1;
+                        break;
+                    }
+                    if (stp == 0) {
+                        if (S.ok[k]) {
+                            res = np;
+                            d = 1;
+                            break;
+                        }
+                        np += 1;
+                    } else {
+                        np += stp;
+                    }
+                }
+            }
+            d = bcast32(d);
+            np = bcast64(np);
+            res = bcast64(res);
+            __syncwarp();
+            if (d) {
+                result = res;
+                done = true;
+            }
+            pos = np;
+            if (pos + 13 > limit) done = true;
+        }
+        if (lane == 0) A.found[idx] = result;
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------------- marker resolution
+// One CTA per output tile of RES_TILE cells of one chunk. A marker cell names
+// the byte `off` positions before its chunk's first byte; that byte lives in
+// an earlier chunk (and may itself be a marker), so each marker follows the
+// chain to a literal cell. Results are staged in shared memory and written
+// with 16-byte stores.
+constexpr int RES_THREADS = 256;
+constexpr int RES_PER_THREAD = 16;
+constexpr int RES_TILE = RES_THREADS * RES_PER_THREAD;
+
+struct ResolveArgs {
+    const uint16_t* cells;
+    const ResolveChunk* chunks;
+    const uint64_t* tile_start;  // n_chunks + 1 prefix of tiles per chunk
+    uint32_t n_chunks;
+    uint64_t n_tiles;
+    uint8_t* out;
+    uint32_t* err;           // [0] flag, [1] chunk, [2] cell lo, [3] cell hi
+    unsigned long long* markers;  // count of marker cells resolved
+};
+
+__device__ __forceinline__ bool chase(const ResolveArgs& A, uint32_t k, uint32_t v, uint32_t* byte) {
+    for (;;) {
+        const ResolveChunk ck = A.chunks[k];
+        uint64_t off = v & 0x7fffu;
+        if (ck.out_start < off + 1 || ck.out_start - 1 - off < ck.member_start) return false;
+        uint64_t target = ck.out_start - 1 - off;
+        uint32_t j = k;
+        do {
+            j--;
+        } while (A.chunks[j].out_start > target || A.chunks[j].out_start + A.chunks[j].n_cells <= target);
+        const ResolveChunk cj = A.chunks[j];
+        v = A.cells[cj.slot_off + (target - cj.out_start)];
+        if (!(v & MARKER16)) {
+            *byte = v & 0xffu;
+            return true;
+        }
+        k = j;
+    }
+}
+
+__global__ void __launch_bounds__(RES_THREADS) k_resolve(ResolveArgs A) {
+    __shared__ __align__(16) uint8_t stage[RES_TILE];
+    __shared__ uint32_t s_chunk;
+    __shared__ uint32_t s_bad;
+    for (uint64_t t = blockIdx.x; t < A.n_tiles; t += gridDim.x) {
+        if (threadIdx.x == 0) {
+            uint32_t lo = 0, hi = A.n_chunks - 1;
+            while (lo < hi) {
+                uint32_t mid = (lo + hi + 1) >> 1;
+                if (A.tile_start[mid] <= t) lo = mid;
+                else hi = mid - 1;
+            }
+            s_chunk = lo;
+            s_bad = 0;
+        }
+        __syncthreads();
+        const uint32_t k = s_chunk;
+        const ResolveChunk ck = A.chunks[k];
+        const uint64_t c0 = (t - A.tile_start[k]) * (uint64_t)RES_TILE;
+        const uint64_t cn = ck.n_cells - c0 < (uint64_t)RES_TILE ? ck.n_cells - c0 : (uint64_t)RES_TILE;
+        const uint32_t mine = threadIdx.x * RES_PER_THREAD;
+        uint32_t nmk = 0, bad = 0;
+        if (mine < cn) {
+            const uint16_t* p = A.cells + ck.slot_off + c0 + mine;
+            uint32_t cell[RES_PER_THREAD];
+            if (mine + RES_PER_THREAD <= cn) {
+                uint4 a = *reinterpret_cast<const uint4*>(p);
+                uint4 b = *reinterpret_cast<const uint4*>(p + 8);
+                uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+                for (int i = 0; i < 8; i++) {
+                    cell[2 * i] = w[i] & 0xffffu;
+                    cell[2 * i + 1] = w[i] >> 16;
+                }
+            } else {
+                for (int i = 0; i < RES_PER_THREAD; i++) cell[i] = (mine + i < cn) ? p[i] : 0u;
+            }
+            for (int i = 0; i < RES_PER_THREAD; i++) {
+                uint32_t v = cell[i];
+                if (v & MARKER16) {
+                    nmk++;
+                    if (!chase(A, k, v, &v)) bad = 1;
+                }
+                stage[mine + i] = (uint8_t)v;
+            }
+        }
+        if (bad) atomicOr(&s_bad, 1u);
+        if (nmk) atomicAdd(A.markers, (unsigned long long)nmk);
+        __syncthreads();
+        if (s_bad && threadIdx.x == 0 && atomicCAS(A.err, 0u, 1u) == 0u) {
+            A.err[1] = k;
+            A.err[2] = (uint32_t)c0;
+            A.err[3] = (uint32_t)(c0 >> 32);
+        }
+        // write stage[0..cn) to out[ck.out_start + c0 ...] with aligned 16-byte stores
+        uint8_t* dst = A.out + ck.out_start + c0;
+        const uint32_t head = (uint32_t)((16 - ((uintptr_t)dst & 15)) & 15);
+        const uint32_t h = head < cn ? head : (uint32_t)cn;
+        if (threadIdx.x < h) dst[threadIdx.x] = stage[threadIdx.x];
+        const uint32_t body = (uint32_t)((cn - h) / 16);
+        for (uint32_t i = threadIdx.x; i < body; i += blockDim.x) {
+            const uint8_t* sp = stage + h + i * 16;
+            uint4 v;
+            uint8_t tmp[16];
+            for (int q = 0; q < 16; q++) tmp[q] = sp[q];
+            v.x = (uint32_t)tmp[0] | ((uint32_t)tmp[1] << 8) | ((uint32_t)tmp[2] << 16) | ((uint32_t)tmp[3] << 24);
+            v.y = (uint32_t)tmp[4] | ((uint32_t)tmp[5] << 8) | ((uint32_t)tmp[6] << 16) | ((uint32_t)tmp[7] << 24);
+            v.z = (uint32_t)tmp[8] | ((uint32_t)tmp[9] << 8) | ((uint32_t)tmp[10] << 16) | ((uint32_t)tmp[11] << 24);
+            v.w = (uint32_t)tmp[12] | ((uint32_t)tmp[13] << 8) | ((uint32_t)tmp[14] << 16) | ((uint32_t)tmp[15] << 24);
+            *reinterpret_cast<uint4*>(dst + h + i * 16) = v;
+        }
+        for (uint32_t i = h + body * 16 + threadIdx.x; i < cn; i += blockDim.x) dst[i] = stage[i];
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------- CRC-32
+// Raw CRC (register starts at 0, no final inversion) is linear:
+//   raw(A||B) = raw(A) * x^(8|B|) + raw(B)   (mod P)
+// and crc32(M) = raw(M) ^ (0xffffffff * x^(8|M|)) ^ 0xffffffff.
+// Multiplication mod P is bit-serial in the reflected domain (bit 31 = x^0).
+__device__ __forceinline__ uint32_t gf2_mulmod(uint32_t a, uint32_t b) {
+    uint32_t p = 0;
+    for (int i = 0; i < 32; i++) {
+        p ^= (0u - ((a >> (31 - i)) & 1u)) & b;
+        b = (b >> 1) ^ ((0u - (b & 1u)) & 0xEDB88320u);
+    }
+    return p;
+}
+__device__ __forceinline__ uint32_t xpow8n(uint64_t n) {  // x^(8n) mod P
+    uint32_t p = 0x80000000u;
+    int k = 3;
+    while (n) {
+        if (n & 1) p = gf2_mulmod(c_x2k[k], p);
+        n >>= 1;
+        k++;
+    }
+    return p;
+}
+
+constexpr int CRC_THREADS = 256;
+
+struct CrcArgs {
+    const uint8_t* data;
+    const CrcPiece* pieces;
+    uint32_t n_pieces;
+    uint32_t* piece_crc;   // raw CRC per piece
+    const uint32_t* table; // 8 x 256 slice-by-8 table
+};
+
+// One CTA per piece; each warp takes a contiguous 1/8th, each lane a
+// contiguous 1/32nd of that; lanes and warps are combined with gf2_mulmod.
+__global__ void __launch_bounds__(CRC_THREADS) k_crc_pieces(CrcArgs A) {
+    __shared__ uint32_t T[8][256];
+    __shared__ uint32_t wcrc[CRC_THREADS / 32];
+    __shared__ uint64_t wlen[CRC_THREADS / 32];
+    for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) T[i >> 8][i & 255] = A.table[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (uint32_t pi = blockIdx.x; pi < A.n_pieces; pi += gridDim.x) {
+        const CrcPiece pc = A.pieces[pi];
+        const uint64_t per_thread = (pc.len + blockDim.x - 1) / blockDim.x;
+        const uint64_t seg = (per_thread + 7) & ~7ull;
+        const uint64_t t = (uint64_t)warp * 32 + lane;
+        uint64_t b = t * seg;
+        uint64_t e = b + seg;
+        if (b > pc.len) b = pc.len;
+        if (e > pc.len) e = pc.len;
+        const uint8_t* p = A.data + pc.start;
+        uint32_t c = 0;
+        uint64_t i = b;
+        for (; i < e && ((uintptr_t)(p + i) & 7); i++) c = T[0][(c ^ p[i]) & 0xff] ^ (c >> 8);
+        for (; i + 8 <= e; i += 8) {
+            uint2 w = *reinterpret_cast<const uint2*>(p + i);
+            uint32_t lo = w.x ^ c, hi = w.y;
+            c = T[7][lo & 0xff] ^ T[6][(lo >> 8) & 0xff] ^ T[5][(lo >> 16) & 0xff] ^ T[4][lo >> 24] ^
+                T[3][hi & 0xff] ^ T[2][(hi >> 8) & 0xff] ^ T[1][(hi >> 16) & 0xff] ^ T[0][hi >> 24];
+        }
+        for (; i < e; i++) c = T[0][(c ^ p[i]) & 0xff] ^ (c >> 8);
+        uint64_t len = e - b;
+        // combine lanes in order: (c_a, l_a) (+) (c_b, l_b) = (c_a*x^(8 l_b) ^ c_b, l_a + l_b)
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t oc = __shfl_down_sync(FULLMASK, c, o);
+            uint64_t ol = __shfl_down_sync(FULLMASK, len, o);
+            if ((lane & (2 * o - 1)) == 0 && lane + o < 32) {
+                c = (ol ? gf2_mulmod(c, xpow8n(ol)) : c) ^ oc;
+                len += ol;
+            }
+        }
+        if (lane == 0) {
+            wcrc[warp] = c;
+            wlen[warp] = len;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t cc = wcrc[0];
+            for (int w = 1; w < nw; w++)
+                if (wlen[w]) cc = gf2_mulmod(cc, xpow8n(wlen[w])) ^ wcrc[w];
+            A.piece_crc[pi] = cc;
+        }
+        __syncthreads();
+    }
+}
+
+struct CrcMemberArgs {
+    const CrcPiece* pieces;
+    const uint32_t* piece_crc;
+    const uint32_t* member_piece_start;  // n_members + 1
+    uint32_t n_members;
+    const uint32_t* expected_crc;
+    const uint32_t* expected_isize;
+    uint32_t* got_crc;
+    uint64_t* got_len;
+    int32_t* status;  // DS_OK / DS_CRC / DS_ISIZE
+};
+
+// One warp per member: fold its pieces in order, finalise, compare with the trailer.
+__global__ void k_crc_members(CrcMemberArgs A) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (m >= A.n_members) return;  // warp-uniform
+    const uint32_t p0 = A.member_piece_start[m], p1 = A.member_piece_start[m + 1];
+    const uint32_t np = p1 - p0;
+    const uint32_t per = (np + 31) / 32;
+    uint32_t b = p0 + lane * per, e = b + per;
+    if (b > p1) b = p1;
+    if (e > p1) e = p1;
+    uint32_t c = 0;
+    uint64_t len = 0;
+    for (uint32_t i = b; i < e; i++) {
+        uint64_t l = A.pieces[i].len;
+        c = (l ? gf2_mulmod(c, xpow8n(l)) : c) ^ A.piece_crc[i];
+        len += l;
+    }
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t oc = __shfl_down_sync(FULLMASK, c, o);
+        uint64_t ol = __shfl_down_sync(FULLMASK, len, o);
+        if ((lane & (2 * o - 1)) == 0 && lane + o < 32) {
+            c = (ol ? gf2_mulmod(c, xpow8n(ol)) : c) ^ oc;
+            len += ol;
+        }
+    }
+    if (lane == 0) {
+        uint32_t crc = c ^ (len ? gf2_mulmod(0xffffffffu, xpow8n(len)) : 0xffffffffu) ^ 0xffffffffu;
+        A.got_crc[m] = crc;
+        A.got_len[m] = len;
+        int32_t st = DS_OK;
+        if (crc != A.expected_crc[m]) st = DS_CRC;
+        else if ((uint32_t)len != A.expected_isize[m]) st = DS_ISIZE;
+        A.status[m] = st;
+    }
+}
+
+}  // namespace rrg

@@ -1,0 +1,108 @@
+import hashlib
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+REFERENCE_CORPUS = "/root/reference/tests/corpus"
+EMU_DIR = os.path.join(ROOT, "tests", "emu")
+EMU_LIB = os.path.join(EMU_DIR, "librrg_gpu_emu.so")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and the built librrg_gpu.so")
+    config.addinivalue_line("markers", "slow: longer CPU tests")
+
+
+def sha256(b: bytes) -> str:
+    return hashlib.sha256(b).hexdigest()
+
+
+def golden_fixtures():
+    sums = json.load(open(os.path.join(GOLDEN, "sums.json")))
+    return [(name, os.path.join(GOLDEN, name), meta) for name, meta in sorted(sums.items())]
+
+
+def ascii_payload(n: int, seed: int) -> bytes:
+    """Seeded printable-ASCII LCG payload (the reference tests' generator shape)."""
+    import numpy as np
+    out = np.empty(n, dtype=np.uint8)
+    s = (seed | 1) & 0xFFFFFFFFFFFFFFFF
+    # vectorised LCG: s_{k} = a^k s_0 + c (a^k - 1)/(a - 1) is awkward in numpy; step in blocks
+    a, c = 6364136223846793005, 1442695040888963407
+    mask = (1 << 64) - 1
+    i = 0
+    block = []
+    while i < n:
+        s = (s * a + c) & mask
+        block.append(((s >> 56) % 95) + 32)
+        i += 1
+        if len(block) == 65536 or i == n:
+            out[i - len(block):i] = block
+            block = []
+    return out.tobytes()
+
+
+def gzip_cli(data: bytes, level: int = 6) -> bytes:
+    return subprocess.run(["gzip", f"-{level}", "-n", "-c"], input=data, stdout=subprocess.PIPE,
+                          check=True).stdout
+
+
+def build_emu_lib() -> str:
+    """Compile the product sources against the CPU warp emulation (tests only)."""
+    srcs = [os.path.join(ROOT, "rusty_rapidgzip_b200", "csrc", f) for f in
+            ("rrg_gpu.cu", "rrg_kernels.cuh", "rrg_common.h")] + [os.path.join(EMU_DIR, "cuda_emu.h"),
+                                                                  os.path.join(ROOT, "include", "rrg_gpu.h")]
+    if not os.path.exists(EMU_LIB) or any(os.path.getmtime(s) > os.path.getmtime(EMU_LIB) for s in srcs):
+        subprocess.check_call([
+            "g++", "-std=c++20", "-O2", "-g", "-x", "c++", "-DRRG_EMU", "-include",
+            os.path.join(EMU_DIR, "cuda_emu.h"), "-I", os.path.join(ROOT, "include"), "-I",
+            os.path.join(ROOT, "rusty_rapidgzip_b200", "csrc"), "-fPIC", "-shared", "-pthread",
+            "-o", EMU_LIB, os.path.join(ROOT, "rusty_rapidgzip_b200", "csrc", "rrg_gpu.cu")])
+    return EMU_LIB
+
+
+@pytest.fixture(scope="session")
+def emu_decoder_factory():
+    lib = build_emu_lib()
+    from rusty_rapidgzip_b200 import Config, Decoder
+
+    def make(**kw):
+        kw.setdefault("device", -1)
+        return Decoder(Config(**kw), lib=lib)
+
+    return make
+
+
+@pytest.fixture(scope="session")
+def gpu_lib():
+    """The real CUDA build; GPU tests fail loudly when it is missing."""
+    import torch
+    assert torch.cuda.is_available(), "GPU test needs CUDA"
+    from rusty_rapidgzip_b200 import build as B
+    path = B.build()
+    assert os.path.exists(path), "librrg_gpu.so was not built"
+    return path
+
+
+@pytest.fixture()
+def gpu_decoder_factory(gpu_lib):
+    from rusty_rapidgzip_b200 import Config, Decoder
+    made = []
+
+    def make(**kw):
+        kw.setdefault("device", 0)
+        d = Decoder(Config(**kw), lib=gpu_lib)
+        made.append(d)
+        return d
+
+    yield make
+    for d in made:
+        d.close()

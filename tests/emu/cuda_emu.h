@@ -1,0 +1,247 @@
+// cuda_emu.h — CPU emulation of the CUDA subset used by rusty_rapidgzip_b200/csrc.
+//
+// TEST INFRASTRUCTURE ONLY. Lets the unit tests compile the product's kernel
+// and host sources with g++ (-DRRG_EMU -include cuda_emu.h) and run them on
+// the CPU: every thread of a block is a std::thread; warp shuffles, ballots,
+// matches and __syncwarp go through a per-warp exchange with a 32-party
+// barrier; __syncthreads is a block barrier; blocks of a launch run one after
+// another. Device memory is host memory. The resulting library is used only by
+// `-m "not gpu"` tests and never stands in for the GPU build.
+#pragma once
+#include <barrier>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <functional>
+#include <memory>
+#include <thread>
+#include <vector>
+
+#define __global__
+#define __device__
+#define __host__
+#define __forceinline__ inline
+#define __noinline__ __attribute__((noinline))
+#define __constant__
+#define __shared__ static
+#define __launch_bounds__(...)
+#define __align__(n) __attribute__((aligned(n)))
+
+struct dim3 {
+    unsigned x = 1, y = 1, z = 1;
+    dim3(unsigned a = 1, unsigned b = 1, unsigned c = 1) : x(a), y(b), z(c) {}
+};
+struct uint2 {
+    unsigned x, y;
+};
+struct __attribute__((aligned(16))) uint4 {
+    unsigned x, y, z, w;
+};
+
+typedef int cudaError_t;
+typedef void* cudaStream_t;
+typedef struct emu_event* cudaEvent_t;
+enum : int { cudaSuccess = 0, cudaErrorMemoryAllocation = 2, cudaErrorInvalidValue = 1 };
+enum cudaMemcpyKind { cudaMemcpyHostToHost, cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost, cudaMemcpyDeviceToDevice, cudaMemcpyDefault };
+enum cudaDeviceAttr { cudaDevAttrMultiProcessorCount = 16, cudaDevAttrMaxSharedMemoryPerBlockOptin = 97 };
+enum cudaFuncAttribute { cudaFuncAttributeMaxDynamicSharedMemorySize = 8 };
+#define cudaStreamNonBlocking 1u
+#define cudaEventDisableTiming 2u
+
+namespace emu {
+
+struct Warp {
+    std::barrier<> bar{32};
+    uint64_t slot[32];
+};
+struct Block {
+    std::unique_ptr<std::barrier<>> bar;
+    std::vector<std::unique_ptr<Warp>> warps;
+};
+inline thread_local Block* t_block = nullptr;
+inline thread_local Warp* t_warp = nullptr;
+inline thread_local dim3 t_tid, t_bid, t_bdim, t_gdim;
+inline std::vector<unsigned char>& dyn_buf() {
+    static std::vector<unsigned char> b;
+    return b;
+}
+inline unsigned char* dyn_smem() { return dyn_buf().data(); }
+
+inline void launch(dim3 grid, dim3 block, size_t smem, const std::function<void()>& body) {
+    unsigned nthreads = block.x;
+    auto& buf = dyn_buf();
+    if (buf.size() < smem + 64) buf.assign(smem + 64, 0);
+    for (unsigned b = 0; b < grid.x; b++) {
+        Block blk;
+        blk.bar = std::make_unique<std::barrier<>>(nthreads);
+        for (unsigned w = 0; w < (nthreads + 31) / 32; w++) blk.warps.push_back(std::make_unique<Warp>());
+        std::vector<std::thread> th;
+        th.reserve(nthreads);
+        for (unsigned t = 0; t < nthreads; t++) {
+            th.emplace_back([&, t, b] {
+                t_block = &blk;
+                t_warp = blk.warps[t / 32].get();
+                t_tid = dim3(t);
+                t_bid = dim3(b);
+                t_bdim = block;
+                t_gdim = grid;
+                body();
+            });
+        }
+        for (auto& x : th) x.join();
+    }
+}
+
+}  // namespace emu
+
+#define threadIdx (emu::t_tid)
+#define blockIdx (emu::t_bid)
+#define blockDim (emu::t_bdim)
+#define gridDim (emu::t_gdim)
+
+inline void __syncthreads() { emu::t_block->bar->arrive_and_wait(); }
+inline void __syncwarp(unsigned = 0xffffffffu) { emu::t_warp->bar.arrive_and_wait(); }
+
+template <class T>
+inline T emu_exchange(T v, int src) {
+    static_assert(sizeof(T) <= 8, "shuffle width");
+    emu::Warp* w = emu::t_warp;
+    int lane = emu::t_tid.x & 31;
+    uint64_t raw = 0;
+    std::memcpy(&raw, &v, sizeof(T));
+    w->slot[lane] = raw;
+    w->bar.arrive_and_wait();
+    uint64_t got = w->slot[src & 31];
+    w->bar.arrive_and_wait();
+    T r;
+    std::memcpy(&r, &got, sizeof(T));
+    return r;
+}
+template <class T>
+inline T __shfl_sync(unsigned, T v, int src) {
+    return emu_exchange(v, src);
+}
+template <class T>
+inline T __shfl_xor_sync(unsigned, T v, int m) {
+    return emu_exchange(v, (int)(emu::t_tid.x & 31) ^ m);
+}
+template <class T>
+inline T __shfl_down_sync(unsigned, T v, unsigned d) {
+    int lane = emu::t_tid.x & 31;
+    int src = lane + (int)d < 32 ? lane + (int)d : lane;
+    return emu_exchange(v, src);
+}
+inline unsigned __ballot_sync(unsigned, int pred) {
+    emu::Warp* w = emu::t_warp;
+    int lane = emu::t_tid.x & 31;
+    w->slot[lane] = pred ? 1 : 0;
+    w->bar.arrive_and_wait();
+    unsigned m = 0;
+    for (int i = 0; i < 32; i++)
+        if (w->slot[i]) m |= 1u << i;
+    w->bar.arrive_and_wait();
+    return m;
+}
+inline unsigned __match_any_sync(unsigned, unsigned v) {
+    emu::Warp* w = emu::t_warp;
+    int lane = emu::t_tid.x & 31;
+    w->slot[lane] = v;
+    w->bar.arrive_and_wait();
+    unsigned m = 0;
+    for (int i = 0; i < 32; i++)
+        if (w->slot[i] == v) m |= 1u << i;
+    w->bar.arrive_and_wait();
+    return m;
+}
+inline int __popc(unsigned v) { return __builtin_popcount(v); }
+inline unsigned __brev(unsigned v) {
+    unsigned r = 0;
+    for (int i = 0; i < 32; i++) r |= ((v >> i) & 1u) << (31 - i);
+    return r;
+}
+template <class T>
+inline T __ldg(const T* p) {
+    return *p;
+}
+inline unsigned atomicAdd(unsigned* p, unsigned v) { return __atomic_fetch_add(p, v, __ATOMIC_SEQ_CST); }
+inline unsigned long long atomicAdd(unsigned long long* p, unsigned long long v) {
+    return __atomic_fetch_add(p, v, __ATOMIC_SEQ_CST);
+}
+inline unsigned atomicOr(unsigned* p, unsigned v) { return __atomic_fetch_or(p, v, __ATOMIC_SEQ_CST); }
+inline unsigned atomicCAS(unsigned* p, unsigned cmp, unsigned v) {
+    __atomic_compare_exchange_n(p, &cmp, v, false, __ATOMIC_SEQ_CST, __ATOMIC_SEQ_CST);
+    return cmp;
+}
+
+// ---- runtime API (device memory is host memory)
+inline cudaError_t cudaMalloc(void** p, size_t n) {
+    *p = std::aligned_alloc(256, (n + 255) & ~(size_t)255);
+    return *p ? cudaSuccess : cudaErrorMemoryAllocation;
+}
+inline cudaError_t cudaFree(void* p) {
+    std::free(p);
+    return cudaSuccess;
+}
+inline cudaError_t cudaMallocHost(void** p, size_t n) { return cudaMalloc(p, n); }
+inline cudaError_t cudaFreeHost(void* p) { return cudaFree(p); }
+inline cudaError_t cudaMemcpy(void* d, const void* s, size_t n, cudaMemcpyKind) {
+    if (n) std::memmove(d, s, n);
+    return cudaSuccess;
+}
+inline cudaError_t cudaMemcpyAsync(void* d, const void* s, size_t n, cudaMemcpyKind k, cudaStream_t = nullptr) {
+    return cudaMemcpy(d, s, n, k);
+}
+inline cudaError_t cudaMemset(void* d, int v, size_t n) {
+    std::memset(d, v, n);
+    return cudaSuccess;
+}
+inline cudaError_t cudaMemsetAsync(void* d, int v, size_t n, cudaStream_t = nullptr) { return cudaMemset(d, v, n); }
+template <class T>
+inline cudaError_t cudaMemcpyToSymbol(T& sym, const void* src, size_t n, size_t off = 0,
+                                      cudaMemcpyKind = cudaMemcpyHostToDevice) {
+    std::memcpy((char*)&sym + off, src, n);
+    return cudaSuccess;
+}
+inline cudaError_t cudaStreamCreateWithFlags(cudaStream_t* s, unsigned) {
+    *s = (void*)0x1;
+    return cudaSuccess;
+}
+inline cudaError_t cudaStreamDestroy(cudaStream_t) { return cudaSuccess; }
+inline cudaError_t cudaStreamSynchronize(cudaStream_t) { return cudaSuccess; }
+struct emu_event {
+    int x;
+};
+inline cudaError_t cudaEventCreateWithFlags(cudaEvent_t* e, unsigned) {
+    *e = new emu_event{0};
+    return cudaSuccess;
+}
+inline cudaError_t cudaEventCreate(cudaEvent_t* e) {
+    *e = new emu_event{0};
+    return cudaSuccess;
+}
+inline cudaError_t cudaEventRecord(cudaEvent_t, cudaStream_t = nullptr) { return cudaSuccess; }
+inline cudaError_t cudaEventElapsedTime(float* ms, cudaEvent_t, cudaEvent_t) {
+    *ms = 0.f;
+    return cudaSuccess;
+}
+inline cudaError_t cudaEventSynchronize(cudaEvent_t) { return cudaSuccess; }
+inline cudaError_t cudaEventDestroy(cudaEvent_t e) {
+    delete e;
+    return cudaSuccess;
+}
+inline cudaError_t cudaGetDevice(int* d) {
+    *d = 0;
+    return cudaSuccess;
+}
+inline cudaError_t cudaSetDevice(int) { return cudaSuccess; }
+inline cudaError_t cudaDeviceGetAttribute(int* v, cudaDeviceAttr a, int) {
+    *v = a == cudaDevAttrMultiProcessorCount ? 2 : 232448;
+    return cudaSuccess;
+}
+template <class F>
+inline cudaError_t cudaFuncSetAttribute(F, cudaFuncAttribute, int) {
+    return cudaSuccess;
+}
+inline const char* cudaGetErrorString(cudaError_t e) { return e ? "emulated error" : "no error"; }
+inline cudaError_t cudaGetLastError() { return cudaSuccess; }
+inline cudaError_t cudaDeviceSynchronize() { return cudaSuccess; }

@@ -1,0 +1,298 @@
+"""Parity of the CUDA decoder (through the C ABI) with the CPU oracle.
+
+Bit-exact bytes, identical block-finder offsets, identical speculative chunk
+contents (bytes + markers + end offset), identical CRC32, identical error
+kinds. Large inputs are checked through size-independent properties: the
+SHA-256 of the whole stream and the per-member CRC32/ISIZE the decoder
+verifies itself.
+"""
+import hashlib
+import json
+import os
+import struct
+import zlib
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import GOLDEN, golden_fixtures, gzip_cli, sha256
+from rusty_rapidgzip_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(data: bytes):
+    import torch
+    t = torch.empty(max(len(data), 1), dtype=torch.uint8, device="cuda")
+    if data:
+        t[: len(data)].copy_(torch.frombuffer(bytearray(data), dtype=torch.uint8))
+    torch.cuda.synchronize()
+    return t
+
+
+@pytest.mark.parametrize("name,path,meta", golden_fixtures(), ids=[g[0] for g in golden_fixtures()])
+@pytest.mark.parametrize("gpu_chunk", [0, 4096])
+def test_golden_fixtures(gpu_decoder_factory, name, path, meta, gpu_chunk):
+    d = gpu_decoder_factory(gpu_chunk_bytes=gpu_chunk)
+    data = open(path, "rb").read()
+    out = d.decompress(data)
+    assert len(out) == meta["raw_size"]
+    assert sha256(out) == meta["sha256"]
+
+
+def test_raw_deflate_vectors(gpu_decoder_factory):
+    d = gpu_decoder_factory()
+    for v in json.load(open(os.path.join(GOLDEN, "miri_edge_vectors.json"))):
+        plain = bytes.fromhex(v["plain"])
+        gz = bytes([0x1F, 0x8B, 8, 0, 0, 0, 0, 0, 0, 0xFF]) + bytes.fromhex(v["deflate"]) + \
+            struct.pack("<II", zlib.crc32(plain), len(plain))
+        assert d.decompress(gz) == plain, v["name"]
+
+
+@pytest.mark.parametrize("gpu_chunk", [8192, 65536, 0])
+def test_fastq_level6(gpu_decoder_factory, gpu_chunk):
+    raw, gz = W.config0(8 << 20, seed=5)
+    d = gpu_decoder_factory(gpu_chunk_bytes=gpu_chunk)
+    out, st = d.count(gz)
+    assert out == len(raw)
+    got = d.decompress(gz)
+    assert got == raw
+    assert got == oracle.read_gz(gz, 4, 1 << 20)
+
+
+@pytest.mark.parametrize("gpu_chunk", [16384, 0])
+def test_zipf_level9(gpu_decoder_factory, gpu_chunk):
+    raw, gz = W.config1(24 << 20, seed=6)
+    d = gpu_decoder_factory(gpu_chunk_bytes=gpu_chunk)
+    out = d.decompress(gz)
+    assert out == raw
+
+
+def test_device_resident_matches_host(gpu_decoder_factory):
+    import torch
+    raw, gz = W.config1(16 << 20, seed=8)
+    d = gpu_decoder_factory(gpu_chunk_bytes=32768)
+    din = dev(gz)
+    dout = torch.empty(len(raw) + 64, dtype=torch.uint8, device="cuda")
+    n, st = d.decode_device(din, len(gz), dout, dout.numel())
+    assert n == len(raw)
+    assert bytes(dout[:n].cpu().numpy()) == raw
+    assert st.gpu_chunks > 1 and st.markers > 0
+    # too small an output buffer reports the size needed
+    from rusty_rapidgzip_b200 import CapacityError
+    small = torch.empty(1024, dtype=torch.uint8, device="cuda")
+    with pytest.raises(CapacityError) as e:
+        d.decode_device(din, len(gz), small, small.numel())
+    assert e.value.required == len(raw)
+
+
+def test_block_finder_parity(gpu_decoder_factory):
+    raw, gz = W.config0(4 << 20, seed=9)
+    body = gz[10:]
+    nbits = len(body) * 8
+    targets = list(range(8 * 4096, nbits, 8 * 12288))
+    limits = targets[1:] + [nbits]
+    d = gpu_decoder_factory()
+    got = d.find_blocks(dev(body), len(body), targets, limits)
+    want = [oracle.find_next_dynamic_block(body, t, lim) for t, lim in zip(targets, limits)]
+    assert got == want
+    assert sum(x is not None for x in got) > len(got) // 2
+    # exhaustive limits on random data must terminate and agree
+    g = np.random.default_rng(1).integers(0, 256, 1 << 16, dtype=np.uint8).tobytes()
+    t2 = list(range(0, len(g) * 8, 8 * 4096))
+    l2 = [len(g) * 8] * len(t2)
+    assert d.find_blocks(dev(g), len(g), t2, l2) == [oracle.find_next_dynamic_block(g, t, l) for t, l in zip(t2, l2)]
+
+
+def test_speculative_chunk_parity(gpu_decoder_factory):
+    raw, gz = W.config1(4 << 20, seed=10)
+    body = gz[10:]
+    d = gpu_decoder_factory()
+    db = dev(body)
+    b1 = oracle.find_next_dynamic_block(body, 300_000 * 8, len(body) * 8)
+    b2 = oracle.find_next_dynamic_block(body, 700_000 * 8, len(body) * 8)
+    for start, hint in ((0, b1), (b1, b2), (b2, 1 << 62)):
+        want = oracle.decode_chunk(body, start, hint)
+        got_bytes, mp, mo, end, fin = d.decode_chunk(db, len(body), start, hint)
+        assert got_bytes == want.bytes
+        assert np.array_equal(mp, want.marker_pos)
+        assert np.array_equal(mo, want.marker_off)
+        assert end == want.actual_end_bit
+        assert fin == want.final_block
+
+
+def test_resolve_markers_parity(gpu_decoder_factory):
+    import torch
+    raw, gz = W.config1(2 << 20, seed=11)
+    body = gz[10:]
+    b1 = oracle.find_next_dynamic_block(body, 200_000 * 8, len(body) * 8)
+    first = oracle.decode_chunk(body, 0, b1)
+    rest = oracle.decode_chunk(body, b1, 1 << 62)
+    tail = first.bytes[-32768:]
+    d = gpu_decoder_factory()
+    dbytes = dev(rest.bytes)
+    dpos = torch.tensor(rest.marker_pos.astype(np.int64), dtype=torch.int64, device="cuda").to(torch.int32)
+    doff = torch.tensor(rest.marker_off.astype(np.int32), device="cuda").to(torch.int16)
+    torch.cuda.synchronize()
+    d.resolve_markers(dbytes, len(rest.bytes), dpos, doff, len(rest.marker_pos), dev(tail), len(tail))
+    torch.cuda.synchronize()
+    assert bytes(dbytes[: len(rest.bytes)].cpu().numpy()) == raw[len(first.bytes):]
+
+
+@pytest.mark.parametrize("n", [0, 1, 7, 4096, (1 << 20) + 13, 40 << 20])
+def test_crc32_parity(gpu_decoder_factory, n):
+    data = np.random.default_rng(n).integers(0, 256, n, dtype=np.uint8).tobytes()
+    d = gpu_decoder_factory()
+    assert d.crc32(dev(data), n) == zlib.crc32(data)
+
+
+def test_bgzf(gpu_decoder_factory):
+    raw = W.fastq_like(12 << 20, 12)
+    b = W.bgzf(raw, 5)
+    d = gpu_decoder_factory()
+    assert d.decompress(b) == raw
+    out, st = d.count(b)
+    assert out == len(raw) and st.members == (len(raw) + 65279) // 65280
+
+
+def _stored_member(data: bytes) -> bytes:
+    n = len(data)
+    return bytes([0x1F, 0x8B, 8, 0, 0, 0, 0, 0, 0, 0xFF, 1]) + struct.pack("<HH", n, n ^ 0xFFFF) + data + \
+        struct.pack("<II", zlib.crc32(data), n)
+
+
+def _stored_bgzf(data: bytes) -> bytes:
+    n = len(data)
+    body = bytes([1]) + struct.pack("<HH", n, n ^ 0xFFFF) + data
+    hdr = bytes([0x1F, 0x8B, 8, 4, 0, 0, 0, 0, 0, 0xFF]) + struct.pack("<H", 6) + b"BC" + \
+        struct.pack("<HH", 2, 18 + len(body) + 8 - 1)
+    return hdr + body + struct.pack("<II", zlib.crc32(data), n)
+
+
+@pytest.mark.parametrize("first,second", [("bgzf", "bgzf"), ("gz", "gz"), ("bgzf", "gz"), ("gz", "bgzf")])
+def test_bgzf_gz_combinations(gpu_decoder_factory, first, second):
+    mk = {"gz": _stored_member, "bgzf": _stored_bgzf}
+    d = gpu_decoder_factory()
+    assert d.decompress(mk[first](b"hello ") + mk[second](b"world")) == b"hello world"
+
+
+def test_batch_of_files(gpu_decoder_factory):
+    import torch
+    files = W.config3_files(n_files=12, seed=4, lo=4 << 10, hi=2 << 20)
+    blobs = [gz for _, gz in files]
+    offs = np.cumsum([0] + [len(b) for b in blobs])[:-1].tolist()
+    raws = [r for r, _ in files]
+    ooffs = np.cumsum([0] + [len(r) for r in raws])[:-1].tolist()
+    din = dev(b"".join(blobs))
+    dout = torch.empty(sum(len(r) for r in raws) + 16, dtype=torch.uint8, device="cuda")
+    d = gpu_decoder_factory()
+    lens, status, st = d.decode_batch(din, offs, [len(b) for b in blobs], dout, ooffs, [len(r) for r in raws])
+    assert status == [0] * len(files)
+    assert lens == [len(r) for r in raws]
+    host = dout.cpu().numpy().tobytes()
+    for r, o in zip(raws, ooffs):
+        assert host[o:o + len(r)] == r
+
+
+def test_concat_members(gpu_decoder_factory):
+    parts = [W.fastq_like(n, i) for i, n in enumerate([1, 100, 65_537, 1, 300_000, 7, 1_000_000])]
+    gz = b"".join(gzip_cli(p, [6, 1, 9][i % 3]) for i, p in enumerate(parts))
+    for gc in (4096, 65536):
+        d = gpu_decoder_factory(gpu_chunk_bytes=gc)
+        assert d.decompress(gz) == b"".join(parts)
+    parts = [b"", b"abc", b"", b"", b"def" * 1000, b""] + [f"member-{i}-payload\n".encode() for i in range(500)]
+    gz = b"".join(gzip_cli(p) for p in parts)
+    d = gpu_decoder_factory(gpu_chunk_bytes=4096)
+    assert d.decompress(gz) == b"".join(parts)
+
+
+def test_nested_gzip(gpu_decoder_factory):
+    original = np.random.default_rng(0xC0FFEE).integers(32, 127, 2 << 20, dtype=np.uint8).tobytes()
+    inner = gzip_cli(original, 6)
+    outer = gzip_cli(inner, 6)
+    d = gpu_decoder_factory(gpu_chunk_bytes=16384)
+    out, st = [], None
+    st = d.decode_host(outer, out.append)
+    assert b"".join(out) == inner
+    assert st.speculation_failures > 0
+
+
+def test_mixed_block_types(gpu_decoder_factory):
+    p = W.fastq_like(300_000, 1) + W.random_bytes(300_000, 5) + W.zipf_text(300_000, 3)
+    gz = gzip_cli(p, 1)
+    d = gpu_decoder_factory(gpu_chunk_bytes=16384)
+    assert d.decompress(gz) == p
+
+
+def _expect(code, fn):
+    from rusty_rapidgzip_b200 import RrgError
+    with pytest.raises(RrgError) as e:
+        fn()
+    return e.value
+
+
+def test_error_kinds_match_oracle(gpu_decoder_factory):
+    d = gpu_decoder_factory()
+    good = gzip_cli(W.fastq_like(200_000, 3), 6)
+    cases = {
+        "magic": b"\x00\x01" + good[2:],
+        "method": good[:2] + b"\x07" + good[3:],
+        "flags": good[:3] + b"\x20" + good[4:],
+        "empty": b"",
+        "crc": good[:-8] + bytes([good[-8] ^ 1]) + good[-7:],
+        "isize": good[:-4] + struct.pack("<I", 5),
+        "second_crc": gzip_cli(b"first") + good[:-8] + bytes([good[-8] ^ 1]) + good[-7:],
+    }
+    for name, data in cases.items():
+        with pytest.raises(oracle.OracleError) as oe:
+            oracle.read_gz(data, 2)
+        err = _expect(None, lambda: d.decompress(data))
+        assert err.code == oe.value.code, name
+        if name in ("crc", "second_crc"):
+            assert err.member == oe.value.member
+            assert err.expected == oe.value.expected and err.got_crc == oe.value.got_crc
+    # truncation: an error either way (EOF or Truncated, like the reference)
+    err = _expect(None, lambda: d.decompress(good[:-4]))
+    assert err.code in (5, 8)
+
+
+def test_read_gz_path_sink_and_close(tmp_path, gpu_decoder_factory):
+    from rusty_rapidgzip_b200 import SinkClosed, read_gz, Config
+    raw, gz = W.config0(6 << 20, seed=13)
+    p = tmp_path / "x.gz"
+    p.write_bytes(gz)
+    chunks = []
+    st = read_gz(p, chunks.append, Config(device=0, chunk_size_bytes=1 << 20))
+    assert b"".join(chunks) == raw
+    assert st.uncompressed_bytes == len(raw) and st.compressed_bytes == len(gz)
+    assert st.chunks_decoded == len(chunks) and len(chunks) > 1
+    got = []
+
+    def closing(b):
+        got.append(b)
+        raise SinkClosed()
+
+    st2 = read_gz(p, closing, Config(device=0, chunk_size_bytes=1 << 20))
+    assert len(got) == 1 and raw.startswith(got[0])
+    z = tmp_path / "zero.gz"
+    z.write_bytes(b"")
+    from rusty_rapidgzip_b200 import GzipError
+    with pytest.raises(GzipError) as e:
+        read_gz(z, lambda b: None, Config(device=0))
+    assert e.value.kind == "Truncated"
+
+
+def test_large_stream_properties(gpu_decoder_factory):
+    """256 MiB of the Zipf-text shape: SHA-256 of the whole stream plus the
+    decoder's own CRC32/ISIZE check; device and host entry points agree."""
+    import torch
+    raw, gz = W.config1(256 << 20, seed=14)
+    d = gpu_decoder_factory()
+    din = dev(gz)
+    dout = torch.empty(len(raw) + 64, dtype=torch.uint8, device="cuda")
+    n, st = d.decode_device(din, len(gz), dout, dout.numel())
+    assert n == len(raw)
+    h = hashlib.sha256(dout[:n].cpu().numpy().tobytes()).hexdigest()
+    assert h == sha256(raw)
+    assert st.members == 1 and st.gpu_chunks > 100
