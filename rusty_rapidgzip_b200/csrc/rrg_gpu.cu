@@ -624,14 +624,11 @@ int member_route(rrg_ctx* c, const uint8_t* d_file, uint64_t len, uint64_t body_
             // false boundary or failed speculative decode: re-decode from the anchor
             c->st.speculation_failures++;
             if (it.end_hint != ~0ull && expected >= it.end_hint) continue;  // empty chunk
+            // the anchor lies at or after the guessed start (the previous chunk
+            // stops on a block edge at/after its end hint), so the re-decode
+            // spans no more input than the guess did and reuses its slot
             it.start_bit = expected;
             it.id = next_id++;
-            if (arena + it.out_cap > arena_cap) {
-                set_err(err, RRG_ERR_OUT_OF_MEMORY, "re-decode arena exhausted");
-                return RRG_ERR_OUT_OF_MEMORY;
-            }
-            it.out_off = arena;
-            arena += it.out_cap;
             std::vector<ChunkItem> one{it};
             std::vector<ChunkResult> r1;
             std::vector<MemberRec> m1;

@@ -1,0 +1,86 @@
+"""Kernel and host logic of the product sources, compiled against the CPU warp
+emulation (tests/emu/cuda_emu.h) and checked against the oracle on small
+inputs. Runs without a GPU; the GPU build is covered by test_gpu_parity.py."""
+import os
+import struct
+import zlib
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import GOLDEN, gzip_cli, sha256
+from rusty_rapidgzip_b200 import workloads as W
+
+
+def haddr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+SMALL_GOLDEN = ["synth-empty.gz", "synth-single-byte.gz", "synth-concat-members.gz", "synth-zeros-1m.gz",
+                "synth-spaces-1m.gz"]
+
+
+@pytest.mark.parametrize("name", SMALL_GOLDEN)
+def test_small_golden(emu_decoder_factory, name):
+    import json
+    meta = json.load(open(os.path.join(GOLDEN, "sums.json")))[name]
+    d = emu_decoder_factory()
+    out = d.decompress(open(os.path.join(GOLDEN, name), "rb").read())
+    assert sha256(out) == meta["sha256"]
+
+
+def test_multi_chunk_speculative(emu_decoder_factory):
+    raw, gz = W.config1(192 << 10, seed=3)
+    d = emu_decoder_factory(gpu_chunk_bytes=8192)
+    out, st = [], None
+    st = d.decode_host(gz, out.append)
+    assert b"".join(out) == raw
+    assert st.gpu_chunks >= 3 and st.markers > 0
+
+
+def test_bgzf_and_concat(emu_decoder_factory):
+    raw = W.fastq_like(150_000, 2)
+    d = emu_decoder_factory()
+    assert d.decompress(W.bgzf(raw, 5)) == raw
+    parts = [b"", b"abc", b"x" * 5000, b""]
+    assert d.decompress(b"".join(gzip_cli(p) for p in parts)) == b"".join(parts)
+
+
+def test_errors(emu_decoder_factory):
+    from rusty_rapidgzip_b200 import RrgError
+    d = emu_decoder_factory()
+    good = gzip_cli(b"some payload " * 200, 6)
+    for data in (b"\x00\x01" + good[2:], good[:-8] + bytes([good[-8] ^ 1]) + good[-7:],
+                 good[:-4] + struct.pack("<I", 5), b""):
+        with pytest.raises(oracle.OracleError) as oe:
+            oracle.read_gz(data, 2)
+        with pytest.raises(RrgError) as ge:
+            d.decompress(data)
+        assert ge.value.code == oe.value.code
+
+
+def test_finder_parity(emu_decoder_factory):
+    raw, gz = W.config0(400_000, seed=4)
+    body = np.frombuffer(gz[10:], dtype=np.uint8).copy()
+    nbits = body.size * 8
+    targets = list(range(8 * 2048, nbits, 8 * 24000))
+    limits = targets[1:] + [nbits]
+    d = emu_decoder_factory()
+    got = d.find_blocks(haddr(body), body.size, targets, limits)
+    assert got == [oracle.find_next_dynamic_block(body.tobytes(), t, l) for t, l in zip(targets, limits)]
+
+
+def test_chunk_and_crc_parity(emu_decoder_factory):
+    raw, gz = W.config1(300_000, seed=5)
+    body = np.frombuffer(gz[10:], dtype=np.uint8).copy()
+    b1 = oracle.find_next_dynamic_block(body.tobytes(), 60_000 * 8, body.size * 8)
+    d = emu_decoder_factory()
+    want = oracle.decode_chunk(body.tobytes(), b1, 1 << 62)
+    got_bytes, mp, mo, end, fin = d.decode_chunk(haddr(body), body.size, b1, 1 << 62, max_bytes=1 << 20,
+                                                 max_markers=1 << 20)
+    assert got_bytes == want.bytes
+    assert np.array_equal(mp, want.marker_pos) and np.array_equal(mo, want.marker_off)
+    assert end == want.actual_end_bit and fin
+    data = np.random.default_rng(1).integers(0, 256, 300_001, dtype=np.uint8)
+    assert d.crc32(haddr(data), data.size) == zlib.crc32(data.tobytes())
