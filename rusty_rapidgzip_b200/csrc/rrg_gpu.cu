@@ -225,7 +225,7 @@ struct rrg_ctx {
 
     // device buffers (grow-only)
     DBuf items, results, order, queue, mbs, mbcount, cells, out, targets, limits, found, next_lut, chunks,
-        tiles, rerr, markers, crc_table, pieces, piece_crc, mpiece, exp_crc, exp_isize, got_crc, got_len,
+        tiles, rerr, markers, win, crc_table, pieces, piece_crc, mpiece, exp_crc, exp_isize, got_crc, got_len,
         mstatus, comp;
     // pinned host staging
     uint8_t* h_stage[2] = {nullptr, nullptr};
@@ -515,6 +515,49 @@ int ensure_out(rrg_ctx* c, OutTarget& t, uint64_t need, uint64_t keep, rrg_error
     return 0;
 }
 
+// ------------------------------------------------------------ resolve
+// Windows (init + chase), then cells -> bytes. Returns 0 or an error code.
+int run_resolve(rrg_ctx* c, const std::vector<ResolveChunk>& rchunks, const std::vector<uint64_t>& tile_start,
+                uint8_t* d_dst, rrg_error* err) {
+    const uint32_t nc = (uint32_t)rchunks.size();
+    if (!nc) return 0;
+    CK(dgrow(c->chunks, nc * sizeof(ResolveChunk)));
+    CK(dgrow(c->tiles, (nc + 1) * 8));
+    CK(dgrow(c->rerr, 16));
+    CK(dgrow(c->markers, 8));
+    CK(dgrow(c->win, (size_t)nc * WINDOW * 4));
+    CK(cudaMemcpyAsync(c->chunks.p, rchunks.data(), nc * sizeof(ResolveChunk), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->tiles.p, tile_start.data(), (nc + 1) * 8, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(c->rerr.p, 0, 16, c->stream));
+    CK(cudaMemsetAsync(c->markers.p, 0, 8, c->stream));
+    ResolveArgs R{(const uint16_t*)c->cells.p, (const ResolveChunk*)c->chunks.p, (const uint64_t*)c->tiles.p, nc,
+                  tile_start.back(), d_dst, (uint32_t*)c->win.p, (uint32_t*)c->rerr.p,
+                  (unsigned long long*)c->markers.p};
+    const uint64_t wcells = (uint64_t)nc * WINDOW;
+    const uint32_t wgrid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((wcells + 255) / 256, (uint64_t)c->n_sm * 32));
+    uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(tile_start.back(), (uint64_t)c->n_sm * 16));
+    KTimer kt(c->stream);
+    RRG_LAUNCH(k_win_init, wgrid, 256, 0, c->stream, R);
+    LAUNCHED(c);
+    RRG_LAUNCH(k_win_chase, wgrid, 256, 0, c->stream, R);
+    LAUNCHED(c);
+    RRG_LAUNCH(k_resolve, grid, RES_THREADS, 0, c->stream, R);
+    kt.stop();
+    LAUNCHED(c);
+    uint32_t e4[4];
+    unsigned long long nmk = 0;
+    CK(cudaMemcpyAsync(e4, c->rerr.p, 16, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(&nmk, c->markers.p, 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->st.resolve_ms += kt.ms();
+    c->st.markers += nmk;
+    if (e4[0]) {
+        set_err(err, RRG_ERR_DEFLATE_INVALID, "%s", msg_text(MSG_MARKER_WINDOW));
+        return RRG_ERR_DEFLATE_INVALID;
+    }
+    return 0;
+}
+
 // ------------------------------------------------------------ member route
 struct Decoded {
     uint64_t total = 0;  // bytes written at d_dst
@@ -713,38 +756,8 @@ int member_route(rrg_ctx* c, const uint8_t* d_file, uint64_t len, uint64_t body_
     if (rc) return rc;
     uint8_t* d_dst = tgt.p;
     // ---- resolve markers + compact
-    if (!rchunks.empty()) {
-        double t0 = now_ms();
-        const uint32_t nc = (uint32_t)rchunks.size();
-        CK(dgrow(c->chunks, nc * sizeof(ResolveChunk)));
-        CK(dgrow(c->tiles, (nc + 1) * 8));
-        CK(dgrow(c->rerr, 16));
-        CK(dgrow(c->markers, 8));
-        CK(cudaMemcpyAsync(c->chunks.p, rchunks.data(), nc * sizeof(ResolveChunk), cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(c->tiles.p, tile_start.data(), (nc + 1) * 8, cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemsetAsync(c->rerr.p, 0, 16, c->stream));
-        CK(cudaMemsetAsync(c->markers.p, 0, 8, c->stream));
-        // chunk table holds global positions relative to d_dst
-        ResolveArgs R{(const uint16_t*)c->cells.p, (const ResolveChunk*)c->chunks.p, (const uint64_t*)c->tiles.p, nc,
-                      tile_start.back(), d_dst, (uint32_t*)c->rerr.p, (unsigned long long*)c->markers.p};
-        uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(tile_start.back(), (uint64_t)c->n_sm * 16));
-        KTimer kt(c->stream);
-        RRG_LAUNCH(k_resolve, grid, RES_THREADS, 0, c->stream, R);
-        kt.stop();
-        LAUNCHED(c);
-        uint32_t e4[4];
-        unsigned long long nmk = 0;
-        CK(cudaMemcpyAsync(e4, c->rerr.p, 16, cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaMemcpyAsync(&nmk, c->markers.p, 8, cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
-        c->st.resolve_ms += kt.ms();
-        (void)t0;
-        c->st.markers += nmk;
-        if (e4[0]) {
-            set_err(err, RRG_ERR_DEFLATE_INVALID, "%s", msg_text(MSG_MARKER_WINDOW));
-            return RRG_ERR_DEFLATE_INVALID;
-        }
-    }
+    rc = run_resolve(c, rchunks, tile_start, d_dst, err);
+    if (rc) return rc;
     // spans carry positions relative to d_dst
     return check_members(c, d_dst, spans, member_base, err);
 }
@@ -1029,7 +1042,7 @@ rrg_ctx* rrg_gpu_create(const rrg_config* cfg, rrg_error* err) {
 
 void rrg_gpu_destroy(rrg_ctx* c) {
     if (!c) return;
-    DBuf* bufs[] = {&c->items,  &c->results, &c->order,     &c->queue,    &c->mbs,      &c->mbcount,   &c->cells,
+    DBuf* bufs[] = {&c->win, &c->items,  &c->results, &c->order,     &c->queue,    &c->mbs,      &c->mbcount,   &c->cells,
                     &c->out,    &c->targets, &c->limits,    &c->found,    &c->next_lut, &c->chunks,    &c->tiles,
                     &c->rerr,   &c->markers, &c->crc_table, &c->pieces,   &c->piece_crc, &c->mpiece,   &c->exp_crc,
                     &c->exp_isize, &c->got_crc, &c->got_len, &c->mstatus, &c->comp};
@@ -1294,26 +1307,8 @@ int rrg_gpu_resolve_markers(rrg_ctx* c, uint8_t* d_bytes, size_t n_bytes, const 
     }
     ch.push_back(ResolveChunk{tl, base, nb, 0});
     ts.push_back(ts.back() + (nb + RES_TILE - 1) / RES_TILE);
-    const uint32_t nc = (uint32_t)ch.size();
-    CK(dgrow(c->chunks, nc * sizeof(ResolveChunk)));
-    CK(dgrow(c->tiles, (nc + 1) * 8));
-    CK(dgrow(c->rerr, 16));
-    CK(dgrow(c->markers, 8));
-    CK(cudaMemcpy(c->chunks.p, ch.data(), nc * sizeof(ResolveChunk), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c->tiles.p, ts.data(), (nc + 1) * 8, cudaMemcpyHostToDevice));
-    CK(cudaMemset(c->rerr.p, 0, 16));
-    CK(cudaMemset(c->markers.p, 0, 8));
-    ResolveArgs R{(const uint16_t*)c->cells.p, (const ResolveChunk*)c->chunks.p, (const uint64_t*)c->tiles.p, nc,
-                  ts.back(), (uint8_t*)c->out.p, (uint32_t*)c->rerr.p, (unsigned long long*)c->markers.p};
-    RRG_LAUNCH(k_resolve, (uint32_t)std::max<uint64_t>(1, ts.back()), RES_THREADS, 0, c->stream, R);
-    LAUNCHED(c);
-    CK(cudaStreamSynchronize(c->stream));
-    uint32_t e4[4];
-    CK(cudaMemcpy(e4, c->rerr.p, 16, cudaMemcpyDeviceToHost));
-    if (e4[0]) {
-        set_err(err, RRG_ERR_DEFLATE_INVALID, "%s", msg_text(MSG_MARKER_WINDOW));
-        return RRG_ERR_DEFLATE_INVALID;
-    }
+    int rc = run_resolve(c, ch, ts, (uint8_t*)c->out.p, err);
+    if (rc) return rc;
     CK(cudaMemcpy(d_bytes, (const uint8_t*)c->out.p + tl, nb, cudaMemcpyDeviceToDevice));
     return 0;
 }

@@ -1045,11 +1045,23 @@ __global__ void k_find_blocks(FindArgs A) {
 }
 
 // ------------------------------------------------------- marker resolution
-// One CTA per output tile of RES_TILE cells of one chunk. A marker cell names
-// the byte `off` positions before its chunk's first byte; that byte lives in
-// an earlier chunk (and may itself be a marker), so each marker follows the
-// chain to a literal cell. Results are staged in shared memory and written
-// with 16-byte stores.
+// A marker cell of chunk k with prefix offset `off` names the byte `off`
+// positions before chunk k's first byte, i.e. cell 32767-off of chunk k's
+// predecessor window WIN_k = output positions [start_k - 32768, start_k).
+// Resolution runs in three steps (the B200 form of the reference's serial
+// tail chain, pipeline.rs:1045-1078, followed by resolve_markers,
+// speculative.rs:175-213):
+//   k_win_init   every window cell becomes a resolved byte, an INVALID mark
+//                (position before the chunk's member), or a pointer to the
+//                window cell its own marker names (always in an earlier window);
+//   k_win_chase  every pointer follows its chain to a byte and is overwritten
+//                in place, so later chases stop early (pointers only lead to
+//                earlier windows, so every chain ends);
+//   k_resolve    every cell of every chunk becomes its byte with at most one
+//                gather from its chunk's window; cells are compacted into the
+//                contiguous output with 16-byte stores.
+constexpr uint32_t WIN_BYTE = 0x80000000u;     // resolved: low 8 bits = byte
+constexpr uint32_t WIN_INVALID = 0xC0000000u;  // resolved to an error
 constexpr int RES_THREADS = 256;
 constexpr int RES_PER_THREAD = 16;
 constexpr int RES_TILE = RES_THREADS * RES_PER_THREAD;
@@ -1061,27 +1073,58 @@ struct ResolveArgs {
     uint32_t n_chunks;
     uint64_t n_tiles;
     uint8_t* out;
+    uint32_t* win;           // n_chunks * WINDOW entries
     uint32_t* err;           // [0] flag, [1] chunk, [2] cell lo, [3] cell hi
     unsigned long long* markers;  // count of marker cells resolved
 };
 
-__device__ __forceinline__ bool chase(const ResolveArgs& A, uint32_t k, uint32_t v, uint32_t* byte) {
-    for (;;) {
+__global__ void __launch_bounds__(256) k_win_init(ResolveArgs A) {
+    const uint64_t total = (uint64_t)A.n_chunks * WINDOW;
+    for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < total;
+         c += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t k = (uint32_t)(c / WINDOW), i = (uint32_t)(c % WINDOW);
         const ResolveChunk ck = A.chunks[k];
-        uint64_t off = v & 0x7fffu;
-        if (ck.out_start < off + 1 || ck.out_start - 1 - off < ck.member_start) return false;
-        uint64_t target = ck.out_start - 1 - off;
-        uint32_t j = k;
-        do {
-            j--;
-        } while (A.chunks[j].out_start > target || A.chunks[j].out_start + A.chunks[j].n_cells <= target);
-        const ResolveChunk cj = A.chunks[j];
-        v = A.cells[cj.slot_off + (target - cj.out_start)];
-        if (!(v & MARKER16)) {
-            *byte = v & 0xffu;
-            return true;
+        uint32_t w;
+        if (ck.out_start + i < (uint64_t)WINDOW || ck.out_start + i - WINDOW < ck.member_start) {
+            w = WIN_INVALID;
+        } else {
+            const uint64_t g = ck.out_start + i - WINDOW;  // < out_start of chunk k
+            uint32_t j = k;
+            do {
+                j--;
+            } while (j > 0 && A.chunks[j].out_start > g);
+            const ResolveChunk cj = A.chunks[j];
+            if (j >= k || g < cj.out_start || g - cj.out_start >= cj.n_cells) {
+                w = WIN_INVALID;  // unreachable for a consistent chunk table
+            } else {
+                const uint32_t v = A.cells[cj.slot_off + (g - cj.out_start)];
+                w = (v & MARKER16) ? (j * WINDOW + (WINDOW - 1 - (v & 0x7fffu))) : (WIN_BYTE | v);
+            }
         }
-        k = j;
+        A.win[c] = w;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_win_chase(ResolveArgs A) {
+    const uint64_t total = (uint64_t)A.n_chunks * WINDOW;
+    volatile uint32_t* win = A.win;
+    for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < total;
+         c += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t w = win[c];
+        if (w & WIN_BYTE) continue;
+        uint32_t t = w;
+        uint64_t prev_win = c / WINDOW;
+        for (;;) {  // every hop must reach a strictly earlier window: at most n_chunks steps
+            if ((uint64_t)(t / WINDOW) >= prev_win) {
+                w = WIN_INVALID;
+                break;
+            }
+            prev_win = t / WINDOW;
+            w = win[t];
+            if (w & WIN_BYTE) break;
+            t = w;
+        }
+        win[c] = w;
     }
 }
 
@@ -1103,6 +1146,7 @@ __global__ void __launch_bounds__(RES_THREADS) k_resolve(ResolveArgs A) {
         __syncthreads();
         const uint32_t k = s_chunk;
         const ResolveChunk ck = A.chunks[k];
+        const uint32_t* win = A.win + (uint64_t)k * WINDOW;
         const uint64_t c0 = (t - A.tile_start[k]) * (uint64_t)RES_TILE;
         const uint64_t cn = ck.n_cells - c0 < (uint64_t)RES_TILE ? ck.n_cells - c0 : (uint64_t)RES_TILE;
         const uint32_t mine = threadIdx.x * RES_PER_THREAD;
@@ -1121,13 +1165,14 @@ __global__ void __launch_bounds__(RES_THREADS) k_resolve(ResolveArgs A) {
             } else {
                 for (int i = 0; i < RES_PER_THREAD; i++) cell[i] = (mine + i < cn) ? p[i] : 0u;
             }
+            // independent gathers: all issued before any is consumed
+            uint32_t got[RES_PER_THREAD];
+            for (int i = 0; i < RES_PER_THREAD; i++)
+                got[i] = (cell[i] & MARKER16) ? win[WINDOW - 1 - (cell[i] & 0x7fffu)] : (WIN_BYTE | cell[i]);
             for (int i = 0; i < RES_PER_THREAD; i++) {
-                uint32_t v = cell[i];
-                if (v & MARKER16) {
-                    nmk++;
-                    if (!chase(A, k, v, &v)) bad = 1;
-                }
-                stage[mine + i] = (uint8_t)v;
+                nmk += (cell[i] & MARKER16) ? 1u : 0u;
+                if (got[i] == WIN_INVALID || !(got[i] & WIN_BYTE)) bad = 1;
+                stage[mine + i] = (uint8_t)got[i];
             }
         }
         if (bad) atomicOr(&s_bad, 1u);
@@ -1147,12 +1192,10 @@ __global__ void __launch_bounds__(RES_THREADS) k_resolve(ResolveArgs A) {
         for (uint32_t i = threadIdx.x; i < body; i += blockDim.x) {
             const uint8_t* sp = stage + h + i * 16;
             uint4 v;
-            uint8_t tmp[16];
-            for (int q = 0; q < 16; q++) tmp[q] = sp[q];
-            v.x = (uint32_t)tmp[0] | ((uint32_t)tmp[1] << 8) | ((uint32_t)tmp[2] << 16) | ((uint32_t)tmp[3] << 24);
-            v.y = (uint32_t)tmp[4] | ((uint32_t)tmp[5] << 8) | ((uint32_t)tmp[6] << 16) | ((uint32_t)tmp[7] << 24);
-            v.z = (uint32_t)tmp[8] | ((uint32_t)tmp[9] << 8) | ((uint32_t)tmp[10] << 16) | ((uint32_t)tmp[11] << 24);
-            v.w = (uint32_t)tmp[12] | ((uint32_t)tmp[13] << 8) | ((uint32_t)tmp[14] << 16) | ((uint32_t)tmp[15] << 24);
+            v.x = (uint32_t)sp[0] | ((uint32_t)sp[1] << 8) | ((uint32_t)sp[2] << 16) | ((uint32_t)sp[3] << 24);
+            v.y = (uint32_t)sp[4] | ((uint32_t)sp[5] << 8) | ((uint32_t)sp[6] << 16) | ((uint32_t)sp[7] << 24);
+            v.z = (uint32_t)sp[8] | ((uint32_t)sp[9] << 8) | ((uint32_t)sp[10] << 16) | ((uint32_t)sp[11] << 24);
+            v.w = (uint32_t)sp[12] | ((uint32_t)sp[13] << 8) | ((uint32_t)sp[14] << 16) | ((uint32_t)sp[15] << 24);
             *reinterpret_cast<uint4*>(dst + h + i * 16) = v;
         }
         for (uint32_t i = h + body * 16 + threadIdx.x; i < cn; i += blockDim.x) dst[i] = stage[i];
