@@ -593,7 +593,7 @@ int member_route(rrg_ctx* c, const uint8_t* d_file, uint64_t len, uint64_t body_
         CK(cudaMemsetAsync(c->queue.p, 0, 16, c->stream));
         FindArgs F{body, blen, (const uint64_t*)c->targets.p, (const uint64_t*)c->limits.p, (uint64_t*)c->found.p, n,
                    (uint32_t*)c->queue.p, (const uint8_t*)c->next_lut.p, c->finder_tile};
-        const uint32_t W = 8;
+        const uint32_t W = 4;
         uint32_t grid = persistent_blocks(c, 4, n, W);
         KTimer kt(c->stream);
         RRG_LAUNCH(k_find_blocks, grid, W * 32, W * sizeof(FindSmem), c->stream, F);
@@ -1032,6 +1032,7 @@ rrg_ctx* rrg_gpu_create(const rrg_config* cfg, rrg_error* err) {
     int smem_optin = 0;
     cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
     size_t want = (size_t)c->inflate_warps * sizeof(WarpSmem);
+    cudaFuncSetAttribute(k_find_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(4 * sizeof(FindSmem)));
     if (smem_optin > 0 && want > 48 * 1024) {
         cudaFuncSetAttribute(k_inflate<uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)want);
         cudaFuncSetAttribute(k_inflate<uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)want);
@@ -1231,7 +1232,7 @@ int rrg_gpu_find_blocks(rrg_ctx* c, const uint8_t* d_body, size_t body_len, cons
     CK(cudaMemsetAsync(c->queue.p, 0, 16, c->stream));
     FindArgs F{d_body, body_len, (const uint64_t*)c->targets.p, (const uint64_t*)c->limits.p, (uint64_t*)c->found.p,
                (uint32_t)n, (uint32_t*)c->queue.p, (const uint8_t*)c->next_lut.p, c->finder_tile};
-    const uint32_t W = 8;
+    const uint32_t W = 4;
     RRG_LAUNCH(k_find_blocks, persistent_blocks(c, 4, n, W), W * 32, W * sizeof(FindSmem), c->stream, F);
     LAUNCHED(c);
     CK(cudaMemcpyAsync(found, c->found.p, n * 8, cudaMemcpyDeviceToHost, c->stream));

@@ -169,10 +169,11 @@ struct Table {
 };
 
 // Canonical code construction (RFC 1951 §3.2.2), warp-parallel. Rejects an
-// oversubscribed tree with >= 2 symbols (huffman.rs:238-249, non-strict).
-// Returns MSG_NONE or MSG_OVERSUB (uniform across the warp).
+// oversubscribed tree with >= 2 symbols (huffman.rs:238-249); with `strict`
+// also an incomplete one (the block finder's strict build). Returns MSG_NONE
+// or MSG_OVERSUB (uniform across the warp).
 __device__ int warp_build(const uint8_t* len, int n, const Table& T, int lut_bits, int kind, uint16_t* run,
-                          int lane) {
+                          int lane, bool strict = false) {
     const uint32_t lut_size = 1u << lut_bits;
     for (uint32_t i = lane; i < lut_size; i += 32) T.lut[i] = 0;
     uint32_t cnt = 0;
@@ -180,7 +181,7 @@ __device__ int warp_build(const uint8_t* len, int n, const Table& T, int lut_bit
         for (int s = 0; s < n; s++) cnt += (len[s] == (uint32_t)lane);
     uint32_t kraft = (lane >= 1 && lane <= 15) ? (cnt << (15 - lane)) : 0u;
     uint32_t ksum = warp_sum(kraft), nsym = warp_sum(cnt);
-    if (nsym >= 2 && ksum > 32768u) {
+    if (nsym >= 2 && (ksum > 32768u || (strict && ksum != 32768u))) {
         __syncwarp();
         return MSG_OVERSUB;
     }
@@ -815,12 +816,22 @@ __global__ void k_inflate(InflateArgs A) {
 }
 
 // ------------------------------------------------------- block finder
-// One warp per target. The 13-bit prefilter of block_finder.rs:60-101 (BFINAL=0,
-// BTYPE=2, HLIT<=29, HDIST<=29) gives each offset its skip distance; the warp
-// evaluates a tile of offsets in parallel (skip distance, and the strict
-// verification for every prefilter candidate), then lane 0 walks the skip
-// chain through the tile exactly as find_next_dynamic_block does.
+// One warp per target; the search runs over tiles of 1024 bit offsets that
+// start at the current skip-chain position. For its 32 offsets each lane
+// computes, from five register-resident input words:
+//   * the 13-bit prefilter skip of block_finder.rs:60-101 (BFINAL=0, BTYPE=2,
+//     HLIT<=29, HDIST<=29; 0 = candidate), and
+//   * for candidates, the strict Kraft test of the HCLEN precode lengths.
+// The rare offsets that pass both get the full strict verification of
+// block_finder.rs:175-301 (precode, code lengths, complete litlen/dist trees,
+// EOB length, 64 trial symbols) done by the whole warp with shared-memory
+// tables. The reference walks the skip chain one offset at a time; here each
+// lane turns its 32-offset segment into a transfer table (for every entry
+// offset 0..12: exit offset into the next segment, or the first verified
+// offset met), and lane 0 composes the 32 tables. The result is exactly the
+// offset find_next_dynamic_block returns.
 constexpr int FIND_TILE = 1024;
+constexpr uint32_t STEP_END = 14;  // offset + 13 > limit: the scan stops
 
 struct FindArgs {
     const uint8_t* body;
@@ -831,145 +842,181 @@ struct FindArgs {
     uint32_t n;
     uint32_t* queue;
     const uint8_t* next_lut;  // 8192 entries
-    uint32_t tile;            // offsets evaluated per tile (<= FIND_TILE, multiple of 32)
+    uint32_t tile;            // unused (tile width is fixed at 1024 offsets)
 };
 
 struct FindSmem {
-    uint8_t step[FIND_TILE];
-    uint8_t ok[FIND_TILE];
+    uint32_t lit_lut[LUT_SIZE];
+    uint32_t dist_lut[LUT_SIZE];
+    uint32_t pre_lut[1 << PRE_BITS];
+    uint16_t lit_sorted[288];
+    uint16_t dist_sorted[32];
+    uint16_t pre_sorted[32];
+    uint16_t lit_first[16], lit_count[16], lit_off[16];
+    uint16_t dist_first[16], dist_count[16], dist_off[16];
+    uint16_t pre_first[16], pre_count[16], pre_off[16];
+    uint16_t run[16];
+    uint8_t lengths[320];
+    uint8_t pre_len[20];
+    uint8_t trans[32][16];
 };
 
-// Per-thread bit cursor for candidate verification with the reference's exact
-// availability rules (bitreader.rs refill/peek: a read of n bits fails unless n
-// bits remain; a Huffman probe needs 10 bits, a long code 15).
-struct VCur {
-    const Src* s;
-    uint64_t pos;   // bit position relative to s->lo
-    uint64_t total; // bits available
-};
-__device__ __forceinline__ uint32_t vpeek(const VCur& c, uint32_t n) {  // n <= 25, caller checks availability
-    uint64_t a = c.pos + c.s->lo * 8;
-    uint64_t w = a >> 5;
-    uint64_t v = (uint64_t)src_word(*c.s, w) | ((uint64_t)src_word(*c.s, w + 1) << 32);
+// 32 bits starting at bit b (b < 128) of the 5-word register window W.
+__device__ __forceinline__ uint32_t win_bits(const uint32_t W[5], uint32_t b) {
+    const uint32_t q = b >> 5, r = b & 31;
+    const uint32_t lo = q == 0 ? W[0] : q == 1 ? W[1] : q == 2 ? W[2] : W[3];
+    const uint32_t hi = q == 0 ? W[1] : q == 1 ? W[2] : q == 2 ? W[3] : W[4];
+    return r ? ((lo >> r) | (hi << (32 - r))) : lo;
+}
+
+// bits [pos, pos+n) of the source (n <= 25)
+__device__ __forceinline__ uint32_t peek_at(const Src& s, uint64_t pos, uint32_t n) {
+    const uint64_t a = pos + s.lo * 8;
+    const uint64_t w = a >> 5;
+    const uint64_t v = (uint64_t)src_word(s, w) | ((uint64_t)src_word(s, w + 1) << 32);
     return (uint32_t)(v >> (a & 31)) & ((1u << n) - 1u);
 }
-__device__ __forceinline__ bool vread(VCur& c, uint32_t n, uint32_t* v) {
-    if (c.pos + n > c.total) return false;
-    *v = n ? vpeek(c, n) : 0;
-    c.pos += n;
-    return true;
-}
-// canonical decode (count/symbol form); the symbol's code length is returned in *len.
-__device__ __forceinline__ int vdecode(VCur& c, const uint16_t* count, const uint16_t* sym) {
-    if (c.pos + 10 > c.total) return -1;
-    uint32_t bits = vpeek(c, c.pos + 15 <= c.total ? 15 : (uint32_t)(c.total - c.pos));
-    int code = 0, first = 0, index = 0;
-    for (int l = 1; l <= 15; l++) {
-        code |= (int)((bits >> (l - 1)) & 1u);
-        int cnt = count[l];
-        if (code - cnt < first) {
-            if (l > 10 && c.pos + 15 > c.total) return -1;
-            c.pos += (uint64_t)l;
-            return sym[index + (code - first)];
-        }
-        index += cnt;
-        first += cnt;
-        first <<= 1;
-        code <<= 1;
-    }
-    return -1;
-}
-// Strict canonical tables (huffman.rs strict build): counts + symbols sorted.
-__device__ bool vbuild(const uint8_t* len, int n, uint16_t* count, uint16_t* sym) {
-    for (int l = 0; l < 16; l++) count[l] = 0;
-    for (int s = 0; s < n; s++) count[len[s]]++;
-    count[0] = 0;
-    uint32_t total = 0, nsym = 0;
-    for (int l = 1; l < 16; l++) {
-        total += (uint32_t)count[l] << (15 - l);
-        nsym += count[l];
-    }
-    if (nsym >= 2 && total != 32768u) return false;  // oversubscribed or incomplete
-    uint16_t offs[16];
-    offs[1] = 0;
-    for (int l = 1; l < 15; l++) offs[l + 1] = offs[l] + count[l];
-    for (int s = 0; s < n; s++)
-        if (len[s]) sym[offs[len[s]]++] = (uint16_t)s;
-    return true;
-}
 
-// block_finder.rs:175-301 verify_candidate, read_dynamic_header_strict_into, trial_decode.
-__device__ __noinline__ bool verify_candidate(const Src& s, uint64_t total_bits, uint64_t pos) {
-    VCur c{&s, pos, total_bits};
-    uint32_t v;
-    if (!vread(c, 3, &v)) return false;
-    uint32_t hlit, hdist, hclen;
-    if (!vread(c, 5, &hlit) || !vread(c, 5, &hdist) || !vread(c, 4, &hclen)) return false;
-    hlit += 257;
-    hdist += 1;
-    hclen += 4;
-    if (hlit > 286 || hdist > 30) return false;
-    uint8_t cl[19];
-    for (int i = 0; i < 19; i++) cl[i] = 0;
-    for (uint32_t i = 0; i < hclen; i++) {
-        if (!vread(c, 3, &v)) return false;
-        cl[c_cl_order[i]] = (uint8_t)v;
+// Reference-exact reads on lane 0: a read of n bits needs n bits left.
+struct VC {
+    const Src* s;
+    uint64_t pos, total;
+    bool ok;
+    __device__ uint32_t read(uint32_t n) {
+        if (!ok || pos + n > total) {
+            ok = false;
+            return 0;
+        }
+        uint32_t v = n ? peek_at(*s, pos, n) : 0;
+        pos += n;
+        return v;
     }
-    // cheap strict precode check before any table work
-    {
-        uint32_t total = 0, nsym = 0;
-        for (int i = 0; i < 19; i++)
-            if (cl[i]) {
-                total += 1u << (7 - cl[i]);
-                nsym++;
+    // HuffmanDecoder::decode (huffman.rs:356-389): 10 bits must be available
+    // for the LUT probe, 15 for a long code.
+    __device__ uint32_t sym(const Table& T, int lut_bits) {
+        if (!ok || pos + 10 > total) {
+            ok = false;
+            return 0;
+        }
+        const uint32_t avail = total - pos >= 25 ? 25u : (uint32_t)(total - pos);
+        const uint32_t bits = peek_at(*s, pos, avail);
+        uint32_t e = T.lut[bits & ((1u << lut_bits) - 1u)];
+        if (!(e & 15)) {
+            if (pos + 15 > total) {
+                ok = false;
+                return 0;
             }
-        if (nsym >= 2 && total != 128u) return false;
-    }
-    uint16_t pcount[16], psym[19];
-    if (!vbuild(cl, 19, pcount, psym)) return false;
-    uint8_t lengths[320];
-    for (int i = 0; i < 320; i++) lengths[i] = 0;
-    uint32_t total = hlit + hdist, i = 0;
-    while (i < total) {
-        int sym = vdecode(c, pcount, psym);
-        if (sym < 0) return false;
-        if (sym <= 15) {
-            lengths[i++] = (uint8_t)sym;
-        } else if (sym == 16) {
-            if (i == 0 || !vread(c, 2, &v)) return false;
-            uint32_t r = v + 3;
-            if (i + r > total) return false;
-            for (uint32_t j = 0; j < r; j++) lengths[i + j] = lengths[i - 1];
-            i += r;
-        } else if (sym == 17) {
-            if (!vread(c, 3, &v) || i + v + 3 > total) return false;
-            i += v + 3;
-        } else {
-            if (!vread(c, 7, &v) || i + v + 11 > total) return false;
-            i += v + 11;
+            e = long_decode(bits, T, lut_bits, TK_PRE);
+            if (!(e & 15)) {
+                ok = false;
+                return 0;
+            }
         }
+        pos += e & 15;
+        return e >> 16;
     }
-    if (lengths[256] == 0) return false;
-    uint16_t lcount[16], lsym[288], dcount[16], dsym[32];
-    if (!vbuild(lengths, (int)hlit, lcount, lsym)) return false;
-    if (!vbuild(lengths + hlit, (int)hdist, dcount, dsym)) return false;
-    for (int k = 0; k < 64; k++) {
-        int sym = vdecode(c, lcount, lsym);
-        if (sym < 0) return false;
-        if (sym < 256) continue;
-        if (sym == 256) return true;
-        if (sym > 285) return false;
-        uint32_t ex = c_len_extra[sym - 257];
-        if (ex && !vread(c, ex, &v)) return false;
-        int ds = vdecode(c, dcount, dsym);
-        if (ds < 0 || ds >= 30) return false;
-        uint32_t dx = c_dist_extra[ds];
-        if (dx && !vread(c, dx, &v)) return false;
+};
+
+// Full strict verification of one candidate offset (warp-uniform call).
+__device__ __noinline__ bool verify_heavy(FindSmem& S, const Src& src, uint64_t total_bits, uint64_t pos, int lane) {
+    int ok = 1;
+    uint32_t hlit = 0, hdist = 0;
+    uint64_t cur = 0;
+    if (lane == 0) {
+        VC c{&src, pos, total_bits, true};
+        c.read(3);
+        hlit = c.read(5) + 257;
+        hdist = c.read(5) + 1;
+        uint32_t hclen = c.read(4) + 4;
+        for (int i = 0; i < 19; i++) S.pre_len[i] = 0;
+        if (hlit > 286 || hdist > 30) c.ok = false;
+        for (uint32_t i = 0; i < hclen && c.ok; i++) S.pre_len[c_cl_order[i]] = (uint8_t)c.read(3);
+        ok = c.ok ? 1 : 0;
+        cur = c.pos;
     }
-    return true;
+    ok = bcast32(ok);
+    hlit = (uint32_t)bcast32((int32_t)hlit);
+    hdist = (uint32_t)bcast32((int32_t)hdist);
+    cur = bcast64(cur);
+    if (!ok) return false;
+    __syncwarp();
+    const Table PT{S.pre_lut, S.pre_sorted, S.pre_first, S.pre_count, S.pre_off};
+    if (warp_build(S.pre_len, 19, PT, PRE_BITS, TK_PRE, S.run, lane, true)) return false;
+    for (int i = lane; i < 320; i += 32) S.lengths[i] = 0;
+    __syncwarp();
+    if (lane == 0) {
+        VC c{&src, cur, total_bits, true};
+        const uint32_t total = hlit + hdist;
+        uint32_t i = 0;
+        while (i < total && c.ok) {
+            uint32_t sym = c.sym(PT, PRE_BITS);
+            if (!c.ok) break;
+            if (sym <= 15) {
+                S.lengths[i++] = (uint8_t)sym;
+            } else if (sym == 16) {
+                if (i == 0) c.ok = false;
+                uint32_t r = c.read(2) + 3;
+                if (!c.ok || i + r > total) {
+                    c.ok = false;
+                    break;
+                }
+                for (uint32_t j = 0; j < r; j++) S.lengths[i + j] = S.lengths[i - 1];
+                i += r;
+            } else if (sym == 17) {
+                uint32_t r = c.read(3) + 3;
+                if (!c.ok || i + r > total) c.ok = false;
+                i += r;
+            } else if (sym == 18) {
+                uint32_t r = c.read(7) + 11;
+                if (!c.ok || i + r > total) c.ok = false;
+                i += r;
+            } else {
+                c.ok = false;
+            }
+        }
+        if (c.ok && S.lengths[256] == 0) c.ok = false;
+        ok = c.ok ? 1 : 0;
+        cur = c.pos;
+    }
+    ok = bcast32(ok);
+    cur = bcast64(cur);
+    if (!ok) return false;
+    __syncwarp();
+    const Table LT{S.lit_lut, S.lit_sorted, S.lit_first, S.lit_count, S.lit_off};
+    const Table DT{S.dist_lut, S.dist_sorted, S.dist_first, S.dist_count, S.dist_off};
+    if (warp_build(S.lengths, (int)hlit, LT, LUT_BITS, TK_PRE, S.run, lane, true)) return false;
+    if (warp_build(S.lengths + hlit, (int)hdist, DT, LUT_BITS, TK_PRE, S.run, lane, true)) return false;
+    if (lane == 0) {
+        VC c{&src, cur, total_bits, true};
+        bool done = false;
+        for (int k = 0; k < 64 && c.ok && !done; k++) {
+            uint32_t sym = c.sym(LT, LUT_BITS);
+            if (!c.ok) break;
+            if (sym < 256) continue;
+            if (sym == 256) {
+                done = true;
+                break;
+            }
+            if (sym > 285) {
+                c.ok = false;
+                break;
+            }
+            c.read(c_len_extra[sym - 257]);
+            uint32_t ds = c.sym(DT, LUT_BITS);
+            if (!c.ok || ds >= 30) {
+                c.ok = false;
+                break;
+            }
+            c.read(c_dist_extra[ds]);
+        }
+        ok = c.ok ? 1 : 0;
+    }
+    ok = bcast32(ok);
+    __syncwarp();
+    return ok != 0;
 }
 
-__global__ void k_find_blocks(FindArgs A) {
+__global__ void __launch_bounds__(128) k_find_blocks(FindArgs A) {
     RRG_DYN_SMEM(smem_raw);
     __shared__ uint8_t lut[8192];
     for (int i = threadIdx.x; i < 8192; i += blockDim.x) lut[i] = A.next_lut[i];
@@ -978,55 +1025,106 @@ __global__ void k_find_blocks(FindArgs A) {
     FindSmem& S = reinterpret_cast<FindSmem*>(smem_raw)[warp];
     const Src src = make_src(A.body, A.body_len);
     const uint64_t total_bits = A.body_len * 8;
-    const uint32_t tile = A.tile;
     for (;;) {
         uint32_t idx = 0;
         if (lane == 0) idx = atomicAdd(A.queue, 1u);
         idx = (uint32_t)bcast32((int32_t)idx);
         if (idx >= A.n) break;
-        uint64_t from = A.targets[idx];
-        uint64_t limit = A.limits[idx] < total_bits ? A.limits[idx] : total_bits;
+        const uint64_t from = A.targets[idx];
+        const uint64_t limit = A.limits[idx] < total_bits ? A.limits[idx] : total_bits;
         uint64_t result = ~0ull;
         uint64_t pos = from;
-        bool done = from >= limit;
+        bool done = from >= limit || from + 13 > limit;
         while (!done) {
             const uint64_t tb = pos;
-            for (uint32_t k = lane; k < tile; k += 32) {
-                uint64_t p = tb + k;
-                uint8_t stp = 255, ok = 0;
-                if (p + 13 <= limit) {
-                    uint64_t a = p + src.lo * 8;
-                    uint64_t w = a >> 5;
-                    uint64_t v = (uint64_t)src_word(src, w) | ((uint64_t)src_word(src, w + 1) << 32);
-                    uint32_t win = (uint32_t)(v >> (a & 31)) & 0x1fffu;
-                    stp = lut[win];
-                    if (stp == 0) ok = verify_candidate(src, total_bits, p) ? 1 : 0;
+            // ---- per-offset prefilter + precode test for this lane's 32 offsets
+            const uint64_t seg = tb + 32ull * lane;
+            const uint64_t a = seg + src.lo * 8;
+            const uint64_t w0 = a >> 5;
+            const uint32_t sh = (uint32_t)(a & 31);
+            uint32_t W[5];
+            for (int q = 0; q < 5; q++) W[q] = src_word(src, w0 + q);
+            uint64_t stepA = 0, stepB = 0;
+            uint32_t pre = 0;
+            for (uint32_t i = 0; i < 32; i++) {
+                uint32_t st;
+                if (seg + i + 13 > limit) {
+                    st = STEP_END;
+                } else {
+                    const uint32_t b = sh + i;
+                    st = lut[win_bits(W, b) & 0x1fffu];
+                    if (st == 0) {
+                        const uint32_t hclen = (win_bits(W, b + 13) & 15u) + 4;
+                        const uint32_t y = win_bits(W, b + 17), z = win_bits(W, b + 47);
+                        uint32_t kraft = 0, nsym = 0;
+#pragma unroll
+                        for (uint32_t j = 0; j < 19; j++) {
+                            const uint32_t l = j < 10 ? (y >> (3 * j)) & 7u : (z >> (3 * (j - 10))) & 7u;
+                            if (j < hclen && l) {
+                                kraft += 128u >> l;
+                                nsym++;
+                            }
+                        }
+                        if (nsym < 2 || kraft == 128u) pre |= 1u << i;
+                    }
                 }
-                S.step[k] = stp;
-                S.ok[k] = ok;
+                if (i < 16) stepA |= (uint64_t)st << (4 * i);
+                else stepB |= (uint64_t)st << (4 * (i - 16));
+            }
+            // ---- full verification of the offsets that passed the precode test
+            uint32_t okm = 0;
+            unsigned todo = __ballot_sync(FULLMASK, pre != 0);
+            while (todo) {
+                const int L = __ffs(todo) - 1;
+                uint32_t m = __shfl_sync(FULLMASK, pre, L);
+                while (m) {
+                    const int i = __ffs(m) - 1;
+                    m &= m - 1;
+                    const bool ok = verify_heavy(S, src, total_bits, tb + 32ull * L + i, lane);
+                    if (ok && lane == L) okm |= 1u << i;
+                }
+                todo &= todo - 1;
+            }
+            // ---- transfer table of this lane's segment for entry offsets 0..12
+            for (uint32_t e = 0; e < 13; e++) {
+                uint32_t p = e, res = 0xFFu;
+                while (p < 32) {
+                    const uint32_t st = (uint32_t)((p < 16 ? stepA >> (4 * p) : stepB >> (4 * (p - 16))) & 15u);
+                    if (st == STEP_END) {
+                        res = 0xFEu;
+                        break;
+                    }
+                    if (st == 0) {
+                        if ((okm >> p) & 1u) {
+                            res = 0x80u | p;
+                            break;
+                        }
+                        p += 1;
+                    } else {
+                        p += st;
+                    }
+                }
+                S.trans[lane][e] = (uint8_t)(res == 0xFFu ? p - 32 : res);
             }
             __syncwarp();
             int d = 0;
-            uint64_t np = pos, res = ~0ull;
+            uint64_t np = 0, res = ~0ull;
             if (lane == 0) {
-                while (np < tb + tile) {
-                    uint32_t k = (uint32_t)(np - tb);
-                    uint8_t stp = S.step[k];
-                    if (stp == 255) {
+                uint32_t e = 0;
+                for (int sgi = 0; sgi < 32; sgi++) {
+                    const uint32_t t = S.trans[sgi][e];
+                    if (t == 0xFEu) {
                         d = 1;
                         break;
                     }
-                    if (stp == 0) {
-                        if (S.ok[k]) {
-                            res = np;
-                            d = 1;
-                            break;
-                        }
-                        np += 1;
-                    } else {
-                        np += stp;
+                    if (t & 0x80u) {
+                        res = tb + 32ull * sgi + (t & 0x7fu);
+                        d = 1;
+                        break;
                     }
+                    e = t;
                 }
+                np = tb + FIND_TILE + e;
             }
             d = bcast32(d);
             np = bcast64(np);
@@ -1132,6 +1230,8 @@ __global__ void __launch_bounds__(RES_THREADS) k_resolve(ResolveArgs A) {
     __shared__ __align__(16) uint8_t stage[RES_TILE];
     __shared__ uint32_t s_chunk;
     __shared__ uint32_t s_bad;
+    __shared__ uint32_t s_mk;  // marker cells seen by this block (one global add at the end)
+    if (threadIdx.x == 0) s_mk = 0;
     for (uint64_t t = blockIdx.x; t < A.n_tiles; t += gridDim.x) {
         if (threadIdx.x == 0) {
             uint32_t lo = 0, hi = A.n_chunks - 1;
@@ -1176,7 +1276,8 @@ __global__ void __launch_bounds__(RES_THREADS) k_resolve(ResolveArgs A) {
             }
         }
         if (bad) atomicOr(&s_bad, 1u);
-        if (nmk) atomicAdd(A.markers, (unsigned long long)nmk);
+        nmk = warp_sum(nmk);
+        if ((threadIdx.x & 31) == 0 && nmk) atomicAdd(&s_mk, nmk);
         __syncthreads();
         if (s_bad && threadIdx.x == 0 && atomicCAS(A.err, 0u, 1u) == 0u) {
             A.err[1] = k;
@@ -1201,6 +1302,7 @@ __global__ void __launch_bounds__(RES_THREADS) k_resolve(ResolveArgs A) {
         for (uint32_t i = h + body * 16 + threadIdx.x; i < cn; i += blockDim.x) dst[i] = stage[i];
         __syncthreads();
     }
+    if (threadIdx.x == 0 && s_mk) atomicAdd(A.markers, (unsigned long long)s_mk);
 }
 
 // ------------------------------------------------------- CRC-32

@@ -84,3 +84,24 @@ def test_chunk_and_crc_parity(emu_decoder_factory):
     assert end == want.actual_end_bit and fin
     data = np.random.default_rng(1).integers(0, 256, 300_001, dtype=np.uint8)
     assert d.crc32(haddr(data), data.size) == zlib.crc32(data.tobytes())
+
+
+def test_finder_parity_adversarial(emu_decoder_factory):
+    """Random bytes scanned to the end (limit effects) and a gzip-of-gzip body,
+    where real inner headers sit inside the outer stored blocks."""
+    d = emu_decoder_factory()
+    g = np.random.default_rng(7).integers(0, 256, 24_000, dtype=np.uint8)
+    n = g.size * 8
+    targets = list(range(0, n, 9_973)) + [n - 40, n - 14, n - 13, n - 1]
+    limits = [n] * len(targets)
+    got = d.find_blocks(haddr(g), g.size, targets, limits)
+    assert got == [oracle.find_next_dynamic_block(g.tobytes(), t, l) for t, l in zip(targets, limits)]
+    inner = gzip_cli(np.random.default_rng(3).integers(32, 127, 200_000, dtype=np.uint8).tobytes(), 6)
+    outer = np.frombuffer(gzip_cli(inner, 6)[10:], dtype=np.uint8).copy()
+    n = outer.size * 8
+    targets = list(range(8 * 1000, n, 8 * 17_000))
+    limits = [min(t + 8 * 40_000, n) for t in targets]
+    got = d.find_blocks(haddr(outer), outer.size, targets, limits)
+    want = [oracle.find_next_dynamic_block(outer.tobytes(), t, l) for t, l in zip(targets, limits)]
+    assert got == want
+    assert any(w is not None for w in want)
