@@ -74,7 +74,7 @@ class _Config(C.Structure):
         ("gpu_chunk_bytes", C.c_uint64),
         ("finder_tile_bits", C.c_uint64),
         ("warps_per_stream", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("boundary_mode", C.c_int32),
         ("hbm_budget_bytes", C.c_uint64),
     ]
 
@@ -102,6 +102,7 @@ class Config:
     gpu_chunk_bytes: int = 0
     finder_tile_bits: int = 0
     warps_per_stream: int = 0
+    boundary_mode: int = 0
     hbm_budget_bytes: int = 0
 
     def _c(self) -> _Config:
@@ -113,6 +114,7 @@ class Config:
         c.gpu_chunk_bytes = self.gpu_chunk_bytes
         c.finder_tile_bits = self.finder_tile_bits
         c.warps_per_stream = self.warps_per_stream
+        c.boundary_mode = self.boundary_mode
         c.hbm_budget_bytes = self.hbm_budget_bytes
         return c
 

@@ -225,7 +225,7 @@ struct rrg_ctx {
 
     // device buffers (grow-only)
     DBuf items, results, order, queue, mbs, mbcount, cells, out, targets, limits, found, next_lut, chunks,
-        tiles, rerr, markers, win, crc_table, pieces, piece_crc, mpiece, exp_crc, exp_isize, got_crc, got_len,
+        tiles, rerr, markers, win, cand, ncand, vflag, lane_scratch, crc_table, pieces, piece_crc, mpiece, exp_crc, exp_isize, got_crc, got_len,
         mstatus, comp;
     // pinned host staging
     uint8_t* h_stage[2] = {nullptr, nullptr};
@@ -235,6 +235,8 @@ struct rrg_ctx {
 
     // tunables
     uint64_t gpu_chunk = 0;
+    bool lanes = true;         // lane-per-chunk inflate (false: warp-per-chunk)
+    bool scan_bounds = true;   // full-stream boundary scan (false: one finder search per target)
     uint32_t inflate_warps = 4;
     uint32_t finder_tile = 1024;
     double expand = 6.0;
@@ -368,10 +370,28 @@ int launch_inflate(rrg_ctx* c, const uint8_t* d_in, const std::vector<ChunkItem>
         A.mb_cap = mb_cap;
         const uint32_t W = c->inflate_warps;
         const size_t smem = W * sizeof(WarpSmem);
-        const uint32_t per_sm = std::max<uint32_t>(1, (uint32_t)((200 * 1024) / smem));
+        // as many resident blocks per SM as registers and shared memory allow
+        int occ = 0;
+        if (bytes_out) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_inflate<uint8_t>, W * 32, smem);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_inflate<uint16_t>, W * 32, smem);
+        const uint32_t per_sm = std::max<uint32_t>(1, (uint32_t)occ);
         const uint32_t grid = persistent_blocks(c, per_sm, n, W);
         KTimer kt(c->stream);
-        if (bytes_out) {
+        if (c->lanes) {
+            const size_t lsmem = LANE_THREADS * sizeof(LaneTab);
+            int locc = 0;
+            if (bytes_out) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&locc, k_inflate_lanes<uint8_t>, LANE_THREADS, lsmem);
+            else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&locc, k_inflate_lanes<uint16_t>, LANE_THREADS, lsmem);
+            const uint32_t lgrid = persistent_blocks(c, std::max(1, locc), n, LANE_THREADS);
+            CK(dgrow(c->lane_scratch, (size_t)lgrid * LANE_THREADS * sizeof(LaneScratch)));
+            if (bytes_out) {
+                RRG_LAUNCH(k_inflate_lanes<uint8_t>, lgrid, LANE_THREADS, lsmem, c->stream, A,
+                           (LaneScratch*)c->lane_scratch.p);
+            } else {
+                RRG_LAUNCH(k_inflate_lanes<uint16_t>, lgrid, LANE_THREADS, lsmem, c->stream, A,
+                           (LaneScratch*)c->lane_scratch.p);
+            }
+        } else if (bytes_out) {
             RRG_LAUNCH(k_inflate<uint8_t>, grid, W * 32, smem, c->stream, A);
         } else {
             RRG_LAUNCH(k_inflate<uint16_t>, grid, W * 32, smem, c->stream, A);
@@ -558,6 +578,66 @@ int run_resolve(rrg_ctx* c, const std::vector<ResolveChunk>& rchunks, const std:
     return 0;
 }
 
+// ------------------------------------------------------------ boundary scan
+// Every bit offset of the body tested on the device; returns the sorted
+// offsets that pass the block finder's full strict verification.
+int scan_boundaries(rrg_ctx* c, const uint8_t* body, uint64_t blen, std::vector<uint64_t>& verified, rrg_error* err) {
+    verified.clear();
+    if (blen < 4) return 0;
+    KTimer kt(c->stream);
+    uint32_t cap = (uint32_t)std::min<uint64_t>(blen / 32 + 65536, 1ull << 28);
+    uint32_t n = 0;
+    for (int attempt = 0; attempt < 2; attempt++) {
+        CK(dgrow(c->cand, (size_t)cap * 8));
+        CK(dgrow(c->ncand, 16));
+        CK(cudaMemsetAsync(c->ncand.p, 0, 16, c->stream));
+        ScanArgs S{body, blen, (uint64_t*)c->cand.p, (uint32_t*)c->ncand.p, cap};
+        const uint64_t tiles = (blen + 16 + SCAN_TILE - 1) / SCAN_TILE;
+        const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(tiles, (uint64_t)c->n_sm * 8));
+        RRG_LAUNCH(k_scan_candidates, grid, SCAN_THREADS, 0, c->stream, S);
+        LAUNCHED(c);
+        CK(cudaMemcpyAsync(&n, c->ncand.p, 4, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if (n <= cap) break;
+        cap = n + 65536;
+    }
+    if (n) {
+        CK(dgrow(c->vflag, n));
+        CK(dgrow(c->queue, 16));
+        VerifyArgs V{body, blen, (const uint64_t*)c->cand.p, n, (uint8_t*)c->vflag.p, (uint32_t*)c->queue.p};
+        const uint32_t grid = (uint32_t)std::max<uint32_t>(1, std::min<uint32_t>((n + 255) / 256, c->n_sm * 8));
+        RRG_LAUNCH(k_verify_light, grid, 256, 0, c->stream, V);
+        LAUNCHED(c);
+        std::vector<uint8_t> flags(n);
+        std::vector<uint64_t> cands(n);
+        CK(cudaMemcpyAsync(flags.data(), c->vflag.p, n, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(cands.data(), c->cand.p, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        std::vector<uint64_t> surv;
+        for (uint32_t i = 0; i < n; i++)
+            if (flags[i]) surv.push_back(cands[i]);
+        if (!surv.empty()) {
+            const uint32_t m = (uint32_t)surv.size();
+            CK(cudaMemcpyAsync(c->cand.p, surv.data(), (size_t)m * 8, cudaMemcpyHostToDevice, c->stream));
+            CK(cudaMemsetAsync(c->queue.p, 0, 16, c->stream));
+            VerifyArgs H{body, blen, (const uint64_t*)c->cand.p, m, (uint8_t*)c->vflag.p, (uint32_t*)c->queue.p};
+            const uint32_t W = 4;
+            RRG_LAUNCH(k_verify_heavy, persistent_blocks(c, 4, m, W), W * 32, W * sizeof(FindSmem), c->stream, H);
+            LAUNCHED(c);
+            std::vector<uint8_t> ok(m);
+            CK(cudaMemcpyAsync(ok.data(), c->vflag.p, m, cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaStreamSynchronize(c->stream));
+            for (uint32_t i = 0; i < m; i++)
+                if (ok[i]) verified.push_back(surv[i]);
+            std::sort(verified.begin(), verified.end());
+        }
+    }
+    kt.stop();
+    CK(cudaStreamSynchronize(c->stream));
+    c->st.finder_ms += kt.ms();
+    return 0;
+}
+
 // ------------------------------------------------------------ member route
 struct Decoded {
     uint64_t total = 0;  // bytes written at d_dst
@@ -575,9 +655,19 @@ int member_route(rrg_ctx* c, const uint8_t* d_file, uint64_t len, uint64_t body_
     const uint8_t* body = d_file + body_off;
     const uint64_t blen = len - body_off;
     const uint64_t total_bits = blen * 8;
-    const uint64_t G = std::max<uint64_t>(c->gpu_chunk ? c->gpu_chunk : (1ull << 17), 4096);
-    // ---- sub-chunk boundaries: first dynamic block at/after every G bytes
+    const uint64_t G = std::max<uint64_t>(c->gpu_chunk ? c->gpu_chunk : (c->lanes ? (1ull << 14) : (1ull << 17)), 4096);
+    std::vector<uint64_t> starts{0};
+    if (c->scan_bounds) {
+        // ---- sub-chunk boundaries: verified dynamic-block starts, at least G bytes apart
+        std::vector<uint64_t> verified;
+        int rc0 = scan_boundaries(c, body, blen, verified, err);
+        if (rc0) return rc0;
+        for (uint64_t v : verified)
+            if (v >= starts.back() + G * 8) starts.push_back(v);
+    }
+    // ---- or: first dynamic block at/after every G bytes (find_next_dynamic_block per target)
     std::vector<uint64_t> targets, limits, found;
+    if (!c->scan_bounds) {
     for (uint64_t t = G * 8; t < total_bits; t += G * 8) targets.push_back(t);
     for (size_t i = 0; i < targets.size(); i++) limits.push_back(i + 1 < targets.size() ? targets[i + 1] : total_bits);
     found.assign(targets.size(), ~0ull);
@@ -604,9 +694,9 @@ int member_route(rrg_ctx* c, const uint8_t* d_file, uint64_t len, uint64_t body_
         c->st.finder_ms += kt.ms();
         (void)t0;
     }
-    std::vector<uint64_t> starts{0};
     for (uint64_t f : found)
         if (f != ~0ull && f > starts.back()) starts.push_back(f);
+    }
     const size_t n = starts.size();
     // ---- slot arena: every chunk gets expand x its compressed span, plus room for re-decodes
     std::vector<ChunkItem> items(n);
@@ -1033,6 +1123,13 @@ rrg_ctx* rrg_gpu_create(const rrg_config* cfg, rrg_error* err) {
     cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
     size_t want = (size_t)c->inflate_warps * sizeof(WarpSmem);
     cudaFuncSetAttribute(k_find_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(4 * sizeof(FindSmem)));
+    cudaFuncSetAttribute(k_verify_heavy, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(4 * sizeof(FindSmem)));
+    cudaFuncSetAttribute(k_inflate_lanes<uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(LANE_THREADS * sizeof(LaneTab)));
+    cudaFuncSetAttribute(k_inflate_lanes<uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(LANE_THREADS * sizeof(LaneTab)));
+    if (c->cfg.warps_per_stream > 0) c->lanes = false;  // one chunk per warp
+    if (c->cfg.boundary_mode == 1) c->scan_bounds = false;
     if (smem_optin > 0 && want > 48 * 1024) {
         cudaFuncSetAttribute(k_inflate<uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)want);
         cudaFuncSetAttribute(k_inflate<uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)want);
@@ -1043,7 +1140,7 @@ rrg_ctx* rrg_gpu_create(const rrg_config* cfg, rrg_error* err) {
 
 void rrg_gpu_destroy(rrg_ctx* c) {
     if (!c) return;
-    DBuf* bufs[] = {&c->win, &c->items,  &c->results, &c->order,     &c->queue,    &c->mbs,      &c->mbcount,   &c->cells,
+    DBuf* bufs[] = {&c->cand, &c->ncand, &c->vflag, &c->lane_scratch, &c->win, &c->items,  &c->results, &c->order,     &c->queue,    &c->mbs,      &c->mbcount,   &c->cells,
                     &c->out,    &c->targets, &c->limits,    &c->found,    &c->next_lut, &c->chunks,    &c->tiles,
                     &c->rerr,   &c->markers, &c->crc_table, &c->pieces,   &c->piece_crc, &c->mpiece,   &c->exp_crc,
                     &c->exp_isize, &c->got_crc, &c->got_len, &c->mstatus, &c->comp};

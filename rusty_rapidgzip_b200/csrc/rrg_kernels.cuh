@@ -815,6 +815,482 @@ __global__ void k_inflate(InflateArgs A) {
     }
 }
 
+// ------------------------------------------------------- lane-per-chunk inflate
+// Every thread is a whole decoder for one work item (the same item contract
+// as k_inflate): 32 chunks advance per warp instruction, which is what a
+// single-member file split at block boundaries, or a BGZF file, offers in
+// the thousands. Tables are per lane in shared memory: a 9-bit litlen LUT and
+// an 8-bit distance LUT of 16-bit entries plus canonical data for longer
+// codes; code lengths and symbol lists live in a per-thread global scratch.
+constexpr int LL_BITS = 9;
+constexpr int DL_BITS = 8;
+constexpr int LANE_THREADS = 64;
+
+struct LaneTab {
+    uint16_t lit[1 << LL_BITS];
+    uint16_t dist[1 << DL_BITS];
+    uint16_t lfirst[16], lcount[16], loff[16];
+    uint16_t dfirst[16], dcount[16], doff[16];
+};
+
+struct LaneScratch {
+    uint8_t lengths[320];
+    uint16_t lsorted[288];
+    uint16_t dsorted[32];
+};
+
+struct LaneConsts {
+    uint16_t lbase[32];
+    uint16_t dbase[32];
+    uint8_t lextra[32];
+    uint8_t dextra[32];
+};
+
+// lane LUT entries (u16): bits 0-3 code length (0 = not in the LUT),
+// bits 4-5 kind, bits 8-15 value.
+//   litlen: kind 0 literal (value = byte), 1 length (value = length code 0..28), 2 EOB, 3 invalid
+//   dist:   kind 0 (value = distance code 0..29), 1 invalid (30/31)
+//   precode: value = symbol
+__device__ __forceinline__ uint16_t lane_entry(int kind, uint32_t s, uint32_t l) {
+    if (kind == TK_LITLEN) {
+        if (s < 256) return (uint16_t)((s << 8) | l);
+        if (s == 256) return (uint16_t)((2u << 4) | l);
+        if (s <= 285) return (uint16_t)(((s - 257) << 8) | (1u << 4) | l);
+        return (uint16_t)((3u << 4) | l);
+    }
+    if (kind == TK_DIST) return (uint16_t)(s < 30 ? ((s << 8) | l) : ((1u << 4) | l));
+    return (uint16_t)((s << 8) | l);
+}
+
+// Canonical table build for one lane (RFC 1951 §3.2.2); non-strict like
+// huffman.rs build_into: only an oversubscribed tree (>= 2 symbols) fails.
+__device__ int lane_build(const uint8_t* len, int n, uint16_t* lut, int lut_bits, uint16_t* first, uint16_t* count,
+                          uint16_t* off, uint16_t* sorted, int kind) {
+    uint16_t cnt[16], next[16];
+    for (int l = 0; l < 16; l++) cnt[l] = 0;
+    for (int s = 0; s < n; s++) cnt[len[s] & 15]++;
+    cnt[0] = 0;
+    uint32_t kraft = 0, nsym = 0;
+    for (int l = 1; l < 16; l++) {
+        kraft += (uint32_t)cnt[l] << (15 - l);
+        nsym += cnt[l];
+    }
+    if (nsym >= 2 && kraft > 32768u) return MSG_OVERSUB;
+    uint32_t f = 0, o = 0;
+    first[0] = count[0] = off[0] = 0;
+    for (int l = 1; l < 16; l++) {
+        f = (f + cnt[l - 1]) << 1;
+        first[l] = (uint16_t)f;
+        next[l] = (uint16_t)f;
+        count[l] = cnt[l];
+        off[l] = (uint16_t)o;
+        o += cnt[l];
+    }
+    const uint32_t size = 1u << lut_bits;
+    uint32_t* lut32 = reinterpret_cast<uint32_t*>(lut);
+    for (uint32_t i = 0; i < size / 2; i++) lut32[i] = 0;
+    for (int s = 0; s < n; s++) {
+        const uint32_t l = len[s];
+        if (!l) continue;
+        const uint32_t code = next[l]++;
+        sorted[off[l] + (code - first[l])] = (uint16_t)s;
+        if ((int)l <= lut_bits) {
+            const uint16_t e = lane_entry(kind, (uint32_t)s, l);
+            const uint32_t rev = __brev(code) >> (32 - l);
+            for (uint32_t i = rev; i < size; i += 1u << l) lut[i] = e;
+        }
+    }
+    return MSG_NONE;
+}
+
+// Longer codes: canonical decode over lengths lut_bits+1..15. Returns the
+// symbol and sets *l, or returns -1.
+__device__ __forceinline__ int lane_long(uint64_t buf, const uint16_t* first, const uint16_t* count,
+                                         const uint16_t* off, const uint16_t* sorted, int lut_bits, uint32_t* l) {
+    const uint32_t rv = __brev((uint32_t)buf);
+    for (int k = lut_bits + 1; k <= 15; k++) {
+        const uint32_t code = rv >> (32 - k);
+        const uint32_t d = code - first[k];
+        if (d < count[k]) {
+            *l = (uint32_t)k;
+            return sorted[off[k] + d];
+        }
+    }
+    return -1;
+}
+
+struct LaneState {
+    BR br;
+    uint64_t cur, cap, member_start, markers;
+    int32_t status, msg;
+    bool markers_ok, counting;
+};
+
+// Huffman-coded block body for one lane.
+template <typename CellT>
+__device__ void lane_codes(LaneState& st, LaneTab& T, const LaneScratch* scr, const LaneConsts& K, CellT* out) {
+    BR b = st.br;
+    uint64_t cur = st.cur;
+    uint64_t cap = st.counting ? ~0ull : st.cap;
+    const uint64_t hi_bits = b.s.hi * 8;
+    for (;;) {
+        br_refill(b);
+        uint32_t e = T.lit[b.buf & ((1u << LL_BITS) - 1)];
+        uint32_t cl = e & 15;
+        if (!cl) {
+            const int s = lane_long(b.buf, T.lfirst, T.lcount, T.loff, scr->lsorted, LL_BITS, &cl);
+            if (s < 0) {
+                st.status = br_past_end(b) ? DS_EOF : DS_INVALID;
+                st.msg = MSG_NO_CODE;
+                break;
+            }
+            e = lane_entry(TK_LITLEN, (uint32_t)s, cl);
+        }
+        const uint32_t kind = (e >> 4) & 3;
+        if (kind == 0) {
+            if (cur >= cap) {  // output full: the rest is only measured (this symbol again)
+                st.counting = true;
+                cap = ~0ull;
+                continue;
+            }
+            if (!st.counting) out[cur] = (CellT)(e >> 8);
+            cur++;
+            br_consume(b, cl);
+        } else if (kind == 1) {
+            const uint32_t li = e >> 8;
+            const uint32_t ex = K.lextra[li];
+            const uint32_t length = K.lbase[li] + ((uint32_t)(b.buf >> cl) & ((1u << ex) - 1u));
+            const BR save = b;
+            br_consume(b, cl + ex);
+            br_refill(b);
+            uint32_t de = T.dist[b.buf & ((1u << DL_BITS) - 1)];
+            uint32_t dl = de & 15;
+            if (!dl) {
+                const int s = lane_long(b.buf, T.dfirst, T.dcount, T.doff, scr->dsorted, DL_BITS, &dl);
+                if (s < 0) {
+                    st.status = br_past_end(b) ? DS_EOF : DS_INVALID;
+                    st.msg = MSG_NO_CODE;
+                    break;
+                }
+                de = lane_entry(TK_DIST, (uint32_t)s, dl);
+            }
+            if (de & 0x10u) {
+                st.status = DS_INVALID;
+                st.msg = MSG_DIST_RANGE;
+                break;
+            }
+            const uint32_t di = de >> 8;
+            const uint32_t dx = K.dextra[di];
+            const uint32_t d = K.dbase[di] + ((uint32_t)(b.buf >> dl) & ((1u << dx) - 1u));
+            if (cur + length > cap) {
+                b = save;  // output full: re-read this match, measuring only
+                st.counting = true;
+                cap = ~0ull;
+                continue;
+            }
+            br_consume(b, dl + dx);
+            if (!st.counting) {
+                const int64_t c0 = (int64_t)cur;
+                const int64_t ms = (int64_t)st.member_start;
+                int64_t k = 0;
+                // references before the member start: markers (first member of a
+                // speculative chunk) or an error
+                for (; k < (int64_t)length && c0 + k - (int64_t)d < ms; k++) {
+                    const int64_t src = c0 + k - (int64_t)d;
+                    if (st.markers_ok && src < 0) {
+                        out[c0 + k] = (CellT)(MARKER16 | (uint32_t)(-src - 1));
+                        st.markers++;
+                    } else {
+                        st.status = DS_INVALID;
+                        st.msg = MSG_DIST_FAR;
+                        break;
+                    }
+                }
+                if (st.status) break;
+                CellT* dst = out + c0;
+                const CellT* src = out + c0 - d;
+                if (d >= (uint32_t)length) {
+                    for (; k + 4 <= (int64_t)length; k += 4) {
+                        const CellT v0 = src[k], v1 = src[k + 1], v2 = src[k + 2], v3 = src[k + 3];
+                        dst[k] = v0;
+                        dst[k + 1] = v1;
+                        dst[k + 2] = v2;
+                        dst[k + 3] = v3;
+                    }
+                }
+                for (; k < (int64_t)length; k++) dst[k] = src[k];
+            }
+            cur += length;
+        } else if (kind == 2) {
+            br_consume(b, cl);
+            break;
+        } else {
+            st.status = DS_INVALID;
+            st.msg = MSG_LITLEN_RANGE;
+            break;
+        }
+        if (br_tell_abs(b) > hi_bits) {
+            st.status = DS_EOF;
+            break;
+        }
+    }
+    st.br = b;
+    st.cur = cur;
+}
+
+// Dynamic header (inflate.rs:74-145) for one lane.
+__device__ void lane_dynamic(LaneState& st, LaneTab& T, LaneScratch* scr) {
+    BR& b = st.br;
+    const uint32_t hlit = br_read(b, 5) + 257, hdist = br_read(b, 5) + 1, hclen = br_read(b, 4) + 4;
+    if (hlit > 286 || hdist > 30) {
+        st.status = DS_INVALID;
+        st.msg = MSG_HLIT_HDIST;
+        return;
+    }
+    uint8_t pre[19];
+    for (int i = 0; i < 19; i++) pre[i] = 0;
+    for (uint32_t i = 0; i < hclen; i++) pre[c_cl_order[i]] = (uint8_t)br_read(b, 3);
+    if (br_past_end(b)) {
+        st.status = DS_EOF;
+        return;
+    }
+    // precode table (7 bits) in the distance LUT's space
+    for (int i = 0; i < 19; i++) scr->lengths[i] = pre[i];
+    int m = lane_build(scr->lengths, 19, T.dist, PRE_BITS, T.dfirst, T.dcount, T.doff, scr->dsorted, TK_PRE);
+    if (m) {
+        st.status = DS_INVALID;
+        st.msg = m;
+        return;
+    }
+    const uint32_t total = hlit + hdist;
+    for (uint32_t i = 0; i < total; i++) scr->lengths[i] = 0;
+    uint32_t i = 0;
+    while (i < total) {
+        br_refill(b);
+        const uint32_t e = T.dist[b.buf & ((1u << PRE_BITS) - 1)];
+        const uint32_t cl = e & 15;
+        if (!cl) {
+            st.status = DS_INVALID;
+            st.msg = MSG_NO_CODE;
+            return;
+        }
+        br_consume(b, cl);
+        const uint32_t sym = e >> 8;
+        if (sym <= 15) {
+            scr->lengths[i++] = (uint8_t)sym;
+        } else if (sym == 16) {
+            if (i == 0) {
+                st.status = DS_INVALID;
+                st.msg = MSG_CODE16_FIRST;
+                return;
+            }
+            const uint32_t r = br_read(b, 2) + 3;
+            if (i + r > total) {
+                st.status = DS_INVALID;
+                st.msg = MSG_CODE16_OVER;
+                return;
+            }
+            const uint8_t prev = scr->lengths[i - 1];
+            for (uint32_t j = 0; j < r; j++) scr->lengths[i + j] = prev;
+            i += r;
+        } else if (sym == 17) {
+            const uint32_t r = br_read(b, 3) + 3;
+            if (i + r > total) {
+                st.status = DS_INVALID;
+                st.msg = MSG_CODE17_OVER;
+                return;
+            }
+            i += r;
+        } else {
+            const uint32_t r = br_read(b, 7) + 11;
+            if (i + r > total) {
+                st.status = DS_INVALID;
+                st.msg = MSG_CODE18_OVER;
+                return;
+            }
+            i += r;
+        }
+        if (br_past_end(b)) {
+            st.status = DS_EOF;
+            return;
+        }
+    }
+    if (scr->lengths[256] == 0) {
+        st.status = DS_INVALID;
+        st.msg = MSG_EOB_ZERO;
+        return;
+    }
+    m = lane_build(scr->lengths, (int)hlit, T.lit, LL_BITS, T.lfirst, T.lcount, T.loff, scr->lsorted, TK_LITLEN);
+    if (!m)
+        m = lane_build(scr->lengths + hlit, (int)hdist, T.dist, DL_BITS, T.dfirst, T.dcount, T.doff, scr->dsorted,
+                       TK_DIST);
+    if (m) {
+        st.status = DS_INVALID;
+        st.msg = m;
+    }
+}
+
+__device__ void lane_fixed(LaneState& st, LaneTab& T, LaneScratch* scr) {
+    for (int i = 0; i < 288; i++) scr->lengths[i] = i < 144 ? 8 : i < 256 ? 9 : i < 280 ? 7 : 8;
+    for (int i = 0; i < 30; i++) scr->lengths[288 + i] = 5;
+    lane_build(scr->lengths, 288, T.lit, LL_BITS, T.lfirst, T.lcount, T.loff, scr->lsorted, TK_LITLEN);
+    lane_build(scr->lengths + 288, 30, T.dist, DL_BITS, T.dfirst, T.dcount, T.doff, scr->dsorted, TK_DIST);
+    (void)st;
+}
+
+template <typename CellT>
+__device__ void lane_stored(LaneState& st, CellT* out) {
+    BR& b = st.br;
+    br_consume(b, b.bits & 7);
+    const uint32_t len = br_read(b, 16), nlen = br_read(b, 16);
+    if ((len ^ 0xffffu) != nlen) {
+        st.status = DS_INVALID;
+        st.msg = MSG_STORED_NLEN;
+        return;
+    }
+    const uint64_t bp = br_tell(b) >> 3;
+    if (b.s.lo + bp + len > b.s.hi) {
+        st.status = DS_EOF;
+        return;
+    }
+    if (!st.counting && st.cur + len > st.cap) st.counting = true;
+    if (!st.counting)
+        for (uint32_t i = 0; i < len; i++) out[st.cur + i] = (CellT)src_byte(b.s, bp + i);
+    st.cur += len;
+    br_seek(b, (bp + len) * 8);
+}
+
+template <typename CellT>
+__device__ void lane_item(const InflateArgs& A, uint32_t item_idx, LaneTab& T, LaneScratch* scr, const LaneConsts& K) {
+    const ChunkItem it = A.items[item_idx];
+    CellT* out = (CellT*)A.out + it.out_off;
+    LaneState st;
+    st.br.s = make_src(A.in + it.in_off, it.in_len);
+    st.br.nw = 0;
+    st.br.buf = 0;
+    st.br.bits = 0;
+    st.cur = 0;
+    st.cap = it.out_cap;
+    st.member_start = 0;
+    st.markers = 0;
+    st.status = 0;
+    st.msg = 0;
+    st.markers_ok = (it.flags & ITEM_MARKERS) != 0 && sizeof(CellT) == 2;
+    st.counting = false;
+    const uint64_t body_len = it.in_len;
+    uint64_t start = it.start_bit;
+    uint32_t trailer_crc = 0, trailer_isize = 0;
+    if (it.flags & ITEM_ONE_MEMBER) {
+        uint64_t hl = 0;
+        int msg = 0;
+        st.status = dev_parse_header(st.br.s, 0, &hl, &msg);
+        st.msg = msg;
+        start = hl * 8;
+    }
+    if (!st.status) {
+        if (start > body_len * 8) st.status = DS_EOF;
+        else br_seek(st.br, start);
+    }
+    bool final_block = false, fixed_loaded = false;
+    uint32_t n_members = 0;
+    uint64_t end_bit = 0;
+    while (!st.status) {
+        if (br_tell(st.br) >= it.end_hint) break;
+        uint32_t bfinal = 0;
+        for (;;) {
+            bfinal = br_read(st.br, 1);
+            const uint32_t bt = br_read(st.br, 2);
+            if (br_past_end(st.br)) {
+                st.status = DS_EOF;
+                break;
+            }
+            if (bt == 0) {
+                lane_stored<CellT>(st, out);
+            } else if (bt == 1) {
+                if (!fixed_loaded) lane_fixed(st, T, scr);
+                fixed_loaded = true;
+                lane_codes<CellT>(st, T, scr, K, out);
+            } else if (bt == 2) {
+                fixed_loaded = false;
+                lane_dynamic(st, T, scr);
+                if (!st.status) lane_codes<CellT>(st, T, scr, K, out);
+            } else {
+                st.status = DS_INVALID;
+                st.msg = MSG_RESERVED_BTYPE;
+            }
+            if (st.status || bfinal) break;
+            if (br_tell(st.br) >= it.end_hint) break;
+        }
+        if (st.status || !bfinal) break;
+        br_consume(st.br, st.br.bits & 7);
+        const uint64_t tb = br_tell(st.br) >> 3;
+        if (tb + 8 > body_len) {
+            st.status = DS_TRUNCATED;
+            break;
+        }
+        trailer_crc = le32_at(st.br.s, tb);
+        trailer_isize = le32_at(st.br.s, tb + 4);
+        if (!(it.flags & ITEM_ONE_MEMBER)) {
+            const uint32_t slot = atomicAdd(A.mb_count, 1u);
+            if (slot < A.mb_cap) {
+                MemberRec r;
+                r.item = it.id;
+                r.seq = n_members;
+                r.cell_off = st.cur;
+                r.crc = trailer_crc;
+                r.isize = trailer_isize;
+                r.trailer_byte = tb;
+                A.mbs[slot] = r;
+            }
+        }
+        n_members++;
+        const uint64_t after = tb + 8;
+        if (after >= body_len || (it.flags & ITEM_ONE_MEMBER)) {
+            final_block = true;
+            end_bit = after * 8;
+            break;
+        }
+        uint64_t hl = 0;
+        int msg = 0;
+        st.status = dev_parse_header(st.br.s, after, &hl, &msg);
+        st.msg = msg;
+        if (st.status) break;
+        br_seek(st.br, (after + hl) * 8);
+        st.member_start = st.cur;
+        st.markers_ok = false;
+    }
+    ChunkResult r;
+    r.n_cells = st.cur;
+    r.actual_end_bit = final_block ? end_bit : br_tell(st.br);
+    r.status = st.status ? st.status : (st.counting ? DS_OVERFLOW : DS_OK);
+    r.msg = st.msg;
+    r.final_block = final_block ? 1 : 0;
+    r.n_members = n_members;
+    r.markers = (it.flags & ITEM_ONE_MEMBER) ? (((uint64_t)trailer_isize << 32) | trailer_crc) : st.markers;
+    r.err_bit = br_tell(st.br);
+    A.results[item_idx] = r;
+}
+
+template <typename CellT>
+__global__ void __launch_bounds__(LANE_THREADS) k_inflate_lanes(InflateArgs A, LaneScratch* scratch) {
+    RRG_DYN_SMEM(smem_raw);
+    __shared__ LaneConsts K;
+    for (int i = threadIdx.x; i < 32; i += blockDim.x) {
+        K.lbase[i] = i < 29 ? c_len_base[i] : 0;
+        K.lextra[i] = i < 29 ? c_len_extra[i] : 0;
+        K.dbase[i] = i < 30 ? c_dist_base[i] : 0;
+        K.dextra[i] = i < 30 ? c_dist_extra[i] : 0;
+    }
+    __syncthreads();
+    LaneTab& T = reinterpret_cast<LaneTab*>(smem_raw)[threadIdx.x];
+    LaneScratch* scr = scratch + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (;;) {
+        const uint32_t idx = atomicAdd(A.queue, 1u);
+        if (idx >= A.n_items) break;
+        lane_item<CellT>(A, A.order ? A.order[idx] : idx, T, scr, K);
+    }
+}
+
 // ------------------------------------------------------- block finder
 // One warp per target; the search runs over tiles of 1024 bit offsets that
 // start at the current skip-chain position. For its 32 offsets each lane
@@ -1138,6 +1614,222 @@ __global__ void __launch_bounds__(128) k_find_blocks(FindArgs A) {
             if (pos + 13 > limit) done = true;
         }
         if (lane == 0) A.found[idx] = result;
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------------- full-stream candidate scan
+// The decode path needs many block boundaries, not the reference's one per
+// target, so it tests every bit offset of the body: 4 KiB tiles staged in
+// shared memory with 16-byte loads, each thread testing the 128 offsets of
+// its 16 bytes (prefilter BFINAL=0, BTYPE=2, HLIT<=29, HDIST<=29, then the
+// strict Kraft test of the precode), survivors compacted with warp ballots.
+// k_verify_light then applies the strict code-length checks of
+// read_dynamic_header_strict_into (block_finder.rs:196-262) per thread, and
+// the last survivors get verify_heavy (tables + 64 trial symbols).
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_TILE = SCAN_THREADS * 16;
+constexpr int SCAN_HALO = 32;
+
+struct ScanArgs {
+    const uint8_t* body;
+    uint64_t body_len;
+    uint64_t* cand;
+    uint32_t* n_cand;
+    uint32_t cap;
+};
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_candidates(ScanArgs A) {
+    __shared__ __align__(16) uint32_t tile[(SCAN_TILE + SCAN_HALO) / 4];
+    const uintptr_t addr = (uintptr_t)A.body;
+    const uint8_t* base = (const uint8_t*)(addr & ~(uintptr_t)15);
+    const uint64_t lo = addr & 15, hi = lo + A.body_len;
+    const uint64_t n_tiles = (hi + SCAN_TILE - 1) / SCAN_TILE;
+    const int lane = threadIdx.x & 31;
+    uint8_t* tb = reinterpret_cast<uint8_t*>(tile);
+    for (uint64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        const uint64_t t0 = t * SCAN_TILE;
+        for (uint32_t q = threadIdx.x; q < (SCAN_TILE + SCAN_HALO) / 16; q += blockDim.x) {
+            const uint64_t b0 = t0 + 16ull * q;
+            if (b0 >= lo && b0 + 16 <= hi) {
+                *reinterpret_cast<uint4*>(tb + 16 * q) = __ldg(reinterpret_cast<const uint4*>(base + b0));
+            } else {
+                for (int k = 0; k < 16; k++) {
+                    const uint64_t p = b0 + k;
+                    tb[16 * q + k] = (p >= lo && p < hi) ? __ldg(base + p) : 0;
+                }
+            }
+        }
+        __syncthreads();
+        uint32_t W[7];
+        for (int q = 0; q < 7; q++) W[q] = tile[threadIdx.x * 4 + q];
+        const uint64_t first_bit = (t0 + 16ull * threadIdx.x) * 8;  // relative to base
+        for (uint32_t i = 0; i < 128; i++) {
+            const uint64_t pa = first_bit + i;
+            bool pass = false;
+            if (pa >= lo * 8 && pa + 13 <= hi * 8) {
+                const uint32_t q = i >> 5, r = i & 31;
+                auto bits = [&](uint32_t off) -> uint32_t {
+                    const uint32_t b = i + off, qq = b >> 5, rr = b & 31;
+                    uint32_t l = 0, h = 0;
+#pragma unroll
+                    for (int z = 0; z < 6; z++) {
+                        if ((uint32_t)z == qq) {
+                            l = W[z];
+                            h = W[z + 1];
+                        }
+                    }
+                    return rr ? ((l >> rr) | (h << (32 - rr))) : l;
+                };
+                (void)q;
+                (void)r;
+                const uint32_t w = bits(0) & 0x1fffu;
+                if ((w & 7u) == 4u && ((w >> 3) & 31u) <= 29u && ((w >> 8) & 31u) <= 29u) {
+                    const uint32_t hclen = (bits(13) & 15u) + 4;
+                    const uint32_t y = bits(17), z = bits(47);
+                    uint32_t kraft = 0, nsym = 0;
+#pragma unroll
+                    for (uint32_t j = 0; j < 19; j++) {
+                        const uint32_t l = j < 10 ? (y >> (3 * j)) & 7u : (z >> (3 * (j - 10))) & 7u;
+                        if (j < hclen && l) {
+                            kraft += 128u >> l;
+                            nsym++;
+                        }
+                    }
+                    pass = nsym < 2 || kraft == 128u;
+                }
+            }
+            const unsigned m = __ballot_sync(FULLMASK, pass);
+            if (m) {
+                uint32_t base_slot = 0;
+                if (lane == __ffs(m) - 1) base_slot = atomicAdd(A.n_cand, (uint32_t)__popc(m));
+                base_slot = __shfl_sync(FULLMASK, base_slot, __ffs(m) - 1);
+                if (pass) {
+                    const uint32_t slot = base_slot + __popc(m & ((1u << lane) - 1u));
+                    if (slot < A.cap) A.cand[slot] = pa - lo * 8;
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+struct VerifyArgs {
+    const uint8_t* body;
+    uint64_t body_len;
+    const uint64_t* cand;
+    uint32_t n;
+    uint8_t* light_ok;  // per candidate
+    uint32_t* queue;
+};
+
+// strict code-length parse without building tables: litlen and distance Kraft
+// sums are accumulated as the lengths are decoded.
+__device__ bool verify_light(const Src& s, uint64_t total_bits, uint64_t pos) {
+    VC c{&s, pos, total_bits, true};
+    c.read(3);
+    const uint32_t hlit = c.read(5) + 257, hdist = c.read(5) + 1, hclen = c.read(4) + 4;
+    if (!c.ok || hlit > 286 || hdist > 30) return false;
+    uint8_t cl[19];
+    for (int i = 0; i < 19; i++) cl[i] = 0;
+    for (uint32_t i = 0; i < hclen; i++) cl[c_cl_order[i]] = (uint8_t)c.read(3);
+    if (!c.ok) return false;
+    uint32_t pc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = 0; i < 19; i++) pc[cl[i]]++;
+    pc[0] = 0;
+    uint32_t k = 0, ns = 0;
+    for (int l = 1; l < 8; l++) {
+        k += pc[l] << (7 - l);
+        ns += pc[l];
+    }
+    if (ns >= 2 && k != 128u) return false;
+    uint8_t sym[19];
+    {
+        uint32_t off[8];
+        off[1] = 0;
+        for (int l = 1; l < 7; l++) off[l + 1] = off[l] + pc[l];
+        for (int i = 0; i < 19; i++)
+            if (cl[i]) sym[off[cl[i]]++] = (uint8_t)i;
+    }
+    const uint32_t total = hlit + hdist;
+    uint32_t i = 0, prev = 0, len256 = 0;
+    uint32_t kl = 0, nl = 0, kd = 0, nd = 0;
+    auto put = [&](uint32_t L) {
+        if (i < hlit) {
+            if (L) {
+                kl += 1u << (15 - L);
+                nl++;
+            }
+            if (i == 256) len256 = L;
+        } else if (L) {
+            kd += 1u << (15 - L);
+            nd++;
+        }
+        i++;
+    };
+    while (i < total) {
+        // precode symbol: HuffmanDecoder::decode needs 10 bits available
+        if (c.pos + 10 > c.total) return false;
+        const uint32_t bits = peek_at(s, c.pos, 7);
+        int code = 0, first = 0, index = 0, got = -1;
+        uint32_t used = 0;
+        for (int l = 1; l <= 7; l++) {
+            code |= (int)((bits >> (l - 1)) & 1u);
+            const int cnt = (int)pc[l];
+            if (code - cnt < first) {
+                got = sym[index + (code - first)];
+                used = (uint32_t)l;
+                break;
+            }
+            index += cnt;
+            first += cnt;
+            first <<= 1;
+            code <<= 1;
+        }
+        if (got < 0) return false;
+        c.pos += used;
+        if (got <= 15) {
+            prev = (uint32_t)got;
+            put(prev);
+        } else if (got == 16) {
+            if (i == 0) return false;
+            const uint32_t r = c.read(2) + 3;
+            if (!c.ok || i + r > total) return false;
+            for (uint32_t j = 0; j < r; j++) put(prev);
+        } else {
+            const uint32_t r = got == 17 ? c.read(3) + 3 : c.read(7) + 11;
+            if (!c.ok || i + r > total) return false;
+            for (uint32_t j = 0; j < r; j++) put(0);
+            prev = 0;
+        }
+    }
+    if (len256 == 0) return false;
+    if (nl >= 2 && kl != 32768u) return false;
+    if (nd >= 2 && kd != 32768u) return false;
+    return true;
+}
+
+__global__ void __launch_bounds__(256) k_verify_light(VerifyArgs A) {
+    const Src s = make_src(A.body, A.body_len);
+    const uint64_t total_bits = A.body_len * 8;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x)
+        A.light_ok[i] = verify_light(s, total_bits, A.cand[i]) ? 1 : 0;
+}
+
+// One warp per light survivor: tables + 64 trial symbols (verify_heavy).
+__global__ void __launch_bounds__(128) k_verify_heavy(VerifyArgs A) {
+    RRG_DYN_SMEM(smem_raw);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    FindSmem& S = reinterpret_cast<FindSmem*>(smem_raw)[warp];
+    const Src s = make_src(A.body, A.body_len);
+    const uint64_t total_bits = A.body_len * 8;
+    for (;;) {
+        uint32_t idx = 0;
+        if (lane == 0) idx = atomicAdd(A.queue, 1u);
+        idx = (uint32_t)bcast32((int32_t)idx);
+        if (idx >= A.n) break;
+        const bool ok = verify_heavy(S, s, total_bits, A.cand[idx], lane);
+        if (lane == 0) A.light_ok[idx] = ok ? 1 : 0;
         __syncwarp();
     }
 }

@@ -50,10 +50,15 @@ def test_raw_deflate_vectors(gpu_decoder_factory):
         assert d.decompress(gz) == plain, v["name"]
 
 
+MODES = [dict(), dict(warps_per_stream=1), dict(boundary_mode=1), dict(warps_per_stream=1, boundary_mode=1)]
+MODE_IDS = ["lanes-scan", "warps-scan", "lanes-targets", "warps-targets"]
+
+
+@pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
 @pytest.mark.parametrize("gpu_chunk", [8192, 65536, 0])
-def test_fastq_level6(gpu_decoder_factory, gpu_chunk):
+def test_fastq_level6(gpu_decoder_factory, gpu_chunk, mode):
     raw, gz = W.config0(8 << 20, seed=5)
-    d = gpu_decoder_factory(gpu_chunk_bytes=gpu_chunk)
+    d = gpu_decoder_factory(gpu_chunk_bytes=gpu_chunk, **mode)
     out, st = d.count(gz)
     assert out == len(raw)
     got = d.decompress(gz)
@@ -61,10 +66,11 @@ def test_fastq_level6(gpu_decoder_factory, gpu_chunk):
     assert got == oracle.read_gz(gz, 4, 1 << 20)
 
 
+@pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
 @pytest.mark.parametrize("gpu_chunk", [16384, 0])
-def test_zipf_level9(gpu_decoder_factory, gpu_chunk):
+def test_zipf_level9(gpu_decoder_factory, gpu_chunk, mode):
     raw, gz = W.config1(24 << 20, seed=6)
-    d = gpu_decoder_factory(gpu_chunk_bytes=gpu_chunk)
+    d = gpu_decoder_factory(gpu_chunk_bytes=gpu_chunk, **mode)
     out = d.decompress(gz)
     assert out == raw
 
@@ -147,10 +153,11 @@ def test_crc32_parity(gpu_decoder_factory, n):
     assert d.crc32(dev(data), n) == zlib.crc32(data)
 
 
-def test_bgzf(gpu_decoder_factory):
+@pytest.mark.parametrize("mode", MODES[:2], ids=MODE_IDS[:2])
+def test_bgzf(gpu_decoder_factory, mode):
     raw = W.fastq_like(12 << 20, 12)
     b = W.bgzf(raw, 5)
-    d = gpu_decoder_factory()
+    d = gpu_decoder_factory(**mode)
     assert d.decompress(b) == raw
     out, st = d.count(b)
     assert out == len(raw) and st.members == (len(raw) + 65279) // 65280
@@ -195,11 +202,12 @@ def test_batch_of_files(gpu_decoder_factory):
         assert host[o:o + len(r)] == r
 
 
-def test_concat_members(gpu_decoder_factory):
+@pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
+def test_concat_members(gpu_decoder_factory, mode):
     parts = [W.fastq_like(n, i) for i, n in enumerate([1, 100, 65_537, 1, 300_000, 7, 1_000_000])]
     gz = b"".join(gzip_cli(p, [6, 1, 9][i % 3]) for i, p in enumerate(parts))
     for gc in (4096, 65536):
-        d = gpu_decoder_factory(gpu_chunk_bytes=gc)
+        d = gpu_decoder_factory(gpu_chunk_bytes=gc, **mode)
         assert d.decompress(gz) == b"".join(parts)
     parts = [b"", b"abc", b"", b"", b"def" * 1000, b""] + [f"member-{i}-payload\n".encode() for i in range(500)]
     gz = b"".join(gzip_cli(p) for p in parts)
@@ -207,21 +215,23 @@ def test_concat_members(gpu_decoder_factory):
     assert d.decompress(gz) == b"".join(parts)
 
 
-def test_nested_gzip(gpu_decoder_factory):
+@pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
+def test_nested_gzip(gpu_decoder_factory, mode):
     original = np.random.default_rng(0xC0FFEE).integers(32, 127, 2 << 20, dtype=np.uint8).tobytes()
     inner = gzip_cli(original, 6)
     outer = gzip_cli(inner, 6)
-    d = gpu_decoder_factory(gpu_chunk_bytes=16384)
+    d = gpu_decoder_factory(gpu_chunk_bytes=16384, **mode)
     out, st = [], None
     st = d.decode_host(outer, out.append)
     assert b"".join(out) == inner
     assert st.speculation_failures > 0
 
 
-def test_mixed_block_types(gpu_decoder_factory):
+@pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
+def test_mixed_block_types(gpu_decoder_factory, mode):
     p = W.fastq_like(300_000, 1) + W.random_bytes(300_000, 5) + W.zipf_text(300_000, 3)
     gz = gzip_cli(p, 1)
-    d = gpu_decoder_factory(gpu_chunk_bytes=16384)
+    d = gpu_decoder_factory(gpu_chunk_bytes=16384, **mode)
     assert d.decompress(gz) == p
 
 
