@@ -196,6 +196,25 @@ int rrg_gpu_poll(rrg_ctx* ctx, int64_t* request_id, uint8_t** out, size_t* out_l
 /* Number of requests submitted but not yet returned by rrg_gpu_poll. */
 int64_t rrg_gpu_pending(rrg_ctx* ctx);
 
+/* CRC32 (IEEE, as crc32fast::hash) of `len` bytes at device address `d_data`,
+ * written to the host word *crc_out, for callers that cannot let a library
+ * allocate device memory (an application that owns the GPU's memory through
+ * its own pool allocator, where a hidden cudaMalloc can fail and a cudaFree
+ * synchronises the device; a latency-critical path that must not stall on
+ * allocation). No counterpart in the reference: it has no device memory.
+ * It calls no cudaMalloc/cudaFree and needs no context. All scratch lives in
+ * one fixed device array of about 336 KB inside this library, which every GPU
+ * that loads the library holds until the process exits; that bounds `len` to
+ * 4 GiB (4294967296 bytes), and longer inputs fail with RRG_ERR_CAPACITY. The
+ * first call on a device looks up that array and loads the CRC tables; make
+ * it before any stream capture. Work is ordered on `stream` (a cudaStream_t,
+ * or NULL for the legacy default stream) and the call returns once the result
+ * is on the host. Every call shares the same array, so calls that overlap on
+ * the GPU (from several host threads or streams) race and must be serialised
+ * by the caller. */
+int rrg_gpu_crc32_noalloc(const uint8_t* d_data, size_t len, uint32_t* crc_out, void* stream,
+                          rrg_error* err);
+
 void rrg_gpu_free(void* p);
 
 /* Library version string and the number of kernels this library has launched

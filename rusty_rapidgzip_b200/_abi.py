@@ -241,6 +241,7 @@ def load_library(path: str | None = None):
                                    C.POINTER(i32), C.POINTER(C.c_double), i32, E]
         L.rrg_gpu_pending.argtypes = [vp]
         L.rrg_gpu_pending.restype = C.c_int64
+        L.rrg_gpu_crc32_noalloc.argtypes = [vp, sz, C.POINTER(C.c_uint32), vp, E]
         L.rrg_gpu_free.argtypes = [vp]
         L.rrg_gpu_version.restype = C.c_char_p
         L.rrg_gpu_kernel_launch_count.restype = C.c_uint64
@@ -477,6 +478,17 @@ def read_gz(path, sink, config: Config | None = None) -> DecodeStats:
 def decompress(data, config: Config | None = None) -> bytes:
     with Decoder(config) as d:
         return d.decompress(data)
+
+
+def crc32_noalloc(d_data, length: int, stream=None, lib: str | None = None) -> int:
+    """CRC32 of a device buffer through rrg_gpu_crc32_noalloc: no device
+    memory is allocated (fixed library scratch; at most 4 GiB per call; calls
+    that overlap on the GPU race)."""
+    out = C.c_uint32()
+    e = _Error()
+    load_library(lib).rrg_gpu_crc32_noalloc(_ptr(d_data), length, C.byref(out), _ptr(stream), C.byref(e))
+    _raise(e)
+    return int(out.value)
 
 
 def kernel_launch_count(lib: str | None = None) -> int:

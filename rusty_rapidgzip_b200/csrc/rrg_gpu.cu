@@ -1532,3 +1532,118 @@ const char* rrg_gpu_version(void) { return "rrg-gpu 0.1 (sm_100a)"; }
 uint64_t rrg_gpu_kernel_launch_count(void) { return g_launches.load(); }
 
 }  // extern "C"
+
+// ====================================================================== allocation-free CRC32
+// For callers that cannot let a library allocate device memory: code that
+// owns all of the GPU's memory through its own pool allocator (a cudaMalloc
+// behind its back can fail once the pool has reserved the device, and the
+// matching cudaFree synchronises the whole device), or a latency-critical
+// serving path that must not stall on allocation. Everything this entry point
+// needs beyond the caller's input and output lives in one fixed, file-scope
+// device array, so a call allocates nothing.
+namespace {
+
+constexpr uint64_t NA_PIECE = 256 * 1024;             // bytes per CRC piece
+constexpr uint32_t NA_MAX_PIECES = 16384;             // => at most 4 GiB per call
+constexpr uint64_t NA_MAX_BYTES = NA_PIECE * NA_MAX_PIECES;
+
+struct NoAllocScratch {
+    uint32_t table[8 * 256];                  // slice-by-8 CRC table
+    CrcPiece pieces[NA_MAX_PIECES];
+    uint32_t piece_crc[NA_MAX_PIECES];
+    uint32_t member_piece_start[2];
+    uint32_t expected_crc, expected_isize, got_crc;
+    int32_t status;
+    uint64_t got_len;
+};
+
+}  // namespace
+
+// The scratch every call shares (about 336 KB, held by every GPU that loads
+// this library until the process exits).
+static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+NoAllocScratch* g_noalloc_dev[64] = {nullptr};  // device address of the scratch, per device ordinal
+
+// Piece descriptors for one buffer; also resets the fields k_crc_members reads.
+__global__ void k_noalloc_pieces(NoAllocScratch* S, uint64_t len, uint32_t n_pieces) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_pieces; i += gridDim.x * blockDim.x) {
+        const uint64_t o = (uint64_t)i * NA_PIECE;
+        S->pieces[i] = CrcPiece{o, len - o < NA_PIECE ? len - o : NA_PIECE};
+        S->piece_crc[i] = 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        S->member_piece_start[0] = 0;
+        S->member_piece_start[1] = n_pieces;
+        S->expected_crc = 0;
+        S->expected_isize = (uint32_t)len;
+        S->got_crc = 0;
+        S->got_len = 0;
+        S->status = 0;
+    }
+}
+
+// First call on the current device: find the scratch's device address and
+// load the CRC tables into it and into constant memory.
+int noalloc_setup(int dev, NoAllocScratch** out, rrg_error* err) {
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (dev < 0 || dev >= 64) {
+        set_err(err, RRG_ERR_INVALID_ARGUMENT, "device ordinal %d out of range", dev);
+        return RRG_ERR_INVALID_ARGUMENT;
+    }
+    if (!g_noalloc_dev[dev]) {
+        std::call_once(g_tab_once, init_tables);
+        void* p = nullptr;
+        CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        CK(cudaMemcpy(p, g_crc_tab, sizeof(g_crc_tab), cudaMemcpyHostToDevice));
+        CK(cudaMemcpyToSymbol(c_x2k, g_x2k, sizeof(g_x2k)));
+        g_noalloc_dev[dev] = (NoAllocScratch*)p;
+    }
+    *out = g_noalloc_dev[dev];
+    return 0;
+}
+
+}  // namespace
+
+extern "C" int rrg_gpu_crc32_noalloc(const uint8_t* d_data, size_t len, uint32_t* crc_out, void* stream,
+                                     rrg_error* err) {
+    rrg_error local_err;
+    if (!err) err = &local_err;
+    std::memset(err, 0, sizeof(*err));
+    if (!crc_out || (len && !d_data)) {
+        set_err(err, RRG_ERR_INVALID_ARGUMENT, "null argument");
+        return RRG_ERR_INVALID_ARGUMENT;
+    }
+    if (len > NA_MAX_BYTES) {
+        set_err(err, RRG_ERR_CAPACITY, "rrg_gpu_crc32_noalloc handles at most %llu bytes per call, got %llu",
+                (unsigned long long)NA_MAX_BYTES, (unsigned long long)len);
+        return RRG_ERR_CAPACITY;
+    }
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    NoAllocScratch* S = nullptr;
+    int rc = noalloc_setup(dev, &S, err);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint32_t np = (uint32_t)((len + NA_PIECE - 1) / NA_PIECE);
+    RRG_LAUNCH(k_noalloc_pieces, (np + 255) / 256 + 1, 256, 0, st, S, (uint64_t)len, np);
+    g_launches.fetch_add(1);
+    CK(cudaGetLastError());
+    if (np) {
+        CrcArgs A{d_data, S->pieces, np, S->piece_crc, S->table};
+        RRG_LAUNCH(k_crc_pieces, std::min<uint32_t>(np, 148u * 8u), CRC_THREADS, 0, st, A);
+        g_launches.fetch_add(1);
+        CK(cudaGetLastError());
+    }
+    CrcMemberArgs B{S->pieces, S->piece_crc, S->member_piece_start, 1, &S->expected_crc, &S->expected_isize,
+                    &S->got_crc, &S->got_len, &S->status};
+    RRG_LAUNCH(k_crc_members, 1, 32, 0, st, B);
+    g_launches.fetch_add(1);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(crc_out, &S->got_crc, 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return 0;
+}

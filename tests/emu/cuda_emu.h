@@ -203,6 +203,11 @@ inline cudaError_t cudaMemcpyToSymbol(T& sym, const void* src, size_t n, size_t 
     std::memcpy((char*)&sym + off, src, n);
     return cudaSuccess;
 }
+template <class T>
+inline cudaError_t cudaGetSymbolAddress(void** p, T& sym) {
+    *p = (void*)&sym;
+    return cudaSuccess;
+}
 inline cudaError_t cudaStreamCreateWithFlags(cudaStream_t* s, unsigned) {
     *s = (void*)0x1;
     return cudaSuccess;

@@ -107,3 +107,12 @@ def test_finder_parity_adversarial(emu_decoder_factory):
     want = [oracle.find_next_dynamic_block(outer.tobytes(), t, l) for t, l in zip(targets, limits)]
     assert got == want
     assert any(w is not None for w in want)
+
+
+def test_noalloc_crc_emulated():
+    from conftest import build_emu_lib
+    from rusty_rapidgzip_b200._abi import crc32_noalloc
+    lib = build_emu_lib()
+    for n in (0, 1, 300_001, (256 << 10) * 3 + 7):
+        data = np.random.default_rng(n).integers(0, 256, n, dtype=np.uint8)
+        assert crc32_noalloc(haddr(data) if n else 1, n, lib=lib) == zlib.crc32(data.tobytes())
