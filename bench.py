@@ -183,7 +183,8 @@ def run_ours(args, raw, gz, desc):
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", device_id=torch.device("cuda", local))
-    dec = Decoder(Config(device=local, gpu_chunk_bytes=args.gpu_chunk, verbose=False))
+    dec = Decoder(Config(device=local, gpu_chunk_bytes=args.gpu_chunk, warps_per_stream=args.warps_per_stream,
+                         boundary_mode=args.boundary_mode, verbose=False))
     stream = torch.cuda.Stream()
     din = torch.empty(len(gz), dtype=torch.uint8, device="cuda")
     din.copy_(torch.frombuffer(bytearray(gz), dtype=torch.uint8))
@@ -282,6 +283,8 @@ def run_ours(args, raw, gz, desc):
             "config": dict(desc, compressed_bytes=C_, parallelism=f"replicas x{world}",
                            l2="inputs (compressed + output) larger than L2; no flush",
                            gpu_chunk_bytes=args.gpu_chunk or "auto", gpu_chunks=ms.gpu_chunks,
+                           inflate="lane-per-chunk" if args.warps_per_stream < 0 else "warp-per-chunk",
+                           boundaries="every offset" if args.boundary_mode == 2 else "per target",
                            markers=ms.markers, speculation_failures=ms.speculation_failures),
             "e2e": {"value": round(e2e_value, 3), "unit": "GB/s", "h2d_bytes_per_step": C_,
                     "d2h_bytes_per_step": U_},
@@ -308,6 +311,8 @@ def main():
     ap.add_argument("--workload", default="zipf1g", choices=["zipf1g", "fastq64m", "bgzf"])
     ap.add_argument("--size", type=int, default=None)
     ap.add_argument("--gpu-chunk", type=int, default=0)
+    ap.add_argument("--warps-per-stream", type=int, default=0, help="-1: one decoder per lane")
+    ap.add_argument("--boundary-mode", type=int, default=0, help="2: test every bit offset")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -585,55 +585,48 @@ int scan_boundaries(rrg_ctx* c, const uint8_t* body, uint64_t blen, std::vector<
     verified.clear();
     if (blen < 4) return 0;
     KTimer kt(c->stream);
-    uint32_t cap = (uint32_t)std::min<uint64_t>(blen / 32 + 65536, 1ull << 28);
-    uint32_t n = 0;
-    for (int attempt = 0; attempt < 2; attempt++) {
-        CK(dgrow(c->cand, (size_t)cap * 8));
-        CK(dgrow(c->ncand, 16));
-        CK(cudaMemsetAsync(c->ncand.p, 0, 16, c->stream));
-        ScanArgs S{body, blen, (uint64_t*)c->cand.p, (uint32_t*)c->ncand.p, cap};
-        const uint64_t tiles = (blen + 16 + SCAN_TILE - 1) / SCAN_TILE;
-        const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(tiles, (uint64_t)c->n_sm * 8));
-        RRG_LAUNCH(k_scan_candidates, grid, SCAN_THREADS, 0, c->stream, S);
-        LAUNCHED(c);
-        CK(cudaMemcpyAsync(&n, c->ncand.p, 4, cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
-        if (n <= cap) break;
-        cap = n + 65536;
-    }
-    if (n) {
-        CK(dgrow(c->vflag, n));
-        CK(dgrow(c->queue, 16));
-        VerifyArgs V{body, blen, (const uint64_t*)c->cand.p, n, (uint8_t*)c->vflag.p, (uint32_t*)c->queue.p};
-        const uint32_t grid = (uint32_t)std::max<uint32_t>(1, std::min<uint32_t>((n + 255) / 256, c->n_sm * 8));
-        RRG_LAUNCH(k_verify_light, grid, 256, 0, c->stream, V);
-        LAUNCHED(c);
-        std::vector<uint8_t> flags(n);
-        std::vector<uint64_t> cands(n);
-        CK(cudaMemcpyAsync(flags.data(), c->vflag.p, n, cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaMemcpyAsync(cands.data(), c->cand.p, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
-        std::vector<uint64_t> surv;
-        for (uint32_t i = 0; i < n; i++)
-            if (flags[i]) surv.push_back(cands[i]);
-        if (!surv.empty()) {
-            const uint32_t m = (uint32_t)surv.size();
-            CK(cudaMemcpyAsync(c->cand.p, surv.data(), (size_t)m * 8, cudaMemcpyHostToDevice, c->stream));
-            CK(cudaMemsetAsync(c->queue.p, 0, 16, c->stream));
-            VerifyArgs H{body, blen, (const uint64_t*)c->cand.p, m, (uint8_t*)c->vflag.p, (uint32_t*)c->queue.p};
-            const uint32_t W = 4;
-            RRG_LAUNCH(k_verify_heavy, persistent_blocks(c, 4, m, W), W * 32, W * sizeof(FindSmem), c->stream, H);
-            LAUNCHED(c);
-            std::vector<uint8_t> ok(m);
-            CK(cudaMemcpyAsync(ok.data(), c->vflag.p, m, cudaMemcpyDeviceToHost, c->stream));
-            CK(cudaStreamSynchronize(c->stream));
-            for (uint32_t i = 0; i < m; i++)
-                if (ok[i]) verified.push_back(surv[i]);
-            std::sort(verified.begin(), verified.end());
-        }
-    }
+    // candidates (prefilter + precode), then light-verify survivors, then the
+    // heavy check; counts stay on the device between the three kernels
+    const uint32_t cap = (uint32_t)std::min<uint64_t>(blen / 64 + 65536, 1ull << 28);
+    const uint32_t cap2 = std::max<uint32_t>(cap / 16, 65536);
+    CK(dgrow(c->cand, (size_t)cap * 8 + (size_t)cap2 * 8));
+    CK(dgrow(c->ncand, 64));
+    CK(dgrow(c->vflag, cap2));
+    CK(cudaMemsetAsync(c->ncand.p, 0, 64, c->stream));
+    uint64_t* cand = (uint64_t*)c->cand.p;
+    uint64_t* surv = cand + cap;
+    uint32_t* counts = (uint32_t*)c->ncand.p;  // [0] candidates, [1] survivors, [2] heavy queue
+    ScanArgs S{body, blen, cand, counts, cap};
+    const uint64_t tiles = (blen + 16 + SCAN_TILE - 1) / SCAN_TILE;
+    RRG_LAUNCH(k_scan_candidates, (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(tiles, (uint64_t)c->n_sm * 8)),
+               SCAN_THREADS, 0, c->stream, S);
+    LAUNCHED(c);
+    VerifyArgs V{body, blen, cand, counts, cap, surv, counts + 1, cap2, nullptr, nullptr};
+    RRG_LAUNCH(k_verify_light, c->n_sm * 8, 256, 0, c->stream, V);
+    LAUNCHED(c);
+    VerifyArgs H{body, blen, surv, counts + 1, cap2, nullptr, nullptr, 0, (uint8_t*)c->vflag.p, counts + 2};
+    const uint32_t W = 4;
+    RRG_LAUNCH(k_verify_heavy, c->n_sm * 4, W * 32, W * sizeof(FindSmem), c->stream, H);
+    LAUNCHED(c);
     kt.stop();
+    uint32_t cnt[2] = {0, 0};
+    CK(cudaMemcpyAsync(cnt, counts, 8, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    if (cnt[0] > cap || cnt[1] > cap2) {
+        set_err(err, RRG_ERR_OUT_OF_MEMORY, "boundary scan: %u candidates exceed the list", cnt[0]);
+        return RRG_ERR_OUT_OF_MEMORY;
+    }
+    const uint32_t m = cnt[1];
+    std::vector<uint64_t> sv(m);
+    std::vector<uint8_t> ok(m);
+    if (m) {
+        CK(cudaMemcpyAsync(sv.data(), surv, (size_t)m * 8, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(ok.data(), c->vflag.p, m, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    for (uint32_t i = 0; i < m; i++)
+        if (ok[i]) verified.push_back(sv[i]);
+    std::sort(verified.begin(), verified.end());
     c->st.finder_ms += kt.ms();
     return 0;
 }

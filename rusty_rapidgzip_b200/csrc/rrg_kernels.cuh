@@ -241,8 +241,7 @@ struct WarpSmem {
     uint32_t lit_lut[LUT_SIZE];
     uint32_t dist_lut[LUT_SIZE];
     uint32_t pre_lut[1 << PRE_BITS];
-    uint32_t ent[NB];
-    uint32_t epos[NB];
+    uint2 ep[NB];  // per batch symbol: x = entry (literal flag|byte, or dist<<9|length), y = output offset
     uint16_t lit_sorted[288];
     uint16_t dist_sorted[32];
     uint16_t pre_sorted[32];
@@ -292,11 +291,11 @@ __device__ __forceinline__ Table pre_table(WarpSmem& S) {
     return Table{S.pre_lut, S.pre_sorted, S.pre_first, S.pre_count, S.pre_off};
 }
 
-__device__ __forceinline__ int find_entry(const uint32_t* epos, int n, uint32_t j) {
+__device__ __forceinline__ int find_entry(const uint2* ep, int n, uint32_t j) {
     int lo = 0, hi = n - 1;
     while (lo < hi) {
         int mid = (lo + hi + 1) >> 1;
-        if (epos[mid] <= j) lo = mid;
+        if (ep[mid].y <= j) lo = mid;
         else hi = mid - 1;
     }
     return lo;
@@ -469,7 +468,88 @@ __device__ void decode_codes(WarpSmem& S, ItemState& st, CellT* out, int lane) {
         if (lane == 0) {
             uint64_t room = st.counting ? ~0ull : (st.cap > st.cur ? st.cap - st.cur : 0);
             BR b = st.br;
-            while (n < NB) {
+            // Fast path: the batch surely fits the slot (<= NB * 258 cells) and every
+            // word it can load (a batch consumes <= NB * 48 bits) lies inside the input.
+            const bool fast = room >= (uint64_t)NB * 258 && (b.nw + 56) * 4 <= b.s.hi && b.nw * 4 >= b.s.lo;
+            if (fast) {
+                const uint32_t* base_w = reinterpret_cast<const uint32_t*>(b.s.base);
+                const uint32_t* wp = base_w + b.nw;
+                uint64_t buf = b.buf;
+                uint32_t bits = b.bits;
+                while (n < NB) {
+                    if (bits <= 32) {
+                        buf |= (uint64_t)__ldg(wp) << bits;
+                        wp++;
+                        bits += 32;
+                    }
+                    uint32_t e = S.lit_lut[buf & (LUT_SIZE - 1)];
+                    uint32_t cl = e & 15;
+                    if (!cl) {
+                        e = long_decode(buf, LT, LUT_BITS, TK_LITLEN);
+                        cl = e & 15;
+                        if (!cl) {
+                            status = DS_INVALID;
+                            msg = MSG_NO_CODE;
+                            break;
+                        }
+                    }
+                    const uint32_t kind = (e >> 4) & 3;
+                    if (kind == 0) {
+                        buf >>= cl;
+                        bits -= cl;
+                        S.ep[n] = make_uint2(0x80000000u | (e >> 16), pos);
+                        pos += 1;
+                        n++;
+                    } else if (kind == 1) {
+                        const uint32_t ex = (e >> 8) & 15;
+                        const uint32_t length = (e >> 16) + ((uint32_t)(buf >> cl) & ((1u << ex) - 1u));
+                        buf >>= cl + ex;
+                        bits -= cl + ex;
+                        if (bits <= 32) {
+                            buf |= (uint64_t)__ldg(wp) << bits;
+                            wp++;
+                            bits += 32;
+                        }
+                        uint32_t de = S.dist_lut[buf & (LUT_SIZE - 1)];
+                        uint32_t dl = de & 15;
+                        if (!dl) {
+                            de = long_decode(buf, DT, LUT_BITS, TK_DIST);
+                            dl = de & 15;
+                            if (!dl) {
+                                status = DS_INVALID;
+                                msg = MSG_NO_CODE;
+                                break;
+                            }
+                        }
+                        if (((de >> 4) & 3) == 3) {
+                            status = DS_INVALID;
+                            msg = MSG_DIST_RANGE;
+                            break;
+                        }
+                        const uint32_t dx = (de >> 8) & 15;
+                        const uint32_t dist = (de >> 16) + ((uint32_t)(buf >> dl) & ((1u << dx) - 1u));
+                        buf >>= dl + dx;
+                        bits -= dl + dx;
+                        S.ep[n] = make_uint2((dist << 9) | length, pos);
+                        pos += length;
+                        n++;
+                    } else if (kind == 2) {
+                        buf >>= cl;
+                        bits -= cl;
+                        stop = 1;
+                        break;
+                    } else {
+                        status = DS_INVALID;
+                        msg = MSG_LITLEN_RANGE;
+                        break;
+                    }
+                }
+                b.nw = (uint64_t)(wp - base_w);
+                b.buf = buf;
+                b.bits = bits;
+                if (!status && br_past_end(b)) status = DS_EOF;
+            }
+            while (!fast && n < NB) {
                 const BR save = b;
                 br_refill(b);
                 uint32_t e = S.lit_lut[b.buf & (LUT_SIZE - 1)];
@@ -491,8 +571,7 @@ __device__ void decode_codes(WarpSmem& S, ItemState& st, CellT* out, int lane) {
                         break;
                     }
                     br_consume(b, cl);
-                    S.ent[n] = 0x80000000u | (e >> 16);
-                    S.epos[n] = pos;
+                    S.ep[n] = make_uint2(0x80000000u | (e >> 16), pos);
                     pos += 1;
                     n++;
                 } else if (kind == 1) {
@@ -524,8 +603,7 @@ __device__ void decode_codes(WarpSmem& S, ItemState& st, CellT* out, int lane) {
                     uint32_t dx = (de >> 8) & 15;
                     uint32_t dist = (de >> 16) + ((uint32_t)(b.buf >> dl) & ((1u << dx) - 1u));
                     br_consume(b, dl + dx);
-                    S.ent[n] = (dist << 9) | length;
-                    S.epos[n] = pos;
+                    S.ep[n] = make_uint2((dist << 9) | length, pos);
                     pos += length;
                     n++;
                 } else if (kind == 2) {
@@ -554,21 +632,22 @@ __device__ void decode_codes(WarpSmem& S, ItemState& st, CellT* out, int lane) {
             uint32_t bad = 0, mk = 0;
             const uint64_t cur = st.cur;
             for (uint32_t j = lane; j < pos; j += 32) {
-                int k = find_entry(S.epos, n, j);
+                int k = find_entry(S.ep, n, j);
                 uint32_t jj = j, cell = 0;
                 for (;;) {
-                    uint32_t e = S.ent[k];
+                    uint32_t e = S.ep[k].x;
                     if (e & 0x80000000u) {
                         cell = e & 0xffu;
                         break;
                     }
                     uint32_t d = e >> 9;
-                    uint32_t t = jj - S.epos[k];
+                    const uint32_t ek = S.ep[k].y;
+                    uint32_t t = jj - ek;
                     if (t >= d) t %= d;
-                    int64_t src = (int64_t)S.epos[k] - (int64_t)d + (int64_t)t;
+                    int64_t src = (int64_t)ek - (int64_t)d + (int64_t)t;
                     if (src >= 0) {
                         jj = (uint32_t)src;
-                        k = find_entry(S.epos, k, jj);
+                        k = find_entry(S.ep, k, jj);
                         continue;
                     }
                     int64_t a = (int64_t)cur + src;
@@ -800,8 +879,9 @@ __device__ void inflate_item(WarpSmem& S, const InflateArgs& A, uint32_t item_id
     __syncwarp();
 }
 
+// 128 threads (4 warps) per block, >= 5 blocks per SM: 20 decoding warps per SM
 template <typename CellT>
-__global__ void k_inflate(InflateArgs A) {
+__global__ void __launch_bounds__(128, 5) k_inflate(InflateArgs A) {
     RRG_DYN_SMEM(smem_raw);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     WarpSmem& S = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
@@ -1718,8 +1798,12 @@ struct VerifyArgs {
     const uint8_t* body;
     uint64_t body_len;
     const uint64_t* cand;
-    uint32_t n;
-    uint8_t* light_ok;  // per candidate
+    const uint32_t* n_ptr;  // number of candidates (device word written by the previous kernel)
+    uint32_t cap;           // entries of `cand` that exist
+    uint64_t* out;          // survivors, appended
+    uint32_t* n_out;
+    uint32_t out_cap;
+    uint8_t* ok;            // k_verify_heavy: per-survivor verdict
     uint32_t* queue;
 };
 
@@ -1809,11 +1893,18 @@ __device__ bool verify_light(const Src& s, uint64_t total_bits, uint64_t pos) {
     return true;
 }
 
+// Survivors are appended to A.out (order is restored on the host).
 __global__ void __launch_bounds__(256) k_verify_light(VerifyArgs A) {
     const Src s = make_src(A.body, A.body_len);
     const uint64_t total_bits = A.body_len * 8;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x)
-        A.light_ok[i] = verify_light(s, total_bits, A.cand[i]) ? 1 : 0;
+    const uint32_t n = *A.n_ptr < A.cap ? *A.n_ptr : A.cap;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint64_t pos = A.cand[i];
+        if (verify_light(s, total_bits, pos)) {
+            const uint32_t slot = atomicAdd(A.n_out, 1u);
+            if (slot < A.out_cap) A.out[slot] = pos;
+        }
+    }
 }
 
 // One warp per light survivor: tables + 64 trial symbols (verify_heavy).
@@ -1823,13 +1914,14 @@ __global__ void __launch_bounds__(128) k_verify_heavy(VerifyArgs A) {
     FindSmem& S = reinterpret_cast<FindSmem*>(smem_raw)[warp];
     const Src s = make_src(A.body, A.body_len);
     const uint64_t total_bits = A.body_len * 8;
+    const uint32_t n = *A.n_ptr < A.cap ? *A.n_ptr : A.cap;
     for (;;) {
         uint32_t idx = 0;
         if (lane == 0) idx = atomicAdd(A.queue, 1u);
         idx = (uint32_t)bcast32((int32_t)idx);
-        if (idx >= A.n) break;
+        if (idx >= n) break;
         const bool ok = verify_heavy(S, s, total_bits, A.cand[idx], lane);
-        if (lane == 0) A.light_ok[idx] = ok ? 1 : 0;
+        if (lane == 0) A.ok[idx] = ok ? 1 : 0;
         __syncwarp();
     }
 }

@@ -31,12 +31,13 @@ struct dim3 {
     unsigned x = 1, y = 1, z = 1;
     dim3(unsigned a = 1, unsigned b = 1, unsigned c = 1) : x(a), y(b), z(c) {}
 };
-struct uint2 {
+struct __attribute__((aligned(8))) uint2 {
     unsigned x, y;
 };
 struct __attribute__((aligned(16))) uint4 {
     unsigned x, y, z, w;
 };
+inline uint2 make_uint2(unsigned x, unsigned y) { return uint2{x, y}; }
 
 typedef int cudaError_t;
 typedef void* cudaStream_t;
