@@ -1709,7 +1709,7 @@ __global__ void __launch_bounds__(128) k_find_blocks(FindArgs A) {
 // the last survivors get verify_heavy (tables + 64 trial symbols).
 constexpr int SCAN_THREADS = 256;
 constexpr int SCAN_TILE = SCAN_THREADS * 16;
-constexpr int SCAN_HALO = 32;
+constexpr int SCAN_HALO = 48;  // the last thread reads up to 2.5 words past its 16 bytes
 
 struct ScanArgs {
     const uint8_t* body;
@@ -1719,13 +1719,18 @@ struct ScanArgs {
     uint32_t cap;
 };
 
+// 32 bits of the staged tile starting at bit b (b + 32 <= 8 * tile bytes)
+__device__ __forceinline__ uint32_t tile_bits(const uint32_t* tw, uint32_t b) {
+    const uint32_t q = b >> 5, r = b & 31;
+    return __funnelshift_r(tw[q], tw[q + 1], r);
+}
+
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_candidates(ScanArgs A) {
     __shared__ __align__(16) uint32_t tile[(SCAN_TILE + SCAN_HALO) / 4];
     const uintptr_t addr = (uintptr_t)A.body;
     const uint8_t* base = (const uint8_t*)(addr & ~(uintptr_t)15);
     const uint64_t lo = addr & 15, hi = lo + A.body_len;
     const uint64_t n_tiles = (hi + SCAN_TILE - 1) / SCAN_TILE;
-    const int lane = threadIdx.x & 31;
     uint8_t* tb = reinterpret_cast<uint8_t*>(tile);
     for (uint64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
         const uint64_t t0 = t * SCAN_TILE;
@@ -1741,52 +1746,51 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_candidates(ScanArgs A) {
             }
         }
         __syncthreads();
-        uint32_t W[7];
-        for (int q = 0; q < 7; q++) W[q] = tile[threadIdx.x * 4 + q];
-        const uint64_t first_bit = (t0 + 16ull * threadIdx.x) * 8;  // relative to base
-        for (uint32_t i = 0; i < 128; i++) {
-            const uint64_t pa = first_bit + i;
-            bool pass = false;
-            if (pa >= lo * 8 && pa + 13 <= hi * 8) {
-                const uint32_t q = i >> 5, r = i & 31;
-                auto bits = [&](uint32_t off) -> uint32_t {
-                    const uint32_t b = i + off, qq = b >> 5, rr = b & 31;
-                    uint32_t l = 0, h = 0;
+        // phase 1: prefilter every offset of this thread's 16 bytes (4 groups of 32)
+        const uint64_t tile_bit0 = t0 * 8;
+        const uint32_t w0 = threadIdx.x * 4;
+        uint32_t mask[4];
 #pragma unroll
-                    for (int z = 0; z < 6; z++) {
-                        if ((uint32_t)z == qq) {
-                            l = W[z];
-                            h = W[z + 1];
-                        }
-                    }
-                    return rr ? ((l >> rr) | (h << (32 - rr))) : l;
-                };
-                (void)q;
-                (void)r;
-                const uint32_t w = bits(0) & 0x1fffu;
-                if ((w & 7u) == 4u && ((w >> 3) & 31u) <= 29u && ((w >> 8) & 31u) <= 29u) {
-                    const uint32_t hclen = (bits(13) & 15u) + 4;
-                    const uint32_t y = bits(17), z = bits(47);
-                    uint32_t kraft = 0, nsym = 0;
+        for (int q = 0; q < 4; q++) {
+            const uint32_t a = tile[w0 + q], b = tile[w0 + q + 1];
+            uint32_t m = 0;
 #pragma unroll
-                    for (uint32_t j = 0; j < 19; j++) {
-                        const uint32_t l = j < 10 ? (y >> (3 * j)) & 7u : (z >> (3 * (j - 10))) & 7u;
-                        if (j < hclen && l) {
-                            kraft += 128u >> l;
-                            nsym++;
-                        }
-                    }
-                    pass = nsym < 2 || kraft == 128u;
+            for (int r = 0; r < 32; r++) {
+                const uint32_t w = __funnelshift_r(a, b, r);
+                const bool c = (w & 7u) == 4u && ((w >> 3) & 31u) <= 29u && ((w >> 8) & 31u) <= 29u;
+                m |= (c ? 1u : 0u) << r;
+            }
+            // only offsets p with lo*8 <= p and p + 13 <= hi*8 are tested
+            const uint64_t g0 = tile_bit0 + 32ull * (w0 + q);
+            if (g0 < lo * 8 || g0 + 32 + 13 > hi * 8) {
+                for (int r = 0; r < 32; r++) {
+                    const uint64_t pa = g0 + r;
+                    if (pa < lo * 8 || pa + 13 > hi * 8) m &= ~(1u << r);
                 }
             }
-            const unsigned m = __ballot_sync(FULLMASK, pass);
-            if (m) {
-                uint32_t base_slot = 0;
-                if (lane == __ffs(m) - 1) base_slot = atomicAdd(A.n_cand, (uint32_t)__popc(m));
-                base_slot = __shfl_sync(FULLMASK, base_slot, __ffs(m) - 1);
-                if (pass) {
-                    const uint32_t slot = base_slot + __popc(m & ((1u << lane) - 1u));
-                    if (slot < A.cap) A.cand[slot] = pa - lo * 8;
+            mask[q] = m;
+        }
+        // phase 2: strict precode Kraft test of each candidate
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            uint32_t m = mask[q];
+            while (m) {
+                const uint32_t r = __ffs(m) - 1;
+                m &= m - 1;
+                const uint32_t boff = 32 * (w0 + q) + r;  // bit offset inside the tile
+                const uint32_t hclen = (tile_bits(tile, boff + 13) & 15u) + 4;
+                const uint32_t y = tile_bits(tile, boff + 17), z = tile_bits(tile, boff + 47);
+                uint32_t kraft = 0, nsym = 0;
+#pragma unroll
+                for (uint32_t j = 0; j < 19; j++) {
+                    const uint32_t l = j < 10 ? (y >> (3 * j)) & 7u : (z >> (3 * (j - 10))) & 7u;
+                    const bool use = j < hclen && l;
+                    kraft += use ? (128u >> l) : 0u;
+                    nsym += use ? 1u : 0u;
+                }
+                if (nsym < 2 || kraft == 128u) {
+                    const uint32_t slot = atomicAdd(A.n_cand, 1u);
+                    if (slot < A.cap) A.cand[slot] = tile_bit0 + boff - lo * 8;
                 }
             }
         }

@@ -156,6 +156,10 @@ inline unsigned __match_any_sync(unsigned, unsigned v) {
 }
 inline int __popc(unsigned v) { return __builtin_popcount(v); }
 inline int __ffs(int v) { return __builtin_ffs(v); }
+inline unsigned __funnelshift_r(unsigned lo, unsigned hi, unsigned sh) {
+    sh &= 31;
+    return sh ? (lo >> sh) | (hi << (32 - sh)) : lo;
+}
 inline unsigned __brev(unsigned v) {
     unsigned r = 0;
     for (int i = 0; i < 32; i++) r |= ((v >> i) & 1u) << (31 - i);
