@@ -284,7 +284,7 @@ def run_ours(args, raw, gz, desc):
                            l2="inputs (compressed + output) larger than L2; no flush",
                            gpu_chunk_bytes=args.gpu_chunk or "auto", gpu_chunks=ms.gpu_chunks,
                            inflate="lane-per-chunk" if args.warps_per_stream < 0 else "warp-per-chunk",
-                           boundaries="every offset" if args.boundary_mode == 2 else "per target",
+                           boundaries="per target" if args.boundary_mode == 1 else "every offset",
                            markers=ms.markers, speculation_failures=ms.speculation_failures),
             "e2e": {"value": round(e2e_value, 3), "unit": "GB/s", "h2d_bytes_per_step": C_,
                     "d2h_bytes_per_step": U_},
@@ -312,7 +312,7 @@ def main():
     ap.add_argument("--size", type=int, default=None)
     ap.add_argument("--gpu-chunk", type=int, default=0)
     ap.add_argument("--warps-per-stream", type=int, default=0, help="-1: one decoder per lane")
-    ap.add_argument("--boundary-mode", type=int, default=0, help="2: test every bit offset")
+    ap.add_argument("--boundary-mode", type=int, default=0, help="1: one finder search per target")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

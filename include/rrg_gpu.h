@@ -75,8 +75,9 @@ typedef struct rrg_config {
     uint64_t gpu_chunk_bytes;    /* speculative sub-chunk size on the GPU; 0 = autotuned */
     uint64_t finder_tile_bits;   /* block-finder tile width in bits; 0 = autotuned */
     int32_t warps_per_stream;    /* 0 or 1 = one chunk per warp; -1 = one decoder per lane (32 chunks per warp) */
-    int32_t boundary_mode;       /* 0 or 1 = one search per target as find_next_dynamic_block does
-                                    (block_finder.rs:109); 2 = test every bit offset of the body */
+    int32_t boundary_mode;       /* 0 = test every bit offset of the body and keep verified block starts
+                                    >= gpu_chunk_bytes apart; 1 = one search per target as
+                                    find_next_dynamic_block does (block_finder.rs:109) */
     uint64_t hbm_budget_bytes;   /* serving admission budget; 0 = 120 GB */
 } rrg_config;
 

@@ -236,7 +236,7 @@ struct rrg_ctx {
     // tunables
     uint64_t gpu_chunk = 0;
     bool lanes = false;        // lane-per-chunk inflate (default: one chunk per warp)
-    bool scan_bounds = false;  // full-stream boundary scan (default: one finder search per target)
+    bool scan_bounds = true;   // full-stream boundary scan (boundary_mode 1: one finder search per target)
     uint32_t inflate_warps = 4;
     uint32_t finder_tile = 1024;
     double expand = 6.0;
@@ -1122,7 +1122,7 @@ rrg_ctx* rrg_gpu_create(const rrg_config* cfg, rrg_error* err) {
     cudaFuncSetAttribute(k_inflate_lanes<uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(LANE_THREADS * sizeof(LaneTab)));
     if (c->cfg.warps_per_stream < 0) c->lanes = true;  // -1: one decoder per lane (32 chunks per warp)
-    if (c->cfg.boundary_mode == 2) c->scan_bounds = true;
+    if (c->cfg.boundary_mode == 1) c->scan_bounds = false;
     if (smem_optin > 0 && want > 48 * 1024) {
         cudaFuncSetAttribute(k_inflate<uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)want);
         cudaFuncSetAttribute(k_inflate<uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)want);

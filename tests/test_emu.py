@@ -30,8 +30,8 @@ def test_small_golden(emu_decoder_factory, name):
     assert sha256(out) == meta["sha256"]
 
 
-@pytest.mark.parametrize("mode", [dict(), dict(warps_per_stream=-1), dict(boundary_mode=2)],
-                         ids=["warps-targets", "lanes-targets", "warps-scan"])
+@pytest.mark.parametrize("mode", [dict(), dict(warps_per_stream=-1), dict(boundary_mode=1)],
+                         ids=["warps-scan", "lanes-scan", "warps-targets"])
 def test_multi_chunk_speculative(emu_decoder_factory, mode):
     raw, gz = W.config1(192 << 10, seed=3)
     d = emu_decoder_factory(gpu_chunk_bytes=8192, **mode)

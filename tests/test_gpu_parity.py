@@ -50,8 +50,8 @@ def test_raw_deflate_vectors(gpu_decoder_factory):
         assert d.decompress(gz) == plain, v["name"]
 
 
-MODES = [dict(), dict(warps_per_stream=-1), dict(boundary_mode=2), dict(warps_per_stream=-1, boundary_mode=2)]
-MODE_IDS = ["warps-targets", "lanes-targets", "warps-scan", "lanes-scan"]
+MODES = [dict(), dict(warps_per_stream=-1), dict(boundary_mode=1), dict(warps_per_stream=-1, boundary_mode=1)]
+MODE_IDS = ["warps-scan", "lanes-scan", "warps-targets", "lanes-targets"]
 
 
 @pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
