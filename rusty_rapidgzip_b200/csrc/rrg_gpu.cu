@@ -240,6 +240,7 @@ struct rrg_ctx {
     uint32_t inflate_warps = 4;
     uint32_t finder_tile = 1024;
     double expand = 6.0;
+    uint64_t slots = 0;        // resident decoders of one inflate wave (lazy)
 
     rrg_stats st{};
     uint64_t launches = 0;
@@ -423,9 +424,14 @@ struct MemberSpan {
     uint64_t trailer_byte;
 };
 
-int check_members(rrg_ctx* c, const uint8_t* d_out, const std::vector<MemberSpan>& ms, uint32_t member_base,
-                  rrg_error* err) {
+// CRC32/ISIZE of every span on the device; per-span status (DS_OK, DS_CRC,
+// DS_ISIZE), computed CRC and length come back in stv/got/glen.
+int crc_spans(rrg_ctx* c, const uint8_t* d_out, const std::vector<MemberSpan>& ms, std::vector<int32_t>& stv,
+              std::vector<uint32_t>& got, std::vector<uint64_t>& glen, rrg_error* err) {
     const uint32_t nm = (uint32_t)ms.size();
+    stv.assign(nm, 0);
+    got.assign(nm, 0);
+    glen.assign(nm, 0);
     if (!nm) return 0;
     const uint64_t PIECE = 256 * 1024;
     std::vector<CrcPiece> pieces;
@@ -440,7 +446,6 @@ int check_members(rrg_ctx* c, const uint8_t* d_out, const std::vector<MemberSpan
     }
     mstart[nm] = (uint32_t)pieces.size();
     const uint32_t np = (uint32_t)pieces.size();
-    double t0 = now_ms();
     CK(dgrow(c->pieces, std::max<size_t>(np, 1) * sizeof(CrcPiece)));
     CK(dgrow(c->piece_crc, std::max<size_t>(np, 1) * 4));
     CK(dgrow(c->mpiece, (nm + 1) * 4));
@@ -466,42 +471,50 @@ int check_members(rrg_ctx* c, const uint8_t* d_out, const std::vector<MemberSpan
     RRG_LAUNCH(k_crc_members, (nm * 32 + 255) / 256, 256, 0, c->stream, B);
     kt.stop();
     LAUNCHED(c);
-    std::vector<int32_t> stv(nm);
-    std::vector<uint32_t> got(nm);
-    std::vector<uint64_t> glen(nm);
     CK(cudaMemcpyAsync(stv.data(), c->mstatus.p, nm * 4, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpyAsync(got.data(), c->got_crc.p, nm * 4, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpyAsync(glen.data(), c->got_len.p, nm * 8, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     c->st.crc_ms += kt.ms();
-    (void)t0;
     c->st.members += nm;
-    for (uint32_t m = 0; m < nm; m++) {
-        if (stv[m] == DS_CRC) {
-            set_err(err, RRG_ERR_CRC_MISMATCH,
-                    "CRC32 mismatch in member #%u (uncompressed bytes: %llu, trailer at byte %llu): expected "
-                    "%#010x, got %#010x",
-                    member_base + m, (unsigned long long)glen[m], (unsigned long long)ms[m].trailer_byte,
-                    ms[m].crc, got[m]);
-            err->member = member_base + m;
-            err->expected = ms[m].crc;
-            err->got_crc = got[m];
-            err->uncompressed = glen[m];
-            err->trailer_byte = ms[m].trailer_byte;
-            return RRG_ERR_CRC_MISMATCH;
-        }
-        if (stv[m] == DS_ISIZE) {
-            set_err(err, RRG_ERR_ISIZE_MISMATCH,
-                    "ISIZE mismatch in member #%u (trailer at byte %llu): expected %u, got %llu", member_base + m,
-                    (unsigned long long)ms[m].trailer_byte, ms[m].isize, (unsigned long long)glen[m]);
-            err->member = member_base + m;
-            err->expected = ms[m].isize;
-            err->got = glen[m];
-            err->uncompressed = glen[m];
-            err->trailer_byte = ms[m].trailer_byte;
-            return RRG_ERR_ISIZE_MISMATCH;
-        }
+    return 0;
+}
+
+// GzipError::{CrcMismatch, IsizeMismatch} for one member (gzip.rs:26-60).
+int member_error(rrg_error* err, const MemberSpan& m, uint32_t member, int32_t st, uint32_t got, uint64_t glen) {
+    if (st == DS_CRC) {
+        set_err(err, RRG_ERR_CRC_MISMATCH,
+                "CRC32 mismatch in member #%u (uncompressed bytes: %llu, trailer at byte %llu): expected "
+                "%#010x, got %#010x",
+                member, (unsigned long long)glen, (unsigned long long)m.trailer_byte, m.crc, got);
+        err->member = member;
+        err->expected = m.crc;
+        err->got_crc = got;
+        err->uncompressed = glen;
+        err->trailer_byte = m.trailer_byte;
+        return RRG_ERR_CRC_MISMATCH;
     }
+    set_err(err, RRG_ERR_ISIZE_MISMATCH, "ISIZE mismatch in member #%u (trailer at byte %llu): expected %u, got %llu",
+            member, (unsigned long long)m.trailer_byte, m.isize, (unsigned long long)glen);
+    err->member = member;
+    err->expected = m.isize;
+    err->got = glen;
+    err->uncompressed = glen;
+    err->trailer_byte = m.trailer_byte;
+    return RRG_ERR_ISIZE_MISMATCH;
+}
+
+// All spans of one stream: the first failing member is the error.
+int check_members(rrg_ctx* c, const uint8_t* d_out, const std::vector<MemberSpan>& ms, uint32_t member_base,
+                  rrg_error* err) {
+    std::vector<int32_t> stv;
+    std::vector<uint32_t> got;
+    std::vector<uint64_t> glen;
+    int rc = crc_spans(c, d_out, ms, stv, got, glen, err);
+    if (rc) return rc;
+    for (size_t m = 0; m < ms.size(); m++)
+        if (stv[m] == DS_CRC || stv[m] == DS_ISIZE)
+            return member_error(err, ms[m], member_base + (uint32_t)m, stv[m], got[m], glen[m]);
     return 0;
 }
 
@@ -538,7 +551,7 @@ int ensure_out(rrg_ctx* c, OutTarget& t, uint64_t need, uint64_t keep, rrg_error
 // ------------------------------------------------------------ resolve
 // Windows (init + chase), then cells -> bytes. Returns 0 or an error code.
 int run_resolve(rrg_ctx* c, const std::vector<ResolveChunk>& rchunks, const std::vector<uint64_t>& tile_start,
-                uint8_t* d_dst, rrg_error* err) {
+                uint8_t* d_dst, rrg_error* err, int64_t* bad_chunk = nullptr) {
     const uint32_t nc = (uint32_t)rchunks.size();
     if (!nc) return 0;
     CK(dgrow(c->chunks, nc * sizeof(ResolveChunk)));
@@ -572,6 +585,7 @@ int run_resolve(rrg_ctx* c, const std::vector<ResolveChunk>& rchunks, const std:
     c->st.resolve_ms += kt.ms();
     c->st.markers += nmk;
     if (e4[0]) {
+        if (bad_chunk) *bad_chunk = e4[1];
         set_err(err, RRG_ERR_DEFLATE_INVALID, "%s", msg_text(MSG_MARKER_WINDOW));
         return RRG_ERR_DEFLATE_INVALID;
     }
@@ -632,96 +646,211 @@ int scan_boundaries(rrg_ctx* c, const uint8_t* body, uint64_t blen, std::vector<
 }
 
 // ------------------------------------------------------------ member route
+// Decoders resident at once on the device: warps (or lanes) of one full wave
+// of the inflate kernel.
+uint64_t inflate_slots(rrg_ctx* c) {
+    if (!c->slots) {
+        int occ = 0;
+        if (c->lanes) {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_inflate_lanes<uint16_t>, LANE_THREADS,
+                                                          LANE_THREADS * sizeof(LaneTab));
+            c->slots = (uint64_t)c->n_sm * std::max(occ, 1) * LANE_THREADS;
+        } else {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_inflate<uint16_t>, c->inflate_warps * 32,
+                                                          c->inflate_warps * sizeof(WarpSmem));
+            c->slots = (uint64_t)c->n_sm * std::max(occ, 1) * c->inflate_warps;
+        }
+    }
+    return c->slots;
+}
+
 struct Decoded {
-    uint64_t total = 0;  // bytes written at d_dst
+    uint64_t total = 0;  // bytes written at the job's destination
     uint64_t consumed = 0;
     uint32_t members = 0;
 };
 
 uint64_t round8(uint64_t v) { return (v + 7) & ~7ull; }
 
-// Decodes the gzip member stream whose first member body starts at byte
-// `body_off` of d_file (the first member's header already parsed) into
-// tgt.p[dst_off ..]. On RRG_ERR_CAPACITY `out->total` holds the size required.
-int member_route(rrg_ctx* c, const uint8_t* d_file, uint64_t len, uint64_t body_off, OutTarget& tgt, uint64_t dst_off,
-                 uint32_t member_base, Decoded* out, rrg_error* err) {
-    const uint8_t* body = d_file + body_off;
-    const uint64_t blen = len - body_off;
-    const uint64_t total_bits = blen * 8;
-    const uint64_t G = std::max<uint64_t>(c->gpu_chunk ? c->gpu_chunk : (c->lanes ? (1ull << 14) : (1ull << 17)), 4096);
-    std::vector<uint64_t> starts{0};
+// One gzip member stream (a file, or what follows a BGZF prefix) for the
+// member route. Several jobs share every kernel launch.
+struct MemberJob {
+    uint64_t file_off = 0;    // the file's first byte in the base buffer
+    uint64_t len = 0;         // file bytes from file_off
+    uint64_t body_off = 0;    // first member's deflate body, relative to file_off
+    uint64_t dst_off = 0;     // first output byte in the target
+    uint64_t dst_cap = ~0ull; // output bytes available at dst_off (~0: the target grows)
+    uint32_t member_base = 0; // index of the first member, for error reports
+    // results
+    int rc = 0;
+    rrg_error err{};
+    Decoded out;
+};
+
+namespace mr {
+struct Acc {
+    ChunkItem it;
+    ChunkResult r;
+    std::vector<MemberRec> m;
+};
+struct JobState {
+    size_t first = 0, n = 0;  // the job's initial items
+    size_t k = 0;             // next initial item to chain
+    uint64_t expected = 0;
+    bool final_seen = false, done = false;
+    std::vector<Acc> acc;
+    std::vector<size_t> overflow;  // indices into acc
+    int64_t pending = -1;          // index into the current re-decode list
+};
+}  // namespace mr
+
+// Decodes every job's member stream (pipeline.rs:468-1041 per job) with one
+// boundary search, one inflate launch (plus rare re-decode launches), one
+// resolve and one CRC pass for all of them. A failing job gets its own
+// rc/err and leaves the others untouched; the return value is non-zero only
+// for failures of the whole batch (device errors, allocation).
+int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& jobs, OutTarget& tgt, rrg_error* err) {
+    using namespace mr;
+    const size_t nj = jobs.size();
+    // Sub-chunk spacing. A fixed gpu_chunk_bytes takes the first boundary at
+    // least that far from the previous one. Otherwise the compressed bytes of
+    // all jobs are spread over one wave of the inflate kernel's resident
+    // decoders: each job gets chunks in proportion to its size, and each
+    // boundary is the verified block start nearest its ideal position.
+    uint64_t total_c = 0;
+    for (const MemberJob& j : jobs) total_c += j.len - j.body_off;
+    const bool fixed_g = c->gpu_chunk != 0;
+    const uint64_t g_min = c->lanes ? (8ull << 10) : (32ull << 10);
+    const uint64_t slots = inflate_slots(c);
+    const uint64_t G = fixed_g ? std::max<uint64_t>(c->gpu_chunk, 4096)
+                               : std::max<uint64_t>(g_min, (total_c + slots - 1) / slots);
+    std::vector<std::vector<uint64_t>> starts(nj, std::vector<uint64_t>{0});
+    auto fail = [&](MemberJob& j, int st, int msg, uint64_t where) { j.rc = status_err(&j.err, st, msg, where); };
+    // ---- sub-chunk boundaries
     if (c->scan_bounds) {
-        // ---- sub-chunk boundaries: verified dynamic-block starts, at least G bytes apart
-        std::vector<uint64_t> verified;
-        int rc0 = scan_boundaries(c, body, blen, verified, err);
-        if (rc0) return rc0;
-        for (uint64_t v : verified)
-            if (v >= starts.back() + G * 8) starts.push_back(v);
+        // verified dynamic-block starts; the bodies are scanned in clusters of
+        // nearby ranges, one scan per cluster
+        std::vector<size_t> big;
+        for (size_t i = 0; i < nj; i++)
+            if (jobs[i].len - jobs[i].body_off > G) big.push_back(i);
+        std::sort(big.begin(), big.end(), [&](size_t a, size_t b) { return jobs[a].file_off < jobs[b].file_off; });
+        for (size_t a = 0; a < big.size();) {
+            uint64_t lo = jobs[big[a]].file_off + jobs[big[a]].body_off, hi = jobs[big[a]].file_off + jobs[big[a]].len;
+            size_t b = a + 1;
+            while (b < big.size() && jobs[big[b]].file_off + jobs[big[b]].body_off <= hi + (1u << 20)) {
+                hi = std::max(hi, jobs[big[b]].file_off + jobs[big[b]].len);
+                b++;
+            }
+            std::vector<uint64_t> verified;
+            int rc0 = scan_boundaries(c, d_base + lo, hi - lo, verified, err);
+            if (rc0) return rc0;
+            // verified offsets are sorted bit offsets from `lo`
+            for (size_t q = a; q < b; q++) {
+                MemberJob& j = jobs[big[q]];
+                const uint64_t b0 = (j.file_off + j.body_off - lo) * 8, b1 = (j.file_off + j.len - lo) * 8;
+                auto& st = starts[big[q]];
+                auto lo_it = std::lower_bound(verified.begin(), verified.end(), b0);
+                auto hi_it = std::lower_bound(lo_it, verified.end(), b1);
+                if (fixed_g) {
+                    for (auto it = lo_it; it != hi_it; ++it)
+                        if (*it - b0 >= st.back() + G * 8) st.push_back(*it - b0);
+                } else {
+                    const uint64_t nbits = b1 - b0;
+                    const uint64_t K = std::max<uint64_t>(1, (nbits / 8 + G / 2) / G);
+                    for (uint64_t k = 1; k < K; k++) {
+                        const uint64_t ideal = b0 + nbits * k / K;
+                        auto it = std::lower_bound(lo_it, hi_it, ideal);
+                        uint64_t best = ~0ull;
+                        if (it != hi_it) best = *it;
+                        if (it != lo_it && (best == ~0ull || ideal - *(it - 1) < best - ideal)) best = *(it - 1);
+                        if (best != ~0ull && best - b0 > st.back()) st.push_back(best - b0);
+                    }
+                }
+            }
+            a = b;
+        }
+    } else {
+        // first dynamic block at/after every G bytes (find_next_dynamic_block per target)
+        std::vector<uint64_t> targets, limits;
+        std::vector<size_t> owner;
+        for (size_t i = 0; i < nj; i++) {
+            const uint64_t base_bit = (jobs[i].file_off + jobs[i].body_off) * 8;
+            const uint64_t total_bits = (jobs[i].len - jobs[i].body_off) * 8;
+            const size_t t0 = targets.size();
+            for (uint64_t t = G * 8; t < total_bits; t += G * 8) {
+                targets.push_back(base_bit + t);
+                owner.push_back(i);
+            }
+            for (size_t q = t0; q < targets.size(); q++)
+                limits.push_back(q + 1 < targets.size() ? targets[q + 1] : base_bit + total_bits);
+        }
+        if (!targets.empty()) {
+            const uint32_t n = (uint32_t)targets.size();
+            std::vector<uint64_t> found(n, ~0ull);
+            uint64_t span_hi = 0;
+            for (const MemberJob& j : jobs) span_hi = std::max(span_hi, j.file_off + j.len);
+            CK(dgrow(c->targets, n * 8));
+            CK(dgrow(c->limits, n * 8));
+            CK(dgrow(c->found, n * 8));
+            CK(dgrow(c->queue, 16));
+            CK(cudaMemcpyAsync(c->targets.p, targets.data(), n * 8, cudaMemcpyHostToDevice, c->stream));
+            CK(cudaMemcpyAsync(c->limits.p, limits.data(), n * 8, cudaMemcpyHostToDevice, c->stream));
+            CK(cudaMemsetAsync(c->queue.p, 0, 16, c->stream));
+            FindArgs F{d_base, span_hi, (const uint64_t*)c->targets.p, (const uint64_t*)c->limits.p,
+                       (uint64_t*)c->found.p, n, (uint32_t*)c->queue.p, (const uint8_t*)c->next_lut.p, c->finder_tile};
+            const uint32_t W = 4;
+            uint32_t grid = persistent_blocks(c, 4, n, W);
+            KTimer kt(c->stream);
+            RRG_LAUNCH(k_find_blocks, grid, W * 32, W * sizeof(FindSmem), c->stream, F);
+            kt.stop();
+            LAUNCHED(c);
+            CK(cudaMemcpyAsync(found.data(), c->found.p, n * 8, cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaStreamSynchronize(c->stream));
+            c->st.finder_ms += kt.ms();
+            for (uint32_t q = 0; q < n; q++) {
+                const size_t i = owner[q];
+                const uint64_t base_bit = (jobs[i].file_off + jobs[i].body_off) * 8;
+                if (found[q] != ~0ull && found[q] - base_bit > starts[i].back()) starts[i].push_back(found[q] - base_bit);
+            }
+        }
     }
-    // ---- or: first dynamic block at/after every G bytes (find_next_dynamic_block per target)
-    std::vector<uint64_t> targets, limits, found;
-    if (!c->scan_bounds) {
-    for (uint64_t t = G * 8; t < total_bits; t += G * 8) targets.push_back(t);
-    for (size_t i = 0; i < targets.size(); i++) limits.push_back(i + 1 < targets.size() ? targets[i + 1] : total_bits);
-    found.assign(targets.size(), ~0ull);
-    if (!targets.empty()) {
-        const uint32_t n = (uint32_t)targets.size();
-        double t0 = now_ms();
-        CK(dgrow(c->targets, n * 8));
-        CK(dgrow(c->limits, n * 8));
-        CK(dgrow(c->found, n * 8));
-        CK(dgrow(c->queue, 16));
-        CK(cudaMemcpyAsync(c->targets.p, targets.data(), n * 8, cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(c->limits.p, limits.data(), n * 8, cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemsetAsync(c->queue.p, 0, 16, c->stream));
-        FindArgs F{body, blen, (const uint64_t*)c->targets.p, (const uint64_t*)c->limits.p, (uint64_t*)c->found.p, n,
-                   (uint32_t*)c->queue.p, (const uint8_t*)c->next_lut.p, c->finder_tile};
-        const uint32_t W = 4;
-        uint32_t grid = persistent_blocks(c, 4, n, W);
-        KTimer kt(c->stream);
-        RRG_LAUNCH(k_find_blocks, grid, W * 32, W * sizeof(FindSmem), c->stream, F);
-        kt.stop();
-        LAUNCHED(c);
-        CK(cudaMemcpyAsync(found.data(), c->found.p, n * 8, cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
-        c->st.finder_ms += kt.ms();
-        (void)t0;
-    }
-    for (uint64_t f : found)
-        if (f != ~0ull && f > starts.back()) starts.push_back(f);
-    }
-    const size_t n = starts.size();
-    // ---- slot arena: every chunk gets expand x its compressed span, plus room for re-decodes
-    std::vector<ChunkItem> items(n);
+    // ---- items and the slot arena: every chunk gets expand x its compressed span
+    std::vector<ChunkItem> items;
+    std::vector<JobState> js(nj);
     uint64_t arena = 0;
-    for (size_t k = 0; k < n; k++) {
-        ChunkItem& it = items[k];
-        it.in_off = body_off;
-        it.in_len = blen;
-        it.start_bit = starts[k];
-        it.end_hint = k + 1 < n ? starts[k + 1] : ~0ull;
-        uint64_t span = ((k + 1 < n ? starts[k + 1] : total_bits) - starts[k] + 7) / 8;
-        it.out_cap = round8((uint64_t)(span * c->expand) + 65536);
-        it.out_off = arena;
-        it.flags = ITEM_MARKERS;
-        it.id = (uint32_t)k;
-        arena += it.out_cap;
+    uint32_t next_id = 0;
+    for (size_t i = 0; i < nj; i++) {
+        const MemberJob& j = jobs[i];
+        const uint64_t blen = j.len - j.body_off, total_bits = blen * 8;
+        const auto& st = starts[i];
+        js[i].first = items.size();
+        js[i].n = st.size();
+        for (size_t k = 0; k < st.size(); k++) {
+            ChunkItem it;
+            it.in_off = j.file_off + j.body_off;
+            it.in_len = blen;
+            it.start_bit = st[k];
+            it.end_hint = k + 1 < st.size() ? st[k + 1] : ~0ull;
+            const uint64_t span = ((k + 1 < st.size() ? st[k + 1] : total_bits) - st[k] + 7) / 8;
+            it.out_cap = round8((uint64_t)(span * c->expand) + 65536);
+            it.out_off = arena;
+            // the first chunk too, as in the reference: a reference before the
+            // stream's start becomes a marker that fails to resolve
+            it.flags = ITEM_MARKERS;
+            it.id = next_id++;
+            arena += it.out_cap;
+            items.push_back(it);
+        }
     }
-    uint64_t arena_cap = arena + arena / 4 + (1u << 20);
+    const uint64_t arena_cap = arena + arena / 4 + (1u << 20);
     CK(dgrow(c->cells, arena_cap * 2));
     std::vector<ChunkResult> res;
     std::vector<MemberRec> mrecs;
     mrecs.reserve(4096);
-    int rc = launch_inflate(c, d_file, items, false, c->cells.p, res, &mrecs, err);
+    int rc = launch_inflate(c, d_base, items, false, c->cells.p, res, &mrecs, err);
     if (rc) return rc;
-    c->st.gpu_chunks += n;
+    c->st.gpu_chunks += items.size();
 
-    // ---- anchored chain (pipeline.rs:758-809)
-    struct Acc {
-        ChunkItem it;
-        ChunkResult r;
-        std::vector<MemberRec> m;
-    };
     std::unordered_map<uint32_t, std::vector<MemberRec>> by_item;
     auto bucket = [&](const std::vector<MemberRec>& all) {
         for (const MemberRec& m : all) by_item[m.item].push_back(m);
@@ -736,113 +865,223 @@ int member_route(rrg_ctx* c, const uint8_t* d_file, uint64_t len, uint64_t body_
         return v;
     };
     bucket(mrecs);
-    std::vector<Acc> acc;  // accepted chunks in stream order
-    uint64_t expected = 0;
-    bool final_seen = false;
-    uint32_t next_id = (uint32_t)n;
-    std::vector<size_t> overflow_pending;  // indices into acc needing a bigger slot
-    for (size_t k = 0; k < n && !final_seen; k++) {
-        ChunkItem it = items[k];
-        ChunkResult r = res[k];
-        if (it.start_bit == expected && (r.status == DS_OK || r.status == DS_OVERFLOW)) {
-            acc.push_back(Acc{it, r, take_recs(it.id)});
-        } else {
-            // false boundary or failed speculative decode: re-decode from the anchor
-            c->st.speculation_failures++;
-            if (it.end_hint != ~0ull && expected >= it.end_hint) continue;  // empty chunk
-            // the anchor lies at or after the guessed start (the previous chunk
-            // stops on a block edge at/after its end hint), so the re-decode
-            // spans no more input than the guess did and reuses its slot
-            it.start_bit = expected;
-            it.id = next_id++;
-            std::vector<ChunkItem> one{it};
-            std::vector<ChunkResult> r1;
-            std::vector<MemberRec> m1;
-            m1.reserve(4096);
-            rc = launch_inflate(c, d_file, one, false, c->cells.p, r1, &m1, err);
-            if (rc) return rc;
-            r = r1[0];
-            if (r.status != DS_OK && r.status != DS_OVERFLOW)
-                return status_err(err, r.status, r.msg, body_off + r.err_bit / 8);
-            bucket(m1);
-            acc.push_back(Acc{it, r, take_recs(it.id)});
+    // ---- anchored chain (pipeline.rs:758-809), in rounds: every job walks its
+    // chunks until one needs a re-decode from the true anchor; the re-decodes
+    // of all jobs share one launch
+    for (;;) {
+        std::vector<ChunkItem> redo;
+        std::vector<size_t> redo_job;
+        for (size_t i = 0; i < nj; i++) {
+            JobState& s = js[i];
+            MemberJob& j = jobs[i];
+            while (!s.done && s.pending < 0) {
+                if (s.final_seen || s.k >= s.n) {
+                    s.done = true;
+                    if (!s.final_seen) {
+                        set_err(&j.err, RRG_ERR_IO, "parallel decode produced no final block");
+                        j.rc = RRG_ERR_IO;
+                    }
+                    break;
+                }
+                ChunkItem it = items[s.first + s.k];
+                const ChunkResult r = res[s.first + s.k];
+                if (it.start_bit == s.expected && (r.status == DS_OK || r.status == DS_OVERFLOW)) {
+                    s.acc.push_back(Acc{it, r, take_recs(it.id)});
+                } else {
+                    // false boundary or failed speculative decode: re-decode from the anchor
+                    c->st.speculation_failures++;
+                    if (it.end_hint != ~0ull && s.expected >= it.end_hint) {  // empty chunk
+                        s.k++;
+                        continue;
+                    }
+                    // the anchor lies at or after the guessed start (the previous chunk
+                    // stops on a block edge at/after its end hint), so the re-decode
+                    // spans no more input than the guess did and reuses its slot
+                    it.start_bit = s.expected;
+                    it.id = next_id++;
+                    s.pending = (int64_t)redo.size();
+                    redo.push_back(it);
+                    redo_job.push_back(i);
+                    break;
+                }
+                if (s.acc.back().r.status == DS_OVERFLOW) s.overflow.push_back(s.acc.size() - 1);
+                s.expected = s.acc.back().r.actual_end_bit;
+                s.final_seen = s.acc.back().r.final_block != 0;
+                s.k++;
+            }
         }
-        if (acc.back().r.status == DS_OVERFLOW) overflow_pending.push_back(acc.size() - 1);
-        expected = acc.back().r.actual_end_bit;
-        final_seen = acc.back().r.final_block != 0;
-    }
-    if (!final_seen) {
-        set_err(err, RRG_ERR_IO, "parallel decode produced no final block");
-        return RRG_ERR_IO;
+        if (redo.empty()) break;
+        std::vector<ChunkResult> r1;
+        std::vector<MemberRec> m1;
+        m1.reserve(4096);
+        rc = launch_inflate(c, d_base, redo, false, c->cells.p, r1, &m1, err);
+        if (rc) return rc;
+        bucket(m1);
+        for (size_t q = 0; q < redo.size(); q++) {
+            JobState& s = js[redo_job[q]];
+            MemberJob& j = jobs[redo_job[q]];
+            s.pending = -1;
+            const ChunkResult& r = r1[q];
+            if (r.status != DS_OK && r.status != DS_OVERFLOW) {
+                fail(j, r.status, r.msg, j.file_off + j.body_off + r.err_bit / 8);
+                s.done = true;
+                continue;
+            }
+            s.acc.push_back(Acc{redo[q], r, take_recs(redo[q].id)});
+            if (r.status == DS_OVERFLOW) s.overflow.push_back(s.acc.size() - 1);
+            s.expected = r.actual_end_bit;
+            s.final_seen = r.final_block != 0;
+            s.k++;
+        }
     }
     // ---- overflowed slots: decode again with the exact size now known
-    if (!overflow_pending.empty()) {
+    {
         std::vector<ChunkItem> redo;
-        for (size_t a : overflow_pending) {
-            ChunkItem it = acc[a].it;
-            it.out_cap = round8(acc[a].r.n_cells + 8);
-            it.id = next_id++;
-            redo.push_back(it);
-        }
+        std::vector<std::pair<size_t, size_t>> where;  // (job, acc index)
         uint64_t need = 0;
-        for (auto& it : redo) need += it.out_cap;
-        if (arena + need > arena_cap) {
-            // the slots were far too small for this data: decode everything
-            // again with a larger expansion estimate (DEFLATE expands <= 1032x)
-            if (c->expand >= 1100.0) {
-                set_err(err, RRG_ERR_OUT_OF_MEMORY, "output slot arena exhausted");
-                return RRG_ERR_OUT_OF_MEMORY;
+        for (size_t i = 0; i < nj; i++) {
+            if (jobs[i].rc) continue;
+            for (size_t a : js[i].overflow) {
+                ChunkItem it = js[i].acc[a].it;
+                it.out_cap = round8(js[i].acc[a].r.n_cells + 8);
+                it.id = next_id++;
+                need += it.out_cap;
+                redo.push_back(it);
+                where.push_back({i, a});
             }
-            c->expand = std::min(1100.0, c->expand * 8);
-            return member_route(c, d_file, len, body_off, tgt, dst_off, member_base, out, err);
         }
-        for (auto& it : redo) {
-            it.out_off = arena;
-            arena += it.out_cap;
-        }
-        std::vector<ChunkResult> r2;
-        std::vector<MemberRec> m2;
-        m2.reserve(4096);
-        rc = launch_inflate(c, d_file, redo, false, c->cells.p, r2, &m2, err);
-        if (rc) return rc;
-        bucket(m2);
-        for (size_t i = 0; i < redo.size(); i++) {
-            if (r2[i].status != DS_OK) return status_err(err, r2[i].status, r2[i].msg, body_off + r2[i].err_bit / 8);
-            Acc& a = acc[overflow_pending[i]];
-            a.it = redo[i];
-            a.r = r2[i];
-            a.m = take_recs(redo[i].id);
+        if (!redo.empty()) {
+            if (arena + need > arena_cap) {
+                // the slots were far too small for this data: decode everything
+                // again with a larger expansion estimate (DEFLATE expands <= 1032x)
+                if (c->expand >= 1100.0) {
+                    set_err(err, RRG_ERR_OUT_OF_MEMORY, "output slot arena exhausted");
+                    return RRG_ERR_OUT_OF_MEMORY;
+                }
+                c->expand = std::min(1100.0, c->expand * 8);
+                for (MemberJob& j : jobs) {
+                    j.rc = 0;
+                    j.err = rrg_error{};
+                    j.out = Decoded{};
+                }
+                return members_route(c, d_base, jobs, tgt, err);
+            }
+            for (auto& it : redo) {
+                it.out_off = arena;
+                arena += it.out_cap;
+            }
+            std::vector<ChunkResult> r2;
+            std::vector<MemberRec> m2;
+            m2.reserve(4096);
+            rc = launch_inflate(c, d_base, redo, false, c->cells.p, r2, &m2, err);
+            if (rc) return rc;
+            bucket(m2);
+            for (size_t q = 0; q < redo.size(); q++) {
+                MemberJob& j = jobs[where[q].first];
+                if (j.rc) continue;
+                if (r2[q].status != DS_OK) {
+                    fail(j, r2[q].status, r2[q].msg, j.file_off + j.body_off + r2[q].err_bit / 8);
+                    continue;
+                }
+                Acc& a = js[where[q].first].acc[where[q].second];
+                a.it = redo[q];
+                a.r = r2[q];
+                a.m = take_recs(redo[q].id);
+            }
         }
     }
     // ---- output layout and member spans
+    uint64_t grow_need = 0;
+    for (size_t i = 0; i < nj; i++) {
+        MemberJob& j = jobs[i];
+        if (j.rc) continue;
+        uint64_t pos = 0;
+        for (const Acc& a : js[i].acc) pos += a.r.n_cells;
+        j.out.total = pos;
+        j.out.consumed = j.file_off + j.body_off + js[i].expected / 8;
+        if (j.dst_cap != ~0ull && pos > j.dst_cap) {
+            set_err(&j.err, RRG_ERR_CAPACITY, "output buffer too small: need %llu bytes", (unsigned long long)pos);
+            j.rc = RRG_ERR_CAPACITY;
+            continue;
+        }
+        grow_need = std::max(grow_need, j.dst_off + pos);
+    }
+    if (tgt.grow) {
+        uint64_t keep = ~0ull;
+        for (const MemberJob& j : jobs) keep = std::min(keep, j.dst_off);
+        rc = ensure_out(c, tgt, grow_need, keep == ~0ull ? 0 : keep, err);
+        if (rc) return rc;
+    }
     std::vector<ResolveChunk> rchunks;
+    std::vector<size_t> chunk_job;
     std::vector<uint64_t> tile_start{0};
     std::vector<MemberSpan> spans;
-    uint64_t pos = 0, mstart = 0;
-    for (const Acc& a : acc) {
-        if (a.r.n_cells) {
-            ResolveChunk rc2{dst_off + pos, a.it.out_off, a.r.n_cells, dst_off + mstart};
-            rchunks.push_back(rc2);
-            tile_start.push_back(tile_start.back() + (a.r.n_cells + RES_TILE - 1) / RES_TILE);
+    std::vector<size_t> span_job;
+    std::vector<uint32_t> span_member;
+    for (size_t i = 0; i < nj; i++) {
+        MemberJob& j = jobs[i];
+        if (j.rc) continue;
+        uint64_t pos = 0, mstart = 0;
+        uint32_t nm = 0;
+        for (const Acc& a : js[i].acc) {
+            if (a.r.n_cells) {
+                rchunks.push_back(ResolveChunk{j.dst_off + pos, a.it.out_off, a.r.n_cells, j.dst_off + mstart});
+                chunk_job.push_back(i);
+                tile_start.push_back(tile_start.back() + (a.r.n_cells + RES_TILE - 1) / RES_TILE);
+            }
+            for (const MemberRec& m : a.m) {
+                const uint64_t end = pos + m.cell_off;
+                spans.push_back(MemberSpan{j.dst_off + mstart, end - mstart, m.crc, m.isize,
+                                           j.file_off + j.body_off + m.trailer_byte});
+                span_job.push_back(i);
+                span_member.push_back(j.member_base + nm++);
+                mstart = end;
+            }
+            pos += a.r.n_cells;
         }
-        for (const MemberRec& m : a.m) {
-            uint64_t end = pos + m.cell_off;
-            spans.push_back(MemberSpan{dst_off + mstart, end - mstart, m.crc, m.isize, body_off + m.trailer_byte});
-            mstart = end;
-        }
-        pos += a.r.n_cells;
+        j.out.members = nm;
     }
-    out->total = pos;
-    out->consumed = body_off + expected / 8;
-    out->members = (uint32_t)spans.size();
-    rc = ensure_out(c, tgt, dst_off + pos, dst_off, err);
+    // ---- resolve markers + compact; a failing chunk fails its job only
+    int64_t bad = -1;
+    rrg_error rerr{};
+    rc = run_resolve(c, rchunks, tile_start, tgt.p, &rerr, &bad);
+    if (rc && (rc != RRG_ERR_DEFLATE_INVALID || bad < 0 || (uint64_t)bad >= chunk_job.size())) {
+        if (err) *err = rerr;
+        return rc;
+    }
+    if (rc) {
+        jobs[chunk_job[bad]].rc = rc;
+        jobs[chunk_job[bad]].err = rerr;
+    }
+    // ---- CRC32/ISIZE of every member (spans are positions in the target)
+    std::vector<int32_t> stv;
+    std::vector<uint32_t> got;
+    std::vector<uint64_t> glen;
+    rc = crc_spans(c, tgt.p, spans, stv, got, glen, err);
     if (rc) return rc;
-    uint8_t* d_dst = tgt.p;
-    // ---- resolve markers + compact
-    rc = run_resolve(c, rchunks, tile_start, d_dst, err);
+    for (size_t m = 0; m < spans.size(); m++) {
+        MemberJob& j = jobs[span_job[m]];
+        if (j.rc || (stv[m] != DS_CRC && stv[m] != DS_ISIZE)) continue;
+        j.rc = member_error(&j.err, spans[m], span_member[m], stv[m], got[m], glen[m]);
+    }
+    return 0;
+}
+
+// One member stream at d_file (its first header already parsed) into
+// tgt.p[dst_off ..]. On RRG_ERR_CAPACITY `out->total` holds the size required.
+int member_route(rrg_ctx* c, const uint8_t* d_file, uint64_t len, uint64_t body_off, OutTarget& tgt, uint64_t dst_off,
+                 uint32_t member_base, Decoded* out, rrg_error* err) {
+    std::vector<MemberJob> jobs(1);
+    jobs[0].len = len;
+    jobs[0].body_off = body_off;
+    jobs[0].dst_off = dst_off;
+    jobs[0].dst_cap = tgt.grow ? ~0ull : (tgt.cap > dst_off ? tgt.cap - dst_off : 0);
+    jobs[0].member_base = member_base;
+    int rc = members_route(c, d_file, jobs, tgt, err);
+    *out = jobs[0].out;
     if (rc) return rc;
-    // spans carry positions relative to d_dst
-    return check_members(c, d_dst, spans, member_base, err);
+    if (jobs[0].rc && err) *err = jobs[0].err;
+    return jobs[0].rc;
 }
 
 // ------------------------------------------------------------ BGZF route

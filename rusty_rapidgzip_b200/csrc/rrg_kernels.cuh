@@ -50,6 +50,8 @@ __constant__ uint32_t c_x2k[67];
 constexpr int LUT_BITS = 10;
 constexpr int LUT_SIZE = 1 << LUT_BITS;
 constexpr int PRE_BITS = 7;
+constexpr int DIST_BITS = 8;  // inflate's distance LUT; longer codes (~1% of distances) take long_decode
+constexpr int DIST_SIZE = 1 << DIST_BITS;
 constexpr int NB = 32;  // symbols per decode batch
 
 // ------------------------------------------------------- warp helpers
@@ -239,8 +241,10 @@ __device__ __noinline__ uint32_t long_decode(uint64_t buf, const Table& T, int l
 // ------------------------------------------------------- inflate kernel
 struct WarpSmem {
     uint32_t lit_lut[LUT_SIZE];
-    uint32_t dist_lut[LUT_SIZE];
-    uint32_t pre_lut[1 << PRE_BITS];
+    union {  // the precode table is dead once the distance table is built
+        uint32_t dist_lut[DIST_SIZE];
+        uint32_t pre_lut[1 << PRE_BITS];
+    };
     uint2 ep[NB];  // per batch symbol: x = entry (literal flag|byte, or dist<<9|length), y = output offset
     uint16_t lit_sorted[288];
     uint16_t dist_sorted[32];
@@ -402,7 +406,7 @@ __device__ void read_dynamic(WarpSmem& S, ItemState& st, int lane) {
     }
     __syncwarp();
     msg = warp_build(S.lengths, (int)hlit, lit_table(S), LUT_BITS, TK_LITLEN, S.run, lane);
-    if (!msg) msg = warp_build(S.lengths + hlit, (int)hdist, dist_table(S), LUT_BITS, TK_DIST, S.run, lane);
+    if (!msg) msg = warp_build(S.lengths + hlit, (int)hdist, dist_table(S), DIST_BITS, TK_DIST, S.run, lane);
     if (msg) {
         st.status = DS_INVALID;
         st.msg = msg;
@@ -417,7 +421,7 @@ __device__ void load_fixed(WarpSmem& S, int lane) {
     for (int i = lane; i < 30; i += 32) S.lengths[288 + i] = 5;
     __syncwarp();
     warp_build(S.lengths, 288, lit_table(S), LUT_BITS, TK_LITLEN, S.run, lane);
-    warp_build(S.lengths + 288, 30, dist_table(S), LUT_BITS, TK_DIST, S.run, lane);
+    warp_build(S.lengths + 288, 30, dist_table(S), DIST_BITS, TK_DIST, S.run, lane);
     if (lane == 0) S.fixed_loaded = 1;
     __syncwarp();
 }
@@ -510,10 +514,10 @@ __device__ void decode_codes(WarpSmem& S, ItemState& st, CellT* out, int lane) {
                             wp++;
                             bits += 32;
                         }
-                        uint32_t de = S.dist_lut[buf & (LUT_SIZE - 1)];
+                        uint32_t de = S.dist_lut[buf & (DIST_SIZE - 1)];
                         uint32_t dl = de & 15;
                         if (!dl) {
-                            de = long_decode(buf, DT, LUT_BITS, TK_DIST);
+                            de = long_decode(buf, DT, DIST_BITS, TK_DIST);
                             dl = de & 15;
                             if (!dl) {
                                 status = DS_INVALID;
@@ -579,10 +583,10 @@ __device__ void decode_codes(WarpSmem& S, ItemState& st, CellT* out, int lane) {
                     uint32_t length = (e >> 16) + ((uint32_t)(b.buf >> cl) & ((1u << ex) - 1u));
                     br_consume(b, cl + ex);
                     br_refill(b);
-                    uint32_t de = S.dist_lut[b.buf & (LUT_SIZE - 1)];
+                    uint32_t de = S.dist_lut[b.buf & (DIST_SIZE - 1)];
                     uint32_t dl = de & 15;
                     if (!dl) {
-                        de = long_decode(b.buf, DT, LUT_BITS, TK_DIST);
+                        de = long_decode(b.buf, DT, DIST_BITS, TK_DIST);
                         dl = de & 15;
                         if (!dl) {
                             status = br_past_end(b) ? DS_EOF : DS_INVALID;
@@ -631,8 +635,19 @@ __device__ void decode_codes(WarpSmem& S, ItemState& st, CellT* out, int lane) {
         if (!st.counting && n) {
             uint32_t bad = 0, mk = 0;
             const uint64_t cur = st.cur;
-            for (uint32_t j = lane; j < pos; j += 32) {
-                int k = find_entry(S.ep, n, j);
+            // Lane k holds the start of entry k. For each 32-cell group one OR
+            // over the warp marks the entries that start inside it, so a lane's
+            // entry is (entries started before the group) + (starts at or below
+            // the lane) - 1: no search.
+            const uint32_t my_start = lane < n ? S.ep[lane].y : 0xffffffffu;
+            uint32_t before = 0;
+            for (uint32_t j0 = 0; j0 < pos; j0 += 32) {
+                const uint32_t j = j0 + lane;
+                const uint32_t rel = my_start - j0;
+                const uint32_t starts = __reduce_or_sync(FULLMASK, rel < 32u ? (1u << rel) : 0u);
+                int k = (int)(before + __popc(starts & (0xffffffffu >> (31 - lane)))) - 1;
+                before += __popc(starts);
+                if (j >= pos) break;  // last group only: no collective follows in this pass
                 uint32_t jj = j, cell = 0;
                 for (;;) {
                     uint32_t e = S.ep[k].x;
@@ -879,9 +894,12 @@ __device__ void inflate_item(WarpSmem& S, const InflateArgs& A, uint32_t item_id
     __syncwarp();
 }
 
-// 128 threads (4 warps) per block, >= 5 blocks per SM: 20 decoding warps per SM
+#ifndef RRG_INFLATE_MIN_BLOCKS
+#define RRG_INFLATE_MIN_BLOCKS 5
+#endif
+// 128 threads (4 warps) per block, >= RRG_INFLATE_MIN_BLOCKS blocks per SM
 template <typename CellT>
-__global__ void __launch_bounds__(128, 5) k_inflate(InflateArgs A) {
+__global__ void __launch_bounds__(128, RRG_INFLATE_MIN_BLOCKS) k_inflate(InflateArgs A) {
     RRG_DYN_SMEM(smem_raw);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     WarpSmem& S = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
@@ -2037,30 +2055,30 @@ __global__ void __launch_bounds__(RES_THREADS) k_resolve(ResolveArgs A) {
         const uint32_t* win = A.win + (uint64_t)k * WINDOW;
         const uint64_t c0 = (t - A.tile_start[k]) * (uint64_t)RES_TILE;
         const uint64_t cn = ck.n_cells - c0 < (uint64_t)RES_TILE ? ck.n_cells - c0 : (uint64_t)RES_TILE;
-        const uint32_t mine = threadIdx.x * RES_PER_THREAD;
+        // warp w owns cells [512w, 512w + 512) of the tile, lane ln the cells
+        // 512w + ln + 32i: one gather instruction covers 32 consecutive cells,
+        // whose window sources are mostly consecutive too (copied runs), so a
+        // warp's gathers touch few cache lines
+        const uint32_t wbase = (threadIdx.x >> 5) * (32 * RES_PER_THREAD), ln = threadIdx.x & 31;
         uint32_t nmk = 0, bad = 0;
-        if (mine < cn) {
-            const uint16_t* p = A.cells + ck.slot_off + c0 + mine;
+        if (wbase < cn) {
+            const uint16_t* p = A.cells + ck.slot_off + c0 + wbase + ln;
+            const uint32_t lim = (uint32_t)(cn - wbase);  // cells of this warp's span that exist
             uint32_t cell[RES_PER_THREAD];
-            if (mine + RES_PER_THREAD <= cn) {
-                uint4 a = *reinterpret_cast<const uint4*>(p);
-                uint4 b = *reinterpret_cast<const uint4*>(p + 8);
-                uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-                for (int i = 0; i < 8; i++) {
-                    cell[2 * i] = w[i] & 0xffffu;
-                    cell[2 * i + 1] = w[i] >> 16;
-                }
-            } else {
-                for (int i = 0; i < RES_PER_THREAD; i++) cell[i] = (mine + i < cn) ? p[i] : 0u;
-            }
+#pragma unroll
+            for (int i = 0; i < RES_PER_THREAD; i++) cell[i] = (ln + 32u * i < lim) ? p[32 * i] : 0u;
             // independent gathers: all issued before any is consumed
             uint32_t got[RES_PER_THREAD];
+#pragma unroll
             for (int i = 0; i < RES_PER_THREAD; i++)
                 got[i] = (cell[i] & MARKER16) ? win[WINDOW - 1 - (cell[i] & 0x7fffu)] : (WIN_BYTE | cell[i]);
+#pragma unroll
             for (int i = 0; i < RES_PER_THREAD; i++) {
-                nmk += (cell[i] & MARKER16) ? 1u : 0u;
-                if (got[i] == WIN_INVALID || !(got[i] & WIN_BYTE)) bad = 1;
-                stage[mine + i] = (uint8_t)got[i];
+                if (ln + 32u * i < lim) {
+                    nmk += (cell[i] & MARKER16) ? 1u : 0u;
+                    if (got[i] == WIN_INVALID || !(got[i] & WIN_BYTE)) bad = 1;
+                    stage[wbase + ln + 32 * i] = (uint8_t)got[i];
+                }
             }
         }
         if (bad) atomicOr(&s_bad, 1u);

@@ -154,6 +154,16 @@ inline unsigned __match_any_sync(unsigned, unsigned v) {
     w->bar.arrive_and_wait();
     return m;
 }
+inline unsigned __reduce_or_sync(unsigned, unsigned v) {
+    emu::Warp* w = emu::t_warp;
+    int lane = emu::t_tid.x & 31;
+    w->slot[lane] = v;
+    w->bar.arrive_and_wait();
+    unsigned m = 0;
+    for (int i = 0; i < 32; i++) m |= (unsigned)w->slot[i];
+    w->bar.arrive_and_wait();
+    return m;
+}
 inline int __popc(unsigned v) { return __builtin_popcount(v); }
 inline int __ffs(int v) { return __builtin_ffs(v); }
 inline unsigned __funnelshift_r(unsigned lo, unsigned hi, unsigned sh) {
