@@ -92,6 +92,7 @@ typedef struct rrg_stats {
     uint64_t members;              /* gzip members verified */
     uint64_t kernel_launches;      /* kernels launched by this call */
     double finder_ms, inflate_ms, resolve_ms, crc_ms, h2d_ms, d2h_ms, total_ms;
+    uint64_t graph_launches;       /* captured decode graphs replayed by this call (BGZF route) */
 } rrg_stats;
 
 /* Sink: called in stream order with consecutive pieces of decompressed output.

@@ -85,7 +85,8 @@ _STAT_F64 = ["finder_ms", "inflate_ms", "resolve_ms", "crc_ms", "h2d_ms", "d2h_m
 
 
 class _Stats(C.Structure):
-    _fields_ = [(n, C.c_uint64) for n in _STAT_U64] + [(n, C.c_double) for n in _STAT_F64]
+    _fields_ = ([(n, C.c_uint64) for n in _STAT_U64] + [(n, C.c_double) for n in _STAT_F64]
+                + [("graph_launches", C.c_uint64)])
 
 
 SINK_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_uint8), C.c_size_t)
@@ -130,11 +131,12 @@ class DecodeStats:
     markers: int = 0
     members: int = 0
     kernel_launches: int = 0
+    graph_launches: int = 0
     timings_ms: dict = field(default_factory=dict)
 
     @classmethod
     def _from(cls, s: _Stats) -> "DecodeStats":
-        return cls(**{n: int(getattr(s, n)) for n in _STAT_U64},
+        return cls(**{n: int(getattr(s, n)) for n in _STAT_U64}, graph_launches=int(s.graph_launches),
                    timings_ms={n[:-3]: float(getattr(s, n)) for n in _STAT_F64})
 
 

@@ -203,16 +203,18 @@ int64_t host_bgzf_size(const uint8_t* in, size_t len) {
     return -1;
 }
 
-uint32_t le32(const uint8_t* p) {
-    return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
-}
-
 struct DBuf {
     void* p = nullptr;
     size_t cap = 0;
 };
 
 }  // namespace
+
+// buffers and shapes a captured BGZF decode graph refers to
+struct BgzfKey {
+    const void* p[24];
+    uint64_t v[6];
+};
 
 // ====================================================================== ctx
 struct rrg_ctx {
@@ -241,6 +243,16 @@ struct rrg_ctx {
     uint32_t finder_tile = 1024;
     double expand = 6.0;
     uint64_t slots = 0;        // resident decoders of one inflate wave (lazy)
+    DBuf sniff;                // per-file header results of a batch
+    // BGZF route: device member table and the captured decode graph
+    DBuf bg_bcount, bg_bbase, bg_coff, bg_csize, bg_small;
+    uint64_t* h_bg = nullptr;  // pinned: the 64 result bytes of one BGZF decode
+    uint32_t bg_cap = 0;
+    bool use_graphs = true;
+#ifndef RRG_EMU
+    cudaGraphExec_t bg_exec = nullptr;
+    BgzfKey bg_key{};
+#endif
 
     rrg_stats st{};
     uint64_t launches = 0;
@@ -358,7 +370,7 @@ int launch_inflate(rrg_ctx* c, const uint8_t* d_in, const std::vector<ChunkItem>
         CK(cudaMemcpyAsync(c->order.p, order.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
         CK(cudaMemsetAsync(c->queue.p, 0, 16, c->stream));
         CK(cudaMemsetAsync(c->mbcount.p, 0, 16, c->stream));
-        InflateArgs A;
+        InflateArgs A{};
         A.in = d_in;
         A.items = (const ChunkItem*)c->items.p;
         A.results = (ChunkResult*)c->results.p;
@@ -681,6 +693,7 @@ struct MemberJob {
     uint64_t dst_off = 0;     // first output byte in the target
     uint64_t dst_cap = ~0ull; // output bytes available at dst_off (~0: the target grows)
     uint32_t member_base = 0; // index of the first member, for error reports
+    double expand = 0;        // output cells per compressed byte to reserve (0: the context's estimate)
     // results
     int rc = 0;
     rrg_error err{};
@@ -814,12 +827,77 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
             }
         }
     }
+    std::vector<JobState> js(nj);
+    uint32_t next_id = 0;
+    std::unordered_map<uint32_t, std::vector<MemberRec>> by_item;
+    auto bucket = [&](const std::vector<MemberRec>& all) {
+        for (const MemberRec& m : all) by_item[m.item].push_back(m);
+    };
+    auto take_recs = [&](uint32_t id) {
+        std::vector<MemberRec> v;
+        auto f = by_item.find(id);
+        if (f != by_item.end()) {
+            v.swap(f->second);
+            std::sort(v.begin(), v.end(), [](const MemberRec& a, const MemberRec& b) { return a.seq < b.seq; });
+        }
+        return v;
+    };
+    // ---- a stream of one chunk with a fixed destination decodes straight to
+    // its bytes: it cannot hold markers, so there is nothing to resolve
+    std::vector<char> direct(nj, 0);
+    std::vector<std::vector<MemberRec>> direct_recs(nj);
+    {
+        std::vector<ChunkItem> ditems;
+        std::vector<size_t> djob;
+        for (size_t i = 0; i < nj && !tgt.grow; i++) {
+            if (starts[i].size() != 1) continue;
+            const MemberJob& j = jobs[i];
+            direct[i] = 1;
+            ChunkItem it{};
+            it.in_off = j.file_off + j.body_off;
+            it.in_len = j.len - j.body_off;
+            it.start_bit = 0;
+            it.end_hint = ~0ull;
+            it.out_off = j.dst_off;
+            it.out_cap = j.dst_cap;
+            it.flags = 0;
+            it.id = next_id++;
+            ditems.push_back(it);
+            djob.push_back(i);
+        }
+        if (!ditems.empty()) {
+            std::vector<ChunkResult> dres;
+            std::vector<MemberRec> dm;
+            dm.reserve(4096);
+            int rc0 = launch_inflate(c, d_base, ditems, true, tgt.p, dres, &dm, err);
+            if (rc0) return rc0;
+            c->st.gpu_chunks += ditems.size();
+            bucket(dm);
+            for (size_t q = 0; q < ditems.size(); q++) {
+                MemberJob& j = jobs[djob[q]];
+                const ChunkResult& r = dres[q];
+                js[djob[q]].done = true;
+                j.out.total = r.n_cells;
+                j.out.consumed = j.file_off + j.body_off + r.actual_end_bit / 8;
+                if (r.status == DS_OVERFLOW) {
+                    set_err(&j.err, RRG_ERR_CAPACITY, "output buffer too small: need %llu bytes",
+                            (unsigned long long)r.n_cells);
+                    j.rc = RRG_ERR_CAPACITY;
+                } else if (r.status != DS_OK) {
+                    fail(j, r.status, r.msg, j.file_off + j.body_off + r.err_bit / 8);
+                } else if (!r.final_block) {
+                    set_err(&j.err, RRG_ERR_IO, "parallel decode produced no final block");
+                    j.rc = RRG_ERR_IO;
+                }
+                direct_recs[djob[q]] = take_recs(ditems[q].id);
+            }
+        }
+    }
     // ---- items and the slot arena: every chunk gets expand x its compressed span
     std::vector<ChunkItem> items;
-    std::vector<JobState> js(nj);
     uint64_t arena = 0;
-    uint32_t next_id = 0;
     for (size_t i = 0; i < nj; i++) {
+        if (direct[i]) continue;
         const MemberJob& j = jobs[i];
         const uint64_t blen = j.len - j.body_off, total_bits = blen * 8;
         const auto& st = starts[i];
@@ -832,7 +910,7 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
             it.start_bit = st[k];
             it.end_hint = k + 1 < st.size() ? st[k + 1] : ~0ull;
             const uint64_t span = ((k + 1 < st.size() ? st[k + 1] : total_bits) - st[k] + 7) / 8;
-            it.out_cap = round8((uint64_t)(span * c->expand) + 65536);
+            it.out_cap = round8((uint64_t)(span * (j.expand > 0 ? j.expand : c->expand)) + 65536);
             it.out_off = arena;
             // the first chunk too, as in the reference: a reference before the
             // stream's start becomes a marker that fails to resolve
@@ -851,19 +929,6 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
     if (rc) return rc;
     c->st.gpu_chunks += items.size();
 
-    std::unordered_map<uint32_t, std::vector<MemberRec>> by_item;
-    auto bucket = [&](const std::vector<MemberRec>& all) {
-        for (const MemberRec& m : all) by_item[m.item].push_back(m);
-    };
-    auto take_recs = [&](uint32_t id) {
-        std::vector<MemberRec> v;
-        auto f = by_item.find(id);
-        if (f != by_item.end()) {
-            v.swap(f->second);
-            std::sort(v.begin(), v.end(), [](const MemberRec& a, const MemberRec& b) { return a.seq < b.seq; });
-        }
-        return v;
-    };
     bucket(mrecs);
     // ---- anchored chain (pipeline.rs:758-809), in rounds: every job walks its
     // chunks until one needs a re-decode from the true anchor; the re-decodes
@@ -954,15 +1019,19 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
             if (arena + need > arena_cap) {
                 // the slots were far too small for this data: decode everything
                 // again with a larger expansion estimate (DEFLATE expands <= 1032x)
-                if (c->expand >= 1100.0) {
+                // (size hints from the trailers are dropped first)
+                bool hinted = false;
+                for (const MemberJob& j : jobs) hinted |= j.expand > 0;
+                if (!hinted && c->expand >= 1100.0) {
                     set_err(err, RRG_ERR_OUT_OF_MEMORY, "output slot arena exhausted");
                     return RRG_ERR_OUT_OF_MEMORY;
                 }
-                c->expand = std::min(1100.0, c->expand * 8);
+                if (!hinted) c->expand = std::min(1100.0, c->expand * 8);
                 for (MemberJob& j : jobs) {
                     j.rc = 0;
                     j.err = rrg_error{};
                     j.out = Decoded{};
+                    j.expand = 0;
                 }
                 return members_route(c, d_base, jobs, tgt, err);
             }
@@ -994,7 +1063,7 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
     uint64_t grow_need = 0;
     for (size_t i = 0; i < nj; i++) {
         MemberJob& j = jobs[i];
-        if (j.rc) continue;
+        if (j.rc || direct[i]) continue;
         uint64_t pos = 0;
         for (const Acc& a : js[i].acc) pos += a.r.n_cells;
         j.out.total = pos;
@@ -1023,6 +1092,17 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
         if (j.rc) continue;
         uint64_t pos = 0, mstart = 0;
         uint32_t nm = 0;
+        if (direct[i]) {
+            for (const MemberRec& m : direct_recs[i]) {
+                spans.push_back(MemberSpan{j.dst_off + mstart, m.cell_off - mstart, m.crc, m.isize,
+                                           j.file_off + j.body_off + m.trailer_byte});
+                span_job.push_back(i);
+                span_member.push_back(j.member_base + nm++);
+                mstart = m.cell_off;
+            }
+            j.out.members = nm;
+            continue;
+        }
         for (const Acc& a : js[i].acc) {
             if (a.r.n_cells) {
                 rchunks.push_back(ResolveChunk{j.dst_off + pos, a.it.out_off, a.r.n_cells, j.dst_off + mstart});
@@ -1085,84 +1165,243 @@ int member_route(rrg_ctx* c, const uint8_t* d_file, uint64_t len, uint64_t body_
 }
 
 // ------------------------------------------------------------ BGZF route
-struct BgzfMember {
-    uint64_t off, size;
-    uint32_t isize, crc;
-};
+// The whole BGZF decode is enqueued without a host round trip: member scan,
+// chain walk, one persistent k_inflate<u8> launch over every member, CRC
+// pieces and combine, and a first-failure reduction; the host reads 64 bytes
+// of results at the end. The sequence is captured into a CUDA graph and
+// replayed while the buffers it names stay the same.
+constexpr int BGK_KERNELS = 9;  // kernels in one BGZF decode
 
-// Walk BGZF members from offset 0 (pipeline.rs:1524-1541). Needs the whole
-// file in host memory. Returns the remainder offset.
-uint64_t bgzf_walk(const uint8_t* h, uint64_t len, std::vector<BgzfMember>& ms, bool* truncated) {
-    uint64_t pos = 0;
-    *truncated = false;
-    while (pos < len) {
-        int64_t sz = host_bgzf_size(h + pos, len - pos);
-        if (sz < 0) break;
-        if (pos + (uint64_t)sz > len) {
-            *truncated = true;
-            break;
-        }
-        BgzfMember m{pos, (uint64_t)sz, 0, 0};
-        if (sz >= 8) {
-            m.crc = le32(h + pos + sz - 8);
-            m.isize = le32(h + pos + sz - 4);
-        }
-        ms.push_back(m);
-        pos += (uint64_t)sz;
+int bgzf_enqueue(rrg_ctx* c, const uint8_t* d_file, uint64_t len, uint8_t* d_out, uint64_t out_cap, uint32_t sgrid,
+                 uint64_t per_block, uint32_t cap, rrg_error* err) {
+    uint64_t* small = (uint64_t*)c->bg_small.p;
+    uint32_t* nmem = (uint32_t*)(small + 4);
+    uint32_t* first = (uint32_t*)(small + 5);
+    uint32_t* ncand = (uint32_t*)(small + 6);
+    BgzfScanArgs S{d_file, len, per_block, (uint32_t*)c->bg_bcount.p, (uint32_t*)c->bg_bbase.p,
+                   (uint64_t*)c->bg_coff.p, (uint32_t*)c->bg_csize.p, cap, ncand};
+    RRG_LAUNCH(k_bgzf_count, sgrid, BG_THREADS, 0, c->stream, S);
+    LAUNCHED(c);
+    RRG_LAUNCH(k_bgzf_prefix, 1, 1024, 0, c->stream, S, sgrid);
+    LAUNCHED(c);
+    RRG_LAUNCH(k_bgzf_collect, sgrid, BG_THREADS, 0, c->stream, S);
+    LAUNCHED(c);
+    BgzfChainArgs C{d_file, len, (const uint64_t*)c->bg_coff.p, (const uint32_t*)c->bg_csize.p, ncand, cap,
+                    (ChunkItem*)c->items.p, cap, (CrcPiece*)c->pieces.p, (uint32_t*)c->mpiece.p,
+                    (uint32_t*)c->exp_crc.p, (uint32_t*)c->exp_isize.p, out_cap, nmem, small};
+    RRG_LAUNCH(k_bgzf_chain, 1, 32, 0, c->stream, C);
+    LAUNCHED(c);
+    CK(cudaMemsetAsync(c->queue.p, 0, 16, c->stream));
+    CK(cudaMemsetAsync(first, 0xff, 8, c->stream));
+    InflateArgs A{};
+    A.in = d_file;
+    A.items = (const ChunkItem*)c->items.p;
+    A.results = (ChunkResult*)c->results.p;
+    A.n_items = cap;
+    A.n_items_dev = nmem;
+    A.order = nullptr;
+    A.queue = (uint32_t*)c->queue.p;
+    A.out = d_out;
+    A.mbs = (MemberRec*)c->mbs.p;
+    A.mb_count = (uint32_t*)c->mbcount.p;
+    A.mb_cap = 0;
+    if (c->lanes) {
+        int locc = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&locc, k_inflate_lanes<uint8_t>, LANE_THREADS,
+                                                      LANE_THREADS * sizeof(LaneTab));
+        const uint32_t lgrid = (uint32_t)c->n_sm * std::max(1, locc);
+        RRG_LAUNCH(k_inflate_lanes<uint8_t>, lgrid, LANE_THREADS, LANE_THREADS * sizeof(LaneTab), c->stream, A,
+                   (LaneScratch*)c->lane_scratch.p);
+    } else {
+        const uint32_t W = c->inflate_warps;
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_inflate<uint8_t>, W * 32, W * sizeof(WarpSmem));
+        RRG_LAUNCH(k_inflate<uint8_t>, (uint32_t)c->n_sm * std::max(1, occ), W * 32, W * sizeof(WarpSmem), c->stream,
+                   A);
     }
-    return pos;
+    LAUNCHED(c);
+    RRG_LAUNCH(k_bgzf_fix, c->n_sm * 4, 256, 0, c->stream, (const ChunkResult*)c->results.p, (CrcPiece*)c->pieces.p,
+               (uint32_t*)c->exp_crc.p, (uint32_t*)c->exp_isize.p, (const uint32_t*)nmem);
+    LAUNCHED(c);
+    CrcArgs P{d_out, (const CrcPiece*)c->pieces.p, 0, (uint32_t*)c->piece_crc.p, (const uint32_t*)c->crc_table.p, nmem};
+    RRG_LAUNCH(k_crc_pieces, c->n_sm * 8, CRC_THREADS, 0, c->stream, P);
+    LAUNCHED(c);
+    CrcMemberArgs M{(const CrcPiece*)c->pieces.p, (const uint32_t*)c->piece_crc.p, (const uint32_t*)c->mpiece.p, 0,
+                    (const uint32_t*)c->exp_crc.p, (const uint32_t*)c->exp_isize.p, (uint32_t*)c->got_crc.p,
+                    (uint64_t*)c->got_len.p, (int32_t*)c->mstatus.p, nmem};
+    RRG_LAUNCH(k_crc_members, c->n_sm * 4, 256, 0, c->stream, M);
+    LAUNCHED(c);
+    RRG_LAUNCH(k_bgzf_first_bad, c->n_sm * 4, 256, 0, c->stream, (const ChunkResult*)c->results.p,
+               (const int32_t*)c->mstatus.p, (const uint32_t*)nmem, first);
+    LAUNCHED(c);
+    CK(cudaMemcpyAsync(c->h_bg, small, 64, cudaMemcpyDeviceToHost, c->stream));
+    return 0;
 }
 
-int bgzf_route(rrg_ctx* c, const uint8_t* d_file, const std::vector<BgzfMember>& ms, OutTarget& tgt, Decoded* out,
-               rrg_error* err) {
-    const size_t nm = ms.size();
-    std::vector<ChunkItem> items(nm);
-    uint64_t pos = 0;
-    for (size_t i = 0; i < nm; i++) {
-        ChunkItem& it = items[i];
-        it.in_off = ms[i].off;
-        it.in_len = ms[i].size;
-        it.start_bit = 0;
-        it.end_hint = ~0ull;
-        it.out_off = pos;
-        it.out_cap = ms[i].isize;
-        it.flags = ITEM_ONE_MEMBER;
-        it.id = (uint32_t)i;
-        pos += ms[i].isize;
+// Decodes the BGZF members from byte 0 of d_file into tgt; *rem = where the
+// member chain ended, *truncated = the member there runs past the file.
+int bgzf_route(rrg_ctx* c, const uint8_t* d_file, uint64_t len, OutTarget& tgt, Decoded* out, uint64_t* rem,
+               bool* truncated, rrg_error* err) {
+    *out = Decoded{};
+    if (!c->h_bg) CK(cudaMallocHost((void**)&c->h_bg, 64));
+    uint32_t cap = std::max<uint32_t>(c->bg_cap, (uint32_t)std::min<uint64_t>(len / 2048 + 4096, 1u << 30));
+    const uint32_t sgrid =
+        (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)c->n_sm * 8, (len + BG_STEP - 1) / BG_STEP));
+    const uint64_t per_block = ((len + sgrid - 1) / sgrid + BG_STEP - 1) / BG_STEP * BG_STEP;
+    const uint64_t* hb = c->h_bg;
+    for (int attempt = 0;; attempt++) {
+        if (attempt > 4) {
+            set_err(err, RRG_ERR_OUT_OF_MEMORY, "BGZF member table does not converge");
+            return RRG_ERR_OUT_OF_MEMORY;
+        }
+        c->bg_cap = cap;
+        CK(dgrow(c->bg_bcount, (size_t)sgrid * 4));
+        CK(dgrow(c->bg_bbase, (size_t)(sgrid + 1) * 4));
+        CK(dgrow(c->bg_coff, (size_t)cap * 8));
+        CK(dgrow(c->bg_csize, (size_t)cap * 4));
+        CK(dgrow(c->bg_small, 64));
+        CK(dgrow(c->items, (size_t)cap * sizeof(ChunkItem)));
+        CK(dgrow(c->results, (size_t)cap * sizeof(ChunkResult)));
+        CK(dgrow(c->pieces, (size_t)cap * sizeof(CrcPiece)));
+        CK(dgrow(c->piece_crc, (size_t)cap * 4));
+        CK(dgrow(c->mpiece, (size_t)(cap + 1) * 4));
+        CK(dgrow(c->exp_crc, (size_t)cap * 4));
+        CK(dgrow(c->exp_isize, (size_t)cap * 4));
+        CK(dgrow(c->got_crc, (size_t)cap * 4));
+        CK(dgrow(c->got_len, (size_t)cap * 8));
+        CK(dgrow(c->mstatus, (size_t)cap * 4));
+        CK(dgrow(c->queue, 16));
+        CK(dgrow(c->mbs, sizeof(MemberRec)));
+        CK(dgrow(c->mbcount, 16));
+        if (c->lanes) {
+            int locc = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&locc, k_inflate_lanes<uint8_t>, LANE_THREADS,
+                                                          LANE_THREADS * sizeof(LaneTab));
+            CK(dgrow(c->lane_scratch, (size_t)c->n_sm * std::max(1, locc) * LANE_THREADS * sizeof(LaneScratch)));
+        }
+        KTimer kt(c->stream);
+        bool ran = false;
+#ifndef RRG_EMU
+        BgzfKey key{};
+        const DBuf* bs[] = {&c->bg_bcount, &c->bg_bbase, &c->bg_coff, &c->bg_csize, &c->bg_small, &c->items,
+                            &c->results,   &c->pieces,   &c->piece_crc, &c->mpiece, &c->exp_crc,  &c->exp_isize,
+                            &c->got_crc,   &c->got_len,  &c->mstatus, &c->queue,  &c->mbs,      &c->mbcount,
+                            &c->lane_scratch, &c->crc_table};
+        for (size_t i = 0; i < sizeof(bs) / sizeof(bs[0]); i++) key.p[i] = bs[i]->p;
+        key.p[20] = d_file;
+        key.p[21] = tgt.p;
+        key.p[22] = c->stream;
+        key.p[23] = c->h_bg;
+        key.v[0] = len;
+        key.v[1] = tgt.cap;
+        key.v[2] = cap;
+        key.v[3] = sgrid;
+        key.v[4] = c->lanes;
+        key.v[5] = c->inflate_warps;
+        if (c->use_graphs) {
+            if (!c->bg_exec || std::memcmp(&key, &c->bg_key, sizeof(key)) != 0) {
+                if (c->bg_exec) cudaGraphExecDestroy(c->bg_exec);
+                c->bg_exec = nullptr;
+                cudaGraph_t g = nullptr;
+                if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                    const uint64_t l0 = c->launches;
+                    int rc = bgzf_enqueue(c, d_file, len, tgt.p, tgt.cap, sgrid, per_block, cap, err);
+                    const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+                    // kernels recorded into the graph are counted when it runs
+                    g_launches.fetch_sub(c->launches - l0);
+                    c->launches = l0;
+                    if (rc == 0 && e == cudaSuccess && g &&
+                        cudaGraphInstantiate(&c->bg_exec, g, 0) == cudaSuccess) {
+                        c->bg_key = key;
+                    } else {
+                        c->bg_exec = nullptr;
+                    }
+                    if (g) cudaGraphDestroy(g);
+                }
+                cudaGetLastError();  // a failed capture leaves no sticky error; run directly below
+            }
+            if (c->bg_exec) {
+                CK(cudaGraphLaunch(c->bg_exec, c->stream));
+                g_launches.fetch_add(BGK_KERNELS);
+                c->launches += BGK_KERNELS;
+                c->st.graph_launches++;
+                ran = true;
+            }
+        }
+#endif
+        if (!ran) {
+            int rc = bgzf_enqueue(c, d_file, len, tgt.p, tgt.cap, sgrid, per_block, cap, err);
+            if (rc) return rc;
+        }
+        kt.stop();
+        CK(cudaStreamSynchronize(c->stream));
+        c->st.inflate_ms += kt.ms();
+        const uint64_t flags = hb[2];
+        const uint32_t n_cand = ((const uint32_t*)(hb + 6))[0];
+        if (flags & (BG_CAND_OVERFLOW | BG_ITEM_OVERFLOW)) {
+            cap = std::max<uint32_t>(n_cand, (uint32_t)hb[3]) + 4096;
+            continue;
+        }
+        if (flags & BG_OUT_CAPACITY) {
+            if (tgt.grow) {
+                int rc = ensure_out(c, tgt, hb[1], 0, err);
+                if (rc) return rc;
+                continue;
+            }
+            out->total = hb[1];
+            set_err(err, RRG_ERR_CAPACITY, "output buffer too small: need %llu bytes", (unsigned long long)hb[1]);
+            return RRG_ERR_CAPACITY;
+        }
+        break;
     }
-    out->total = pos;
-    out->members = (uint32_t)nm;
-    out->consumed = nm ? ms.back().off + ms.back().size : 0;
-    int rc0 = ensure_out(c, tgt, pos, 0, err);
-    if (rc0) return rc0;
-    uint8_t* d_dst = tgt.p;
-    std::vector<ChunkResult> res;
-    int rc = launch_inflate(c, d_file, items, true, d_dst, res, nullptr, err);
-    if (rc) return rc;
+    const uint32_t nm = (uint32_t)hb[3];
+    out->total = hb[1];
+    out->members = nm;
+    out->consumed = hb[0];
+    *rem = hb[0];
+    *truncated = (hb[2] & BG_TRUNCATED) != 0;
     c->st.gpu_chunks += nm;
-    std::vector<MemberSpan> spans(nm);
-    for (size_t i = 0; i < nm; i++) {
-        const ChunkResult& r = res[i];
-        uint64_t trailer = ms[i].off + ms[i].size - 8;
+    c->st.members += nm;
+    const uint32_t* first = (const uint32_t*)(hb + 5);
+    if (first[0] != ~0u) {  // a member failed to decode
+        const uint32_t i = first[0];
+        ChunkResult r;
+        ChunkItem it;
+        CK(cudaMemcpy(&r, (const ChunkResult*)c->results.p + i, sizeof(r), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&it, (const ChunkItem*)c->items.p + i, sizeof(it), cudaMemcpyDeviceToHost));
+        const uint64_t trailer = it.in_off + it.in_len - 8;
         if (r.status == DS_OVERFLOW) {
-            set_err(err, RRG_ERR_ISIZE_MISMATCH, "ISIZE mismatch in member #%zu (trailer at byte %llu): expected %u, got %llu",
-                    i, (unsigned long long)trailer, ms[i].isize, (unsigned long long)r.n_cells);
-            err->member = (uint32_t)i;
-            err->expected = ms[i].isize;
+            set_err(err, RRG_ERR_ISIZE_MISMATCH, "ISIZE mismatch in member #%u (trailer at byte %llu): expected %u, got %llu",
+                    i, (unsigned long long)trailer, (uint32_t)it.out_cap, (unsigned long long)r.n_cells);
+            err->member = i;
+            err->expected = (uint32_t)it.out_cap;
             err->got = r.n_cells;
             err->trailer_byte = trailer;
             return RRG_ERR_ISIZE_MISMATCH;
         }
-        if (r.status != DS_OK) return status_err(err, r.status, r.msg, ms[i].off + r.err_bit / 8);
-        uint32_t tcrc = (uint32_t)r.markers, tisz = (uint32_t)(r.markers >> 32);
-        spans[i] = MemberSpan{items[i].out_off, r.n_cells, tcrc, tisz, trailer};
+        return status_err(err, r.status, r.msg, it.in_off + r.err_bit / 8);
     }
-    return check_members(c, d_dst, spans, 0, err);
+    if (first[1] != ~0u) {  // a member's CRC32 or ISIZE did not match its trailer
+        const uint32_t i = first[1];
+        ChunkItem it;
+        int32_t st = 0;
+        uint32_t got = 0, ecrc = 0, eisz = 0;
+        uint64_t glen = 0;
+        CK(cudaMemcpy(&it, (const ChunkItem*)c->items.p + i, sizeof(it), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&st, (const int32_t*)c->mstatus.p + i, 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&got, (const uint32_t*)c->got_crc.p + i, 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&glen, (const uint64_t*)c->got_len.p + i, 8, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&ecrc, (const uint32_t*)c->exp_crc.p + i, 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&eisz, (const uint32_t*)c->exp_isize.p + i, 4, cudaMemcpyDeviceToHost));
+        MemberSpan m{it.out_off, glen, ecrc, eisz, it.in_off + it.in_len - 8};
+        return member_error(err, m, i, st, got, glen);
+    }
+    return 0;
 }
 
 // ------------------------------------------------------------ whole file
 // Decode a whole gzip file at d_file (device) into d_dst. `h_file` (optional)
-// is the same bytes in host memory, used for the BGZF walk.
+// is the same bytes in host memory, used for header parsing.
 int decode_file(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_t* h_file, OutTarget& tgt, Decoded* out,
                 rrg_error* err) {
     *out = Decoded{};
@@ -1183,31 +1422,36 @@ int decode_file(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_t* 
         hp = head.data();
     }
     if (host_bgzf_size(hp, hlen) >= 0) {
-        std::vector<uint8_t> whole;
-        if (!h_file) {
-            whole.resize(len);
-            CK(cudaMemcpy(whole.data(), d_file, len, cudaMemcpyDeviceToHost));
-            h_file = whole.data();
-        }
-        std::vector<BgzfMember> ms;
-        bool trunc = false;
-        uint64_t rem = bgzf_walk(h_file, len, ms, &trunc);
         Decoded d1;
-        rc = bgzf_route(c, d_file, ms, tgt, &d1, err);
-        if (rc) {
-            out->total = d1.total;
-            return rc;
-        }
+        uint64_t rem = 0;
+        bool trunc = false;
+        rc = bgzf_route(c, d_file, len, tgt, &d1, &rem, &trunc, err);
+        out->total = d1.total;
+        if (rc) return rc;
         if (trunc) {
             set_err(err, RRG_ERR_TRUNCATED, "truncated gzip stream");
             return RRG_ERR_TRUNCATED;
         }
-        out->total = d1.total;
         out->members = d1.members;
         if (rem < len) {
+            // what follows the BGZF members is an ordinary member stream
+            std::vector<uint8_t> rh;
+            const uint8_t* rp = h_file ? h_file + rem : nullptr;
+            uint64_t rl = len - rem;
+            if (!rp) {
+                rl = std::min<uint64_t>(rl, 1 << 16);
+                rh.resize(rl);
+                CK(cudaMemcpy(rh.data(), d_file + rem, rl, cudaMemcpyDeviceToHost));
+                rp = rh.data();
+            }
             size_t hl;
             int detail;
-            int st = host_parse_header(h_file + rem, len - rem, &hl, &detail);
+            int st = host_parse_header(rp, rl, &hl, &detail);
+            if (st == DS_TRUNCATED && rl < len - rem) {
+                rh.resize(len - rem);
+                CK(cudaMemcpy(rh.data(), d_file + rem, len - rem, cudaMemcpyDeviceToHost));
+                st = host_parse_header(rh.data(), len - rem, &hl, &detail);
+            }
             if (st) return status_err(err, st, detail, rem);
             Decoded d2;
             rc = member_route(c, d_file, len, rem + hl, tgt, d1.total, d1.members, &d2, err);
@@ -1320,6 +1564,111 @@ int decode_host_impl(rrg_ctx* c, const uint8_t* data, size_t len, rrg_sink_fn si
     return rc;
 }
 
+// ------------------------------------------------------------ batches
+// Independent gzip files (or members) already on the device, each with its
+// own output range. Headers are parsed on the device; BGZF files take the
+// BGZF route one by one; every other file is a job of the member route, in
+// waves whose reserved output cells fit the device budget.
+int batch_impl(rrg_ctx* c, const uint8_t* d_in, const uint64_t* in_off, const uint64_t* in_len, uint8_t* d_out,
+               const uint64_t* out_off, const uint64_t* out_cap, uint64_t* out_len, int32_t* status, size_t n,
+               rrg_error* err) {
+    int rc = upload_tables(c, err);
+    if (rc || !n) return rc;
+    // ---- headers, BGZF sniff and the trailers' size hints, one thread per file
+    CK(dgrow(c->sniff, n * 40));
+    uint8_t* sb = (uint8_t*)c->sniff.p;
+    uint64_t* d_off = (uint64_t*)sb;
+    uint64_t* d_len = d_off + n;
+    uint64_t* d_body = d_len + n;
+    int64_t* d_bgzf = (int64_t*)(d_body + n);
+    int32_t* d_st = (int32_t*)(d_bgzf + n);
+    int32_t* d_msg = d_st + n;
+    uint32_t* d_isz = (uint32_t*)(d_msg + n);
+    CK(cudaMemcpyAsync(d_off, in_off, n * 8, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(d_len, in_len, n * 8, cudaMemcpyHostToDevice, c->stream));
+    SniffArgs SA{d_in, d_off, d_len, (uint32_t)n, d_st, d_msg, d_body, d_bgzf, d_isz};
+    RRG_LAUNCH(k_sniff, (uint32_t)std::min<size_t>((n + 255) / 256, (size_t)c->n_sm * 4), 256, 0, c->stream, SA);
+    LAUNCHED(c);
+    std::vector<uint64_t> body(n);
+    std::vector<int64_t> bg(n);
+    std::vector<int32_t> hst(n), hmsg(n);
+    std::vector<uint32_t> isz(n);
+    CK(cudaMemcpyAsync(body.data(), d_body, n * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(bg.data(), d_bgzf, n * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(hst.data(), d_st, n * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(hmsg.data(), d_msg, n * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(isz.data(), d_isz, n * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::vector<MemberJob> jobs;
+    std::vector<size_t> job_item;
+    for (size_t i = 0; i < n; i++) {
+        out_len[i] = 0;
+        status[i] = RRG_OK;
+        if (in_len[i] == 0) {
+            status[i] = RRG_ERR_TRUNCATED;
+            continue;
+        }
+        if (bg[i] >= 0) {  // BGZF file: its own device walk and decode
+            rrg_error e{};
+            OutTarget t{d_out + out_off[i], out_cap[i], false};
+            Decoded d;
+            int r = decode_file(c, d_in + in_off[i], in_len[i], nullptr, t, &d, &e);
+            if (r == RRG_ERR_CUDA || r == RRG_ERR_OUT_OF_MEMORY) {
+                if (err) *err = e;
+                return r;
+            }
+            status[i] = r;
+            out_len[i] = d.total;
+            continue;
+        }
+        if (hst[i]) {
+            rrg_error e{};
+            status[i] = status_err(&e, hst[i], hmsg[i], 0);
+            continue;
+        }
+        MemberJob j;
+        j.file_off = in_off[i];
+        j.len = in_len[i];
+        j.body_off = body[i];
+        j.dst_off = out_off[i];
+        j.dst_cap = out_cap[i];
+        const uint64_t blen = j.len - j.body_off;
+        // ISIZE of the (last) member: a size hint for the reserved cells
+        if (isz[i] && blen)
+            j.expand = std::min(c->expand, std::max(1.05, 1.25 * (double)isz[i] / (double)blen + 0.05));
+        jobs.push_back(j);
+        job_item.push_back(i);
+    }
+    // ---- waves: reserved cells (2 bytes each) within the budget and free memory
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    const uint64_t budget = std::max<uint64_t>(
+        8ull << 20, std::min<uint64_t>(c->cfg.hbm_budget_bytes, (uint64_t)((free_b + c->cells.cap) * 0.6)));
+    OutTarget tgt{d_out, ~0ull, false};
+    for (size_t a = 0; a < jobs.size();) {
+        size_t b = a;
+        uint64_t need = 0;
+        while (b < jobs.size()) {
+            const MemberJob& j = jobs[b];
+            const uint64_t blen = j.len - j.body_off;
+            const uint64_t cells = (uint64_t)((double)blen * (j.expand > 0 ? j.expand : c->expand) * 1.6) + (1u << 20);
+            if (b > a && need + 2 * cells > budget) break;
+            need += 2 * cells;
+            b++;
+        }
+        std::vector<MemberJob> wave(jobs.begin() + a, jobs.begin() + b);
+        rc = members_route(c, d_in, wave, tgt, err);
+        if (rc) return rc;
+        for (size_t q = 0; q < wave.size(); q++) {
+            const size_t i = job_item[a + q];
+            status[i] = wave[q].rc;
+            out_len[i] = wave[q].out.total;
+        }
+        a = b;
+    }
+    return 0;
+}
+
 }  // namespace
 
 // ====================================================================== C ABI
@@ -1375,11 +1724,16 @@ void rrg_gpu_destroy(rrg_ctx* c) {
     DBuf* bufs[] = {&c->cand, &c->ncand, &c->vflag, &c->lane_scratch, &c->win, &c->items,  &c->results, &c->order,     &c->queue,    &c->mbs,      &c->mbcount,   &c->cells,
                     &c->out,    &c->targets, &c->limits,    &c->found,    &c->next_lut, &c->chunks,    &c->tiles,
                     &c->rerr,   &c->markers, &c->crc_table, &c->pieces,   &c->piece_crc, &c->mpiece,   &c->exp_crc,
-                    &c->exp_isize, &c->got_crc, &c->got_len, &c->mstatus, &c->comp};
+                    &c->exp_isize, &c->got_crc, &c->got_len, &c->mstatus, &c->comp, &c->bg_bcount, &c->bg_bbase,
+                    &c->bg_coff, &c->bg_csize, &c->bg_small, &c->sniff};
+#ifndef RRG_EMU
+    if (c->bg_exec) cudaGraphExecDestroy(c->bg_exec);
+#endif
     for (DBuf* b : bufs)
         if (b->p) cudaFree(b->p);
     for (auto& p : c->h_stage)
         if (p) cudaFreeHost(p);
+    if (c->h_bg) cudaFreeHost(c->h_bg);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
 }
@@ -1478,63 +1832,19 @@ int rrg_gpu_decode_batch(rrg_ctx* c, const uint8_t* d_in, const uint64_t* in_off
     c->st = rrg_stats{};
     c->launches = 0;
     c->stream = stream ? (cudaStream_t)stream : c->own_stream;
-    int rc = upload_tables(c, err);
-    if (rc) {
-        c->stream = c->own_stream;
-        return rc;
-    }
-    std::vector<ChunkItem> items(n);
-    for (size_t i = 0; i < n; i++) {
-        items[i] = ChunkItem{in_off[i], in_len[i], 0, ~0ull, out_off[i], out_cap[i], ITEM_ONE_MEMBER, (uint32_t)i};
-        c->st.compressed_bytes += in_len[i];
-    }
-    std::vector<ChunkResult> res;
-    rc = launch_inflate(c, d_in, items, true, d_out, res, nullptr, err);
+    int rc = batch_impl(c, d_in, in_off, in_len, d_out, out_off, out_cap, out_len, status, n, err);
     int first_bad = RRG_OK;
     if (!rc) {
-        std::vector<MemberSpan> spans;
-        std::vector<size_t> idx;
         for (size_t i = 0; i < n; i++) {
-            const ChunkResult& r = res[i];
-            out_len[i] = r.n_cells;
-            if (r.status == DS_OVERFLOW) status[i] = RRG_ERR_CAPACITY;
-            else if (r.status != DS_OK) {
-                rrg_error tmp;
-                status[i] = status_err(&tmp, r.status, r.msg, in_off[i] + r.err_bit / 8);
-            } else {
-                status[i] = RRG_OK;
-                spans.push_back(MemberSpan{out_off[i], r.n_cells, (uint32_t)r.markers, (uint32_t)(r.markers >> 32),
-                                           in_off[i] + in_len[i] - 8});
-                idx.push_back(i);
-            }
-        }
-        // per-member CRC/ISIZE: check each independently
-        if (!spans.empty()) {
-            rrg_error tmp;
-            int crc_rc = check_members(c, d_out, spans, 0, &tmp);
-            if (crc_rc == RRG_ERR_CRC_MISMATCH || crc_rc == RRG_ERR_ISIZE_MISMATCH) {
-                // find every failing member
-                std::vector<int32_t> stv(spans.size());
-                cudaMemcpy(stv.data(), c->mstatus.p, spans.size() * 4, cudaMemcpyDeviceToHost);
-                for (size_t j = 0; j < spans.size(); j++)
-                    if (stv[j] == DS_CRC) status[idx[j]] = RRG_ERR_CRC_MISMATCH;
-                    else if (stv[j] == DS_ISIZE) status[idx[j]] = RRG_ERR_ISIZE_MISMATCH;
-            } else if (crc_rc) {
-                rc = crc_rc;
-                if (err) *err = tmp;
-            }
-        }
-        for (size_t i = 0; i < n && !rc; i++)
-            if (status[i] != RRG_OK) {
+            c->st.compressed_bytes += in_len[i];
+            if (status[i] == RRG_OK) c->st.uncompressed_bytes += out_len[i];
+            else if (first_bad == RRG_OK) {
                 first_bad = status[i];
                 set_err(err, status[i], "batch item %zu failed with status %d", i, status[i]);
-                break;
             }
-        for (size_t i = 0; i < n; i++)
-            if (status[i] == RRG_OK) c->st.uncompressed_bytes += out_len[i];
+        }
     }
     c->stream = c->own_stream;
-    c->st.gpu_chunks = n;
     c->st.kernel_launches = c->launches;
     c->st.total_ms = now_ms() - t_all;
     if (stats) *stats = c->st;

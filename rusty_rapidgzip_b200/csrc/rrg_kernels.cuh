@@ -264,6 +264,7 @@ struct InflateArgs {
     const ChunkItem* items;
     ChunkResult* results;
     uint32_t n_items;
+    const uint32_t* n_items_dev;  // when set, the item count is read here (device-built work lists)
     const uint32_t* order;   // optional permutation of the work queue (largest first)
     uint32_t* queue;         // work-queue head
     void* out;               // cell arena (u16) or byte output (u8)
@@ -907,7 +908,7 @@ __global__ void __launch_bounds__(128, RRG_INFLATE_MIN_BLOCKS) k_inflate(Inflate
         uint32_t idx = 0;
         if (lane == 0) idx = atomicAdd(A.queue, 1u);
         idx = (uint32_t)bcast32((int32_t)idx);
-        if (idx >= A.n_items) break;
+        if (idx >= (A.n_items_dev ? *A.n_items_dev : A.n_items)) break;
         uint32_t item = A.order ? A.order[idx] : idx;
         inflate_item<CellT>(S, A, item, lane);
     }
@@ -1384,7 +1385,7 @@ __global__ void __launch_bounds__(LANE_THREADS) k_inflate_lanes(InflateArgs A, L
     LaneScratch* scr = scratch + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     for (;;) {
         const uint32_t idx = atomicAdd(A.queue, 1u);
-        if (idx >= A.n_items) break;
+        if (idx >= (A.n_items_dev ? *A.n_items_dev : A.n_items)) break;
         lane_item<CellT>(A, A.order ? A.order[idx] : idx, T, scr, K);
     }
 }
@@ -2143,6 +2144,7 @@ struct CrcArgs {
     uint32_t n_pieces;
     uint32_t* piece_crc;   // raw CRC per piece
     const uint32_t* table; // 8 x 256 slice-by-8 table
+    const uint32_t* n_dev; // when set, the piece count is read here
 };
 
 // One CTA per piece; each warp takes a contiguous 1/8th, each lane a
@@ -2154,7 +2156,8 @@ __global__ void __launch_bounds__(CRC_THREADS) k_crc_pieces(CrcArgs A) {
     for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) T[i >> 8][i & 255] = A.table[i];
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (uint32_t pi = blockIdx.x; pi < A.n_pieces; pi += gridDim.x) {
+    const uint32_t n_pieces = A.n_dev ? *A.n_dev : A.n_pieces;
+    for (uint32_t pi = blockIdx.x; pi < n_pieces; pi += gridDim.x) {
         const CrcPiece pc = A.pieces[pi];
         const uint64_t per_thread = (pc.len + blockDim.x - 1) / blockDim.x;
         const uint64_t seg = (per_thread + 7) & ~7ull;
@@ -2209,42 +2212,368 @@ struct CrcMemberArgs {
     uint32_t* got_crc;
     uint64_t* got_len;
     int32_t* status;  // DS_OK / DS_CRC / DS_ISIZE
+    const uint32_t* n_dev;  // when set, the member count is read here
 };
 
 // One warp per member: fold its pieces in order, finalise, compare with the trailer.
 __global__ void k_crc_members(CrcMemberArgs A) {
     const int lane = threadIdx.x & 31;
-    const uint32_t m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (m >= A.n_members) return;  // warp-uniform
-    const uint32_t p0 = A.member_piece_start[m], p1 = A.member_piece_start[m + 1];
-    const uint32_t np = p1 - p0;
-    const uint32_t per = (np + 31) / 32;
-    uint32_t b = p0 + lane * per, e = b + per;
-    if (b > p1) b = p1;
-    if (e > p1) e = p1;
-    uint32_t c = 0;
-    uint64_t len = 0;
-    for (uint32_t i = b; i < e; i++) {
-        uint64_t l = A.pieces[i].len;
-        c = (l ? gf2_mulmod(c, xpow8n(l)) : c) ^ A.piece_crc[i];
-        len += l;
-    }
-    for (int o = 1; o < 32; o <<= 1) {
-        uint32_t oc = __shfl_down_sync(FULLMASK, c, o);
-        uint64_t ol = __shfl_down_sync(FULLMASK, len, o);
-        if ((lane & (2 * o - 1)) == 0 && lane + o < 32) {
-            c = (ol ? gf2_mulmod(c, xpow8n(ol)) : c) ^ oc;
-            len += ol;
+    const uint32_t n_members = A.n_dev ? *A.n_dev : A.n_members;
+    for (uint32_t m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; m < n_members;
+         m += (gridDim.x * blockDim.x) >> 5) {  // warp-uniform
+        const uint32_t p0 = A.member_piece_start[m], p1 = A.member_piece_start[m + 1];
+        const uint32_t np = p1 - p0;
+        const uint32_t per = (np + 31) / 32;
+        uint32_t b = p0 + lane * per, e = b + per;
+        if (b > p1) b = p1;
+        if (e > p1) e = p1;
+        uint32_t c = 0;
+        uint64_t len = 0;
+        for (uint32_t i = b; i < e; i++) {
+            uint64_t l = A.pieces[i].len;
+            c = (l ? gf2_mulmod(c, xpow8n(l)) : c) ^ A.piece_crc[i];
+            len += l;
+        }
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t oc = __shfl_down_sync(FULLMASK, c, o);
+            uint64_t ol = __shfl_down_sync(FULLMASK, len, o);
+            if ((lane & (2 * o - 1)) == 0 && lane + o < 32) {
+                c = (ol ? gf2_mulmod(c, xpow8n(ol)) : c) ^ oc;
+                len += ol;
+            }
+        }
+        if (lane == 0) {
+            uint32_t crc = c ^ (len ? gf2_mulmod(0xffffffffu, xpow8n(len)) : 0xffffffffu) ^ 0xffffffffu;
+            A.got_crc[m] = crc;
+            A.got_len[m] = len;
+            int32_t st = DS_OK;
+            if (crc != A.expected_crc[m]) st = DS_CRC;
+            else if ((uint32_t)len != A.expected_isize[m]) st = DS_ISIZE;
+            A.status[m] = st;
         }
     }
+}
+
+// ------------------------------------------------------- gzip header sniffing
+// gzip.rs:311-351 parse_bgzf_block_size at byte `at` of s: the member size
+// from the BC extra subfield (BSIZE + 1), or -1 (None).
+__device__ int64_t dev_bgzf_size(const Src& s, uint64_t at) {
+    const uint64_t n = s.hi - s.lo;
+    if (at + 12 > n) return -1;
+    if (src_byte(s, at) != 0x1f || src_byte(s, at + 1) != 0x8b || src_byte(s, at + 2) != 8 || !(src_byte(s, at + 3) & 4))
+        return -1;
+    const uint64_t xlen = src_byte(s, at + 10) | (src_byte(s, at + 11) << 8);
+    if (at + 12 + xlen > n) return -1;
+    uint64_t p = at + 12;
+    const uint64_t end = p + xlen;
+    while (p + 4 <= end) {
+        const uint64_t slen = src_byte(s, p + 2) | (src_byte(s, p + 3) << 8);
+        if (p + 4 + slen > end) return -1;
+        if (src_byte(s, p) == 'B' && src_byte(s, p + 1) == 'C' && slen == 2)
+            return (int64_t)(src_byte(s, p + 4) | (src_byte(s, p + 5) << 8)) + 1;
+        p += 4 + slen;
+    }
+    return -1;
+}
+
+// Per file of a batch: header status and length (gzip.rs:252-300), the BGZF
+// size of its first member (or -1), and the trailer's ISIZE (a size hint).
+struct SniffArgs {
+    const uint8_t* base;
+    const uint64_t* off;
+    const uint64_t* len;
+    uint32_t n;
+    int32_t* status;
+    int32_t* msg;
+    uint64_t* body_off;
+    int64_t* bgzf;
+    uint32_t* isize;
+};
+
+__global__ void k_sniff(SniffArgs A) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {
+        const Src s = make_src(A.base + A.off[i], A.len[i]);
+        uint64_t hl = 0;
+        int msg = 0;
+        A.status[i] = dev_parse_header(s, 0, &hl, &msg);
+        A.msg[i] = msg;
+        A.body_off[i] = hl;
+        A.bgzf[i] = dev_bgzf_size(s, 0);
+        A.isize[i] = A.len[i] >= 4 ? le32_at(s, A.len[i] - 4) : 0u;
+    }
+}
+
+// ------------------------------------------------------- BGZF member walk
+// The reference walks BGZF members one header at a time (pipeline.rs:1524-1541).
+// Here every byte offset is tested for a BGZF member header in parallel, the
+// hits are compacted in file order (count, prefix, collect), and one warp
+// follows the chain offset -> offset + size through the sorted hits, 32 at a
+// time, writing the per-member work items, CRC pieces and trailer values.
+// Hits that are not on the chain (header-like bytes inside compressed data)
+// are skipped. Nothing returns to the host between these kernels and the
+// decode that follows, so the whole BGZF decode is one captured graph.
+constexpr int BG_THREADS = 256;
+constexpr int BG_SPAN = 16;                      // bytes per thread per step
+constexpr int BG_STEP = BG_THREADS * BG_SPAN;    // bytes per block per step
+
+struct BgzfScanArgs {
+    const uint8_t* file;
+    uint64_t len;
+    uint64_t per_block;      // bytes per block (a multiple of BG_STEP)
+    uint32_t* block_count;   // [gridDim.x]
+    uint32_t* block_base;    // [gridDim.x + 1]
+    uint64_t* cand_off;
+    uint32_t* cand_size;
+    uint32_t cap;
+    uint32_t* n_cand;
+};
+
+// hits in this thread's BG_SPAN bytes starting at p0, as a bit mask; sizes in sz[]
+__device__ __forceinline__ uint32_t bg_hits(const Src& s, uint64_t p0, uint64_t len, uint32_t* sz) {
+    uint32_t m = 0;
+#pragma unroll
+    for (int k = 0; k < BG_SPAN; k++) {
+        const uint64_t p = p0 + k;
+        if (p < len && src_byte(s, p) == 0x1f && src_byte(s, p + 1) == 0x8b) {
+            const int64_t z = dev_bgzf_size(s, p);
+            if (z >= 0) {
+                m |= 1u << k;
+                sz[k] = (uint32_t)z;
+            }
+        }
+    }
+    return m;
+}
+
+__global__ void __launch_bounds__(BG_THREADS) k_bgzf_count(BgzfScanArgs A) {
+    __shared__ uint32_t tot;
+    if (threadIdx.x == 0) tot = 0;
+    __syncthreads();
+    const Src s = make_src(A.file, A.len);
+    const uint64_t b0 = (uint64_t)blockIdx.x * A.per_block;
+    const uint64_t b1 = b0 + A.per_block < A.len ? b0 + A.per_block : A.len;
+    uint32_t mine = 0;
+    uint32_t sz[BG_SPAN];
+    for (uint64_t p = b0 + (uint64_t)threadIdx.x * BG_SPAN; p < b1; p += BG_STEP)
+        mine += __popc(bg_hits(s, p, b1, sz));
+    mine = warp_sum(mine);
+    if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&tot, mine);
+    __syncthreads();
+    if (threadIdx.x == 0) A.block_count[blockIdx.x] = tot;
+}
+
+// one block: exclusive prefix of the per-block counts
+__global__ void __launch_bounds__(1024) k_bgzf_prefix(BgzfScanArgs A, uint32_t n_blocks) {
+    __shared__ uint32_t wsum[32];
+    __shared__ uint32_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t base = 0; base < n_blocks; base += blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t v = i < n_blocks ? A.block_count[i] : 0u;
+        uint32_t x = v;  // inclusive scan in the warp
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(FULLMASK, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t w = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0u;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(FULLMASK, w, o);
+                if (lane >= o) w += y;
+            }
+            wsum[lane] = w;  // inclusive over warps
+        }
+        __syncthreads();
+        const uint32_t before = carry + (warp ? wsum[warp - 1] : 0u) + x - v;
+        if (i < n_blocks) A.block_base[i] = before;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = before + v;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        A.block_base[n_blocks] = carry;
+        *A.n_cand = carry;
+    }
+}
+
+__global__ void __launch_bounds__(BG_THREADS) k_bgzf_collect(BgzfScanArgs A) {
+    __shared__ uint32_t wsum[BG_THREADS / 32];
+    __shared__ uint32_t run;
+    if (threadIdx.x == 0) run = A.block_base[blockIdx.x];
+    __syncthreads();
+    const Src s = make_src(A.file, A.len);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t b0 = (uint64_t)blockIdx.x * A.per_block;
+    const uint64_t b1 = b0 + A.per_block < A.len ? b0 + A.per_block : A.len;
+    uint32_t sz[BG_SPAN];
+    for (uint64_t q = b0; q < b1; q += BG_STEP) {  // block-uniform trip count
+        const uint64_t p = q + (uint64_t)threadIdx.x * BG_SPAN;
+        const uint32_t m = p < b1 ? bg_hits(s, p, b1, sz) : 0u;
+        const uint32_t v = __popc(m);
+        uint32_t x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(FULLMASK, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[warp] = x;
+        __syncthreads();
+        uint32_t wb = 0, tot = 0;
+        for (int w = 0; w < BG_THREADS / 32; w++) {
+            if (w < warp) wb += wsum[w];
+            tot += wsum[w];
+        }
+        uint32_t at = run + wb + x - v;
+        for (uint32_t mm = m; mm; mm &= mm - 1) {
+            const int k = __ffs((int)mm) - 1;
+            if (at < A.cap) {
+                A.cand_off[at] = p + (uint64_t)k;
+                A.cand_size[at] = sz[k];
+            }
+            at++;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) run += tot;
+        __syncthreads();
+    }
+}
+
+enum : uint32_t { BG_TRUNCATED = 1, BG_CAND_OVERFLOW = 2, BG_ITEM_OVERFLOW = 4, BG_OUT_CAPACITY = 8 };
+
+struct BgzfChainArgs {
+    const uint8_t* file;
+    uint64_t len;
+    const uint64_t* cand_off;
+    const uint32_t* cand_size;
+    const uint32_t* n_cand;
+    uint32_t cap;
+    ChunkItem* items;
+    uint32_t item_cap;
+    CrcPiece* pieces;
+    uint32_t* mpiece;        // member -> first piece (one piece per member), n + 1 entries
+    uint32_t* exp_crc;
+    uint32_t* exp_isize;
+    uint64_t out_cap;
+    uint32_t* n_members;     // members to decode (0 when they do not fit)
+    uint64_t* info;          // [0] end of the member chain, [1] output bytes, [2] BG_* flags, [3] members on the chain
+};
+
+// One warp. Member k+1 starts where member k ends (pipeline.rs:1524-1541).
+__global__ void __launch_bounds__(32) k_bgzf_chain(BgzfChainArgs A) {
+    const int lane = threadIdx.x & 31;
+    const Src s = make_src(A.file, A.len);
+    uint32_t flags = 0;
+    uint32_t n = *A.n_cand;
+    if (n > A.cap) {
+        flags |= BG_CAND_OVERFLOW;
+        n = A.cap;
+    }
+    uint64_t expected = 0, total = 0;
+    uint32_t i = 0, m = 0;
+    while (expected < A.len) {
+        // first hit at or after `expected`
+        bool found = false;
+        while (i < n) {
+            const uint32_t j = i + lane;
+            const bool ge = j >= n || A.cand_off[j] >= expected;
+            const uint32_t bal = __ballot_sync(FULLMASK, ge);
+            if (bal) {
+                i += __ffs((int)bal) - 1;
+                found = true;
+                break;
+            }
+            i += 32;
+        }
+        if (!found || i >= n || A.cand_off[i] != expected) break;  // no member here: the chain ends
+        const uint32_t j = i + lane;
+        const bool ok = j < n;
+        const uint64_t off = ok ? A.cand_off[j] : 0;
+        const uint64_t sz = ok ? A.cand_size[j] : 0;
+        const uint64_t prev_end = __shfl_up_sync(FULLMASK, off + sz, 1);
+        const bool link = ok && (lane == 0 ? off == expected : off == prev_end);
+        const bool fits = off + sz <= A.len;
+        const uint32_t acc = __ballot_sync(FULLMASK, link && fits);
+        const uint32_t k = ~acc ? (uint32_t)(__ffs((int)~acc) - 1) : 32u;  // leading run of chained hits
+        const uint32_t trunc = __ballot_sync(FULLMASK, link && !fits);
+        const bool mine = (uint32_t)lane < k;
+        uint32_t isz = 0, crc = 0;
+        if (mine && sz >= 8) {
+            crc = le32_at(s, off + sz - 8);
+            isz = le32_at(s, off + sz - 4);
+        }
+        uint64_t x = isz;  // inclusive scan of member output sizes
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t y = __shfl_up_sync(FULLMASK, x, o);
+            if (lane >= o) x += y;
+        }
+        if (mine && m + lane < A.item_cap) {
+            const uint32_t idx = m + lane;
+            ChunkItem it;
+            it.in_off = off;
+            it.in_len = sz;
+            it.start_bit = 0;
+            it.end_hint = ~0ull;
+            it.out_off = total + x - isz;
+            it.out_cap = isz;
+            it.flags = ITEM_ONE_MEMBER;
+            it.id = idx;
+            A.items[idx] = it;
+            A.pieces[idx] = CrcPiece{total + x - isz, isz};
+            A.mpiece[idx] = idx;
+            A.exp_crc[idx] = crc;
+            A.exp_isize[idx] = isz;
+        }
+        if (k) {
+            total += __shfl_sync(FULLMASK, x, (int)k - 1);
+            expected = __shfl_sync(FULLMASK, off + sz, (int)k - 1);
+            m += k;
+            i += k;
+        }
+        // the hit right after the run sits where the chain expects a member
+        // but ends past the file: truncated (the host walk's `pos + sz > len`)
+        if (k < 32 && ((trunc >> k) & 1u)) {
+            flags |= BG_TRUNCATED;
+            break;
+        }
+    }
+    if (m > A.item_cap) flags |= BG_ITEM_OVERFLOW;
+    if (total > A.out_cap) flags |= BG_OUT_CAPACITY;
     if (lane == 0) {
-        uint32_t crc = c ^ (len ? gf2_mulmod(0xffffffffu, xpow8n(len)) : 0xffffffffu) ^ 0xffffffffu;
-        A.got_crc[m] = crc;
-        A.got_len[m] = len;
-        int32_t st = DS_OK;
-        if (crc != A.expected_crc[m]) st = DS_CRC;
-        else if ((uint32_t)len != A.expected_isize[m]) st = DS_ISIZE;
-        A.status[m] = st;
+        const uint32_t nm = (flags & (BG_CAND_OVERFLOW | BG_ITEM_OVERFLOW | BG_OUT_CAPACITY)) ? 0u : m;
+        *A.n_members = nm;
+        if (nm < A.item_cap) A.mpiece[nm] = nm;
+        A.info[0] = expected;
+        A.info[1] = total;
+        A.info[2] = flags;
+        A.info[3] = m;
+    }
+}
+
+// After the decode: every member's CRC piece covers what was decoded (ISIZE
+// was only its slot size) and is checked against the trailer that followed
+// its deflate stream, as one-member decoding reads it.
+__global__ void k_bgzf_fix(const ChunkResult* res, CrcPiece* pieces, uint32_t* exp_crc, uint32_t* exp_isize,
+                           const uint32_t* n_members) {
+    const uint32_t n = *n_members;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const ChunkResult r = res[i];
+        pieces[i].len = r.status == DS_OK ? r.n_cells : 0;
+        exp_crc[i] = (uint32_t)r.markers;
+        exp_isize[i] = (uint32_t)(r.markers >> 32);
+    }
+}
+
+// First member (in file order) whose decode failed -> first[0], and first
+// member whose CRC32/ISIZE failed -> first[1] (both stay ~0 when none did).
+__global__ void k_bgzf_first_bad(const ChunkResult* res, const int32_t* crc_status, const uint32_t* n_members,
+                                 uint32_t* first) {
+    const uint32_t n = *n_members;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (res[i].status != DS_OK) atomicMin(&first[0], i);
+        else if (crc_status[i] != DS_OK) atomicMin(&first[1], i);
     }
 }
 

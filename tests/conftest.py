@@ -4,6 +4,8 @@ import os
 import subprocess
 import sys
 
+import numpy as np
+
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -106,3 +108,24 @@ def gpu_decoder_factory(gpu_lib):
     yield make
     for d in made:
         d.close()
+
+
+def bgzf_cases():
+    """BGZF inputs that exercise the device member walk: chains longer than a
+    warp's 32-hit step, an EOF block, header-like bytes stored verbatim inside
+    members (hits that are not on the chain), a plain member after the BGZF
+    members, truncation inside a member and a corrupt trailer CRC."""
+    from rusty_rapidgzip_b200 import workloads as W
+    rng = np.random.default_rng(7)
+    small = W.bgzf(W.fastq_like(70_000, 3), 5, block=1000)  # ~70 members
+    eof = bytes.fromhex("1f8b08040000000000ff0600424302001b0003000000000000000000")
+    inner = W.bgzf(rng.integers(0, 256, 3000, dtype=np.uint8).tobytes(), 1, block=700)
+    fake = W.bgzf(inner * 3, 0, block=4000)  # stored blocks: inner headers appear verbatim
+    plain = gzip_cli(b"trailing plain member " * 50)
+    cut = small[: len(small) - 300]
+    bad = bytearray(small)
+    m0 = int.from_bytes(bad[16:18], "little") + 1  # first member's size
+    m1 = m0 + int.from_bytes(bad[m0 + 16:m0 + 18], "little") + 1
+    bad[m1 - 8] ^= 0x40  # second member's CRC
+    return {"chain": small + eof, "false-headers": fake, "then-plain": small + plain, "truncated": cut,
+            "crc": bytes(bad)}

@@ -127,6 +127,12 @@ inline T __shfl_xor_sync(unsigned, T v, int m) {
     return emu_exchange(v, (int)(emu::t_tid.x & 31) ^ m);
 }
 template <class T>
+inline T __shfl_up_sync(unsigned, T v, unsigned d) {
+    int lane = emu::t_tid.x & 31;
+    int src = lane - (int)d >= 0 ? lane - (int)d : lane;
+    return emu_exchange(v, src);
+}
+template <class T>
 inline T __shfl_down_sync(unsigned, T v, unsigned d) {
     int lane = emu::t_tid.x & 31;
     int src = lane + (int)d < 32 ? lane + (int)d : lane;
@@ -184,6 +190,12 @@ inline unsigned long long atomicAdd(unsigned long long* p, unsigned long long v)
     return __atomic_fetch_add(p, v, __ATOMIC_SEQ_CST);
 }
 inline unsigned atomicOr(unsigned* p, unsigned v) { return __atomic_fetch_or(p, v, __ATOMIC_SEQ_CST); }
+inline unsigned atomicMin(unsigned* p, unsigned v) {
+    unsigned cur = __atomic_load_n(p, __ATOMIC_SEQ_CST);
+    while (v < cur && !__atomic_compare_exchange_n(p, &cur, v, false, __ATOMIC_SEQ_CST, __ATOMIC_SEQ_CST)) {
+    }
+    return cur;
+}
 inline unsigned atomicCAS(unsigned* p, unsigned cmp, unsigned v) {
     __atomic_compare_exchange_n(p, &cmp, v, false, __ATOMIC_SEQ_CST, __ATOMIC_SEQ_CST);
     return cmp;
@@ -199,6 +211,11 @@ inline cudaError_t cudaFree(void* p) {
     return cudaSuccess;
 }
 inline cudaError_t cudaMallocHost(void** p, size_t n) { return cudaMalloc(p, n); }
+inline cudaError_t cudaMemGetInfo(size_t* free_b, size_t* total_b) {  // a nominal 8 GiB device
+    *free_b = 8ull << 30;
+    *total_b = 8ull << 30;
+    return cudaSuccess;
+}
 inline cudaError_t cudaFreeHost(void* p) { return cudaFree(p); }
 inline cudaError_t cudaMemcpy(void* d, const void* s, size_t n, cudaMemcpyKind) {
     if (n) std::memmove(d, s, n);

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import oracle
-from conftest import GOLDEN, gzip_cli, sha256
+from conftest import GOLDEN, bgzf_cases, gzip_cli, sha256
 from rusty_rapidgzip_b200 import workloads as W
 
 
@@ -116,3 +116,78 @@ def test_noalloc_crc_emulated():
     for n in (0, 1, 300_001, (256 << 10) * 3 + 7):
         data = np.random.default_rng(n).integers(0, 256, n, dtype=np.uint8)
         assert crc32_noalloc(haddr(data) if n else 1, n, lib=lib) == zlib.crc32(data.tobytes())
+
+
+@pytest.mark.parametrize("case", ["chain", "false-headers", "then-plain", "truncated", "crc"])
+def test_bgzf_device_walk(emu_decoder_factory, case):
+    data = bgzf_cases()[case]
+    d = emu_decoder_factory()
+    try:
+        want = oracle.read_gz(data, 2)
+    except oracle.OracleError as oe:
+        from rusty_rapidgzip_b200 import RrgError
+        with pytest.raises(RrgError) as ge:
+            d.decompress(data)
+        assert (ge.value.code, ge.value.member, ge.value.trailer_byte) == (oe.code, oe.member, oe.trailer_byte)
+        return
+    assert d.decompress(data) == want
+
+
+def batch_items():
+    """Files for one batch: a multi-chunk member, small single-chunk members,
+    concatenated members, a BGZF file, a file with a bad CRC and a file whose
+    output range is too small (capacity status)."""
+    big_raw, big = W.config0(600_000, seed=5)
+    small_raw = b"small file " * 300
+    cat_raw = b"alpha" * 100 + b"beta" * 2000
+    bg_raw = W.fastq_like(40_000, 6)
+    bad = bytearray(gzip_cli(b"corrupt me " * 100))
+    bad[-8] ^= 1
+    items = [(big_raw, big, len(big_raw)), (small_raw, gzip_cli(small_raw), len(small_raw)),
+             (cat_raw, gzip_cli(b"alpha" * 100) + gzip_cli(b"beta" * 2000), len(cat_raw)),
+             (bg_raw, W.bgzf(bg_raw, 5, block=5000), len(bg_raw)),
+             (None, bytes(bad), 2000), (small_raw, gzip_cli(small_raw), 100)]
+    return items
+
+
+def run_batch(d, items, dev):
+    blobs = [gz for _, gz, _ in items]
+    offs = np.cumsum([0] + [len(b) for b in blobs])[:-1].tolist()
+    caps = [cap for _, _, cap in items]
+    ooffs = np.cumsum([0] + caps)[:-1].tolist()
+    din, dout, host = dev(b"".join(blobs), sum(caps) + 64)
+    lens, status, st = d.decode_batch(din, offs, [len(b) for b in blobs], dout, ooffs, caps)
+    out = host()
+    return [out[o:o + n] for o, n in zip(ooffs, lens)], lens, status
+
+
+def expected_status(gz):
+    try:
+        oracle.read_gz(gz, 2)
+        return 0
+    except oracle.OracleError as e:
+        return e.code
+
+
+@pytest.mark.parametrize("budget", [0, 1], ids=["one-wave", "waves"])
+def test_batch_mixed(emu_decoder_factory, budget):
+    """budget 1: the smallest wave size, so the files go through several waves."""
+    items = batch_items()
+    keep = []
+
+    def dev(data, out_n):
+        a = np.frombuffer(data, dtype=np.uint8).copy()
+        o = np.zeros(out_n, dtype=np.uint8)
+        keep.extend([a, o])
+        return haddr(a), haddr(o), lambda: o.tobytes()
+
+    d = emu_decoder_factory(hbm_budget_bytes=budget)
+    outs, lens, status = run_batch(d, items, dev)
+    for (raw, gz, cap), got, n, stt in zip(items, outs, lens, status):
+        want = expected_status(gz)
+        if want == 0 and raw is not None and len(raw) > cap:
+            assert stt == 24 and n == len(raw)  # capacity: the size needed comes back
+        else:
+            assert stt == want
+            if want == 0:
+                assert got == raw

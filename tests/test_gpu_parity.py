@@ -306,3 +306,58 @@ def test_large_stream_properties(gpu_decoder_factory):
     h = hashlib.sha256(dout[:n].cpu().numpy().tobytes()).hexdigest()
     assert h == sha256(raw)
     assert st.members == 1 and st.gpu_chunks > 100
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["chain", "false-headers", "then-plain", "truncated", "crc"])
+def test_bgzf_device_walk(gpu_decoder_factory, case):
+    """The device BGZF member walk (scan, compaction, chain) against the oracle,
+    including the error kind, member index and trailer position."""
+    from conftest import bgzf_cases
+    from rusty_rapidgzip_b200 import RrgError
+    data = bgzf_cases()[case]
+    d = gpu_decoder_factory()
+    try:
+        want = oracle.read_gz(data, 2)
+    except oracle.OracleError as oe:
+        with pytest.raises(RrgError) as ge:
+            d.decompress(data)
+        assert (ge.value.code, ge.value.member, ge.value.trailer_byte) == (oe.code, oe.member, oe.trailer_byte)
+        return
+    assert d.decompress(data) == want
+    # a second decode of the same layout replays the captured graph
+    import numpy as np
+    import torch
+    din = torch.from_numpy(np.frombuffer(data, dtype=np.uint8).copy()).cuda()
+    dout = torch.empty(len(want) + 64, dtype=torch.uint8, device="cuda")
+    for _ in range(2):
+        n, st = d.decode_device(din, len(data), dout, dout.numel())
+        assert n == len(want) and bytes(dout[:n].cpu().numpy()) == want
+    assert st.graph_launches == 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("budget", [0, 1], ids=["one-wave", "waves"])
+def test_batch_mixed(gpu_decoder_factory, budget):
+    """A batch mixing multi-chunk, single-chunk, multi-member and BGZF files, a
+    corrupt file and a too-small output range; per-item status and bytes against
+    the oracle, in one wave and in several."""
+    import torch
+    from test_emu import batch_items, expected_status, run_batch
+
+    def devbuf(data, out_n):
+        din = torch.from_numpy(np.frombuffer(data, dtype=np.uint8).copy()).cuda()
+        dout = torch.zeros(out_n, dtype=torch.uint8, device="cuda")
+        return din, dout, lambda: dout.cpu().numpy().tobytes()
+
+    items = batch_items()
+    d = gpu_decoder_factory(hbm_budget_bytes=budget)
+    outs, lens, status = run_batch(d, items, devbuf)
+    for (raw, gz, cap), got, n, stt in zip(items, outs, lens, status):
+        want = expected_status(gz)
+        if want == 0 and raw is not None and len(raw) > cap:
+            assert stt == 24 and n == len(raw)
+        else:
+            assert stt == want
+            if want == 0:
+                assert got == raw
