@@ -131,17 +131,43 @@ int rrg_gpu_decode_device(rrg_ctx* ctx, const uint8_t* d_in, size_t len, uint8_t
                           size_t out_cap, size_t* out_len, void* stream, rrg_stats* stats,
                           rrg_error* err);
 
-/* Batched decode of `n` independent gzip files/members already on the device
- * (one persistent-kernel launch over a device work queue; see the BGZF batch
- * path pipeline.rs:1357-1636 and decode_gzip_member libdeflate_ffi.rs:137-176).
- * Input i is d_in[in_off[i] .. in_off[i]+in_len[i]); its output goes to
- * d_out[out_off[i] ..] with room for out_cap[i] bytes; out_len[i] and status[i]
- * (enum rrg_status) are written to host arrays. in_off/in_len/out_off/out_cap
- * are host arrays. Returns the first failing status (RRG_OK if all passed). */
+/* Batched decode of `n` independent gzip files already on the device (the
+ * per-file work of read_gz, lib.rs:366-496, for many files at once; BGZF files
+ * as in pipeline.rs:1357-1636). Headers are parsed on the device. BGZF files
+ * take the device member walk and one persistent decode per file (a captured
+ * CUDA graph). All other files share one boundary scan, one persistent inflate
+ * launch over a device work queue, one resolve and one CRC pass; a file small
+ * enough for one sub-chunk decodes straight to its output bytes. Files are
+ * processed in waves whose reserved scratch fits rrg_config.hbm_budget_bytes
+ * (and the free device memory). Input i is d_in[in_off[i] .. +in_len[i]); its
+ * output goes to d_out[out_off[i] ..] with room for out_cap[i] bytes; out_len[i]
+ * and status[i] (enum rrg_status) are written to host arrays; RRG_ERR_CAPACITY
+ * leaves the size needed in out_len[i]. in_off/in_len/out_off/out_cap are host
+ * arrays. Returns the first failing status (RRG_OK if all passed). */
 int rrg_gpu_decode_batch(rrg_ctx* ctx, const uint8_t* d_in, const uint64_t* in_off,
                          const uint64_t* in_len, uint8_t* d_out, const uint64_t* out_off,
                          const uint64_t* out_cap, uint64_t* out_len, int32_t* status, size_t n,
                          void* stream, rrg_stats* stats, rrg_error* err);
+
+/* Settings chosen by rrg_gpu_autotune. */
+typedef struct rrg_tuning {
+    uint64_t gpu_chunk_bytes;   /* speculative sub-chunk size; 0 = one wave of resident decoders */
+    int32_t boundary_mode;      /* 0 = boundary scan of every bit offset, 1 = one search per target */
+    int32_t warps_per_member;   /* BGZF: 1 = one warp decodes a whole member; 2-4 = sub-chunks per member */
+    uint64_t finder_tile_bits;  /* boundary-scan tile width (8192, 16384 or 32768 bits) */
+    double best_ms;             /* batch time on the sample with the chosen settings */
+    double default_ms;          /* batch time on the sample with the settings before tuning */
+    uint32_t trials;            /* settings timed */
+} rrg_tuning;
+
+/* Autotuner. Decodes the sample batch (same arguments as rrg_gpu_decode_batch)
+ * under a coordinate sweep of sub-chunk size, boundary search and scan tile
+ * width, and warps per BGZF member, three runs each, and keeps the fastest
+ * setting in the context for later calls. The reference has no autotuner
+ * (its chunk size is a fixed Config field, lib.rs:50-100). */
+int rrg_gpu_autotune(rrg_ctx* ctx, const uint8_t* d_in, const uint64_t* in_off, const uint64_t* in_len,
+                     uint8_t* d_out, const uint64_t* out_off, const uint64_t* out_cap, size_t n, void* stream,
+                     rrg_tuning* result, rrg_error* err);
 
 /* ---- kernel-level entry points (each replaces one reference function) ---- */
 

@@ -84,6 +84,12 @@ _STAT_U64 = ["compressed_bytes", "uncompressed_bytes", "chunks_decoded", "specul
 _STAT_F64 = ["finder_ms", "inflate_ms", "resolve_ms", "crc_ms", "h2d_ms", "d2h_ms", "total_ms"]
 
 
+class _Tuning(C.Structure):
+    _fields_ = [("gpu_chunk_bytes", C.c_uint64), ("boundary_mode", C.c_int32), ("warps_per_member", C.c_int32),
+                ("finder_tile_bits", C.c_uint64), ("best_ms", C.c_double), ("default_ms", C.c_double),
+                ("trials", C.c_uint32)]
+
+
 class _Stats(C.Structure):
     _fields_ = ([(n, C.c_uint64) for n in _STAT_U64] + [(n, C.c_double) for n in _STAT_F64]
                 + [("graph_launches", C.c_uint64)])
@@ -232,6 +238,8 @@ def load_library(path: str | None = None):
         L.rrg_gpu_decode_device.argtypes = [vp, vp, sz, vp, sz, C.POINTER(sz), vp, S, E]
         L.rrg_gpu_decode_batch.argtypes = [vp, vp, C.POINTER(u64), C.POINTER(u64), vp, C.POINTER(u64),
                                            C.POINTER(u64), C.POINTER(u64), C.POINTER(i32), sz, vp, S, E]
+        L.rrg_gpu_autotune.argtypes = [vp, vp, C.POINTER(u64), C.POINTER(u64), vp, C.POINTER(u64), C.POINTER(u64),
+                                       sz, vp, C.POINTER(_Tuning), E]
         L.rrg_gpu_find_blocks.argtypes = [vp, vp, sz, C.POINTER(u64), C.POINTER(u64), C.POINTER(u64), sz, E]
         L.rrg_gpu_crc32.argtypes = [vp, vp, sz, C.POINTER(C.c_uint32), E]
         L.rrg_gpu_resolve_markers.argtypes = [vp, vp, sz, vp, vp, sz, vp, sz, E]
@@ -394,6 +402,17 @@ class Decoder:
         if e.code not in (OK,) and e.code >= ERR_CUDA and e.code != ERR_CAPACITY:
             _raise(e)
         return [int(ol[i]) for i in range(n)], [int(stv[i]) for i in range(n)], DecodeStats._from(st)
+
+    def autotune(self, d_in, in_off, in_len, d_out, out_off, out_cap, stream=None) -> dict:
+        """Sweep the tunables on a sample batch (decode_batch's arguments) and keep
+        the fastest setting in this decoder; returns the chosen setting."""
+        n = len(in_off)
+        A = C.c_uint64 * max(n, 1)
+        t, e = _Tuning(), _Error()
+        self._L.rrg_gpu_autotune(self._ctx, _ptr(d_in), A(*in_off), A(*in_len), _ptr(d_out), A(*out_off),
+                                 A(*out_cap), n, _ptr(stream), C.byref(t), C.byref(e))
+        _raise(e)
+        return {f: getattr(t, f) for f, _ in _Tuning._fields_}
 
     # -------------------------------------------------------------- kernels
     def find_blocks(self, d_body, body_len: int, targets, limits):

@@ -241,9 +241,12 @@ struct rrg_ctx {
     bool scan_bounds = true;   // full-stream boundary scan (boundary_mode 1: one finder search per target)
     uint32_t inflate_warps = 4;
     uint32_t finder_tile = 1024;
+    uint32_t scan_threads = 256;  // boundary scan tile = scan_threads x 16 bytes
+    uint32_t warps_per_member = 1; // BGZF: 1 = a member per warp; 2-4 = sub-chunks per member
     double expand = 6.0;
     uint64_t slots = 0;        // resident decoders of one inflate wave (lazy)
     DBuf sniff;                // per-file header results of a batch
+    DBuf tile_chunk;           // resolve: chunk of every tile
     // BGZF route: device member table and the captured decode graph
     DBuf bg_bcount, bg_bbase, bg_coff, bg_csize, bg_small;
     uint64_t* h_bg = nullptr;  // pinned: the 64 result bytes of one BGZF decode
@@ -573,9 +576,16 @@ int run_resolve(rrg_ctx* c, const std::vector<ResolveChunk>& rchunks, const std:
     CK(dgrow(c->win, (size_t)nc * WINDOW * 4));
     CK(cudaMemcpyAsync(c->chunks.p, rchunks.data(), nc * sizeof(ResolveChunk), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->tiles.p, tile_start.data(), (nc + 1) * 8, cudaMemcpyHostToDevice, c->stream));
+    const uint64_t n_tiles = tile_start.back();
+    std::vector<uint32_t> tchunk(n_tiles);
+    for (uint32_t k = 0; k < nc; k++)
+        for (uint64_t t = tile_start[k]; t < tile_start[k + 1]; t++) tchunk[t] = k;
+    CK(dgrow(c->tile_chunk, std::max<uint64_t>(n_tiles, 1) * 4));
+    if (n_tiles) CK(cudaMemcpyAsync(c->tile_chunk.p, tchunk.data(), n_tiles * 4, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemsetAsync(c->rerr.p, 0, 16, c->stream));
     CK(cudaMemsetAsync(c->markers.p, 0, 8, c->stream));
-    ResolveArgs R{(const uint16_t*)c->cells.p, (const ResolveChunk*)c->chunks.p, (const uint64_t*)c->tiles.p, nc,
+    ResolveArgs R{(const uint16_t*)c->cells.p, (const ResolveChunk*)c->chunks.p, (const uint64_t*)c->tiles.p,
+                  (const uint32_t*)c->tile_chunk.p, nc,
                   tile_start.back(), d_dst, (uint32_t*)c->win.p, (uint32_t*)c->rerr.p,
                   (unsigned long long*)c->markers.p};
     const uint64_t wcells = (uint64_t)nc * WINDOW;
@@ -623,9 +633,14 @@ int scan_boundaries(rrg_ctx* c, const uint8_t* body, uint64_t blen, std::vector<
     uint64_t* surv = cand + cap;
     uint32_t* counts = (uint32_t*)c->ncand.p;  // [0] candidates, [1] survivors, [2] heavy queue
     ScanArgs S{body, blen, cand, counts, cap};
-    const uint64_t tiles = (blen + 16 + SCAN_TILE - 1) / SCAN_TILE;
-    RRG_LAUNCH(k_scan_candidates, (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(tiles, (uint64_t)c->n_sm * 8)),
-               SCAN_THREADS, 0, c->stream, S);
+    // tile width: scan_threads x 16 bytes per block step (64, 128 or 256 threads)
+    const uint32_t st = c->scan_threads;
+    const uint64_t tb = (uint64_t)st * 16;
+    const uint32_t sgrid = (uint32_t)std::max<uint64_t>(
+        1, std::min<uint64_t>((blen + 16 + tb - 1) / tb, (uint64_t)c->n_sm * (2048 / st)));
+    if (st == 64) RRG_LAUNCH(k_scan_candidates<64>, sgrid, 64, 0, c->stream, S);
+    else if (st == 128) RRG_LAUNCH(k_scan_candidates<128>, sgrid, 128, 0, c->stream, S);
+    else RRG_LAUNCH(k_scan_candidates<256>, sgrid, 256, 0, c->stream, S);
     LAUNCHED(c);
     VerifyArgs V{body, blen, cand, counts, cap, surv, counts + 1, cap2, nullptr, nullptr};
     RRG_LAUNCH(k_verify_light, c->n_sm * 8, 256, 0, c->stream, V);
@@ -1421,6 +1436,19 @@ int decode_file(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_t* 
         CK(cudaMemcpy(head.data(), d_file, hlen, cudaMemcpyDeviceToHost));
         hp = head.data();
     }
+    if (host_bgzf_size(hp, hlen) >= 0 && c->warps_per_member > 1) {
+        // W warps per member: the file as one member stream, split at verified
+        // block starts every (first member's size / W) compressed bytes
+        size_t hl = 0;
+        int detail = 0;
+        if (host_parse_header(hp, hlen, &hl, &detail) == DS_OK) {
+            const uint64_t g_save = c->gpu_chunk;
+            c->gpu_chunk = std::max<uint64_t>(4096, (uint64_t)host_bgzf_size(hp, hlen) / c->warps_per_member);
+            rc = member_route(c, d_file, len, hl, tgt, 0, 0, out, err);
+            c->gpu_chunk = g_save;
+            return rc;
+        }
+    }
     if (host_bgzf_size(hp, hlen) >= 0) {
         Decoded d1;
         uint64_t rem = 0;
@@ -1669,6 +1697,109 @@ int batch_impl(rrg_ctx* c, const uint8_t* d_in, const uint64_t* in_off, const ui
     return 0;
 }
 
+// ------------------------------------------------------------ autotuner
+// Times the batch path on the caller's sample under a coordinate sweep of the
+// tunables (sub-chunk size, boundary search and scan tile, warps per BGZF
+// member) and keeps the fastest setting in the context.
+struct Tunables {
+    uint64_t gpu_chunk;
+    bool scan_bounds;
+    uint32_t scan_threads, warps_per_member;
+};
+Tunables get_tun(const rrg_ctx* c) { return Tunables{c->gpu_chunk, c->scan_bounds, c->scan_threads, c->warps_per_member}; }
+void set_tun(rrg_ctx* c, const Tunables& t) {
+    c->gpu_chunk = t.gpu_chunk;
+    c->scan_bounds = t.scan_bounds;
+    c->scan_threads = t.scan_threads;
+    c->warps_per_member = t.warps_per_member;
+}
+
+int autotune_impl(rrg_ctx* c, const uint8_t* d_in, const uint64_t* in_off, const uint64_t* in_len, uint8_t* d_out,
+                  const uint64_t* out_off, const uint64_t* out_cap, size_t n, rrg_tuning* res, rrg_error* err) {
+    std::vector<uint64_t> olen(n);
+    std::vector<int32_t> stv(n);
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    uint32_t trials = 0;
+    // best of 2 timed runs after one untimed run; infinity if any item fails
+    auto measure = [&](const Tunables& t, double* ms) -> int {
+        set_tun(c, t);
+        double best = 1e30;
+#ifdef RRG_EMU
+        const int reps = 1;  // the CPU emulation checks the sweep, not the timings
+#else
+        const int reps = 3;
+#endif
+        for (int r = 0; r < reps; r++) {
+            CK(cudaEventRecord(e0, c->stream));
+            int rc = batch_impl(c, d_in, in_off, in_len, d_out, out_off, out_cap, olen.data(), stv.data(), n, err);
+            if (rc) return rc;
+            CK(cudaEventRecord(e1, c->stream));
+            CK(cudaEventSynchronize(e1));
+            float f = 0;
+            cudaEventElapsedTime(&f, e0, e1);
+            for (size_t i = 0; i < n; i++)
+                if (stv[i] != RRG_OK) f = 1e30f;
+            if (r || reps == 1) best = std::min(best, (double)f);
+        }
+        trials++;
+        *ms = best;
+        return 0;
+    };
+    bool any_bgzf = false;
+    for (size_t i = 0; i < n; i++) {
+        uint8_t h[64] = {0};
+        const size_t k = (size_t)std::min<uint64_t>(in_len[i], sizeof(h));
+        CK(cudaMemcpy(h, d_in + in_off[i], k, cudaMemcpyDeviceToHost));
+        any_bgzf |= host_bgzf_size(h, k) >= 0;
+    }
+    Tunables best = get_tun(c), t = best;
+    double best_ms = 0, ms = 0;
+    int rc = measure(best, &best_ms);
+    if (rc) return rc;
+    const double default_ms = best_ms;
+    // 1. sub-chunk size (0 = one wave of resident decoders)
+    for (uint64_t g : {0ull, 32ull << 10, 64ull << 10, 128ull << 10, 256ull << 10, 1ull << 20}) {
+        t = best;
+        t.gpu_chunk = g;
+        if (g == best.gpu_chunk) continue;
+        if ((rc = measure(t, &ms))) return rc;
+        if (ms < best_ms) best = t, best_ms = ms;
+    }
+    // 2. boundary search: the scan with each tile width, or one search per target
+    for (uint32_t st : {64u, 128u, 256u, 0u}) {
+        t = best;
+        t.scan_bounds = st != 0;
+        if (st) t.scan_threads = st;
+        if (t.scan_bounds == best.scan_bounds && t.scan_threads == best.scan_threads) continue;
+        if ((rc = measure(t, &ms))) return rc;
+        if (ms < best_ms) best = t, best_ms = ms;
+    }
+    // 3. warps per BGZF member
+    if (any_bgzf)
+        for (uint32_t w = 1; w <= 4; w++) {
+            t = best;
+            t.warps_per_member = w;
+            if (w == best.warps_per_member) continue;
+            if ((rc = measure(t, &ms))) return rc;
+            if (ms < best_ms) best = t, best_ms = ms;
+        }
+    set_tun(c, best);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (res) {
+        res->gpu_chunk_bytes = best.gpu_chunk;
+        res->boundary_mode = best.scan_bounds ? 0 : 1;
+        res->finder_tile_bits = (uint64_t)best.scan_threads * 16 * 8;
+        res->warps_per_member = (int32_t)best.warps_per_member;
+        res->best_ms = best_ms;
+        res->default_ms = default_ms;
+        res->trials = trials;
+    }
+    return 0;
+}
+
 }  // namespace
 
 // ====================================================================== C ABI
@@ -1680,7 +1811,12 @@ rrg_ctx* rrg_gpu_create(const rrg_config* cfg, rrg_error* err) {
     if (!c->cfg.chunk_size_bytes) c->cfg.chunk_size_bytes = 4ull << 20;
     if (!c->cfg.hbm_budget_bytes) c->cfg.hbm_budget_bytes = 120ull * 1000 * 1000 * 1000;
     c->gpu_chunk = c->cfg.gpu_chunk_bytes;
-    if (c->cfg.finder_tile_bits) c->finder_tile = (uint32_t)std::min<uint64_t>(FIND_TILE, (c->cfg.finder_tile_bits + 31) & ~31ull);
+    if (c->cfg.finder_tile_bits) {
+        c->finder_tile = (uint32_t)std::min<uint64_t>(FIND_TILE, (c->cfg.finder_tile_bits + 31) & ~31ull);
+        // the boundary scan's tile: 8192, 16384 or 32768 bits (1, 2 or 4 KiB)
+        c->scan_threads = c->cfg.finder_tile_bits <= 8192 ? 64 : c->cfg.finder_tile_bits <= 16384 ? 128 : 256;
+    }
+    if (c->cfg.warps_per_stream > 1) c->warps_per_member = (uint32_t)std::min(4, c->cfg.warps_per_stream);
     cudaError_t e;
     if (c->cfg.device >= 0) {
         e = cudaSetDevice(c->cfg.device);
@@ -1725,7 +1861,7 @@ void rrg_gpu_destroy(rrg_ctx* c) {
                     &c->out,    &c->targets, &c->limits,    &c->found,    &c->next_lut, &c->chunks,    &c->tiles,
                     &c->rerr,   &c->markers, &c->crc_table, &c->pieces,   &c->piece_crc, &c->mpiece,   &c->exp_crc,
                     &c->exp_isize, &c->got_crc, &c->got_len, &c->mstatus, &c->comp, &c->bg_bcount, &c->bg_bbase,
-                    &c->bg_coff, &c->bg_csize, &c->bg_small, &c->sniff};
+                    &c->bg_coff, &c->bg_csize, &c->bg_small, &c->sniff, &c->tile_chunk};
 #ifndef RRG_EMU
     if (c->bg_exec) cudaGraphExecDestroy(c->bg_exec);
 #endif
@@ -1849,6 +1985,23 @@ int rrg_gpu_decode_batch(rrg_ctx* c, const uint8_t* d_in, const uint64_t* in_off
     c->st.total_ms = now_ms() - t_all;
     if (stats) *stats = c->st;
     return rc ? rc : first_bad;
+}
+
+int rrg_gpu_autotune(rrg_ctx* c, const uint8_t* d_in, const uint64_t* in_off, const uint64_t* in_len, uint8_t* d_out,
+                     const uint64_t* out_off, const uint64_t* out_cap, size_t n, void* stream, rrg_tuning* result,
+                     rrg_error* err) {
+    rrg_error local_err;
+    if (!err) err = &local_err;
+    if (!c || !n || !d_in || !in_off || !in_len || !d_out || !out_off || !out_cap) {
+        set_err(err, RRG_ERR_INVALID_ARGUMENT, "null argument or empty sample");
+        return RRG_ERR_INVALID_ARGUMENT;
+    }
+    std::memset(err, 0, sizeof(*err));
+    c->st = rrg_stats{};
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    int rc = autotune_impl(c, d_in, in_off, in_len, d_out, out_off, out_cap, n, result, err);
+    c->stream = c->own_stream;
+    return rc;
 }
 
 int rrg_gpu_find_blocks(rrg_ctx* c, const uint8_t* d_body, size_t body_len, const uint64_t* targets,

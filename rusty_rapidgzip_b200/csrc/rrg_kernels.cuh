@@ -1726,8 +1726,6 @@ __global__ void __launch_bounds__(128) k_find_blocks(FindArgs A) {
 // k_verify_light then applies the strict code-length checks of
 // read_dynamic_header_strict_into (block_finder.rs:196-262) per thread, and
 // the last survivors get verify_heavy (tables + 64 trial symbols).
-constexpr int SCAN_THREADS = 256;
-constexpr int SCAN_TILE = SCAN_THREADS * 16;
 constexpr int SCAN_HALO = 48;  // the last thread reads up to 2.5 words past its 16 bytes
 
 struct ScanArgs {
@@ -1744,16 +1742,24 @@ __device__ __forceinline__ uint32_t tile_bits(const uint32_t* tw, uint32_t b) {
     return __funnelshift_r(tw[q], tw[q + 1], r);
 }
 
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_candidates(ScanArgs A) {
-    __shared__ __align__(16) uint32_t tile[(SCAN_TILE + SCAN_HALO) / 4];
+constexpr int SCAN_LIST = 1024;  // candidates a tile stages in shared memory before one global append
+
+// ST threads per block; a tile is ST * 16 bytes (the finder tile width knob)
+template <int ST>
+__global__ void __launch_bounds__(ST) k_scan_candidates(ScanArgs A) {
+    constexpr int TILE = ST * 16;
+    __shared__ __align__(16) uint32_t tile[(TILE + SCAN_HALO) / 4];
+    __shared__ uint32_t s_list[SCAN_LIST];
+    __shared__ uint32_t s_n, s_base;
     const uintptr_t addr = (uintptr_t)A.body;
     const uint8_t* base = (const uint8_t*)(addr & ~(uintptr_t)15);
     const uint64_t lo = addr & 15, hi = lo + A.body_len;
-    const uint64_t n_tiles = (hi + SCAN_TILE - 1) / SCAN_TILE;
+    const uint64_t n_tiles = (hi + TILE - 1) / TILE;
     uint8_t* tb = reinterpret_cast<uint8_t*>(tile);
     for (uint64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
-        const uint64_t t0 = t * SCAN_TILE;
-        for (uint32_t q = threadIdx.x; q < (SCAN_TILE + SCAN_HALO) / 16; q += blockDim.x) {
+        const uint64_t t0 = t * TILE;
+        if (threadIdx.x == 0) s_n = 0;
+        for (uint32_t q = threadIdx.x; q < (TILE + SCAN_HALO) / 16; q += blockDim.x) {
             const uint64_t b0 = t0 + 16ull * q;
             if (b0 >= lo && b0 + 16 <= hi) {
                 *reinterpret_cast<uint4*>(tb + 16 * q) = __ldg(reinterpret_cast<const uint4*>(base + b0));
@@ -1772,13 +1778,13 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_candidates(ScanArgs A) {
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const uint32_t a = tile[w0 + q], b = tile[w0 + q + 1];
-            uint32_t m = 0;
-#pragma unroll
-            for (int r = 0; r < 32; r++) {
-                const uint32_t w = __funnelshift_r(a, b, r);
-                const bool c = (w & 7u) == 4u && ((w >> 3) & 31u) <= 29u && ((w >> 8) & 31u) <= 29u;
-                m |= (c ? 1u : 0u) << r;
-            }
+            // bit-sliced over the 32 offsets: bit r of f(k) is header bit k at offset r.
+            // BFINAL=0, BTYPE=2 (bits 0,1,2 = 0,0,1); HLIT <= 29 and HDIST <= 29
+            // (not bits 4-7 all set, not bits 9-12 all set)
+#define RRG_F(k) __funnelshift_r(a, b, k)
+            uint32_t m = ~RRG_F(0) & ~RRG_F(1) & RRG_F(2) & ~(RRG_F(4) & RRG_F(5) & RRG_F(6) & RRG_F(7)) &
+                         ~(RRG_F(9) & RRG_F(10) & RRG_F(11) & RRG_F(12));
+#undef RRG_F
             // only offsets p with lo*8 <= p and p + 13 <= hi*8 are tested
             const uint64_t g0 = tile_bit0 + 32ull * (w0 + q);
             if (g0 < lo * 8 || g0 + 32 + 13 > hi * 8) {
@@ -1808,11 +1814,23 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_candidates(ScanArgs A) {
                     nsym += use ? 1u : 0u;
                 }
                 if (nsym < 2 || kraft == 128u) {
-                    const uint32_t slot = atomicAdd(A.n_cand, 1u);
-                    if (slot < A.cap) A.cand[slot] = tile_bit0 + boff - lo * 8;
+                    const uint32_t k = atomicAdd(&s_n, 1u);
+                    if (k < SCAN_LIST) {
+                        s_list[k] = boff;
+                    } else {  // a crowded tile: straight to the global list
+                        const uint32_t slot = atomicAdd(A.n_cand, 1u);
+                        if (slot < A.cap) A.cand[slot] = tile_bit0 + boff - lo * 8;
+                    }
                 }
             }
         }
+        // one global append per tile for the staged candidates
+        __syncthreads();
+        const uint32_t ns = s_n < SCAN_LIST ? s_n : SCAN_LIST;
+        if (threadIdx.x == 0) s_base = ns ? atomicAdd(A.n_cand, ns) : 0u;
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < ns; i += blockDim.x)
+            if (s_base + i < A.cap) A.cand[s_base + i] = tile_bit0 + s_list[i] - lo * 8;
         __syncthreads();
     }
 }
@@ -1975,6 +1993,7 @@ struct ResolveArgs {
     const uint16_t* cells;
     const ResolveChunk* chunks;
     const uint64_t* tile_start;  // n_chunks + 1 prefix of tiles per chunk
+    const uint32_t* tile_chunk;  // n_tiles: the chunk each tile belongs to
     uint32_t n_chunks;
     uint64_t n_tiles;
     uint8_t* out;
@@ -2041,13 +2060,7 @@ __global__ void __launch_bounds__(RES_THREADS) k_resolve(ResolveArgs A) {
     if (threadIdx.x == 0) s_mk = 0;
     for (uint64_t t = blockIdx.x; t < A.n_tiles; t += gridDim.x) {
         if (threadIdx.x == 0) {
-            uint32_t lo = 0, hi = A.n_chunks - 1;
-            while (lo < hi) {
-                uint32_t mid = (lo + hi + 1) >> 1;
-                if (A.tile_start[mid] <= t) lo = mid;
-                else hi = mid - 1;
-            }
-            s_chunk = lo;
+            s_chunk = A.tile_chunk[t];
             s_bad = 0;
         }
         __syncthreads();

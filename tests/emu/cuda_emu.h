@@ -9,6 +9,8 @@
 // `-m "not gpu"` tests and never stands in for the GPU build.
 #pragma once
 #include <barrier>
+#include <condition_variable>
+#include <mutex>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -68,7 +70,60 @@ inline std::vector<unsigned char>& dyn_buf() {
 }
 inline unsigned char* dyn_smem() { return dyn_buf().data(); }
 
+// Worker threads are created once and reused: thread i of every block runs on
+// pool thread i (a block needs all of its threads alive at once for the
+// barriers). Launches from several host threads are serialised.
+struct Pool {
+    std::mutex mu;
+    std::condition_variable cv, done_cv;
+    std::vector<std::thread> th;
+    uint64_t gen = 0;
+    unsigned active = 0, remaining = 0;
+    const std::function<void(unsigned)>* job = nullptr;
+
+    void ensure(unsigned n) {
+        while (th.size() < n) {
+            const unsigned id = (unsigned)th.size();
+            th.emplace_back([this, id] { loop(id); });
+            th.back().detach();
+        }
+    }
+    void loop(unsigned id) {
+        uint64_t seen = 0;
+        std::unique_lock<std::mutex> lk(mu);
+        for (;;) {
+            cv.wait(lk, [&] { return gen != seen; });
+            seen = gen;
+            if (id >= active) continue;
+            const std::function<void(unsigned)>* j = job;
+            lk.unlock();
+            (*j)(id);
+            lk.lock();
+            if (--remaining == 0) done_cv.notify_all();
+        }
+    }
+    void run(unsigned n, const std::function<void(unsigned)>& f) {
+        ensure(n);
+        std::unique_lock<std::mutex> lk(mu);
+        job = &f;
+        active = n;
+        remaining = n;
+        gen++;
+        cv.notify_all();
+        done_cv.wait(lk, [&] { return remaining == 0; });
+    }
+};
+inline Pool& pool() {
+    static Pool* p = new Pool;  // never destroyed: its threads outlive static destruction
+    return *p;
+}
+inline std::mutex& launch_mutex() {
+    static std::mutex m;
+    return m;
+}
+
 inline void launch(dim3 grid, dim3 block, size_t smem, const std::function<void()>& body) {
+    std::lock_guard<std::mutex> guard(launch_mutex());
     unsigned nthreads = block.x;
     auto& buf = dyn_buf();
     if (buf.size() < smem + 64) buf.assign(smem + 64, 0);
@@ -76,20 +131,16 @@ inline void launch(dim3 grid, dim3 block, size_t smem, const std::function<void(
         Block blk;
         blk.bar = std::make_unique<std::barrier<>>(nthreads);
         for (unsigned w = 0; w < (nthreads + 31) / 32; w++) blk.warps.push_back(std::make_unique<Warp>());
-        std::vector<std::thread> th;
-        th.reserve(nthreads);
-        for (unsigned t = 0; t < nthreads; t++) {
-            th.emplace_back([&, t, b] {
-                t_block = &blk;
-                t_warp = blk.warps[t / 32].get();
-                t_tid = dim3(t);
-                t_bid = dim3(b);
-                t_bdim = block;
-                t_gdim = grid;
-                body();
-            });
-        }
-        for (auto& x : th) x.join();
+        const std::function<void(unsigned)> one = [&, b](unsigned t) {
+            t_block = &blk;
+            t_warp = blk.warps[t / 32].get();
+            t_tid = dim3(t);
+            t_bid = dim3(b);
+            t_bdim = block;
+            t_gdim = grid;
+            body();
+        };
+        pool().run(nthreads, one);
     }
 }
 

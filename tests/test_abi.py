@@ -53,15 +53,20 @@ def test_struct_layouts_match_c(tmp_path):
     from rusty_rapidgzip_b200 import _abi
     src = tmp_path / "sz.c"
     src.write_text('#include "rrg_gpu.h"\n#include <stdio.h>\n#include <stddef.h>\n'
-                   'int main(){printf("%zu %zu %zu %zu\\n", sizeof(rrg_error), sizeof(rrg_config), '
-                   'sizeof(rrg_stats), offsetof(rrg_stats, finder_ms));return 0;}\n')
+                   'int main(){printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(rrg_error), sizeof(rrg_config), '
+                   'sizeof(rrg_stats), offsetof(rrg_stats, finder_ms), offsetof(rrg_stats, graph_launches), '
+                   'sizeof(rrg_tuning), offsetof(rrg_tuning, best_ms));return 0;}\n')
     exe = tmp_path / "sz"
     subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)])
-    e, c, s, off = map(int, subprocess.run([str(exe)], stdout=subprocess.PIPE, text=True).stdout.split())
+    e, c, s, off, goff, t, toff = map(int, subprocess.run([str(exe)], stdout=subprocess.PIPE,
+                                                         text=True).stdout.split())
     assert C.sizeof(_abi._Error) == e
     assert C.sizeof(_abi._Config) == c
     assert C.sizeof(_abi._Stats) == s
     assert _abi._Stats.finder_ms.offset == off
+    assert _abi._Stats.graph_launches.offset == goff
+    assert C.sizeof(_abi._Tuning) == t
+    assert _abi._Tuning.best_ms.offset == toff
 
 
 def test_missing_library_fails_loudly(tmp_path):

@@ -191,3 +191,29 @@ def test_batch_mixed(emu_decoder_factory, budget):
             assert stt == want
             if want == 0:
                 assert got == raw
+
+
+def test_autotune(emu_decoder_factory):
+    """The sweep runs every setting on the sample and leaves a setting under
+    which the batch still decodes exactly."""
+    raw_a, gz_a = W.config0(12_000, seed=8)
+    items = [(raw_a, gz_a, len(raw_a))]
+    keep = []
+
+    def dev(data, out_n):
+        a = np.frombuffer(data, dtype=np.uint8).copy()
+        o = np.zeros(out_n, dtype=np.uint8)
+        keep.extend([a, o])
+        return haddr(a), haddr(o), lambda: o.tobytes()
+
+    d = emu_decoder_factory()
+    blobs = [gz for _, gz, _ in items]
+    offs = np.cumsum([0] + [len(b) for b in blobs])[:-1].tolist()
+    caps = [cap for _, _, cap in items]
+    ooffs = np.cumsum([0] + caps)[:-1].tolist()
+    din, dout, _ = dev(b"".join(blobs), sum(caps) + 64)
+    t = d.autotune(din, offs, [len(b) for b in blobs], dout, ooffs, caps)
+    assert t["trials"] == 9 and t["best_ms"] <= t["default_ms"] * 1.0001  # 1 + 5 sizes + 3 searches
+    assert t["boundary_mode"] in (0, 1) and t["warps_per_member"] == 1  # no BGZF in the sample
+    outs, lens, status = run_batch(d, items, dev)
+    assert status == [0] and outs == [raw_a]

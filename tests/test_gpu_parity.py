@@ -361,3 +361,32 @@ def test_batch_mixed(gpu_decoder_factory, budget):
             assert stt == want
             if want == 0:
                 assert got == raw
+
+
+@pytest.mark.gpu
+def test_autotune(gpu_decoder_factory):
+    """The sweep (sub-chunk size, boundary search and scan tile, warps per BGZF
+    member) on a sample batch, then the batch decodes exactly under the chosen
+    setting."""
+    import torch
+    from test_emu import run_batch
+    raw_a, gz_a = W.config1(6 << 20, seed=8)
+    raw_b = W.fastq_like(3 << 20, 9)
+    items = [(raw_a, gz_a, len(raw_a)), (raw_b, W.bgzf(raw_b, 5), len(raw_b))]
+
+    def devbuf(data, out_n):
+        din = torch.from_numpy(np.frombuffer(data, dtype=np.uint8).copy()).cuda()
+        dout = torch.zeros(out_n, dtype=torch.uint8, device="cuda")
+        return din, dout, lambda: dout.cpu().numpy().tobytes()
+
+    d = gpu_decoder_factory()
+    blobs = [gz for _, gz, _ in items]
+    offs = np.cumsum([0] + [len(b) for b in blobs])[:-1].tolist()
+    caps = [cap for _, _, cap in items]
+    ooffs = np.cumsum([0] + caps)[:-1].tolist()
+    din, dout, _ = devbuf(b"".join(blobs), sum(caps) + 64)
+    t = d.autotune(din, offs, [len(b) for b in blobs], dout, ooffs, caps)
+    assert t["trials"] >= 12 and 0 < t["best_ms"] <= t["default_ms"] * 1.0001
+    assert t["boundary_mode"] in (0, 1) and 1 <= t["warps_per_member"] <= 4
+    outs, lens, status = run_batch(d, items, devbuf)
+    assert status == [0, 0] and outs == [raw_a, raw_b]
