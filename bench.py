@@ -28,6 +28,8 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -87,7 +89,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             threading.Thread(target=self._read, daemon=True).start()
         except OSError:
             self.proc = None
@@ -190,6 +192,16 @@ def run_ours(args, raw, gz, desc):
     din.copy_(torch.frombuffer(bytearray(gz), dtype=torch.uint8))
     dout = torch.empty(len(raw) + 64, dtype=torch.uint8, device="cuda")
     torch.cuda.synchronize()
+    tuning = None
+    if args.workload == "bgzf" and args.warps_per_stream == 0:
+        # autotune (untimed) on the file's first 2048 members
+        off, k = 0, 0
+        while k < 2048 and off + 18 <= len(gz):
+            off += int.from_bytes(gz[off + 16:off + 18], "little") + 1
+            k += 1
+        s_out = torch.empty(k * 65536 + 64, dtype=torch.uint8, device="cuda")
+        tuning = dec.autotune(din, [0], [off], s_out, [0], [s_out.numel()])
+        del s_out
 
     def step():
         n, st = dec.decode_device(din, len(gz), dout, dout.numel(), stream=stream.cuda_stream)
@@ -285,7 +297,8 @@ def run_ours(args, raw, gz, desc):
                            gpu_chunk_bytes=args.gpu_chunk or "auto", gpu_chunks=ms.gpu_chunks,
                            inflate="lane-per-chunk" if args.warps_per_stream < 0 else "warp-per-chunk",
                            boundaries="per target" if args.boundary_mode == 1 else "every offset",
-                           markers=ms.markers, speculation_failures=ms.speculation_failures),
+                           markers=ms.markers, speculation_failures=ms.speculation_failures,
+                           graph_launches=ms.graph_launches, autotuned=tuning),
             "e2e": {"value": round(e2e_value, 3), "unit": "GB/s", "h2d_bytes_per_step": C_,
                     "d2h_bytes_per_step": U_},
             "gpu_launches": int(launches),
@@ -302,13 +315,197 @@ def run_ours(args, raw, gz, desc):
     dec.close()
 
 
+def run_files_reference(args):
+    """Reference arm of the many-files workload: the oracle port decodes files
+    one after another on all host threads, within a bounded sample per step."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+    from rusty_rapidgzip_b200 import workloads as W
+    threads = os.cpu_count() or 1
+    files = list(W.config3_stream(args.size or 2000, seed=3))
+    nb, t_all, it = 0, 0.0, 0
+    for _ in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        done = 0
+        while time.perf_counter() - t0 < 5.0:
+            raw, gz = files[it % len(files)]
+            it += 1
+            n, _ = oracle.read_gz_count(gz, num_threads=threads)
+            assert n == len(raw)
+            done += n
+        if _ >= args.warmup:
+            nb += done
+            t_all += time.perf_counter() - t0
+    value = nb / t_all / 1e9
+    line = {"metric": "decompressed GB/s", "value": round(value, 3), "unit": "GB/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1000 * t_all / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator)",
+            "config": {"workload": "independent_gzip_files_log_uniform_4KiB_256MiB_mixed_content",
+                       "files": len(files), "parallelism": "cpu threads"},
+            "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+                             "sample": "5 s of files in order per step, oracle/ C restatement on all host threads"},
+            "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_files(args):
+    """Many independent gzip files (log-uniform 4 KiB - 256 MiB, four content
+    kinds) decoded as one batch per step: device-resident batch time (value),
+    the plain path (one decode_device per file) for comparison, and end to end
+    with host buffers."""
+    import hashlib
+    import torch
+    import torch.distributed as dist
+    from rusty_rapidgzip_b200 import Config, Decoder, kernel_launch_count
+    from rusty_rapidgzip_b200 import workloads as W
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local))
+    n_files = args.size or 2000
+    t_gen = time.perf_counter()
+    gzs, sums, lens = [], [], []
+    sample = []  # (raw, gz) of a few files for the CPU baseline and the tuner
+    for i, (raw, gz) in enumerate(W.config3_stream(n_files, seed=3)):
+        gzs.append(gz)
+        sums.append(hashlib.sha256(raw).digest())
+        lens.append(len(raw))
+        if len(raw) < (32 << 20) and len(sample) < 64 and i % 3 == 0:
+            sample.append((raw, gz))
+    t_gen = time.perf_counter() - t_gen
+    in_off = np.cumsum([0] + [len(g) for g in gzs])[:-1].tolist()
+    in_len = [len(g) for g in gzs]
+    out_off = np.cumsum([0] + lens)[:-1].tolist()
+    C_, U_ = sum(in_len), sum(lens)
+    blob = np.empty(C_, dtype=np.uint8)
+    for g, o in zip(gzs, in_off):
+        blob[o:o + len(g)] = np.frombuffer(g, dtype=np.uint8)
+    del gzs
+    din = torch.from_numpy(blob).cuda()
+    dout = torch.empty(U_ + 64, dtype=torch.uint8, device="cuda")
+    dec = Decoder(Config(device=local))
+    stream = torch.cuda.Stream()
+    # ---- autotune on a sample (untimed)
+    s_gz = [g for _, g in sample]
+    s_raw = [r for r, _ in sample]
+    s_in = torch.from_numpy(np.frombuffer(b"".join(s_gz), dtype=np.uint8).copy()).cuda()
+    s_out = torch.empty(sum(len(r) for r in s_raw) + 64, dtype=torch.uint8, device="cuda")
+    tuning = dec.autotune(s_in, np.cumsum([0] + [len(g) for g in s_gz])[:-1].tolist(), [len(g) for g in s_gz],
+                          s_out, np.cumsum([0] + [len(r) for r in s_raw])[:-1].tolist(), [len(r) for r in s_raw])
+    del s_in, s_out
+
+    def step():
+        got, status, st = dec.decode_batch(din, in_off, in_len, dout, out_off, lens, stream=stream.cuda_stream)
+        assert status == [0] * n_files, [x for x in status if x][:5]
+        return st
+
+    for _ in range(max(args.warmup, 1)):
+        step()
+    torch.cuda.synchronize()
+    host = dout.cpu().numpy()
+    for o, n, h in zip(out_off, lens, sums):
+        if hashlib.sha256(host[o:o + n].tobytes()).digest() != h:
+            raise SystemExit("decoded bytes differ from the generator output")
+    del host
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        l0 = kernel_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        stats = [step() for _ in range(args.steps)]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        launches = kernel_launch_count() - l0
+    t = e0.elapsed_time(e1) / 1000.0
+    if world > 1:
+        tt = torch.tensor([t], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt.item())
+    value = world * U_ * args.steps / t / 1e9
+    # ---- plain path: one device-resident decode per file, same buffers
+    torch.cuda.synchronize()
+    p0 = torch.cuda.Event(enable_timing=True)
+    p1 = torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    for o, n, io, il in zip(out_off, lens, in_off, in_len):
+        m, _ = dec.decode_device(din[io:], il, dout[o:], n, stream=stream.cuda_stream)
+        assert m == n
+    p1.record(stream)
+    torch.cuda.synchronize()
+    plain = U_ / (p0.elapsed_time(p1) / 1000.0) / 1e9
+    # ---- end to end: pinned host input -> batch -> pinned host output, every step
+    e2e = None
+    try:
+        pin_in = torch.from_numpy(blob).pin_memory()
+        pin_out = torch.empty(U_ + 64, dtype=torch.uint8, pin_memory=True)
+        times = []
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            din.copy_(pin_in, non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+            step()
+            pin_out.copy_(dout, non_blocking=True)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+        te = sum(times)
+        e2e = {"value": round(world * U_ * args.steps / te / 1e9, 3), "unit": "GB/s", "h2d_bytes_per_step": C_,
+               "d2h_bytes_per_step": U_ + 64}
+        del pin_in, pin_out
+    except RuntimeError as ex:  # pinned memory unavailable for this size
+        e2e = {"value": None, "unit": "GB/s", "note": f"pinned buffers unavailable: {ex}"[:200]}
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        import oracle
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        nb = 0
+        for raw, gz in sample:
+            n, _ = oracle.read_gz_count(gz, num_threads=threads)
+            assert n == len(raw)
+            nb += n
+            if time.perf_counter() - t0 > 20:
+                break
+        cpu = {"value": round(nb / (time.perf_counter() - t0) / 1e9, 3), "unit": "GB/s", "cores": threads,
+               "kind": "port", "sample": f"{nb} bytes from up to 64 of the files (< 32 MiB each), one after another, "
+                                         "oracle/ C restatement of the reference pipeline on all host threads"}
+    if rank == 0:
+        st = stats[-1]
+        kern = {k: round(statistics.mean(s_.timings_ms[k] for s_ in stats), 3)
+                for k in ("finder", "inflate", "resolve", "crc")}
+        line = {
+            "metric": "decompressed GB/s", "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * t / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded generator)",
+            "config": {"workload": "independent_gzip_files_log_uniform_4KiB_256MiB_mixed_content",
+                       "files": n_files, "uncompressed_bytes": U_, "compressed_bytes": C_,
+                       "parallelism": f"replicas x{world}", "l2": "inputs larger than L2; no flush",
+                       "plain_per_file_gbs": round(plain, 3), "autotuned": tuning,
+                       "gpu_chunks": st.gpu_chunks, "generation_s": round(t_gen, 1)},
+            "e2e": e2e, "gpu_launches": int(launches), "kernels_ms": kern,
+            "clocks": clk.summary(), "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    dec.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="zipf1g", choices=["zipf1g", "fastq64m", "bgzf"])
+    ap.add_argument("--workload", default="zipf1g", choices=["zipf1g", "fastq64m", "bgzf", "files"])
     ap.add_argument("--size", type=int, default=None)
     ap.add_argument("--gpu-chunk", type=int, default=0)
     ap.add_argument("--warps-per-stream", type=int, default=0, help="-1: one decoder per lane")
@@ -317,6 +514,12 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         print("note: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.workload == "files":
+        if args.impl == "reference":
+            run_files_reference(args)
+        else:
+            run_files(args)
+        return
     raw, gz, desc = workload(args.workload, args.size)
     if args.impl == "reference":
         run_reference(args, raw, gz, desc)

@@ -274,8 +274,19 @@ def config3_sizes(n_files: int = 2000, seed: int = 3, lo: int = 4 << 10, hi: int
 
 def config3_files(n_files: int = 2000, seed: int = 3, lo: int = 4 << 10, hi: int = 256 << 20):
     """Independent single-member gzip files of log-uniform size and mixed content."""
-    files = []
-    for size, kind, s in config3_sizes(n_files, seed, lo, hi):
+    return [(raw, gz) for raw, gz in config3_stream(n_files, seed, lo, hi)]
+
+
+def config3_stream(n_files: int = 2000, seed: int = 3, lo: int = 4 << 10, hi: int = 256 << 20,
+                   threads: int | None = None):
+    """config3_files generated in parallel, yielded in order as (raw, gz)."""
+    import os
+    spec = config3_sizes(n_files, seed, lo, hi)
+
+    def one(t):
+        size, kind, s = t
         raw = make_content(kind, size, s)
-        files.append((raw, gzip_member(raw, CONTENT_LEVEL[kind])))
-    return files
+        return raw, gzip_member(raw, CONTENT_LEVEL[kind])
+
+    with ThreadPoolExecutor(max_workers=threads or os.cpu_count()) as ex:
+        yield from ex.map(one, spec)
