@@ -455,8 +455,21 @@ __device__ void stored_block(WarpSmem& S, ItemState& st, CellT* out, int lane) {
         return;
     }
     if (!st.counting && st.cur + len > st.cap) st.counting = true;
-    if (!st.counting)
-        for (uint32_t i = lane; i < len; i += 32) out[st.cur + i] = (CellT)src_byte(st.br.s, bp + i);
+    if (!st.counting) {
+        // bounds were checked above: plain byte loads, 16 per lane in flight,
+        // each load and store instruction covering 32 consecutive bytes/cells
+        const uint8_t* src = st.br.s.base + st.br.s.lo + bp;
+        CellT* dst = out + st.cur;
+        uint32_t i = 0;
+        for (; i + 512 <= len; i += 512) {
+            uint32_t v[16];
+#pragma unroll
+            for (int k = 0; k < 16; k++) v[k] = __ldg(src + i + 32 * k + lane);
+#pragma unroll
+            for (int k = 0; k < 16; k++) dst[i + 32 * k + lane] = (CellT)v[k];
+        }
+        for (i += lane; i < len; i += 32) dst[i] = (CellT)__ldg(src + i);
+    }
     st.cur += len;
     if (lane == 0) br_seek(st.br, (bp + len) * 8);
     __syncwarp();
