@@ -207,17 +207,47 @@ int rrg_gpu_decode_chunk(rrg_ctx* ctx, const uint8_t* d_body, size_t body_len,
 
 /* ---- serving loop (continuous batching under an HBM budget) ---- */
 
+/* The reference has no serving loop; this is the request path a service puts
+ * on top of read_gz (lib.rs:366-496). Engines are sub-contexts, each with its
+ * own stream, device scratch (resident across requests) and host thread. An
+ * idle engine takes the oldest waiting requests whose device bytes (input,
+ * output from the trailer's ISIZE, decode scratch) fit the HBM budget
+ * (rrg_config.hbm_budget_bytes) next to the requests already admitted, and
+ * decodes them as one batch (rrg_gpu_decode_batch's path). Requests submitted
+ * while other batches run join the next batch an engine takes, so several
+ * batches overlap on the device. Finished requests wait in a bounded
+ * completion queue; engines take no new work while it is full. */
+
+/* Counters of the serving loop. */
+typedef struct rrg_serve_stats {
+    uint64_t submitted, completed, batches;
+    uint64_t max_batch;          /* most requests decoded together in one batch */
+    uint64_t engines_busy, max_engines_busy;
+    uint64_t in_use_bytes, peak_in_use_bytes, budget_bytes;
+    uint64_t waiting;            /* submitted, not yet admitted */
+    uint64_t bytes_out;          /* decompressed bytes finished */
+} rrg_serve_stats;
+
+/* Start the serving loop with `engines` engines (0 = 2) and a completion queue
+ * of `max_ready` entries (0 = 64). rrg_gpu_submit starts it with the defaults
+ * if it is not running. */
+int rrg_gpu_serve_start(rrg_ctx* ctx, uint32_t engines, uint32_t max_ready, rrg_error* err);
+
+/* Stop the engines (waits for the batches on the device); unpolled results are
+ * dropped. rrg_gpu_destroy calls it. */
+void rrg_gpu_serve_stop(rrg_ctx* ctx);
+
+int rrg_gpu_serve_stats(rrg_ctx* ctx, rrg_serve_stats* out);
+
 /* Submit a whole gzip file held in host memory (copied at submit). Returns a
- * request id >= 0, or -1 on error. Requests are admitted to the GPU as slots
- * and HBM budget free up; admitted requests' work overlaps on the device. */
+ * request id >= 0, or -1 on error. */
 int64_t rrg_gpu_submit(rrg_ctx* ctx, const uint8_t* data, size_t len, rrg_error* err);
 
-/* Drive the serving loop once and collect one finished request if any.
- * Returns 1 and fills the outputs when a request finished, 0 if none finished
- * within `timeout_ms`, or a negative rrg_status on failure. `*out` is a
- * malloc'd buffer the caller frees with rrg_gpu_free; `*latency_ms` is
- * submit-to-finish wall time. A request that failed returns 1 with
- * *status != RRG_OK and *out == NULL. */
+/* Collect one finished request, waiting up to `timeout_ms`. Returns 1 and
+ * fills the outputs, 0 if none finished in time, or a negative rrg_status on
+ * failure. `*out` is a malloc'd buffer the caller frees with rrg_gpu_free;
+ * `*latency_ms` is submit-to-finish wall time. A request that failed returns 1
+ * with *status != RRG_OK and *out == NULL. */
 int rrg_gpu_poll(rrg_ctx* ctx, int64_t* request_id, uint8_t** out, size_t* out_len,
                  int32_t* status, double* latency_ms, int32_t timeout_ms, rrg_error* err);
 

@@ -90,6 +90,12 @@ class _Tuning(C.Structure):
                 ("trials", C.c_uint32)]
 
 
+class _ServeStats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("submitted", "completed", "batches", "max_batch", "engines_busy",
+                                          "max_engines_busy", "in_use_bytes", "peak_in_use_bytes", "budget_bytes",
+                                          "waiting", "bytes_out")]
+
+
 class _Stats(C.Structure):
     _fields_ = ([(n, C.c_uint64) for n in _STAT_U64] + [(n, C.c_double) for n in _STAT_F64]
                 + [("graph_launches", C.c_uint64)])
@@ -249,6 +255,10 @@ def load_library(path: str | None = None):
         L.rrg_gpu_submit.restype = C.c_int64
         L.rrg_gpu_poll.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(sz),
                                    C.POINTER(i32), C.POINTER(C.c_double), i32, E]
+        L.rrg_gpu_serve_start.argtypes = [vp, C.c_uint32, C.c_uint32, E]
+        L.rrg_gpu_serve_stop.argtypes = [vp]
+        L.rrg_gpu_serve_stop.restype = None
+        L.rrg_gpu_serve_stats.argtypes = [vp, C.POINTER(_ServeStats)]
         L.rrg_gpu_pending.argtypes = [vp]
         L.rrg_gpu_pending.restype = C.c_int64
         L.rrg_gpu_crc32_noalloc.argtypes = [vp, sz, C.POINTER(C.c_uint32), vp, E]
@@ -486,6 +496,20 @@ class Decoder:
 
     def pending(self) -> int:
         return int(self._L.rrg_gpu_pending(self._ctx))
+
+    def serve_start(self, engines: int = 0, max_ready: int = 0):
+        """Start the serving loop (rrg_gpu_serve_start); submit() starts it with defaults."""
+        e = _Error()
+        self._L.rrg_gpu_serve_start(self._ctx, engines, max_ready, C.byref(e))
+        _raise(e)
+
+    def serve_stop(self):
+        self._L.rrg_gpu_serve_stop(self._ctx)
+
+    def serve_stats(self) -> dict:
+        st = _ServeStats()
+        self._L.rrg_gpu_serve_stats(self._ctx, C.byref(st))
+        return {f: int(getattr(st, f)) for f, _ in _ServeStats._fields_}
 
 
 def read_gz(path, sink, config: Config | None = None) -> DecodeStats:

@@ -27,6 +27,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <condition_variable>
 #include <deque>
 #include <unordered_map>
 #include <mutex>
@@ -203,6 +204,10 @@ int64_t host_bgzf_size(const uint8_t* in, size_t len) {
     return -1;
 }
 
+uint64_t le32h(const uint8_t* p) {
+    return (uint64_t)p[0] | ((uint64_t)p[1] << 8) | ((uint64_t)p[2] << 16) | ((uint64_t)p[3] << 24);
+}
+
 struct DBuf {
     void* p = nullptr;
     size_t cap = 0;
@@ -260,15 +265,45 @@ struct rrg_ctx {
     rrg_stats st{};
     uint64_t launches = 0;
 
-    // serving
-    std::mutex srv_mu;
+    // serving loop (created on first use)
+    struct Server* srv = nullptr;
+    std::mutex srv_create_mu;
+};
+
+// Serving loop. Each engine is a sub-context with its own stream and
+// device scratch, resident across requests, and its own host thread. An idle
+// engine takes the oldest waiting requests that fit the HBM budget together
+// (continuous batching: requests that arrive while other batches are on the
+// GPU join the next batch an engine takes) and decodes them as one batch;
+// engines overlap on the device. Finished requests wait in a bounded
+// completion queue: engines stop taking work while it is full.
+struct Server {
     struct Req {
         int64_t id;
         std::vector<uint8_t> data;
         double t_submit;
+        uint64_t out_need = 0;  // exact output size once known (a retry after RRG_ERR_CAPACITY)
     };
-    std::deque<Req> srv_queue;
-    int64_t srv_next_id = 0;
+    struct Done {
+        int64_t id;
+        uint8_t* out;
+        size_t len;
+        int32_t status;
+        double t_submit;
+        double latency_ms;
+    };
+    std::vector<rrg_ctx*> engines;
+    std::vector<std::thread> threads;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Req> waiting;
+    std::deque<Done> done;
+    uint64_t budget = 0, in_use = 0;
+    uint32_t max_ready = 64, max_batch = 64;
+    bool stop = false;
+    int64_t next_id = 0;
+    int64_t outstanding = 0;  // submitted and not yet polled
+    rrg_serve_stats stats{};
 };
 
 namespace {
@@ -1800,6 +1835,178 @@ int autotune_impl(rrg_ctx* c, const uint8_t* d_in, const uint64_t* in_off, const
     return 0;
 }
 
+// ------------------------------------------------------------ serving engines
+// Device bytes a request holds while admitted: its input, its output and
+// the speculative-decode scratch (u16 cells plus slack), from the trailer's
+// ISIZE as the size hint.
+uint64_t serve_reserve(const Server::Req& r, double expand_cap) {
+    const uint64_t c = r.data.size();
+    const uint64_t isz = c >= 4 ? le32h(r.data.data() + c - 4) : 0;
+    const uint64_t out = r.out_need ? r.out_need : std::max<uint64_t>(isz, c);
+    const double ex = c ? std::min(expand_cap, std::max(1.05, 1.25 * (double)out / (double)c + 0.05)) : 1.0;
+    return c + out + (uint64_t)(2.0 * 1.6 * ex * (double)c) + (2ull << 20);
+}
+
+void engine_loop(Server* S, rrg_ctx* E) {
+    if (E->cfg.device >= 0) cudaSetDevice(E->cfg.device);
+    else cudaSetDevice(E->device);
+    for (;;) {
+        std::vector<Server::Req> batch;
+        uint64_t reserved = 0;
+        {
+            std::unique_lock<std::mutex> lk(S->mu);
+            S->cv_work.wait(lk, [&] {
+                if (S->stop) return true;
+                if (S->waiting.empty() || S->done.size() >= S->max_ready) return false;
+                return S->in_use == 0 || S->in_use + serve_reserve(S->waiting.front(), E->expand) <= S->budget;
+            });
+            if (S->stop) return;
+            // the oldest waiting requests that fit together (at least one)
+            while (!S->waiting.empty() && batch.size() < S->max_batch) {
+                const uint64_t r = serve_reserve(S->waiting.front(), E->expand);
+                if (!batch.empty() || S->in_use) {
+                    if (S->in_use + reserved + r > S->budget) break;
+                }
+                reserved += r;
+                batch.push_back(std::move(S->waiting.front()));
+                S->waiting.pop_front();
+                if (S->in_use + reserved > S->budget) break;  // a lone request above the budget
+            }
+            S->in_use += reserved;
+            S->stats.batches++;
+            S->stats.max_batch = std::max<uint64_t>(S->stats.max_batch, batch.size());
+            S->stats.engines_busy++;
+            S->stats.max_engines_busy = std::max(S->stats.max_engines_busy, S->stats.engines_busy);
+            S->stats.peak_in_use_bytes = std::max(S->stats.peak_in_use_bytes, S->in_use);
+        }
+        // ---- one batch on this engine's stream
+        const size_t n = batch.size();
+        std::vector<uint64_t> in_off(n), in_len(n), out_off(n), out_cap(n), out_len(n, 0);
+        std::vector<int32_t> status(n, RRG_OK);
+        uint64_t ti = 0, to = 0;
+        for (size_t i = 0; i < n; i++) {
+            const Server::Req& r = batch[i];
+            const uint64_t c = r.data.size();
+            const uint64_t isz = c >= 4 ? le32h(r.data.data() + c - 4) : 0;
+            in_off[i] = ti;
+            in_len[i] = c;
+            ti += (c + 255) & ~255ull;
+            out_off[i] = to;
+            out_cap[i] = r.out_need ? r.out_need : std::max<uint64_t>(isz, c);
+            to += (out_cap[i] + 255) & ~255ull;
+        }
+        rrg_error err{};
+        int rc = 0;
+        auto fail_all = [&](int code) {
+            for (size_t i = 0; i < n; i++) status[i] = code;
+        };
+        if (dgrow(E->comp, ti + 64) != cudaSuccess || dgrow(E->out, to + 64) != cudaSuccess) {
+            fail_all(RRG_ERR_OUT_OF_MEMORY);
+        } else {
+            for (size_t i = 0; i < n && !rc; i++)
+                if (in_len[i] && cudaMemcpyAsync((uint8_t*)E->comp.p + in_off[i], batch[i].data.data(), in_len[i],
+                                                 cudaMemcpyHostToDevice, E->stream) != cudaSuccess)
+                    rc = RRG_ERR_CUDA;
+            if (!rc) {
+                E->st = rrg_stats{};
+                rc = batch_impl(E, (const uint8_t*)E->comp.p, in_off.data(), in_len.data(), (uint8_t*)E->out.p,
+                                out_off.data(), out_cap.data(), out_len.data(), status.data(), n, &err);
+            }
+            if (rc) fail_all(rc);
+        }
+        std::vector<Server::Done> fin;
+        std::vector<Server::Req> retry;
+        for (size_t i = 0; i < n; i++) {
+            Server::Req& r = batch[i];
+            if (status[i] == RRG_ERR_CAPACITY && !r.out_need && out_len[i] > out_cap[i]) {
+                r.out_need = out_len[i];  // the ISIZE hint was short (several members): again, exact
+                retry.push_back(std::move(r));
+                continue;
+            }
+            Server::Done d{r.id, nullptr, 0, status[i], r.t_submit, 0.0};
+            if (status[i] == RRG_OK) {
+                d.out = (uint8_t*)std::malloc(std::max<uint64_t>(out_len[i], 1));
+                d.len = out_len[i];
+                if (!d.out) {
+                    d.status = RRG_ERR_OUT_OF_MEMORY;
+                    d.len = 0;
+                } else if (out_len[i] && cudaMemcpyAsync(d.out, (const uint8_t*)E->out.p + out_off[i], out_len[i],
+                                                         cudaMemcpyDeviceToHost, E->stream) != cudaSuccess) {
+                    d.status = RRG_ERR_CUDA;
+                }
+            }
+            fin.push_back(d);
+        }
+        cudaStreamSynchronize(E->stream);
+        const double t_fin = now_ms();
+        {
+            std::lock_guard<std::mutex> g(S->mu);
+            S->in_use -= reserved;
+            S->stats.engines_busy--;
+            for (auto& r : retry) S->waiting.push_front(std::move(r));
+            for (auto& d : fin) {
+                if (d.status != RRG_OK && d.out) {
+                    std::free(d.out);
+                    d.out = nullptr;
+                    d.len = 0;
+                }
+                d.latency_ms = t_fin - d.t_submit;
+                S->done.push_back(d);
+                S->stats.completed++;
+                S->stats.bytes_out += d.len;
+            }
+            S->cv_done.notify_all();
+            S->cv_work.notify_all();
+        }
+    }
+}
+
+int serve_start(rrg_ctx* c, uint32_t engines, uint32_t max_ready, rrg_error* err) {
+    std::lock_guard<std::mutex> g(c->srv_create_mu);
+    if (c->srv) return 0;
+    Server* S = new Server();
+    S->budget = c->cfg.hbm_budget_bytes;
+    if (max_ready) S->max_ready = max_ready;
+    const uint32_t ne = engines ? std::min<uint32_t>(engines, 8) : 2;
+    for (uint32_t i = 0; i < ne; i++) {
+        rrg_config cfg = c->cfg;
+        cfg.device = c->device;
+        rrg_ctx* E = rrg_gpu_create(&cfg, err);
+        if (!E) {
+            for (rrg_ctx* x : S->engines) rrg_gpu_destroy(x);
+            delete S;
+            return err ? err->code : RRG_ERR_CUDA;
+        }
+        // the owner's tuned settings
+        E->gpu_chunk = c->gpu_chunk;
+        E->scan_bounds = c->scan_bounds;
+        E->scan_threads = c->scan_threads;
+        E->warps_per_member = c->warps_per_member;
+        E->lanes = c->lanes;
+        S->engines.push_back(E);
+    }
+    for (rrg_ctx* E : S->engines) S->threads.emplace_back(engine_loop, S, E);
+    c->srv = S;
+    return 0;
+}
+
+void serve_stop(rrg_ctx* c) {
+    std::lock_guard<std::mutex> g(c->srv_create_mu);
+    Server* S = c->srv;
+    if (!S) return;
+    {
+        std::lock_guard<std::mutex> l(S->mu);
+        S->stop = true;
+        S->cv_work.notify_all();
+    }
+    for (auto& t : S->threads) t.join();
+    for (rrg_ctx* E : S->engines) rrg_gpu_destroy(E);
+    for (auto& d : S->done)
+        if (d.out) std::free(d.out);
+    delete S;
+    c->srv = nullptr;
+}
+
 }  // namespace
 
 // ====================================================================== C ABI
@@ -1857,6 +2064,7 @@ rrg_ctx* rrg_gpu_create(const rrg_config* cfg, rrg_error* err) {
 
 void rrg_gpu_destroy(rrg_ctx* c) {
     if (!c) return;
+    serve_stop(c);
     DBuf* bufs[] = {&c->cand, &c->ncand, &c->vflag, &c->lane_scratch, &c->win, &c->items,  &c->results, &c->order,     &c->queue,    &c->mbs,      &c->mbcount,   &c->cells,
                     &c->out,    &c->targets, &c->limits,    &c->found,    &c->next_lut, &c->chunks,    &c->tiles,
                     &c->rerr,   &c->markers, &c->crc_table, &c->pieces,   &c->piece_crc, &c->mpiece,   &c->exp_crc,
@@ -2161,63 +2369,84 @@ int rrg_gpu_decode_chunk(rrg_ctx* c, const uint8_t* d_body, size_t body_len, uin
     return 0;
 }
 
+int rrg_gpu_serve_start(rrg_ctx* c, uint32_t engines, uint32_t max_ready, rrg_error* err) {
+    if (!c) {
+        set_err(err, RRG_ERR_INVALID_ARGUMENT, "null context");
+        return RRG_ERR_INVALID_ARGUMENT;
+    }
+    return serve_start(c, engines, max_ready, err);
+}
+
+void rrg_gpu_serve_stop(rrg_ctx* c) {
+    if (c) serve_stop(c);
+}
+
+int rrg_gpu_serve_stats(rrg_ctx* c, rrg_serve_stats* out) {
+    if (!c || !out) return RRG_ERR_INVALID_ARGUMENT;
+    std::memset(out, 0, sizeof(*out));
+    if (!c->srv) return 0;
+    std::lock_guard<std::mutex> g(c->srv->mu);
+    *out = c->srv->stats;
+    out->in_use_bytes = c->srv->in_use;
+    out->budget_bytes = c->srv->budget;
+    out->waiting = c->srv->waiting.size();
+    return 0;
+}
+
 int64_t rrg_gpu_submit(rrg_ctx* c, const uint8_t* data, size_t len, rrg_error* err) {
     if (!c || (!data && len)) {
         set_err(err, RRG_ERR_INVALID_ARGUMENT, "null argument");
         return -1;
     }
-    std::lock_guard<std::mutex> g(c->srv_mu);
-    rrg_ctx::Req r;
-    r.id = c->srv_next_id++;
+    const double t0 = now_ms();
+    if (!c->srv) {
+        int rc = serve_start(c, 0, 0, err);
+        if (rc) return -1;
+    }
+    Server* S = c->srv;
+    Server::Req r;
+    r.t_submit = t0;
     r.data.assign(data, data + len);
-    r.t_submit = now_ms();
-    c->srv_queue.push_back(std::move(r));
-    return c->srv_queue.back().id;
+    std::lock_guard<std::mutex> g(S->mu);
+    r.id = S->next_id++;
+    const int64_t id = r.id;
+    S->waiting.push_back(std::move(r));
+    S->outstanding++;
+    S->stats.submitted++;
+    S->cv_work.notify_all();
+    return id;
 }
 
 int rrg_gpu_poll(rrg_ctx* c, int64_t* request_id, uint8_t** out, size_t* out_len, int32_t* status, double* latency_ms,
                  int32_t timeout_ms, rrg_error* err) {
-    (void)timeout_ms;
     if (!c || !request_id || !out || !out_len || !status) {
         set_err(err, RRG_ERR_INVALID_ARGUMENT, "null argument");
         return -RRG_ERR_INVALID_ARGUMENT;
     }
-    rrg_ctx::Req r;
-    {
-        std::lock_guard<std::mutex> g(c->srv_mu);
-        if (c->srv_queue.empty()) return 0;
-        r = std::move(c->srv_queue.front());
-        c->srv_queue.pop_front();
-    }
-    struct Coll {
-        std::vector<uint8_t> v;
-    } coll;
-    auto sink = [](void* u, const uint8_t* p, size_t n) -> int {
-        auto* cc = (Coll*)u;
-        cc->v.insert(cc->v.end(), p, p + n);
-        return 0;
-    };
-    rrg_error e2;
-    int rc = decode_host_impl(c, r.data.data(), r.data.size(), sink, &coll, nullptr, &e2);
-    *request_id = r.id;
-    *status = rc;
-    *latency_ms = now_ms() - r.t_submit;
-    if (rc) {
-        *out = nullptr;
-        *out_len = 0;
-        if (err) *err = e2;
-        return 1;
-    }
-    *out = (uint8_t*)std::malloc(std::max<size_t>(coll.v.size(), 1));
-    if (!coll.v.empty()) std::memcpy(*out, coll.v.data(), coll.v.size());
-    *out_len = coll.v.size();
+    if (!c->srv) return 0;
+    Server* S = c->srv;
+    std::unique_lock<std::mutex> lk(S->mu);
+    if (S->done.empty() && timeout_ms > 0)
+        S->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] { return !S->done.empty(); });
+    if (S->done.empty()) return 0;
+    Server::Done d = S->done.front();
+    S->done.pop_front();
+    S->outstanding--;
+    S->cv_work.notify_all();  // room in the completion queue
+    lk.unlock();
+    *request_id = d.id;
+    *out = d.out;
+    *out_len = d.len;
+    *status = d.status;
+    if (latency_ms) *latency_ms = d.latency_ms;
     return 1;
 }
 
 int64_t rrg_gpu_pending(rrg_ctx* c) {
     if (!c) return -1;
-    std::lock_guard<std::mutex> g(c->srv_mu);
-    return (int64_t)c->srv_queue.size();
+    if (!c->srv) return 0;
+    std::lock_guard<std::mutex> g(c->srv->mu);
+    return c->srv->outstanding;
 }
 
 void rrg_gpu_free(void* p) { std::free(p); }

@@ -129,3 +129,48 @@ def bgzf_cases():
     bad[m1 - 8] ^= 0x40  # second member's CRC
     return {"chain": small + eof, "false-headers": fake, "then-plain": small + plain, "truncated": cut,
             "crc": bytes(bad)}
+
+
+def serve_requests(n: int, seed: int, hi: int):
+    """Mixed decode requests for the serving loop: the four content kinds of the
+    many-files workload at log-uniform sizes up to `hi` bytes, plus a BGZF file,
+    a two-member file and a request with a corrupt CRC."""
+    from rusty_rapidgzip_b200 import workloads as W
+    reqs = [gz for _, gz in W.config3_files(n_files=n, seed=seed, lo=4 << 10, hi=hi)]
+    reqs.append(W.bgzf(W.fastq_like(200_000, seed), 5, block=20_000))
+    reqs.append(gzip_cli(b"first member " * 500) + gzip_cli(b"second member " * 4000))
+    bad = bytearray(gzip_cli(b"payload with a broken trailer " * 100))
+    bad[-8] ^= 0x10
+    reqs.append(bytes(bad))
+    return reqs
+
+
+def run_serving(d, reqs, seed: int, gap_s: float):
+    """Submit `reqs` from a thread at random gaps (open loop) while this thread
+    polls; returns {request index: (status, bytes or None)}."""
+    import random
+    import threading
+    import time
+    rng = random.Random(seed)
+    ids = {}
+    order = list(range(len(reqs)))
+
+    def feeder():
+        for i in order:
+            ids[d.submit(reqs[i])] = i
+            time.sleep(rng.random() * gap_s)
+
+    th = threading.Thread(target=feeder)
+    th.start()
+    got = {}
+    deadline = time.time() + 600
+    while len(got) < len(reqs) and time.time() < deadline:
+        r = d.poll(timeout_ms=200)
+        if r is None:
+            continue
+        rid, data, status, lat = r
+        while rid not in ids:
+            time.sleep(0.001)
+        got[ids[rid]] = (status, data)
+    th.join()
+    return got

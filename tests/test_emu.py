@@ -217,3 +217,25 @@ def test_autotune(emu_decoder_factory):
     assert t["boundary_mode"] in (0, 1) and t["warps_per_member"] == 1  # no BGZF in the sample
     outs, lens, status = run_batch(d, items, dev)
     assert status == [0] and outs == [raw_a]
+
+
+def test_serving_alone_and_in_the_mix(emu_decoder_factory):
+    """Every request's result (bytes and status) is the same decoded alone and
+    in the serving loop's mix, with two engines and a budget small enough that
+    requests queue for admission."""
+    from conftest import run_serving, serve_requests
+    reqs = serve_requests(6, seed=11, hi=96 << 10)
+    alone = emu_decoder_factory()
+    want = {}
+    for i, gz in enumerate(reqs):
+        try:
+            want[i] = (0, alone.decompress(gz))
+        except Exception as e:  # noqa: BLE001 - compared by status code below
+            want[i] = (e.code, None)
+    d = emu_decoder_factory(hbm_budget_bytes=6 << 20)
+    d.serve_start(engines=2, max_ready=4)
+    got = run_serving(d, reqs, seed=1, gap_s=0.0)
+    assert got == want
+    st = d.serve_stats()
+    assert st["completed"] == len(reqs) and st["batches"] >= 2
+    assert d.pending() == 0

@@ -390,3 +390,28 @@ def test_autotune(gpu_decoder_factory):
     assert t["boundary_mode"] in (0, 1) and 1 <= t["warps_per_member"] <= 4
     outs, lens, status = run_batch(d, items, devbuf)
     assert status == [0, 0] and outs == [raw_a, raw_b]
+
+
+@pytest.mark.gpu
+def test_serving_alone_and_in_the_mix(gpu_decoder_factory):
+    """Serving loop: each request's bytes and status are the same decoded alone
+    and in the mix; requests queue for a 256 MiB budget, batches hold several
+    requests (continuous batching) and both engines run at once (overlap)."""
+    from conftest import run_serving, serve_requests
+    reqs = serve_requests(40, seed=12, hi=24 << 20)
+    alone = gpu_decoder_factory()
+    want = {}
+    for i, gz in enumerate(reqs):
+        try:
+            want[i] = (0, alone.decompress(gz))
+        except Exception as e:  # noqa: BLE001 - compared by status code below
+            want[i] = (e.code, None)
+    budget = 256 << 20
+    d = gpu_decoder_factory(hbm_budget_bytes=budget)
+    d.serve_start(engines=2, max_ready=8)
+    got = run_serving(d, reqs, seed=2, gap_s=0.002)
+    assert got == want
+    st = d.serve_stats()
+    assert st["completed"] == len(reqs) and d.pending() == 0
+    assert st["max_batch"] >= 2 and st["max_engines_busy"] == 2
+    assert st["peak_in_use_bytes"] > 0
