@@ -315,6 +315,122 @@ def run_ours(args, raw, gz, desc):
     dec.close()
 
 
+def run_serve(args):
+    """Serving: open-loop Poisson arrivals of decode requests (sizes log-uniform
+    64 KiB - 1 GiB, content mixed as in the many-files workload) at each rate
+    for --duration seconds, through submit/poll with the HBM budget. At most
+    --max-outstanding requests may be waiting (later arrivals are counted as
+    rejected) so host memory stays bounded when a rate exceeds capacity."""
+    import hashlib
+    import random
+    import threading
+    import ctypes as C
+    import torch
+    from concurrent.futures import ThreadPoolExecutor
+    from rusty_rapidgzip_b200 import Config, Decoder
+    from rusty_rapidgzip_b200 import workloads as W
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    torch.cuda.set_device(0)
+    n_pool = args.size or 48
+    t_gen = time.perf_counter()
+    pool, sums, lens = [], [], []
+    for raw, gz in W.config3_stream(n_pool, seed=4, lo=64 << 10, hi=1 << 30):
+        pool.append(gz)
+        sums.append(hashlib.sha256(raw).digest())
+        lens.append(len(raw))
+    t_gen = time.perf_counter() - t_gen
+    rates = [float(x) for x in args.rates.split(",")]
+    dec = Decoder(Config(device=0))
+    dec.serve_start(engines=2, max_ready=16)
+    # warm-up: every pool item once (untimed; grows the engines' resident scratch)
+    for gz in pool:
+        dec.submit(gz)
+    for _ in pool:
+        while dec.poll(timeout_ms=1000) is None:
+            pass
+    per_rate = []
+    hasher = ThreadPoolExecutor(max_workers=4)
+    for rate in rates:
+        rng = random.Random(int(rate * 1000))
+        sched, lock = {}, threading.Lock()
+        done, bad = [], []
+        rejected = [0]
+
+        def feeder():
+            t0 = time.perf_counter()
+            t = t0
+            while True:
+                t += rng.expovariate(rate)
+                if t - t0 > args.duration:
+                    break
+                now = time.perf_counter()
+                if t > now:
+                    time.sleep(t - now)
+                k = rng.randrange(n_pool)
+                if dec.pending() >= args.max_outstanding:
+                    rejected[0] += 1
+                    continue
+                rid = dec.submit(pool[k])
+                with lock:
+                    sched[rid] = (t, k)
+
+        def check(addr, n, k):
+            ok = n == lens[k] and hashlib.sha256((C.c_uint8 * n).from_address(addr)).digest() == sums[k]
+            dec.free(addr)
+            return ok
+
+        th = threading.Thread(target=feeder)
+        t_start = time.perf_counter()
+        th.start()
+        futs = []
+        while th.is_alive() or dec.pending() > 0:
+            r = dec.poll_raw(timeout_ms=100)
+            if r is None:
+                continue
+            now = time.perf_counter()
+            rid, addr, n, status, _ = r
+            while True:
+                with lock:
+                    if rid in sched:
+                        t_arr, k = sched.pop(rid)
+                        break
+                time.sleep(0.0005)
+            done.append((now - t_arr, lens[k], now))
+            if status != 0:
+                bad.append(status)
+                dec.free(addr)
+            else:
+                futs.append(hasher.submit(check, addr, n, k))
+        th.join()
+        ok = all(f.result() for f in futs)
+        if bad or not ok:
+            raise SystemExit(f"serving produced wrong results at {rate} req/s: statuses {bad[:5]}, bytes ok {ok}")
+        lat = sorted(x[0] * 1000 for x in done)
+        span = max(x[2] for x in done) - t_start
+        per_rate.append({"rate_req_s": rate, "completed": len(done), "rejected": rejected[0],
+                         "offered_gbs": round(rate * statistics.mean(lens) / 1e9, 3),
+                         "sustained_gbs": round(sum(x[1] for x in done) / span / 1e9, 3),
+                         "p50_ms": round(lat[len(lat) // 2], 2), "p99_ms": round(lat[min(len(lat) - 1, int(len(lat) * 0.99))], 2)})
+    hasher.shutdown()
+    st = dec.serve_stats()
+    dec.close()
+    top = per_rate[-1]
+    line = {"metric": "decompressed GB/s", "value": top["sustained_gbs"], "unit": "GB/s", "n_gpus": 1,
+            "steps": len(rates), "warmup": 1, "ms_per_step": round(args.duration * 1000, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator)",
+            "config": {"workload": "serving_poisson_requests_log_uniform_64KiB_1GiB_mixed_content",
+                       "pool_requests": n_pool, "pool_uncompressed_bytes": sum(lens),
+                       "duration_s_per_rate": args.duration, "hbm_budget_bytes": st["budget_bytes"], "engines": 2,
+                       "max_outstanding": args.max_outstanding, "per_rate": per_rate,
+                       "serve_stats": st, "generation_s": round(t_gen, 1)},
+            "e2e": {"value": top["sustained_gbs"], "unit": "GB/s",
+                    "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                    "note": "the serving path itself is end to end: host request bytes in, host result bytes out"},
+            "latency_ms": {"p50": top["p50_ms"], "p99": top["p99_ms"]}}
+    print(json.dumps(line), flush=True)
+
+
 def run_files_reference(args):
     """Reference arm of the many-files workload: the oracle port decodes files
     one after another on all host threads, within a bounded sample per step."""
@@ -505,7 +621,10 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="zipf1g", choices=["zipf1g", "fastq64m", "bgzf", "files"])
+    ap.add_argument("--workload", default="zipf1g", choices=["zipf1g", "fastq64m", "bgzf", "files", "serve"])
+    ap.add_argument("--rates", default="10,50,200", help="serve: request rates (req/s)")
+    ap.add_argument("--duration", type=float, default=20.0, help="serve: seconds of arrivals per rate")
+    ap.add_argument("--max-outstanding", type=int, default=32, help="serve: waiting requests before rejecting")
     ap.add_argument("--size", type=int, default=None)
     ap.add_argument("--gpu-chunk", type=int, default=0)
     ap.add_argument("--warps-per-stream", type=int, default=0, help="-1: one decoder per lane")
@@ -514,6 +633,12 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         print("note: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.workload == "serve":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving loop"}))
+        else:
+            run_serve(args)
+        return
     if args.workload == "files":
         if args.impl == "reference":
             run_files_reference(args)

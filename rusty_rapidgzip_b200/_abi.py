@@ -494,6 +494,28 @@ class Decoder:
             self._L.rrg_gpu_free(out)
         return int(rid.value), data, int(stv.value), float(lat.value)
 
+    def poll_raw(self, timeout_ms: int = 0):
+        """Like poll, without copying the result: -> None, or (request_id,
+        address, length, status, latency_ms); release the address with free()."""
+        rid = C.c_int64()
+        out = C.POINTER(C.c_uint8)()
+        n = C.c_size_t()
+        stv = C.c_int32()
+        lat = C.c_double()
+        e = _Error()
+        r = self._L.rrg_gpu_poll(self._ctx, C.byref(rid), C.byref(out), C.byref(n), C.byref(stv), C.byref(lat),
+                                 timeout_ms, C.byref(e))
+        if r < 0:
+            _raise(e)
+        if r == 0:
+            return None
+        addr = C.cast(out, C.c_void_p).value or 0
+        return int(rid.value), addr, int(n.value), int(stv.value), float(lat.value)
+
+    def free(self, addr: int):
+        if addr:
+            self._L.rrg_gpu_free(addr)
+
     def pending(self) -> int:
         return int(self._L.rrg_gpu_pending(self._ctx))
 

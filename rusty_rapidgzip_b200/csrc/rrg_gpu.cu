@@ -660,14 +660,16 @@ int scan_boundaries(rrg_ctx* c, const uint8_t* body, uint64_t blen, std::vector<
     // heavy check; counts stay on the device between the three kernels
     const uint32_t cap = (uint32_t)std::min<uint64_t>(blen / 64 + 65536, 1ull << 28);
     const uint32_t cap2 = std::max<uint32_t>(cap / 16, 65536);
-    CK(dgrow(c->cand, (size_t)cap * 8 + (size_t)cap2 * 8));
+    const uint32_t cap3 = (uint32_t)std::min<uint64_t>(blen / 1024 + 4096, 1ull << 26);
+    CK(dgrow(c->cand, (size_t)cap * 8 + (size_t)cap2 * 8 + (size_t)cap3 * 8));
     CK(dgrow(c->ncand, 64));
     CK(dgrow(c->vflag, cap2));
     CK(cudaMemsetAsync(c->ncand.p, 0, 64, c->stream));
     uint64_t* cand = (uint64_t*)c->cand.p;
     uint64_t* surv = cand + cap;
-    uint32_t* counts = (uint32_t*)c->ncand.p;  // [0] candidates, [1] survivors, [2] heavy queue
-    ScanArgs S{body, blen, cand, counts, cap};
+    uint64_t* stored = surv + cap2;
+    uint32_t* counts = (uint32_t*)c->ncand.p;  // [0] candidates, [1] survivors, [2] heavy queue, [3] stored
+    ScanArgs S{body, blen, cand, counts, cap, stored, counts + 3, cap3};
     // tile width: scan_threads x 16 bytes per block step (64, 128 or 256 threads)
     const uint32_t st = c->scan_threads;
     const uint64_t tb = (uint64_t)st * 16;
@@ -685,9 +687,16 @@ int scan_boundaries(rrg_ctx* c, const uint8_t* body, uint64_t blen, std::vector<
     RRG_LAUNCH(k_verify_heavy, c->n_sm * 4, W * 32, W * sizeof(FindSmem), c->stream, H);
     LAUNCHED(c);
     kt.stop();
-    uint32_t cnt[2] = {0, 0};
-    CK(cudaMemcpyAsync(cnt, counts, 8, cudaMemcpyDeviceToHost, c->stream));
+    uint32_t cnt[4] = {0, 0, 0, 0};
+    CK(cudaMemcpyAsync(cnt, counts, 16, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    if (cnt[3]) {  // stored-block starts need no verification (the anchored chain checks them)
+        const uint32_t ns = std::min(cnt[3], cap3);
+        std::vector<uint64_t> st(ns);
+        CK(cudaMemcpyAsync(st.data(), stored, (size_t)ns * 8, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        verified.insert(verified.end(), st.begin(), st.end());
+    }
     if (cnt[0] > cap || cnt[1] > cap2) {
         set_err(err, RRG_ERR_OUT_OF_MEMORY, "boundary scan: %u candidates exceed the list", cnt[0]);
         return RRG_ERR_OUT_OF_MEMORY;
@@ -1835,6 +1844,25 @@ int autotune_impl(rrg_ctx* c, const uint8_t* d_in, const uint64_t* in_off, const
     return 0;
 }
 
+// Frees every device buffer of the context (they grow again on demand).
+void release_scratch(rrg_ctx* c) {
+    DBuf* bufs[] = {&c->cand, &c->ncand, &c->vflag, &c->lane_scratch, &c->win, &c->items,  &c->results, &c->order,     &c->queue,    &c->mbs,      &c->mbcount,   &c->cells,
+                    &c->out,    &c->targets, &c->limits,    &c->found,    &c->next_lut, &c->chunks,    &c->tiles,
+                    &c->rerr,   &c->markers, &c->crc_table, &c->pieces,   &c->piece_crc, &c->mpiece,   &c->exp_crc,
+                    &c->exp_isize, &c->got_crc, &c->got_len, &c->mstatus, &c->comp, &c->bg_bcount, &c->bg_bbase,
+                    &c->bg_coff, &c->bg_csize, &c->bg_small, &c->sniff, &c->tile_chunk};
+#ifndef RRG_EMU
+    if (c->bg_exec) cudaGraphExecDestroy(c->bg_exec);
+    c->bg_exec = nullptr;
+#endif
+    for (DBuf* b : bufs) {
+        if (b->p) cudaFree(b->p);
+        b->p = nullptr;
+        b->cap = 0;
+    }
+    c->tables_uploaded = false;
+}
+
 // ------------------------------------------------------------ serving engines
 // Device bytes a request holds while admitted: its input, its output and
 // the speculative-decode scratch (u16 cells plus slack), from the trailer's
@@ -1861,9 +1889,13 @@ void engine_loop(Server* S, rrg_ctx* E) {
                 return S->in_use == 0 || S->in_use + serve_reserve(S->waiting.front(), E->expand) <= S->budget;
             });
             if (S->stop) return;
-            // the oldest waiting requests that fit together (at least one)
+            // the oldest waiting requests that fit together (at least one). A
+            // batch stays within this engine's share of the budget, so the
+            // engines' resident scratch stays within the budget as a whole.
+            const uint64_t slice = S->budget / S->engines.size();
             while (!S->waiting.empty() && batch.size() < S->max_batch) {
                 const uint64_t r = serve_reserve(S->waiting.front(), E->expand);
+                if (!batch.empty() && reserved + r > slice) break;
                 if (!batch.empty() || S->in_use) {
                     if (S->in_use + reserved + r > S->budget) break;
                 }
@@ -1900,9 +1932,13 @@ void engine_loop(Server* S, rrg_ctx* E) {
         auto fail_all = [&](int code) {
             for (size_t i = 0; i < n; i++) status[i] = code;
         };
-        if (dgrow(E->comp, ti + 64) != cudaSuccess || dgrow(E->out, to + 64) != cudaSuccess) {
-            fail_all(RRG_ERR_OUT_OF_MEMORY);
-        } else {
+        for (int attempt = 0; attempt < 2; attempt++) {
+            rc = 0;
+            std::fill(status.begin(), status.end(), RRG_OK);
+            if (dgrow(E->comp, ti + 64) != cudaSuccess || dgrow(E->out, to + 64) != cudaSuccess) {
+                cudaGetLastError();
+                rc = RRG_ERR_OUT_OF_MEMORY;
+            }
             for (size_t i = 0; i < n && !rc; i++)
                 if (in_len[i] && cudaMemcpyAsync((uint8_t*)E->comp.p + in_off[i], batch[i].data.data(), in_len[i],
                                                  cudaMemcpyHostToDevice, E->stream) != cudaSuccess)
@@ -1912,8 +1948,12 @@ void engine_loop(Server* S, rrg_ctx* E) {
                 rc = batch_impl(E, (const uint8_t*)E->comp.p, in_off.data(), in_len.data(), (uint8_t*)E->out.p,
                                 out_off.data(), out_cap.data(), out_len.data(), status.data(), n, &err);
             }
-            if (rc) fail_all(rc);
+            if (rc != RRG_ERR_OUT_OF_MEMORY) break;
+            // device memory ran out: drop this engine's resident scratch, once more
+            cudaGetLastError();
+            release_scratch(E);
         }
+        if (rc) fail_all(rc);
         std::vector<Server::Done> fin;
         std::vector<Server::Req> retry;
         for (size_t i = 0; i < n; i++) {
@@ -1939,6 +1979,8 @@ void engine_loop(Server* S, rrg_ctx* E) {
         }
         cudaStreamSynchronize(E->stream);
         const double t_fin = now_ms();
+        // a lone request above this engine's share grew its scratch past it: give it back
+        if (reserved > S->budget / S->engines.size()) release_scratch(E);
         {
             std::lock_guard<std::mutex> g(S->mu);
             S->in_use -= reserved;
@@ -2065,16 +2107,7 @@ rrg_ctx* rrg_gpu_create(const rrg_config* cfg, rrg_error* err) {
 void rrg_gpu_destroy(rrg_ctx* c) {
     if (!c) return;
     serve_stop(c);
-    DBuf* bufs[] = {&c->cand, &c->ncand, &c->vflag, &c->lane_scratch, &c->win, &c->items,  &c->results, &c->order,     &c->queue,    &c->mbs,      &c->mbcount,   &c->cells,
-                    &c->out,    &c->targets, &c->limits,    &c->found,    &c->next_lut, &c->chunks,    &c->tiles,
-                    &c->rerr,   &c->markers, &c->crc_table, &c->pieces,   &c->piece_crc, &c->mpiece,   &c->exp_crc,
-                    &c->exp_isize, &c->got_crc, &c->got_len, &c->mstatus, &c->comp, &c->bg_bcount, &c->bg_bbase,
-                    &c->bg_coff, &c->bg_csize, &c->bg_small, &c->sniff, &c->tile_chunk};
-#ifndef RRG_EMU
-    if (c->bg_exec) cudaGraphExecDestroy(c->bg_exec);
-#endif
-    for (DBuf* b : bufs)
-        if (b->p) cudaFree(b->p);
+    release_scratch(c);
     for (auto& p : c->h_stage)
         if (p) cudaFreeHost(p);
     if (c->h_bg) cudaFreeHost(c->h_bg);

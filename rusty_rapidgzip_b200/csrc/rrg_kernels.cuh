@@ -1747,6 +1747,9 @@ struct ScanArgs {
     uint64_t* cand;
     uint32_t* n_cand;
     uint32_t cap;
+    uint64_t* stored;       // stored-block starts (bit offsets), appended
+    uint32_t* n_stored;
+    uint32_t stored_cap;
 };
 
 // 32 bits of the staged tile starting at bit b (b + 32 <= 8 * tile bytes)
@@ -1784,6 +1787,28 @@ __global__ void __launch_bounds__(ST) k_scan_candidates(ScanArgs A) {
             }
         }
         __syncthreads();
+        // stored blocks (no reference counterpart: its finder looks for dynamic
+        // blocks only). A stored block that follows a stored block, or an empty
+        // sync-flush block, starts at a byte: header byte 0x00 or 0x01 (BFINAL,
+        // BTYPE=00, zero padding), then LEN and NLEN = ~LEN. This thread tests
+        // the header byte at each of its 16 bytes, so LEN..NLEN reach 4 bytes
+        // into the halo. A false start only costs the anchored chain a re-decode.
+        {
+            const uint32_t b0 = threadIdx.x * 16;
+#pragma unroll 4
+            for (uint32_t k = 0; k < 16; k++) {
+                const uint32_t j = b0 + k;
+                const uint64_t g = t0 + j;  // header byte, relative to `base`
+                if (tb[j] <= 1u && g >= lo && g + 5 <= hi) {
+                    const uint32_t len = tb[j + 1] | ((uint32_t)tb[j + 2] << 8);
+                    const uint32_t nlen = tb[j + 3] | ((uint32_t)tb[j + 4] << 8);
+                    if ((len ^ nlen) == 0xffffu) {
+                        const uint32_t slot = atomicAdd(A.n_stored, 1u);
+                        if (slot < A.stored_cap) A.stored[slot] = (g - lo) * 8;
+                    }
+                }
+            }
+        }
         // phase 1: prefilter every offset of this thread's 16 bytes (4 groups of 32)
         const uint64_t tile_bit0 = t0 * 8;
         const uint32_t w0 = threadIdx.x * 4;

@@ -239,3 +239,18 @@ def test_serving_alone_and_in_the_mix(emu_decoder_factory):
     st = d.serve_stats()
     assert st["completed"] == len(reqs) and st["batches"] >= 2
     assert d.pending() == 0
+
+
+def test_stored_block_chunks(emu_decoder_factory):
+    """Incompressible input (zlib's stored blocks) splits at stored-block starts
+    too, and mixed stored/dynamic content decodes exactly across the splits."""
+    rng = np.random.default_rng(13)
+    rnd = rng.integers(0, 256, 300_000, dtype=np.uint8).tobytes()
+    text = W.fastq_like(200_000, 13)
+    for raw, level in ((rnd, 1), (text[:100_000] + rnd[:150_000] + text[100_000:], 6)):
+        gz = W.gzip_member(raw, level)
+        d = emu_decoder_factory(gpu_chunk_bytes=16384)
+        out = []
+        st = d.decode_host(gz, out.append)
+        assert b"".join(out) == raw
+        assert st.gpu_chunks >= 3
