@@ -488,6 +488,7 @@ class Decoder:
             _raise(e)
         if r == 0:
             return None
+        self.last_poll_error = e.message.decode(errors="replace") if stv.value else ""
         data = None
         if out:
             data = C.string_at(out, n.value)

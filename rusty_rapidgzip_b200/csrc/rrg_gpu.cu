@@ -291,6 +291,7 @@ struct Server {
         int32_t status;
         double t_submit;
         double latency_ms;
+        rrg_error err;  // the failure's detail (code 0 when it succeeded)
     };
     std::vector<rrg_ctx*> engines;
     std::vector<std::thread> threads;
@@ -1647,7 +1648,8 @@ int batch_impl(rrg_ctx* c, const uint8_t* d_in, const uint64_t* in_off, const ui
     int rc = upload_tables(c, err);
     if (rc || !n) return rc;
     // ---- headers, BGZF sniff and the trailers' size hints, one thread per file
-    CK(dgrow(c->sniff, n * 40));
+    // 4 x 8-byte and 3 x 4-byte values per file
+    CK(dgrow(c->sniff, n * 44));
     uint8_t* sb = (uint8_t*)c->sniff.p;
     uint64_t* d_off = (uint64_t*)sb;
     uint64_t* d_len = d_off + n;
@@ -1963,7 +1965,11 @@ void engine_loop(Server* S, rrg_ctx* E) {
                 retry.push_back(std::move(r));
                 continue;
             }
-            Server::Done d{r.id, nullptr, 0, status[i], r.t_submit, 0.0};
+            Server::Done d{r.id, nullptr, 0, status[i], r.t_submit, 0.0, rrg_error{}};
+            if (status[i] != RRG_OK) {
+                if (rc && err.code) d.err = err;  // the whole batch failed: its error
+                else set_err(&d.err, status[i], "request failed with status %d", status[i]);
+            }
             if (status[i] == RRG_OK) {
                 d.out = (uint8_t*)std::malloc(std::max<uint64_t>(out_len[i], 1));
                 d.len = out_len[i];
@@ -1992,6 +1998,7 @@ void engine_loop(Server* S, rrg_ctx* E) {
                     d.out = nullptr;
                     d.len = 0;
                 }
+                if (d.status != RRG_OK && !d.err.code) set_err(&d.err, d.status, "result copy failed");
                 d.latency_ms = t_fin - d.t_submit;
                 S->done.push_back(d);
                 S->stats.completed++;
@@ -2472,6 +2479,7 @@ int rrg_gpu_poll(rrg_ctx* c, int64_t* request_id, uint8_t** out, size_t* out_len
     *out_len = d.len;
     *status = d.status;
     if (latency_ms) *latency_ms = d.latency_ms;
+    if (err) *err = d.err;
     return 1;
 }
 

@@ -172,5 +172,7 @@ def run_serving(d, reqs, seed: int, gap_s: float):
         while rid not in ids:
             time.sleep(0.001)
         got[ids[rid]] = (status, data)
+        if status:
+            print(f"request {ids[rid]}: status {status}: {d.last_poll_error}")
     th.join()
     return got
