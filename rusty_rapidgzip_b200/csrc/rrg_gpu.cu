@@ -315,7 +315,11 @@ cudaError_t dgrow(DBuf& b, size_t n) {
     if (b.p) cudaFree(b.p);
     b.p = nullptr;
     b.cap = 0;
+#ifdef RRG_STRICT_ALLOC
+    size_t c = n;  // exact sizes, so an address checker sees any overrun
+#else
     size_t c = n + n / 8 + 256;
+#endif
     cudaError_t e = cudaMalloc(&b.p, c);
     if (e == cudaSuccess) b.cap = c;
     return e;

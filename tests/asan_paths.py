@@ -1,0 +1,44 @@
+"""Runs the batch, BGZF, member and serving paths of the emulated build under
+AddressSanitizer with exact device-buffer sizes (RRG_STRICT_ALLOC), so that an
+index past the end of any device buffer fails here rather than on a GPU.
+Started by test_emu.py::test_address_sanitizer in its own process."""
+import sys
+
+import numpy as np
+
+sys.path.insert(0, sys.argv[2])
+from conftest import bgzf_cases, run_serving, serve_requests  # noqa: E402
+from rusty_rapidgzip_b200 import Config, Decoder  # noqa: E402
+from rusty_rapidgzip_b200 import workloads as W  # noqa: E402
+from test_emu import batch_items, haddr, run_batch  # noqa: E402
+
+lib = sys.argv[1]
+d = Decoder(Config(device=-1, gpu_chunk_bytes=8192), lib=lib)
+raw, gz = W.config1(40 << 10, seed=3)
+assert d.decompress(gz) == raw
+for case, data in bgzf_cases().items():
+    if case in ("chain", "truncated", "crc"):
+        try:
+            d.decompress(data)
+        except Exception:  # noqa: BLE001 - error cases are expected; only memory safety is checked here
+            pass
+keep = []
+
+
+def dev(data, out_n):
+    a = np.frombuffer(data, dtype=np.uint8).copy()
+    o = np.zeros(out_n, dtype=np.uint8)
+    keep.extend([a, o])
+    return haddr(a), haddr(o), lambda: o.tobytes()
+
+
+small = [(r, g, c) for r, g, c in batch_items() if len(g) < 100_000]
+for budget in (0, 1):
+    b = Decoder(Config(device=-1, hbm_budget_bytes=budget), lib=lib)
+    run_batch(b, small, dev)
+s = Decoder(Config(device=-1, hbm_budget_bytes=4 << 20), lib=lib)
+s.serve_start(engines=2, max_ready=2)
+got = run_serving(s, serve_requests(1, seed=5, hi=16 << 10), seed=3, gap_s=0.0)
+assert len(got) == 4
+s.close()
+print("asan paths ok")

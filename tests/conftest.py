@@ -137,7 +137,7 @@ def serve_requests(n: int, seed: int, hi: int):
     a two-member file and a request with a corrupt CRC."""
     from rusty_rapidgzip_b200 import workloads as W
     reqs = [gz for _, gz in W.config3_files(n_files=n, seed=seed, lo=4 << 10, hi=hi)]
-    reqs.append(W.bgzf(W.fastq_like(200_000, seed), 5, block=20_000))
+    reqs.append(W.bgzf(W.fastq_like(min(200_000, 2 * hi), seed), 5, block=20_000))
     reqs.append(gzip_cli(b"first member " * 500) + gzip_cli(b"second member " * 4000))
     bad = bytearray(gzip_cli(b"payload with a broken trailer " * 100))
     bad[-8] ^= 0x10

@@ -254,7 +254,11 @@ inline unsigned atomicCAS(unsigned* p, unsigned cmp, unsigned v) {
 
 // ---- runtime API (device memory is host memory)
 inline cudaError_t cudaMalloc(void** p, size_t n) {
+#ifdef RRG_STRICT_ALLOC
+    *p = std::malloc(n ? n : 1);  // exact size (16-byte aligned): an address checker sees overruns
+#else
     *p = std::aligned_alloc(256, (n + 255) & ~(size_t)255);
+#endif
     return *p ? cudaSuccess : cudaErrorMemoryAllocation;
 }
 inline cudaError_t cudaFree(void* p) {

@@ -137,7 +137,7 @@ def batch_items():
     """Files for one batch: a multi-chunk member, small single-chunk members,
     concatenated members, a BGZF file, a file with a bad CRC and a file whose
     output range is too small (capacity status)."""
-    big_raw, big = W.config0(600_000, seed=5)
+    big_raw, big = W.config0(300_000, seed=5)
     small_raw = b"small file " * 300
     cat_raw = b"alpha" * 100 + b"beta" * 2000
     bg_raw = W.fastq_like(40_000, 6)
@@ -224,7 +224,7 @@ def test_serving_alone_and_in_the_mix(emu_decoder_factory):
     in the serving loop's mix, with two engines and a budget small enough that
     requests queue for admission."""
     from conftest import run_serving, serve_requests
-    reqs = serve_requests(6, seed=11, hi=96 << 10)
+    reqs = serve_requests(3, seed=11, hi=32 << 10)
     alone = emu_decoder_factory()
     want = {}
     for i, gz in enumerate(reqs):
@@ -245,12 +245,32 @@ def test_stored_block_chunks(emu_decoder_factory):
     """Incompressible input (zlib's stored blocks) splits at stored-block starts
     too, and mixed stored/dynamic content decodes exactly across the splits."""
     rng = np.random.default_rng(13)
-    rnd = rng.integers(0, 256, 300_000, dtype=np.uint8).tobytes()
-    text = W.fastq_like(200_000, 13)
-    for raw, level in ((rnd, 1), (text[:100_000] + rnd[:150_000] + text[100_000:], 6)):
+    rnd = rng.integers(0, 256, 120_000, dtype=np.uint8).tobytes()
+    text = W.fastq_like(80_000, 13)
+    for raw, level in ((rnd, 1), (text[:40_000] + rnd[:60_000] + text[40_000:], 6)):
         gz = W.gzip_member(raw, level)
         d = emu_decoder_factory(gpu_chunk_bytes=16384)
         out = []
         st = d.decode_host(gz, out.append)
         assert b"".join(out) == raw
         assert st.gpu_chunks >= 3
+
+
+def test_address_sanitizer(tmp_path):
+    """Batch, BGZF, member and serving paths of the emulated build with exact
+    device-buffer sizes under AddressSanitizer: any index past the end of a
+    device buffer fails here instead of on a GPU."""
+    import subprocess
+    import sys
+    from conftest import EMU_DIR, ROOT
+    lib = str(tmp_path / "librrg_gpu_emu_asan.so")
+    subprocess.check_call([
+        "g++", "-std=c++20", "-O1", "-g", "-fsanitize=address", "-fno-omit-frame-pointer", "-x", "c++", "-DRRG_EMU",
+        "-DRRG_STRICT_ALLOC", "-include", os.path.join(EMU_DIR, "cuda_emu.h"), "-I", os.path.join(ROOT, "include"),
+        "-I", os.path.join(ROOT, "rusty_rapidgzip_b200", "csrc"), "-fPIC", "-shared", "-pthread", "-o", lib,
+        os.path.join(ROOT, "rusty_rapidgzip_b200", "csrc", "rrg_gpu.cu")])
+    asan = subprocess.run(["gcc", "-print-file-name=libasan.so"], stdout=subprocess.PIPE, text=True).stdout.strip()
+    env = dict(os.environ, LD_PRELOAD=asan, ASAN_OPTIONS="detect_leaks=0:abort_on_error=1")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "tests", "asan_paths.py"), lib, os.path.join(ROOT, "tests")],
+                       env=env, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True, timeout=1200)
+    assert r.returncode == 0 and "asan paths ok" in r.stdout, r.stdout[-4000:]
