@@ -613,7 +613,10 @@ int run_resolve(rrg_ctx* c, const std::vector<ResolveChunk>& rchunks, const std:
     CK(dgrow(c->tiles, (nc + 1) * 8));
     CK(dgrow(c->rerr, 16));
     CK(dgrow(c->markers, 8));
-    CK(dgrow(c->win, (size_t)nc * WINDOW * 4));
+    CK(dgrow(c->win, (size_t)nc * WINDOW * 5 + (size_t)nc * 4));  // u32 windows, byte windows, flags
+    uint8_t* winb = (uint8_t*)c->win.p + (size_t)nc * WINDOW * 4;
+    uint32_t* win_bad = (uint32_t*)(winb + (size_t)nc * WINDOW);
+    CK(cudaMemsetAsync(win_bad, 0, (size_t)nc * 4, c->stream));
     CK(cudaMemcpyAsync(c->chunks.p, rchunks.data(), nc * sizeof(ResolveChunk), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->tiles.p, tile_start.data(), (nc + 1) * 8, cudaMemcpyHostToDevice, c->stream));
     const uint64_t n_tiles = tile_start.back();
@@ -627,7 +630,7 @@ int run_resolve(rrg_ctx* c, const std::vector<ResolveChunk>& rchunks, const std:
     ResolveArgs R{(const uint16_t*)c->cells.p, (const ResolveChunk*)c->chunks.p, (const uint64_t*)c->tiles.p,
                   (const uint32_t*)c->tile_chunk.p, nc,
                   tile_start.back(), d_dst, (uint32_t*)c->win.p, (uint32_t*)c->rerr.p,
-                  (unsigned long long*)c->markers.p};
+                  (unsigned long long*)c->markers.p, winb, win_bad};
     const uint64_t wcells = (uint64_t)nc * WINDOW;
     const uint32_t wgrid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((wcells + 255) / 256, (uint64_t)c->n_sm * 32));
     uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(tile_start.back(), (uint64_t)c->n_sm * 16));
@@ -908,12 +911,16 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
     };
     // ---- a stream of one chunk with a fixed destination decodes straight to
     // its bytes: it cannot hold markers, so there is nothing to resolve
+    // (only when no stream is split: otherwise they join the one speculative
+    // launch, so that a single persistent wave covers every stream)
     std::vector<char> direct(nj, 0);
     std::vector<std::vector<MemberRec>> direct_recs(nj);
+    bool any_split = false;
+    for (size_t i = 0; i < nj; i++) any_split |= starts[i].size() > 1;
     {
         std::vector<ChunkItem> ditems;
         std::vector<size_t> djob;
-        for (size_t i = 0; i < nj && !tgt.grow; i++) {
+        for (size_t i = 0; i < nj && !tgt.grow && !any_split; i++) {
             if (starts[i].size() != 1) continue;
             const MemberJob& j = jobs[i];
             direct[i] = 1;

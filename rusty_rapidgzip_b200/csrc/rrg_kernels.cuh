@@ -2038,6 +2038,8 @@ struct ResolveArgs {
     uint32_t* win;           // n_chunks * WINDOW entries
     uint32_t* err;           // [0] flag, [1] chunk, [2] cell lo, [3] cell hi
     unsigned long long* markers;  // count of marker cells resolved
+    uint8_t* winb;           // n_chunks * WINDOW: the resolved windows as bytes
+    uint32_t* win_bad;       // n_chunks: 1 if the chunk's window holds an INVALID entry
 };
 
 __global__ void __launch_bounds__(256) k_win_init(ResolveArgs A) {
@@ -2073,20 +2075,24 @@ __global__ void __launch_bounds__(256) k_win_chase(ResolveArgs A) {
     for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < total;
          c += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t w = win[c];
-        if (w & WIN_BYTE) continue;
-        uint32_t t = w;
-        uint64_t prev_win = c / WINDOW;
-        for (;;) {  // every hop must reach a strictly earlier window: at most n_chunks steps
-            if ((uint64_t)(t / WINDOW) >= prev_win) {
-                w = WIN_INVALID;
-                break;
+        if (!(w & WIN_BYTE)) {
+            uint32_t t = w;
+            uint64_t prev_win = c / WINDOW;
+            for (;;) {  // every hop must reach a strictly earlier window: at most n_chunks steps
+                if ((uint64_t)(t / WINDOW) >= prev_win) {
+                    w = WIN_INVALID;
+                    break;
+                }
+                prev_win = t / WINDOW;
+                w = win[t];
+                if (w & WIN_BYTE) break;
+                t = w;
             }
-            prev_win = t / WINDOW;
-            w = win[t];
-            if (w & WIN_BYTE) break;
-            t = w;
+            win[c] = w;
         }
-        win[c] = w;
+        // the byte copy k_resolve gathers from (a quarter of the u32 window's bytes)
+        A.winb[c] = (uint8_t)w;
+        if (w == WIN_INVALID) A.win_bad[c / WINDOW] = 1u;
     }
 }
 
@@ -2105,6 +2111,8 @@ __global__ void __launch_bounds__(RES_THREADS) k_resolve(ResolveArgs A) {
         const uint32_t k = s_chunk;
         const ResolveChunk ck = A.chunks[k];
         const uint32_t* win = A.win + (uint64_t)k * WINDOW;
+        const uint8_t* winb = A.winb + (uint64_t)k * WINDOW;
+        const bool win_clean = A.win_bad[k] == 0u;  // uniform over the tile
         const uint64_t c0 = (t - A.tile_start[k]) * (uint64_t)RES_TILE;
         const uint64_t cn = ck.n_cells - c0 < (uint64_t)RES_TILE ? ck.n_cells - c0 : (uint64_t)RES_TILE;
         // warp w owns cells [512w, 512w + 512) of the tile, lane ln the cells
@@ -2121,9 +2129,15 @@ __global__ void __launch_bounds__(RES_THREADS) k_resolve(ResolveArgs A) {
             for (int i = 0; i < RES_PER_THREAD; i++) cell[i] = (ln + 32u * i < lim) ? p[32 * i] : 0u;
             // independent gathers: all issued before any is consumed
             uint32_t got[RES_PER_THREAD];
+            if (win_clean) {
 #pragma unroll
-            for (int i = 0; i < RES_PER_THREAD; i++)
-                got[i] = (cell[i] & MARKER16) ? win[WINDOW - 1 - (cell[i] & 0x7fffu)] : (WIN_BYTE | cell[i]);
+                for (int i = 0; i < RES_PER_THREAD; i++)
+                    got[i] = WIN_BYTE | ((cell[i] & MARKER16) ? (uint32_t)winb[WINDOW - 1 - (cell[i] & 0x7fffu)] : cell[i]);
+            } else {
+#pragma unroll
+                for (int i = 0; i < RES_PER_THREAD; i++)
+                    got[i] = (cell[i] & MARKER16) ? win[WINDOW - 1 - (cell[i] & 0x7fffu)] : (WIN_BYTE | cell[i]);
+            }
 #pragma unroll
             for (int i = 0; i < RES_PER_THREAD; i++) {
                 if (ln + 32u * i < lim) {
