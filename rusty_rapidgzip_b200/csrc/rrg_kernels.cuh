@@ -1789,20 +1789,30 @@ __global__ void __launch_bounds__(ST) k_scan_candidates(ScanArgs A) {
         __syncthreads();
         // stored blocks (no reference counterpart: its finder looks for dynamic
         // blocks only). A stored block that follows a stored block, or an empty
-        // sync-flush block, starts at a byte: header byte 0x00 or 0x01 (BFINAL,
-        // BTYPE=00, zero padding), then LEN and NLEN = ~LEN. This thread tests
-        // the header byte at each of its 16 bytes, so LEN..NLEN reach 4 bytes
-        // into the halo. A false start only costs the anchored chain a re-decode.
+        // sync-flush block, starts at a byte: header byte 0x00 (BFINAL=0,
+        // BTYPE=00, zero padding), then LEN and NLEN = ~LEN. To keep chance
+        // matches inside compressed data (about one per 8 MB) from becoming
+        // chunk starts, a non-empty block counts only if another stored block
+        // header follows its data. This thread tests the header byte at each of
+        // its 16 bytes, so LEN..NLEN reach 4 bytes into the halo. A false start
+        // would only cost the anchored chain a re-decode.
         {
             const uint32_t b0 = threadIdx.x * 16;
 #pragma unroll 4
             for (uint32_t k = 0; k < 16; k++) {
                 const uint32_t j = b0 + k;
                 const uint64_t g = t0 + j;  // header byte, relative to `base`
-                if (tb[j] <= 1u && g >= lo && g + 5 <= hi) {
+                if (tb[j] == 0u && g >= lo && g + 5 <= hi) {
                     const uint32_t len = tb[j + 1] | ((uint32_t)tb[j + 2] << 8);
                     const uint32_t nlen = tb[j + 3] | ((uint32_t)tb[j + 4] << 8);
-                    if ((len ^ nlen) == 0xffffu) {
+                    bool ok = (len ^ nlen) == 0xffffu;
+                    if (ok && len) {
+                        const uint64_t q = g + 5 + len;  // the next block's header byte
+                        ok = q + 5 <= hi && __ldg(base + q) <= 1u &&
+                             ((__ldg(base + q + 1) | ((uint32_t)__ldg(base + q + 2) << 8)) ^
+                              (__ldg(base + q + 3) | ((uint32_t)__ldg(base + q + 4) << 8))) == 0xffffu;
+                    }
+                    if (ok) {
                         const uint32_t slot = atomicAdd(A.n_stored, 1u);
                         if (slot < A.stored_cap) A.stored[slot] = (g - lo) * 8;
                     }

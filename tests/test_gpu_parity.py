@@ -306,6 +306,8 @@ def test_large_stream_properties(gpu_decoder_factory):
     h = hashlib.sha256(dout[:n].cpu().numpy().tobytes()).hexdigest()
     assert h == sha256(raw)
     assert st.members == 1 and st.gpu_chunks > 100
+    # every sub-chunk start is a real block start: no speculative decode is redone
+    assert st.speculation_failures == 0
 
 
 @pytest.mark.gpu
