@@ -110,7 +110,7 @@ class Config:
     """Mirrors Config (lib.rs:50-100) plus device tunables (0 = autotuned)."""
     num_threads: int = 0
     chunk_size_bytes: int = 4 << 20
-    verbose: bool = False
+    verbose: int = 0  # 0 off, 1 per-call summary, 2 also every re-decoded sub-chunk
     device: int = -1
     gpu_chunk_bytes: int = 0
     finder_tile_bits: int = 0
@@ -122,7 +122,7 @@ class Config:
         c = _Config()
         c.num_threads = self.num_threads
         c.chunk_size_bytes = self.chunk_size_bytes
-        c.verbose = 1 if self.verbose else 0
+        c.verbose = int(self.verbose)
         c.device = self.device
         c.gpu_chunk_bytes = self.gpu_chunk_bytes
         c.finder_tile_bits = self.finder_tile_bits

@@ -55,6 +55,8 @@ struct ChunkItem {
 enum : uint32_t {
     ITEM_MARKERS = 1u,      // the first member may reference bytes before the chunk (u16 markers)
     ITEM_ONE_MEMBER = 2u,   // input is exactly one gzip member with its header (batch mode)
+    ITEM_STORED_START = 4u, // host only: the start is a stored-block header byte of zeros
+    ITEM_EMPTY_STORED = 8u, // host only: ... of an empty stored block (LEN = 0)
 };
 
 struct ChunkResult {

@@ -660,8 +660,10 @@ int run_resolve(rrg_ctx* c, const std::vector<ResolveChunk>& rchunks, const std:
 // ------------------------------------------------------------ boundary scan
 // Every bit offset of the body tested on the device; returns the sorted
 // offsets that pass the block finder's full strict verification.
-int scan_boundaries(rrg_ctx* c, const uint8_t* body, uint64_t blen, std::vector<uint64_t>& verified, rrg_error* err) {
+int scan_boundaries(rrg_ctx* c, const uint8_t* body, uint64_t blen, std::vector<uint64_t>& verified,
+                    std::vector<uint64_t>* stored_out, rrg_error* err) {
     verified.clear();
+    if (stored_out) stored_out->clear();
     if (blen < 4) return 0;
     KTimer kt(c->stream);
     // candidates (prefilter + precode), then light-verify survivors, then the
@@ -703,7 +705,11 @@ int scan_boundaries(rrg_ctx* c, const uint8_t* body, uint64_t blen, std::vector<
         std::vector<uint64_t> st(ns);
         CK(cudaMemcpyAsync(st.data(), stored, (size_t)ns * 8, cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
-        verified.insert(verified.end(), st.begin(), st.end());
+        for (uint64_t v : st) verified.push_back(v & ~1ull);  // bit 0: empty block
+        if (stored_out) {
+            *stored_out = st;
+            std::sort(stored_out->begin(), stored_out->end());
+        }
     }
     if (cnt[0] > cap || cnt[1] > cap2) {
         set_err(err, RRG_ERR_OUT_OF_MEMORY, "boundary scan: %u candidates exceed the list", cnt[0]);
@@ -805,6 +811,7 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
     const uint64_t G = fixed_g ? std::max<uint64_t>(c->gpu_chunk, 4096)
                                : std::max<uint64_t>(g_min, (total_c + slots - 1) / slots);
     std::vector<std::vector<uint64_t>> starts(nj, std::vector<uint64_t>{0});
+    std::vector<std::vector<uint64_t>> stored_starts(nj);  // sorted, relative to each body
     auto fail = [&](MemberJob& j, int st, int msg, uint64_t where) { j.rc = status_err(&j.err, st, msg, where); };
     // ---- sub-chunk boundaries
     if (c->scan_bounds) {
@@ -821,14 +828,16 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
                 hi = std::max(hi, jobs[big[b]].file_off + jobs[big[b]].len);
                 b++;
             }
-            std::vector<uint64_t> verified;
-            int rc0 = scan_boundaries(c, d_base + lo, hi - lo, verified, err);
+            std::vector<uint64_t> verified, stored;
+            int rc0 = scan_boundaries(c, d_base + lo, hi - lo, verified, &stored, err);
             if (rc0) return rc0;
             // verified offsets are sorted bit offsets from `lo`
             for (size_t q = a; q < b; q++) {
                 MemberJob& j = jobs[big[q]];
                 const uint64_t b0 = (j.file_off + j.body_off - lo) * 8, b1 = (j.file_off + j.len - lo) * 8;
                 auto& st = starts[big[q]];
+                for (auto it = std::lower_bound(stored.begin(), stored.end(), b0); it != stored.end() && *it < b1; ++it)
+                    stored_starts[big[q]].push_back(*it - b0);  // keeps the empty-block bit
                 auto lo_it = std::lower_bound(verified.begin(), verified.end(), b0);
                 auto hi_it = std::lower_bound(lo_it, verified.end(), b1);
                 if (fixed_g) {
@@ -986,6 +995,12 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
             // the first chunk too, as in the reference: a reference before the
             // stream's start becomes a marker that fails to resolve
             it.flags = ITEM_MARKERS;
+            if (k) {
+                if (std::binary_search(stored_starts[i].begin(), stored_starts[i].end(), st[k]))
+                    it.flags |= ITEM_STORED_START;
+                else if (std::binary_search(stored_starts[i].begin(), stored_starts[i].end(), st[k] | 1))
+                    it.flags |= ITEM_STORED_START | ITEM_EMPTY_STORED;
+            }
             it.id = next_id++;
             arena += it.out_cap;
             items.push_back(it);
@@ -1021,11 +1036,25 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
                 }
                 ChunkItem it = items[s.first + s.k];
                 const ChunkResult r = res[s.first + s.k];
-                if (it.start_bit == s.expected && (r.status == DS_OK || r.status == DS_OVERFLOW)) {
+                // A start on a zero header byte of a stored block decodes exactly as
+                // the true start does when that lies in the same byte's first 6 bits
+                // (BFINAL=0 and BTYPE=00 are read from zeros, and the padding ends at
+                // the same byte boundary), or, for an empty block, when the true start
+                // is right after it (the block adds nothing to the output).
+                const uint64_t d = s.expected - it.start_bit;
+                const bool same_start =
+                    it.start_bit == s.expected ||
+                    ((it.flags & ITEM_STORED_START) && s.expected > it.start_bit &&
+                     (d <= 5 || ((it.flags & ITEM_EMPTY_STORED) && d == 40)));
+                if (same_start && (r.status == DS_OK || r.status == DS_OVERFLOW)) {
                     s.acc.push_back(Acc{it, r, take_recs(it.id)});
                 } else {
                     // false boundary or failed speculative decode: re-decode from the anchor
                     c->st.speculation_failures++;
+                    if (c->cfg.verbose >= 2)
+                        std::fprintf(stderr, "[rrg-gpu] re-decode: chunk at bit %llu (flags %u) status %d, anchor %llu\n",
+                                     (unsigned long long)it.start_bit, it.flags, r.status,
+                                     (unsigned long long)s.expected);
                     if (it.end_hint != ~0ull && s.expected >= it.end_hint) {  // empty chunk
                         s.k++;
                         continue;

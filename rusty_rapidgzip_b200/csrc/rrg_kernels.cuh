@@ -1812,9 +1812,9 @@ __global__ void __launch_bounds__(ST) k_scan_candidates(ScanArgs A) {
                              ((__ldg(base + q + 1) | ((uint32_t)__ldg(base + q + 2) << 8)) ^
                               (__ldg(base + q + 3) | ((uint32_t)__ldg(base + q + 4) << 8))) == 0xffffu;
                     }
-                    if (ok) {
+                    if (ok) {  // bit 0 of the (byte-aligned) offset marks an empty block
                         const uint32_t slot = atomicAdd(A.n_stored, 1u);
-                        if (slot < A.stored_cap) A.stored[slot] = (g - lo) * 8;
+                        if (slot < A.stored_cap) A.stored[slot] = (g - lo) * 8 + (len ? 0u : 1u);
                     }
                 }
             }

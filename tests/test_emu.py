@@ -274,3 +274,16 @@ def test_address_sanitizer(tmp_path):
     r = subprocess.run([sys.executable, os.path.join(ROOT, "tests", "asan_paths.py"), lib, os.path.join(ROOT, "tests")],
                        env=env, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True, timeout=1200)
     assert r.returncode == 0 and "asan paths ok" in r.stdout, r.stdout[-4000:]
+
+
+def test_sync_flush_starts_are_not_redone(emu_decoder_factory):
+    """A member made of sync-flushed pieces (empty stored blocks whose header
+    shares a byte with the previous block's last bits): sub-chunks that start
+    on those stored headers decode as from the true start, so nothing is redone."""
+    raw = W.zipf_text(300_000, 21)
+    gz = W.gzip_member(raw, 9, parallel_threshold=0, piece=12_000)
+    d = emu_decoder_factory(gpu_chunk_bytes=8192)
+    out = []
+    st = d.decode_host(gz, out.append)
+    assert b"".join(out) == raw
+    assert st.gpu_chunks >= 4 and st.speculation_failures == 0
