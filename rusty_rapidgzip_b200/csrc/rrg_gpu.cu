@@ -806,7 +806,7 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
     uint64_t total_c = 0;
     for (const MemberJob& j : jobs) total_c += j.len - j.body_off;
     const bool fixed_g = c->gpu_chunk != 0;
-    const uint64_t g_min = c->lanes ? (8ull << 10) : (32ull << 10);
+    const uint64_t g_min = c->lanes ? (8ull << 10) : (16ull << 10);
     const uint64_t slots = inflate_slots(c);
     const uint64_t G = fixed_g ? std::max<uint64_t>(c->gpu_chunk, 4096)
                                : std::max<uint64_t>(g_min, (total_c + slots - 1) / slots);

@@ -142,14 +142,21 @@ __device__ __forceinline__ bool br_past_end(const BR& b) { return br_tell_abs(b)
 // ------------------------------------------------------- Huffman tables
 // LUT entry (u32): bits 0-3 code length (0 = not in the LUT), bits 4-5 kind,
 // bits 8-11 extra-bit count, bits 16-31 value.
-//   litlen kind: 0 literal (value = byte), 1 length (value = base), 2 end of block, 3 invalid (286/287)
+//   litlen kind: 1 length (value = base), 2 end of block, 3 invalid (286/287)
 //   dist kind:   0 distance (value = base), 3 invalid (30/31)
 //   precode:     value = symbol
+// A litlen literal is 0x80000000 | code length << 8 | byte: the sign bit tells
+// it apart in one test, and masked with 0x800000ff it is the batch entry itself.
 enum { TK_LITLEN = 0, TK_DIST = 1, TK_PRE = 2 };
+constexpr uint32_t LIT_FLAG = 0x80000000u;
+
+__device__ __forceinline__ uint32_t entry_len(uint32_t e) {  // code length of any entry
+    return (int32_t)e < 0 ? (e >> 8) & 15u : e & 15u;
+}
 
 __device__ __forceinline__ uint32_t make_entry(int kind, uint32_t sym, uint32_t len) {
     if (kind == TK_LITLEN) {
-        if (sym < 256) return (sym << 16) | len;
+        if (sym < 256) return LIT_FLAG | (len << 8) | sym;
         if (sym == 256) return (2u << 4) | len;
         if (sym <= 285)
             return ((uint32_t)c_len_base[sym - 257] << 16) | ((uint32_t)c_len_extra[sym - 257] << 8) | (1u << 4) | len;
@@ -481,7 +488,7 @@ template <typename CellT>
 __device__ void decode_codes(WarpSmem& S, ItemState& st, CellT* out, int lane) {
     const Table LT = lit_table(S), DT = dist_table(S);
     for (;;) {
-        int n = 0, stop = 0, status = 0, msg = 0;
+        int n = 0, stop = 0, status = 0, msg = 0, fast_flag = 0;
         uint32_t pos = 0;
         if (lane == 0) {
             uint64_t room = st.counting ? ~0ull : (st.cap > st.cur ? st.cap - st.cur : 0);
@@ -489,6 +496,8 @@ __device__ void decode_codes(WarpSmem& S, ItemState& st, CellT* out, int lane) {
             // Fast path: the batch surely fits the slot (<= NB * 258 cells) and every
             // word it can load (a batch consumes <= NB * 48 bits) lies inside the input.
             const bool fast = room >= (uint64_t)NB * 258 && (b.nw + 56) * 4 <= b.s.hi && b.nw * 4 >= b.s.lo;
+            fast_flag = fast ? 1 : 0;
+            bool handoff = false;
             if (fast) {
                 const uint32_t* base_w = reinterpret_cast<const uint32_t*>(b.s.base);
                 const uint32_t* wp = base_w + b.nw;
@@ -500,25 +509,22 @@ __device__ void decode_codes(WarpSmem& S, ItemState& st, CellT* out, int lane) {
                         wp++;
                         bits += 32;
                     }
-                    uint32_t e = S.lit_lut[buf & (LUT_SIZE - 1)];
-                    uint32_t cl = e & 15;
-                    if (!cl) {
-                        e = long_decode(buf, LT, LUT_BITS, TK_LITLEN);
-                        cl = e & 15;
-                        if (!cl) {
-                            status = DS_INVALID;
-                            msg = MSG_NO_CODE;
-                            break;
-                        }
-                    }
-                    const uint32_t kind = (e >> 4) & 3;
-                    if (kind == 0) {
+                    uint32_t e = S.lit_lut[(uint32_t)buf & (LUT_SIZE - 1)];
+                    if ((int32_t)e < 0) {  // literal: the entry is the batch entry
+                        const uint32_t cl = (e >> 8) & 15u;
                         buf >>= cl;
                         bits -= cl;
-                        S.ep[n] = make_uint2(0x80000000u | (e >> 16), pos);
-                        pos += 1;
+                        S.ep[n].x = e & 0x800000ffu;
                         n++;
-                    } else if (kind == 1) {
+                        continue;
+                    }
+                    if (!e) {  // a code longer than the LUT: the checked path takes this symbol
+                        handoff = true;
+                        break;
+                    }
+                    const uint32_t cl = e & 15u;
+                    const uint32_t kind = (e >> 4) & 3;
+                    if (kind == 1) {
                         const uint32_t ex = (e >> 8) & 15;
                         const uint32_t length = (e >> 16) + ((uint32_t)(buf >> cl) & ((1u << ex) - 1u));
                         buf >>= cl + ex;
@@ -528,7 +534,7 @@ __device__ void decode_codes(WarpSmem& S, ItemState& st, CellT* out, int lane) {
                             wp++;
                             bits += 32;
                         }
-                        uint32_t de = S.dist_lut[buf & (DIST_SIZE - 1)];
+                        uint32_t de = S.dist_lut[(uint32_t)buf & (DIST_SIZE - 1)];
                         uint32_t dl = de & 15;
                         if (!dl) {
                             de = long_decode(buf, DT, DIST_BITS, TK_DIST);
@@ -548,8 +554,7 @@ __device__ void decode_codes(WarpSmem& S, ItemState& st, CellT* out, int lane) {
                         const uint32_t dist = (de >> 16) + ((uint32_t)(buf >> dl) & ((1u << dx) - 1u));
                         buf >>= dl + dx;
                         bits -= dl + dx;
-                        S.ep[n] = make_uint2((dist << 9) | length, pos);
-                        pos += length;
+                        S.ep[n].x = (dist << 9) | length;
                         n++;
                     } else if (kind == 2) {
                         buf >>= cl;
@@ -566,22 +571,31 @@ __device__ void decode_codes(WarpSmem& S, ItemState& st, CellT* out, int lane) {
                 b.buf = buf;
                 b.bits = bits;
                 if (!status && br_past_end(b)) status = DS_EOF;
+                if (handoff && !status) {
+                    // the checked path finishes the batch: it needs the entries'
+                    // offsets, which the fast path leaves to the warp
+                    fast_flag = 0;
+                    for (int k = 0; k < n; k++) {
+                        const uint32_t x = S.ep[k].x;
+                        S.ep[k].y = pos;
+                        pos += (x & LIT_FLAG) ? 1u : (x & 511u);
+                    }
+                }
             }
-            while (!fast && n < NB) {
+            while ((!fast || (handoff && !status)) && n < NB) {
                 const BR save = b;
                 br_refill(b);
                 uint32_t e = S.lit_lut[b.buf & (LUT_SIZE - 1)];
-                uint32_t cl = e & 15;
-                if (!cl) {
+                if (!e) {
                     e = long_decode(b.buf, LT, LUT_BITS, TK_LITLEN);
-                    cl = e & 15;
-                    if (!cl) {
+                    if (!e) {
                         status = br_past_end(b) ? DS_EOF : DS_INVALID;
                         msg = MSG_NO_CODE;
                         break;
                     }
                 }
-                uint32_t kind = (e >> 4) & 3;
+                const uint32_t cl = entry_len(e);
+                const uint32_t kind = (int32_t)e < 0 ? 0u : (e >> 4) & 3;
                 if (kind == 0) {
                     if (pos + 1 > room) {  // output full: this symbol is re-read in counting mode
                         b = save;
@@ -589,7 +603,7 @@ __device__ void decode_codes(WarpSmem& S, ItemState& st, CellT* out, int lane) {
                         break;
                     }
                     br_consume(b, cl);
-                    S.ep[n] = make_uint2(0x80000000u | (e >> 16), pos);
+                    S.ep[n] = make_uint2(e & 0x800000ffu, pos);
                     pos += 1;
                     n++;
                 } else if (kind == 1) {
@@ -645,7 +659,22 @@ __device__ void decode_codes(WarpSmem& S, ItemState& st, CellT* out, int lane) {
         stop = bcast32(stop);
         status = bcast32(status);
         msg = bcast32(msg);
+        const int fast_batch = bcast32(fast_flag);
         __syncwarp();
+        if (fast_batch) {
+            // the fast path stores entries only: their output offsets are a warp prefix sum
+            const uint32_t x = lane < n ? S.ep[lane].x : 0u;
+            const uint32_t len = lane < n ? ((x & LIT_FLAG) ? 1u : (x & 511u)) : 0u;
+            uint32_t incl = len;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(FULLMASK, incl, o);
+                if (lane >= o) incl += y;
+            }
+            if (lane < n) S.ep[lane].y = incl - len;
+            pos = __shfl_sync(FULLMASK, incl, 31);
+            __syncwarp();
+        }
         if (!st.counting && n) {
             uint32_t bad = 0, mk = 0;
             const uint64_t cur = st.cur;
@@ -909,7 +938,7 @@ __device__ void inflate_item(WarpSmem& S, const InflateArgs& A, uint32_t item_id
 }
 
 #ifndef RRG_INFLATE_MIN_BLOCKS
-#define RRG_INFLATE_MIN_BLOCKS 5
+#define RRG_INFLATE_MIN_BLOCKS 6
 #endif
 // 128 threads (4 warps) per block, >= RRG_INFLATE_MIN_BLOCKS blocks per SM
 template <typename CellT>
