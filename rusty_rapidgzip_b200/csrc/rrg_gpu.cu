@@ -250,6 +250,12 @@ struct rrg_ctx {
     uint32_t warps_per_member = 1; // BGZF: 1 = a member per warp; 2-4 = sub-chunks per member
     double expand = 6.0;
     uint64_t slots = 0;        // resident decoders of one inflate wave (lazy)
+    // host path: the input's H2D copy in pieces (end byte, event), so the
+    // boundary scan can start on the pieces that have arrived
+    const uint8_t* arr_base = nullptr;
+    std::vector<std::pair<uint64_t, cudaEvent_t>> arr_pieces;
+    cudaEvent_t arr_events[8] = {};
+    cudaStream_t copy_stream = nullptr;
     DBuf sniff;                // per-file header results of a batch
     DBuf tile_chunk;           // resolve: chunk of every tile
     // BGZF route: device member table and the captured decode graph
@@ -386,10 +392,20 @@ uint32_t persistent_blocks(rrg_ctx* c, uint32_t per_sm, uint64_t work_units, uin
     return (uint32_t)std::max<uint64_t>(1, std::min(need, cap));
 }
 
+// The host path's input pieces: make the decode stream wait for all of them.
+int wait_arrival(rrg_ctx* c, rrg_error* err) {
+    if (!c->arr_base) return 0;
+    if (!c->arr_pieces.empty()) CK(cudaStreamWaitEvent(c->stream, c->arr_pieces.back().second, 0));
+    c->arr_base = nullptr;
+    c->arr_pieces.clear();
+    return 0;
+}
+
 // ------------------------------------------------------------ inflate launch
 int launch_inflate(rrg_ctx* c, const uint8_t* d_in, const std::vector<ChunkItem>& items, bool bytes_out,
                    void* d_out_cells, std::vector<ChunkResult>& res, std::vector<MemberRec>* mrecs,
                    rrg_error* err) {
+    if (int rw = wait_arrival(c, err)) return rw;
     const uint32_t n = (uint32_t)items.size();
     res.assign(n, ChunkResult{});
     if (!n) return 0;
@@ -679,16 +695,42 @@ int scan_boundaries(rrg_ctx* c, const uint8_t* body, uint64_t blen, std::vector<
     uint64_t* surv = cand + cap;
     uint64_t* stored = surv + cap2;
     uint32_t* counts = (uint32_t*)c->ncand.p;  // [0] candidates, [1] survivors, [2] heavy queue, [3] stored
-    ScanArgs S{body, blen, cand, counts, cap, stored, counts + 3, cap3};
+    ScanArgs S{body, blen, cand, counts, cap, stored, counts + 3, cap3, 0, ~0ull};
     // tile width: scan_threads x 16 bytes per block step (64, 128 or 256 threads)
     const uint32_t st = c->scan_threads;
     const uint64_t tb = (uint64_t)st * 16;
-    const uint32_t sgrid = (uint32_t)std::max<uint64_t>(
-        1, std::min<uint64_t>((blen + 16 + tb - 1) / tb, (uint64_t)c->n_sm * (2048 / st)));
-    if (st == 64) RRG_LAUNCH(k_scan_candidates<64>, sgrid, 64, 0, c->stream, S);
-    else if (st == 128) RRG_LAUNCH(k_scan_candidates<128>, sgrid, 128, 0, c->stream, S);
-    else RRG_LAUNCH(k_scan_candidates<256>, sgrid, 256, 0, c->stream, S);
-    LAUNCHED(c);
+    const uint64_t n_tiles = ((uint64_t)((uintptr_t)body & 15) + blen + tb - 1) / tb;
+    auto scan = [&](uint64_t t_lo, uint64_t t_hi) -> int {
+        if (t_hi <= t_lo) return 0;
+        S.tile_lo = t_lo;
+        S.tile_hi = t_hi;
+        const uint32_t sgrid =
+            (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(t_hi - t_lo, (uint64_t)c->n_sm * (2048 / st)));
+        if (st == 64) RRG_LAUNCH(k_scan_candidates<64>, sgrid, 64, 0, c->stream, S);
+        else if (st == 128) RRG_LAUNCH(k_scan_candidates<128>, sgrid, 128, 0, c->stream, S);
+        else RRG_LAUNCH(k_scan_candidates<256>, sgrid, 256, 0, c->stream, S);
+        LAUNCHED(c);
+        return 0;
+    };
+    // Input still arriving (host path): scan each tile as soon as its bytes,
+    // and the 64 KiB past them that the stored-block check may read, are here.
+    uint64_t t_done = 0;
+    if (c->arr_base && !c->arr_pieces.empty()) {
+        const uint8_t* tile0 = (const uint8_t*)((uintptr_t)body & ~(uintptr_t)15);
+        const uint64_t skip = (uint64_t)(tile0 - c->arr_base);
+        for (const auto& pc : c->arr_pieces) {
+            CK(cudaStreamWaitEvent(c->stream, pc.second, 0));
+            const uint64_t have = pc.first > skip ? pc.first - skip : 0;
+            const uint64_t t_hi = have > 65600 ? std::min(n_tiles, (have - 65600) / tb) : 0;
+            int rc0 = scan(t_done, t_hi);
+            if (rc0) return rc0;
+            t_done = std::max(t_done, t_hi);
+        }
+        c->arr_base = nullptr;  // everything has arrived for the kernels that follow
+        c->arr_pieces.clear();
+    }
+    int rcs = scan(t_done, n_tiles);
+    if (rcs) return rcs;
     VerifyArgs V{body, blen, cand, counts, cap, surv, counts + 1, cap2, nullptr, nullptr};
     RRG_LAUNCH(k_verify_light, c->n_sm * 8, 256, 0, c->stream, V);
     LAUNCHED(c);
@@ -873,6 +915,7 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
             for (size_t q = t0; q < targets.size(); q++)
                 limits.push_back(q + 1 < targets.size() ? targets[q + 1] : base_bit + total_bits);
         }
+        if (int rw = wait_arrival(c, err)) return rw;
         if (!targets.empty()) {
             const uint32_t n = (uint32_t)targets.size();
             std::vector<uint64_t> found(n, ~0ull);
@@ -1343,6 +1386,7 @@ int bgzf_enqueue(rrg_ctx* c, const uint8_t* d_file, uint64_t len, uint8_t* d_out
 int bgzf_route(rrg_ctx* c, const uint8_t* d_file, uint64_t len, OutTarget& tgt, Decoded* out, uint64_t* rem,
                bool* truncated, rrg_error* err) {
     *out = Decoded{};
+    if (int rw = wait_arrival(c, err)) return rw;
     if (!c->h_bg) CK(cudaMallocHost((void**)&c->h_bg, 64));
     uint32_t cap = std::max<uint32_t>(c->bg_cap, (uint32_t)std::min<uint64_t>(len / 2048 + 4096, 1u << 30));
     const uint32_t sgrid =
@@ -1652,13 +1696,42 @@ int decode_host_impl(rrg_ctx* c, const uint8_t* data, size_t len, rrg_sink_fn si
     }
     double t0 = now_ms();
     CK(dgrow(c->comp, len + 16));
-    CK(cudaMemcpyAsync(c->comp.p, data, len, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
+#ifdef RRG_EMU
+    const size_t pipe_min = 1u << 20;  // the CPU emulation exercises the piecewise path on small inputs
+#else
+    const size_t pipe_min = 16u << 20;
+#endif
+    if (len >= pipe_min && host_bgzf_size(data, len) < 0) {
+        // a member stream: copy in 8 pieces on the copy stream; the boundary
+        // scan starts on each piece as it lands (and everything else waits
+        // for the last one)
+        if (!c->copy_stream) CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        const uint64_t P = (len + 7) / 8;
+        c->arr_pieces.clear();
+        for (int i = 0; i < 8; i++) {
+            const uint64_t o = (uint64_t)i * P;
+            if (o >= len) break;
+            const uint64_t l = std::min<uint64_t>(P, len - o);
+            if (!c->arr_events[i]) CK(cudaEventCreateWithFlags(&c->arr_events[i], cudaEventDisableTiming));
+            CK(cudaMemcpyAsync((uint8_t*)c->comp.p + o, data + o, l, cudaMemcpyHostToDevice, c->copy_stream));
+            CK(cudaEventRecord(c->arr_events[i], c->copy_stream));
+            c->arr_pieces.push_back({o + l, c->arr_events[i]});
+        }
+        c->arr_base = (const uint8_t*)c->comp.p;
+    } else {
+        CK(cudaMemcpyAsync(c->comp.p, data, len, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
     c->st.h2d_ms = now_ms() - t0;
     // output size is only known after the chain; decode into the context buffer
     Decoded d;
     OutTarget tgt{(uint8_t*)c->out.p, c->out.cap, true};
     int rc = decode_file(c, (const uint8_t*)c->comp.p, len, data, tgt, &d, err);
+    if (c->arr_base) {  // a path that launched nothing (an early error): drain the copies
+        c->arr_base = nullptr;
+        c->arr_pieces.clear();
+        cudaStreamSynchronize(c->copy_stream);
+    }
     bool closed = false;
     if (!rc) {
         c->st.uncompressed_bytes = d.total;
@@ -2158,6 +2231,9 @@ void rrg_gpu_destroy(rrg_ctx* c) {
     for (auto& p : c->h_stage)
         if (p) cudaFreeHost(p);
     if (c->h_bg) cudaFreeHost(c->h_bg);
+    for (cudaEvent_t e : c->arr_events)
+        if (e) cudaEventDestroy(e);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
 }

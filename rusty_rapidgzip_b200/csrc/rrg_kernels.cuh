@@ -1779,6 +1779,7 @@ struct ScanArgs {
     uint64_t* stored;       // stored-block starts (bit offsets), appended
     uint32_t* n_stored;
     uint32_t stored_cap;
+    uint64_t tile_lo, tile_hi;  // the tiles this launch covers (input that has arrived)
 };
 
 // 32 bits of the staged tile starting at bit b (b + 32 <= 8 * tile bytes)
@@ -1800,8 +1801,9 @@ __global__ void __launch_bounds__(ST) k_scan_candidates(ScanArgs A) {
     const uint8_t* base = (const uint8_t*)(addr & ~(uintptr_t)15);
     const uint64_t lo = addr & 15, hi = lo + A.body_len;
     const uint64_t n_tiles = (hi + TILE - 1) / TILE;
+    const uint64_t t_end = A.tile_hi < n_tiles ? A.tile_hi : n_tiles;
     uint8_t* tb = reinterpret_cast<uint8_t*>(tile);
-    for (uint64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+    for (uint64_t t = A.tile_lo + blockIdx.x; t < t_end; t += gridDim.x) {
         const uint64_t t0 = t * TILE;
         if (threadIdx.x == 0) s_n = 0;
         for (uint32_t q = threadIdx.x; q < (TILE + SCAN_HALO) / 16; q += blockDim.x) {

@@ -287,3 +287,18 @@ def test_sync_flush_starts_are_not_redone(emu_decoder_factory):
     st = d.decode_host(gz, out.append)
     assert b"".join(out) == raw
     assert st.gpu_chunks >= 4 and st.speculation_failures == 0
+
+
+def test_host_path_scans_pieces_as_they_arrive(emu_decoder_factory):
+    """The host entry point copies a large input in pieces and starts the
+    boundary scan on each piece as it lands; the result is the same as the
+    oracle's and every sub-chunk start is a real block start."""
+    rng = np.random.default_rng(17)
+    raw = W.fastq_like(700_000, 17) + rng.integers(0, 256, 900_000, dtype=np.uint8).tobytes()
+    gz = W.gzip_member(raw, 1)
+    assert len(gz) >= 1 << 20
+    d = emu_decoder_factory(gpu_chunk_bytes=65536)
+    out = []
+    st = d.decode_host(gz, out.append)
+    assert b"".join(out) == raw
+    assert st.gpu_chunks >= 8 and st.speculation_failures == 0
