@@ -226,6 +226,7 @@ typedef struct rrg_serve_stats {
     uint64_t in_use_bytes, peak_in_use_bytes, budget_bytes;
     uint64_t waiting;            /* submitted, not yet admitted */
     uint64_t bytes_out;          /* decompressed bytes finished */
+    double h2d_ms, decode_ms, d2h_ms;  /* engine time copying requests in, decoding, copying results out (summed over engines) */
 } rrg_serve_stats;
 
 /* Start the serving loop with `engines` engines (0 = 2) and a completion queue

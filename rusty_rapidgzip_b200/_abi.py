@@ -93,7 +93,8 @@ class _Tuning(C.Structure):
 class _ServeStats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("submitted", "completed", "batches", "max_batch", "engines_busy",
                                           "max_engines_busy", "in_use_bytes", "peak_in_use_bytes", "budget_bytes",
-                                          "waiting", "bytes_out")]
+                                          "waiting", "bytes_out")] + [
+        (n, C.c_double) for n in ("h2d_ms", "decode_ms", "d2h_ms")]
 
 
 class _Stats(C.Structure):
@@ -532,7 +533,8 @@ class Decoder:
     def serve_stats(self) -> dict:
         st = _ServeStats()
         self._L.rrg_gpu_serve_stats(self._ctx, C.byref(st))
-        return {f: int(getattr(st, f)) for f, _ in _ServeStats._fields_}
+        return {f: (round(getattr(st, f), 3) if f.endswith("_ms") else int(getattr(st, f)))
+                for f, _ in _ServeStats._fields_}
 
 
 def read_gz(path, sink, config: Config | None = None) -> DecodeStats:

@@ -2047,9 +2047,11 @@ void engine_loop(Server* S, rrg_ctx* E) {
         auto fail_all = [&](int code) {
             for (size_t i = 0; i < n; i++) status[i] = code;
         };
+        double t_h2d = 0, t_dec = 0;
         for (int attempt = 0; attempt < 2; attempt++) {
             rc = 0;
             std::fill(status.begin(), status.end(), RRG_OK);
+            const double ta = now_ms();
             if (dgrow(E->comp, ti + 64) != cudaSuccess || dgrow(E->out, to + 64) != cudaSuccess) {
                 cudaGetLastError();
                 rc = RRG_ERR_OUT_OF_MEMORY;
@@ -2058,11 +2060,14 @@ void engine_loop(Server* S, rrg_ctx* E) {
                 if (in_len[i] && cudaMemcpyAsync((uint8_t*)E->comp.p + in_off[i], batch[i].data.data(), in_len[i],
                                                  cudaMemcpyHostToDevice, E->stream) != cudaSuccess)
                     rc = RRG_ERR_CUDA;
+            const double tb = now_ms();
             if (!rc) {
                 E->st = rrg_stats{};
                 rc = batch_impl(E, (const uint8_t*)E->comp.p, in_off.data(), in_len.data(), (uint8_t*)E->out.p,
                                 out_off.data(), out_cap.data(), out_len.data(), status.data(), n, &err);
             }
+            t_h2d += tb - ta;
+            t_dec += now_ms() - tb;
             if (rc != RRG_ERR_OUT_OF_MEMORY) break;
             // device memory ran out: drop this engine's resident scratch, once more
             cudaGetLastError();
@@ -2071,6 +2076,7 @@ void engine_loop(Server* S, rrg_ctx* E) {
         if (rc) fail_all(rc);
         std::vector<Server::Done> fin;
         std::vector<Server::Req> retry;
+        const double t_out = now_ms();
         for (size_t i = 0; i < n; i++) {
             Server::Req& r = batch[i];
             if (status[i] == RRG_ERR_CAPACITY && !r.out_need && out_len[i] > out_cap[i]) {
@@ -2102,6 +2108,9 @@ void engine_loop(Server* S, rrg_ctx* E) {
         if (reserved > S->budget / S->engines.size()) release_scratch(E);
         {
             std::lock_guard<std::mutex> g(S->mu);
+            S->stats.h2d_ms += t_h2d;
+            S->stats.decode_ms += t_dec;
+            S->stats.d2h_ms += t_fin - t_out;
             S->in_use -= reserved;
             S->stats.engines_busy--;
             for (auto& r : retry) S->waiting.push_front(std::move(r));
