@@ -1822,7 +1822,7 @@ int batch_impl(rrg_ctx* c, const uint8_t* d_in, const uint64_t* in_off, const ui
         const uint64_t blen = j.len - j.body_off;
         // ISIZE of the (last) member: a size hint for the reserved cells
         if (isz[i] && blen)
-            j.expand = std::min(c->expand, std::max(1.05, 1.25 * (double)isz[i] / (double)blen + 0.05));
+            j.expand = std::min(1100.0, std::max(1.05, 1.25 * (double)isz[i] / (double)blen + 0.05));
         jobs.push_back(j);
         job_item.push_back(i);
     }
@@ -2095,9 +2095,23 @@ void engine_loop(Server* S, rrg_ctx* E) {
                 if (!d.out) {
                     d.status = RRG_ERR_OUT_OF_MEMORY;
                     d.len = 0;
-                } else if (out_len[i] && cudaMemcpyAsync(d.out, (const uint8_t*)E->out.p + out_off[i], out_len[i],
-                                                         cudaMemcpyDeviceToHost, E->stream) != cudaSuccess) {
-                    d.status = RRG_ERR_CUDA;
+                } else if (out_len[i]) {
+                    // through the engine's pinned double buffer: each piece's copy
+                    // to the result overlaps the next piece's transfer
+                    struct Dst {
+                        uint8_t* p;
+                        size_t at;
+                    } dst{d.out, 0};
+                    auto copy_sink = [](void* u, const uint8_t* p, size_t len) -> int {
+                        Dst* t = (Dst*)u;
+                        std::memcpy(t->p + t->at, p, len);
+                        t->at += len;
+                        return 0;
+                    };
+                    bool closed = false;
+                    rrg_error e2{};
+                    if (deliver(E, (const uint8_t*)E->out.p + out_off[i], out_len[i], copy_sink, &dst, &closed, &e2))
+                        d.status = RRG_ERR_CUDA;
                 }
             }
             fin.push_back(d);
