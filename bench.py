@@ -342,7 +342,7 @@ def run_serve(args):
     t_gen = time.perf_counter() - t_gen
     rates = [float(x) for x in args.rates.split(",")]
     dec = Decoder(Config(device=0))
-    dec.serve_start(engines=2, max_ready=16)
+    dec.serve_start(engines=args.engines, max_ready=16)
     # warm-up: every pool item once (untimed; grows the engines' resident scratch)
     for gz in pool:
         dec.submit(gz)
@@ -421,7 +421,7 @@ def run_serve(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator)",
             "config": {"workload": "serving_poisson_requests_log_uniform_64KiB_1GiB_mixed_content",
                        "pool_requests": n_pool, "pool_uncompressed_bytes": sum(lens),
-                       "duration_s_per_rate": args.duration, "hbm_budget_bytes": st["budget_bytes"], "engines": 2,
+                       "duration_s_per_rate": args.duration, "hbm_budget_bytes": st["budget_bytes"], "engines": args.engines,
                        "max_outstanding": args.max_outstanding, "per_rate": per_rate,
                        "serve_stats": st, "generation_s": round(t_gen, 1)},
             "e2e": {"value": top["sustained_gbs"], "unit": "GB/s",
@@ -625,6 +625,7 @@ def main():
     ap.add_argument("--rates", default="10,50,200", help="serve: request rates (req/s)")
     ap.add_argument("--duration", type=float, default=20.0, help="serve: seconds of arrivals per rate")
     ap.add_argument("--max-outstanding", type=int, default=32, help="serve: waiting requests before rejecting")
+    ap.add_argument("--engines", type=int, default=4, help="serve: decode engines (sub-contexts with their own stream)")
     ap.add_argument("--size", type=int, default=None)
     ap.add_argument("--gpu-chunk", type=int, default=0)
     ap.add_argument("--warps-per-stream", type=int, default=0, help="-1: one decoder per lane")

@@ -274,6 +274,9 @@ int64_t rrg_gpu_pending(rrg_ctx* ctx);
 int rrg_gpu_crc32_noalloc(const uint8_t* d_data, size_t len, uint32_t* crc_out, void* stream,
                           rrg_error* err);
 
+/* Release a result buffer returned by rrg_gpu_poll. Buffers of 1 MiB and more
+ * return to the library's pool (at most 32 GiB held idle) and are reused for
+ * later results, whose pages are then already mapped. */
 void rrg_gpu_free(void* p);
 
 /* Library version string and the number of kernels this library has launched

@@ -1978,6 +1978,65 @@ void release_scratch(rrg_ctx* c) {
     c->tables_uploaded = false;
 }
 
+// ------------------------------------------------------------ result buffers
+// Serving results are host buffers the caller releases with rrg_gpu_free.
+// Freed buffers of 1 MiB and more are kept by size class (powers of two, at
+// most 32 GiB in all) and handed out again, so a steady request stream writes
+// into memory whose pages are already mapped instead of faulting in fresh ones.
+struct ResultPool {
+    std::mutex mu;
+    std::unordered_map<void*, int> cls;           // every pooled block ever handed out -> class
+    std::vector<std::vector<void*>> free_by_cls;  // class -> idle blocks
+    uint64_t idle_bytes = 0;
+};
+ResultPool& result_pool() {
+    static ResultPool* p = new ResultPool;
+    return *p;
+}
+constexpr uint64_t POOL_MIN = 1ull << 20, POOL_MAX_IDLE = 32ull << 30;
+
+void* result_alloc(uint64_t n) {
+    if (n < POOL_MIN) return std::malloc(std::max<uint64_t>(n, 1));
+    int k = 20;
+    while ((1ull << k) < n) k++;
+    ResultPool& P = result_pool();
+    {
+        std::lock_guard<std::mutex> g(P.mu);
+        if ((int)P.free_by_cls.size() > k && !P.free_by_cls[k].empty()) {
+            void* b = P.free_by_cls[k].back();
+            P.free_by_cls[k].pop_back();
+            P.idle_bytes -= 1ull << k;
+            return b;
+        }
+    }
+    void* b = std::malloc(1ull << k);
+    if (b) {
+        std::lock_guard<std::mutex> g(P.mu);
+        P.cls[b] = k;
+    }
+    return b;
+}
+
+void result_free(void* b) {
+    if (!b) return;
+    ResultPool& P = result_pool();
+    {
+        std::lock_guard<std::mutex> g(P.mu);
+        auto it = P.cls.find(b);
+        if (it != P.cls.end()) {
+            const int k = it->second;
+            if (P.idle_bytes + (1ull << k) <= POOL_MAX_IDLE) {
+                if ((int)P.free_by_cls.size() <= k) P.free_by_cls.resize(k + 1);
+                P.free_by_cls[k].push_back(b);
+                P.idle_bytes += 1ull << k;
+                return;
+            }
+            P.cls.erase(it);
+        }
+    }
+    std::free(b);
+}
+
 // ------------------------------------------------------------ serving engines
 // Device bytes a request holds while admitted: its input, its output and
 // the speculative-decode scratch (u16 cells plus slack), from the trailer's
@@ -2090,7 +2149,7 @@ void engine_loop(Server* S, rrg_ctx* E) {
                 else set_err(&d.err, status[i], "request failed with status %d", status[i]);
             }
             if (status[i] == RRG_OK) {
-                d.out = (uint8_t*)std::malloc(std::max<uint64_t>(out_len[i], 1));
+                d.out = (uint8_t*)result_alloc(out_len[i]);
                 d.len = out_len[i];
                 if (!d.out) {
                     d.status = RRG_ERR_OUT_OF_MEMORY;
@@ -2130,7 +2189,7 @@ void engine_loop(Server* S, rrg_ctx* E) {
             for (auto& r : retry) S->waiting.push_front(std::move(r));
             for (auto& d : fin) {
                 if (d.status != RRG_OK && d.out) {
-                    std::free(d.out);
+                    result_free(d.out);
                     d.out = nullptr;
                     d.len = 0;
                 }
@@ -2187,7 +2246,7 @@ void serve_stop(rrg_ctx* c) {
     for (auto& t : S->threads) t.join();
     for (rrg_ctx* E : S->engines) rrg_gpu_destroy(E);
     for (auto& d : S->done)
-        if (d.out) std::free(d.out);
+        if (d.out) result_free(d.out);
     delete S;
     c->srv = nullptr;
 }
@@ -2629,7 +2688,7 @@ int64_t rrg_gpu_pending(rrg_ctx* c) {
     return c->srv->outstanding;
 }
 
-void rrg_gpu_free(void* p) { std::free(p); }
+void rrg_gpu_free(void* p) { result_free(p); }
 
 const char* rrg_gpu_version(void) { return "rrg-gpu 0.1 (sm_100a)"; }
 
