@@ -345,7 +345,7 @@ def run_serve(args):
     dec.serve_start(engines=args.engines, max_ready=16)
     # warm-up: every pool item once (untimed; grows the engines' resident scratch)
     for gz in pool:
-        dec.submit(gz)
+        dec.submit(gz, copy=False)
     for _ in pool:
         while dec.poll(timeout_ms=1000) is None:
             pass
@@ -371,7 +371,7 @@ def run_serve(args):
                 if dec.pending() >= args.max_outstanding:
                     rejected[0] += 1
                     continue
-                rid = dec.submit(pool[k])
+                rid = dec.submit(pool[k], copy=False)
                 with lock:
                     sched[rid] = (t, k)
 

@@ -244,6 +244,12 @@ int rrg_gpu_serve_stats(rrg_ctx* ctx, rrg_serve_stats* out);
  * request id >= 0, or -1 on error. */
 int64_t rrg_gpu_submit(rrg_ctx* ctx, const uint8_t* data, size_t len, rrg_error* err);
 
+/* Same, without the copy: the engine reads `data` in place, so the caller
+ * keeps it valid and unchanged until rrg_gpu_poll has returned this request.
+ * For servers whose request bodies already sit in memory they own: the copy
+ * costs more host time than the decode of a large request. */
+int64_t rrg_gpu_submit_nocopy(rrg_ctx* ctx, const uint8_t* data, size_t len, rrg_error* err);
+
 /* Collect one finished request, waiting up to `timeout_ms`. Returns 1 and
  * fills the outputs, 0 if none finished in time, or a negative rrg_status on
  * failure. `*out` is a malloc'd buffer the caller frees with rrg_gpu_free;

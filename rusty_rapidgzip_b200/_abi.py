@@ -254,6 +254,8 @@ def load_library(path: str | None = None):
                                            C.POINTER(u64), C.POINTER(i32), E]
         L.rrg_gpu_submit.argtypes = [vp, vp, sz, E]
         L.rrg_gpu_submit.restype = C.c_int64
+        L.rrg_gpu_submit_nocopy.argtypes = [vp, vp, sz, E]
+        L.rrg_gpu_submit_nocopy.restype = C.c_int64
         L.rrg_gpu_poll.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(sz),
                                    C.POINTER(i32), C.POINTER(C.c_double), i32, E]
         L.rrg_gpu_serve_start.argtypes = [vp, C.c_uint32, C.c_uint32, E]
@@ -312,6 +314,10 @@ class Decoder:
         self._ctx = self._L.rrg_gpu_create(C.byref(self.config._c()), C.byref(e))
         if not self._ctx:
             _raise(e)
+        import threading
+        self._inflight: dict = {}      # zero-copy requests: id -> the bytes the engines read
+        self._polled_early: set = set()
+        self._inflight_lock = threading.Lock()
 
     def close(self):
         if getattr(self, "_ctx", None):
@@ -466,14 +472,28 @@ class Decoder:
                 bool(fin.value))
 
     # -------------------------------------------------------------- serving
-    def submit(self, data) -> int:
+    def submit(self, data, copy: bool = True) -> int:
+        """Queue a decode request. With copy=False the library reads `data` in
+        place; this decoder keeps a reference to it until poll returns it."""
         addr, n, keep = _host_buffer(data)
         e = _Error()
-        rid = self._L.rrg_gpu_submit(self._ctx, addr, n, C.byref(e))
-        del keep
+        fn = self._L.rrg_gpu_submit if copy else self._L.rrg_gpu_submit_nocopy
+        rid = fn(self._ctx, addr, n, C.byref(e))
         if rid < 0:
             _raise(e)
+        if not copy:
+            with self._inflight_lock:
+                if int(rid) in self._polled_early:  # already finished and polled
+                    self._polled_early.discard(int(rid))
+                else:
+                    self._inflight[int(rid)] = (data, keep)
+        del keep
         return int(rid)
+
+    def _release(self, rid: int):
+        with self._inflight_lock:
+            if self._inflight.pop(rid, None) is None:
+                self._polled_early.add(rid)
 
     def poll(self, timeout_ms: int = 0):
         """-> None, or (request_id, bytes | None, status, latency_ms)."""
@@ -489,6 +509,7 @@ class Decoder:
             _raise(e)
         if r == 0:
             return None
+        self._release(int(rid.value))
         self.last_poll_error = e.message.decode(errors="replace") if stv.value else ""
         data = None
         if out:
@@ -511,6 +532,7 @@ class Decoder:
             _raise(e)
         if r == 0:
             return None
+        self._release(int(rid.value))
         addr = C.cast(out, C.c_void_p).value or 0
         return int(rid.value), addr, int(n.value), int(stv.value), float(lat.value)
 

@@ -286,7 +286,9 @@ struct rrg_ctx {
 struct Server {
     struct Req {
         int64_t id;
-        std::vector<uint8_t> data;
+        std::vector<uint8_t> copy;   // the request's bytes when submit copied them
+        const uint8_t* bytes = nullptr;  // the bytes (the copy, or the caller's buffer)
+        uint64_t len = 0;
         double t_submit;
         uint64_t out_need = 0;  // exact output size once known (a retry after RRG_ERR_CAPACITY)
     };
@@ -2042,8 +2044,8 @@ void result_free(void* b) {
 // the speculative-decode scratch (u16 cells plus slack), from the trailer's
 // ISIZE as the size hint.
 uint64_t serve_reserve(const Server::Req& r, double expand_cap) {
-    const uint64_t c = r.data.size();
-    const uint64_t isz = c >= 4 ? le32h(r.data.data() + c - 4) : 0;
+    const uint64_t c = r.len;
+    const uint64_t isz = c >= 4 ? le32h(r.bytes + c - 4) : 0;
     const uint64_t out = r.out_need ? r.out_need : std::max<uint64_t>(isz, c);
     const double ex = c ? std::min(expand_cap, std::max(1.05, 1.25 * (double)out / (double)c + 0.05)) : 1.0;
     return c + out + (uint64_t)(2.0 * 1.6 * ex * (double)c) + (2ull << 20);
@@ -2092,8 +2094,8 @@ void engine_loop(Server* S, rrg_ctx* E) {
         uint64_t ti = 0, to = 0;
         for (size_t i = 0; i < n; i++) {
             const Server::Req& r = batch[i];
-            const uint64_t c = r.data.size();
-            const uint64_t isz = c >= 4 ? le32h(r.data.data() + c - 4) : 0;
+            const uint64_t c = r.len;
+            const uint64_t isz = c >= 4 ? le32h(r.bytes + c - 4) : 0;
             in_off[i] = ti;
             in_len[i] = c;
             ti += (c + 255) & ~255ull;
@@ -2116,7 +2118,7 @@ void engine_loop(Server* S, rrg_ctx* E) {
                 rc = RRG_ERR_OUT_OF_MEMORY;
             }
             for (size_t i = 0; i < n && !rc; i++)
-                if (in_len[i] && cudaMemcpyAsync((uint8_t*)E->comp.p + in_off[i], batch[i].data.data(), in_len[i],
+                if (in_len[i] && cudaMemcpyAsync((uint8_t*)E->comp.p + in_off[i], batch[i].bytes, in_len[i],
                                                  cudaMemcpyHostToDevice, E->stream) != cudaSuccess)
                     rc = RRG_ERR_CUDA;
             const double tb = now_ms();
@@ -2631,7 +2633,7 @@ int rrg_gpu_serve_stats(rrg_ctx* c, rrg_serve_stats* out) {
     return 0;
 }
 
-int64_t rrg_gpu_submit(rrg_ctx* c, const uint8_t* data, size_t len, rrg_error* err) {
+static int64_t submit_impl(rrg_ctx* c, const uint8_t* data, size_t len, bool copy, rrg_error* err) {
     if (!c || (!data && len)) {
         set_err(err, RRG_ERR_INVALID_ARGUMENT, "null argument");
         return -1;
@@ -2644,7 +2646,13 @@ int64_t rrg_gpu_submit(rrg_ctx* c, const uint8_t* data, size_t len, rrg_error* e
     Server* S = c->srv;
     Server::Req r;
     r.t_submit = t0;
-    r.data.assign(data, data + len);
+    r.len = len;
+    if (copy) {
+        r.copy.assign(data, data + len);
+        r.bytes = r.copy.data();
+    } else {
+        r.bytes = data;
+    }
     std::lock_guard<std::mutex> g(S->mu);
     r.id = S->next_id++;
     const int64_t id = r.id;
@@ -2653,6 +2661,14 @@ int64_t rrg_gpu_submit(rrg_ctx* c, const uint8_t* data, size_t len, rrg_error* e
     S->stats.submitted++;
     S->cv_work.notify_all();
     return id;
+}
+
+int64_t rrg_gpu_submit(rrg_ctx* c, const uint8_t* data, size_t len, rrg_error* err) {
+    return submit_impl(c, data, len, true, err);
+}
+
+int64_t rrg_gpu_submit_nocopy(rrg_ctx* c, const uint8_t* data, size_t len, rrg_error* err) {
+    return submit_impl(c, data, len, false, err);
 }
 
 int rrg_gpu_poll(rrg_ctx* c, int64_t* request_id, uint8_t** out, size_t* out_len, int32_t* status, double* latency_ms,

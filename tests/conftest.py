@@ -145,7 +145,7 @@ def serve_requests(n: int, seed: int, hi: int):
     return reqs
 
 
-def run_serving(d, reqs, seed: int, gap_s: float):
+def run_serving(d, reqs, seed: int, gap_s: float, copy: bool = True):
     """Submit `reqs` from a thread at random gaps (open loop) while this thread
     polls; returns {request index: (status, bytes or None)}."""
     import random
@@ -157,7 +157,7 @@ def run_serving(d, reqs, seed: int, gap_s: float):
 
     def feeder():
         for i in order:
-            ids[d.submit(reqs[i])] = i
+            ids[d.submit(reqs[i], copy=copy)] = i
             time.sleep(rng.random() * gap_s)
 
     th = threading.Thread(target=feeder)

@@ -411,7 +411,7 @@ def test_serving_alone_and_in_the_mix(gpu_decoder_factory):
     budget = 256 << 20
     d = gpu_decoder_factory(hbm_budget_bytes=budget)
     d.serve_start(engines=2, max_ready=8)
-    got = run_serving(d, reqs, seed=2, gap_s=0.002)
+    got = run_serving(d, reqs, seed=2, gap_s=0.002, copy=False)  # zero-copy submits
     assert got == want
     st = d.serve_stats()
     assert st["completed"] == len(reqs) and d.pending() == 0
