@@ -1699,7 +1699,7 @@ int decode_host_impl(rrg_ctx* c, const uint8_t* data, size_t len, rrg_sink_fn si
     double t0 = now_ms();
     CK(dgrow(c->comp, len + 16));
 #ifdef RRG_EMU
-    const size_t pipe_min = 1u << 20;  // the CPU emulation exercises the piecewise path on small inputs
+    const size_t pipe_min = 256u << 10;  // the CPU emulation exercises the piecewise path on small inputs
 #else
     const size_t pipe_min = 16u << 20;
 #endif

@@ -2,14 +2,16 @@
 //
 // TEST INFRASTRUCTURE ONLY. Lets the unit tests compile the product's kernel
 // and host sources with g++ (-DRRG_EMU -include cuda_emu.h) and run them on
-// the CPU: every thread of a block is a std::thread; warp shuffles, ballots,
-// matches and __syncwarp go through a per-warp exchange with a 32-party
-// barrier; __syncthreads is a block barrier; blocks of a launch run one after
-// another. Device memory is host memory. The resulting library is used only by
+// the CPU: every thread of a block is a user-level fiber on the launching
+// thread; warp shuffles, ballots, matches and __syncwarp go through a per-warp
+// exchange with a 32-party barrier; __syncthreads is a block barrier; blocks
+// of a launch run one after another. Device memory is host memory. The resulting library is used only by
 // `-m "not gpu"` tests and never stands in for the GPU build.
 #pragma once
-#include <barrier>
-#include <condition_variable>
+#include <ucontext.h>
+
+#include <cstdio>
+#include <deque>
 #include <mutex>
 #include <cstdint>
 #include <cstdlib>
@@ -53,12 +55,51 @@ enum cudaFuncAttribute { cudaFuncAttributeMaxDynamicSharedMemorySize = 8 };
 
 namespace emu {
 
+// ---- fibers. The threads of a block run as user-level contexts on the
+// launching thread, one at a time; a barrier parks the calling fiber until the
+// last one arrives, which releases them all. No OS threads, no futexes.
+struct Fiber {
+    ucontext_t ctx;
+    char* stack = nullptr;
+    unsigned tid = 0;
+    bool parked = false;
+};
+struct Sched {
+    ucontext_t main;
+    Fiber* cur = nullptr;
+    std::deque<Fiber*> ready;
+    std::function<void(unsigned)> enter;  // sets the fiber's identity, then runs the kernel body
+};
+inline thread_local Sched* t_sched = nullptr;
+
+struct Barrier {
+    unsigned needed, count = 0;
+    std::vector<Fiber*> parked;
+    explicit Barrier(unsigned n) : needed(n) {}
+    void arrive_and_wait() {
+        Sched* s = t_sched;
+        if (++count == needed) {  // the last arrival releases the others and continues
+            count = 0;
+            for (Fiber* f : parked) {
+                f->parked = false;
+                s->ready.push_back(f);
+            }
+            parked.clear();
+            return;
+        }
+        Fiber* me = s->cur;
+        me->parked = true;
+        parked.push_back(me);
+        swapcontext(&me->ctx, &s->main);
+    }
+};
+
 struct Warp {
-    std::barrier<> bar{32};
+    Barrier bar{32};
     uint64_t slot[32];
 };
 struct Block {
-    std::unique_ptr<std::barrier<>> bar;
+    std::unique_ptr<Barrier> bar;
     std::vector<std::unique_ptr<Warp>> warps;
 };
 inline thread_local Block* t_block = nullptr;
@@ -69,69 +110,36 @@ inline std::vector<unsigned char>& dyn_buf() {
     return b;
 }
 inline unsigned char* dyn_smem() { return dyn_buf().data(); }
-
-// Worker threads are created once and reused: thread i of every block runs on
-// pool thread i (a block needs all of its threads alive at once for the
-// barriers). Launches from several host threads are serialised.
-struct Pool {
-    std::mutex mu;
-    std::condition_variable cv, done_cv;
-    std::vector<std::thread> th;
-    uint64_t gen = 0;
-    unsigned active = 0, remaining = 0;
-    const std::function<void(unsigned)>* job = nullptr;
-
-    void ensure(unsigned n) {
-        while (th.size() < n) {
-            const unsigned id = (unsigned)th.size();
-            th.emplace_back([this, id] { loop(id); });
-            th.back().detach();
-        }
-    }
-    void loop(unsigned id) {
-        uint64_t seen = 0;
-        std::unique_lock<std::mutex> lk(mu);
-        for (;;) {
-            cv.wait(lk, [&] { return gen != seen; });
-            seen = gen;
-            if (id >= active) continue;
-            const std::function<void(unsigned)>* j = job;
-            lk.unlock();
-            (*j)(id);
-            lk.lock();
-            if (--remaining == 0) done_cv.notify_all();
-        }
-    }
-    void run(unsigned n, const std::function<void(unsigned)>& f) {
-        ensure(n);
-        std::unique_lock<std::mutex> lk(mu);
-        job = &f;
-        active = n;
-        remaining = n;
-        gen++;
-        cv.notify_all();
-        done_cv.wait(lk, [&] { return remaining == 0; });
-    }
-};
-inline Pool& pool() {
-    static Pool* p = new Pool;  // never destroyed: its threads outlive static destruction
-    return *p;
-}
 inline std::mutex& launch_mutex() {
     static std::mutex m;
     return m;
 }
 
+constexpr size_t FIBER_STACK = 256 << 10;
+
+inline void fiber_main() {
+    Sched* s = t_sched;
+    s->enter(s->cur->tid);
+    // returning ends the fiber: uc_link resumes the scheduler
+}
+
+// Launches from several host threads are serialised (shared memory is static).
 inline void launch(dim3 grid, dim3 block, size_t smem, const std::function<void()>& body) {
     std::lock_guard<std::mutex> guard(launch_mutex());
-    unsigned nthreads = block.x;
+    static std::vector<char*> stacks;  // reused across launches
+    const unsigned nthreads = block.x;
     auto& buf = dyn_buf();
     if (buf.size() < smem + 64) buf.assign(smem + 64, 0);
+    while (stacks.size() < nthreads) stacks.push_back(static_cast<char*>(std::malloc(FIBER_STACK)));
+    std::vector<Fiber> fib(nthreads);
+    Sched sched;
+    Sched* prev = t_sched;
+    t_sched = &sched;
     for (unsigned b = 0; b < grid.x; b++) {
         Block blk;
-        blk.bar = std::make_unique<std::barrier<>>(nthreads);
+        blk.bar = std::make_unique<Barrier>(nthreads);
         for (unsigned w = 0; w < (nthreads + 31) / 32; w++) blk.warps.push_back(std::make_unique<Warp>());
-        const std::function<void(unsigned)> one = [&, b](unsigned t) {
+        sched.enter = [&, b](unsigned t) {
             t_block = &blk;
             t_warp = blk.warps[t / 32].get();
             t_tid = dim3(t);
@@ -140,8 +148,41 @@ inline void launch(dim3 grid, dim3 block, size_t smem, const std::function<void(
             t_gdim = grid;
             body();
         };
-        pool().run(nthreads, one);
+        for (unsigned t = 0; t < nthreads; t++) {
+            Fiber& f = fib[t];
+            f.tid = t;
+            f.parked = false;
+            f.stack = stacks[t];
+            getcontext(&f.ctx);
+            f.ctx.uc_stack.ss_sp = f.stack;
+            f.ctx.uc_stack.ss_size = FIBER_STACK;
+            f.ctx.uc_link = &sched.main;
+            makecontext(&f.ctx, fiber_main, 0);
+            sched.ready.push_back(&f);
+        }
+        unsigned finished = 0;
+        while (!sched.ready.empty()) {
+            Fiber* f = sched.ready.front();
+            sched.ready.pop_front();
+            sched.cur = f;
+            // the identity of the fiber being resumed (thread-locals are per OS thread)
+            t_block = &blk;
+            t_warp = blk.warps[f->tid / 32].get();
+            t_tid = dim3(f->tid);
+            t_bid = dim3(b);
+            t_bdim = block;
+            t_gdim = grid;
+            swapcontext(&sched.main, &f->ctx);
+            // back here when the fiber parked at a barrier or finished
+            if (!f->parked) finished++;
+        }
+        if (finished != nthreads) {
+            std::fprintf(stderr, "cuda_emu: a barrier was never completed (%u of %u threads finished)\n", finished,
+                         nthreads);
+            std::abort();
+        }
     }
+    t_sched = prev;
 }
 
 }  // namespace emu

@@ -224,7 +224,7 @@ def test_serving_alone_and_in_the_mix(emu_decoder_factory):
     in the serving loop's mix, with two engines and a budget small enough that
     requests queue for admission."""
     from conftest import run_serving, serve_requests
-    reqs = serve_requests(3, seed=11, hi=32 << 10)
+    reqs = serve_requests(2, seed=11, hi=16 << 10)
     alone = emu_decoder_factory()
     want = {}
     for i, gz in enumerate(reqs):
@@ -294,10 +294,10 @@ def test_host_path_scans_pieces_as_they_arrive(emu_decoder_factory):
     boundary scan on each piece as it lands; the result is the same as the
     oracle's and every sub-chunk start is a real block start."""
     rng = np.random.default_rng(17)
-    raw = W.fastq_like(700_000, 17) + rng.integers(0, 256, 900_000, dtype=np.uint8).tobytes()
+    raw = W.fastq_like(120_000, 17) + rng.integers(0, 256, 250_000, dtype=np.uint8).tobytes()
     gz = W.gzip_member(raw, 1)
-    assert len(gz) >= 1 << 20
-    d = emu_decoder_factory(gpu_chunk_bytes=65536)
+    assert len(gz) >= 256 << 10
+    d = emu_decoder_factory(gpu_chunk_bytes=32768)
     out = []
     st = d.decode_host(gz, out.append)
     assert b"".join(out) == raw
