@@ -108,6 +108,7 @@ double now_ms() {
 
 // ---------------------------------------------------------------- host CRC
 uint32_t g_crc_tab[8][256];
+uint32_t g_crc_z496[4][256];  // register advanced over 496 zero bytes, per byte position
 uint32_t g_x2k[67];
 std::once_flag g_tab_once;
 
@@ -133,6 +134,12 @@ void init_tables() {
             g_crc_tab[t][n] = c;
         }
     }
+    for (int j = 0; j < 4; j++)
+        for (uint32_t b = 0; b < 256; b++) {
+            uint32_t v = b << (8 * j);
+            for (int i = 0; i < 496; i++) v = g_crc_tab[0][v & 0xff] ^ (v >> 8);
+            g_crc_z496[j][b] = v;
+        }
     g_x2k[0] = 0x40000000u;
     for (int k = 1; k < 67; k++) g_x2k[k] = host_mulmod(g_x2k[k - 1], g_x2k[k - 1]);
 }
@@ -380,8 +387,10 @@ int upload_tables(rrg_ctx* c, rrg_error* err) {
     std::call_once(g_tab_once, init_tables);
     std::call_once(g_lut_once, init_next_lut);
     CK(cudaMemcpyToSymbol(c_x2k, g_x2k, sizeof(g_x2k)));
-    CK(dgrow(c->crc_table, sizeof(g_crc_tab)));
+    CK(dgrow(c->crc_table, sizeof(g_crc_tab) + sizeof(g_crc_z496)));
     CK(cudaMemcpy(c->crc_table.p, g_crc_tab, sizeof(g_crc_tab), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy((uint8_t*)c->crc_table.p + sizeof(g_crc_tab), g_crc_z496, sizeof(g_crc_z496),
+                  cudaMemcpyHostToDevice));
     CK(dgrow(c->next_lut, sizeof(g_next_lut)));
     CK(cudaMemcpy(c->next_lut.p, g_next_lut, sizeof(g_next_lut), cudaMemcpyHostToDevice));
     c->tables_uploaded = true;
@@ -533,9 +542,10 @@ int crc_spans(rrg_ctx* c, const uint8_t* d_out, const std::vector<MemberSpan>& m
     CK(cudaMemcpyAsync(c->exp_isize.p, eisz.data(), nm * 4, cudaMemcpyHostToDevice, c->stream));
     KTimer kt(c->stream);
     if (np) {
-        CrcArgs A{d_out, (const CrcPiece*)c->pieces.p, np, (uint32_t*)c->piece_crc.p, (const uint32_t*)c->crc_table.p};
+        CrcWideArgs A{d_out, (const CrcPiece*)c->pieces.p, np, (uint32_t*)c->piece_crc.p,
+                      (const uint32_t*)c->crc_table.p, nullptr};
         uint32_t grid = persistent_blocks(c, 8, np, 1);
-        RRG_LAUNCH(k_crc_pieces, grid, CRC_THREADS, 0, c->stream, A);
+        RRG_LAUNCH(k_crc_pieces_wide, grid, CRCW_THREADS, 0, c->stream, A);
         LAUNCHED(c);
     }
     CrcMemberArgs B{(const CrcPiece*)c->pieces.p, (const uint32_t*)c->piece_crc.p, (const uint32_t*)c->mpiece.p, nm,
@@ -1368,8 +1378,9 @@ int bgzf_enqueue(rrg_ctx* c, const uint8_t* d_file, uint64_t len, uint8_t* d_out
     RRG_LAUNCH(k_bgzf_fix, c->n_sm * 4, 256, 0, c->stream, (const ChunkResult*)c->results.p, (CrcPiece*)c->pieces.p,
                (uint32_t*)c->exp_crc.p, (uint32_t*)c->exp_isize.p, (const uint32_t*)nmem);
     LAUNCHED(c);
-    CrcArgs P{d_out, (const CrcPiece*)c->pieces.p, 0, (uint32_t*)c->piece_crc.p, (const uint32_t*)c->crc_table.p, nmem};
-    RRG_LAUNCH(k_crc_pieces, c->n_sm * 8, CRC_THREADS, 0, c->stream, P);
+    CrcWideArgs P{d_out, (const CrcPiece*)c->pieces.p, 0, (uint32_t*)c->piece_crc.p, (const uint32_t*)c->crc_table.p,
+                  nmem};
+    RRG_LAUNCH(k_crc_pieces_wide, c->n_sm * 8, CRCW_THREADS, 0, c->stream, P);
     LAUNCHED(c);
     CrcMemberArgs M{(const CrcPiece*)c->pieces.p, (const uint32_t*)c->piece_crc.p, (const uint32_t*)c->mpiece.p, 0,
                     (const uint32_t*)c->exp_crc.p, (const uint32_t*)c->exp_isize.p, (uint32_t*)c->got_crc.p,

@@ -1991,6 +1991,9 @@ __device__ bool verify_light(const Src& s, uint64_t total_bits, uint64_t pos) {
             code <<= 1;
         }
         if (got < 0) return false;
+        // an oversubscribed code stays oversubscribed (the final test needs
+        // sums of exactly 2^15): stop at the first symbol that overshoots
+        if (kl > 32768u || kd > 32768u) return false;
         c.pos += used;
         if (got <= 15) {
             prev = (uint32_t)got;
@@ -2302,6 +2305,77 @@ __global__ void __launch_bounds__(CRC_THREADS) k_crc_pieces(CrcArgs A) {
             uint32_t cc = wcrc[0];
             for (int w = 1; w < nw; w++)
                 if (wlen[w]) cc = gf2_mulmod(cc, xpow8n(wlen[w])) ^ wcrc[w];
+            A.piece_crc[pi] = cc;
+        }
+        __syncthreads();
+    }
+}
+
+// Coalesced form for the decode paths. In each 512-byte row of a piece, lane l
+// of a warp takes bytes [16l, 16l + 16) with one 16-byte load, so a warp reads
+// whole rows. Each lane keeps a CRC register over its own 16-byte chunks as if
+// the other lanes' 496 bytes between them were zeros: before each chunk the
+// register is advanced over 496 zero bytes with four lookups (Z tables, x^3968
+// per byte position). Then slice-by-8 folds in the 16 bytes. Lane registers
+// are shifted to their place in the last row and XORed, warps' segments are
+// combined in order, and the unaligned head and the partial last row are
+// folded in serially.
+constexpr int CRCW_THREADS = 256;
+constexpr int CRCW_ROW = 512;  // bytes per warp row (32 lanes x 16)
+
+struct CrcWideArgs {
+    const uint8_t* data;
+    const CrcPiece* pieces;
+    uint32_t n_pieces;
+    uint32_t* piece_crc;    // raw CRC per piece
+    const uint32_t* table;  // 12 x 256: slice-by-8, then the 496-zero-byte advance per byte position
+    const uint32_t* n_dev;  // when set, the piece count is read here
+};
+
+__global__ void __launch_bounds__(CRCW_THREADS) k_crc_pieces_wide(CrcWideArgs A) {
+    __shared__ uint32_t T[8][256];
+    __shared__ uint32_t Z[4][256];
+    __shared__ uint32_t wcrc[CRCW_THREADS / 32];
+    __shared__ uint64_t wlen[CRCW_THREADS / 32];
+    for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) T[i >> 8][i & 255] = A.table[i];
+    for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) Z[i >> 8][i & 255] = A.table[8 * 256 + i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NW = CRCW_THREADS / 32;
+    const uint32_t n_pieces = A.n_dev ? *A.n_dev : A.n_pieces;
+    for (uint32_t pi = blockIdx.x; pi < n_pieces; pi += gridDim.x) {
+        const CrcPiece pc = A.pieces[pi];
+        const uint8_t* p = A.data + pc.start;
+        const uint64_t head = pc.len < ((16 - ((uintptr_t)p & 15)) & 15) ? pc.len : ((16 - ((uintptr_t)p & 15)) & 15);
+        const uint64_t rows = (pc.len - head) / CRCW_ROW;
+        const uint64_t r0 = (uint64_t)warp * rows / NW, r1 = (uint64_t)(warp + 1) * rows / NW;
+        const uint4* q = reinterpret_cast<const uint4*>(p + head);
+        uint32_t a = 0;
+        for (uint64_t r = r0; r < r1; r++) {
+            const uint4 w = q[r * 32 + lane];
+            a = Z[0][a & 255] ^ Z[1][(a >> 8) & 255] ^ Z[2][(a >> 16) & 255] ^ Z[3][a >> 24];
+            uint32_t lo = w.x ^ a, hi = w.y;
+            a = T[7][lo & 0xff] ^ T[6][(lo >> 8) & 0xff] ^ T[5][(lo >> 16) & 0xff] ^ T[4][lo >> 24] ^
+                T[3][hi & 0xff] ^ T[2][(hi >> 8) & 0xff] ^ T[1][(hi >> 16) & 0xff] ^ T[0][hi >> 24];
+            lo = w.z ^ a;
+            hi = w.w;
+            a = T[7][lo & 0xff] ^ T[6][(lo >> 8) & 0xff] ^ T[5][(lo >> 16) & 0xff] ^ T[4][lo >> 24] ^
+                T[3][hi & 0xff] ^ T[2][(hi >> 8) & 0xff] ^ T[1][(hi >> 16) & 0xff] ^ T[0][hi >> 24];
+        }
+        // bytes after this lane's last chunk in the segment's last row
+        if (r1 > r0 && lane < 31) a = gf2_mulmod(a, xpow8n((uint64_t)(31 - lane) * 16));
+        for (int o = 16; o; o >>= 1) a ^= __shfl_xor_sync(FULLMASK, a, o);
+        if (lane == 0) {
+            wcrc[warp] = a;
+            wlen[warp] = (r1 - r0) * CRCW_ROW;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t cc = 0;
+            for (uint64_t i = 0; i < head; i++) cc = T[0][(cc ^ p[i]) & 0xff] ^ (cc >> 8);
+            for (int w = 0; w < NW; w++)
+                if (wlen[w]) cc = gf2_mulmod(cc, xpow8n(wlen[w])) ^ wcrc[w];
+            for (uint64_t i = head + rows * CRCW_ROW; i < pc.len; i++) cc = T[0][(cc ^ p[i]) & 0xff] ^ (cc >> 8);
             A.piece_crc[pi] = cc;
         }
         __syncthreads();

@@ -302,3 +302,15 @@ def test_host_path_scans_pieces_as_they_arrive(emu_decoder_factory):
     st = d.decode_host(gz, out.append)
     assert b"".join(out) == raw
     assert st.gpu_chunks >= 8 and st.speculation_failures == 0
+
+
+def test_crc_rows_heads_and_tails(emu_decoder_factory):
+    """The coalesced CRC (16-byte rows per lane, zero-run advance between a
+    lane's chunks) at every start alignment, lengths around the row and piece
+    sizes, against zlib."""
+    d = emu_decoder_factory()
+    data = np.random.default_rng(2).integers(0, 256, (3 << 18) + 64, dtype=np.uint8)
+    base = haddr(data)
+    for off in (0, 1, 7, 15):
+        for n in (0, 1, 15, 16, 17, 511, 512, 513, 4095, 4096 * 8 + 3, 262144, 262144 + 777, 3 << 18):
+            assert d.crc32(base + off, n) == zlib.crc32(data[off:off + n].tobytes()), (off, n)
