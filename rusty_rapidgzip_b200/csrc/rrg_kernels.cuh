@@ -2141,33 +2141,32 @@ __global__ void __launch_bounds__(256) k_win_chase(ResolveArgs A) {
 }
 
 __global__ void __launch_bounds__(RES_THREADS) k_resolve(ResolveArgs A) {
-    __shared__ __align__(16) uint8_t stage[RES_TILE];
-    __shared__ uint32_t s_chunk;
-    __shared__ uint32_t s_bad;
-    __shared__ uint32_t s_mk;  // marker cells seen by this block (one global add at the end)
-    if (threadIdx.x == 0) s_mk = 0;
-    for (uint64_t t = blockIdx.x; t < A.n_tiles; t += gridDim.x) {
-        if (threadIdx.x == 0) {
-            s_chunk = A.tile_chunk[t];
-            s_bad = 0;
-        }
-        __syncthreads();
-        const uint32_t k = s_chunk;
+    // Two staging buffers, so one barrier per tile separates a tile's staging
+    // from its stores. A tile's bytes sit at the output's alignment within the
+    // buffer, so whole 16-byte words move with one shared load and one store.
+    __shared__ __align__(16) uint8_t stage[2][RES_TILE + 32];
+    uint32_t nmk = 0;
+    int buf = 0;
+    for (uint64_t t = blockIdx.x; t < A.n_tiles; t += gridDim.x, buf ^= 1) {
+        const uint32_t k = A.tile_chunk[t];
         const ResolveChunk ck = A.chunks[k];
         const uint32_t* win = A.win + (uint64_t)k * WINDOW;
         const uint8_t* winb = A.winb + (uint64_t)k * WINDOW;
         const bool win_clean = A.win_bad[k] == 0u;  // uniform over the tile
         const uint64_t c0 = (t - A.tile_start[k]) * (uint64_t)RES_TILE;
-        const uint64_t cn = ck.n_cells - c0 < (uint64_t)RES_TILE ? ck.n_cells - c0 : (uint64_t)RES_TILE;
+        const uint32_t cn = (uint32_t)(ck.n_cells - c0 < (uint64_t)RES_TILE ? ck.n_cells - c0 : (uint64_t)RES_TILE);
+        uint8_t* dst = A.out + ck.out_start + c0;
+        const uint32_t mis = (uint32_t)((uintptr_t)dst & 15);
+        uint8_t* sb = stage[buf];
         // warp w owns cells [512w, 512w + 512) of the tile, lane ln the cells
         // 512w + ln + 32i: one gather instruction covers 32 consecutive cells,
         // whose window sources are mostly consecutive too (copied runs), so a
         // warp's gathers touch few cache lines
         const uint32_t wbase = (threadIdx.x >> 5) * (32 * RES_PER_THREAD), ln = threadIdx.x & 31;
-        uint32_t nmk = 0, bad = 0;
+        uint32_t bad = 0;
         if (wbase < cn) {
             const uint16_t* p = A.cells + ck.slot_off + c0 + wbase + ln;
-            const uint32_t lim = (uint32_t)(cn - wbase);  // cells of this warp's span that exist
+            const uint32_t lim = cn - wbase;  // cells of this warp's span that exist
             uint32_t cell[RES_PER_THREAD];
 #pragma unroll
             for (int i = 0; i < RES_PER_THREAD; i++) cell[i] = (ln + 32u * i < lim) ? p[32 * i] : 0u;
@@ -2187,38 +2186,30 @@ __global__ void __launch_bounds__(RES_THREADS) k_resolve(ResolveArgs A) {
                 if (ln + 32u * i < lim) {
                     nmk += (cell[i] & MARKER16) ? 1u : 0u;
                     if (got[i] == WIN_INVALID || !(got[i] & WIN_BYTE)) bad = 1;
-                    stage[wbase + ln + 32 * i] = (uint8_t)got[i];
+                    sb[mis + wbase + ln + 32 * i] = (uint8_t)got[i];
                 }
             }
         }
-        if (bad) atomicOr(&s_bad, 1u);
-        nmk = warp_sum(nmk);
-        if ((threadIdx.x & 31) == 0 && nmk) atomicAdd(&s_mk, nmk);
-        __syncthreads();
-        if (s_bad && threadIdx.x == 0 && atomicCAS(A.err, 0u, 1u) == 0u) {
+        if (bad && atomicCAS(A.err, 0u, 1u) == 0u) {  // the first unresolvable cell names its chunk
             A.err[1] = k;
             A.err[2] = (uint32_t)c0;
             A.err[3] = (uint32_t)(c0 >> 32);
         }
-        // write stage[0..cn) to out[ck.out_start + c0 ...] with aligned 16-byte stores
-        uint8_t* dst = A.out + ck.out_start + c0;
-        const uint32_t head = (uint32_t)((16 - ((uintptr_t)dst & 15)) & 15);
-        const uint32_t h = head < cn ? head : (uint32_t)cn;
-        if (threadIdx.x < h) dst[threadIdx.x] = stage[threadIdx.x];
-        const uint32_t body = (uint32_t)((cn - h) / 16);
-        for (uint32_t i = threadIdx.x; i < body; i += blockDim.x) {
-            const uint8_t* sp = stage + h + i * 16;
-            uint4 v;
-            v.x = (uint32_t)sp[0] | ((uint32_t)sp[1] << 8) | ((uint32_t)sp[2] << 16) | ((uint32_t)sp[3] << 24);
-            v.y = (uint32_t)sp[4] | ((uint32_t)sp[5] << 8) | ((uint32_t)sp[6] << 16) | ((uint32_t)sp[7] << 24);
-            v.z = (uint32_t)sp[8] | ((uint32_t)sp[9] << 8) | ((uint32_t)sp[10] << 16) | ((uint32_t)sp[11] << 24);
-            v.w = (uint32_t)sp[12] | ((uint32_t)sp[13] << 8) | ((uint32_t)sp[14] << 16) | ((uint32_t)sp[15] << 24);
-            *reinterpret_cast<uint4*>(dst + h + i * 16) = v;
-        }
-        for (uint32_t i = h + body * 16 + threadIdx.x; i < cn; i += blockDim.x) dst[i] = stage[i];
         __syncthreads();
+        // words of the aligned output covering bytes [mis, mis + cn) of the buffer
+        uint8_t* dst_al = dst - mis;
+        const uint32_t nwords = (mis + cn + 15) / 16;
+        for (uint32_t w = threadIdx.x; w < nwords; w += blockDim.x) {
+            const uint32_t b0 = w * 16, b1 = b0 + 16;
+            if (b0 >= mis && b1 <= mis + cn) {
+                *reinterpret_cast<uint4*>(dst_al + b0) = *reinterpret_cast<const uint4*>(sb + b0);
+            } else {
+                for (uint32_t j = (b0 > mis ? b0 : mis); j < (b1 < mis + cn ? b1 : mis + cn); j++) dst_al[j] = sb[j];
+            }
+        }
     }
-    if (threadIdx.x == 0 && s_mk) atomicAdd(A.markers, (unsigned long long)s_mk);
+    nmk = warp_sum(nmk);
+    if ((threadIdx.x & 31) == 0 && nmk) atomicAdd(A.markers, (unsigned long long)nmk);
 }
 
 // ------------------------------------------------------- CRC-32
