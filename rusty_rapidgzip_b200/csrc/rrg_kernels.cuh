@@ -1797,6 +1797,11 @@ __global__ void __launch_bounds__(ST) k_scan_candidates(ScanArgs A) {
     __shared__ __align__(16) uint32_t tile[(TILE + SCAN_HALO) / 4];
     __shared__ uint32_t s_list[SCAN_LIST];
     __shared__ uint32_t s_n, s_base;
+    __shared__ uint32_t s_kt[64];  // two precode lengths -> Kraft weight (128 >> l) | count << 16
+    if (threadIdx.x < 64) {
+        const uint32_t l1 = threadIdx.x & 7u, l2 = threadIdx.x >> 3;
+        s_kt[threadIdx.x] = (l1 ? 128u >> l1 : 0u) + (l2 ? 128u >> l2 : 0u) + (((l1 ? 1u : 0u) + (l2 ? 1u : 0u)) << 16);
+    }
     const uintptr_t addr = (uintptr_t)A.body;
     const uint8_t* base = (const uint8_t*)(addr & ~(uintptr_t)15);
     const uint64_t lo = addr & 15, hi = lo + A.body_len;
@@ -1883,15 +1888,20 @@ __global__ void __launch_bounds__(ST) k_scan_candidates(ScanArgs A) {
                 m &= m - 1;
                 const uint32_t boff = 32 * (w0 + q) + r;  // bit offset inside the tile
                 const uint32_t hclen = (tile_bits(tile, boff + 13) & 15u) + 4;
-                const uint32_t y = tile_bits(tile, boff + 17), z = tile_bits(tile, boff + 47);
-                uint32_t kraft = 0, nsym = 0;
-#pragma unroll
-                for (uint32_t j = 0; j < 19; j++) {
-                    const uint32_t l = j < 10 ? (y >> (3 * j)) & 7u : (z >> (3 * (j - 10))) & 7u;
-                    const bool use = j < hclen && l;
-                    kraft += use ? (128u >> l) : 0u;
-                    nsym += use ? 1u : 0u;
+                uint32_t y = tile_bits(tile, boff + 17), z = tile_bits(tile, boff + 47);
+                // lengths past HCLEN are absent: clear their fields, then sum
+                // the Kraft weights and counts two 3-bit lengths per lookup
+                if (hclen <= 10) {
+                    y &= (1u << (3 * hclen)) - 1u;
+                    z = 0;
+                } else {
+                    y &= (1u << 30) - 1u;
+                    z &= (1u << (3 * (hclen - 10))) - 1u;
                 }
+                uint32_t acc = 0;
+#pragma unroll
+                for (int j = 0; j < 5; j++) acc += s_kt[(y >> (6 * j)) & 63u] + s_kt[(z >> (6 * j)) & 63u];
+                const uint32_t kraft = acc & 0xffffu, nsym = acc >> 16;
                 if (nsym < 2 || kraft == 128u) {
                     const uint32_t k = atomicAdd(&s_n, 1u);
                     if (k < SCAN_LIST) {
