@@ -1535,7 +1535,16 @@ struct VC {
 };
 
 // Full strict verification of one candidate offset (warp-uniform call).
-__device__ __noinline__ bool verify_heavy(FindSmem& S, const Src& src, uint64_t total_bits, uint64_t pos, int lane) {
+// With `next_header`, a trial that meets the end-of-block code also reads the
+// header of the block that must follow (BFINAL is 0 in every candidate):
+// BTYPE 3, HLIT > 286, HDIST > 30 or a stored LEN/NLEN mismatch reject the
+// candidate. The reference's trial stops at the end-of-block code; a false
+// header whose trees reach it within a few symbols then passes (one such
+// offset is in 256 MiB of level-9 text), so the boundary scan, whose
+// survivors only become sub-chunk starts, asks for this check; the
+// reference-exact finder does not.
+__device__ __noinline__ bool verify_heavy(FindSmem& S, const Src& src, uint64_t total_bits, uint64_t pos, int lane,
+                                          bool next_header = false) {
     int ok = 1;
     uint32_t hlit = 0, hdist = 0;
     uint64_t cur = 0;
@@ -1612,6 +1621,20 @@ __device__ __noinline__ bool verify_heavy(FindSmem& S, const Src& src, uint64_t 
             if (sym < 256) continue;
             if (sym == 256) {
                 done = true;
+                if (next_header) {
+                    c.read(1);
+                    const uint32_t bt = c.read(2);
+                    if (bt == 3) {
+                        c.ok = false;
+                    } else if (bt == 2) {
+                        const uint32_t hl = c.read(5) + 257, hd = c.read(5) + 1;
+                        if (hl > 286 || hd > 30) c.ok = false;
+                    } else if (bt == 0) {
+                        c.read((uint32_t)((8 - (c.pos & 7)) & 7));
+                        const uint32_t len = c.read(16), nlen = c.read(16);
+                        if ((len ^ nlen) != 0xffffu) c.ok = false;
+                    }
+                }
                 break;
             }
             if (sym > 285) {
@@ -2053,7 +2076,7 @@ __global__ void __launch_bounds__(128) k_verify_heavy(VerifyArgs A) {
         if (lane == 0) idx = atomicAdd(A.queue, 1u);
         idx = (uint32_t)bcast32((int32_t)idx);
         if (idx >= n) break;
-        const bool ok = verify_heavy(S, s, total_bits, A.cand[idx], lane);
+        const bool ok = verify_heavy(S, s, total_bits, A.cand[idx], lane, true);
         if (lane == 0) A.ok[idx] = ok ? 1 : 0;
         __syncwarp();
     }

@@ -314,3 +314,38 @@ def test_crc_rows_heads_and_tails(emu_decoder_factory):
     for off in (0, 1, 7, 15):
         for n in (0, 1, 15, 16, 17, 511, 512, 513, 4095, 4096 * 8 + 3, 262144, 262144 + 777, 3 << 18):
             assert d.crc32(base + off, n) == zlib.crc32(data[off:off + n].tobytes()), (off, n)
+
+
+# 48 bytes of zlib level-9 output of Zipf text; bit 5 of the first byte starts
+# a dynamic-block header with complete trees whose 7th symbol is the
+# end-of-block code, followed by a header with HDIST = 32. The reference's
+# strict verification (header, trees and a 64-symbol trial that ends at the
+# end-of-block code) accepts the offset.
+FALSE_HEADER = bytes.fromhex(
+    "921ce0e49f5b05344c2376b3d42ffe89cd2c0fbd49bcbd66aeaaa7b142791cfd"
+    "9acd943eaf7ff7676fe9222fc66fa286")
+
+
+def test_false_header_ending_early_is_no_sub_chunk_start(emu_decoder_factory):
+    """A false dynamic header whose trial meets the end-of-block code within 64
+    symbols (planted in a stored block's payload, at the first offset past one
+    sub-chunk size) is rejected by the next-header check of the boundary scan,
+    so no sub-chunk starts there and nothing is redone."""
+    assert oracle.verify_candidate(FALSE_HEADER, 5)  # the reference accepts it
+    text_a = W.zipf_text(8_000, 5)
+    c = zlib.compressobj(9, zlib.DEFLATED, -15, 8)
+    body = c.compress(text_a) + c.flush(zlib.Z_FULL_FLUSH)
+    assert len(body) < 4000
+    pad = 4100 - (len(body) + 5)
+    payload = b"\xff" * pad + FALSE_HEADER + b"\xff" * 16
+    body += bytes([0]) + len(payload).to_bytes(2, "little") + (len(payload) ^ 0xFFFF).to_bytes(2, "little") + payload
+    text_b = W.zipf_text(20_000, 6)
+    c = zlib.compressobj(9, zlib.DEFLATED, -15, 8)
+    body += c.compress(text_b) + c.flush(zlib.Z_FINISH)
+    raw = text_a + payload + text_b
+    gz = W.GZIP_HEADER + body + (zlib.crc32(raw) & 0xFFFFFFFF).to_bytes(4, "little") + len(raw).to_bytes(4, "little")
+    d = emu_decoder_factory(gpu_chunk_bytes=4096)
+    out = []
+    st = d.decode_host(gz, out.append)
+    assert b"".join(out) == raw
+    assert st.speculation_failures == 0
