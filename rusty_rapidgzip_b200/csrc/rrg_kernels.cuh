@@ -53,6 +53,7 @@ constexpr int PRE_BITS = 7;
 constexpr int DIST_BITS = 8;  // inflate's distance LUT; longer codes (~1% of distances) take long_decode
 constexpr int DIST_SIZE = 1 << DIST_BITS;
 constexpr int NB = 32;  // symbols per decode batch
+constexpr int MAT_GROUPS = 4;  // 32-cell groups whose loads a materialisation pass issues together
 
 // ------------------------------------------------------- warp helpers
 __device__ __forceinline__ uint32_t warp_sum(uint32_t v) {
@@ -145,18 +146,23 @@ __device__ __forceinline__ bool br_past_end(const BR& b) { return br_tell_abs(b)
 //   litlen kind: 1 length (value = base), 2 end of block, 3 invalid (286/287)
 //   dist kind:   0 distance (value = base), 3 invalid (30/31)
 //   precode:     value = symbol
-// A litlen literal is 0x80000000 | code length << 8 | byte: the sign bit tells
-// it apart in one test, and masked with 0x800000ff it is the batch entry itself.
+// A litlen literal is 0x80000000 | code length << 12 | code length << 8 | byte:
+// the sign bit tells it apart in one test, and masked with 0x800000ff it is the
+// batch entry itself. pair_literals() turns a literal whose LUT index also
+// holds the whole code of a second literal into a pair: bit 24 set, bits 8-11
+// the two codes' total length, bits 16-23 the second byte (bits 0-7 and 12-15
+// still describe the first literal alone).
 enum { TK_LITLEN = 0, TK_DIST = 1, TK_PRE = 2 };
 constexpr uint32_t LIT_FLAG = 0x80000000u;
+constexpr uint32_t LIT_PAIR = 1u << 24;
 
-__device__ __forceinline__ uint32_t entry_len(uint32_t e) {  // code length of any entry
-    return (int32_t)e < 0 ? (e >> 8) & 15u : e & 15u;
+__device__ __forceinline__ uint32_t entry_len(uint32_t e) {  // code length of any entry (first literal of a pair)
+    return (int32_t)e < 0 ? (e >> 12) & 15u : e & 15u;
 }
 
 __device__ __forceinline__ uint32_t make_entry(int kind, uint32_t sym, uint32_t len) {
     if (kind == TK_LITLEN) {
-        if (sym < 256) return LIT_FLAG | (len << 8) | sym;
+        if (sym < 256) return LIT_FLAG | (len << 12) | (len << 8) | sym;
         if (sym == 256) return (2u << 4) | len;
         if (sym <= 285)
             return ((uint32_t)c_len_base[sym - 257] << 16) | ((uint32_t)c_len_extra[sym - 257] << 8) | (1u << 4) | len;
@@ -231,6 +237,30 @@ __device__ int warp_build(const uint8_t* len, int n, const Table& T, int lut_bit
     }
     __syncwarp();
     return MSG_NONE;
+}
+
+// Two-literal entries for a built litlen LUT of LUT_BITS bits: where the bits
+// after a literal's code (the index shifted by its length) decode to another
+// literal within the LUT's width, one lookup yields both. Entries keep the
+// first literal's byte and length, so the pass reads entries that other lanes
+// may already have paired.
+__device__ void pair_literals(uint32_t* lut, int lane) {
+    for (uint32_t i = lane; i < (uint32_t)LUT_SIZE; i += 32) {
+        const uint32_t e = lut[i];
+        uint32_t ne = e;
+        if ((int32_t)e < 0) {
+            const uint32_t c1 = (e >> 12) & 15u;
+            const uint32_t e2 = lut[i >> c1];
+            if ((int32_t)e2 < 0) {
+                const uint32_t c2 = (e2 >> 12) & 15u;
+                if (c1 + c2 <= (uint32_t)LUT_BITS)
+                    ne = (e & 0x8000f0ffu) | ((c1 + c2) << 8) | ((e2 & 0xffu) << 16) | LIT_PAIR;
+            }
+        }
+        __syncwarp();
+        lut[i] = ne;
+        __syncwarp();
+    }
 }
 
 // Codes longer than the LUT: canonical decode over lengths lut_bits+1..15.
@@ -414,6 +444,7 @@ __device__ void read_dynamic(WarpSmem& S, ItemState& st, int lane) {
     }
     __syncwarp();
     msg = warp_build(S.lengths, (int)hlit, lit_table(S), LUT_BITS, TK_LITLEN, S.run, lane);
+    if (!msg) pair_literals(S.lit_lut, lane);
     if (!msg) msg = warp_build(S.lengths + hlit, (int)hdist, dist_table(S), DIST_BITS, TK_DIST, S.run, lane);
     if (msg) {
         st.status = DS_INVALID;
@@ -503,19 +534,20 @@ __device__ void decode_codes(WarpSmem& S, ItemState& st, CellT* out, int lane) {
                 const uint32_t* wp = base_w + b.nw;
                 uint64_t buf = b.buf;
                 uint32_t bits = b.bits;
-                while (n < NB) {
+                while (n < NB - 1) {  // a pair may add two entries
                     if (bits <= 32) {
                         buf |= (uint64_t)__ldg(wp) << bits;
                         wp++;
                         bits += 32;
                     }
                     uint32_t e = S.lit_lut[(uint32_t)buf & (LUT_SIZE - 1)];
-                    if ((int32_t)e < 0) {  // literal: the entry is the batch entry
+                    if ((int32_t)e < 0) {  // literal (or two): the entry is the batch entry
                         const uint32_t cl = (e >> 8) & 15u;
                         buf >>= cl;
                         bits -= cl;
                         S.ep[n].x = e & 0x800000ffu;
-                        n++;
+                        S.ep[n + 1].x = LIT_FLAG | ((e >> 16) & 0xffu);  // kept only for a pair
+                        n += 1 + ((e >> 24) & 1u);
                         continue;
                     }
                     if (!e) {  // a code longer than the LUT: the checked path takes this symbol
@@ -682,46 +714,67 @@ __device__ void decode_codes(WarpSmem& S, ItemState& st, CellT* out, int lane) {
             // over the warp marks the entries that start inside it, so a lane's
             // entry is (entries started before the group) + (starts at or below
             // the lane) - 1: no search.
+            // A pass covers MAT_GROUPS groups: every cell is first resolved to a
+            // byte, a marker or an output position written by an earlier batch;
+            // the loads of those positions are issued together, then the cells
+            // are stored (a batch never reads its own cells from memory: sources
+            // inside the batch are followed through its entries).
             const uint32_t my_start = lane < n ? S.ep[lane].y : 0xffffffffu;
             uint32_t before = 0;
-            for (uint32_t j0 = 0; j0 < pos; j0 += 32) {
-                const uint32_t j = j0 + lane;
-                const uint32_t rel = my_start - j0;
-                const uint32_t starts = __reduce_or_sync(FULLMASK, rel < 32u ? (1u << rel) : 0u);
-                int k = (int)(before + __popc(starts & (0xffffffffu >> (31 - lane)))) - 1;
-                before += __popc(starts);
-                if (j >= pos) break;  // last group only: no collective follows in this pass
-                uint32_t jj = j, cell = 0;
-                for (;;) {
-                    uint32_t e = S.ep[k].x;
-                    if (e & 0x80000000u) {
-                        cell = e & 0xffu;
+            for (uint32_t p0 = 0; p0 < pos; p0 += 32u * MAT_GROUPS) {
+                uint32_t cell[MAT_GROUPS];
+                int64_t from[MAT_GROUPS];  // >= 0: output position to load
+#pragma unroll
+                for (int g = 0; g < MAT_GROUPS; g++) {
+                    cell[g] = 0;
+                    from[g] = -1;
+                    const uint32_t j0 = p0 + 32u * g;
+                    if (j0 >= pos) continue;  // warp-uniform
+                    const uint32_t j = j0 + lane;
+                    const uint32_t rel = my_start - j0;
+                    const uint32_t starts = __reduce_or_sync(FULLMASK, rel < 32u ? (1u << rel) : 0u);
+                    int k = (int)(before + __popc(starts & (0xffffffffu >> (31 - lane)))) - 1;
+                    before += __popc(starts);
+                    if (j >= pos) continue;
+                    uint32_t jj = j;
+                    for (;;) {
+                        uint32_t e = S.ep[k].x;
+                        if (e & 0x80000000u) {
+                            cell[g] = e & 0xffu;
+                            break;
+                        }
+                        uint32_t d = e >> 9;
+                        const uint32_t ek = S.ep[k].y;
+                        uint32_t t = jj - ek;
+                        if (t >= d) t %= d;
+                        int64_t src = (int64_t)ek - (int64_t)d + (int64_t)t;
+                        if (src >= 0) {
+                            jj = (uint32_t)src;
+                            k = find_entry(S.ep, k, jj);
+                            continue;
+                        }
+                        int64_t a = (int64_t)cur + src;
+                        if (a >= (int64_t)st.member_start) {
+                            from[g] = a;
+                            break;
+                        }
+                        if (st.markers_ok && a < 0) {
+                            cell[g] = MARKER16 | (uint32_t)(-a - 1);
+                            mk++;
+                            break;
+                        }
+                        bad = 1;
                         break;
                     }
-                    uint32_t d = e >> 9;
-                    const uint32_t ek = S.ep[k].y;
-                    uint32_t t = jj - ek;
-                    if (t >= d) t %= d;
-                    int64_t src = (int64_t)ek - (int64_t)d + (int64_t)t;
-                    if (src >= 0) {
-                        jj = (uint32_t)src;
-                        k = find_entry(S.ep, k, jj);
-                        continue;
-                    }
-                    int64_t a = (int64_t)cur + src;
-                    if (a >= (int64_t)st.member_start) {
-                        cell = (uint32_t)out[a];
-                        break;
-                    }
-                    if (st.markers_ok && a < 0) {
-                        cell = MARKER16 | (uint32_t)(-a - 1);
-                        mk++;
-                        break;
-                    }
-                    bad = 1;
-                    break;
                 }
-                out[cur + j] = (CellT)cell;
+#pragma unroll
+                for (int g = 0; g < MAT_GROUPS; g++)
+                    if (from[g] >= 0) cell[g] = (uint32_t)out[from[g]];
+#pragma unroll
+                for (int g = 0; g < MAT_GROUPS; g++) {
+                    const uint32_t j = p0 + 32u * g + lane;
+                    if (j < pos) out[cur + j] = (CellT)cell[g];
+                }
             }
             bad = warp_sum(bad);
             mk = warp_sum(mk);
