@@ -754,6 +754,9 @@ int scan_boundaries(rrg_ctx* c, const uint8_t* body, uint64_t blen, std::vector<
     uint32_t cnt[4] = {0, 0, 0, 0};
     CK(cudaMemcpyAsync(cnt, counts, 16, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    if (c->cfg.verbose >= 2)
+        std::fprintf(stderr, "[rrg-gpu] boundary scan of %llu bytes: %u candidates, %u after the code-length check, "
+                     "%u stored-block starts\n", (unsigned long long)blen, cnt[0], cnt[1], cnt[3]);
     if (cnt[3]) {  // stored-block starts need no verification (the anchored chain checks them)
         const uint32_t ns = std::min(cnt[3], cap3);
         std::vector<uint64_t> st(ns);

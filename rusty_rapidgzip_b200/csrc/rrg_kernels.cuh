@@ -2015,31 +2015,48 @@ struct VerifyArgs {
 
 // strict code-length parse without building tables: litlen and distance Kraft
 // sums are accumulated as the lengths are decoded.
-__device__ bool verify_light(const Src& s, uint64_t total_bits, uint64_t pos) {
+__device__ bool verify_light(const Src& s, uint64_t total_bits, uint64_t pos, uint8_t* lut) {
     VC c{&s, pos, total_bits, true};
     c.read(3);
     const uint32_t hlit = c.read(5) + 257, hdist = c.read(5) + 1, hclen = c.read(4) + 4;
     if (!c.ok || hlit > 286 || hdist > 30) return false;
-    uint8_t cl[19];
-    for (int i = 0; i < 19; i++) cl[i] = 0;
-    for (uint32_t i = 0; i < hclen; i++) cl[c_cl_order[i]] = (uint8_t)c.read(3);
+    // precode lengths, 3 bits per symbol, and the count of each length (5-bit fields)
+    uint64_t cl = 0;
+    for (uint32_t i = 0; i < hclen; i++) cl |= (uint64_t)c.read(3) << (3 * c_cl_order[i]);
     if (!c.ok) return false;
-    uint32_t pc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int i = 0; i < 19; i++) pc[cl[i]]++;
-    pc[0] = 0;
+    uint64_t cnt = 0;
     uint32_t k = 0, ns = 0;
-    for (int l = 1; l < 8; l++) {
-        k += pc[l] << (7 - l);
-        ns += pc[l];
+#pragma unroll
+    for (int i = 0; i < 19; i++) {
+        const uint32_t l = (uint32_t)(cl >> (3 * i)) & 7u;
+        if (l) {
+            cnt += 1ull << (5 * l);
+            k += 128u >> l;
+            ns++;
+        }
     }
     if (ns >= 2 && k != 128u) return false;
-    uint8_t sym[19];
+    // 7-bit decode table: entry = symbol << 3 | length (0 = no code). Canonical
+    // codes (RFC 1951 3.2.2) in symbol order; next codes in 8-bit fields.
+    uint64_t next = 0;
     {
-        uint32_t off[8];
-        off[1] = 0;
-        for (int l = 1; l < 7; l++) off[l + 1] = off[l] + pc[l];
-        for (int i = 0; i < 19; i++)
-            if (cl[i]) sym[off[cl[i]]++] = (uint8_t)i;
+        uint32_t code = 0;
+#pragma unroll
+        for (int l = 1; l <= 7; l++) {
+            code = (code + (l > 1 ? (uint32_t)(cnt >> (5 * (l - 1))) & 31u : 0u)) << 1;
+            next |= (uint64_t)code << (8 * l);
+        }
+    }
+    for (int i = 0; i < 128; i += 16) *reinterpret_cast<uint4*>(lut + i) = make_uint4(0, 0, 0, 0);
+#pragma unroll
+    for (int i = 0; i < 19; i++) {
+        const uint32_t l = (uint32_t)(cl >> (3 * i)) & 7u;
+        if (l) {
+            const uint32_t code = (uint32_t)(next >> (8 * l)) & 0xffu;
+            next += 1ull << (8 * l);
+            const uint32_t rev = __brev(code) >> (32 - l);
+            for (uint32_t x = rev; x < 128u; x += 1u << l) lut[x] = (uint8_t)((i << 3) | l);
+        }
     }
     const uint32_t total = hlit + hdist;
     uint32_t i = 0, prev = 0, len256 = 0;
@@ -2060,29 +2077,15 @@ __device__ bool verify_light(const Src& s, uint64_t total_bits, uint64_t pos) {
     while (i < total) {
         // precode symbol: HuffmanDecoder::decode needs 10 bits available
         if (c.pos + 10 > c.total) return false;
-        const uint32_t bits = peek_at(s, c.pos, 7);
-        int code = 0, first = 0, index = 0, got = -1;
-        uint32_t used = 0;
-        for (int l = 1; l <= 7; l++) {
-            code |= (int)((bits >> (l - 1)) & 1u);
-            const int cnt = (int)pc[l];
-            if (code - cnt < first) {
-                got = sym[index + (code - first)];
-                used = (uint32_t)l;
-                break;
-            }
-            index += cnt;
-            first += cnt;
-            first <<= 1;
-            code <<= 1;
-        }
-        if (got < 0) return false;
+        const uint32_t e = lut[peek_at(s, c.pos, 7)];
+        if (!e) return false;
         // an oversubscribed code stays oversubscribed (the final test needs
         // sums of exactly 2^15): stop at the first symbol that overshoots
         if (kl > 32768u || kd > 32768u) return false;
-        c.pos += used;
+        c.pos += e & 7u;
+        const uint32_t got = e >> 3;
         if (got <= 15) {
-            prev = (uint32_t)got;
+            prev = got;
             put(prev);
         } else if (got == 16) {
             if (i == 0) return false;
@@ -2104,12 +2107,14 @@ __device__ bool verify_light(const Src& s, uint64_t total_bits, uint64_t pos) {
 
 // Survivors are appended to A.out (order is restored on the host).
 __global__ void __launch_bounds__(256) k_verify_light(VerifyArgs A) {
+    __shared__ __align__(16) uint8_t s_lut[256 * 128];  // one precode table per thread
     const Src s = make_src(A.body, A.body_len);
     const uint64_t total_bits = A.body_len * 8;
     const uint32_t n = *A.n_ptr < A.cap ? *A.n_ptr : A.cap;
+    uint8_t* lut = s_lut + threadIdx.x * 128;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint64_t pos = A.cand[i];
-        if (verify_light(s, total_bits, pos)) {
+        if (verify_light(s, total_bits, pos, lut)) {
             const uint32_t slot = atomicAdd(A.n_out, 1u);
             if (slot < A.out_cap) A.out[slot] = pos;
         }

@@ -42,6 +42,7 @@ struct __attribute__((aligned(16))) uint4 {
     unsigned x, y, z, w;
 };
 inline uint2 make_uint2(unsigned x, unsigned y) { return uint2{x, y}; }
+inline uint4 make_uint4(unsigned x, unsigned y, unsigned z, unsigned w) { return uint4{x, y, z, w}; }
 
 typedef int cudaError_t;
 typedef void* cudaStream_t;
