@@ -724,8 +724,22 @@ int scan_boundaries(rrg_ctx* c, const uint8_t* body, uint64_t blen, std::vector<
         LAUNCHED(c);
         return 0;
     };
+    // both verifications of the candidates found so far; the light one starts
+    // after the candidates it has seen (counts[4]), the heavy one's queue
+    // after the survivors it has seen (counts[2])
+    VerifyArgs V{body, blen, cand, counts, cap, surv, counts + 1, cap2, nullptr, nullptr, counts + 4};
+    VerifyArgs H{body, blen, surv, counts + 1, cap2, nullptr, nullptr, 0, (uint8_t*)c->vflag.p, counts + 2, nullptr};
+    const uint32_t W = 4;
+    auto verify = [&]() -> int {
+        RRG_LAUNCH(k_verify_light, c->n_sm * 8, 256, 0, c->stream, V);
+        LAUNCHED(c);
+        RRG_LAUNCH(k_verify_heavy, c->n_sm * 4, W * 32, W * sizeof(FindSmem), c->stream, H);
+        LAUNCHED(c);
+        return 0;
+    };
     // Input still arriving (host path): scan each tile as soon as its bytes,
-    // and the 64 KiB past them that the stored-block check may read, are here.
+    // and the 64 KiB past them that the stored-block check may read, are here,
+    // and verify its candidates (their reads stay inside that margin).
     uint64_t t_done = 0;
     if (c->arr_base && !c->arr_pieces.empty()) {
         const uint8_t* tile0 = (const uint8_t*)((uintptr_t)body & ~(uintptr_t)15);
@@ -734,22 +748,20 @@ int scan_boundaries(rrg_ctx* c, const uint8_t* body, uint64_t blen, std::vector<
             CK(cudaStreamWaitEvent(c->stream, pc.second, 0));
             const uint64_t have = pc.first > skip ? pc.first - skip : 0;
             const uint64_t t_hi = have > 65600 ? std::min(n_tiles, (have - 65600) / tb) : 0;
+            if (t_hi <= t_done) continue;
             int rc0 = scan(t_done, t_hi);
             if (rc0) return rc0;
-            t_done = std::max(t_done, t_hi);
+            t_done = t_hi;
+            if (int rv = verify()) return rv;
+            RRG_LAUNCH(k_verify_mark, 1, 32, 0, c->stream, counts, cap, cap2);
+            LAUNCHED(c);
         }
         c->arr_base = nullptr;  // everything has arrived for the kernels that follow
         c->arr_pieces.clear();
     }
     int rcs = scan(t_done, n_tiles);
     if (rcs) return rcs;
-    VerifyArgs V{body, blen, cand, counts, cap, surv, counts + 1, cap2, nullptr, nullptr};
-    RRG_LAUNCH(k_verify_light, c->n_sm * 8, 256, 0, c->stream, V);
-    LAUNCHED(c);
-    VerifyArgs H{body, blen, surv, counts + 1, cap2, nullptr, nullptr, 0, (uint8_t*)c->vflag.p, counts + 2};
-    const uint32_t W = 4;
-    RRG_LAUNCH(k_verify_heavy, c->n_sm * 4, W * 32, W * sizeof(FindSmem), c->stream, H);
-    LAUNCHED(c);
+    if (int rv = verify()) return rv;
     kt.stop();
     uint32_t cnt[4] = {0, 0, 0, 0};
     CK(cudaMemcpyAsync(cnt, counts, 16, cudaMemcpyDeviceToHost, c->stream));

@@ -2011,6 +2011,7 @@ struct VerifyArgs {
     uint32_t out_cap;
     uint8_t* ok;            // k_verify_heavy: per-survivor verdict
     uint32_t* queue;
+    const uint32_t* lo_ptr;  // k_verify_light: candidates before this index are done (null: none)
 };
 
 // strict code-length parse without building tables: litlen and distance Kraft
@@ -2111,13 +2112,25 @@ __global__ void __launch_bounds__(256) k_verify_light(VerifyArgs A) {
     const Src s = make_src(A.body, A.body_len);
     const uint64_t total_bits = A.body_len * 8;
     const uint32_t n = *A.n_ptr < A.cap ? *A.n_ptr : A.cap;
+    const uint32_t lo = A.lo_ptr ? *A.lo_ptr : 0u;
     uint8_t* lut = s_lut + threadIdx.x * 128;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (uint32_t i = lo + blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint64_t pos = A.cand[i];
         if (verify_light(s, total_bits, pos, lut)) {
             const uint32_t slot = atomicAdd(A.n_out, 1u);
             if (slot < A.out_cap) A.out[slot] = pos;
         }
+    }
+}
+
+// After the verification of one input piece's candidates (host path, input
+// still arriving): the next light launch starts after the candidates seen so
+// far, the next heavy launch's queue after the survivors seen so far.
+// counts: [0] candidates, [1] survivors, [2] heavy queue, [4] light start.
+__global__ void k_verify_mark(uint32_t* counts, uint32_t cap, uint32_t cap2) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        counts[4] = counts[0] < cap ? counts[0] : cap;
+        counts[2] = counts[1] < cap2 ? counts[1] : cap2;
     }
 }
 

@@ -64,7 +64,7 @@ def build_emu_lib() -> str:
                                                                   os.path.join(ROOT, "include", "rrg_gpu.h")]
     if not os.path.exists(EMU_LIB) or any(os.path.getmtime(s) > os.path.getmtime(EMU_LIB) for s in srcs):
         subprocess.check_call([
-            "g++", "-std=c++20", "-O2", "-g", "-x", "c++", "-DRRG_EMU", "-include",
+            "g++", "-std=c++20", "-O2", "-g", "-Werror=return-type", "-x", "c++", "-DRRG_EMU", "-include",
             os.path.join(EMU_DIR, "cuda_emu.h"), "-I", os.path.join(ROOT, "include"), "-I",
             os.path.join(ROOT, "rusty_rapidgzip_b200", "csrc"), "-fPIC", "-shared", "-pthread",
             "-o", EMU_LIB, os.path.join(ROOT, "rusty_rapidgzip_b200", "csrc", "rrg_gpu.cu")])

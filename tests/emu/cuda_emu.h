@@ -269,6 +269,11 @@ inline unsigned __funnelshift_r(unsigned lo, unsigned hi, unsigned sh) {
     sh &= 31;
     return sh ? (lo >> sh) | (hi << (32 - sh)) : lo;
 }
+inline unsigned __funnelshift_lc(unsigned lo, unsigned hi, unsigned sh) {
+    if (sh > 32) sh = 32;
+    const unsigned long long v = ((unsigned long long)hi << 32) | lo;
+    return (unsigned)((v << sh) >> 32);
+}
 inline unsigned __brev(unsigned v) {
     unsigned r = 0;
     for (int i = 0; i < 32; i++) r |= ((v >> i) & 1u) << (31 - i);

@@ -265,7 +265,7 @@ def test_address_sanitizer(tmp_path):
     from conftest import EMU_DIR, ROOT
     lib = str(tmp_path / "librrg_gpu_emu_asan.so")
     subprocess.check_call([
-        "g++", "-std=c++20", "-O1", "-g", "-fsanitize=address", "-fno-omit-frame-pointer", "-x", "c++", "-DRRG_EMU",
+        "g++", "-std=c++20", "-O1", "-g", "-Werror=return-type", "-fsanitize=address", "-fno-omit-frame-pointer", "-x", "c++", "-DRRG_EMU",
         "-DRRG_STRICT_ALLOC", "-include", os.path.join(EMU_DIR, "cuda_emu.h"), "-I", os.path.join(ROOT, "include"),
         "-I", os.path.join(ROOT, "rusty_rapidgzip_b200", "csrc"), "-fPIC", "-shared", "-pthread", "-o", lib,
         os.path.join(ROOT, "rusty_rapidgzip_b200", "csrc", "rrg_gpu.cu")])
