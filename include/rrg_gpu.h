@@ -114,6 +114,23 @@ void rrg_gpu_destroy(rrg_ctx* ctx);
 int rrg_gpu_read_gz(rrg_ctx* ctx, const char* path, rrg_sink_fn sink, void* user,
                     rrg_stats* stats, rrg_error* err);
 
+/* Compressed input for rrg_gpu_read_stream: copy up to `cap` bytes into `buf`
+ * and return the count, 0 at the end of the input, or a negative value on a
+ * read error (the call then returns RRG_ERR_IO). */
+typedef int64_t (*rrg_read_fn)(void* user, uint8_t* buf, size_t cap);
+
+/* Non-seekable input (pipe, stdin, socket): replaces the streaming routes of
+ * read_gz (lib.rs:378-431; streaming.rs:389-614 read_gz_streaming_parallel).
+ * The stream is read forward and decoded in stripes of about `stripe_bytes`
+ * compressed bytes (0: 256 MiB) plus a lookahead; only the open member's last
+ * 32 KiB of output, its running CRC32/length and the unread input carry over
+ * between stripes, so memory is bounded by a few stripes. Output reaches
+ * `sink` in order. rrg_gpu_read_gz takes this route for paths that are not
+ * regular files. Errors, stats and the sink contract are those of
+ * rrg_gpu_read_gz; stats->compressed_bytes counts the bytes read. */
+int rrg_gpu_read_stream(rrg_ctx* ctx, rrg_read_fn read_fn, void* read_user, rrg_sink_fn sink, void* user,
+                        uint64_t stripe_bytes, rrg_stats* stats, rrg_error* err);
+
 /* Same as rrg_gpu_read_gz for a gzip file already in host memory (`data` may be
  * pageable or pinned). Replaces read_gz's mmap'd InputBytes (pipeline.rs:47-50). */
 int rrg_gpu_decode_host(rrg_ctx* ctx, const uint8_t* data, size_t len, rrg_sink_fn sink,

@@ -103,6 +103,7 @@ class _Stats(C.Structure):
 
 
 SINK_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_uint8), C.c_size_t)
+READ_FN = C.CFUNCTYPE(C.c_int64, C.c_void_p, C.POINTER(C.c_uint8), C.c_size_t)
 
 
 # ------------------------------------------------------------------ API types
@@ -242,6 +243,7 @@ def load_library(path: str | None = None):
         L.rrg_gpu_destroy.argtypes = [vp]
         L.rrg_gpu_read_gz.argtypes = [vp, C.c_char_p, SINK_FN, vp, S, E]
         L.rrg_gpu_decode_host.argtypes = [vp, vp, sz, SINK_FN, vp, S, E]
+        L.rrg_gpu_read_stream.argtypes = [vp, READ_FN, vp, SINK_FN, vp, u64, S, E]
         L.rrg_gpu_decode_device.argtypes = [vp, vp, sz, vp, sz, C.POINTER(sz), vp, S, E]
         L.rrg_gpu_decode_batch.argtypes = [vp, vp, C.POINTER(u64), C.POINTER(u64), vp, C.POINTER(u64),
                                            C.POINTER(u64), C.POINTER(u64), C.POINTER(i32), sz, vp, S, E]
@@ -363,6 +365,53 @@ class Decoder:
     def read_gz(self, path, sink) -> DecodeStats:
         """read_gz (lib.rs:366-496) for a file path."""
         return self._run(self._L.rrg_gpu_read_gz, os.fsencode(os.fspath(path)), sink=sink)
+
+    def read_stream(self, source, sink, stripe_bytes: int = 0) -> DecodeStats:
+        """read_gz's non-seekable route (lib.rs:378-431, streaming.rs:389-614):
+        `source` is a binary file object (readinto/read) or a callable
+        taking a byte count and returning bytes (b"" at the end). Decoding
+        runs stripe by stripe as the input is read."""
+        failure = []
+        if hasattr(source, "readinto"):
+            def pull(buf, cap):
+                return source.readinto(memoryview(buf).cast("B")[:cap]) or 0
+        else:
+            reader = source.read if hasattr(source, "read") else source
+
+            def pull(buf, cap):
+                b = reader(cap)
+                C.memmove(buf, b, len(b))
+                return len(b)
+
+        def rcb(_u, p, cap):
+            try:
+                arr = (C.c_uint8 * cap).from_address(C.addressof(p.contents))
+                return int(pull(arr, cap))
+            except BaseException as ex:  # surfaced after the call returns
+                failure.append(ex)
+                return -1
+
+        target = _as_sink(sink)
+
+        def cb(_u, p, n):
+            if target is None:
+                return 0
+            try:
+                r = target(C.string_at(p, n))
+            except SinkClosed:
+                return 1
+            except BaseException as ex:
+                failure.append(ex)
+                return 1
+            return 1 if r is False else 0
+
+        st, e = _Stats(), _Error()
+        self._L.rrg_gpu_read_stream(self._ctx, READ_FN(rcb), None, SINK_FN(cb), None, int(stripe_bytes),
+                                    C.byref(st), C.byref(e))
+        if failure:
+            raise failure[0]
+        _raise(e)
+        return DecodeStats._from(st)
 
     def decode_host(self, data, sink) -> DecodeStats:
         """read_gz over a gzip file already in host memory."""

@@ -86,6 +86,8 @@ struct ResolveChunk {
     uint64_t slot_off;    // first cell in the slot arena
     uint64_t n_cells;
     uint64_t member_start;  // global output byte where the chunk's first member began
+    uint64_t job_out;       // first output byte of the chunk's job: bytes in [member_start, job_out)
+                            // were written by earlier calls (a stripe's prefix) and are read from the output
 };
 
 // A CRC piece: output bytes [start, start+len) all belonging to one member.

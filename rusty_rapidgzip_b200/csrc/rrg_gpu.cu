@@ -240,7 +240,7 @@ struct rrg_ctx {
     // device buffers (grow-only)
     DBuf items, results, order, queue, mbs, mbcount, cells, out, targets, limits, found, next_lut, chunks,
         tiles, rerr, markers, win, cand, ncand, vflag, lane_scratch, crc_table, pieces, piece_crc, mpiece, exp_crc, exp_isize, got_crc, got_len,
-        mstatus, comp;
+        mstatus, comp, pfx;
     // pinned host staging
     uint8_t* h_stage[2] = {nullptr, nullptr};
     size_t h_stage_cap = 0;
@@ -836,11 +836,37 @@ struct MemberJob {
     uint64_t dst_cap = ~0ull; // output bytes available at dst_off (~0: the target grows)
     uint32_t member_base = 0; // index of the first member, for error reports
     double expand = 0;        // output cells per compressed byte to reserve (0: the context's estimate)
+    // A stripe of a non-seekable stream: decoding starts at start_bit (relative
+    // to body_off) inside a member whose earlier bytes have been delivered,
+    // and stops at the first block edge at or after stop_bit. The last
+    // prefix_len of those bytes sit in the target just before dst_off (for
+    // back-references); crc_prev/len_prev are their CRC32 and count.
+    uint64_t start_bit = 0;
+    uint64_t stop_bit = ~0ull;  // ~0: decode to the end of the input
+    uint64_t report_off = 0;    // added to input offsets in error reports (the stripe's place in the stream)
+    uint64_t prefix_len = 0;
+    uint32_t crc_prev = 0;
+    uint64_t len_prev = 0;
     // results
     int rc = 0;
     rrg_error err{};
     Decoded out;
+    uint64_t end_bit = 0;       // where decoding stopped, relative to body_off
+    bool open_member = false;   // stopped inside a member (stripe jobs)
+    uint64_t open_start = 0;    // output offset (from dst_off) where that member's bytes in this stripe begin
+    uint32_t open_crc = 0;      // CRC32 and length of that member so far, earlier stripes included
+    uint64_t open_len = 0;
 };
+
+// CRC32 of A||B from CRC32(A), CRC32(B) and |B| (GF(2) polynomial product
+// with x^(8|B|) from the x^(2^k) table).
+uint32_t host_crc_combine(uint32_t a, uint32_t b, uint64_t len_b) {
+    uint32_t p = 0x80000000u;  // x^0
+    const uint64_t n = len_b;
+    for (int k = 0; k < 61; k++)
+        if ((n >> k) & 1u) p = host_mulmod(p, g_x2k[k + 3]);
+    return host_mulmod(a, p) ^ b;
+}
 
 namespace mr {
 struct Acc {
@@ -879,7 +905,8 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
     const uint64_t slots = inflate_slots(c);
     const uint64_t G = fixed_g ? std::max<uint64_t>(c->gpu_chunk, 4096)
                                : std::max<uint64_t>(g_min, (total_c + slots - 1) / slots);
-    std::vector<std::vector<uint64_t>> starts(nj, std::vector<uint64_t>{0});
+    std::vector<std::vector<uint64_t>> starts(nj);
+    for (size_t i = 0; i < nj; i++) starts[i].push_back(jobs[i].start_bit);
     std::vector<std::vector<uint64_t>> stored_starts(nj);  // sorted, relative to each body
     auto fail = [&](MemberJob& j, int st, int msg, uint64_t where) { j.rc = status_err(&j.err, st, msg, where); };
     // ---- sub-chunk boundaries
@@ -907,16 +934,19 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
                 auto& st = starts[big[q]];
                 for (auto it = std::lower_bound(stored.begin(), stored.end(), b0); it != stored.end() && *it < b1; ++it)
                     stored_starts[big[q]].push_back(*it - b0);  // keeps the empty-block bit
-                auto lo_it = std::lower_bound(verified.begin(), verified.end(), b0);
-                auto hi_it = std::lower_bound(lo_it, verified.end(), b1);
+                // a stripe job splits only its own bit range
+                const uint64_t s0 = b0 + j.start_bit;
+                const uint64_t s1 = j.stop_bit == ~0ull ? b1 : std::min(b1, b0 + j.stop_bit);
+                auto lo_it = std::lower_bound(verified.begin(), verified.end(), s0);
+                auto hi_it = std::lower_bound(lo_it, verified.end(), std::max(s0, s1));
                 if (fixed_g) {
                     for (auto it = lo_it; it != hi_it; ++it)
                         if (*it - b0 >= st.back() + G * 8) st.push_back(*it - b0);
                 } else {
-                    const uint64_t nbits = b1 - b0;
+                    const uint64_t nbits = s1 > s0 ? s1 - s0 : 0;
                     const uint64_t K = std::max<uint64_t>(1, (nbits / 8 + G / 2) / G);
                     for (uint64_t k = 1; k < K; k++) {
-                        const uint64_t ideal = b0 + nbits * k / K;
+                        const uint64_t ideal = s0 + nbits * k / K;
                         auto it = std::lower_bound(lo_it, hi_it, ideal);
                         uint64_t best = ~0ull;
                         if (it != hi_it) best = *it;
@@ -933,9 +963,9 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
         std::vector<size_t> owner;
         for (size_t i = 0; i < nj; i++) {
             const uint64_t base_bit = (jobs[i].file_off + jobs[i].body_off) * 8;
-            const uint64_t total_bits = (jobs[i].len - jobs[i].body_off) * 8;
+            const uint64_t total_bits = std::min((jobs[i].len - jobs[i].body_off) * 8, jobs[i].stop_bit);
             const size_t t0 = targets.size();
-            for (uint64_t t = G * 8; t < total_bits; t += G * 8) {
+            for (uint64_t t = jobs[i].start_bit + G * 8; t < total_bits; t += G * 8) {
                 targets.push_back(base_bit + t);
                 owner.push_back(i);
             }
@@ -974,6 +1004,7 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
         }
     }
     std::vector<JobState> js(nj);
+    for (size_t i = 0; i < nj; i++) js[i].expected = jobs[i].start_bit;
     uint32_t next_id = 0;
     std::unordered_map<uint32_t, std::vector<MemberRec>> by_item;
     auto bucket = [&](const std::vector<MemberRec>& all) {
@@ -1000,7 +1031,7 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
         std::vector<ChunkItem> ditems;
         std::vector<size_t> djob;
         for (size_t i = 0; i < nj && !tgt.grow && !any_split; i++) {
-            if (starts[i].size() != 1) continue;
+            if (starts[i].size() != 1 || jobs[i].start_bit || jobs[i].stop_bit != ~0ull) continue;
             const MemberJob& j = jobs[i];
             direct[i] = 1;
             ChunkItem it{};
@@ -1034,7 +1065,7 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
                             (unsigned long long)r.n_cells);
                     j.rc = RRG_ERR_CAPACITY;
                 } else if (r.status != DS_OK) {
-                    fail(j, r.status, r.msg, j.file_off + j.body_off + r.err_bit / 8);
+                    fail(j, r.status, r.msg, j.report_off + j.file_off + j.body_off + r.err_bit / 8);
                 } else if (!r.final_block) {
                     set_err(&j.err, RRG_ERR_IO, "parallel decode produced no final block");
                     j.rc = RRG_ERR_IO;
@@ -1058,7 +1089,7 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
             it.in_off = j.file_off + j.body_off;
             it.in_len = blen;
             it.start_bit = st[k];
-            it.end_hint = k + 1 < st.size() ? st[k + 1] : ~0ull;
+            it.end_hint = k + 1 < st.size() ? st[k + 1] : j.stop_bit;
             const uint64_t span = ((k + 1 < st.size() ? st[k + 1] : total_bits) - st[k] + 7) / 8;
             it.out_cap = round8((uint64_t)(span * (j.expand > 0 ? j.expand : c->expand)) + 65536);
             it.out_off = arena;
@@ -1098,7 +1129,8 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
             while (!s.done && s.pending < 0) {
                 if (s.final_seen || s.k >= s.n) {
                     s.done = true;
-                    if (!s.final_seen) {
+                    // a stripe job ends at the block edge past its stop bit
+                    if (!s.final_seen && !(j.stop_bit != ~0ull && s.expected >= j.stop_bit)) {
                         set_err(&j.err, RRG_ERR_IO, "parallel decode produced no final block");
                         j.rc = RRG_ERR_IO;
                     }
@@ -1158,7 +1190,7 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
             s.pending = -1;
             const ChunkResult& r = r1[q];
             if (r.status != DS_OK && r.status != DS_OVERFLOW) {
-                fail(j, r.status, r.msg, j.file_off + j.body_off + r.err_bit / 8);
+                fail(j, r.status, r.msg, j.report_off + j.file_off + j.body_off + r.err_bit / 8);
                 s.done = true;
                 continue;
             }
@@ -1219,7 +1251,7 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
                 MemberJob& j = jobs[where[q].first];
                 if (j.rc) continue;
                 if (r2[q].status != DS_OK) {
-                    fail(j, r2[q].status, r2[q].msg, j.file_off + j.body_off + r2[q].err_bit / 8);
+                    fail(j, r2[q].status, r2[q].msg, j.report_off + j.file_off + j.body_off + r2[q].err_bit / 8);
                     continue;
                 }
                 Acc& a = js[where[q].first].acc[where[q].second];
@@ -1238,6 +1270,7 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
         for (const Acc& a : js[i].acc) pos += a.r.n_cells;
         j.out.total = pos;
         j.out.consumed = j.file_off + j.body_off + js[i].expected / 8;
+        j.end_bit = js[i].expected;
         if (j.dst_cap != ~0ull && pos > j.dst_cap) {
             set_err(&j.err, RRG_ERR_CAPACITY, "output buffer too small: need %llu bytes", (unsigned long long)pos);
             j.rc = RRG_ERR_CAPACITY;
@@ -1257,17 +1290,22 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
     std::vector<MemberSpan> spans;
     std::vector<size_t> span_job;
     std::vector<uint32_t> span_member;
+    // 0: a whole member; 1: a member continued from earlier stripes, ended
+    // here; 2: the member a stripe stops in (no trailer yet)
+    std::vector<uint8_t> span_kind;
     for (size_t i = 0; i < nj; i++) {
         MemberJob& j = jobs[i];
         if (j.rc) continue;
         uint64_t pos = 0, mstart = 0;
         uint32_t nm = 0;
+        const bool continued = j.start_bit != 0 || j.len_prev != 0;
         if (direct[i]) {
             for (const MemberRec& m : direct_recs[i]) {
                 spans.push_back(MemberSpan{j.dst_off + mstart, m.cell_off - mstart, m.crc, m.isize,
-                                           j.file_off + j.body_off + m.trailer_byte});
+                                           j.report_off + j.file_off + j.body_off + m.trailer_byte});
                 span_job.push_back(i);
                 span_member.push_back(j.member_base + nm++);
+                span_kind.push_back(0);
                 mstart = m.cell_off;
             }
             j.out.members = nm;
@@ -1275,21 +1313,32 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
         }
         for (const Acc& a : js[i].acc) {
             if (a.r.n_cells) {
-                rchunks.push_back(ResolveChunk{j.dst_off + pos, a.it.out_off, a.r.n_cells, j.dst_off + mstart});
+                // the first member of a stripe began before dst_off: its last
+                // prefix_len bytes there serve the chunk windows
+                const uint64_t ms = (nm == 0 && continued) ? j.dst_off - j.prefix_len : j.dst_off + mstart;
+                rchunks.push_back(ResolveChunk{j.dst_off + pos, a.it.out_off, a.r.n_cells, ms, j.dst_off});
                 chunk_job.push_back(i);
                 tile_start.push_back(tile_start.back() + (a.r.n_cells + RES_TILE - 1) / RES_TILE);
             }
             for (const MemberRec& m : a.m) {
                 const uint64_t end = pos + m.cell_off;
                 spans.push_back(MemberSpan{j.dst_off + mstart, end - mstart, m.crc, m.isize,
-                                           j.file_off + j.body_off + m.trailer_byte});
+                                           j.report_off + j.file_off + j.body_off + m.trailer_byte});
                 span_job.push_back(i);
-                span_member.push_back(j.member_base + nm++);
+                span_member.push_back(j.member_base + nm);
+                span_kind.push_back(nm == 0 && continued ? 1 : 0);
+                nm++;
                 mstart = end;
             }
             pos += a.r.n_cells;
         }
         j.out.members = nm;
+        if (j.stop_bit != ~0ull && !js[i].final_seen) {
+            spans.push_back(MemberSpan{j.dst_off + mstart, pos - mstart, 0, 0, 0});
+            span_job.push_back(i);
+            span_member.push_back(j.member_base + nm);
+            span_kind.push_back(nm == 0 && continued ? 3 : 2);  // 3: also the continued first member
+        }
     }
     // ---- resolve markers + compact; a failing chunk fails its job only
     int64_t bad = -1;
@@ -1311,7 +1360,20 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
     if (rc) return rc;
     for (size_t m = 0; m < spans.size(); m++) {
         MemberJob& j = jobs[span_job[m]];
-        if (j.rc || (stv[m] != DS_CRC && stv[m] != DS_ISIZE)) continue;
+        if (j.rc) continue;
+        if (span_kind[m] >= 2) {  // the member continues in the next stripe
+            j.open_member = true;
+            j.open_start = spans[m].out_start - j.dst_off;
+            j.open_crc = span_kind[m] == 3 ? host_crc_combine(j.crc_prev, got[m], glen[m]) : got[m];
+            j.open_len = (span_kind[m] == 3 ? j.len_prev : 0) + glen[m];
+            continue;
+        }
+        if (span_kind[m] == 1) {  // whole-member check with the earlier stripes' bytes
+            got[m] = host_crc_combine(j.crc_prev, got[m], glen[m]);
+            glen[m] += j.len_prev;
+            stv[m] = got[m] != spans[m].crc ? DS_CRC : (uint32_t)glen[m] != spans[m].isize ? DS_ISIZE : DS_OK;
+        }
+        if (stv[m] != DS_CRC && stv[m] != DS_ISIZE) continue;
         j.rc = member_error(&j.err, spans[m], span_member[m], stv[m], got[m], glen[m]);
     }
     return 0;
@@ -1776,6 +1838,161 @@ int decode_host_impl(rrg_ctx* c, const uint8_t* data, size_t len, rrg_sink_fn si
                      (unsigned long long)c->st.speculation_failures, (unsigned long long)c->st.markers, c->st.finder_ms,
                      c->st.inflate_ms, c->st.resolve_ms, c->st.crc_ms, c->st.total_ms);
     return rc;
+}
+
+// ------------------------------------------------------------ non-seekable input
+// A stream read forward in stripes (streaming.rs:389-614 keeps a sliding read
+// buffer for the same reason). Each stripe is a job of the member route that
+// starts at the exact bit where the previous one stopped and stops at the
+// first block edge past its stop bit, leaving a lookahead of input unread so
+// that the last sub-chunk can finish its block. Between stripes only the open
+// member's last 32 KiB of output (for back-references), its running CRC32 and
+// length, and the unread input survive, so memory stays a few stripes whatever
+// the stream's length.
+int stream_impl(rrg_ctx* c, rrg_read_fn rd, void* ruser, rrg_sink_fn sink, void* suser, uint64_t stripe_bytes,
+                rrg_stats* stats, rrg_error* err) {
+    double t_all = now_ms();
+    c->st = rrg_stats{};
+    c->launches = 0;
+    int rc = upload_tables(c, err);
+    if (rc) return rc;
+    const uint64_t S = stripe_bytes ? std::max<uint64_t>(stripe_bytes, 1 << 16) : (256ull << 20);
+    uint64_t L = std::max<uint64_t>(1ull << 16, S / 8);  // lookahead; doubled when a block outruns it
+    std::vector<uint8_t> hb;
+    uint64_t have = 0, in_base = 0;  // hb[0..have) = stream bytes [in_base, in_base + have)
+    bool eof = false;
+    auto fill = [&](uint64_t want) -> int {
+        if (hb.size() < want) hb.resize(want);
+        while (!eof && have < want) {
+            const int64_t r = rd(ruser, hb.data() + have, (size_t)(want - have));
+            if (r < 0) {
+                set_err(err, RRG_ERR_IO, "io: stream read failed");
+                return RRG_ERR_IO;
+            }
+            if (r == 0) eof = true;
+            else have += (uint64_t)r;
+        }
+        return 0;
+    };
+    constexpr uint64_t PRE = 32768;  // the prefix region in front of every stripe's output
+    bool in_member = false, any = false;
+    uint64_t start_bit = 0, len_prev = 0, prefix_len = 0;
+    uint32_t crc_prev = 0, members = 0;
+    uint64_t total_out = 0;
+    CK(dgrow(c->pfx, PRE));
+    OutTarget tgt{(uint8_t*)c->out.p, c->out.cap, true};
+    rc = ensure_out(c, tgt, PRE + 4096, 0, err);
+    if (rc) return rc;
+    for (;;) {
+        if ((rc = fill(S + L))) return rc;
+        uint64_t body_off = 0;
+        if (!in_member) {
+            if (have == 0 && eof) break;  // end of the stream between members
+            size_t hl = 0;
+            int detail = 0;
+            int st = host_parse_header(hb.data(), have, &hl, &detail);
+            if (st) {
+                if (st == DS_TRUNCATED && !eof) {
+                    if ((rc = fill(have + L))) return rc;
+                    continue;
+                }
+                return status_err(err, st, detail, in_base);
+            }
+            body_off = hl;
+            start_bit = 0;
+            crc_prev = 0;
+            len_prev = 0;
+            prefix_len = 0;
+            in_member = true;
+        }
+        // the stop bit: a lookahead's worth before the end of what has been read
+        uint64_t stop = ~0ull;
+        if (!eof) {
+            const uint64_t lim = have > L ? have - L : 0;
+            if (lim * 8 <= body_off * 8 + start_bit + 8) {  // too little read for a stripe
+                if ((rc = fill(have + S))) return rc;
+                continue;
+            }
+            stop = lim * 8 - body_off * 8;
+        }
+        CK(dgrow(c->comp, have + 16));
+        if (have) CK(cudaMemcpyAsync(c->comp.p, hb.data(), have, cudaMemcpyHostToDevice, c->stream));
+        if (prefix_len)
+            CK(cudaMemcpyAsync(tgt.p + PRE - prefix_len, (const uint8_t*)c->pfx.p + PRE - prefix_len, prefix_len,
+                               cudaMemcpyDeviceToDevice, c->stream));
+        std::vector<MemberJob> jobs(1);
+        MemberJob& j = jobs[0];
+        j.len = have;
+        j.body_off = body_off;
+        j.dst_off = PRE;
+        j.member_base = members;
+        j.start_bit = start_bit;
+        j.stop_bit = stop;
+        j.report_off = in_base;
+        j.prefix_len = prefix_len;
+        j.crc_prev = crc_prev;
+        j.len_prev = len_prev;
+        c->st.compressed_bytes = in_base + have;
+        rc = members_route(c, (const uint8_t*)c->comp.p, jobs, tgt, err);
+        if (rc) return rc;
+        if (j.rc) {
+            // a block that runs past the read input: read more and redo the stripe
+            if (!eof && (j.rc == RRG_ERR_DEFLATE_EOF || j.rc == RRG_ERR_TRUNCATED)) {
+                L *= 2;
+                if ((rc = fill(have + L))) return rc;
+                continue;
+            }
+            if (err) *err = j.err;
+            return j.rc;
+        }
+        any = true;
+        if (c->cfg.verbose >= 2)
+            std::fprintf(stderr, "[rrg-gpu] stripe at stream byte %llu: %llu bytes read, start bit %llu, stop bit %llu, "
+                         "%llu bytes out, %s\n", (unsigned long long)in_base, (unsigned long long)have,
+                         (unsigned long long)start_bit, (unsigned long long)stop, (unsigned long long)j.out.total,
+                         j.open_member ? "member open" : "members closed");
+        bool closed = false;
+        rc = deliver(c, tgt.p + PRE, j.out.total, sink, suser, &closed, err);
+        if (rc) return rc;
+        total_out += j.out.total;
+        members += j.out.members;
+        if (closed) break;  // the sink stopped taking bytes (pipeline.rs:1028-1030)
+        uint64_t used;
+        if (j.open_member) {
+            const uint64_t end_bit = body_off * 8 + j.end_bit;
+            used = end_bit / 8;
+            start_bit = end_bit % 8;
+            crc_prev = j.open_crc;
+            len_prev = j.open_len;
+            // the open member's last bytes: this stripe's output from its start,
+            // after the previous prefix when the member continues it
+            const uint64_t p = std::min<uint64_t>(PRE, len_prev);
+            if (p)
+                CK(cudaMemcpyAsync((uint8_t*)c->pfx.p + PRE - p, tgt.p + PRE + j.out.total - p, p,
+                                   cudaMemcpyDeviceToDevice, c->stream));
+            prefix_len = p;
+        } else {
+            used = j.out.consumed;  // the members ended inside the read input
+            in_member = false;
+        }
+        std::memmove(hb.data(), hb.data() + used, (size_t)(have - used));
+        have -= used;
+        in_base += used;
+        if (!in_member && have == 0 && eof) break;
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    if (!any) {
+        set_err(err, RRG_ERR_TRUNCATED, "truncated gzip stream");
+        if (stats) *stats = c->st;
+        return RRG_ERR_TRUNCATED;
+    }
+    c->st.compressed_bytes = in_base + have;
+    c->st.uncompressed_bytes = total_out;
+    c->st.members = members;
+    c->st.kernel_launches = c->launches;
+    c->st.total_ms = now_ms() - t_all;
+    if (stats) *stats = c->st;
+    return 0;
 }
 
 // ------------------------------------------------------------ batches
@@ -2378,28 +2595,43 @@ int rrg_gpu_read_gz(rrg_ctx* c, const char* path, rrg_sink_fn sink, void* user, 
         close(fd);
         return RRG_ERR_IO;
     }
-    std::vector<uint8_t> data;
-    if (S_ISREG(sb.st_mode)) {
-        data.resize((size_t)sb.st_size);
-        size_t got = 0;
-        while (got < data.size()) {
-            ssize_t r = read(fd, data.data() + got, data.size() - got);
-            if (r <= 0) break;
-            got += (size_t)r;
-        }
-        data.resize(got);
-    } else {
-        // pipes / character devices: read to EOF (lib.rs:383-431 streams these)
-        uint8_t buf[1 << 16];
-        for (;;) {
-            ssize_t r = read(fd, buf, sizeof(buf));
-            if (r <= 0) break;
-            data.insert(data.end(), buf, buf + r);
-        }
+    if (!S_ISREG(sb.st_mode)) {
+        // pipes, sockets, character devices: decoded stripe by stripe as they
+        // are read (lib.rs:378-431 streams these)
+        if (err) std::memset(err, 0, sizeof(*err));
+        auto rd = [](void* u, uint8_t* buf, size_t cap) -> int64_t {
+            for (;;) {
+                const ssize_t r = read(*(int*)u, buf, cap);
+                if (r >= 0 || errno != EINTR) return (int64_t)r;
+            }
+        };
+        const int rc = stream_impl(c, rd, &fd, sink, user, 0, stats, err);
+        close(fd);
+        return rc;
     }
+    std::vector<uint8_t> data((size_t)sb.st_size);
+    size_t got = 0;
+    while (got < data.size()) {
+        ssize_t r = read(fd, data.data() + got, data.size() - got);
+        if (r <= 0) break;
+        got += (size_t)r;
+    }
+    data.resize(got);
     close(fd);
     if (err) std::memset(err, 0, sizeof(*err));
     return decode_host_impl(c, data.data(), data.size(), sink, user, stats, err);
+}
+
+int rrg_gpu_read_stream(rrg_ctx* c, rrg_read_fn read_fn, void* read_user, rrg_sink_fn sink, void* user,
+                        uint64_t stripe_bytes, rrg_stats* stats, rrg_error* err) {
+    rrg_error local_err;
+    if (!err) err = &local_err;
+    std::memset(err, 0, sizeof(*err));
+    if (!c || !read_fn) {
+        set_err(err, RRG_ERR_INVALID_ARGUMENT, "null context or read callback");
+        return RRG_ERR_INVALID_ARGUMENT;
+    }
+    return stream_impl(c, read_fn, read_user, sink, user, stripe_bytes, stats, err);
 }
 
 int rrg_gpu_decode_device(rrg_ctx* c, const uint8_t* d_in, size_t len, uint8_t* d_out, size_t out_cap, size_t* out_len,

@@ -2199,6 +2199,8 @@ __global__ void __launch_bounds__(256) k_win_init(ResolveArgs A) {
         uint32_t w;
         if (ck.out_start + i < (uint64_t)WINDOW || ck.out_start + i - WINDOW < ck.member_start) {
             w = WIN_INVALID;
+        } else if (ck.out_start + i - WINDOW < ck.job_out) {
+            w = WIN_BYTE | A.out[ck.out_start + i - WINDOW];  // a stripe's prefix, written by the previous call
         } else {
             const uint64_t g = ck.out_start + i - WINDOW;  // < out_start of chunk k
             uint32_t j = k;

@@ -1,4 +1,4 @@
-"""Runs the batch, BGZF, member and serving paths of the emulated build under
+"""Runs the batch, BGZF, member, stream and serving paths of the emulated build under
 AddressSanitizer with exact device-buffer sizes (RRG_STRICT_ALLOC), so that an
 index past the end of any device buffer fails here rather than on a GPU.
 Started by test_emu.py::test_address_sanitizer in its own process."""
@@ -22,6 +22,12 @@ for case, data in bgzf_cases().items():
             d.decompress(data)
         except Exception:  # noqa: BLE001 - error cases are expected; only memory safety is checked here
             pass
+import io  # noqa: E402
+
+raw2, gz2 = W.config1(200 << 10, seed=4)
+out = []
+d.read_stream(io.BytesIO(gz2), out.append, stripe_bytes=65536)  # several stripes
+assert b"".join(out) == raw2
 keep = []
 
 

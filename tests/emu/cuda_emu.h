@@ -283,6 +283,10 @@ template <class T>
 inline T __ldg(const T* p) {
     return *p;
 }
+template <typename T>
+inline T __ldcg(const T* p) {
+    return *p;
+}
 inline unsigned atomicAdd(unsigned* p, unsigned v) { return __atomic_fetch_add(p, v, __ATOMIC_SEQ_CST); }
 inline unsigned long long atomicAdd(unsigned long long* p, unsigned long long v) {
     return __atomic_fetch_add(p, v, __ATOMIC_SEQ_CST);

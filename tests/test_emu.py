@@ -257,7 +257,7 @@ def test_stored_block_chunks(emu_decoder_factory):
 
 
 def test_address_sanitizer(tmp_path):
-    """Batch, BGZF, member and serving paths of the emulated build with exact
+    """Batch, BGZF, member, stream and serving paths of the emulated build with exact
     device-buffer sizes under AddressSanitizer: any index past the end of a
     device buffer fails here instead of on a GPU."""
     import subprocess
@@ -349,3 +349,69 @@ def test_false_header_ending_early_is_no_sub_chunk_start(emu_decoder_factory):
     st = d.decode_host(gz, out.append)
     assert b"".join(out) == raw
     assert st.speculation_failures == 0
+
+
+def stream_cases():
+    """(name, gzip bytes): one member over many stripes, members with stored
+    blocks and an empty member, a member whose CRC32 is wrong, a truncated one."""
+    raw, gz = W.config1(600 << 10, seed=3)
+    rnd = np.random.default_rng(8).integers(0, 256, 150_000, dtype=np.uint8).tobytes()
+    parts = [raw[:100_000], rnd, raw[100_000:300_000], b"", raw[300_000:]]
+    multi = b"".join(W.gzip_member(p, 6) for p in parts)
+    bad = bytearray(gz)
+    bad[-8] ^= 0x40
+    return [("one-member", gz), ("members", multi), ("crc", bytes(bad)), ("truncated", gz[:150_000])]
+
+
+@pytest.mark.parametrize("case", [c[0] for c in stream_cases()])
+def test_read_stream_stripes(emu_decoder_factory, case):
+    """Non-seekable input decoded in 64 KiB stripes: the output, the member
+    count and every error (code, member, trailer byte) are the oracle's."""
+    import io
+    data = dict(stream_cases())[case]
+    d = emu_decoder_factory(gpu_chunk_bytes=8192)
+    out = []
+    try:
+        want = oracle.read_gz(data, 2)
+    except oracle.OracleError as oe:
+        from rusty_rapidgzip_b200 import RrgError
+        with pytest.raises(RrgError) as ge:
+            d.read_stream(io.BytesIO(data), out.append, stripe_bytes=65536)
+        assert ge.value.code == oe.code
+        if oe.code in (6, 7):  # CrcMismatch / IsizeMismatch carry the member and its trailer's offset
+            assert (ge.value.member, ge.value.trailer_byte) == (oe.member, oe.trailer_byte)
+        return
+    st = d.read_stream(io.BytesIO(data), out.append, stripe_bytes=65536)
+    assert b"".join(out) == want
+    assert st.compressed_bytes == len(data) and st.uncompressed_bytes == len(want)
+
+
+def test_read_gz_from_a_pipe(emu_decoder_factory, tmp_path):
+    """read_gz on a named pipe takes the stripe route; a sink that closes early
+    ends the call without an error."""
+    import threading
+    raw, gz = W.config1(300 << 10, seed=9)
+    fifo = str(tmp_path / "in.gz")
+    os.mkfifo(fifo)
+
+    def writer():
+        with open(fifo, "wb") as f:
+            f.write(gz)
+
+    t = threading.Thread(target=writer)
+    t.start()
+    d = emu_decoder_factory(gpu_chunk_bytes=8192)
+    out = []
+    st = d.read_gz(fifo, out.append)
+    t.join()
+    assert b"".join(out) == raw and st.compressed_bytes == len(gz)
+    import io
+    from rusty_rapidgzip_b200 import SinkClosed
+
+    def first_only(b):
+        out2.append(b)
+        raise SinkClosed
+
+    out2 = []
+    d.read_stream(io.BytesIO(gz), first_only, stripe_bytes=65536)
+    assert len(out2) == 1 and raw.startswith(out2[0])

@@ -417,3 +417,68 @@ def test_serving_alone_and_in_the_mix(gpu_decoder_factory):
     assert st["completed"] == len(reqs) and d.pending() == 0
     assert st["max_batch"] >= 2 and st["max_engines_busy"] == 2
     assert st["peak_in_use_bytes"] > 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("stripe", [4 << 20, 0], ids=["4MiB-stripes", "default-stripes"])
+def test_read_stream_gpu(gpu_decoder_factory, stripe):
+    """A 64 MiB Zipf member and a multi-member stream read forward stripe by
+    stripe: bytes equal the generator's, counts equal the input's."""
+    import io
+    raw, gz = W.config1(64 << 20, seed=11)
+    d = gpu_decoder_factory()
+    h, n = hashlib.sha256(), [0]
+
+    def sink(b):
+        h.update(b)
+        n[0] += len(b)
+
+    st = d.read_stream(io.BytesIO(gz), sink, stripe_bytes=stripe)
+    assert n[0] == len(raw) and h.digest() == hashlib.sha256(raw).digest()
+    assert st.compressed_bytes == len(gz) and st.speculation_failures == 0
+    rnd = np.random.default_rng(12).integers(0, 256, 3 << 20, dtype=np.uint8).tobytes()
+    parts = [raw[: 20 << 20], rnd, b"", raw[20 << 20:]]
+    multi = b"".join(W.gzip_member(p, 6) for p in parts)
+    out = []
+    st = d.read_stream(io.BytesIO(multi), out.append, stripe_bytes=stripe)
+    assert b"".join(out) == b"".join(parts) and st.members == 4
+
+
+@pytest.mark.gpu
+def test_read_stream_gpu_errors(gpu_decoder_factory):
+    """A CRC32 error in a member spanning stripes and a truncated stream give
+    the oracle's error (code; member and trailer offset for CRC32)."""
+    import io
+    from rusty_rapidgzip_b200 import RrgError
+    raw, gz = W.config1(8 << 20, seed=13)
+    bad = bytearray(gz)
+    bad[-8] ^= 1
+    d = gpu_decoder_factory()
+    for data in (bytes(bad), gz[: len(gz) // 2]):
+        with pytest.raises(oracle.OracleError) as oe:
+            oracle.read_gz(data, 4)
+        with pytest.raises(RrgError) as ge:
+            d.read_stream(io.BytesIO(data), None, stripe_bytes=1 << 20)
+        assert ge.value.code == oe.value.code
+        if oe.value.code == 6:
+            assert (ge.value.member, ge.value.trailer_byte) == (oe.value.member, oe.value.trailer_byte)
+
+
+@pytest.mark.gpu
+def test_read_gz_pipe_gpu(gpu_decoder_factory, tmp_path):
+    """read_gz on a named pipe decodes through the stripe route."""
+    import threading
+    raw, gz = W.config0(32 << 20, seed=14)
+    fifo = str(tmp_path / "in.gz")
+    os.mkfifo(fifo)
+
+    def writer():
+        with open(fifo, "wb") as f:
+            f.write(gz)
+
+    t = threading.Thread(target=writer)
+    t.start()
+    out = []
+    st = gpu_decoder_factory().read_gz(fifo, out.append)
+    t.join()
+    assert b"".join(out) == raw and st.compressed_bytes == len(gz)
