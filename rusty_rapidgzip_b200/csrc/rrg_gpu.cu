@@ -1858,13 +1858,21 @@ int stream_impl(rrg_ctx* c, rrg_read_fn rd, void* ruser, rrg_sink_fn sink, void*
     if (rc) return rc;
     const uint64_t S = stripe_bytes ? std::max<uint64_t>(stripe_bytes, 1 << 16) : (256ull << 20);
     uint64_t L = std::max<uint64_t>(1ull << 16, S / 8);  // lookahead; doubled when a block outruns it
-    std::vector<uint8_t> hb;
-    uint64_t have = 0, in_base = 0;  // hb[0..have) = stream bytes [in_base, in_base + have)
+    // the read buffer is pinned (c->h_in), so each stripe's copy runs at link speed
+    uint64_t have = 0, in_base = 0;  // h_in[0..have) = stream bytes [in_base, in_base + have)
     bool eof = false;
     auto fill = [&](uint64_t want) -> int {
-        if (hb.size() < want) hb.resize(want);
+        if (c->h_in_cap < want) {
+            uint8_t* nb = nullptr;
+            const size_t cap = (size_t)want;
+            CK(cudaMallocHost((void**)&nb, cap));
+            if (have) std::memcpy(nb, c->h_in, (size_t)have);
+            if (c->h_in) cudaFreeHost(c->h_in);
+            c->h_in = nb;
+            c->h_in_cap = cap;
+        }
         while (!eof && have < want) {
-            const int64_t r = rd(ruser, hb.data() + have, (size_t)(want - have));
+            const int64_t r = rd(ruser, c->h_in + have, (size_t)(want - have));
             if (r < 0) {
                 set_err(err, RRG_ERR_IO, "io: stream read failed");
                 return RRG_ERR_IO;
@@ -1890,7 +1898,7 @@ int stream_impl(rrg_ctx* c, rrg_read_fn rd, void* ruser, rrg_sink_fn sink, void*
             if (have == 0 && eof) break;  // end of the stream between members
             size_t hl = 0;
             int detail = 0;
-            int st = host_parse_header(hb.data(), have, &hl, &detail);
+            int st = host_parse_header(c->h_in, have, &hl, &detail);
             if (st) {
                 if (st == DS_TRUNCATED && !eof) {
                     if ((rc = fill(have + L))) return rc;
@@ -1916,7 +1924,7 @@ int stream_impl(rrg_ctx* c, rrg_read_fn rd, void* ruser, rrg_sink_fn sink, void*
             stop = lim * 8 - body_off * 8;
         }
         CK(dgrow(c->comp, have + 16));
-        if (have) CK(cudaMemcpyAsync(c->comp.p, hb.data(), have, cudaMemcpyHostToDevice, c->stream));
+        if (have) CK(cudaMemcpyAsync(c->comp.p, c->h_in, have, cudaMemcpyHostToDevice, c->stream));
         if (prefix_len)
             CK(cudaMemcpyAsync(tgt.p + PRE - prefix_len, (const uint8_t*)c->pfx.p + PRE - prefix_len, prefix_len,
                                cudaMemcpyDeviceToDevice, c->stream));
@@ -1975,7 +1983,8 @@ int stream_impl(rrg_ctx* c, rrg_read_fn rd, void* ruser, rrg_sink_fn sink, void*
             used = j.out.consumed;  // the members ended inside the read input
             in_member = false;
         }
-        std::memmove(hb.data(), hb.data() + used, (size_t)(have - used));
+        CK(cudaStreamSynchronize(c->stream));  // the copy out of h_in has finished
+        std::memmove(c->h_in, c->h_in + used, (size_t)(have - used));
         have -= used;
         in_base += used;
         if (!in_member && have == 0 && eof) break;
@@ -2558,6 +2567,7 @@ void rrg_gpu_destroy(rrg_ctx* c) {
     for (auto& p : c->h_stage)
         if (p) cudaFreeHost(p);
     if (c->h_bg) cudaFreeHost(c->h_bg);
+    if (c->h_in) cudaFreeHost(c->h_in);
     for (cudaEvent_t e : c->arr_events)
         if (e) cudaEventDestroy(e);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
