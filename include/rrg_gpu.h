@@ -131,6 +131,30 @@ typedef int64_t (*rrg_read_fn)(void* user, uint8_t* buf, size_t cap);
 int rrg_gpu_read_stream(rrg_ctx* ctx, rrg_read_fn read_fn, void* read_user, rrg_sink_fn sink, void* user,
                         uint64_t stripe_bytes, rrg_stats* stats, rrg_error* err);
 
+/* Seek index of a member stream (the reference has none; README.md:45 lists
+ * random access as absent). rrg_gpu_index_build decodes the file once (CRC32
+ * and ISIZE checked) and keeps block starts at least `spacing` output bytes
+ * apart (0: 4 MiB), each with the 32 KiB of output before it. BGZF files are
+ * refused (RRG_ERR_INVALID_ARGUMENT): each member is already a seek point. */
+typedef struct rrg_index rrg_index;
+int rrg_gpu_index_build(rrg_ctx* ctx, const uint8_t* data, size_t len, uint64_t spacing, rrg_index** out,
+                        rrg_stats* stats, rrg_error* err);
+/* Output bytes [off, off + n) of the file the index was built on (`data`,
+ * `len`: the same file in host memory) into host `dst`. Decodes from the
+ * checkpoint at or before `off` to the first at or past `off + n`, in
+ * parallel like any stripe. Members are decoded only in part, so CRC32/ISIZE
+ * are not checked here. */
+int rrg_gpu_read_range(rrg_ctx* ctx, const uint8_t* data, size_t len, const rrg_index* idx, uint64_t off,
+                       uint64_t n, uint8_t* dst, rrg_error* err);
+uint64_t rrg_index_total_out(const rrg_index* idx);  /* decompressed size of the file */
+size_t rrg_index_count(const rrg_index* idx);        /* checkpoints */
+/* Checkpoint k: its output offset and the file-absolute bit where its block starts. */
+int rrg_index_point(const rrg_index* idx, size_t k, uint64_t* out_off, uint64_t* in_bit);
+/* Byte image of the index: returns the size needed; writes it when `cap` suffices. */
+size_t rrg_index_serialize(const rrg_index* idx, uint8_t* buf, size_t cap);
+rrg_index* rrg_index_deserialize(const uint8_t* buf, size_t n, rrg_error* err);
+void rrg_index_free(rrg_index* idx);
+
 /* Same as rrg_gpu_read_gz for a gzip file already in host memory (`data` may be
  * pageable or pinned). Replaces read_gz's mmap'd InputBytes (pipeline.rs:47-50). */
 int rrg_gpu_decode_host(rrg_ctx* ctx, const uint8_t* data, size_t len, rrg_sink_fn sink,

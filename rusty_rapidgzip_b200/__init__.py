@@ -15,6 +15,7 @@ from ._abi import (  # noqa: F401
     GzipError,
     IoError,
     RrgError,
+    SeekIndex,
     SinkClosed,
     decompress,
     kernel_launch_count,
@@ -25,6 +26,6 @@ from ._abi import (  # noqa: F401
 
 __all__ = [
     "CapacityError", "Config", "DecodeStats", "Decoder", "DeflateError", "DeviceError", "GzipError",
-    "IoError", "RrgError", "SinkClosed", "decompress", "kernel_launch_count", "library_path",
+    "IoError", "RrgError", "SeekIndex", "SinkClosed", "decompress", "kernel_launch_count", "library_path",
     "load_library", "read_gz",
 ]

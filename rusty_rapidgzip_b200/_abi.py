@@ -244,6 +244,19 @@ def load_library(path: str | None = None):
         L.rrg_gpu_read_gz.argtypes = [vp, C.c_char_p, SINK_FN, vp, S, E]
         L.rrg_gpu_decode_host.argtypes = [vp, vp, sz, SINK_FN, vp, S, E]
         L.rrg_gpu_read_stream.argtypes = [vp, READ_FN, vp, SINK_FN, vp, u64, S, E]
+        L.rrg_gpu_index_build.argtypes = [vp, vp, sz, u64, C.POINTER(vp), S, E]
+        L.rrg_gpu_read_range.argtypes = [vp, vp, sz, vp, u64, u64, vp, E]
+        L.rrg_index_total_out.argtypes = [vp]
+        L.rrg_index_total_out.restype = u64
+        L.rrg_index_count.argtypes = [vp]
+        L.rrg_index_count.restype = sz
+        L.rrg_index_point.argtypes = [vp, sz, C.POINTER(u64), C.POINTER(u64)]
+        L.rrg_index_serialize.argtypes = [vp, vp, sz]
+        L.rrg_index_serialize.restype = sz
+        L.rrg_index_deserialize.argtypes = [vp, sz, E]
+        L.rrg_index_deserialize.restype = vp
+        L.rrg_index_free.argtypes = [vp]
+        L.rrg_index_free.restype = None
         L.rrg_gpu_decode_device.argtypes = [vp, vp, sz, vp, sz, C.POINTER(sz), vp, S, E]
         L.rrg_gpu_decode_batch.argtypes = [vp, vp, C.POINTER(u64), C.POINTER(u64), vp, C.POINTER(u64),
                                            C.POINTER(u64), C.POINTER(u64), C.POINTER(i32), sz, vp, S, E]
@@ -304,6 +317,51 @@ def _as_sink(sink):
         if hasattr(sink, m):
             return getattr(sink, m)
     raise TypeError("sink must be callable or have send()/put()")
+
+
+class SeekIndex:
+    """Checkpoints of one member stream for random access (rrg_index)."""
+
+    def __init__(self, lib, ptr: int):
+        self._L, self._p = lib, ptr
+
+    @classmethod
+    def load(cls, blob: bytes, lib: str | None = None) -> "SeekIndex":
+        L = load_library(lib)
+        e = _Error()
+        p = L.rrg_index_deserialize(blob, len(blob), C.byref(e))
+        _raise(e)
+        return cls(L, p)
+
+    @property
+    def total_out(self) -> int:
+        return int(self._L.rrg_index_total_out(self._p))
+
+    def points(self) -> list[tuple[int, int]]:
+        """(output offset, file-absolute bit) of every checkpoint."""
+        pts = []
+        for k in range(int(self._L.rrg_index_count(self._p))):
+            o, b = C.c_uint64(), C.c_uint64()
+            self._L.rrg_index_point(self._p, k, C.byref(o), C.byref(b))
+            pts.append((o.value, b.value))
+        return pts
+
+    def serialize(self) -> bytes:
+        n = self._L.rrg_index_serialize(self._p, None, 0)
+        buf = (C.c_char * n)()
+        self._L.rrg_index_serialize(self._p, C.addressof(buf), n)
+        return buf.raw
+
+    def close(self):
+        if self._p:
+            self._L.rrg_index_free(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Decoder:
@@ -412,6 +470,27 @@ class Decoder:
             raise failure[0]
         _raise(e)
         return DecodeStats._from(st)
+
+    def build_index(self, data, spacing: int = 0) -> "SeekIndex":
+        """Seek index of a member stream in host memory (no reference
+        counterpart): checkpoints at least `spacing` output bytes apart (0:
+        4 MiB) with their 32 KiB windows, from one CRC-checked decode."""
+        addr, n, keep = _host_buffer(data)
+        out, st, e = C.c_void_p(), _Stats(), _Error()
+        self._L.rrg_gpu_index_build(self._ctx, addr, n, int(spacing), C.byref(out), C.byref(st), C.byref(e))
+        del keep
+        _raise(e)
+        return SeekIndex(self._L, out.value)
+
+    def read_range(self, data, index: "SeekIndex", off: int, n: int) -> bytes:
+        """Output bytes [off, off + n) of `data` (the file `index` was built on)."""
+        addr, ln, keep = _host_buffer(data)
+        dst = (C.c_char * max(n, 1))()
+        e = _Error()
+        self._L.rrg_gpu_read_range(self._ctx, addr, ln, index._p, int(off), int(n), C.addressof(dst), C.byref(e))
+        del keep
+        _raise(e)
+        return dst.raw[:n]
 
     def decode_host(self, data, sink) -> DecodeStats:
         """read_gz over a gzip file already in host memory."""

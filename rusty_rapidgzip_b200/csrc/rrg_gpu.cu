@@ -844,6 +844,10 @@ struct MemberJob {
     uint64_t start_bit = 0;
     uint64_t stop_bit = ~0ull;  // ~0: decode to the end of the input
     uint64_t report_off = 0;    // added to input offsets in error reports (the stripe's place in the stream)
+    bool check_crc = true;      // false: a range read from a seek point (members are only partly decoded)
+    // when set: every sub-chunk start the chain kept, as (bit relative to
+    // body_off, output offset relative to dst_off), for a seek index
+    std::vector<std::pair<uint64_t, uint64_t>>* capture = nullptr;
     uint64_t prefix_len = 0;
     uint32_t crc_prev = 0;
     uint64_t len_prev = 0;
@@ -1284,6 +1288,20 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
         rc = ensure_out(c, tgt, grow_need, keep == ~0ull ? 0 : keep, err);
         if (rc) return rc;
     }
+    for (size_t i = 0; i < nj; i++) {
+        MemberJob& j = jobs[i];
+        if (j.rc || !j.capture) continue;
+        j.capture->clear();
+        if (direct[i]) {
+            j.capture->push_back({j.start_bit, 0});
+            continue;
+        }
+        uint64_t pos = 0;
+        for (const Acc& a : js[i].acc) {
+            j.capture->push_back({a.it.start_bit, pos});
+            pos += a.r.n_cells;
+        }
+    }
     std::vector<ResolveChunk> rchunks;
     std::vector<size_t> chunk_job;
     std::vector<uint64_t> tile_start{0};
@@ -1360,7 +1378,7 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
     if (rc) return rc;
     for (size_t m = 0; m < spans.size(); m++) {
         MemberJob& j = jobs[span_job[m]];
-        if (j.rc) continue;
+        if (j.rc || !j.check_crc) continue;
         if (span_kind[m] >= 2) {  // the member continues in the next stripe
             j.open_member = true;
             j.open_start = spans[m].out_start - j.dst_off;
@@ -2004,6 +2022,148 @@ int stream_impl(rrg_ctx* c, rrg_read_fn rd, void* ruser, rrg_sink_fn sink, void*
     return 0;
 }
 
+// ------------------------------------------------------------ seek index
+// Random access into a member stream (the reference has none: README.md:45).
+// A full, CRC-checked decode records the sub-chunk starts the anchored chain
+// kept: each is a block start with its exact bit and output offset. Kept at
+// least `spacing` output bytes apart, each checkpoint stores the 32 KiB of
+// output before it. A range read is then a stripe job (the same machinery as
+// the stream route) from the checkpoint at or before the range, with that
+// window as its prefix, to the first checkpoint at or past the range's end.
+}  // namespace
+
+struct rrg_index {
+    uint64_t file_len = 0, body_off = 0, total_out = 0;
+    std::vector<uint64_t> in_bit;    // relative to body_off
+    std::vector<uint64_t> out_off;   // output offset of the checkpoint
+    std::vector<uint32_t> win_len;   // bytes of window before it (<= 32768)
+    std::vector<uint8_t> win;        // 32768 bytes per checkpoint, right-aligned
+};
+
+namespace {
+int index_build_impl(rrg_ctx* c, const uint8_t* data, size_t len, uint64_t spacing, rrg_index** out,
+                     rrg_stats* stats, rrg_error* err) {
+    double t_all = now_ms();
+    c->st = rrg_stats{};
+    c->launches = 0;
+    c->st.compressed_bytes = len;
+    int rc = upload_tables(c, err);
+    if (rc) return rc;
+    size_t hl = 0;
+    int detail = 0;
+    int st = host_parse_header(data, len, &hl, &detail);
+    if (st) return status_err(err, st, detail, 0);
+    if (host_bgzf_size(data, len) >= 0) {
+        set_err(err, RRG_ERR_INVALID_ARGUMENT, "BGZF: every member already starts a seekable block");
+        return RRG_ERR_INVALID_ARGUMENT;
+    }
+    CK(dgrow(c->comp, len + 16));
+    CK(cudaMemcpyAsync(c->comp.p, data, len, cudaMemcpyHostToDevice, c->stream));
+    std::vector<std::pair<uint64_t, uint64_t>> cps;
+    std::vector<MemberJob> jobs(1);
+    jobs[0].len = len;
+    jobs[0].body_off = hl;
+    jobs[0].capture = &cps;
+    OutTarget tgt{(uint8_t*)c->out.p, c->out.cap, true};
+    rc = members_route(c, (const uint8_t*)c->comp.p, jobs, tgt, err);
+    if (rc) return rc;
+    if (jobs[0].rc) {
+        if (err) *err = jobs[0].err;
+        return jobs[0].rc;
+    }
+    auto* idx = new rrg_index;
+    idx->file_len = len;
+    idx->body_off = hl;
+    idx->total_out = jobs[0].out.total;
+    constexpr uint64_t W = 32768;
+    for (const auto& cp : cps) {
+        if (!idx->out_off.empty() && cp.second < idx->out_off.back() + spacing) continue;
+        idx->in_bit.push_back(cp.first);
+        idx->out_off.push_back(cp.second);
+        idx->win_len.push_back((uint32_t)std::min(W, cp.second));
+    }
+    idx->win.assign(idx->out_off.size() * W, 0);
+    for (size_t k = 0; k < idx->out_off.size(); k++) {
+        const uint64_t wl = idx->win_len[k];
+        if (wl) {
+            cudaError_t e = cudaMemcpyAsync(idx->win.data() + k * W + (W - wl), tgt.p + idx->out_off[k] - wl, wl,
+                                            cudaMemcpyDeviceToHost, c->stream);
+            if (e != cudaSuccess) {
+                delete idx;
+                return cuda_fail(err, e, "index windows");
+            }
+        }
+    }
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+        delete idx;
+        return cuda_fail(err, e, "index windows");
+    }
+    c->st.uncompressed_bytes = idx->total_out;
+    c->st.kernel_launches = c->launches;
+    c->st.total_ms = now_ms() - t_all;
+    if (stats) *stats = c->st;
+    *out = idx;
+    return 0;
+}
+
+int read_range_impl(rrg_ctx* c, const uint8_t* data, size_t len, const rrg_index* idx, uint64_t off, uint64_t n,
+                    uint8_t* dst, rrg_error* err) {
+    if (len != idx->file_len || off > idx->total_out || n > idx->total_out - off || idx->out_off.empty()) {
+        set_err(err, RRG_ERR_INVALID_ARGUMENT, "range or file does not match the index");
+        return RRG_ERR_INVALID_ARGUMENT;
+    }
+    if (!n) return 0;
+    int rc = upload_tables(c, err);
+    if (rc) return rc;
+    // checkpoints around [off, off + n)
+    const auto& oo = idx->out_off;
+    const size_t lo = (size_t)(std::upper_bound(oo.begin(), oo.end(), off) - oo.begin()) - 1;
+    const size_t hi = (size_t)(std::lower_bound(oo.begin(), oo.end(), off + n) - oo.begin());
+    const uint64_t bit0 = idx->body_off * 8 + idx->in_bit[lo];
+    const uint64_t byte0 = bit0 / 8;
+    // input from the first checkpoint's byte to the last one's, plus room for
+    // the bit reader's read-ahead (or to the end of the file)
+    const uint64_t end_byte =
+        hi < oo.size() ? std::min<uint64_t>(len, (idx->body_off * 8 + idx->in_bit[hi]) / 8 + (64u << 10)) : len;
+    const uint64_t clen = end_byte - byte0;
+    CK(dgrow(c->comp, clen + 16));
+    CK(cudaMemcpyAsync(c->comp.p, data + byte0, clen, cudaMemcpyHostToDevice, c->stream));
+    constexpr uint64_t W = 32768;
+    const uint64_t wl = idx->win_len[lo];
+    OutTarget tgt{(uint8_t*)c->out.p, c->out.cap, true};
+    rc = ensure_out(c, tgt, W + 4096, 0, err);
+    if (rc) return rc;
+    if (wl)
+        CK(cudaMemcpyAsync(tgt.p + W - wl, idx->win.data() + lo * W + (W - wl), wl, cudaMemcpyHostToDevice,
+                           c->stream));
+    std::vector<MemberJob> jobs(1);
+    MemberJob& j = jobs[0];
+    j.len = clen;
+    j.body_off = 0;
+    j.start_bit = bit0 - byte0 * 8;
+    j.stop_bit = hi < oo.size() ? idx->body_off * 8 + idx->in_bit[hi] - byte0 * 8 : ~0ull;
+    j.dst_off = W;
+    j.prefix_len = wl;
+    j.len_prev = wl;  // decoding continues a member (its CRC is not checked)
+    j.check_crc = false;
+    j.report_off = byte0;
+    rc = members_route(c, (const uint8_t*)c->comp.p, jobs, tgt, err);
+    if (rc) return rc;
+    if (j.rc) {
+        if (err) *err = j.err;
+        return j.rc;
+    }
+    const uint64_t skip = off - oo[lo];
+    if (skip + n > j.out.total) {
+        set_err(err, RRG_ERR_DEFLATE_INVALID, "seek point decode ended early");
+        return RRG_ERR_DEFLATE_INVALID;
+    }
+    CK(cudaMemcpyAsync(dst, tgt.p + W + skip, n, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
 // ------------------------------------------------------------ batches
 // Independent gzip files (or members) already on the device, each with its
 // own output range. Headers are parsed on the device; BGZF files take the
@@ -2631,6 +2791,117 @@ int rrg_gpu_read_gz(rrg_ctx* c, const char* path, rrg_sink_fn sink, void* user, 
     if (err) std::memset(err, 0, sizeof(*err));
     return decode_host_impl(c, data.data(), data.size(), sink, user, stats, err);
 }
+
+int rrg_gpu_index_build(rrg_ctx* c, const uint8_t* data, size_t len, uint64_t spacing, rrg_index** out,
+                        rrg_stats* stats, rrg_error* err) {
+    rrg_error local_err;
+    if (!err) err = &local_err;
+    std::memset(err, 0, sizeof(*err));
+    if (!c || !data || !out) {
+        set_err(err, RRG_ERR_INVALID_ARGUMENT, "null context, data or index pointer");
+        return RRG_ERR_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    if (len == 0) {
+        set_err(err, RRG_ERR_TRUNCATED, "truncated gzip stream");
+        return RRG_ERR_TRUNCATED;
+    }
+    return index_build_impl(c, data, len, spacing ? spacing : (4ull << 20), out, stats, err);
+}
+
+int rrg_gpu_read_range(rrg_ctx* c, const uint8_t* data, size_t len, const rrg_index* idx, uint64_t off, uint64_t n,
+                       uint8_t* dst, rrg_error* err) {
+    rrg_error local_err;
+    if (!err) err = &local_err;
+    std::memset(err, 0, sizeof(*err));
+    if (!c || !data || !idx || (!dst && n)) {
+        set_err(err, RRG_ERR_INVALID_ARGUMENT, "null context, data, index or destination");
+        return RRG_ERR_INVALID_ARGUMENT;
+    }
+    return read_range_impl(c, data, len, idx, off, n, dst, err);
+}
+
+uint64_t rrg_index_total_out(const rrg_index* idx) { return idx ? idx->total_out : 0; }
+
+size_t rrg_index_count(const rrg_index* idx) { return idx ? idx->out_off.size() : 0; }
+
+int rrg_index_point(const rrg_index* idx, size_t k, uint64_t* out_off, uint64_t* in_bit) {
+    if (!idx || k >= idx->out_off.size()) return RRG_ERR_INVALID_ARGUMENT;
+    if (out_off) *out_off = idx->out_off[k];
+    if (in_bit) *in_bit = idx->body_off * 8 + idx->in_bit[k];
+    return 0;
+}
+
+// "RRGI", version 1, file_len, body_off, total_out, count, then per checkpoint
+// in_bit, out_off, win_len and the window's bytes (all little-endian).
+size_t rrg_index_serialize(const rrg_index* idx, uint8_t* buf, size_t cap) {
+    if (!idx) return 0;
+    size_t need = 8 + 4 * 8;
+    for (size_t k = 0; k < idx->out_off.size(); k++) need += 20 + idx->win_len[k];
+    if (!buf || cap < need) return need;
+    uint8_t* p = buf;
+    auto put = [&](uint64_t v, int nb) {
+        for (int i = 0; i < nb; i++) *p++ = (uint8_t)(v >> (8 * i));
+    };
+    std::memcpy(p, "RRGI", 4);
+    p += 4;
+    put(1, 4);
+    put(idx->file_len, 8);
+    put(idx->body_off, 8);
+    put(idx->total_out, 8);
+    put(idx->out_off.size(), 8);
+    for (size_t k = 0; k < idx->out_off.size(); k++) {
+        put(idx->in_bit[k], 8);
+        put(idx->out_off[k], 8);
+        put(idx->win_len[k], 4);
+        std::memcpy(p, idx->win.data() + k * 32768 + (32768 - idx->win_len[k]), idx->win_len[k]);
+        p += idx->win_len[k];
+    }
+    return need;
+}
+
+rrg_index* rrg_index_deserialize(const uint8_t* buf, size_t n, rrg_error* err) {
+    rrg_error local_err;
+    if (!err) err = &local_err;
+    std::memset(err, 0, sizeof(*err));
+    const uint8_t* p = buf;
+    const uint8_t* end = buf ? buf + n : nullptr;
+    auto get = [&](int nb, uint64_t* v) {
+        if (!p || end - p < nb) return false;
+        *v = 0;
+        for (int i = 0; i < nb; i++) *v |= (uint64_t)p[i] << (8 * i);
+        p += nb;
+        return true;
+    };
+    uint64_t ver = 0, cnt = 0;
+    auto* idx = new rrg_index;
+    bool ok = buf && n >= 8 && std::memcmp(buf, "RRGI", 4) == 0;
+    if (ok) {
+        p += 4;
+        ok = get(4, &ver) && ver == 1 && get(8, &idx->file_len) && get(8, &idx->body_off) &&
+             get(8, &idx->total_out) && get(8, &cnt) && cnt <= n / 20;
+    }
+    for (uint64_t k = 0; ok && k < cnt; k++) {
+        uint64_t ib = 0, oo = 0, wl = 0;
+        ok = get(8, &ib) && get(8, &oo) && get(4, &wl) && wl <= 32768 && (uint64_t)(end - p) >= wl &&
+             (idx->out_off.empty() || oo > idx->out_off.back()) && oo <= idx->total_out;
+        if (!ok) break;
+        idx->in_bit.push_back(ib);
+        idx->out_off.push_back(oo);
+        idx->win_len.push_back((uint32_t)wl);
+        idx->win.resize(idx->out_off.size() * 32768, 0);
+        std::memcpy(idx->win.data() + k * 32768 + (32768 - wl), p, wl);
+        p += wl;
+    }
+    if (!ok || idx->out_off.empty() || idx->out_off[0] != 0) {
+        delete idx;
+        set_err(err, RRG_ERR_INVALID_ARGUMENT, "not a seek index");
+        return nullptr;
+    }
+    return idx;
+}
+
+void rrg_index_free(rrg_index* idx) { delete idx; }
 
 int rrg_gpu_read_stream(rrg_ctx* c, rrg_read_fn read_fn, void* read_user, rrg_sink_fn sink, void* user,
                         uint64_t stripe_bytes, rrg_stats* stats, rrg_error* err) {

@@ -1,4 +1,4 @@
-"""Runs the batch, BGZF, member, stream and serving paths of the emulated build under
+"""Runs the batch, BGZF, member, stream, seek-index and serving paths of the emulated build under
 AddressSanitizer with exact device-buffer sizes (RRG_STRICT_ALLOC), so that an
 index past the end of any device buffer fails here rather than on a GPU.
 Started by test_emu.py::test_address_sanitizer in its own process."""
@@ -28,6 +28,10 @@ raw2, gz2 = W.config1(200 << 10, seed=4)
 out = []
 d.read_stream(io.BytesIO(gz2), out.append, stripe_bytes=65536)  # several stripes
 assert b"".join(out) == raw2
+idx = d.build_index(gz2, spacing=32 << 10)  # seek index and range reads
+pts = idx.points()
+assert d.read_range(gz2, idx, pts[1][0] - 10, 50_000) == raw2[pts[1][0] - 10:pts[1][0] + 49_990]
+assert d.read_range(gz2, idx, len(raw2) - 100, 100) == raw2[-100:]
 keep = []
 
 

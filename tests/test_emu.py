@@ -415,3 +415,38 @@ def test_read_gz_from_a_pipe(emu_decoder_factory, tmp_path):
     out2 = []
     d.read_stream(io.BytesIO(gz), first_only, stripe_bytes=65536)
     assert len(out2) == 1 and raw.startswith(out2[0])
+
+
+def test_seek_index(emu_decoder_factory):
+    """A seek index from one decode: every range read from its checkpoints
+    (inside one interval, across several, at the ends, across a member
+    boundary) equals the same bytes of the oracle's output; the byte image
+    round-trips; mismatched files, ranges past the end and BGZF are refused."""
+    raw, gz = W.config1(500 << 10, seed=15)
+    tail = W.fastq_like(120_000, 15)
+    data = gz + W.gzip_member(tail, 6)
+    want = oracle.read_gz(data, 2)
+    assert want == raw + tail
+    d = emu_decoder_factory(gpu_chunk_bytes=8192)
+    idx = d.build_index(data, spacing=64 << 10)
+    pts = idx.points()
+    assert idx.total_out == len(want) and len(pts) >= 5 and pts[0][0] == 0
+    assert all(b - a >= 64 << 10 for (a, _), (b, _) in zip(pts, pts[1:]))
+    rng = np.random.default_rng(15)
+    cases = [(0, 1000), (len(want) - 777, 777), (pts[2][0] - 5, 10), (pts[1][0] + 1, pts[3][0] - pts[1][0]),
+             (len(raw) - 3000, 6000), (0, len(want))]
+    cases += [(int(o), int(n)) for o, n in zip(rng.integers(0, len(want) - 50_000, 4), rng.integers(1, 50_000, 4))]
+    for off, n in cases:
+        assert d.read_range(data, idx, off, n) == want[off:off + n], (off, n)
+    from conftest import build_emu_lib
+    from rusty_rapidgzip_b200 import RrgError, SeekIndex
+    again = SeekIndex.load(idx.serialize(), lib=build_emu_lib())
+    assert again.points() == pts and again.total_out == idx.total_out
+    assert d.read_range(data, again, pts[-1][0], len(want) - pts[-1][0]) == want[pts[-1][0]:]
+    with pytest.raises(RrgError) as e1:
+        d.build_index(W.bgzf(tail, 5))
+    with pytest.raises(RrgError) as e2:
+        d.read_range(data[:-1], idx, 0, 10)
+    with pytest.raises(RrgError) as e3:
+        d.read_range(data, idx, len(want) - 5, 10)
+    assert e1.value.code == e2.value.code == e3.value.code == 22  # RRG_ERR_INVALID_ARGUMENT

@@ -482,3 +482,23 @@ def test_read_gz_pipe_gpu(gpu_decoder_factory, tmp_path):
     st = gpu_decoder_factory().read_gz(fifo, out.append)
     t.join()
     assert b"".join(out) == raw and st.compressed_bytes == len(gz)
+
+
+@pytest.mark.gpu
+def test_seek_index_gpu(gpu_decoder_factory):
+    """Seek index of a 128 MiB Zipf member plus a FASTQ member: random ranges
+    read from checkpoints equal the generator's bytes."""
+    raw, gz = W.config1(128 << 20, seed=16)
+    tail = W.fastq_like(8 << 20, 16)
+    data = gz + W.gzip_member(tail, 6)
+    whole = raw + tail
+    d = gpu_decoder_factory()
+    idx = d.build_index(data)
+    pts = idx.points()
+    assert idx.total_out == len(whole) and len(pts) >= 30
+    rng = np.random.default_rng(16)
+    cases = [(0, 4096), (len(raw) - 100_000, 300_000), (pts[-1][0], len(whole) - pts[-1][0])]
+    cases += [(int(o), int(n)) for o, n in zip(rng.integers(0, len(whole), 6), rng.integers(1, 9 << 20, 6))]
+    for off, n in cases:
+        n = min(n, len(whole) - off)
+        assert d.read_range(data, idx, off, n) == whole[off:off + n], (off, n)
