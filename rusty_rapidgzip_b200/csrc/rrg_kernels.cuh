@@ -2221,7 +2221,9 @@ __global__ void __launch_bounds__(256) k_win_init(ResolveArgs A) {
 
 __global__ void __launch_bounds__(256) k_win_chase(ResolveArgs A) {
     const uint64_t total = (uint64_t)A.n_chunks * WINDOW;
-    volatile uint32_t* win = A.win;
+    // Plain loads: a chain may see a cell before or after its owner resolved
+    // it; a pointer and the byte it resolves to lead to the same byte.
+    uint32_t* win = A.win;
     for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < total;
          c += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t w = win[c];
