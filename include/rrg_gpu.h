@@ -127,7 +127,10 @@ typedef int64_t (*rrg_read_fn)(void* user, uint8_t* buf, size_t cap);
  * between stripes, so memory is bounded by a few stripes. Output reaches
  * `sink` in order. rrg_gpu_read_gz takes this route for paths that are not
  * regular files. Errors, stats and the sink contract are those of
- * rrg_gpu_read_gz; stats->compressed_bytes counts the bytes read. */
+ * rrg_gpu_read_gz; stats->compressed_bytes counts the bytes read. `read_fn`
+ * is called from a thread of the library, one call at a time, so that the
+ * next stripe is read while the GPU decodes the current one; when the call
+ * returns early (an error, a closed sink) it first waits for a read in flight. */
 int rrg_gpu_read_stream(rrg_ctx* ctx, rrg_read_fn read_fn, void* read_user, rrg_sink_fn sink, void* user,
                         uint64_t stripe_bytes, rrg_stats* stats, rrg_error* err);
 

@@ -240,7 +240,7 @@ struct rrg_ctx {
     // device buffers (grow-only)
     DBuf items, results, order, queue, mbs, mbcount, cells, out, targets, limits, found, next_lut, chunks,
         tiles, rerr, markers, win, cand, ncand, vflag, lane_scratch, crc_table, pieces, piece_crc, mpiece, exp_crc, exp_isize, got_crc, got_len,
-        mstatus, comp, pfx;
+        mstatus, comp, comp2, pfx;
     // pinned host staging
     uint8_t* h_stage[2] = {nullptr, nullptr};
     size_t h_stage_cap = 0;
@@ -1867,6 +1867,82 @@ int decode_host_impl(rrg_ctx* c, const uint8_t* data, size_t len, rrg_sink_fn si
 // member's last 32 KiB of output (for back-references), its running CRC32 and
 // length, and the unread input survive, so memory stays a few stripes whatever
 // the stream's length.
+//
+// Reading overlaps decoding: a reader thread fills one of two pinned buffers
+// with the next stripe's bytes while the device decodes the current stripe.
+// A stripe is assembled on the device: the previous stripe's unread bytes
+// (moved there device to device) followed by the newly read ones.
+
+// One background read at a time into a caller's buffer.
+struct StreamReader {
+    rrg_read_fn rd;
+    void* user;
+    std::mutex m;
+    std::condition_variable cv;
+    std::thread th;
+    uint8_t* buf = nullptr;
+    uint64_t want = 0, got = 0;
+    bool busy = false, quit = false, eof = false, failed = false;
+    StreamReader(rrg_read_fn r, void* u) : rd(r), user(u) {
+        th = std::thread([this] {
+            std::unique_lock<std::mutex> lk(m);
+            for (;;) {
+                cv.wait(lk, [this] { return busy || quit; });
+                if (quit) return;
+                uint8_t* b = buf;
+                const uint64_t w = want;
+                lk.unlock();
+                uint64_t n = 0;
+                bool e = false, f = false;
+                while (n < w) {
+                    const int64_t r = rd(user, b + n, (size_t)(w - n));
+                    if (r < 0) {
+                        f = true;
+                        break;
+                    }
+                    if (r == 0) {
+                        e = true;
+                        break;
+                    }
+                    n += (uint64_t)r;
+                }
+                lk.lock();
+                got = n;
+                eof = eof || e;
+                failed = failed || f;
+                busy = false;
+                cv.notify_all();
+            }
+        });
+    }
+    ~StreamReader() {
+        {
+            std::unique_lock<std::mutex> lk(m);
+            cv.wait(lk, [this] { return !busy; });
+            quit = true;
+        }
+        cv.notify_all();
+        th.join();
+    }
+    void start(uint8_t* b, uint64_t w) {  // no read may be in flight
+        std::lock_guard<std::mutex> lk(m);
+        buf = b;
+        want = w;
+        got = 0;
+        busy = !eof && w > 0;
+        cv.notify_all();
+    }
+    uint64_t wait(bool* at_eof, bool* fail) {
+        std::unique_lock<std::mutex> lk(m);
+        cv.wait(lk, [this] { return !busy; });
+        *at_eof = eof;
+        *fail = failed;
+        const uint64_t n = got;
+        got = 0;
+        return n;
+    }
+};
+
 int stream_impl(rrg_ctx* c, rrg_read_fn rd, void* ruser, rrg_sink_fn sink, void* suser, uint64_t stripe_bytes,
                 rrg_stats* stats, rrg_error* err) {
     double t_all = now_ms();
@@ -1876,50 +1952,76 @@ int stream_impl(rrg_ctx* c, rrg_read_fn rd, void* ruser, rrg_sink_fn sink, void*
     if (rc) return rc;
     const uint64_t S = stripe_bytes ? std::max<uint64_t>(stripe_bytes, 1 << 16) : (256ull << 20);
     uint64_t L = std::max<uint64_t>(1ull << 16, S / 8);  // lookahead; doubled when a block outruns it
-    // the read buffer is pinned (c->h_in), so each stripe's copy runs at link speed
-    uint64_t have = 0, in_base = 0;  // h_in[0..have) = stream bytes [in_base, in_base + have)
-    bool eof = false;
-    auto fill = [&](uint64_t want) -> int {
-        if (c->h_in_cap < want) {
-            uint8_t* nb = nullptr;
-            const size_t cap = (size_t)want;
-            CK(cudaMallocHost((void**)&nb, cap));
-            if (have) std::memcpy(nb, c->h_in, (size_t)have);
-            if (c->h_in) cudaFreeHost(c->h_in);
-            c->h_in = nb;
-            c->h_in_cap = cap;
-        }
-        while (!eof && have < want) {
-            const int64_t r = rd(ruser, c->h_in + have, (size_t)(want - have));
-            if (r < 0) {
-                set_err(err, RRG_ERR_IO, "io: stream read failed");
-                return RRG_ERR_IO;
-            }
-            if (r == 0) eof = true;
-            else have += (uint64_t)r;
-        }
-        return 0;
-    };
     constexpr uint64_t PRE = 32768;  // the prefix region in front of every stripe's output
-    bool in_member = false, any = false;
-    uint64_t start_bit = 0, len_prev = 0, prefix_len = 0;
-    uint32_t crc_prev = 0, members = 0;
-    uint64_t total_out = 0;
+    // two pinned read buffers of S + L bytes each (c->h_in)
+    const uint64_t PB = S + L;
+    if (c->h_in_cap < 2 * PB) {
+        if (c->h_in) cudaFreeHost(c->h_in);
+        c->h_in = nullptr;
+        c->h_in_cap = 0;
+        CK(cudaMallocHost((void**)&c->h_in, (size_t)(2 * PB)));
+        c->h_in_cap = (size_t)(2 * PB);
+    }
+    uint8_t* pb[2] = {c->h_in, c->h_in + PB};
+    // the stripe on the device: comp[0..have); comp2 takes the unread tail
+    uint64_t dcap = 2 * PB + 16;
+    CK(dgrow(c->comp, dcap));
+    CK(dgrow(c->comp2, dcap));
     CK(dgrow(c->pfx, PRE));
     OutTarget tgt{(uint8_t*)c->out.p, c->out.cap, true};
     rc = ensure_out(c, tgt, PRE + 4096, 0, err);
     if (rc) return rc;
+    StreamReader reader(rd, ruser);
+    int cur = 0;
+    reader.start(pb[cur], PB);
+    uint64_t have = 0, in_base = 0;  // comp[0..have) = stream bytes [in_base, in_base + have)
+    bool eof = false;
+    // append the read in flight (buffer pb[cur]) to the device stripe and start
+    // the next read into the other buffer
+    auto take = [&](uint64_t next_want) -> int {
+        bool fail = false;
+        const uint64_t n = reader.wait(&eof, &fail);
+        if (fail) {
+            set_err(err, RRG_ERR_IO, "io: stream read failed");
+            return RRG_ERR_IO;
+        }
+        if (have + n + 16 > dcap) {  // a stripe grown by retries: keep its bytes
+            const uint64_t ncap = 2 * (have + n) + 16;
+            CK(dgrow(c->comp2, ncap));
+            if (have) CK(cudaMemcpyAsync(c->comp2.p, c->comp.p, have, cudaMemcpyDeviceToDevice, c->stream));
+            CK(cudaStreamSynchronize(c->stream));
+            std::swap(c->comp, c->comp2);
+            CK(dgrow(c->comp2, ncap));
+            dcap = ncap;
+        }
+        if (n) CK(cudaMemcpyAsync((uint8_t*)c->comp.p + have, pb[cur], n, cudaMemcpyHostToDevice, c->stream));
+        have += n;
+        CK(cudaStreamSynchronize(c->stream));  // pb[cur] may be refilled from here on
+        cur ^= 1;
+        if (!eof) reader.start(pb[cur], std::min(next_want, PB));
+        return 0;
+    };
+    if ((rc = take(S))) return rc;
+    bool in_member = false, any = false;
+    uint64_t start_bit = 0, len_prev = 0, prefix_len = 0;
+    uint32_t crc_prev = 0, members = 0;
+    uint64_t total_out = 0;
+    std::vector<uint8_t> head;
     for (;;) {
-        if ((rc = fill(S + L))) return rc;
         uint64_t body_off = 0;
         if (!in_member) {
             if (have == 0 && eof) break;  // end of the stream between members
+            head.resize((size_t)std::min<uint64_t>(have, 1 << 16));
+            if (!head.empty()) {
+                CK(cudaMemcpyAsync(head.data(), c->comp.p, head.size(), cudaMemcpyDeviceToHost, c->stream));
+                CK(cudaStreamSynchronize(c->stream));
+            }
             size_t hl = 0;
             int detail = 0;
-            int st = host_parse_header(c->h_in, have, &hl, &detail);
+            int st = host_parse_header(head.data(), head.size(), &hl, &detail);
             if (st) {
                 if (st == DS_TRUNCATED && !eof) {
-                    if ((rc = fill(have + L))) return rc;
+                    if ((rc = take(S))) return rc;
                     continue;
                 }
                 return status_err(err, st, detail, in_base);
@@ -1936,13 +2038,11 @@ int stream_impl(rrg_ctx* c, rrg_read_fn rd, void* ruser, rrg_sink_fn sink, void*
         if (!eof) {
             const uint64_t lim = have > L ? have - L : 0;
             if (lim * 8 <= body_off * 8 + start_bit + 8) {  // too little read for a stripe
-                if ((rc = fill(have + S))) return rc;
+                if ((rc = take(S))) return rc;
                 continue;
             }
             stop = lim * 8 - body_off * 8;
         }
-        CK(dgrow(c->comp, have + 16));
-        if (have) CK(cudaMemcpyAsync(c->comp.p, c->h_in, have, cudaMemcpyHostToDevice, c->stream));
         if (prefix_len)
             CK(cudaMemcpyAsync(tgt.p + PRE - prefix_len, (const uint8_t*)c->pfx.p + PRE - prefix_len, prefix_len,
                                cudaMemcpyDeviceToDevice, c->stream));
@@ -1965,7 +2065,7 @@ int stream_impl(rrg_ctx* c, rrg_read_fn rd, void* ruser, rrg_sink_fn sink, void*
             // a block that runs past the read input: read more and redo the stripe
             if (!eof && (j.rc == RRG_ERR_DEFLATE_EOF || j.rc == RRG_ERR_TRUNCATED)) {
                 L *= 2;
-                if ((rc = fill(have + L))) return rc;
+                if ((rc = take(S))) return rc;
                 continue;
             }
             if (err) *err = j.err;
@@ -2001,10 +2101,16 @@ int stream_impl(rrg_ctx* c, rrg_read_fn rd, void* ruser, rrg_sink_fn sink, void*
             used = j.out.consumed;  // the members ended inside the read input
             in_member = false;
         }
-        CK(cudaStreamSynchronize(c->stream));  // the copy out of h_in has finished
-        std::memmove(c->h_in, c->h_in + used, (size_t)(have - used));
+        // the unread bytes move to the front of the other device buffer
+        if (have > used)
+            CK(cudaMemcpyAsync(c->comp2.p, (const uint8_t*)c->comp.p + used, have - used, cudaMemcpyDeviceToDevice,
+                               c->stream));
+        std::swap(c->comp, c->comp2);
         have -= used;
         in_base += used;
+        if (!eof) {  // a read is in flight until the stream ends
+            if ((rc = take(used ? used : S))) return rc;
+        }
         if (!in_member && have == 0 && eof) break;
     }
     CK(cudaStreamSynchronize(c->stream));
@@ -2378,7 +2484,7 @@ void release_scratch(rrg_ctx* c) {
     DBuf* bufs[] = {&c->cand, &c->ncand, &c->vflag, &c->lane_scratch, &c->win, &c->items,  &c->results, &c->order,     &c->queue,    &c->mbs,      &c->mbcount,   &c->cells,
                     &c->out,    &c->targets, &c->limits,    &c->found,    &c->next_lut, &c->chunks,    &c->tiles,
                     &c->rerr,   &c->markers, &c->crc_table, &c->pieces,   &c->piece_crc, &c->mpiece,   &c->exp_crc,
-                    &c->exp_isize, &c->got_crc, &c->got_len, &c->mstatus, &c->comp, &c->bg_bcount, &c->bg_bbase,
+                    &c->exp_isize, &c->got_crc, &c->got_len, &c->mstatus, &c->comp, &c->comp2, &c->pfx, &c->bg_bcount, &c->bg_bbase,
                     &c->bg_coff, &c->bg_csize, &c->bg_small, &c->sniff, &c->tile_chunk};
 #ifndef RRG_EMU
     if (c->bg_exec) cudaGraphExecDestroy(c->bg_exec);
