@@ -744,6 +744,12 @@ int scan_boundaries(rrg_ctx* c, const uint8_t* body, uint64_t blen, std::vector<
     if (c->arr_base && !c->arr_pieces.empty()) {
         const uint8_t* tile0 = (const uint8_t*)((uintptr_t)body & ~(uintptr_t)15);
         const uint64_t skip = (uint64_t)(tile0 - c->arr_base);
+#ifdef RRG_EMU
+        const uint64_t piece_min = 0;  // the CPU emulation exercises per-piece verification on small inputs
+#else
+        const uint64_t piece_min = 16ull << 20;
+#endif
+        const bool per_piece = c->arr_pieces.size() > 1 && c->arr_pieces[0].first >= piece_min;
         for (const auto& pc : c->arr_pieces) {
             CK(cudaStreamWaitEvent(c->stream, pc.second, 0));
             const uint64_t have = pc.first > skip ? pc.first - skip : 0;
@@ -752,9 +758,13 @@ int scan_boundaries(rrg_ctx* c, const uint8_t* body, uint64_t blen, std::vector<
             int rc0 = scan(t_done, t_hi);
             if (rc0) return rc0;
             t_done = t_hi;
-            if (int rv = verify()) return rv;
-            RRG_LAUNCH(k_verify_mark, 1, 32, 0, c->stream, counts, cap, cap2);
-            LAUNCHED(c);
+            // verification per piece pays only when a piece's copy outlasts
+            // the launches (pieces of at least 16 MiB); smaller inputs verify once
+            if (per_piece) {
+                if (int rv = verify()) return rv;
+                RRG_LAUNCH(k_verify_mark, 1, 32, 0, c->stream, counts, cap, cap2);
+                LAUNCHED(c);
+            }
         }
         c->arr_base = nullptr;  // everything has arrived for the kernels that follow
         c->arr_pieces.clear();
