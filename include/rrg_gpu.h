@@ -316,7 +316,9 @@ int64_t rrg_gpu_pending(rrg_ctx* ctx);
  * that loads the library holds until the process exits; that bounds `len` to
  * 4 GiB (4294967296 bytes), and longer inputs fail with RRG_ERR_CAPACITY. The
  * first call on a device looks up that array and loads the CRC tables; make
- * it before any stream capture. Work is ordered on `stream` (a cudaStream_t,
+ * it before any stream capture. A new CUDA context on the device (after
+ * cudaDeviceReset) gets a fresh copy of the array, and the next call there
+ * repeats that set-up. Work is ordered on `stream` (a cudaStream_t,
  * or NULL for the legacy default stream) and the call returns once the result
  * is on the host. Every call shares the same array, so calls that overlap on
  * the GPU (from several host threads or streams) race and must be serialised

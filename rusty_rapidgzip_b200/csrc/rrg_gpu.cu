@@ -7,7 +7,11 @@
 //                     back-references emitted as 16-bit marker cells
 //   host chain     -> anchored verification (pipeline.rs:758-809): chunk k is kept iff
 //                     it starts where chunk k-1 stopped; otherwise it is re-decoded
-//   k_resolve      -> markers chased to literal cells, cells compacted to bytes
+//   k_win_maps, k_win_bases -> the tail chain as composed window maps: every chunk's
+//                     window relative to its group's first window, then those windows
+//   k_res_tails    -> every chunk's last 32 KiB of cells to bytes through its map
+//   k_res_heads    -> the other cells to bytes, markers gathered from the 32 KiB of
+//                     output before the chunk
 //   k_crc_*        -> CRC32/ISIZE of every member from per-piece CRCs + GF(2) combine
 // BGZF route (pipeline.rs:1357-1636): members found by a header walk, one warp
 // per member through the persistent k_inflate<u8> work queue, CRC as above.
@@ -23,6 +27,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -264,8 +269,7 @@ struct rrg_ctx {
     cudaEvent_t arr_events[8] = {};
     cudaStream_t copy_stream = nullptr;
     DBuf sniff;                // per-file header results of a batch
-    DBuf tile_chunk;           // resolve: chunk of every tile
-    // BGZF route: device member table and the captured decode graph
+        // BGZF route: device member table and the captured decode graph
     DBuf bg_bcount, bg_bbase, bg_coff, bg_csize, bg_small;
     uint64_t* h_bg = nullptr;  // pinned: the 64 result bytes of one BGZF decode
     uint32_t bg_cap = 0;
@@ -323,6 +327,8 @@ struct Server {
 };
 
 namespace {
+
+uint64_t round8(uint64_t v) { return (v + 7) & ~7ull; }
 
 cudaError_t dgrow(DBuf& b, size_t n) {
     if (n == 0) n = 16;
@@ -632,44 +638,94 @@ int ensure_out(rrg_ctx* c, OutTarget& t, uint64_t need, uint64_t keep, rrg_error
 }
 
 // ------------------------------------------------------------ resolve
-// Windows (init + chase), then cells -> bytes. Returns 0 or an error code.
-int run_resolve(rrg_ctx* c, const std::vector<ResolveChunk>& rchunks, const std::vector<uint64_t>& tile_start,
-                uint8_t* d_dst, rrg_error* err, int64_t* bad_chunk = nullptr) {
+// Window maps, group base windows, chunk tails, then the rest of every chunk,
+// into d_dst. Chunks of one job are consecutive in `rchunks` with rising
+// out_start; the job's first chunk has out_start == job_out. Returns 0 or an
+// error code; a failure names its chunk in *bad_chunk.
+int run_resolve(rrg_ctx* c, const std::vector<ResolveChunk>& rchunks, uint8_t* d_dst, rrg_error* err,
+                int64_t* bad_chunk = nullptr) {
     const uint32_t nc = (uint32_t)rchunks.size();
     if (!nc) return 0;
-    CK(dgrow(c->chunks, nc * sizeof(ResolveChunk)));
-    CK(dgrow(c->tiles, (nc + 1) * 8));
+    // groups: runs of about sqrt(0.7 x chunks of the job) consecutive chunks,
+    // which balances the chunk-after-chunk map building inside a group against
+    // the group-after-group base pass of the job
+    std::vector<ResGroup> groups;
+    std::vector<ResJob> jobs;
+    std::vector<uint32_t> chunk_group(nc);
+    for (uint32_t a = 0; a < nc;) {
+        uint32_t b = a + 1;
+        while (b < nc && rchunks[b].job_out == rchunks[a].job_out && rchunks[b].out_start > rchunks[b - 1].out_start)
+            b++;
+        const uint32_t cj = b - a;
+        const uint32_t S = std::max<uint32_t>(1, (uint32_t)std::ceil(std::sqrt(0.7 * cj)));
+        jobs.push_back(ResJob{(uint32_t)groups.size(), (cj + S - 1) / S});
+        for (uint32_t f = a; f < b; f += S) {
+            const uint32_t n = std::min(S, b - f);
+            for (uint32_t k = f; k < f + n; k++) chunk_group[k] = (uint32_t)groups.size();
+            groups.push_back(ResGroup{f, n});
+        }
+        a = b;
+    }
+    const uint32_t ng = (uint32_t)groups.size(), nj = (uint32_t)jobs.size();
+    // per chunk: tail tiles and head segments, as prefixes the kernels search
+    std::vector<uint64_t> pre(2 * (size_t)(nc + 1));
+    uint64_t* tt = pre.data();
+    uint64_t* hs = pre.data() + nc + 1;
+    tt[0] = hs[0] = 0;
+    for (uint32_t k = 0; k < nc; k++) {
+        const uint64_t n = rchunks[k].n_cells;
+        const uint32_t lo = res_tail_lo(n) & ~(uint32_t)(RES_TAIL_TILE - 1);
+        tt[k + 1] = tt[k] + (WINDOW - lo) / RES_TAIL_TILE;
+        hs[k + 1] = hs[k] + (res_head_end(n) + RES_HEAD_SEG - 1) / RES_HEAD_SEG;
+    }
+    // one upload: chunks, groups, jobs, chunk_group, prefixes
+    const size_t o_grp = round8(nc * sizeof(ResolveChunk)), o_job = o_grp + round8(ng * sizeof(ResGroup)),
+                 o_cg = o_job + round8(nj * sizeof(ResJob)), o_pre = o_cg + round8(nc * 4),
+                 total = o_pre + pre.size() * 8;
+    std::vector<uint8_t> blob(total);
+    std::memcpy(blob.data(), rchunks.data(), nc * sizeof(ResolveChunk));
+    std::memcpy(blob.data() + o_grp, groups.data(), ng * sizeof(ResGroup));
+    std::memcpy(blob.data() + o_job, jobs.data(), nj * sizeof(ResJob));
+    std::memcpy(blob.data() + o_cg, chunk_group.data(), nc * 4);
+    std::memcpy(blob.data() + o_pre, pre.data(), pre.size() * 8);
+    CK(dgrow(c->chunks, total));
+    CK(dgrow(c->win, ((size_t)nc + ng) * WINDOW * 2));
     CK(dgrow(c->rerr, 16));
     CK(dgrow(c->markers, 8));
-    CK(dgrow(c->win, (size_t)nc * WINDOW * 5 + (size_t)nc * 4));  // u32 windows, byte windows, flags
-    uint8_t* winb = (uint8_t*)c->win.p + (size_t)nc * WINDOW * 4;
-    uint32_t* win_bad = (uint32_t*)(winb + (size_t)nc * WINDOW);
-    CK(cudaMemsetAsync(win_bad, 0, (size_t)nc * 4, c->stream));
-    CK(cudaMemcpyAsync(c->chunks.p, rchunks.data(), nc * sizeof(ResolveChunk), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(c->tiles.p, tile_start.data(), (nc + 1) * 8, cudaMemcpyHostToDevice, c->stream));
-    const uint64_t n_tiles = tile_start.back();
-    std::vector<uint32_t> tchunk(n_tiles);
-    for (uint32_t k = 0; k < nc; k++)
-        for (uint64_t t = tile_start[k]; t < tile_start[k + 1]; t++) tchunk[t] = k;
-    CK(dgrow(c->tile_chunk, std::max<uint64_t>(n_tiles, 1) * 4));
-    if (n_tiles) CK(cudaMemcpyAsync(c->tile_chunk.p, tchunk.data(), n_tiles * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->chunks.p, blob.data(), total, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemsetAsync(c->rerr.p, 0, 16, c->stream));
     CK(cudaMemsetAsync(c->markers.p, 0, 8, c->stream));
-    ResolveArgs R{(const uint16_t*)c->cells.p, (const ResolveChunk*)c->chunks.p, (const uint64_t*)c->tiles.p,
-                  (const uint32_t*)c->tile_chunk.p, nc,
-                  tile_start.back(), d_dst, (uint32_t*)c->win.p, (uint32_t*)c->rerr.p,
-                  (unsigned long long*)c->markers.p, winb, win_bad};
-    const uint64_t wcells = (uint64_t)nc * WINDOW;
-    const uint32_t wgrid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((wcells + 255) / 256, (uint64_t)c->n_sm * 32));
-    uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(tile_start.back(), (uint64_t)c->n_sm * 16));
+    uint8_t* dev = (uint8_t*)c->chunks.p;
+    ResolveArgs R{};
+    R.cells = (uint16_t*)c->cells.p;
+    R.chunks = (const ResolveChunk*)dev;
+    R.n_chunks = nc;
+    R.groups = (const ResGroup*)(dev + o_grp);
+    R.n_groups = ng;
+    R.jobs = (const ResJob*)(dev + o_job);
+    R.n_jobs = nj;
+    R.chunk_group = (const uint32_t*)(dev + o_cg);
+    R.tail_tiles = (const uint64_t*)(dev + o_pre);
+    R.head_segs = (const uint64_t*)(dev + o_pre) + nc + 1;
+    R.maps = (uint16_t*)c->win.p;
+    R.bases = (uint16_t*)c->win.p + (size_t)nc * WINDOW;
+    R.out = d_dst;
+    R.err = (uint32_t*)c->rerr.p;
+    R.markers = (unsigned long long*)c->markers.p;
+    const uint32_t tgrid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(tt[nc], (uint64_t)c->n_sm * 8));
+    const uint32_t hgrid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(hs[nc], (uint64_t)c->n_sm * 4));
     KTimer kt(c->stream);
-    RRG_LAUNCH(k_win_init, wgrid, 256, 0, c->stream, R);
+    RRG_LAUNCH(k_win_maps, std::min<uint32_t>(ng, c->n_sm), WM_THREADS, WM_SMEM, c->stream, R);
     LAUNCHED(c);
-    RRG_LAUNCH(k_win_chase, wgrid, 256, 0, c->stream, R);
+    RRG_LAUNCH(k_win_bases, std::min<uint32_t>(nj, c->n_sm), WM_THREADS, WINDOW * 2, c->stream, R);
     LAUNCHED(c);
-    RRG_LAUNCH(k_resolve, grid, RES_THREADS, 0, c->stream, R);
+    RRG_LAUNCH(k_res_tails, tgrid, RES_THREADS, 0, c->stream, R);
+    LAUNCHED(c);
+    if (hs[nc]) {
+        RRG_LAUNCH(k_res_heads, hgrid, RES_THREADS, 0, c->stream, R);
+        LAUNCHED(c);
+    }
     kt.stop();
-    LAUNCHED(c);
     uint32_t e4[4];
     unsigned long long nmk = 0;
     CK(cudaMemcpyAsync(e4, c->rerr.p, 16, cudaMemcpyDeviceToHost, c->stream));
@@ -833,8 +889,6 @@ struct Decoded {
     uint64_t consumed = 0;
     uint32_t members = 0;
 };
-
-uint64_t round8(uint64_t v) { return (v + 7) & ~7ull; }
 
 // One gzip member stream (a file, or what follows a BGZF prefix) for the
 // member route. Several jobs share every kernel launch.
@@ -1314,7 +1368,6 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
     }
     std::vector<ResolveChunk> rchunks;
     std::vector<size_t> chunk_job;
-    std::vector<uint64_t> tile_start{0};
     std::vector<MemberSpan> spans;
     std::vector<size_t> span_job;
     std::vector<uint32_t> span_member;
@@ -1346,7 +1399,6 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
                 const uint64_t ms = (nm == 0 && continued) ? j.dst_off - j.prefix_len : j.dst_off + mstart;
                 rchunks.push_back(ResolveChunk{j.dst_off + pos, a.it.out_off, a.r.n_cells, ms, j.dst_off});
                 chunk_job.push_back(i);
-                tile_start.push_back(tile_start.back() + (a.r.n_cells + RES_TILE - 1) / RES_TILE);
             }
             for (const MemberRec& m : a.m) {
                 const uint64_t end = pos + m.cell_off;
@@ -1371,7 +1423,7 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
     // ---- resolve markers + compact; a failing chunk fails its job only
     int64_t bad = -1;
     rrg_error rerr{};
-    rc = run_resolve(c, rchunks, tile_start, tgt.p, &rerr, &bad);
+    rc = run_resolve(c, rchunks, tgt.p, &rerr, &bad);
     if (rc && (rc != RRG_ERR_DEFLATE_INVALID || bad < 0 || (uint64_t)bad >= chunk_job.size())) {
         if (err) *err = rerr;
         return rc;
@@ -2242,6 +2294,10 @@ int read_range_impl(rrg_ctx* c, const uint8_t* data, size_t len, const rrg_index
     // the bit reader's read-ahead (or to the end of the file)
     const uint64_t end_byte =
         hi < oo.size() ? std::min<uint64_t>(len, (idx->body_off * 8 + idx->in_bit[hi]) / 8 + (64u << 10)) : len;
+    if (byte0 >= len || end_byte <= byte0 || (hi < oo.size() && idx->in_bit[hi] <= idx->in_bit[lo])) {
+        set_err(err, RRG_ERR_INVALID_ARGUMENT, "seek index checkpoints lie outside the file");
+        return RRG_ERR_INVALID_ARGUMENT;
+    }
     const uint64_t clen = end_byte - byte0;
     CK(dgrow(c->comp, clen + 16));
     CK(cudaMemcpyAsync(c->comp.p, data + byte0, clen, cudaMemcpyHostToDevice, c->stream));
@@ -2495,7 +2551,7 @@ void release_scratch(rrg_ctx* c) {
                     &c->out,    &c->targets, &c->limits,    &c->found,    &c->next_lut, &c->chunks,    &c->tiles,
                     &c->rerr,   &c->markers, &c->crc_table, &c->pieces,   &c->piece_crc, &c->mpiece,   &c->exp_crc,
                     &c->exp_isize, &c->got_crc, &c->got_len, &c->mstatus, &c->comp, &c->comp2, &c->pfx, &c->bg_bcount, &c->bg_bbase,
-                    &c->bg_coff, &c->bg_csize, &c->bg_small, &c->sniff, &c->tile_chunk};
+                    &c->bg_coff, &c->bg_csize, &c->bg_small, &c->sniff};
 #ifndef RRG_EMU
     if (c->bg_exec) cudaGraphExecDestroy(c->bg_exec);
     c->bg_exec = nullptr;
@@ -2821,6 +2877,8 @@ rrg_ctx* rrg_gpu_create(const rrg_config* cfg, rrg_error* err) {
     cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
     size_t want = (size_t)c->inflate_warps * sizeof(WarpSmem);
     cudaFuncSetAttribute(k_find_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(4 * sizeof(FindSmem)));
+    cudaFuncSetAttribute(k_win_maps, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WM_SMEM);
+    cudaFuncSetAttribute(k_win_bases, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(WINDOW * 2));
     cudaFuncSetAttribute(k_verify_heavy, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(4 * sizeof(FindSmem)));
     cudaFuncSetAttribute(k_inflate_lanes<uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(LANE_THREADS * sizeof(LaneTab)));
@@ -2999,8 +3057,12 @@ rrg_index* rrg_index_deserialize(const uint8_t* buf, size_t n, rrg_error* err) {
     }
     for (uint64_t k = 0; ok && k < cnt; k++) {
         uint64_t ib = 0, oo = 0, wl = 0;
-        ok = get(8, &ib) && get(8, &oo) && get(4, &wl) && wl <= 32768 && (uint64_t)(end - p) >= wl &&
-             (idx->out_off.empty() || oo > idx->out_off.back()) && oo <= idx->total_out;
+        // checkpoints lie inside the file's body, in increasing bit and output
+        // order, and carry at most one window of history
+        ok = get(8, &ib) && get(8, &oo) && get(4, &wl) && wl <= 32768 && wl <= oo && (uint64_t)(end - p) >= wl &&
+             (idx->out_off.empty() || (oo > idx->out_off.back() && ib > idx->in_bit.back())) &&
+             oo <= idx->total_out && idx->body_off < idx->file_len &&
+             ib < (idx->file_len - idx->body_off) * 8;
         if (!ok) break;
         idx->in_bit.push_back(ib);
         idx->out_off.push_back(oo);
@@ -3009,7 +3071,7 @@ rrg_index* rrg_index_deserialize(const uint8_t* buf, size_t n, rrg_error* err) {
         std::memcpy(idx->win.data() + k * 32768 + (32768 - wl), p, wl);
         p += wl;
     }
-    if (!ok || idx->out_off.empty() || idx->out_off[0] != 0) {
+    if (!ok || idx->out_off.empty() || idx->out_off[0] != 0 || idx->file_len > (1ull << 61)) {
         delete idx;
         set_err(err, RRG_ERR_INVALID_ARGUMENT, "not a seek index");
         return nullptr;
@@ -3169,43 +3231,22 @@ int rrg_gpu_resolve_markers(rrg_ctx* c, uint8_t* d_bytes, size_t n_bytes, const 
     }
     if (err) std::memset(err, 0, sizeof(*err));
     if (!n_markers) return 0;
-    // Express the reference's (bytes, markers, prev_tail) triple as two chunks
-    // of cells: the tail (all literals) followed by the chunk, whose marker
-    // cells carry their prefix offsets; k_resolve then writes tail || bytes.
-    const uint64_t tl = tail_len, nb = n_bytes;
-    const uint64_t cells_n = round8(tl) + round8(nb);
-    CK(dgrow(c->cells, cells_n * 2 + 64));
-    CK(dgrow(c->out, tl + nb + 64));
-    std::vector<uint16_t> hc(cells_n, 0);
-    std::vector<uint8_t> tail(tl), bytes(nb);
-    std::vector<uint32_t> mp(n_markers);
-    std::vector<uint16_t> mo(n_markers);
-    if (tl) CK(cudaMemcpy(tail.data(), d_tail, tl, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(bytes.data(), d_bytes, nb, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(mp.data(), d_out_pos, n_markers * 4, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(mo.data(), d_prefix_offset, n_markers * 2, cudaMemcpyDeviceToHost));
-    for (uint64_t i = 0; i < tl; i++) hc[i] = tail[i];
-    const uint64_t base = round8(tl);
-    for (uint64_t i = 0; i < nb; i++) hc[base + i] = bytes[i];
-    for (size_t i = 0; i < n_markers; i++) {
-        if (mo[i] >= tl || mp[i] >= nb) {
-            set_err(err, RRG_ERR_DEFLATE_INVALID, "%s", msg_text(MSG_MARKER_WINDOW));
-            return RRG_ERR_DEFLATE_INVALID;
-        }
-        hc[base + mp[i]] = (uint16_t)(MARKER16 | mo[i]);
+    // resolve_markers (speculative.rs:175-213) on the device: one thread per
+    // marker writes its byte from the tail; an offset past the tail or a
+    // position past the bytes fails the call
+    CK(dgrow(c->rerr, 16));
+    CK(cudaMemsetAsync(c->rerr.p, 0, 16, c->stream));
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((n_markers + 255) / 256, c->n_sm * 16ull));
+    RRG_LAUNCH(k_resolve_list, grid, 256, 0, c->stream, d_bytes, (uint64_t)n_bytes, d_out_pos, d_prefix_offset,
+               (uint64_t)n_markers, d_tail, (uint64_t)tail_len, (uint32_t*)c->rerr.p);
+    LAUNCHED(c);
+    uint32_t bad = 0;
+    CK(cudaMemcpyAsync(&bad, c->rerr.p, 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (bad) {
+        set_err(err, RRG_ERR_DEFLATE_INVALID, "%s", msg_text(MSG_MARKER_WINDOW));
+        return RRG_ERR_DEFLATE_INVALID;
     }
-    CK(cudaMemcpy(c->cells.p, hc.data(), cells_n * 2, cudaMemcpyHostToDevice));
-    std::vector<ResolveChunk> ch;
-    std::vector<uint64_t> ts{0};
-    if (tl) {
-        ch.push_back(ResolveChunk{0, 0, tl, 0});
-        ts.push_back(ts.back() + (tl + RES_TILE - 1) / RES_TILE);
-    }
-    ch.push_back(ResolveChunk{tl, base, nb, 0});
-    ts.push_back(ts.back() + (nb + RES_TILE - 1) / RES_TILE);
-    int rc = run_resolve(c, ch, ts, (uint8_t*)c->out.p, err);
-    if (rc) return rc;
-    CK(cudaMemcpy(d_bytes, (const uint8_t*)c->out.p + tl, nb, cudaMemcpyDeviceToDevice));
     return 0;
 }
 
@@ -3400,7 +3441,45 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocS
 namespace {
 
 std::mutex g_noalloc_mu;
-NoAllocScratch* g_noalloc_dev[64] = {nullptr};  // device address of the scratch, per device ordinal
+// Per device ordinal: the scratch's device address and the id of the CUDA
+// context it was set up in. A new context on that device (after
+// cudaDeviceReset, for example) holds a fresh copy of the array without the
+// tables, so the set-up runs again there.
+struct NoAllocDev {
+    NoAllocScratch* p = nullptr;
+    unsigned long long ctx_id = 0;
+};
+NoAllocDev g_noalloc_dev[64];
+
+// Unique id of the calling thread's current context (cuCtxGetCurrent and
+// cuCtxGetId, reached through the runtime's driver entry points); 0 when no
+// context is current or the driver does not provide them.
+unsigned long long current_ctx_id() {
+#ifdef RRG_EMU
+    return 1;
+#else
+    using GetCurrent = int (*)(void**);
+    using GetId = int (*)(void*, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = (GetCurrent)f;
+        f = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (GetId)f;
+    });
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+    return id;
+#endif
+}
 
 // Piece descriptors for one buffer; also resets the fields k_crc_members reads.
 __global__ void k_noalloc_pieces(NoAllocScratch* S, uint64_t len, uint32_t n_pieces) {
@@ -3420,23 +3499,29 @@ __global__ void k_noalloc_pieces(NoAllocScratch* S, uint64_t len, uint32_t n_pie
     }
 }
 
-// First call on the current device: find the scratch's device address and
-// load the CRC tables into it and into constant memory.
+// First call on the current device (or in a new context on it): find the
+// scratch's device address and load the CRC tables into it and into constant
+// memory.
 int noalloc_setup(int dev, NoAllocScratch** out, rrg_error* err) {
     std::lock_guard<std::mutex> g(g_noalloc_mu);
     if (dev < 0 || dev >= 64) {
         set_err(err, RRG_ERR_INVALID_ARGUMENT, "device ordinal %d out of range", dev);
         return RRG_ERR_INVALID_ARGUMENT;
     }
-    if (!g_noalloc_dev[dev]) {
+    NoAllocDev& D = g_noalloc_dev[dev];
+    // before the runtime's first call on this device no context is current
+    // (id 0); the set-up below creates it
+    const unsigned long long id = current_ctx_id();
+    if (!D.p || (id != 0 && id != D.ctx_id)) {
         std::call_once(g_tab_once, init_tables);
         void* p = nullptr;
         CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
         CK(cudaMemcpy(p, g_crc_tab, sizeof(g_crc_tab), cudaMemcpyHostToDevice));
         CK(cudaMemcpyToSymbol(c_x2k, g_x2k, sizeof(g_x2k)));
-        g_noalloc_dev[dev] = (NoAllocScratch*)p;
+        D.p = (NoAllocScratch*)p;
+        D.ctx_id = current_ctx_id();
     }
-    *out = g_noalloc_dev[dev];
+    *out = D.p;
     return 0;
 }
 

@@ -6,8 +6,9 @@
 //   k_inflate      — rrg/src/pipeline.rs:1080-1185 decode_one_chunk with
 //                    rrg/src/deflate/fast_inflate.rs:1794-2234 (u16 marker cells), or a
 //                    whole member into final bytes (gzip.rs:197-249 decode_one_indexed_fast)
-//   k_resolve      — rrg/src/deflate/speculative.rs:175-213 resolve_markers together with the
-//                    tail chain of rrg/src/pipeline.rs:1045-1078, fused with the chunk compaction
+//   k_win_maps / k_win_bases / k_res_tails / k_res_heads — rrg/src/deflate/speculative.rs:175-213
+//                    resolve_markers together with the tail chain of rrg/src/pipeline.rs:1045-1078,
+//                    fused with the chunk compaction
 //   k_crc_pieces / k_crc_members — crc32fast hashing + combine (rrg/src/pipeline.rs:712-732, :885-916)
 //
 // This header is compiled by nvcc for sm_100a (rrg_kernels.cu) and, for the
@@ -1840,7 +1841,9 @@ __global__ void __launch_bounds__(128) k_find_blocks(FindArgs A) {
 // target, so it tests every bit offset of the body: 4 KiB tiles staged in
 // shared memory with 16-byte loads, each thread testing the 128 offsets of
 // its 16 bytes (prefilter BFINAL=0, BTYPE=2, HLIT<=29, HDIST<=29, then the
-// strict Kraft test of the precode), survivors compacted with warp ballots.
+// strict Kraft test of the precode). A tile's survivors are appended to a
+// shared-memory list with shared atomics and copied out with one global
+// atomicAdd per tile.
 // k_verify_light then applies the strict code-length checks of
 // read_dynamic_header_strict_into (block_finder.rs:196-262) per thread, and
 // the last survivors get verify_heavy (tables + 64 trial symbols).
@@ -2154,173 +2157,331 @@ __global__ void __launch_bounds__(128) k_verify_heavy(VerifyArgs A) {
 }
 
 // ------------------------------------------------------- marker resolution
-// A marker cell of chunk k with prefix offset `off` names the byte `off`
-// positions before chunk k's first byte, i.e. cell 32767-off of chunk k's
-// predecessor window WIN_k = output positions [start_k - 32768, start_k).
-// Resolution runs in three steps (the B200 form of the reference's serial
-// tail chain, pipeline.rs:1045-1078, followed by resolve_markers,
-// speculative.rs:175-213):
-//   k_win_init   every window cell becomes a resolved byte, an INVALID mark
-//                (position before the chunk's member), or a pointer to the
-//                window cell its own marker names (always in an earlier window);
-//   k_win_chase  every pointer follows its chain to a byte and is overwritten
-//                in place, so later chases stop early (pointers only lead to
-//                earlier windows, so every chain ends);
-//   k_resolve    every cell of every chunk becomes its byte with at most one
-//                gather from its chunk's window; cells are compacted into the
-//                contiguous output with 16-byte stores.
-constexpr uint32_t WIN_BYTE = 0x80000000u;     // resolved: low 8 bits = byte
-constexpr uint32_t WIN_INVALID = 0xC0000000u;  // resolved to an error
+// A marker cell 0x8000|m of chunk k names the output byte m + 1 positions
+// before chunk k's first byte (speculative.rs:12-17, :41), so every marker
+// points into W_k, the 32 KiB of output before chunk k. The reference builds
+// W_{k+1} from W_k one chunk after another (the tail chain,
+// pipeline.rs:1045-1078) and then resolves each chunk against its window
+// (resolve_markers, speculative.rs:175-213). Marker chains are long (the
+// first occurrence of a frequent word may lie many chunks back), so the chain
+// is restated as composition of window maps. A window map describes each of
+// the 32768 bytes of a window as a literal, a position in an earlier base
+// window (WM_REF | index) or an unresolvable byte (WM_BAD). Four kernels:
+//   k_win_maps    one block per group of consecutive chunks of a job: R_k,
+//                 the map of W_{k+1} relative to the group's first window, is
+//                 built chunk after chunk in shared memory from chunk k's last
+//                 32 KiB of cells and R_{k-1} (one gather per byte);
+//   k_win_bases   one block per job: the groups' first windows as bytes, one
+//                 group after another (one gather per byte per group);
+//   k_res_tails   the last 32 KiB of every chunk: R_k through its group's
+//                 base window straight into the output;
+//   k_res_heads   every other cell with at most one gather from the 32 KiB of
+//                 output before its chunk, staged in shared memory once per
+//                 64 Ki-cell segment; cells read 16 bytes at a time, bytes
+//                 written as aligned 8-byte words.
+// Device traffic: 2 bytes read and 1 written per cell, plus about 6 bytes per
+// window byte for the maps.
 constexpr int RES_THREADS = 256;
-constexpr int RES_PER_THREAD = 16;
-constexpr int RES_TILE = RES_THREADS * RES_PER_THREAD;
+constexpr int RES_CELLS = 8;                             // cells per thread per step (one 16-byte load)
+constexpr int RES_TAIL_TILE = RES_THREADS * RES_CELLS;   // window bytes per tail tile
+constexpr uint64_t RES_HEAD_SEG = 65536;                 // head cells per window staging
+constexpr int WM_THREADS = 1024;
+constexpr uint32_t WM_REF = 0x8000u;  // | index into the base window
+constexpr uint32_t WM_BAD = 0x4000u;  // the byte lies before its member (or the output)
 
-struct ResolveArgs {
-    const uint16_t* cells;
-    const ResolveChunk* chunks;
-    const uint64_t* tile_start;  // n_chunks + 1 prefix of tiles per chunk
-    const uint32_t* tile_chunk;  // n_tiles: the chunk each tile belongs to
-    uint32_t n_chunks;
-    uint64_t n_tiles;
-    uint8_t* out;
-    uint32_t* win;           // n_chunks * WINDOW entries
-    uint32_t* err;           // [0] flag, [1] chunk, [2] cell lo, [3] cell hi
-    unsigned long long* markers;  // count of marker cells resolved
-    uint8_t* winb;           // n_chunks * WINDOW: the resolved windows as bytes
-    uint32_t* win_bad;       // n_chunks: 1 if the chunk's window holds an INVALID entry
+struct ResGroup {
+    uint32_t first;  // first chunk
+    uint32_t n;      // consecutive chunks
+};
+struct ResJob {
+    uint32_t first;  // first group
+    uint32_t n;      // consecutive groups
 };
 
-__global__ void __launch_bounds__(256) k_win_init(ResolveArgs A) {
-    const uint64_t total = (uint64_t)A.n_chunks * WINDOW;
-    for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < total;
-         c += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t k = (uint32_t)(c / WINDOW), i = (uint32_t)(c % WINDOW);
-        const ResolveChunk ck = A.chunks[k];
-        uint32_t w;
-        if (ck.out_start + i < (uint64_t)WINDOW || ck.out_start + i - WINDOW < ck.member_start) {
-            w = WIN_INVALID;
-        } else if (ck.out_start + i - WINDOW < ck.job_out) {
-            w = WIN_BYTE | A.out[ck.out_start + i - WINDOW];  // a stripe's prefix, written by the previous call
-        } else {
-            const uint64_t g = ck.out_start + i - WINDOW;  // < out_start of chunk k
-            uint32_t j = k;
-            do {
-                j--;
-            } while (j > 0 && A.chunks[j].out_start > g);
-            const ResolveChunk cj = A.chunks[j];
-            if (j >= k || g < cj.out_start || g - cj.out_start >= cj.n_cells) {
-                w = WIN_INVALID;  // unreachable for a consistent chunk table
-            } else {
-                const uint32_t v = A.cells[cj.slot_off + (g - cj.out_start)];
-                w = (v & MARKER16) ? (j * WINDOW + (WINDOW - 1 - (v & 0x7fffu))) : (WIN_BYTE | v);
-            }
+struct ResolveArgs {
+    uint16_t* cells;
+    const ResolveChunk* chunks;
+    uint32_t n_chunks;
+    const ResGroup* groups;
+    uint32_t n_groups;
+    const ResJob* jobs;
+    uint32_t n_jobs;
+    const uint32_t* chunk_group;  // n_chunks
+    const uint64_t* tail_tiles;   // n_chunks + 1: prefix of each chunk's tail tiles
+    const uint64_t* head_segs;    // n_chunks + 1: prefix of each chunk's head segments
+    uint16_t* maps;               // n_chunks x WINDOW: R_k
+    uint16_t* bases;              // n_groups x WINDOW: each group's first window (byte or WM_BAD)
+    uint8_t* out;
+    uint32_t* err;                // [0] flag, [1] chunk, [2] cell lo, [3] cell hi
+    unsigned long long* markers;  // count of marker cells resolved
+};
+
+// Cells of a chunk that the head kernel resolves: all but the last 32 KiB.
+__host__ __device__ __forceinline__ uint64_t res_head_end(uint64_t n) { return n > WINDOW ? n - WINDOW : 0; }
+// First window index of R_k that lies inside chunk k.
+__host__ __device__ __forceinline__ uint32_t res_tail_lo(uint64_t n) {
+    return n >= WINDOW ? 0u : (uint32_t)(WINDOW - n);
+}
+
+// The chunk owning work unit t: the largest k with pre[k] <= t (pre[0] = 0,
+// pre[n] > t).
+__device__ __forceinline__ uint32_t res_unit_chunk(const uint64_t* pre, uint32_t n, uint64_t t) {
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (pre[mid] <= t) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// The warp's 32 lanes hold the bytes of output positions [p, p + 256) as one
+// little-endian 64-bit word each (lane l: bytes p + 8l .. p + 8l + 7); bytes
+// [lo, n) of that span are written. A whole span goes out as aligned 8-byte
+// words, the two words it shares with its neighbours byte by byte; anything
+// else byte by byte.
+__device__ __forceinline__ void warp_store8(uint8_t* dst, uint64_t v, uint32_t lo, uint32_t n, int lane) {
+    const uint32_t mis = (uint32_t)((uintptr_t)dst & 7u);
+    const uint64_t prev = __shfl_up_sync(FULLMASK, v, 1);
+    if (lo == 0 && n == 32u * RES_CELLS) {
+        if (mis == 0) {
+            *reinterpret_cast<uint64_t*>(dst + 8 * lane) = v;
+            return;
         }
-        A.win[c] = w;
+        uint8_t* al = dst - mis;
+        if (lane > 0) *reinterpret_cast<uint64_t*>(al + 8 * lane) = (v << (8 * mis)) | (prev >> (64 - 8 * mis));
+        else
+            for (uint32_t b = 0; b < 8 - mis; b++) dst[b] = (uint8_t)(v >> (8 * b));
+        if (lane == 31)
+            for (uint32_t b = 8 - mis; b < 8; b++) dst[8 * 31 + b] = (uint8_t)(v >> (8 * b));
+        return;
+    }
+    for (uint32_t b = 0; b < 8; b++) {
+        const uint32_t x = 8u * lane + b;
+        if (x >= lo && x < n) dst[x] = (uint8_t)(v >> (8 * b));
     }
 }
 
-__global__ void __launch_bounds__(256) k_win_chase(ResolveArgs A) {
-    const uint64_t total = (uint64_t)A.n_chunks * WINDOW;
-    // Plain loads: a chain may see a cell before or after its owner resolved
-    // it; a pointer and the byte it resolves to lead to the same byte.
-    uint32_t* win = A.win;
-    for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < total;
-         c += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t w = win[c];
-        if (!(w & WIN_BYTE)) {
-            uint32_t t = w;
-            uint64_t prev_win = c / WINDOW;
-            for (;;) {  // every hop must reach a strictly earlier window: at most n_chunks steps
-                if ((uint64_t)(t / WINDOW) >= prev_win) {
-                    w = WIN_INVALID;
-                    break;
-                }
-                prev_win = t / WINDOW;
-                w = win[t];
-                if (w & WIN_BYTE) break;
-                t = w;
-            }
-            win[c] = w;
-        }
-        // the byte copy k_resolve gathers from (a quarter of the u32 window's bytes)
-        A.winb[c] = (uint8_t)w;
-        if (w == WIN_INVALID) A.win_bad[c / WINDOW] = 1u;
+__device__ __forceinline__ void res_fail(const ResolveArgs& A, uint32_t k, uint64_t cell) {
+    if (atomicCAS(A.err, 0u, 1u) == 0u) {  // the first unresolvable cell names its chunk
+        A.err[1] = k;
+        A.err[2] = (uint32_t)cell;
+        A.err[3] = (uint32_t)(cell >> 32);
     }
 }
 
-// At most 64 registers: four resident blocks per SM instead of three, more
-// gathers in flight for this latency-bound kernel (3.36 -> 3.10 ms of resolve
-// per GiB of Zipf text).
-__global__ void __launch_bounds__(RES_THREADS, 4) k_resolve(ResolveArgs A) {
-    // Two staging buffers, so one barrier per tile separates a tile's staging
-    // from its stores. A tile's bytes sit at the output's alignment within the
-    // buffer, so whole 16-byte words move with one shared load and one store.
-    __shared__ __align__(16) uint8_t stage[2][RES_TILE + 32];
+// Dynamic shared memory: two maps (R_{k-1}, R_k) and the chunk's last 32 KiB
+// of cells (plus 8 for the 16-byte-aligned staging).
+constexpr size_t WM_SMEM = (size_t)(3 * WINDOW + 8) * 2;
+
+__global__ void __launch_bounds__(WM_THREADS, 1) k_win_maps(ResolveArgs A) {
+    RRG_DYN_SMEM(sm);
+    uint16_t* maps2 = reinterpret_cast<uint16_t*>(sm);  // two maps, alternating by step
+    uint16_t* stage = maps2 + 2 * WINDOW;
     uint32_t nmk = 0;
-    int buf = 0;
-    for (uint64_t t = blockIdx.x; t < A.n_tiles; t += gridDim.x, buf ^= 1) {
-        const uint32_t k = A.tile_chunk[t];
-        const ResolveChunk ck = A.chunks[k];
-        const uint32_t* win = A.win + (uint64_t)k * WINDOW;
-        const uint8_t* winb = A.winb + (uint64_t)k * WINDOW;
-        const bool win_clean = A.win_bad[k] == 0u;  // uniform over the tile
-        const uint64_t c0 = (t - A.tile_start[k]) * (uint64_t)RES_TILE;
-        const uint32_t cn = (uint32_t)(ck.n_cells - c0 < (uint64_t)RES_TILE ? ck.n_cells - c0 : (uint64_t)RES_TILE);
-        uint8_t* dst = A.out + ck.out_start + c0;
-        const uint32_t mis = (uint32_t)((uintptr_t)dst & 15);
-        uint8_t* sb = stage[buf];
-        // warp w owns cells [512w, 512w + 512) of the tile, lane ln the cells
-        // 512w + ln + 32i: one gather instruction covers 32 consecutive cells,
-        // whose window sources are mostly consecutive too (copied runs), so a
-        // warp's gathers touch few cache lines
-        const uint32_t wbase = (threadIdx.x >> 5) * (32 * RES_PER_THREAD), ln = threadIdx.x & 31;
-        uint32_t bad = 0;
-        if (wbase < cn) {
-            const uint16_t* p = A.cells + ck.slot_off + c0 + wbase + ln;
-            const uint32_t lim = cn - wbase;  // cells of this warp's span that exist
-            uint32_t cell[RES_PER_THREAD];
-#pragma unroll
-            for (int i = 0; i < RES_PER_THREAD; i++) cell[i] = (ln + 32u * i < lim) ? p[32 * i] : 0u;
-            // independent gathers: all issued before any is consumed
-            uint32_t got[RES_PER_THREAD];
-            if (win_clean) {
-#pragma unroll
-                for (int i = 0; i < RES_PER_THREAD; i++)
-                    got[i] = WIN_BYTE | ((cell[i] & MARKER16) ? (uint32_t)winb[WINDOW - 1 - (cell[i] & 0x7fffu)] : cell[i]);
-            } else {
-#pragma unroll
-                for (int i = 0; i < RES_PER_THREAD; i++)
-                    got[i] = (cell[i] & MARKER16) ? win[WINDOW - 1 - (cell[i] & 0x7fffu)] : (WIN_BYTE | cell[i]);
-            }
-#pragma unroll
-            for (int i = 0; i < RES_PER_THREAD; i++) {
-                if (ln + 32u * i < lim) {
-                    nmk += (cell[i] & MARKER16) ? 1u : 0u;
-                    if (got[i] == WIN_INVALID || !(got[i] & WIN_BYTE)) bad = 1;
-                    sb[mis + wbase + ln + 32 * i] = (uint8_t)got[i];
+    for (uint32_t g = blockIdx.x; g < A.n_groups; g += gridDim.x) {
+        const ResGroup G = A.groups[g];
+        for (uint32_t t = 0; t < G.n; t++) {
+            const uint32_t k = G.first + t;
+            const ResolveChunk ck = A.chunks[k];
+            const uint64_t n = ck.n_cells, end = ck.out_start + n;
+            // stage cells [c_lo, n) with aligned 16-byte loads from cell s0
+            // (the slot starts on an 8-cell boundary); stage[x] = cell s0 + x
+            const uint64_t c_lo = n > WINDOW ? n - WINDOW : 0, s0 = c_lo & ~7ull;
+            const uint4* src = reinterpret_cast<const uint4*>(A.cells + ck.slot_off + s0);
+            const uint32_t nq = (uint32_t)((n - s0 + 7) / 8);
+            for (uint32_t q = threadIdx.x; q < nq; q += blockDim.x)
+                reinterpret_cast<uint4*>(stage)[q] = src[q];
+            __syncthreads();  // also: the previous step's map is complete
+            const uint16_t* prv = maps2 + ((t + 1) & 1) * WINDOW;
+            uint16_t* cur = maps2 + (t & 1) * WINDOW;
+            uint16_t* Rk = A.maps + (uint64_t)k * WINDOW;
+            for (uint32_t i = threadIdx.x; i < WINDOW; i += blockDim.x) {
+                uint32_t r, j = 0;
+                bool gather = false;
+                if (end < (uint64_t)(WINDOW - i)) {
+                    r = WM_BAD;  // before the output's start
+                } else if (end - WINDOW + i >= ck.out_start) {
+                    const uint32_t v = stage[end - WINDOW + i - ck.out_start - s0];
+                    if (!(v & MARKER16)) {
+                        r = v;
+                    } else {
+                        const uint64_t m = v & 0x7fffu;
+                        nmk++;
+                        if (ck.out_start < m + 1 || ck.out_start - 1 - m < ck.member_start) {
+                            r = WM_BAD;
+                        } else {
+                            j = WINDOW - 1 - (uint32_t)m;
+                            gather = true;
+                        }
+                    }
+                } else {
+                    j = (uint32_t)n + i;  // a short chunk: the byte lies in W_k
+                    gather = true;
                 }
+                if (gather) r = t ? prv[j] : (WM_REF | j);
+                cur[i] = (uint16_t)r;
+                Rk[i] = (uint16_t)r;
             }
-        }
-        if (bad && atomicCAS(A.err, 0u, 1u) == 0u) {  // the first unresolvable cell names its chunk
-            A.err[1] = k;
-            A.err[2] = (uint32_t)c0;
-            A.err[3] = (uint32_t)(c0 >> 32);
-        }
-        __syncthreads();
-        // words of the aligned output covering bytes [mis, mis + cn) of the buffer
-        uint8_t* dst_al = dst - mis;
-        const uint32_t nwords = (mis + cn + 15) / 16;
-        for (uint32_t w = threadIdx.x; w < nwords; w += blockDim.x) {
-            const uint32_t b0 = w * 16, b1 = b0 + 16;
-            if (b0 >= mis && b1 <= mis + cn) {
-                *reinterpret_cast<uint4*>(dst_al + b0) = *reinterpret_cast<const uint4*>(sb + b0);
-            } else {
-                for (uint32_t j = (b0 > mis ? b0 : mis); j < (b1 < mis + cn ? b1 : mis + cn); j++) dst_al[j] = sb[j];
-            }
+            __syncthreads();  // the staging buffer is free again
         }
     }
     nmk = warp_sum(nmk);
     if ((threadIdx.x & 31) == 0 && nmk) atomicAdd(A.markers, (unsigned long long)nmk);
+}
+
+// Each job's groups in order: the first group's base window is the 32 KiB
+// before the job (a stripe's prefix, already in the output, or WM_BAD); each
+// next base applies the previous group's last map to the previous base.
+__global__ void __launch_bounds__(WM_THREADS, 1) k_win_bases(ResolveArgs A) {
+    RRG_DYN_SMEM(sm);
+    uint16_t* cur = reinterpret_cast<uint16_t*>(sm);
+    constexpr uint32_t PER = WINDOW / WM_THREADS;
+    for (uint32_t jb = blockIdx.x; jb < A.n_jobs; jb += gridDim.x) {
+        const ResJob J = A.jobs[jb];
+        for (uint32_t q = 0; q < J.n; q++) {
+            const uint32_t g = J.first + q;
+            uint16_t* B = A.bases + (uint64_t)g * WINDOW;
+            uint32_t nv[PER];
+            if (q == 0) {
+                const ResolveChunk ck = A.chunks[A.groups[g].first];
+#pragma unroll
+                for (uint32_t e = 0; e < PER; e++) {
+                    const uint32_t i = threadIdx.x + e * WM_THREADS;
+                    uint32_t r = WM_BAD;
+                    if (ck.out_start >= (uint64_t)(WINDOW - i)) {
+                        const uint64_t pos = ck.out_start - WINDOW + i;
+                        if (pos >= ck.member_start && pos < ck.job_out) r = A.out[pos];
+                    }
+                    nv[e] = r;
+                }
+            } else {
+                const ResGroup P = A.groups[g - 1];
+                const uint16_t* R = A.maps + (uint64_t)(P.first + P.n - 1) * WINDOW;
+#pragma unroll
+                for (uint32_t e = 0; e < PER; e++) nv[e] = R[threadIdx.x + e * WM_THREADS];
+#pragma unroll
+                for (uint32_t e = 0; e < PER; e++)
+                    if (nv[e] & WM_REF) nv[e] = cur[nv[e] & 0x7fffu];
+            }
+            __syncthreads();  // every read of the previous base is done
+#pragma unroll
+            for (uint32_t e = 0; e < PER; e++) {
+                cur[threadIdx.x + e * WM_THREADS] = (uint16_t)nv[e];
+                B[threadIdx.x + e * WM_THREADS] = (uint16_t)nv[e];
+            }
+            __syncthreads();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(RES_THREADS) k_res_tails(ResolveArgs A) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t n_tiles = A.tail_tiles[A.n_chunks];
+    for (uint64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        const uint32_t k = res_unit_chunk(A.tail_tiles, A.n_chunks, t);
+        const ResolveChunk ck = A.chunks[k];
+        const uint32_t i_lo = res_tail_lo(ck.n_cells);
+        // window index of this warp's first byte; tiles cover [i_lo & ~(TILE-1), WINDOW)
+        const uint32_t i0 = (i_lo & ~(uint32_t)(RES_TAIL_TILE - 1)) +
+                            (uint32_t)(t - A.tail_tiles[k]) * RES_TAIL_TILE + warp * (32 * RES_CELLS);
+        if (i0 + 32 * RES_CELLS <= i_lo) continue;  // warp-uniform: entirely before the chunk
+        const uint16_t* R = A.maps + (uint64_t)k * WINDOW;
+        const uint16_t* B = A.bases + (uint64_t)A.chunk_group[k] * WINDOW;
+        const uint4 q = reinterpret_cast<const uint4*>(R + i0)[lane];
+        const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+        uint64_t v = 0;
+        bool bad = false;
+#pragma unroll
+        for (int e = 0; e < RES_CELLS; e++) {
+            const uint32_t i = i0 + RES_CELLS * lane + e;
+            uint32_t r = (w[e >> 1] >> (16 * (e & 1))) & 0xffffu;
+            if (r & WM_REF) r = B[r & 0x7fffu];
+            if (i >= i_lo) bad |= (r & WM_BAD) != 0;
+            v |= (uint64_t)(r & 0xffu) << (8 * e);
+        }
+        if (bad) res_fail(A, k, i0);
+        // window index i is output byte out_start + n - WINDOW + i
+        uint8_t* dst = A.out + (ck.out_start + ck.n_cells - WINDOW + i0);
+        warp_store8(dst, v, i_lo > i0 ? i_lo - i0 : 0u, 32u * RES_CELLS, lane);
+    }
+}
+
+// Four blocks per SM: 4 x 32 KiB windows in shared memory.
+__global__ void __launch_bounds__(RES_THREADS, 4) k_res_heads(ResolveArgs A) {
+    __shared__ __align__(16) uint8_t win[WINDOW + 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t n_segs = A.head_segs[A.n_chunks];
+    uint32_t nmk = 0;
+    for (uint64_t s = blockIdx.x; s < n_segs; s += gridDim.x) {
+        const uint32_t k = res_unit_chunk(A.head_segs, A.n_chunks, s);
+        const ResolveChunk ck = A.chunks[k];
+        const uint64_t h_end = res_head_end(ck.n_cells);
+        const uint64_t s0 = (s - A.head_segs[k]) * RES_HEAD_SEG;
+        const uint64_t s1 = s0 + RES_HEAD_SEG < h_end ? s0 + RES_HEAD_SEG : h_end;
+        // markers of this chunk may name positions [out_start - lim, out_start)
+        const uint64_t lim = ck.out_start - ck.member_start;
+        // stage the 32 KiB before the chunk: whole aligned 16-byte words inside
+        // [w_lo, out_start), bytes at the edges; win[i] holds output byte wa + i
+        const uint64_t w_lo = ck.out_start > WINDOW ? ck.out_start - WINDOW : 0;
+        const uintptr_t a_lo = (uintptr_t)(A.out + w_lo) & ~(uintptr_t)15;
+        const uint64_t wa = (uint64_t)(a_lo - (uintptr_t)A.out);  // may sit up to 15 bytes before w_lo
+        __syncthreads();  // the previous segment's readers are done with win
+        for (uint64_t q = threadIdx.x; 16 * q < WINDOW + 16; q += blockDim.x) {
+            const uint64_t p = wa + 16 * q;  // relative to A.out, p + 16 > w_lo
+            if (p >= ck.out_start) break;
+            if (p >= w_lo && p + 16 <= ck.out_start) {
+                *reinterpret_cast<uint4*>(win + 16 * q) = *reinterpret_cast<const uint4*>(A.out + p);
+            } else {
+                for (int b = 0; b < 16; b++)
+                    if (p + b >= w_lo && p + b < ck.out_start) win[16 * q + b] = A.out[p + b];
+            }
+        }
+        __syncthreads();
+        const uint64_t wbase = ck.out_start - 1 - wa;  // win index of the byte before the chunk
+        for (uint64_t c0 = s0 + (uint64_t)warp * (32 * RES_CELLS); c0 < s1; c0 += RES_THREADS * RES_CELLS) {
+            const uint64_t left = s1 - c0;
+            const uint32_t n = left < 32u * RES_CELLS ? (uint32_t)left : 32u * RES_CELLS;
+            const uint64_t ci = c0 + (uint64_t)RES_CELLS * lane;
+            uint4 q = make_uint4(0, 0, 0, 0);
+            if (ci < s1) q = *reinterpret_cast<const uint4*>(A.cells + ck.slot_off + ci);
+            const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+            uint64_t v = 0;
+            bool bad = false;
+#pragma unroll
+            for (int i = 0; i < RES_CELLS; i++) {
+                const uint32_t cl = (w[i >> 1] >> (16 * (i & 1))) & 0xffffu;
+                uint32_t b = cl;
+                if ((cl & MARKER16) && ci + i < s1) {  // cells past s1 belong to the tail
+                    const uint32_t m = cl & 0x7fffu;
+                    nmk++;
+                    // m < lim keeps wbase - m inside the staged bytes
+                    if ((uint64_t)m < lim) b = win[wbase - m];
+                    else bad = true;
+                }
+                v |= (uint64_t)(b & 0xffu) << (8 * i);
+            }
+            if (bad) res_fail(A, k, ci);
+            warp_store8(A.out + ck.out_start + c0, v, 0u, n, lane);
+        }
+    }
+    nmk = warp_sum(nmk);
+    if (lane == 0 && nmk) atomicAdd(A.markers, (unsigned long long)nmk);
+}
+
+// The reference-shaped entry point's scatter (speculative.rs:175-213):
+// bytes[out_pos[i]] = tail[tail_len - 1 - prefix_offset[i]].
+__global__ void k_resolve_list(uint8_t* bytes, uint64_t n_bytes, const uint32_t* out_pos, const uint16_t* prefix_off,
+                               uint64_t n_markers, const uint8_t* tail, uint64_t tail_len, uint32_t* err) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_markers;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t o = prefix_off[i], p = out_pos[i];
+        if (o >= tail_len || p >= n_bytes) {
+            atomicOr(err, 1u);
+            continue;
+        }
+        bytes[p] = tail[tail_len - 1 - o];
+    }
 }
 
 // ------------------------------------------------------- CRC-32

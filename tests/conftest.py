@@ -13,7 +13,10 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-REFERENCE_CORPUS = "/root/reference/tests/corpus"
+# The rusty_rapidgzip checkout whose committed corpus pins the oracle: set
+# RRG_REFERENCE_DIR to its root (the pinning test skips where it is absent).
+REFERENCE_DIR = os.environ.get("RRG_REFERENCE_DIR", "/root/reference")
+REFERENCE_CORPUS = os.path.join(REFERENCE_DIR, "tests", "corpus")
 EMU_DIR = os.path.join(ROOT, "tests", "emu")
 EMU_LIB = os.path.join(EMU_DIR, "librrg_gpu_emu.so")
 

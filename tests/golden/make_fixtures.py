@@ -10,7 +10,8 @@
    crates/rusty-rapidgzip/tests/miri_edge.rs, read from that file as text.
 3. ``sums.json`` — file -> {sha256, raw_size, pinned_to_reference}.
 
-Run in a checkout that has the reference next to it:
+Run with the reference checkout's root as the argument, or in
+RRG_REFERENCE_DIR:
     python tests/golden/make_fixtures.py [/path/to/rusty_rapidgzip]
 """
 from __future__ import annotations
@@ -23,7 +24,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("RRG_REFERENCE_DIR", "/root/reference")
 
 PAYLOADS = {
     "synth-empty.gz": (b"", 6),

@@ -450,3 +450,67 @@ def test_seek_index(emu_decoder_factory):
     with pytest.raises(RrgError) as e3:
         d.read_range(data, idx, len(want) - 5, 10)
     assert e1.value.code == e2.value.code == e3.value.code == 22  # RRG_ERR_INVALID_ARGUMENT
+
+
+def test_seek_index_images_are_checked(emu_decoder_factory):
+    """Index images that are truncated, or whose checkpoints lie past the end
+    of the file, out of order or with more window than output, are refused
+    when loaded; nothing reaches a decode."""
+    import struct as S
+    from conftest import build_emu_lib
+    from rusty_rapidgzip_b200 import RrgError, SeekIndex
+    raw, gz = W.config1(300 << 10, seed=16)
+    d = emu_decoder_factory(gpu_chunk_bytes=8192)
+    idx = d.build_index(gz, spacing=32 << 10)
+    blob = idx.serialize()
+    lib = build_emu_lib()
+    assert SeekIndex.load(blob, lib=lib).points() == idx.points()
+    file_len, body_off, total_out, cnt = S.unpack_from("<QQQQ", blob, 8)
+    assert cnt >= 3
+
+    def cps(b):  # offsets of each checkpoint record
+        out, p = [], 40
+        for _ in range(cnt):
+            out.append(p)
+            p += 20 + S.unpack_from("<I", b, p + 16)[0]
+        return out
+
+    recs = cps(blob)
+
+    def patched(rec, field, value, fmt="<Q"):
+        b = bytearray(blob)
+        S.pack_into(fmt, b, recs[rec] + field, value)
+        return bytes(b)
+
+    bad = {
+        "truncated": blob[: len(blob) - 100],
+        "header only": blob[:40],
+        "huge bit": patched(1, 0, 1 << 62),
+        "bit past the end": patched(2, 0, (file_len - body_off) * 8),
+        "bits out of order": patched(2, 0, S.unpack_from("<Q", blob, recs[1])[0]),
+        "body past the end": blob[:16] + S.pack("<Q", file_len) + blob[24:],
+        "window longer than the output": patched(1, 8, 100),
+    }
+    for name, b in bad.items():
+        with pytest.raises(RrgError) as e:
+            SeekIndex.load(b, lib=lib)
+        assert e.value.code == 22, name  # RRG_ERR_INVALID_ARGUMENT
+
+
+def test_resolve_long_chunks_and_unaligned_output(emu_decoder_factory):
+    """Sub-chunks far longer than the 32 KiB window: their tails resolve by
+    chasing markers through earlier chunks' cells, the rest in several 64 Ki
+    cell segments from the staged window. Output starts at odd addresses, so
+    every 8-byte word store is realigned; bytes outside the output stay put."""
+    raw, gz = W.config1(1200 << 10, seed=17)
+    d = emu_decoder_factory(gpu_chunk_bytes=120 << 10)
+    out = []
+    st = d.decode_host(gz, out.append)
+    assert b"".join(out) == raw
+    assert st.gpu_chunks >= 3 and st.markers > 0 and st.speculation_failures == 0
+    src = np.frombuffer(gz, dtype=np.uint8).copy()
+    for shift in (3, 5):
+        dst = np.full(len(raw) + 16, 0xA5, dtype=np.uint8)
+        n, st2 = d.decode_device(haddr(src), len(gz), haddr(dst) + shift, len(raw))
+        assert n == len(raw) and dst[shift:shift + n].tobytes() == raw
+        assert (dst[:shift] == 0xA5).all() and (dst[shift + n:] == 0xA5).all()

@@ -36,5 +36,28 @@ def test_noalloc_crc_matches_context_entry_point(gpu_lib):
         stream = torch.cuda.Stream()
         buf = _dev(big)
         assert crc32_noalloc(buf, len(big), stream=stream.cuda_stream, lib=gpu_lib) == zlib.crc32(big)
+        # unaligned starts: every 256 KiB piece keeps the input's misalignment
+        for shift in (1, 3, 7):
+            n = len(big) - shift
+            assert crc32_noalloc(buf[shift:], n, lib=gpu_lib) == d.crc32(buf[shift:], n) == zlib.crc32(big[shift:])
         with pytest.raises(CapacityError, match="at most"):
             crc32_noalloc(buf, (4 << 30) + 1, lib=gpu_lib)
+
+
+def test_noalloc_crc_at_its_size_limit(gpu_lib):
+    """Exactly 4 GiB is accepted and agrees with the context-based entry point
+    (whose kernels differ); one byte more is refused."""
+    import torch
+    from rusty_rapidgzip_b200 import CapacityError, Config, Decoder
+    from rusty_rapidgzip_b200._abi import crc32_noalloc
+    n = 4 << 30
+    g = torch.Generator(device="cuda")
+    g.manual_seed(11)
+    buf = torch.randint(0, 256, (n,), dtype=torch.uint8, device="cuda", generator=g)
+    torch.cuda.synchronize()
+    with Decoder(Config(device=0), lib=gpu_lib) as d:
+        want = d.crc32(buf, n)
+    for _ in range(2):
+        assert crc32_noalloc(buf, n, lib=gpu_lib) == want
+    with pytest.raises(CapacityError, match="at most"):
+        crc32_noalloc(buf, n + 1, lib=gpu_lib)
