@@ -2271,57 +2271,88 @@ __device__ __forceinline__ void res_fail(const ResolveArgs& A, uint32_t k, uint6
 }
 
 // Dynamic shared memory: two maps (R_{k-1}, R_k) and the chunk's last 32 KiB
-// of cells (plus 8 for the 16-byte-aligned staging).
+// of cells (staged from an 8-cell boundary, so 8 more).
 constexpr size_t WM_SMEM = (size_t)(3 * WINDOW + 8) * 2;
+constexpr uint32_t WM_VEC = WINDOW / (8 * WM_THREADS);  // 8-entry vectors per thread per map
+
+__device__ __forceinline__ uint32_t u16_of(const uint4& q, int e) {
+    const uint32_t w = e < 2 ? q.x : e < 4 ? q.y : e < 6 ? q.z : q.w;
+    return (w >> (16 * (e & 1))) & 0xffffu;
+}
+__device__ __forceinline__ uint4 pack_u16x8(const uint32_t (&r)[8]) {
+    return make_uint4(r[0] | (r[1] << 16), r[2] | (r[3] << 16), r[4] | (r[5] << 16), r[6] | (r[7] << 16));
+}
+
+// Cells [s0, n) of chunk k as 16-byte words, WM_VEC per thread (zeros past the end).
+__device__ __forceinline__ void wm_load(const ResolveArgs& A, uint32_t k, uint4 (&v)[WM_VEC]) {
+    const ResolveChunk ck = A.chunks[k];
+    const uint64_t n = ck.n_cells, s0 = (n > WINDOW ? n - WINDOW : 0) & ~7ull;
+    const uint4* src = reinterpret_cast<const uint4*>(A.cells + ck.slot_off + s0);
+    const uint32_t nq = (uint32_t)((n - s0 + 7) / 8);
+#pragma unroll
+    for (uint32_t q = 0; q < WM_VEC; q++) {
+        const uint32_t x = threadIdx.x + q * WM_THREADS;
+        v[q] = x < nq ? src[x] : make_uint4(0, 0, 0, 0);
+    }
+}
 
 __global__ void __launch_bounds__(WM_THREADS, 1) k_win_maps(ResolveArgs A) {
     RRG_DYN_SMEM(sm);
     uint16_t* maps2 = reinterpret_cast<uint16_t*>(sm);  // two maps, alternating by step
-    uint16_t* stage = maps2 + 2 * WINDOW;
+    uint16_t* stage = maps2 + 2 * WINDOW;               // stage[x]: cell s0 + x of the chunk
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t nmk = 0;
     for (uint32_t g = blockIdx.x; g < A.n_groups; g += gridDim.x) {
         const ResGroup G = A.groups[g];
+        uint4 nxt[WM_VEC];
+        wm_load(A, G.first, nxt);
         for (uint32_t t = 0; t < G.n; t++) {
             const uint32_t k = G.first + t;
             const ResolveChunk ck = A.chunks[k];
             const uint64_t n = ck.n_cells, end = ck.out_start + n;
-            // stage cells [c_lo, n) with aligned 16-byte loads from cell s0
-            // (the slot starts on an 8-cell boundary); stage[x] = cell s0 + x
             const uint64_t c_lo = n > WINDOW ? n - WINDOW : 0, s0 = c_lo & ~7ull;
-            const uint4* src = reinterpret_cast<const uint4*>(A.cells + ck.slot_off + s0);
             const uint32_t nq = (uint32_t)((n - s0 + 7) / 8);
-            for (uint32_t q = threadIdx.x; q < nq; q += blockDim.x)
-                reinterpret_cast<uint4*>(stage)[q] = src[q];
+#pragma unroll
+            for (uint32_t q = 0; q < WM_VEC; q++) {
+                const uint32_t x = threadIdx.x + q * WM_THREADS;
+                if (x < nq) reinterpret_cast<uint4*>(stage)[x] = nxt[q];
+            }
+            if (nq > WM_VEC * WM_THREADS && threadIdx.x == 0)  // the 4097th word of a misaligned tail
+                reinterpret_cast<uint4*>(stage)[WM_VEC * WM_THREADS] =
+                    reinterpret_cast<const uint4*>(A.cells + ck.slot_off + s0)[WM_VEC * WM_THREADS];
             __syncthreads();  // also: the previous step's map is complete
+            if (t + 1 < G.n) wm_load(A, k + 1, nxt);  // in flight while this step computes
             const uint16_t* prv = maps2 + ((t + 1) & 1) * WINDOW;
             uint16_t* cur = maps2 + (t & 1) * WINDOW;
             uint16_t* Rk = A.maps + (uint64_t)k * WINDOW;
-            for (uint32_t i = threadIdx.x; i < WINDOW; i += blockDim.x) {
-                uint32_t r, j = 0;
-                bool gather = false;
-                if (end < (uint64_t)(WINDOW - i)) {
-                    r = WM_BAD;  // before the output's start
-                } else if (end - WINDOW + i >= ck.out_start) {
-                    const uint32_t v = stage[end - WINDOW + i - ck.out_start - s0];
-                    if (!(v & MARKER16)) {
-                        r = v;
-                    } else {
-                        const uint64_t m = v & 0x7fffu;
-                        nmk++;
-                        if (ck.out_start < m + 1 || ck.out_start - 1 - m < ck.member_start) {
-                            r = WM_BAD;
-                        } else {
-                            j = WINDOW - 1 - (uint32_t)m;
-                            gather = true;
+            const uint64_t lim = ck.out_start - ck.member_start;  // markers m < lim stay inside the member
+            const uint32_t i_lo = res_tail_lo(n);
+            // stage index of window index i (for i >= i_lo)
+            const uint32_t off = (uint32_t)(c_lo - s0) - i_lo;
+            const bool plain = i_lo == 0 && end >= WINDOW;  // block-uniform: every entry is a cell
+            // lane-consecutive entries: conflict-free shared loads, coalesced stores
+            for (uint32_t sp = warp; sp < WINDOW / 256; sp += WM_THREADS / 32) {
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    const uint32_t i = sp * 256 + lane + 32 * e;
+                    const uint32_t si = i + off;  // wraps below i_lo of a short chunk (unused there)
+                    const uint32_t v = stage[si < WINDOW + 8 ? si : 0u];
+                    const uint32_t mk = v >> 15, m = v & 0x7fffu, j = WINDOW - 1 - m;
+                    const uint32_t via = t ? (uint32_t)prv[j] : (WM_REF | j);
+                    uint32_t r = mk ? ((uint64_t)m < lim ? via : WM_BAD) : v;
+                    nmk += mk;
+                    if (!plain) {
+                        if (end < (uint64_t)(WINDOW - i)) {
+                            r = WM_BAD;  // before the output's start
+                            nmk -= mk;
+                        } else if (i < i_lo) {
+                            r = t ? (uint32_t)prv[(uint32_t)n + i] : (WM_REF | ((uint32_t)n + i));  // lies in W_k
+                            nmk -= mk;
                         }
                     }
-                } else {
-                    j = (uint32_t)n + i;  // a short chunk: the byte lies in W_k
-                    gather = true;
+                    cur[i] = (uint16_t)r;
+                    Rk[i] = (uint16_t)r;
                 }
-                if (gather) r = t ? prv[j] : (WM_REF | j);
-                cur[i] = (uint16_t)r;
-                Rk[i] = (uint16_t)r;
             }
             __syncthreads();  // the staging buffer is free again
         }
@@ -2336,39 +2367,51 @@ __global__ void __launch_bounds__(WM_THREADS, 1) k_win_maps(ResolveArgs A) {
 __global__ void __launch_bounds__(WM_THREADS, 1) k_win_bases(ResolveArgs A) {
     RRG_DYN_SMEM(sm);
     uint16_t* cur = reinterpret_cast<uint16_t*>(sm);
-    constexpr uint32_t PER = WINDOW / WM_THREADS;
     for (uint32_t jb = blockIdx.x; jb < A.n_jobs; jb += gridDim.x) {
         const ResJob J = A.jobs[jb];
         for (uint32_t q = 0; q < J.n; q++) {
             const uint32_t g = J.first + q;
             uint16_t* B = A.bases + (uint64_t)g * WINDOW;
-            uint32_t nv[PER];
+            uint4 nv[WM_VEC];
             if (q == 0) {
                 const ResolveChunk ck = A.chunks[A.groups[g].first];
 #pragma unroll
-                for (uint32_t e = 0; e < PER; e++) {
-                    const uint32_t i = threadIdx.x + e * WM_THREADS;
-                    uint32_t r = WM_BAD;
-                    if (ck.out_start >= (uint64_t)(WINDOW - i)) {
-                        const uint64_t pos = ck.out_start - WINDOW + i;
-                        if (pos >= ck.member_start && pos < ck.job_out) r = A.out[pos];
+                for (uint32_t v = 0; v < WM_VEC; v++) {
+                    const uint32_t i0 = 8 * (threadIdx.x + v * WM_THREADS);
+                    uint32_t r[8];
+#pragma unroll
+                    for (int e = 0; e < 8; e++) {
+                        const uint32_t i = i0 + e;
+                        r[e] = WM_BAD;
+                        if (ck.out_start >= (uint64_t)(WINDOW - i)) {
+                            const uint64_t pos = ck.out_start - WINDOW + i;
+                            if (pos >= ck.member_start && pos < ck.job_out) r[e] = A.out[pos];
+                        }
                     }
-                    nv[e] = r;
+                    nv[v] = pack_u16x8(r);
                 }
             } else {
                 const ResGroup P = A.groups[g - 1];
-                const uint16_t* R = A.maps + (uint64_t)(P.first + P.n - 1) * WINDOW;
+                const uint4* R = reinterpret_cast<const uint4*>(A.maps + (uint64_t)(P.first + P.n - 1) * WINDOW);
 #pragma unroll
-                for (uint32_t e = 0; e < PER; e++) nv[e] = R[threadIdx.x + e * WM_THREADS];
+                for (uint32_t v = 0; v < WM_VEC; v++) nv[v] = R[threadIdx.x + v * WM_THREADS];
 #pragma unroll
-                for (uint32_t e = 0; e < PER; e++)
-                    if (nv[e] & WM_REF) nv[e] = cur[nv[e] & 0x7fffu];
+                for (uint32_t v = 0; v < WM_VEC; v++) {
+                    uint32_t r[8];
+#pragma unroll
+                    for (int e = 0; e < 8; e++) {
+                        const uint32_t x = u16_of(nv[v], e);
+                        r[e] = (x & WM_REF) ? (uint32_t)cur[x & 0x7fffu] : x;
+                    }
+                    nv[v] = pack_u16x8(r);
+                }
             }
             __syncthreads();  // every read of the previous base is done
 #pragma unroll
-            for (uint32_t e = 0; e < PER; e++) {
-                cur[threadIdx.x + e * WM_THREADS] = (uint16_t)nv[e];
-                B[threadIdx.x + e * WM_THREADS] = (uint16_t)nv[e];
+            for (uint32_t v = 0; v < WM_VEC; v++) {
+                const uint32_t i0 = 8 * (threadIdx.x + v * WM_THREADS);
+                *reinterpret_cast<uint4*>(cur + i0) = nv[v];
+                *reinterpret_cast<uint4*>(B + i0) = nv[v];
             }
             __syncthreads();
         }
@@ -2439,28 +2482,38 @@ __global__ void __launch_bounds__(RES_THREADS, 4) k_res_heads(ResolveArgs A) {
         }
         __syncthreads();
         const uint64_t wbase = ck.out_start - 1 - wa;  // win index of the byte before the chunk
-        for (uint64_t c0 = s0 + (uint64_t)warp * (32 * RES_CELLS); c0 < s1; c0 += RES_THREADS * RES_CELLS) {
+        const uint16_t* cells = A.cells + ck.slot_off;
+        constexpr uint64_t STEP = RES_THREADS * RES_CELLS;
+        // the next step's cells are loaded before this step's are processed
+        uint64_t c0 = s0 + (uint64_t)warp * (32 * RES_CELLS);
+        uint4 qn = make_uint4(0, 0, 0, 0);
+        if (c0 + RES_CELLS * lane < s1) qn = *reinterpret_cast<const uint4*>(cells + c0 + RES_CELLS * lane);
+        for (; c0 < s1; c0 += STEP) {
             const uint64_t left = s1 - c0;
             const uint32_t n = left < 32u * RES_CELLS ? (uint32_t)left : 32u * RES_CELLS;
             const uint64_t ci = c0 + (uint64_t)RES_CELLS * lane;
-            uint4 q = make_uint4(0, 0, 0, 0);
-            if (ci < s1) q = *reinterpret_cast<const uint4*>(A.cells + ck.slot_off + ci);
+            const uint4 q = qn;
+            qn = make_uint4(0, 0, 0, 0);
+            if (ci + STEP < s1) qn = *reinterpret_cast<const uint4*>(cells + ci + STEP);
             const uint32_t w[4] = {q.x, q.y, q.z, q.w};
-            uint64_t v = 0;
             bool bad = false;
+            // cells past s1 belong to the tail kernel
+            const uint32_t nvalid = ci < s1 ? (s1 - ci < RES_CELLS ? (uint32_t)(s1 - ci) : RES_CELLS) : 0u;
+            uint32_t lo32 = 0, hi32 = 0;
 #pragma unroll
             for (int i = 0; i < RES_CELLS; i++) {
                 const uint32_t cl = (w[i >> 1] >> (16 * (i & 1))) & 0xffffu;
-                uint32_t b = cl;
-                if ((cl & MARKER16) && ci + i < s1) {  // cells past s1 belong to the tail
-                    const uint32_t m = cl & 0x7fffu;
-                    nmk++;
-                    // m < lim keeps wbase - m inside the staged bytes
-                    if ((uint64_t)m < lim) b = win[wbase - m];
-                    else bad = true;
-                }
-                v |= (uint64_t)(b & 0xffu) << (8 * i);
+                const uint32_t mk = (cl >> 15) & ((uint32_t)i < nvalid ? 1u : 0u), m = cl & 0x7fffu;
+                // a marker m < lim reads win[wbase - m]; others read a clamped, unused byte
+                const uint32_t x = (uint32_t)wbase - m;
+                const uint32_t wb = win[x < WINDOW + 32 ? x : 0u];
+                const uint32_t b = mk ? wb : cl;
+                nmk += mk;
+                bad |= mk && (uint64_t)m >= lim;
+                if (i < 4) lo32 |= (b & 0xffu) << (8 * i);
+                else hi32 |= (b & 0xffu) << (8 * (i - 4));
             }
+            const uint64_t v = ((uint64_t)hi32 << 32) | lo32;
             if (bad) res_fail(A, k, ci);
             warp_store8(A.out + ck.out_start + c0, v, 0u, n, lane);
         }
