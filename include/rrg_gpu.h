@@ -79,6 +79,10 @@ typedef struct rrg_config {
                                     >= gpu_chunk_bytes apart; 1 = one search per target as
                                     find_next_dynamic_block does (block_finder.rs:109) */
     uint64_t hbm_budget_bytes;   /* serving admission budget; 0 = 120 GB */
+    int32_t host_pipeline;       /* rrg_gpu_decode_host/read_gz: 0 = decode a large single-member stream
+                                    in waves with the copy to the host overlapped (falls back to the
+                                    checked path on any irregularity); -1 = always the checked path */
+    int32_t reserved;
 } rrg_config;
 
 /* Mirrors DecodeStats (lib.rs:103-108), plus device-path counters. */
@@ -93,6 +97,8 @@ typedef struct rrg_stats {
     uint64_t kernel_launches;      /* kernels launched by this call */
     double finder_ms, inflate_ms, resolve_ms, crc_ms, h2d_ms, d2h_ms, total_ms;
     uint64_t graph_launches;       /* captured decode graphs replayed by this call (BGZF route) */
+    uint64_t pipeline_waves;       /* waves of the pipelined host path (0: not taken) */
+    uint64_t pipeline_fallbacks;   /* 1 when the pipelined path handed the rest to the checked path */
 } rrg_stats;
 
 /* Sink: called in stream order with consecutive pieces of decompressed output.

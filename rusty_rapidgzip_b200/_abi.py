@@ -76,6 +76,8 @@ class _Config(C.Structure):
         ("warps_per_stream", C.c_int32),
         ("boundary_mode", C.c_int32),
         ("hbm_budget_bytes", C.c_uint64),
+        ("host_pipeline", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 
@@ -99,7 +101,8 @@ class _ServeStats(C.Structure):
 
 class _Stats(C.Structure):
     _fields_ = ([(n, C.c_uint64) for n in _STAT_U64] + [(n, C.c_double) for n in _STAT_F64]
-                + [("graph_launches", C.c_uint64)])
+                + [("graph_launches", C.c_uint64), ("pipeline_waves", C.c_uint64),
+                   ("pipeline_fallbacks", C.c_uint64)])
 
 
 SINK_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_uint8), C.c_size_t)
@@ -119,6 +122,7 @@ class Config:
     warps_per_stream: int = 0
     boundary_mode: int = 0
     hbm_budget_bytes: int = 0
+    host_pipeline: int = 0  # -1: the host path never decodes in overlapped waves
 
     def _c(self) -> _Config:
         c = _Config()
@@ -131,6 +135,7 @@ class Config:
         c.warps_per_stream = self.warps_per_stream
         c.boundary_mode = self.boundary_mode
         c.hbm_budget_bytes = self.hbm_budget_bytes
+        c.host_pipeline = self.host_pipeline
         return c
 
 
@@ -146,11 +151,14 @@ class DecodeStats:
     members: int = 0
     kernel_launches: int = 0
     graph_launches: int = 0
+    pipeline_waves: int = 0
+    pipeline_fallbacks: int = 0
     timings_ms: dict = field(default_factory=dict)
 
     @classmethod
     def _from(cls, s: _Stats) -> "DecodeStats":
         return cls(**{n: int(getattr(s, n)) for n in _STAT_U64}, graph_launches=int(s.graph_launches),
+                   pipeline_waves=int(s.pipeline_waves), pipeline_fallbacks=int(s.pipeline_fallbacks),
                    timings_ms={n[:-3]: float(getattr(s, n)) for n in _STAT_F64})
 
 

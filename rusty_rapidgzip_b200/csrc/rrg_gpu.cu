@@ -268,6 +268,17 @@ struct rrg_ctx {
     std::vector<std::pair<uint64_t, cudaEvent_t>> arr_pieces;
     cudaEvent_t arr_events[8] = {};
     cudaStream_t copy_stream = nullptr;
+    // pipelined host path: inflate waves alternate between two streams; the
+    // chain checks, resolves and CRC pieces run in order on a high-priority
+    // stream, the result copies on copy_stream
+    cudaStream_t wave_stream[2] = {nullptr, nullptr};
+    cudaStream_t res_stream = nullptr;
+    DBuf pipe;                       // wave tables, states, CRC pieces
+    uint8_t* h_ring = nullptr;       // pinned result pieces
+    size_t h_ring_cap = 0;           // bytes per piece buffer
+    uint8_t* h_wave = nullptr;       // pinned wave outcomes
+    size_t h_wave_cap = 0;
+    bool pipeline = true;            // take the pipelined path where it applies
     DBuf sniff;                // per-file header results of a batch
         // BGZF route: device member table and the captured decode graph
     DBuf bg_bcount, bg_bbase, bg_coff, bg_csize, bg_small;
@@ -1853,6 +1864,440 @@ int deliver(rrg_ctx* c, const uint8_t* d_src, uint64_t n, rrg_sink_fn sink, void
     return 0;
 }
 
+}  // namespace
+
+// ------------------------------------------------------------ pipelined host path
+// One large member stream from host memory to the sink, with the copy of the
+// output to the host overlapping the decode. The sub-chunks are decoded in
+// W waves (each one resident set of decoders, in stream order); each wave's
+// anchored chain is checked and its output laid out on the device
+// (k_wave_chain), so its resolve, CRC pieces and device-to-host copy queue
+// behind its inflate while the next wave decodes. The reference's output stage
+// likewise sends chunks while later chunks decode (pipeline.rs:873-935): bytes
+// of the member go out as they are resolved, and the member's CRC32/ISIZE is
+// checked before its last piece is delivered. Any irregularity stops the
+// pipeline at that wave; the rest is decoded on the checked path from the
+// last verified bit.
+namespace {
+
+struct PipeWave {
+    uint32_t first = 0, n = 0;       // items
+    uint32_t piece_off = 0, piece_cap = 0;
+    size_t grp_off = 0;              // offset of this wave's ResGroup/ResJob/chunk_group tables in the blob
+    uint32_t n_groups = 0;
+};
+
+int ensure_ring(rrg_ctx* c, size_t piece, uint32_t waves, rrg_error* err) {
+    constexpr int RING = 4;
+    if (c->h_ring_cap < piece) {
+        if (c->h_ring) cudaFreeHost(c->h_ring);
+        c->h_ring = nullptr;
+        c->h_ring_cap = 0;
+        CK(cudaMallocHost((void**)&c->h_ring, piece * RING));
+        c->h_ring_cap = piece;
+    }
+    const size_t need = (size_t)waves * (sizeof(WaveInfo) + 16) + 64;
+    if (c->h_wave_cap < need) {
+        if (c->h_wave) cudaFreeHost(c->h_wave);
+        c->h_wave = nullptr;
+        c->h_wave_cap = 0;
+        CK(cudaMallocHost((void**)&c->h_wave, need));
+        c->h_wave_cap = need;
+    }
+    return 0;
+}
+
+// Waves the pipelined path would use for a body of `blen` compressed bytes:
+// each wave needs one sub-chunk of at least 24 KiB per resident decoder.
+uint32_t pipeline_waves(rrg_ctx* c, uint64_t blen) {
+    if (!c->pipeline || !c->scan_bounds || c->lanes || c->gpu_chunk) return 0;
+    const uint64_t per_wave = inflate_slots(c) * (24ull << 10);
+    return (uint32_t)std::min<uint64_t>(4, blen / per_wave);
+}
+
+// Returns 0 with *taken = false when the file does not suit the pipeline
+// (nothing has been decoded or delivered then).
+int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_t* h_file, uint64_t hl,
+                   rrg_sink_fn sink, void* user, bool* closed, uint64_t* total_out, bool* taken, rrg_error* err) {
+    *taken = false;
+    *closed = false;
+    const uint64_t blen = len - hl;
+    const uint32_t W = pipeline_waves(c, blen);
+    if (W < 2 || len < 8) return 0;
+    *taken = true;
+    c->st.pipeline_waves = W;
+    const uint8_t* body = d_file + hl;
+    // ---- boundaries (the scan overlaps the input's arrival) and sub-chunk starts
+    std::vector<uint64_t> verified, stored;
+    if (int rc = scan_boundaries(c, body, blen, verified, &stored, err)) return rc;
+    const uint64_t slots = inflate_slots(c);
+    const uint64_t G = std::max<uint64_t>(16ull << 10, (blen + W * slots - 1) / (W * slots));
+    const uint64_t nbits = blen * 8;
+    const uint64_t K = std::max<uint64_t>(1, (blen + G / 2) / G);
+    std::vector<uint64_t> st{0};
+    for (uint64_t k = 1; k < K; k++) {
+        const uint64_t ideal = nbits * k / K;
+        auto it = std::lower_bound(verified.begin(), verified.end(), ideal);
+        uint64_t best = ~0ull;
+        if (it != verified.end()) best = *it;
+        if (it != verified.begin() && (best == ~0ull || ideal - *(it - 1) < best - ideal)) best = *(it - 1);
+        if (best != ~0ull && best > st.back() && best < nbits) st.push_back(best);
+    }
+    const uint32_t n = (uint32_t)st.size();
+    // ---- items and the slot arena
+    std::vector<ChunkItem> items(n);
+    uint64_t arena = 0;
+    for (uint32_t k = 0; k < n; k++) {
+        ChunkItem& it = items[k];
+        it.in_off = hl;
+        it.in_len = blen;
+        it.start_bit = st[k];
+        it.end_hint = k + 1 < n ? st[k + 1] : ~0ull;
+        const uint64_t span = ((k + 1 < n ? st[k + 1] : nbits) - st[k] + 7) / 8;
+        it.out_cap = round8((uint64_t)(span * c->expand) + 65536);
+        it.out_off = arena;
+        it.flags = ITEM_MARKERS;
+        if (k) {
+            if (std::binary_search(stored.begin(), stored.end(), st[k])) it.flags |= ITEM_STORED_START;
+            else if (std::binary_search(stored.begin(), stored.end(), st[k] | 1))
+                it.flags |= ITEM_STORED_START | ITEM_EMPTY_STORED;
+        }
+        it.id = k;
+        arena += it.out_cap;
+    }
+    // ---- waves: contiguous runs of items; per wave the resolve tables and a
+    // CRC piece region large enough for any output its slots can hold
+    const uint32_t Wn = std::min<uint32_t>(W, n);
+    std::vector<PipeWave> waves(Wn);
+    std::vector<uint32_t> order(n);
+    std::vector<uint8_t> tabs;  // ResGroup[], ResJob[1], chunk_group[] per wave, 8-byte aligned
+    uint32_t max_n = 0, max_g = 0, total_pieces = 0;
+    uint64_t out_bound = 0;
+    for (uint32_t w = 0; w < Wn; w++) {
+        PipeWave& pw = waves[w];
+        pw.first = (uint32_t)((uint64_t)n * w / Wn);
+        pw.n = (uint32_t)((uint64_t)n * (w + 1) / Wn) - pw.first;
+        uint64_t cap = 0;
+        for (uint32_t q = 0; q < pw.n; q++) cap += items[pw.first + q].out_cap;
+        out_bound += cap;
+        pw.piece_off = total_pieces;
+        pw.piece_cap = (uint32_t)(cap / WAVE_PIECE + 2);
+        total_pieces += pw.piece_cap;
+        // largest spans first within the wave
+        for (uint32_t q = 0; q < pw.n; q++) order[pw.first + q] = pw.first + q;
+        std::stable_sort(order.begin() + pw.first, order.begin() + pw.first + pw.n, [&](uint32_t a, uint32_t b) {
+            return items[a].out_cap > items[b].out_cap;
+        });
+        const uint32_t S = std::max<uint32_t>(1, (uint32_t)std::ceil(std::sqrt(0.7 * pw.n)));
+        pw.n_groups = (pw.n + S - 1) / S;
+        pw.grp_off = tabs.size();
+        std::vector<ResGroup> gr(pw.n_groups);
+        std::vector<uint32_t> cg(pw.n);
+        for (uint32_t g = 0; g < pw.n_groups; g++) {
+            gr[g] = ResGroup{g * S, std::min(S, pw.n - g * S)};
+            for (uint32_t q = gr[g].first; q < gr[g].first + gr[g].n; q++) cg[q] = g;
+        }
+        const ResJob jb{0, pw.n_groups};
+        const size_t o1 = round8(pw.n_groups * sizeof(ResGroup)), o2 = o1 + round8(sizeof(ResJob));
+        tabs.resize(pw.grp_off + o2 + round8(pw.n * 4));
+        std::memcpy(tabs.data() + pw.grp_off, gr.data(), pw.n_groups * sizeof(ResGroup));
+        std::memcpy(tabs.data() + pw.grp_off + o1, &jb, sizeof(jb));
+        std::memcpy(tabs.data() + pw.grp_off + o2, cg.data(), pw.n * 4);
+        max_n = std::max(max_n, pw.n);
+        max_g = std::max(max_g, pw.n_groups);
+    }
+    // ---- device memory
+    // pipe layout: state | infos | live | n_pieces[W] | fin (exp/got/status/mpiece) |
+    //              chunks[max_n] | tail_tiles[max_n+1] | head_segs[max_n+1] | pieces | piece_crc | tabs
+    const size_t o_info = 64, o_live = o_info + round8(Wn * sizeof(WaveInfo)), o_np = o_live + 8,
+                 o_fin = o_np + round8(Wn * 4), o_chunks = o_fin + 64,
+                 o_tt = o_chunks + round8((size_t)max_n * sizeof(ResolveChunk)), o_hs = o_tt + ((size_t)max_n + 1) * 8,
+                 o_pc = o_hs + ((size_t)max_n + 1) * 8, o_pcrc = o_pc + (size_t)total_pieces * sizeof(CrcPiece),
+                 o_tabs = o_pcrc + round8((size_t)total_pieces * 4), p_total = o_tabs + tabs.size();
+    const uint64_t isize_hint = le32h(h_file + len - 4);
+    OutTarget tgt{(uint8_t*)c->out.p, c->out.cap, true};
+    const uint64_t out_cap = std::min<uint64_t>(out_bound, std::max<uint64_t>(isize_hint, 2 * len) + (1u << 20));
+    if (int rc = ensure_out(c, tgt, out_cap, 0, err)) return rc;
+    CK(dgrow(c->pipe, p_total));
+    CK(dgrow(c->items, (size_t)n * sizeof(ChunkItem)));
+    CK(dgrow(c->results, (size_t)n * sizeof(ChunkResult)));
+    CK(dgrow(c->order, (size_t)n * 4));
+    CK(dgrow(c->queue, (size_t)Wn * 16));
+    CK(dgrow(c->mbs, 4096 * sizeof(MemberRec)));
+    CK(dgrow(c->mbcount, 16));
+    CK(dgrow(c->cells, (arena + 8) * 2));
+    CK(dgrow(c->win, ((size_t)max_n + max_g) * WINDOW * 2));
+    CK(dgrow(c->rerr, 16));
+    CK(dgrow(c->markers, 8));
+    CK(dgrow(c->crc_table, sizeof(g_crc_tab) + sizeof(g_crc_z496)));
+    if (int rc = ensure_ring(c, 16u << 20, Wn, err)) return rc;
+    if (!c->res_stream) {
+        int least = 0, greatest = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        CK(cudaStreamCreateWithPriority(&c->res_stream, cudaStreamNonBlocking, greatest));
+        for (auto& ws : c->wave_stream) CK(cudaStreamCreateWithPriority(&ws, cudaStreamNonBlocking, least));
+    }
+    if (!c->copy_stream) CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    uint8_t* P = (uint8_t*)c->pipe.p;
+    WaveState st0{0, 0, 1, 0};
+    CK(cudaMemcpyAsync(P, &st0, sizeof(st0), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(P + o_tabs, tabs.data(), tabs.size(), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->items.p, items.data(), (size_t)n * sizeof(ChunkItem), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->order.p, order.data(), (size_t)n * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(c->queue.p, 0, (size_t)Wn * 16, c->stream));
+    CK(cudaMemsetAsync(c->mbcount.p, 0, 16, c->stream));
+    CK(cudaMemsetAsync(c->rerr.p, 0, 16, c->stream));
+    CK(cudaMemsetAsync(c->markers.p, 0, 8, c->stream));
+    // the final member check: one member over every wave's piece region
+    const uint32_t mps[2] = {0, total_pieces};
+    CK(cudaMemcpyAsync(P + o_fin + 48, mps, 8, cudaMemcpyHostToDevice, c->stream));
+    // every stream starts after the input, the scan and these uploads
+    cudaEvent_t ev0 = nullptr;
+    std::vector<cudaEvent_t> evs;  // destroyed on every return
+    struct EvGuard {
+        std::vector<cudaEvent_t>& v;
+        ~EvGuard() {
+            for (cudaEvent_t e : v) cudaEventDestroy(e);
+        }
+    } guard{evs};
+    auto mkev = [&](cudaEvent_t* e, bool timing) -> cudaError_t {
+        cudaError_t r = timing ? cudaEventCreate(e) : cudaEventCreateWithFlags(e, cudaEventDisableTiming);
+        if (r == cudaSuccess) evs.push_back(*e);
+        return r;
+    };
+    CK(mkev(&ev0, true));
+    CK(cudaEventRecord(ev0, c->stream));
+    for (auto ws : c->wave_stream) CK(cudaStreamWaitEvent(ws, ev0, 0));
+    CK(cudaStreamWaitEvent(c->res_stream, ev0, 0));
+    CK(cudaStreamWaitEvent(c->copy_stream, ev0, 0));
+    // ---- enqueue every wave: inflate | chain check, resolve, CRC pieces
+    const uint32_t IW = c->inflate_warps;
+    const size_t ismem = IW * sizeof(WarpSmem);
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_inflate<uint16_t>, IW * 32, ismem);
+    std::vector<cudaEvent_t> e_chain(Wn), e_res(Wn), e_inf(Wn);
+    WaveInfo* h_info = (WaveInfo*)c->h_wave;
+    uint32_t* h_err = (uint32_t*)(c->h_wave + Wn * sizeof(WaveInfo));  // resolve error word per wave
+    uint32_t* h_fin = h_err + Wn + 1;                                    // status, got_crc, got_len lo/hi
+    for (uint32_t w = 0; w < Wn; w++) {
+        const PipeWave& pw = waves[w];
+        cudaStream_t ws = c->wave_stream[w & 1];
+        InflateArgs A{};
+        A.in = d_file;
+        A.items = (const ChunkItem*)c->items.p;
+        A.results = (ChunkResult*)c->results.p;
+        A.n_items = pw.n;
+        A.order = (const uint32_t*)c->order.p + pw.first;
+        A.queue = (uint32_t*)c->queue.p + 4 * w;
+        A.out = c->cells.p;
+        A.mbs = (MemberRec*)c->mbs.p;
+        A.mb_count = (uint32_t*)c->mbcount.p;
+        A.mb_cap = 4096;
+        RRG_LAUNCH(k_inflate<uint16_t>, persistent_blocks(c, std::max(1, occ), pw.n, IW), IW * 32, ismem, ws, A);
+        LAUNCHED(c);
+        CK(mkev(&e_inf[w], true));
+        CK(cudaEventRecord(e_inf[w], ws));
+        cudaStream_t rs = c->res_stream;
+        CK(cudaStreamWaitEvent(rs, e_inf[w], 0));
+        WaveArgs WA{};
+        WA.items = (const ChunkItem*)c->items.p;
+        WA.results = (const ChunkResult*)c->results.p;
+        WA.first = pw.first;
+        WA.n = pw.n;
+        WA.last_item = n - 1;
+        WA.state = (WaveState*)P;
+        WA.info = (WaveInfo*)(P + o_info) + w;
+        WA.live = (uint32_t*)(P + o_live);
+        WA.chunks = (ResolveChunk*)(P + o_chunks);
+        WA.tail_tiles = (uint64_t*)(P + o_tt);
+        WA.head_segs = (uint64_t*)(P + o_hs);
+        WA.pieces = (CrcPiece*)(P + o_pc) + pw.piece_off;
+        WA.piece_cap = pw.piece_cap;
+        WA.n_pieces = (uint32_t*)(P + o_np) + w;
+        WA.out_cap = tgt.cap;
+        WA.mbs = (const MemberRec*)c->mbs.p;
+        WA.mb_count = (const uint32_t*)c->mbcount.p;
+        WA.exp_crc = (uint32_t*)(P + o_fin);
+        WA.exp_isize = (uint32_t*)(P + o_fin) + 1;
+        RRG_LAUNCH(k_wave_chain, 1, WAVE_THREADS, 0, rs, WA);
+        LAUNCHED(c);
+        CK(cudaMemcpyAsync(h_info + w, WA.info, sizeof(WaveInfo), cudaMemcpyDeviceToHost, rs));
+        CK(mkev(&e_chain[w], false));
+        CK(cudaEventRecord(e_chain[w], rs));
+        ResolveArgs R{};
+        R.cells = (uint16_t*)c->cells.p;
+        R.chunks = WA.chunks;
+        R.n_chunks = pw.n;
+        R.groups = (const ResGroup*)(P + o_tabs + pw.grp_off);
+        R.n_groups = pw.n_groups;
+        const size_t o1 = round8(pw.n_groups * sizeof(ResGroup)), o2 = o1 + round8(sizeof(ResJob));
+        R.jobs = (const ResJob*)(P + o_tabs + pw.grp_off + o1);
+        R.n_jobs = 1;
+        R.chunk_group = (const uint32_t*)(P + o_tabs + pw.grp_off + o2);
+        R.tail_tiles = WA.tail_tiles;
+        R.head_segs = WA.head_segs;
+        R.maps = (uint16_t*)c->win.p;
+        R.bases = (uint16_t*)c->win.p + (size_t)max_n * WINDOW;
+        R.out = tgt.p;
+        R.err = (uint32_t*)c->rerr.p;
+        R.markers = (unsigned long long*)c->markers.p;
+        R.live = WA.live;
+        RRG_LAUNCH(k_win_maps, std::min<uint32_t>(pw.n_groups, c->n_sm), WM_THREADS, WM_SMEM, rs, R);
+        LAUNCHED(c);
+        RRG_LAUNCH(k_win_bases, 1, WM_THREADS, WINDOW * 2, rs, R);
+        LAUNCHED(c);
+        RRG_LAUNCH(k_res_tails, c->n_sm * 8, RES_THREADS, 0, rs, R);
+        LAUNCHED(c);
+        RRG_LAUNCH(k_res_heads, c->n_sm * 4, RES_THREADS, 0, rs, R);
+        LAUNCHED(c);
+        CrcWideArgs CA{tgt.p, WA.pieces, pw.piece_cap, (uint32_t*)(P + o_pcrc) + pw.piece_off,
+                       (const uint32_t*)c->crc_table.p, WA.n_pieces};
+        RRG_LAUNCH(k_crc_pieces_wide, persistent_blocks(c, 8, pw.piece_cap, 1), CRCW_THREADS, 0, rs, CA);
+        LAUNCHED(c);
+        CK(cudaMemcpyAsync(h_err + w, c->rerr.p, 4, cudaMemcpyDeviceToHost, rs));
+        CK(mkev(&e_res[w], false));
+        CK(cudaEventRecord(e_res[w], rs));
+    }
+    // the member's CRC32/ISIZE over all pieces (meaningful when every wave passed)
+    {
+        uint32_t* fin = (uint32_t*)(P + o_fin);
+        CrcMemberArgs B{(const CrcPiece*)(P + o_pc), (const uint32_t*)(P + o_pcrc), fin + 12, 1, fin, fin + 1,
+                        fin + 2, (uint64_t*)(fin + 4), (int32_t*)(fin + 6)};
+        RRG_LAUNCH(k_crc_members, 1, 32, 0, c->res_stream, B);
+        LAUNCHED(c);
+        CK(cudaMemcpyAsync(h_fin, fin, 32, cudaMemcpyDeviceToHost, c->res_stream));
+    }
+    cudaEvent_t e_fin = nullptr;
+    CK(mkev(&e_fin, true));
+    CK(cudaEventRecord(e_fin, c->res_stream));
+    auto drain = [&]() {
+        for (auto ws : c->wave_stream) cudaStreamSynchronize(ws);
+        cudaStreamSynchronize(c->res_stream);
+        cudaStreamSynchronize(c->copy_stream);
+    };
+    // ---- deliver: pieces of each wave's output through a ring of pinned buffers
+    constexpr uint32_t RING = 4;
+    const uint64_t PS = c->h_ring_cap;
+    cudaEvent_t ring_ev[RING];
+    for (auto& e : ring_ev) CK(mkev(&e, false));
+    struct Piece {
+        uint64_t off, len;
+        uint32_t wave;
+    };
+    std::vector<Piece> pcs;
+    uint64_t total = 0;
+    uint32_t known = 0;  // waves whose pieces are listed
+    size_t issued = 0, delivered = 0;
+    int failed_wave = -1;
+    const double t_start = now_ms();
+    auto issue = [&](size_t i) -> cudaError_t {
+        const Piece& pc = pcs[i];
+        cudaError_t e = cudaStreamWaitEvent(c->copy_stream, e_res[pc.wave], 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(c->h_ring + (i % RING) * PS, tgt.p + pc.off, pc.len, cudaMemcpyDeviceToHost,
+                                c->copy_stream);
+        if (e == cudaSuccess) e = cudaEventRecord(ring_ev[i % RING], c->copy_stream);
+        return e;
+    };
+    for (;;) {
+        // learn the next wave's outcome when its pieces are needed
+        if (issued == pcs.size() && known < Wn && failed_wave < 0) {
+            CK(cudaEventSynchronize(e_chain[known]));
+            const WaveInfo wi = h_info[known];
+            if (!wi.ok) {
+                failed_wave = (int)known;
+            } else {
+                for (uint64_t o = 0; o < wi.out_len; o += PS)
+                    pcs.push_back(Piece{wi.out_begin + o, std::min(PS, wi.out_len - o), known});
+                total = wi.out_begin + wi.out_len;
+                known++;
+            }
+            continue;
+        }
+        while (issued < pcs.size() && issued < delivered + RING) CK(issue(issued++));
+        if (delivered == issued) break;  // nothing in flight: all waves done, or stopped at a failed wave
+        const Piece& pc = pcs[delivered];
+        CK(cudaEventSynchronize(ring_ev[delivered % RING]));
+        if (h_err[pc.wave]) {
+            drain();
+            set_err(err, RRG_ERR_DEFLATE_INVALID, "%s", msg_text(MSG_MARKER_WINDOW));
+            return RRG_ERR_DEFLATE_INVALID;
+        }
+        const bool very_last = failed_wave < 0 && known == Wn && delivered + 1 == pcs.size();
+        if (very_last) {  // the member's trailer is checked before its last piece goes out
+            CK(cudaEventSynchronize(e_fin));
+            if (h_fin[6] == DS_CRC || h_fin[6] == DS_ISIZE) {
+                drain();
+                const WaveInfo& li = h_info[Wn - 1];
+                const MemberSpan ms{0, total, h_fin[0], h_fin[1], hl + li.trailer_byte};
+                return member_error(err, ms, 0, (int32_t)h_fin[6], h_fin[2],
+                                    (uint64_t)h_fin[4] | ((uint64_t)h_fin[5] << 32));
+            }
+        }
+        c->st.chunks_decoded++;
+        if (sink && sink(user, c->h_ring + (delivered % RING) * PS, (size_t)pc.len)) {
+            *closed = true;
+            drain();
+            *total_out = total;
+            return 0;
+        }
+        delivered++;
+    }
+    drain();
+    {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, ev0, e_inf[Wn - 1]) == cudaSuccess) c->st.inflate_ms += ms;
+        if (cudaEventElapsedTime(&ms, ev0, e_fin) == cudaSuccess) c->st.resolve_ms += 0;  // overlapped
+    }
+    c->st.gpu_chunks += n;
+    c->st.d2h_ms += now_ms() - t_start;
+    unsigned long long nmk = 0;
+    CK(cudaMemcpy(&nmk, c->markers.p, 8, cudaMemcpyDeviceToHost));
+    c->st.markers += nmk;
+    if (failed_wave < 0) {
+        c->st.members += 1;
+        *total_out = total;
+        return 0;
+    }
+    // ---- the rest on the checked path, from the last verified bit
+    c->st.pipeline_fallbacks = 1;
+    WaveState S{};
+    CK(cudaMemcpy(&S, P, sizeof(S), cudaMemcpyDeviceToHost));
+    if (c->cfg.verbose >= 2)
+        std::fprintf(stderr, "[rrg-gpu] pipeline stopped at wave %d (sub-chunk %d, status %d): checked path from bit %llu\n",
+                     failed_wave, h_info[failed_wave].fail_item, h_info[failed_wave].fail_status,
+                     (unsigned long long)S.expected);
+    std::vector<MemberJob> jobs(1);
+    MemberJob& j = jobs[0];
+    j.len = len;
+    j.body_off = hl;
+    j.start_bit = S.expected;
+    j.dst_off = S.out_end;
+    j.prefix_len = std::min<uint64_t>(WINDOW, S.out_end);
+    if (S.out_end) {
+        std::vector<int32_t> stv;
+        std::vector<uint32_t> got;
+        std::vector<uint64_t> glen;
+        const uint64_t members = c->st.members;  // the prefix's CRC32 checks no member
+        if (int rc = crc_spans(c, tgt.p, {MemberSpan{0, S.out_end, 0, 0, 0}}, stv, got, glen, err)) return rc;
+        c->st.members = members;
+        j.crc_prev = got[0];
+        j.len_prev = glen[0];
+    }
+    tgt.cap = c->out.cap;
+    if (int rc = members_route(c, d_file, jobs, tgt, err)) return rc;
+    if (j.rc) {
+        if (err) *err = j.err;
+        return j.rc;
+    }
+    *total_out = S.out_end + j.out.total;
+    return deliver(c, tgt.p + S.out_end, j.out.total, sink, user, closed, err);
+}
+
+}  // namespace
+
+namespace {
+
 int decode_host_impl(rrg_ctx* c, const uint8_t* data, size_t len, rrg_sink_fn sink, void* user, rrg_stats* stats,
                      rrg_error* err) {
     double t_all = now_ms();
@@ -1893,19 +2338,33 @@ int decode_host_impl(rrg_ctx* c, const uint8_t* data, size_t len, rrg_sink_fn si
         CK(cudaStreamSynchronize(c->stream));
     }
     c->st.h2d_ms = now_ms() - t0;
-    // output size is only known after the chain; decode into the context buffer
-    Decoded d;
-    OutTarget tgt{(uint8_t*)c->out.p, c->out.cap, true};
-    int rc = decode_file(c, (const uint8_t*)c->comp.p, len, data, tgt, &d, err);
+    int rc = upload_tables(c, err);
+    bool closed = false, taken = false;
+    if (!rc && host_bgzf_size(data, len) < 0) {
+        // a large member stream: decode in waves with the copy-out overlapped
+        size_t hl = 0;
+        int detail = 0;
+        if (host_parse_header(data, len, &hl, &detail) == DS_OK) {
+            uint64_t total = 0;
+            rc = pipelined_host(c, (const uint8_t*)c->comp.p, len, data, hl, sink, user, &closed, &total, &taken,
+                                err);
+            if (taken) c->st.uncompressed_bytes = total;
+        }
+    }
+    if (!rc && !taken) {
+        // output size is only known after the chain; decode into the context buffer
+        Decoded d;
+        OutTarget tgt{(uint8_t*)c->out.p, c->out.cap, true};
+        rc = decode_file(c, (const uint8_t*)c->comp.p, len, data, tgt, &d, err);
+        if (!rc) {
+            c->st.uncompressed_bytes = d.total;
+            rc = deliver(c, tgt.p, d.total, sink, user, &closed, err);
+        }
+    }
     if (c->arr_base) {  // a path that launched nothing (an early error): drain the copies
         c->arr_base = nullptr;
         c->arr_pieces.clear();
         cudaStreamSynchronize(c->copy_stream);
-    }
-    bool closed = false;
-    if (!rc) {
-        c->st.uncompressed_bytes = d.total;
-        rc = deliver(c, tgt.p, d.total, sink, user, &closed, err);
     }
     c->st.kernel_launches = c->launches;
     c->st.total_ms = now_ms() - t_all;
@@ -2551,7 +3010,7 @@ void release_scratch(rrg_ctx* c) {
                     &c->out,    &c->targets, &c->limits,    &c->found,    &c->next_lut, &c->chunks,    &c->tiles,
                     &c->rerr,   &c->markers, &c->crc_table, &c->pieces,   &c->piece_crc, &c->mpiece,   &c->exp_crc,
                     &c->exp_isize, &c->got_crc, &c->got_len, &c->mstatus, &c->comp, &c->comp2, &c->pfx, &c->bg_bcount, &c->bg_bbase,
-                    &c->bg_coff, &c->bg_csize, &c->bg_small, &c->sniff};
+                    &c->bg_coff, &c->bg_csize, &c->bg_small, &c->sniff, &c->pipe};
 #ifndef RRG_EMU
     if (c->bg_exec) cudaGraphExecDestroy(c->bg_exec);
     c->bg_exec = nullptr;
@@ -2847,6 +3306,7 @@ rrg_ctx* rrg_gpu_create(const rrg_config* cfg, rrg_error* err) {
     if (cfg) c->cfg = *cfg;
     if (!c->cfg.chunk_size_bytes) c->cfg.chunk_size_bytes = 4ull << 20;
     if (!c->cfg.hbm_budget_bytes) c->cfg.hbm_budget_bytes = 120ull * 1000 * 1000 * 1000;
+    c->pipeline = c->cfg.host_pipeline >= 0;
     c->gpu_chunk = c->cfg.gpu_chunk_bytes;
     if (c->cfg.finder_tile_bits) {
         c->finder_tile = (uint32_t)std::min<uint64_t>(FIND_TILE, (c->cfg.finder_tile_bits + 31) & ~31ull);
@@ -2905,6 +3365,11 @@ void rrg_gpu_destroy(rrg_ctx* c) {
     for (cudaEvent_t e : c->arr_events)
         if (e) cudaEventDestroy(e);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    for (cudaStream_t s : c->wave_stream)
+        if (s) cudaStreamDestroy(s);
+    if (c->res_stream) cudaStreamDestroy(c->res_stream);
+    if (c->h_ring) cudaFreeHost(c->h_ring);
+    if (c->h_wave) cudaFreeHost(c->h_wave);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
 }

@@ -2214,6 +2214,7 @@ struct ResolveArgs {
     uint8_t* out;
     uint32_t* err;                // [0] flag, [1] chunk, [2] cell lo, [3] cell hi
     unsigned long long* markers;  // count of marker cells resolved
+    const uint32_t* live;         // when set and 0, the kernels do nothing (a failed pipeline wave)
 };
 
 // Cells of a chunk that the head kernel resolves: all but the last 32 KiB.
@@ -2297,6 +2298,7 @@ __device__ __forceinline__ void wm_load(const ResolveArgs& A, uint32_t k, uint4 
 }
 
 __global__ void __launch_bounds__(WM_THREADS, 1) k_win_maps(ResolveArgs A) {
+    if (A.live && *A.live == 0) return;
     RRG_DYN_SMEM(sm);
     uint16_t* maps2 = reinterpret_cast<uint16_t*>(sm);  // two maps, alternating by step
     uint16_t* stage = maps2 + 2 * WINDOW;               // stage[x]: cell s0 + x of the chunk
@@ -2365,6 +2367,7 @@ __global__ void __launch_bounds__(WM_THREADS, 1) k_win_maps(ResolveArgs A) {
 // before the job (a stripe's prefix, already in the output, or WM_BAD); each
 // next base applies the previous group's last map to the previous base.
 __global__ void __launch_bounds__(WM_THREADS, 1) k_win_bases(ResolveArgs A) {
+    if (A.live && *A.live == 0) return;
     RRG_DYN_SMEM(sm);
     uint16_t* cur = reinterpret_cast<uint16_t*>(sm);
     for (uint32_t jb = blockIdx.x; jb < A.n_jobs; jb += gridDim.x) {
@@ -2419,6 +2422,7 @@ __global__ void __launch_bounds__(WM_THREADS, 1) k_win_bases(ResolveArgs A) {
 }
 
 __global__ void __launch_bounds__(RES_THREADS) k_res_tails(ResolveArgs A) {
+    if (A.live && *A.live == 0) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t n_tiles = A.tail_tiles[A.n_chunks];
     for (uint64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
@@ -2452,6 +2456,7 @@ __global__ void __launch_bounds__(RES_THREADS) k_res_tails(ResolveArgs A) {
 
 // Four blocks per SM: 4 x 32 KiB windows in shared memory.
 __global__ void __launch_bounds__(RES_THREADS, 4) k_res_heads(ResolveArgs A) {
+    if (A.live && *A.live == 0) return;
     __shared__ __align__(16) uint8_t win[WINDOW + 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t n_segs = A.head_segs[A.n_chunks];
@@ -2499,19 +2504,23 @@ __global__ void __launch_bounds__(RES_THREADS, 4) k_res_heads(ResolveArgs A) {
             bool bad = false;
             // cells past s1 belong to the tail kernel
             const uint32_t nvalid = ci < s1 ? (s1 - ci < RES_CELLS ? (uint32_t)(s1 - ci) : RES_CELLS) : 0u;
-            uint32_t lo32 = 0, hi32 = 0;
+            // eight literals: their low bytes, two byte permutes
+            uint32_t lo32 = __byte_perm(w[0], w[1], 0x6420), hi32 = __byte_perm(w[2], w[3], 0x6420);
+            if ((w[0] | w[1] | w[2] | w[3]) & 0x80008000u) {
+                lo32 = hi32 = 0;
 #pragma unroll
-            for (int i = 0; i < RES_CELLS; i++) {
-                const uint32_t cl = (w[i >> 1] >> (16 * (i & 1))) & 0xffffu;
-                const uint32_t mk = (cl >> 15) & ((uint32_t)i < nvalid ? 1u : 0u), m = cl & 0x7fffu;
-                // a marker m < lim reads win[wbase - m]; others read a clamped, unused byte
-                const uint32_t x = (uint32_t)wbase - m;
-                const uint32_t wb = win[x < WINDOW + 32 ? x : 0u];
-                const uint32_t b = mk ? wb : cl;
-                nmk += mk;
-                bad |= mk && (uint64_t)m >= lim;
-                if (i < 4) lo32 |= (b & 0xffu) << (8 * i);
-                else hi32 |= (b & 0xffu) << (8 * (i - 4));
+                for (int i = 0; i < RES_CELLS; i++) {
+                    const uint32_t cl = (w[i >> 1] >> (16 * (i & 1))) & 0xffffu;
+                    const uint32_t mk = (cl >> 15) & ((uint32_t)i < nvalid ? 1u : 0u), m = cl & 0x7fffu;
+                    // a marker m < lim reads win[wbase - m]; others read a clamped, unused byte
+                    const uint32_t x = (uint32_t)wbase - m;
+                    const uint32_t wb = win[x < WINDOW + 32 ? x : 0u];
+                    const uint32_t b = mk ? wb : cl;
+                    nmk += mk;
+                    bad |= mk && (uint64_t)m >= lim;
+                    if (i < 4) lo32 |= (b & 0xffu) << (8 * i);
+                    else hi32 |= (b & 0xffu) << (8 * (i - 4));
+                }
             }
             const uint64_t v = ((uint64_t)hi32 << 32) | lo32;
             if (bad) res_fail(A, k, ci);
@@ -2534,6 +2543,173 @@ __global__ void k_resolve_list(uint8_t* bytes, uint64_t n_bytes, const uint32_t*
             continue;
         }
         bytes[p] = tail[tail_len - 1 - o];
+    }
+}
+
+// ------------------------------------------------------- pipelined member decode
+// A large single-member stream decodes in waves of sub-chunks, each wave one
+// resident set of decoders. k_wave_chain checks a wave's anchored chain on the
+// device (pipeline.rs:758-809: each sub-chunk starts where the previous one
+// stopped) and lays out its output, so the wave's resolve, CRC pieces and copy
+// to the host are queued behind its inflate with no host round trip. Any
+// irregularity (a false start, a full slot, a member ending before the last
+// sub-chunk, a full output buffer) stops the pipeline at that wave: the kernel
+// leaves the state of the last good wave for the host, which decodes the rest
+// from there on the checked path.
+struct WaveState {         // carried from wave to wave on the device
+    uint64_t expected;     // body-relative bit where the next sub-chunk must start
+    uint64_t out_end;      // output bytes laid out so far
+    uint32_t live;         // 0 once a wave failed
+    uint32_t pad;
+};
+struct WaveInfo {          // one wave's outcome, copied to the host
+    uint64_t out_begin, out_len;
+    uint64_t trailer_byte; // body-relative trailer offset (last wave)
+    uint32_t ok;
+    int32_t fail_item;     // index in the wave of the first failing sub-chunk
+    int32_t fail_status;
+    uint32_t final_seen;
+};
+struct WaveArgs {
+    const ChunkItem* items;    // all waves' items; this wave's are [first, first + n)
+    const ChunkResult* results;
+    uint32_t first, n;
+    uint32_t last_item;        // global index of the stream's last sub-chunk
+    WaveState* state;
+    WaveInfo* info;
+    uint32_t* live;            // gate of this wave's resolve and CRC launches
+    ResolveChunk* chunks;      // n entries
+    uint64_t* tail_tiles;      // n + 1
+    uint64_t* head_segs;       // n + 1
+    CrcPiece* pieces;          // this wave's region of piece_cap pieces
+    uint32_t piece_cap;
+    uint32_t* n_pieces;        // pieces laid out (0 when the wave failed)
+    uint64_t out_cap;
+    const MemberRec* mbs;
+    const uint32_t* mb_count;
+    uint32_t* exp_crc;         // the member trailer (last wave)
+    uint32_t* exp_isize;
+};
+constexpr int WAVE_THREADS = 1024;
+constexpr uint64_t WAVE_PIECE = 256 * 1024;  // CRC piece bytes
+
+// Exclusive block-wide prefix of one value per thread; returns the total.
+__device__ __forceinline__ uint64_t block_scan(uint64_t v, uint64_t* sh, uint64_t* excl) {
+    const int t = threadIdx.x;
+    sh[t] = v;
+    __syncthreads();
+    for (int o = 1; o < WAVE_THREADS; o <<= 1) {
+        const uint64_t x = t >= o ? sh[t - o] : 0;
+        __syncthreads();
+        sh[t] += x;
+        __syncthreads();
+    }
+    *excl = sh[t] - v;
+    const uint64_t total = sh[WAVE_THREADS - 1];
+    __syncthreads();
+    return total;
+}
+
+__global__ void __launch_bounds__(WAVE_THREADS, 1) k_wave_chain(WaveArgs A) {
+    __shared__ uint64_t sh[WAVE_THREADS];
+    __shared__ int32_t s_fail, s_status;
+    const int t = threadIdx.x;
+    const WaveState S = *A.state;
+    if (t == 0) {
+        s_fail = S.live ? 0x7fffffff : -1;
+        s_status = 0;
+    }
+    __syncthreads();
+    // each thread checks a contiguous run of sub-chunks
+    const uint32_t per = (A.n + WAVE_THREADS - 1) / WAVE_THREADS;
+    const uint32_t b = t * per < A.n ? t * per : A.n, e = b + per < A.n ? b + per : A.n;
+    uint64_t cells = 0, tiles = 0, segs = 0;
+    for (uint32_t q = b; q < e; q++) {
+        const uint32_t k = A.first + q;
+        const ChunkItem it = A.items[k];
+        const ChunkResult r = A.results[k];
+        const uint64_t expected = q == 0 ? S.expected : A.results[k - 1].actual_end_bit;
+        // a start on a stored block's zero header byte decodes as the true start
+        // in the same byte's first 6 bits, or right after an empty block
+        const uint64_t d = expected - it.start_bit;
+        const bool same = it.start_bit == expected ||
+                          ((it.flags & ITEM_STORED_START) && expected > it.start_bit &&
+                           (d <= 5 || ((it.flags & ITEM_EMPTY_STORED) && d == 40)));
+        const bool last = k == A.last_item;
+        bool ok = same && r.status == DS_OK;
+        ok = ok && (last ? (r.final_block && r.n_members == 1) : (!r.final_block && r.n_members == 0));
+        if (!ok) {
+            atomicMin(reinterpret_cast<unsigned int*>(&s_fail), q);
+            continue;
+        }
+        cells += r.n_cells;
+        tiles += (WINDOW - (res_tail_lo(r.n_cells) & ~(uint32_t)(RES_TAIL_TILE - 1))) / RES_TAIL_TILE;
+        segs += (res_head_end(r.n_cells) + RES_HEAD_SEG - 1) / RES_HEAD_SEG;
+    }
+    __syncthreads();
+    uint64_t c_ex, t_ex, s_ex;
+    const uint64_t total = block_scan(cells, sh, &c_ex);
+    const uint64_t n_tiles = block_scan(tiles, sh, &t_ex);
+    const uint64_t n_segs = block_scan(segs, sh, &s_ex);
+    const uint64_t out_begin = S.out_end, out_len = total;
+    const uint32_t np = (uint32_t)((out_len + WAVE_PIECE - 1) / WAVE_PIECE);
+    if (t == 0 && s_fail == 0x7fffffff && (out_begin + out_len > A.out_cap || np > A.piece_cap)) s_fail = (int32_t)A.n;
+    __syncthreads();
+    if (s_fail != 0x7fffffff) {  // uniform: this wave and every later one do nothing
+        if (t == 0) {
+            if (s_fail >= 0 && s_fail < (int32_t)A.n) s_status = A.results[A.first + s_fail].status;
+            A.state->live = 0;
+            *A.live = 0;
+            *A.n_pieces = 0;
+            A.info->ok = 0;
+            A.info->fail_item = s_fail;
+            A.info->fail_status = s_status;
+            A.info->out_begin = out_begin;
+            A.info->out_len = 0;
+        }
+        return;
+    }
+    for (uint32_t q = b; q < e; q++) {
+        const uint32_t k = A.first + q;
+        const uint64_t n = A.results[k].n_cells;
+        A.chunks[q] = ResolveChunk{out_begin + c_ex, A.items[k].out_off, n, 0, out_begin};
+        A.tail_tiles[q] = t_ex;
+        A.head_segs[q] = s_ex;
+        c_ex += n;
+        t_ex += (WINDOW - (res_tail_lo(n) & ~(uint32_t)(RES_TAIL_TILE - 1))) / RES_TAIL_TILE;
+        s_ex += (res_head_end(n) + RES_HEAD_SEG - 1) / RES_HEAD_SEG;
+    }
+    for (uint32_t p = t; p < A.piece_cap; p += WAVE_THREADS) {
+        const uint64_t o = (uint64_t)p * WAVE_PIECE;
+        A.pieces[p] = p < np ? CrcPiece{out_begin + o, out_len - o < WAVE_PIECE ? out_len - o : WAVE_PIECE}
+                             : CrcPiece{out_begin + out_len, 0};
+    }
+    const uint32_t lastq = A.n - 1;
+    const bool has_last = A.first + lastq == A.last_item;
+    uint64_t tb = 0;
+    if (t == 0) {
+        A.tail_tiles[A.n] = n_tiles;
+        A.head_segs[A.n] = n_segs;
+        *A.n_pieces = A.piece_cap;
+        if (has_last) {  // the trailer of the stream's only member
+            const uint32_t id = A.items[A.last_item].id, nm = *A.mb_count;
+            for (uint32_t i = 0; i < nm; i++)
+                if (A.mbs[i].item == id) {
+                    *A.exp_crc = A.mbs[i].crc;
+                    *A.exp_isize = A.mbs[i].isize;
+                    tb = A.mbs[i].trailer_byte;
+                }
+        }
+        A.state->expected = A.results[A.first + lastq].actual_end_bit;
+        A.state->out_end = out_begin + out_len;
+        *A.live = 1;
+        A.info->ok = 1;
+        A.info->fail_item = -1;
+        A.info->fail_status = 0;
+        A.info->out_begin = out_begin;
+        A.info->out_len = out_len;
+        A.info->trailer_byte = tb;
+        A.info->final_seen = has_last ? 1u : 0u;
     }
 }
 

@@ -264,6 +264,12 @@ inline unsigned __reduce_or_sync(unsigned, unsigned v) {
     return m;
 }
 inline int __popc(unsigned v) { return __builtin_popcount(v); }
+inline unsigned __byte_perm(unsigned x, unsigned y, unsigned s) {  // PTX prmt, default mode
+    const uint64_t v = ((uint64_t)y << 32) | x;
+    unsigned r = 0;
+    for (int i = 0; i < 4; i++) r |= (unsigned)((v >> (8 * ((s >> (4 * i)) & 7))) & 0xff) << (8 * i);
+    return r;
+}
 inline int __ffs(int v) { return __builtin_ffs(v); }
 inline unsigned __funnelshift_r(unsigned lo, unsigned hi, unsigned sh) {
     sh &= 31;
@@ -348,6 +354,15 @@ inline cudaError_t cudaGetSymbolAddress(void** p, T& sym) {
 }
 inline cudaError_t cudaStreamCreateWithFlags(cudaStream_t* s, unsigned) {
     *s = (void*)0x1;
+    return cudaSuccess;
+}
+inline cudaError_t cudaStreamCreateWithPriority(cudaStream_t* s, unsigned, int) {
+    *s = (void*)0x1;
+    return cudaSuccess;
+}
+inline cudaError_t cudaDeviceGetStreamPriorityRange(int* least, int* greatest) {
+    *least = 0;
+    *greatest = -1;
     return cudaSuccess;
 }
 inline cudaError_t cudaStreamDestroy(cudaStream_t) { return cudaSuccess; }

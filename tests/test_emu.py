@@ -514,3 +514,60 @@ def test_resolve_long_chunks_and_unaligned_output(emu_decoder_factory):
         n, st2 = d.decode_device(haddr(src), len(gz), haddr(dst) + shift, len(raw))
         assert n == len(raw) and dst[shift:shift + n].tobytes() == raw
         assert (dst[:shift] == 0xA5).all() and (dst[shift + n:] == 0xA5).all()
+
+
+def test_pipelined_host_path(emu_decoder_factory):
+    """A member stream large enough for several waves takes the pipelined host
+    path: its output equals the generator's and the checked path's, the sink
+    sees it in order, and a closed sink stops it early."""
+    raw, gz = W.config1(2600 << 10, seed=18)
+    d = emu_decoder_factory()
+    out = []
+    st = d.decode_host(gz, out.append)
+    assert b"".join(out) == raw
+    assert st.pipeline_waves >= 2 and st.pipeline_fallbacks == 0 and st.uncompressed_bytes == len(raw)
+    assert st.members == 1 and st.markers > 0
+    ref = emu_decoder_factory(host_pipeline=-1)
+    out2 = []
+    st2 = ref.decode_host(gz, out2.append)
+    assert b"".join(out2) == raw and st2.pipeline_waves == 0
+    from rusty_rapidgzip_b200 import SinkClosed
+
+    first = []
+
+    def one(b):
+        first.append(bytes(b))
+        raise SinkClosed
+
+    d.decode_host(gz, one)
+    assert len(first) == 1 and raw.startswith(first[0])
+
+
+def test_pipelined_host_path_falls_back(emu_decoder_factory):
+    """Nested gzip makes false sub-chunk starts: the pipeline stops at the first
+    wave whose chain breaks and the checked path decodes the rest from the last
+    verified bit, with the member's CRC32 over both parts. A two-member file
+    and a corrupt trailer take the same way; errors match the oracle's."""
+    from rusty_rapidgzip_b200 import RrgError
+    original = np.random.default_rng(0xC0FFEE).integers(32, 127, 1400 << 10, dtype=np.uint8).tobytes()
+    inner = gzip_cli(original, 6)
+    outer = gzip_cli(inner, 6)
+    d = emu_decoder_factory()
+    out = []
+    st = d.decode_host(outer, out.append)
+    assert b"".join(out) == inner
+    assert st.pipeline_waves >= 2
+    raw, gz = W.config1(2600 << 10, seed=19)
+    two = gz + gzip_cli(b"second member " * 1000)
+    out = []
+    st = d.decode_host(two, out.append)
+    assert b"".join(out) == raw + b"second member " * 1000
+    assert st.pipeline_waves >= 2 and st.pipeline_fallbacks == 1 and st.members == 2
+    bad = bytearray(gz)
+    bad[-8] ^= 0x20
+    with pytest.raises(oracle.OracleError) as oe:
+        oracle.read_gz(bytes(bad), 2)
+    with pytest.raises(RrgError) as ge:
+        d.decode_host(bytes(bad), lambda b: None)
+    assert ge.value.code == oe.value.code
+    assert ge.value.expected == oe.value.expected and ge.value.got_crc == oe.value.got_crc
