@@ -268,11 +268,8 @@ struct rrg_ctx {
     std::vector<std::pair<uint64_t, cudaEvent_t>> arr_pieces;
     cudaEvent_t arr_events[8] = {};
     cudaStream_t copy_stream = nullptr;
-    // pipelined host path: inflate waves alternate between two streams; the
-    // chain checks, resolves and CRC pieces run in order on a high-priority
-    // stream, the result copies on copy_stream
-    cudaStream_t wave_stream[2] = {nullptr, nullptr};
-    cudaStream_t res_stream = nullptr;
+    // pipelined host path: waves decode, resolve and checksum in order on the
+    // context stream while earlier waves' output copies run on copy_stream
     DBuf pipe;                       // wave tables, states, CRC pieces
     uint8_t* h_ring = nullptr;       // pinned result pieces
     size_t h_ring_cap = 0;           // bytes per piece buffer
@@ -1908,10 +1905,10 @@ int ensure_ring(rrg_ctx* c, size_t piece, uint32_t waves, rrg_error* err) {
 }
 
 // Waves the pipelined path would use for a body of `blen` compressed bytes:
-// each wave needs one sub-chunk of at least 24 KiB per resident decoder.
+// each wave needs one sub-chunk of at least 32 KiB per resident decoder.
 uint32_t pipeline_waves(rrg_ctx* c, uint64_t blen) {
     if (!c->pipeline || !c->scan_bounds || c->lanes || c->gpu_chunk) return 0;
-    const uint64_t per_wave = inflate_slots(c) * (24ull << 10);
+    const uint64_t per_wave = inflate_slots(c) * (32ull << 10);
     return (uint32_t)std::min<uint64_t>(4, blen / per_wave);
 }
 
@@ -1931,18 +1928,49 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
     std::vector<uint64_t> verified, stored;
     if (int rc = scan_boundaries(c, body, blen, verified, &stored, err)) return rc;
     const uint64_t slots = inflate_slots(c);
-    const uint64_t G = std::max<uint64_t>(16ull << 10, (blen + W * slots - 1) / (W * slots));
     const uint64_t nbits = blen * 8;
-    const uint64_t K = std::max<uint64_t>(1, (blen + G / 2) / G);
-    std::vector<uint64_t> st{0};
-    for (uint64_t k = 1; k < K; k++) {
-        const uint64_t ideal = nbits * k / K;
-        auto it = std::lower_bound(verified.begin(), verified.end(), ideal);
-        uint64_t best = ~0ull;
-        if (it != verified.end()) best = *it;
-        if (it != verified.begin() && (best == ~0ull || ideal - *(it - 1) < best - ideal)) best = *(it - 1);
-        if (best != ~0ull && best > st.back() && best < nbits) st.push_back(best);
+    // block starts the chunks may begin at, and wave edges among them nearest
+    // to equal shares of the input
+    std::vector<uint64_t> cand{0};
+    for (uint64_t v : verified)
+        if (v > cand.back() && v < nbits) cand.push_back(v);
+    std::vector<size_t> wedge{0};
+    for (uint32_t w = 1; w < W; w++) {
+        const uint64_t ideal = nbits * w / W;
+        size_t i = (size_t)(std::lower_bound(cand.begin(), cand.end(), ideal) - cand.begin());
+        if (i == cand.size() || (i > 0 && ideal - cand[i - 1] < cand[i] - ideal)) i--;
+        if (i > wedge.back()) wedge.push_back(i);
     }
+    wedge.push_back(cand.size());
+    auto end_of = [&](size_t i) { return i < cand.size() ? cand[i] : nbits; };
+    // within a wave (one item per resident decoder), runs of consecutive blocks
+    // whose largest span is as small as possible: the wave ends with its
+    // largest sub-chunk, and a block is the finest unit a sub-chunk can take
+    std::vector<uint64_t> st;
+    std::vector<uint32_t> wfirst;
+    for (size_t w = 0; w + 1 < wedge.size(); w++) {
+        const size_t a = wedge[w], b = wedge[w + 1];
+        auto runs = [&](uint64_t B, std::vector<uint64_t>* out) {
+            uint64_t cnt = 0;
+            for (size_t i = a; i < b;) {
+                size_t j = i + 1;
+                while (j < b && end_of(j + 1) - cand[i] <= B) j++;
+                if (out) out->push_back(cand[i]);
+                cnt++;
+                i = j;
+            }
+            return cnt;
+        };
+        uint64_t lo = 1, hi = end_of(b) - cand[a];
+        while (lo < hi) {  // the smallest largest span that fits one wave
+            const uint64_t mid = lo + (hi - lo) / 2;
+            if (runs(mid, nullptr) <= slots) hi = mid;
+            else lo = mid + 1;
+        }
+        wfirst.push_back((uint32_t)st.size());
+        runs(lo, &st);
+    }
+    wfirst.push_back((uint32_t)st.size());
     const uint32_t n = (uint32_t)st.size();
     // ---- items and the slot arena
     std::vector<ChunkItem> items(n);
@@ -1967,7 +1995,7 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
     }
     // ---- waves: contiguous runs of items; per wave the resolve tables and a
     // CRC piece region large enough for any output its slots can hold
-    const uint32_t Wn = std::min<uint32_t>(W, n);
+    const uint32_t Wn = (uint32_t)wfirst.size() - 1;
     std::vector<PipeWave> waves(Wn);
     std::vector<uint32_t> order(n);
     std::vector<uint8_t> tabs;  // ResGroup[], ResJob[1], chunk_group[] per wave, 8-byte aligned
@@ -1975,8 +2003,8 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
     uint64_t out_bound = 0;
     for (uint32_t w = 0; w < Wn; w++) {
         PipeWave& pw = waves[w];
-        pw.first = (uint32_t)((uint64_t)n * w / Wn);
-        pw.n = (uint32_t)((uint64_t)n * (w + 1) / Wn) - pw.first;
+        pw.first = wfirst[w];
+        pw.n = wfirst[w + 1] - wfirst[w];
         uint64_t cap = 0;
         for (uint32_t q = 0; q < pw.n; q++) cap += items[pw.first + q].out_cap;
         out_bound += cap;
@@ -2031,12 +2059,6 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
     CK(dgrow(c->markers, 8));
     CK(dgrow(c->crc_table, sizeof(g_crc_tab) + sizeof(g_crc_z496)));
     if (int rc = ensure_ring(c, 16u << 20, Wn, err)) return rc;
-    if (!c->res_stream) {
-        int least = 0, greatest = 0;
-        CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-        CK(cudaStreamCreateWithPriority(&c->res_stream, cudaStreamNonBlocking, greatest));
-        for (auto& ws : c->wave_stream) CK(cudaStreamCreateWithPriority(&ws, cudaStreamNonBlocking, least));
-    }
     if (!c->copy_stream) CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
     uint8_t* P = (uint8_t*)c->pipe.p;
     WaveState st0{0, 0, 1, 0};
@@ -2067,8 +2089,6 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
     };
     CK(mkev(&ev0, true));
     CK(cudaEventRecord(ev0, c->stream));
-    for (auto ws : c->wave_stream) CK(cudaStreamWaitEvent(ws, ev0, 0));
-    CK(cudaStreamWaitEvent(c->res_stream, ev0, 0));
     CK(cudaStreamWaitEvent(c->copy_stream, ev0, 0));
     // ---- enqueue every wave: inflate | chain check, resolve, CRC pieces
     const uint32_t IW = c->inflate_warps;
@@ -2081,7 +2101,7 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
     uint32_t* h_fin = h_err + Wn + 1;                                    // status, got_crc, got_len lo/hi
     for (uint32_t w = 0; w < Wn; w++) {
         const PipeWave& pw = waves[w];
-        cudaStream_t ws = c->wave_stream[w & 1];
+        cudaStream_t ws = c->stream;
         InflateArgs A{};
         A.in = d_file;
         A.items = (const ChunkItem*)c->items.p;
@@ -2097,8 +2117,7 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
         LAUNCHED(c);
         CK(mkev(&e_inf[w], true));
         CK(cudaEventRecord(e_inf[w], ws));
-        cudaStream_t rs = c->res_stream;
-        CK(cudaStreamWaitEvent(rs, e_inf[w], 0));
+        cudaStream_t rs = c->stream;
         WaveArgs WA{};
         WA.items = (const ChunkItem*)c->items.p;
         WA.results = (const ChunkResult*)c->results.p;
@@ -2106,7 +2125,7 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
         WA.n = pw.n;
         WA.last_item = n - 1;
         WA.state = (WaveState*)P;
-        WA.info = (WaveInfo*)(P + o_info) + w;
+        WA.info = h_info + w;  // mapped pinned memory: no copy queued behind the output
         WA.live = (uint32_t*)(P + o_live);
         WA.chunks = (ResolveChunk*)(P + o_chunks);
         WA.tail_tiles = (uint64_t*)(P + o_tt);
@@ -2121,8 +2140,7 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
         WA.exp_isize = (uint32_t*)(P + o_fin) + 1;
         RRG_LAUNCH(k_wave_chain, 1, WAVE_THREADS, 0, rs, WA);
         LAUNCHED(c);
-        CK(cudaMemcpyAsync(h_info + w, WA.info, sizeof(WaveInfo), cudaMemcpyDeviceToHost, rs));
-        CK(mkev(&e_chain[w], false));
+        CK(mkev(&e_chain[w], true));
         CK(cudaEventRecord(e_chain[w], rs));
         ResolveArgs R{};
         R.cells = (uint16_t*)c->cells.p;
@@ -2154,8 +2172,9 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
                        (const uint32_t*)c->crc_table.p, WA.n_pieces};
         RRG_LAUNCH(k_crc_pieces_wide, persistent_blocks(c, 8, pw.piece_cap, 1), CRCW_THREADS, 0, rs, CA);
         LAUNCHED(c);
-        CK(cudaMemcpyAsync(h_err + w, c->rerr.p, 4, cudaMemcpyDeviceToHost, rs));
-        CK(mkev(&e_res[w], false));
+        RRG_LAUNCH(k_copy_words, 1, 32, 0, rs, (const uint32_t*)c->rerr.p, h_err + w, 1u);
+        LAUNCHED(c);
+        CK(mkev(&e_res[w], true));
         CK(cudaEventRecord(e_res[w], rs));
     }
     // the member's CRC32/ISIZE over all pieces (meaningful when every wave passed)
@@ -2163,16 +2182,16 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
         uint32_t* fin = (uint32_t*)(P + o_fin);
         CrcMemberArgs B{(const CrcPiece*)(P + o_pc), (const uint32_t*)(P + o_pcrc), fin + 12, 1, fin, fin + 1,
                         fin + 2, (uint64_t*)(fin + 4), (int32_t*)(fin + 6)};
-        RRG_LAUNCH(k_crc_members, 1, 32, 0, c->res_stream, B);
+        RRG_LAUNCH(k_crc_members, 1, 32, 0, c->stream, B);
         LAUNCHED(c);
-        CK(cudaMemcpyAsync(h_fin, fin, 32, cudaMemcpyDeviceToHost, c->res_stream));
+        RRG_LAUNCH(k_copy_words, 1, 32, 0, c->stream, (const uint32_t*)fin, h_fin, 8u);
+        LAUNCHED(c);
     }
     cudaEvent_t e_fin = nullptr;
     CK(mkev(&e_fin, true));
-    CK(cudaEventRecord(e_fin, c->res_stream));
+    CK(cudaEventRecord(e_fin, c->stream));
     auto drain = [&]() {
-        for (auto ws : c->wave_stream) cudaStreamSynchronize(ws);
-        cudaStreamSynchronize(c->res_stream);
+        cudaStreamSynchronize(c->stream);
         cudaStreamSynchronize(c->copy_stream);
     };
     // ---- deliver: pieces of each wave's output through a ring of pinned buffers
@@ -2247,7 +2266,20 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
     {
         float ms = 0;
         if (cudaEventElapsedTime(&ms, ev0, e_inf[Wn - 1]) == cudaSuccess) c->st.inflate_ms += ms;
-        if (cudaEventElapsedTime(&ms, ev0, e_fin) == cudaSuccess) c->st.resolve_ms += 0;  // overlapped
+        if (c->cfg.verbose >= 2) {  // the device timeline of every wave, from the end of the scan
+            for (uint32_t w = 0; w < Wn && (failed_wave < 0 || (int)w <= failed_wave); w++) {
+                float a = 0, b = 0, r = 0;
+                cudaEventElapsedTime(&a, ev0, e_inf[w]);
+                cudaEventElapsedTime(&b, ev0, e_chain[w]);
+                cudaEventElapsedTime(&r, ev0, e_res[w]);
+                std::fprintf(stderr, "[rrg-gpu] wave %u: %u sub-chunks, inflate done %.3f ms, chain %.3f ms, "
+                             "resolve+crc done %.3f ms\n", w, waves[w].n, a, b, r);
+            }
+            float f = 0;
+            cudaEventElapsedTime(&f, ev0, e_fin);
+            std::fprintf(stderr, "[rrg-gpu] member check %.3f ms; delivery loop %.3f ms on the host\n", f,
+                         now_ms() - t_start);
+        }
     }
     c->st.gpu_chunks += n;
     c->st.d2h_ms += now_ms() - t_start;
@@ -3365,9 +3397,6 @@ void rrg_gpu_destroy(rrg_ctx* c) {
     for (cudaEvent_t e : c->arr_events)
         if (e) cudaEventDestroy(e);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
-    for (cudaStream_t s : c->wave_stream)
-        if (s) cudaStreamDestroy(s);
-    if (c->res_stream) cudaStreamDestroy(c->res_stream);
     if (c->h_ring) cudaFreeHost(c->h_ring);
     if (c->h_wave) cudaFreeHost(c->h_wave);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);

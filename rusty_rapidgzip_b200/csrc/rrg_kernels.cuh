@@ -2591,6 +2591,12 @@ struct WaveArgs {
     uint32_t* exp_isize;
 };
 constexpr int WAVE_THREADS = 1024;
+
+// n status words to (mapped) host memory, so the host learns them without a
+// copy queued behind the output copies.
+__global__ void k_copy_words(const uint32_t* src, uint32_t* dst, uint32_t n) {
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
 constexpr uint64_t WAVE_PIECE = 256 * 1024;  // CRC piece bytes
 
 // Exclusive block-wide prefix of one value per thread; returns the total.
