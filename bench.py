@@ -45,6 +45,18 @@ def workload(name: str, size: int | None):
         key, make = f"zipf_{n}_s1_v{GEN_VERSION}", lambda: W.config1(n, seed=1)
         desc = {"workload": "zipf_text_level9_single_member", "uncompressed_bytes": n, "zlib_level": 9,
                 "vocabulary": 50000, "zipf_exponent": 1.1}
+    elif name == "zipf_plain":
+        # the same text as one zlib stream written by a single compressor (no
+        # 32 MiB pieces, no sync-flush points); slow to make at 1 GiB
+        n = size or (256 << 20)
+
+        def make():
+            raw = W.zipf_text(n, 1)
+            return raw, W.gzip_member(raw, 9, parallel_threshold=1 << 62)
+
+        key = f"zipfplain_{n}_s1_v{GEN_VERSION}"
+        desc = {"workload": "zipf_text_level9_single_member_one_zlib_stream", "uncompressed_bytes": n,
+                "zlib_level": 9, "vocabulary": 50000, "zipf_exponent": 1.1}
     elif name == "fastq64m":
         n = size or (64 << 20)
         key, make = f"fastq_{n}_s0_v{GEN_VERSION}", lambda: W.config0(n, seed=0)
@@ -673,7 +685,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="zipf1g", choices=["zipf1g", "fastq64m", "bgzf", "files", "serve", "stream"])
+    ap.add_argument("--workload", default="zipf1g",
+                    choices=["zipf1g", "zipf_plain", "fastq64m", "bgzf", "files", "serve", "stream"])
     ap.add_argument("--rates", default="10,50,200", help="serve: request rates (req/s)")
     ap.add_argument("--duration", type=float, default=20.0, help="serve: seconds of arrivals per rate")
     ap.add_argument("--max-outstanding", type=int, default=32, help="serve: waiting requests before rejecting")

@@ -752,8 +752,11 @@ int run_resolve(rrg_ctx* c, const std::vector<ResolveChunk>& rchunks, uint8_t* d
 // ------------------------------------------------------------ boundary scan
 // Every bit offset of the body tested on the device; returns the sorted
 // offsets that pass the block finder's full strict verification.
+// With `tiles` (sorted indices of scan tiles, each scan_threads x 16 bytes
+// from the body's 16-byte-aligned start), only those tiles are tested.
 int scan_boundaries(rrg_ctx* c, const uint8_t* body, uint64_t blen, std::vector<uint64_t>& verified,
-                    std::vector<uint64_t>* stored_out, rrg_error* err) {
+                    std::vector<uint64_t>* stored_out, rrg_error* err,
+                    const std::vector<uint32_t>* tiles = nullptr) {
     verified.clear();
     if (stored_out) stored_out->clear();
     if (blen < 4) return 0;
@@ -771,17 +774,31 @@ int scan_boundaries(rrg_ctx* c, const uint8_t* body, uint64_t blen, std::vector<
     uint64_t* surv = cand + cap;
     uint64_t* stored = surv + cap2;
     uint32_t* counts = (uint32_t*)c->ncand.p;  // [0] candidates, [1] survivors, [2] heavy queue, [3] stored
-    ScanArgs S{body, blen, cand, counts, cap, stored, counts + 3, cap3, 0, ~0ull};
+    ScanArgs S{body, blen, cand, counts, cap, stored, counts + 3, cap3, 0, ~0ull, nullptr, 0};
     // tile width: scan_threads x 16 bytes per block step (64, 128 or 256 threads)
     const uint32_t st = c->scan_threads;
     const uint64_t tb = (uint64_t)st * 16;
     const uint64_t n_tiles = ((uint64_t)((uintptr_t)body & 15) + blen + tb - 1) / tb;
+    if (tiles && !tiles->empty()) {
+        CK(dgrow(c->tiles, tiles->size() * 4));
+        CK(cudaMemcpyAsync(c->tiles.p, tiles->data(), tiles->size() * 4, cudaMemcpyHostToDevice, c->stream));
+    }
     auto scan = [&](uint64_t t_lo, uint64_t t_hi) -> int {
         if (t_hi <= t_lo) return 0;
         S.tile_lo = t_lo;
         S.tile_hi = t_hi;
+        uint64_t work = t_hi - t_lo;
+        if (tiles) {  // the listed tiles in [t_lo, t_hi)
+            const size_t a = std::lower_bound(tiles->begin(), tiles->end(), (uint32_t)t_lo) - tiles->begin();
+            const size_t b = std::lower_bound(tiles->begin(), tiles->end(), (uint32_t)std::min<uint64_t>(t_hi, ~0u)) -
+                             tiles->begin();
+            if (b <= a) return 0;
+            S.tile_list = (const uint32_t*)c->tiles.p + a;
+            S.n_list = (uint32_t)(b - a);
+            work = b - a;
+        }
         const uint32_t sgrid =
-            (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(t_hi - t_lo, (uint64_t)c->n_sm * (2048 / st)));
+            (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(work, (uint64_t)c->n_sm * (2048 / st)));
         if (st == 64) RRG_LAUNCH(k_scan_candidates<64>, sgrid, 64, 0, c->stream, S);
         else if (st == 128) RRG_LAUNCH(k_scan_candidates<128>, sgrid, 128, 0, c->stream, S);
         else RRG_LAUNCH(k_scan_candidates<256>, sgrid, 256, 0, c->stream, S);
@@ -1001,8 +1018,59 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
                 b++;
             }
             std::vector<uint64_t> verified, stored;
-            int rc0 = scan_boundaries(c, d_base + lo, hi - lo, verified, &stored, err);
+            // With automatic spacing only the bytes around each ideal start are
+            // scanned (a window of +-16 KiB holds one or more block starts of
+            // ordinary deflate output); targets whose window held none are
+            // scanned again +-256 KiB wide. Fixed spacing scans everything.
+            std::vector<uint64_t> ideal;  // bits from lo
+            for (size_t q = a; q < b && !fixed_g; q++) {
+                const MemberJob& j = jobs[big[q]];
+                const uint64_t b0 = (j.file_off + j.body_off - lo) * 8, b1 = (j.file_off + j.len - lo) * 8;
+                const uint64_t s0 = b0 + j.start_bit, s1 = j.stop_bit == ~0ull ? b1 : std::min(b1, b0 + j.stop_bit);
+                const uint64_t nbits = s1 > s0 ? s1 - s0 : 0;
+                const uint64_t K = std::max<uint64_t>(1, (nbits / 8 + G / 2) / G);
+                for (uint64_t k = 1; k < K; k++) ideal.push_back(s0 + nbits * k / K);
+            }
+            const uint64_t tb = (uint64_t)c->scan_threads * 16, mis = (uintptr_t)(d_base + lo) & 15;
+            const uint64_t n_tiles = (mis + (hi - lo) + tb - 1) / tb;
+            auto windows = [&](const std::vector<uint64_t>& at, uint64_t half, const std::vector<uint32_t>* skip) {
+                std::vector<uint32_t> t;
+                for (uint64_t x : at) {
+                    const uint64_t byte = x / 8;
+                    const uint64_t t0 = (mis + (byte > half ? byte - half : 0)) / tb;
+                    const uint64_t t1 = std::min(n_tiles - 1, (mis + byte + half) / tb);
+                    for (uint64_t k = t0; k <= t1; k++)
+                        if (!skip || !std::binary_search(skip->begin(), skip->end(), (uint32_t)k)) t.push_back((uint32_t)k);
+                }
+                std::sort(t.begin(), t.end());
+                t.erase(std::unique(t.begin(), t.end()), t.end());
+                return t;
+            };
+            constexpr uint64_t NEAR = 16 << 10, WIDE = 256 << 10;
+            std::vector<uint32_t> tiles;
+            const bool windowed = !fixed_g && !ideal.empty() && n_tiles <= 0xffffffffull &&
+                                  (tiles = windows(ideal, NEAR, nullptr)).size() * 2 < n_tiles;
+            int rc0 = scan_boundaries(c, d_base + lo, hi - lo, verified, &stored, err, windowed ? &tiles : nullptr);
             if (rc0) return rc0;
+            if (windowed) {
+                std::vector<uint64_t> missing;
+                for (uint64_t x : ideal) {
+                    auto it = std::lower_bound(verified.begin(), verified.end(), x > NEAR * 8 ? x - NEAR * 8 : 0);
+                    if (it == verified.end() || *it > x + NEAR * 8) missing.push_back(x);
+                }
+                if (!missing.empty()) {
+                    const std::vector<uint32_t> more = windows(missing, WIDE, &tiles);
+                    std::vector<uint64_t> v2, s2;
+                    if (!more.empty()) {
+                        rc0 = scan_boundaries(c, d_base + lo, hi - lo, v2, &s2, err, &more);
+                        if (rc0) return rc0;
+                        verified.insert(verified.end(), v2.begin(), v2.end());
+                        std::sort(verified.begin(), verified.end());
+                        stored.insert(stored.end(), s2.begin(), s2.end());
+                        std::sort(stored.begin(), stored.end());
+                    }
+                }
+            }
             // verified offsets are sorted bit offsets from `lo`
             for (size_t q = a; q < b; q++) {
                 MemberJob& j = jobs[big[q]];

@@ -1859,6 +1859,8 @@ struct ScanArgs {
     uint32_t* n_stored;
     uint32_t stored_cap;
     uint64_t tile_lo, tile_hi;  // the tiles this launch covers (input that has arrived)
+    const uint32_t* tile_list;  // when set: only these tiles (sorted), n_list of them
+    uint32_t n_list;
 };
 
 // 32 bits of the staged tile starting at bit b (b + 32 <= 8 * tile bytes)
@@ -1887,7 +1889,10 @@ __global__ void __launch_bounds__(ST) k_scan_candidates(ScanArgs A) {
     const uint64_t n_tiles = (hi + TILE - 1) / TILE;
     const uint64_t t_end = A.tile_hi < n_tiles ? A.tile_hi : n_tiles;
     uint8_t* tb = reinterpret_cast<uint8_t*>(tile);
-    for (uint64_t t = A.tile_lo + blockIdx.x; t < t_end; t += gridDim.x) {
+    const uint64_t n_iter = A.tile_list ? A.n_list : (t_end > A.tile_lo ? t_end - A.tile_lo : 0);
+    for (uint64_t it = blockIdx.x; it < n_iter; it += gridDim.x) {
+        const uint64_t t = A.tile_list ? A.tile_list[it] : A.tile_lo + it;
+        if (t >= n_tiles) continue;  // uniform over the block
         const uint64_t t0 = t * TILE;
         if (threadIdx.x == 0) s_n = 0;
         for (uint32_t q = threadIdx.x; q < (TILE + SCAN_HALO) / 16; q += blockDim.x) {

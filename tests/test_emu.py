@@ -571,3 +571,18 @@ def test_pipelined_host_path_falls_back(emu_decoder_factory):
         d.decode_host(bytes(bad), lambda b: None)
     assert ge.value.code == oe.value.code
     assert ge.value.expected == oe.value.expected and ge.value.got_crc == oe.value.got_crc
+
+
+@pytest.mark.parametrize("kind", ["zipf", "random"])
+def test_windowed_boundary_scan(emu_decoder_factory, kind):
+    """With automatic spacing only the bytes around each ideal sub-chunk start
+    are scanned (wider where a window holds no start, as in stored data); the
+    bytes equal the generator's and the checked path keeps every start."""
+    raw = W.make_content(kind, (2600 if kind == "zipf" else 1500) << 10, 20)
+    gz = W.gzip_member(raw, W.CONTENT_LEVEL[kind])
+    d = emu_decoder_factory(host_pipeline=-1)
+    src = np.frombuffer(gz, dtype=np.uint8).copy()
+    dst = np.zeros(len(raw) + 64, dtype=np.uint8)
+    n, st = d.decode_device(haddr(src), len(gz), haddr(dst), dst.size)
+    assert n == len(raw) and dst[:n].tobytes() == raw
+    assert st.gpu_chunks >= 4 and st.speculation_failures == 0
