@@ -278,10 +278,13 @@ def config3_files(n_files: int = 2000, seed: int = 3, lo: int = 4 << 10, hi: int
 
 
 def config3_stream(n_files: int = 2000, seed: int = 3, lo: int = 4 << 10, hi: int = 256 << 20,
-                   threads: int | None = None):
-    """config3_files generated in parallel, yielded in order as (raw, gz)."""
+                   threads: int | None = None, only=None):
+    """config3_files generated in parallel, yielded in order as (raw, gz);
+    with ``only`` (indices), just those files."""
     import os
     spec = config3_sizes(n_files, seed, lo, hi)
+    if only is not None:
+        spec = [spec[i] for i in only]
 
     def one(t):
         size, kind, s = t
