@@ -68,7 +68,9 @@ typedef struct rrg_error {
 
 /* Mirrors Config (lib.rs:50-100). */
 typedef struct rrg_config {
-    uint32_t num_threads;        /* host threads for sink delivery/IO; 0 = all cores (Config::num_threads) */
+    uint32_t num_threads;        /* host threads that read a regular file in rrg_gpu_read_gz, in parallel,
+                                    into page-locked memory; 0 = one per core, at most 16
+                                    (Config::num_threads: the host side's parallelism) */
     uint64_t chunk_size_bytes;   /* sink delivery granularity in compressed bytes; 0 = 4 MiB (Config::chunk_size_bytes) */
     int32_t verbose;             /* 0 = Verbosity::Off, 1 = Verbosity::On (stderr lines) */
     int32_t device;              /* CUDA device ordinal; -1 = current device */
@@ -106,6 +108,19 @@ typedef struct rrg_stats {
  * non-zero to close the sink (decoding stops early and the call returns RRG_OK,
  * like a disconnected Sender in pipeline.rs:1028-1030). */
 typedef int (*rrg_sink_fn)(void* user, const uint8_t* data, size_t len);
+
+/* Destination provider (Config::recycle_rx, lib.rs:58-69: the reference's
+ * decode workers pull warm output buffers with try_recv, pipeline.rs:603-607).
+ * Called before a piece of output leaves the device, with the piece's size:
+ * returns a buffer of at least `want` bytes (its capacity in *cap), into which
+ * the piece is copied straight from the device and which the following sink
+ * call receives as `data`. The consumer owns it from then on and may hand it
+ * back through later calls (the recycle_tx side). NULL, or a capacity below
+ * `want`, makes the library use its own staging for that piece. Page-locked
+ * buffers (cudaMallocHost, cudaHostRegister) are filled at the link's rate;
+ * pageable ones are staged by the CUDA runtime. Called on the decoding thread,
+ * in stream order, at most a few pieces ahead of the sink. */
+typedef uint8_t* (*rrg_buffer_fn)(void* user, size_t want, size_t* cap);
 
 typedef struct rrg_ctx rrg_ctx;
 
@@ -168,6 +183,15 @@ void rrg_index_free(rrg_index* idx);
  * pageable or pinned). Replaces read_gz's mmap'd InputBytes (pipeline.rs:47-50). */
 int rrg_gpu_decode_host(rrg_ctx* ctx, const uint8_t* data, size_t len, rrg_sink_fn sink,
                         void* user, rrg_stats* stats, rrg_error* err);
+
+/* rrg_gpu_decode_host and rrg_gpu_read_gz with a destination provider (read_gz
+ * with Config::recycle_rx/recycle_tx set, lib.rs:58-69): each piece of output
+ * is copied from the device into a buffer `get` returns, and `sink` receives
+ * that buffer. `user` is passed to both. */
+int rrg_gpu_decode_host_into(rrg_ctx* ctx, const uint8_t* data, size_t len, rrg_buffer_fn get,
+                             rrg_sink_fn sink, void* user, rrg_stats* stats, rrg_error* err);
+int rrg_gpu_read_gz_into(rrg_ctx* ctx, const char* path, rrg_buffer_fn get, rrg_sink_fn sink,
+                         void* user, rrg_stats* stats, rrg_error* err);
 
 /* Device-resident decode: `d_in` (device, `len` bytes) is a whole gzip file;
  * the decompressed stream is written contiguously to `d_out` (device, capacity

@@ -106,6 +106,7 @@ class _Stats(C.Structure):
 
 
 SINK_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_uint8), C.c_size_t)
+BUF_FN = C.CFUNCTYPE(C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t))
 READ_FN = C.CFUNCTYPE(C.c_int64, C.c_void_p, C.POINTER(C.c_uint8), C.c_size_t)
 
 
@@ -251,6 +252,8 @@ def load_library(path: str | None = None):
         L.rrg_gpu_destroy.argtypes = [vp]
         L.rrg_gpu_read_gz.argtypes = [vp, C.c_char_p, SINK_FN, vp, S, E]
         L.rrg_gpu_decode_host.argtypes = [vp, vp, sz, SINK_FN, vp, S, E]
+        L.rrg_gpu_decode_host_into.argtypes = [vp, vp, sz, BUF_FN, SINK_FN, vp, S, E]
+        L.rrg_gpu_read_gz_into.argtypes = [vp, C.c_char_p, BUF_FN, SINK_FN, vp, S, E]
         L.rrg_gpu_read_stream.argtypes = [vp, READ_FN, vp, SINK_FN, vp, u64, S, E]
         L.rrg_gpu_index_build.argtypes = [vp, vp, sz, u64, C.POINTER(vp), S, E]
         L.rrg_gpu_read_range.argtypes = [vp, vp, sz, vp, u64, u64, vp, E]
@@ -431,6 +434,57 @@ class Decoder:
     def read_gz(self, path, sink) -> DecodeStats:
         """read_gz (lib.rs:366-496) for a file path."""
         return self._run(self._L.rrg_gpu_read_gz, os.fsencode(os.fspath(path)), sink=sink)
+
+    def _run_into(self, fn, arg0, arg1, recycle, sink) -> DecodeStats:
+        """`recycle(want) -> (address, capacity) | None` supplies destination
+        buffers (Config::recycle_rx); `sink(address, length)` then receives
+        each filled buffer (the consumer's; hand it back through `recycle`)."""
+        failure = []
+
+        def get(_u, want, cap):
+            try:
+                r = recycle(int(want))
+            except BaseException as ex:  # surfaced after the call returns
+                failure.append(ex)
+                r = None
+            if not r:
+                return None
+            cap[0] = int(r[1])
+            return int(r[0])
+
+        def cb(_u, p, n):
+            try:
+                r = sink(C.cast(p, C.c_void_p).value, int(n))
+            except SinkClosed:
+                return 1
+            except BaseException as ex:
+                failure.append(ex)
+                return 1
+            return 1 if r is False else 0
+
+        st, e = _Stats(), _Error()
+        fn(self._ctx, arg0, arg1, BUF_FN(get), SINK_FN(cb), None, C.byref(st), C.byref(e))
+        if failure:
+            raise failure[0]
+        _raise(e)
+        return DecodeStats._from(st)
+
+    def decode_host_into(self, data, recycle, sink) -> DecodeStats:
+        """decode_host whose output pieces land in buffers from `recycle`."""
+        addr, n, keep = _host_buffer(data)
+        stats = self._run_into(self._L.rrg_gpu_decode_host_into, addr, n, recycle, sink)
+        del keep
+        return stats
+
+    def read_gz_into(self, path, recycle, sink) -> DecodeStats:
+        """read_gz whose output pieces land in buffers from `recycle`."""
+        p = os.fsencode(os.fspath(path))
+        L = self._L
+
+        def fn(ctx, path_, _unused, get, cb, user, st, e):
+            return L.rrg_gpu_read_gz_into(ctx, path_, get, cb, user, st, e)
+
+        return self._run_into(fn, p, None, recycle, sink)
 
     def read_stream(self, source, sink, stripe_bytes: int = 0) -> DecodeStats:
         """read_gz's non-seekable route (lib.rs:378-431, streaming.rs:389-614):

@@ -251,6 +251,8 @@ struct rrg_ctx {
     size_t h_stage_cap = 0;
     uint8_t* h_in = nullptr;
     size_t h_in_cap = 0;
+    uint8_t* h_file = nullptr;  // page-locked copy of a file read by rrg_gpu_read_gz
+    size_t h_file_cap = 0;
 
     // tunables
     uint64_t gpu_chunk = 0;
@@ -276,6 +278,9 @@ struct rrg_ctx {
     uint8_t* h_wave = nullptr;       // pinned wave outcomes
     size_t h_wave_cap = 0;
     bool pipeline = true;            // take the pipelined path where it applies
+    // destination provider of the current *_into call (null: library staging)
+    rrg_buffer_fn get_buf = nullptr;
+    void* get_user = nullptr;
     DBuf sniff;                // per-file header results of a batch
         // BGZF route: device member table and the captured decode graph
     DBuf bg_bcount, bg_bbase, bg_coff, bg_csize, bg_small;
@@ -1900,9 +1905,16 @@ int deliver(rrg_ctx* c, const uint8_t* d_src, uint64_t n, rrg_sink_fn sink, void
     cudaEvent_t ev[2];
     CK(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+    uint8_t* dst[2] = {c->h_stage[0], c->h_stage[1]};  // the consumer's buffer, or the staging buffer
     auto issue = [&](uint64_t i) -> cudaError_t {
         uint64_t o = i * P, l = std::min(P, n - o);
-        cudaError_t e = cudaMemcpyAsync(c->h_stage[i & 1], d_src + o, l, cudaMemcpyDeviceToHost, c->stream);
+        dst[i & 1] = c->h_stage[i & 1];
+        if (c->get_buf) {
+            size_t cap = 0;
+            uint8_t* b = c->get_buf(c->get_user, (size_t)l, &cap);
+            if (b && cap >= l) dst[i & 1] = b;
+        }
+        cudaError_t e = cudaMemcpyAsync(dst[i & 1], d_src + o, l, cudaMemcpyDeviceToHost, c->stream);
         if (e == cudaSuccess) e = cudaEventRecord(ev[i & 1], c->stream);
         return e;
     };
@@ -1916,7 +1928,7 @@ int deliver(rrg_ctx* c, const uint8_t* d_src, uint64_t n, rrg_sink_fn sink, void
         }
         uint64_t o = i * P, l = std::min(P, n - o);
         c->st.chunks_decoded++;
-        if (sink(user, c->h_stage[i & 1], (size_t)l)) {
+        if (sink(user, dst[i & 1], (size_t)l)) {
             *closed = true;
             break;
         }
@@ -2277,11 +2289,18 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
     size_t issued = 0, delivered = 0;
     int failed_wave = -1;
     const double t_start = now_ms();
+    uint8_t* slot_dst[RING];  // per ring slot: the consumer's buffer or the library's piece buffer
     auto issue = [&](size_t i) -> cudaError_t {
         const Piece& pc = pcs[i];
+        slot_dst[i % RING] = c->h_ring + (i % RING) * PS;
+        if (c->get_buf) {
+            size_t cap = 0;
+            uint8_t* b = c->get_buf(c->get_user, (size_t)pc.len, &cap);
+            if (b && cap >= pc.len) slot_dst[i % RING] = b;
+        }
         cudaError_t e = cudaStreamWaitEvent(c->copy_stream, e_res[pc.wave], 0);
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(c->h_ring + (i % RING) * PS, tgt.p + pc.off, pc.len, cudaMemcpyDeviceToHost,
+            e = cudaMemcpyAsync(slot_dst[i % RING], tgt.p + pc.off, pc.len, cudaMemcpyDeviceToHost,
                                 c->copy_stream);
         if (e == cudaSuccess) e = cudaEventRecord(ring_ev[i % RING], c->copy_stream);
         return e;
@@ -2322,7 +2341,7 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
             }
         }
         c->st.chunks_decoded++;
-        if (sink && sink(user, c->h_ring + (delivered % RING) * PS, (size_t)pc.len)) {
+        if (sink && sink(user, slot_dst[delivered % RING], (size_t)pc.len)) {
             *closed = true;
             drain();
             *total_out = total;
@@ -3125,9 +3144,10 @@ void release_scratch(rrg_ctx* c) {
 
 // ------------------------------------------------------------ result buffers
 // Serving results are host buffers the caller releases with rrg_gpu_free.
-// Freed buffers of 1 MiB and more are kept by size class (powers of two, at
-// most 32 GiB in all) and handed out again, so a steady request stream writes
-// into memory whose pages are already mapped instead of faulting in fresh ones.
+// Buffers of 1 MiB and more are page-locked (the engines copy results into
+// them straight from the device at the link's rate) and, once freed, kept by
+// size class (powers of two, at most 32 GiB in all) and handed out again, so a
+// steady request stream neither pins nor faults in fresh memory.
 struct ResultPool {
     std::mutex mu;
     std::unordered_map<void*, int> cls;           // every pooled block ever handed out -> class
@@ -3154,8 +3174,13 @@ void* result_alloc(uint64_t n) {
             return b;
         }
     }
-    void* b = std::malloc(1ull << k);
-    if (b) {
+    void* b = nullptr;
+    if (cudaMallocHost(&b, 1ull << k) != cudaSuccess) {
+        cudaGetLastError();  // not sticky: fall back to pageable memory
+        b = nullptr;
+    }
+    if (!b) return std::malloc(1ull << k);
+    {
         std::lock_guard<std::mutex> g(P.mu);
         P.cls[b] = k;
     }
@@ -3177,6 +3202,8 @@ void result_free(void* b) {
                 return;
             }
             P.cls.erase(it);
+            cudaFreeHost(b);
+            return;
         }
     }
     std::free(b);
@@ -3299,23 +3326,11 @@ void engine_loop(Server* S, rrg_ctx* E) {
                 if (!d.out) {
                     d.status = RRG_ERR_OUT_OF_MEMORY;
                     d.len = 0;
-                } else if (out_len[i]) {
-                    // through the engine's pinned double buffer: each piece's copy
-                    // to the result overlaps the next piece's transfer
-                    struct Dst {
-                        uint8_t* p;
-                        size_t at;
-                    } dst{d.out, 0};
-                    auto copy_sink = [](void* u, const uint8_t* p, size_t len) -> int {
-                        Dst* t = (Dst*)u;
-                        std::memcpy(t->p + t->at, p, len);
-                        t->at += len;
-                        return 0;
-                    };
-                    bool closed = false;
-                    rrg_error e2{};
-                    if (deliver(E, (const uint8_t*)E->out.p + out_off[i], out_len[i], copy_sink, &dst, &closed, &e2))
-                        d.status = RRG_ERR_CUDA;
+                } else if (out_len[i] &&
+                           cudaMemcpyAsync(d.out, (const uint8_t*)E->out.p + out_off[i], out_len[i],
+                                           cudaMemcpyDeviceToHost, E->stream) != cudaSuccess) {
+                    // one copy per result, straight into its (page-locked) buffer
+                    d.status = RRG_ERR_CUDA;
                 }
             }
             fin.push_back(d);
@@ -3462,6 +3477,7 @@ void rrg_gpu_destroy(rrg_ctx* c) {
         if (p) cudaFreeHost(p);
     if (c->h_bg) cudaFreeHost(c->h_bg);
     if (c->h_in) cudaFreeHost(c->h_in);
+    if (c->h_file) cudaFreeHost(c->h_file);
     for (cudaEvent_t e : c->arr_events)
         if (e) cudaEventDestroy(e);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
@@ -3515,17 +3531,82 @@ int rrg_gpu_read_gz(rrg_ctx* c, const char* path, rrg_sink_fn sink, void* user, 
         close(fd);
         return rc;
     }
-    std::vector<uint8_t> data((size_t)sb.st_size);
-    size_t got = 0;
-    while (got < data.size()) {
-        ssize_t r = read(fd, data.data() + got, data.size() - got);
-        if (r <= 0) break;
-        got += (size_t)r;
+    // The file goes into page-locked memory (so the copy to the device runs at
+    // the link's rate), read by num_threads threads in parallel (0: one per
+    // core, at most 16), each a run of at least 8 MiB.
+    const size_t size = (size_t)sb.st_size;
+    std::vector<uint8_t> fallback;
+    uint8_t* buf = nullptr;
+    if (size <= (16ull << 30)) {
+        if (c->h_file_cap < size) {
+            if (c->h_file) cudaFreeHost(c->h_file);
+            c->h_file = nullptr;
+            c->h_file_cap = 0;
+            if (cudaMallocHost((void**)&c->h_file, std::max<size_t>(size, 1)) == cudaSuccess) c->h_file_cap = size;
+            else cudaGetLastError();
+        }
+        if (c->h_file_cap >= size) buf = c->h_file;
     }
-    data.resize(got);
+    if (!buf) {
+        fallback.resize(size);
+        buf = fallback.data();
+    }
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t want = c->cfg.num_threads ? c->cfg.num_threads : std::min(hw, 16u);
+    const size_t T = std::max<size_t>(1, std::min(want, size / (8u << 20)));
+    std::vector<size_t> got(T, 0);
+    auto reader = [&](size_t t) {
+        const size_t a = size * t / T, b = size * (t + 1) / T;
+        size_t at = a;
+        while (at < b) {
+            const ssize_t r = pread(fd, buf + at, b - at, (off_t)at);
+            if (r < 0 && errno == EINTR) continue;
+            if (r <= 0) break;
+            at += (size_t)r;
+        }
+        got[t] = at - a;
+    };
+    if (T == 1) {
+        reader(0);
+    } else {
+        std::vector<std::thread> th;
+        for (size_t t = 0; t < T; t++) th.emplace_back(reader, t);
+        for (auto& x : th) x.join();
+    }
     close(fd);
+    size_t n = 0;
+    for (size_t t = 0; t < T && got[t] == size * (t + 1) / T - size * t / T; t++) n = size * (t + 1) / T;
     if (err) std::memset(err, 0, sizeof(*err));
-    return decode_host_impl(c, data.data(), data.size(), sink, user, stats, err);
+    return decode_host_impl(c, buf, n, sink, user, stats, err);
+}
+
+// The destination provider is the context's for the duration of one call.
+struct ProviderScope {
+    rrg_ctx* c;
+    ProviderScope(rrg_ctx* ctx, rrg_buffer_fn get, void* user) : c(ctx) {
+        if (c) {
+            c->get_buf = get;
+            c->get_user = user;
+        }
+    }
+    ~ProviderScope() {
+        if (c) {
+            c->get_buf = nullptr;
+            c->get_user = nullptr;
+        }
+    }
+};
+
+int rrg_gpu_decode_host_into(rrg_ctx* c, const uint8_t* data, size_t len, rrg_buffer_fn get, rrg_sink_fn sink,
+                             void* user, rrg_stats* stats, rrg_error* err) {
+    ProviderScope scope(c, get, user);
+    return rrg_gpu_decode_host(c, data, len, sink, user, stats, err);
+}
+
+int rrg_gpu_read_gz_into(rrg_ctx* c, const char* path, rrg_buffer_fn get, rrg_sink_fn sink, void* user,
+                         rrg_stats* stats, rrg_error* err) {
+    ProviderScope scope(c, get, user);
+    return rrg_gpu_read_gz(c, path, sink, user, stats, err);
 }
 
 int rrg_gpu_index_build(rrg_ctx* c, const uint8_t* data, size_t len, uint64_t spacing, rrg_index** out,

@@ -586,3 +586,41 @@ def test_windowed_boundary_scan(emu_decoder_factory, kind):
     n, st = d.decode_device(haddr(src), len(gz), haddr(dst), dst.size)
     assert n == len(raw) and dst[:n].tobytes() == raw
     assert st.gpu_chunks >= 4 and st.speculation_failures == 0
+
+
+@pytest.mark.parametrize("pipelined", [False, True])
+def test_destination_provider(emu_decoder_factory, tmp_path, pipelined):
+    """read_gz with recycled buffers (Config::recycle_rx/tx): every piece lands
+    in a buffer the provider handed out and the sink receives that buffer; a
+    buffer handed back is used again; a provider that declines a piece leaves
+    it to the library's staging. Both the plain and the pipelined host paths."""
+    import ctypes
+    raw, gz = W.config1((2600 if pipelined else 300) << 10, seed=21)
+    path = tmp_path / "f.gz"
+    path.write_bytes(gz)
+    pool, handed, out = [], set(), []
+    calls = [0]
+
+    def recycle(want):
+        calls[0] += 1
+        if calls[0] % 5 == 0:
+            return None  # declined: the library stages this piece
+        b = pool.pop() if pool and pool[-1].size >= want else np.empty(max(want, 1 << 20), dtype=np.uint8)
+        handed.add(b.ctypes.data)
+        keep[b.ctypes.data] = b
+        return b.ctypes.data, b.size
+
+    keep = {}
+
+    def sink(addr, n):
+        out.append(ctypes.string_at(addr, n))
+        if addr in keep:
+            pool.append(keep.pop(addr))  # recycle_tx: back to the provider
+
+    d = emu_decoder_factory(host_pipeline=0 if pipelined else -1)
+    st = d.read_gz_into(path, recycle, sink)
+    assert b"".join(out) == raw
+    assert calls[0] >= 1 and (st.pipeline_waves >= 2) == pipelined
+    out.clear()
+    st = d.decode_host_into(gz, recycle, sink)
+    assert b"".join(out) == raw
