@@ -651,58 +651,135 @@ int ensure_out(rrg_ctx* c, OutTarget& t, uint64_t need, uint64_t keep, rrg_error
 }
 
 // ------------------------------------------------------------ resolve
-// Window maps, group base windows, chunk tails, then the rest of every chunk,
-// into d_dst. Chunks of one job are consecutive in `rchunks` with rising
-// out_start; the job's first chunk has out_start == job_out. Returns 0 or an
-// error code; a failure names its chunk in *bad_chunk.
+// The resolve kernels' grouping of a run of jobs' chunks (consecutive in the
+// chunk table): groups of consecutive chunks sized so one job's groups fill
+// the SMs (k_win_maps runs one block per group, chunk after chunk),
+// supergroups of about sqrt(groups) groups, and the tail units.
+struct ResTables {
+    std::vector<ResGroup> groups, supers;
+    std::vector<ResJob> jobs;
+    std::vector<uint32_t> chunk_group, group_super;
+    std::vector<uint64_t> tail_units;  // groups + 1
+    // one device blob: groups | supers | jobs | chunk_group | group_super | tail_units
+    size_t o_sup = 0, o_job = 0, o_cg = 0, o_gs = 0, o_tu = 0, bytes = 0;
+    void layout() {
+        o_sup = round8(groups.size() * sizeof(ResGroup));
+        o_job = o_sup + round8(supers.size() * sizeof(ResGroup));
+        o_cg = o_job + round8(jobs.size() * sizeof(ResJob));
+        o_gs = o_cg + round8(chunk_group.size() * 4);
+        o_tu = o_gs + round8(group_super.size() * 4);
+        bytes = o_tu + tail_units.size() * 8;
+    }
+    void write(uint8_t* dst) const {
+        std::memcpy(dst, groups.data(), groups.size() * sizeof(ResGroup));
+        std::memcpy(dst + o_sup, supers.data(), supers.size() * sizeof(ResGroup));
+        std::memcpy(dst + o_job, jobs.data(), jobs.size() * sizeof(ResJob));
+        std::memcpy(dst + o_cg, chunk_group.data(), chunk_group.size() * 4);
+        std::memcpy(dst + o_gs, group_super.data(), group_super.size() * 4);
+        std::memcpy(dst + o_tu, tail_units.data(), tail_units.size() * 8);
+    }
+};
+
+void build_res_tables(const std::vector<uint32_t>& job_chunks, uint32_t n_sm, ResTables& T) {
+    T = ResTables{};
+    uint32_t c0 = 0;
+    for (uint32_t cj : job_chunks) {
+        const uint32_t S = std::max<uint32_t>(1, (cj + n_sm - 1) / n_sm);
+        const uint32_t g0 = (uint32_t)T.groups.size();
+        for (uint32_t f = c0; f < c0 + cj; f += S) {
+            const uint32_t n = std::min(S, c0 + cj - f);
+            for (uint32_t k = 0; k < n; k++) T.chunk_group.push_back((uint32_t)T.groups.size());
+            T.groups.push_back(ResGroup{f, n});
+        }
+        const uint32_t ng = (uint32_t)T.groups.size() - g0;
+        const uint32_t SG = std::max<uint32_t>(1, (uint32_t)std::ceil(std::sqrt((double)ng)));
+        const uint32_t s0 = (uint32_t)T.supers.size();
+        for (uint32_t g = g0; g < g0 + ng; g += SG) {
+            const uint32_t n = std::min(SG, g0 + ng - g);
+            for (uint32_t q = 0; q < n; q++) T.group_super.push_back((uint32_t)T.supers.size());
+            T.supers.push_back(ResGroup{g, n});
+        }
+        T.jobs.push_back(ResJob{s0, (uint32_t)T.supers.size() - s0});
+        c0 += cj;
+    }
+    T.tail_units.assign(T.groups.size() + 1, 0);
+    for (size_t g = 0; g < T.groups.size(); g++)
+        T.tail_units[g + 1] = T.tail_units[g] + (T.groups[g].n + RES_TAIL_CHUNKS - 1) / RES_TAIL_CHUNKS;
+    T.layout();
+}
+
+// Device pointers of a tables blob at `dev`, and the map arrays at `win`.
+void res_args(ResolveArgs& R, const ResTables& T, const uint8_t* dev, uint16_t* win, uint32_t n_chunks) {
+    R.n_chunks = n_chunks;
+    R.groups = (const ResGroup*)dev;
+    R.n_groups = (uint32_t)T.groups.size();
+    R.supers = (const ResGroup*)(dev + T.o_sup);
+    R.n_supers = (uint32_t)T.supers.size();
+    R.jobs = (const ResJob*)(dev + T.o_job);
+    R.n_jobs = (uint32_t)T.jobs.size();
+    R.chunk_group = (const uint32_t*)(dev + T.o_cg);
+    R.group_super = (const uint32_t*)(dev + T.o_gs);
+    R.tail_units = (const uint64_t*)(dev + T.o_tu);
+    const size_t W = WINDOW;
+    R.maps = win;
+    R.gmaps = R.maps + (size_t)n_chunks * W;
+    R.bases = R.gmaps + (size_t)R.n_groups * W;
+    R.tmaps = R.bases + (size_t)R.n_groups * W;
+    R.sbases = R.tmaps + (size_t)R.n_supers * W;
+}
+size_t res_win_bytes(const ResTables& T, uint32_t n_chunks) {
+    return ((size_t)n_chunks + 2 * T.groups.size() + 2 * T.supers.size()) * WINDOW * 2;
+}
+
+// The six resolve launches on `s` (tables and head segments already on the device).
+int launch_resolve(rrg_ctx* c, const ResolveArgs& R, cudaStream_t s, rrg_error* err) {
+    const uint32_t nsm = c->n_sm;
+    RRG_LAUNCH(k_win_maps, std::min<uint32_t>(R.n_groups, nsm), WM_THREADS, WM_SMEM, s, R);
+    LAUNCHED(c);
+    RRG_LAUNCH(k_win_supers, std::min<uint32_t>(R.n_supers, nsm), WM_THREADS, WINDOW * 2, s, R);
+    LAUNCHED(c);
+    RRG_LAUNCH(k_win_bases, std::min<uint32_t>(R.n_jobs, nsm), WM_THREADS, WINDOW * 2, s, R);
+    LAUNCHED(c);
+    const uint64_t ex = (uint64_t)R.n_groups * (WINDOW / 8);
+    RRG_LAUNCH(k_win_expand, (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((ex + 255) / 256, nsm * 8ull)),
+               RES_THREADS, 0, s, R);
+    LAUNCHED(c);
+    RRG_LAUNCH(k_res_tails, nsm * 3, RES_THREADS, WINDOW * 2, s, R);
+    LAUNCHED(c);
+    RRG_LAUNCH(k_res_heads, nsm * 4, RES_THREADS, 0, s, R);
+    LAUNCHED(c);
+    return 0;
+}
+
+// Window maps, bases, chunk tails, then the rest of every chunk, into d_dst.
+// Chunks of one job are consecutive in `rchunks` with rising out_start; the
+// job's first chunk has out_start == job_out. Returns 0 or an error code; a
+// failure names its chunk in *bad_chunk.
 int run_resolve(rrg_ctx* c, const std::vector<ResolveChunk>& rchunks, uint8_t* d_dst, rrg_error* err,
                 int64_t* bad_chunk = nullptr) {
     const uint32_t nc = (uint32_t)rchunks.size();
     if (!nc) return 0;
-    // groups: runs of about sqrt(0.7 x chunks of the job) consecutive chunks,
-    // which balances the chunk-after-chunk map building inside a group against
-    // the group-after-group base pass of the job
-    std::vector<ResGroup> groups;
-    std::vector<ResJob> jobs;
-    std::vector<uint32_t> chunk_group(nc);
+    std::vector<uint32_t> job_chunks;
     for (uint32_t a = 0; a < nc;) {
         uint32_t b = a + 1;
         while (b < nc && rchunks[b].job_out == rchunks[a].job_out && rchunks[b].out_start > rchunks[b - 1].out_start)
             b++;
-        const uint32_t cj = b - a;
-        const uint32_t S = std::max<uint32_t>(1, (uint32_t)std::ceil(std::sqrt(0.7 * cj)));
-        jobs.push_back(ResJob{(uint32_t)groups.size(), (cj + S - 1) / S});
-        for (uint32_t f = a; f < b; f += S) {
-            const uint32_t n = std::min(S, b - f);
-            for (uint32_t k = f; k < f + n; k++) chunk_group[k] = (uint32_t)groups.size();
-            groups.push_back(ResGroup{f, n});
-        }
+        job_chunks.push_back(b - a);
         a = b;
     }
-    const uint32_t ng = (uint32_t)groups.size(), nj = (uint32_t)jobs.size();
-    // per chunk: tail tiles and head segments, as prefixes the kernels search
-    std::vector<uint64_t> pre(2 * (size_t)(nc + 1));
-    uint64_t* tt = pre.data();
-    uint64_t* hs = pre.data() + nc + 1;
-    tt[0] = hs[0] = 0;
-    for (uint32_t k = 0; k < nc; k++) {
-        const uint64_t n = rchunks[k].n_cells;
-        const uint32_t lo = res_tail_lo(n) & ~(uint32_t)(RES_TAIL_TILE - 1);
-        tt[k + 1] = tt[k] + (WINDOW - lo) / RES_TAIL_TILE;
-        hs[k + 1] = hs[k] + (res_head_end(n) + RES_HEAD_SEG - 1) / RES_HEAD_SEG;
-    }
-    // one upload: chunks, groups, jobs, chunk_group, prefixes
-    const size_t o_grp = round8(nc * sizeof(ResolveChunk)), o_job = o_grp + round8(ng * sizeof(ResGroup)),
-                 o_cg = o_job + round8(nj * sizeof(ResJob)), o_pre = o_cg + round8(nc * 4),
-                 total = o_pre + pre.size() * 8;
+    ResTables T;
+    build_res_tables(job_chunks, c->n_sm, T);
+    std::vector<uint64_t> hs(nc + 1, 0);
+    for (uint32_t k = 0; k < nc; k++)
+        hs[k + 1] = hs[k] + (res_head_end(rchunks[k].n_cells) + RES_HEAD_SEG - 1) / RES_HEAD_SEG;
+    // one upload: chunks | head segments | tables
+    const size_t o_hs = round8(nc * sizeof(ResolveChunk)), o_t = o_hs + round8((nc + 1) * 8), total = o_t + T.bytes;
     std::vector<uint8_t> blob(total);
     std::memcpy(blob.data(), rchunks.data(), nc * sizeof(ResolveChunk));
-    std::memcpy(blob.data() + o_grp, groups.data(), ng * sizeof(ResGroup));
-    std::memcpy(blob.data() + o_job, jobs.data(), nj * sizeof(ResJob));
-    std::memcpy(blob.data() + o_cg, chunk_group.data(), nc * 4);
-    std::memcpy(blob.data() + o_pre, pre.data(), pre.size() * 8);
+    std::memcpy(blob.data() + o_hs, hs.data(), (nc + 1) * 8);
+    T.write(blob.data() + o_t);
     CK(dgrow(c->chunks, total));
-    CK(dgrow(c->win, ((size_t)nc + ng) * WINDOW * 2));
+    CK(dgrow(c->win, res_win_bytes(T, nc)));
     CK(dgrow(c->rerr, 16));
     CK(dgrow(c->markers, 8));
     CK(cudaMemcpyAsync(c->chunks.p, blob.data(), total, cudaMemcpyHostToDevice, c->stream));
@@ -712,32 +789,13 @@ int run_resolve(rrg_ctx* c, const std::vector<ResolveChunk>& rchunks, uint8_t* d
     ResolveArgs R{};
     R.cells = (uint16_t*)c->cells.p;
     R.chunks = (const ResolveChunk*)dev;
-    R.n_chunks = nc;
-    R.groups = (const ResGroup*)(dev + o_grp);
-    R.n_groups = ng;
-    R.jobs = (const ResJob*)(dev + o_job);
-    R.n_jobs = nj;
-    R.chunk_group = (const uint32_t*)(dev + o_cg);
-    R.tail_tiles = (const uint64_t*)(dev + o_pre);
-    R.head_segs = (const uint64_t*)(dev + o_pre) + nc + 1;
-    R.maps = (uint16_t*)c->win.p;
-    R.bases = (uint16_t*)c->win.p + (size_t)nc * WINDOW;
+    R.head_segs = (const uint64_t*)(dev + o_hs);
+    res_args(R, T, dev + o_t, (uint16_t*)c->win.p, nc);
     R.out = d_dst;
     R.err = (uint32_t*)c->rerr.p;
     R.markers = (unsigned long long*)c->markers.p;
-    const uint32_t tgrid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(tt[nc], (uint64_t)c->n_sm * 8));
-    const uint32_t hgrid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(hs[nc], (uint64_t)c->n_sm * 4));
     KTimer kt(c->stream);
-    RRG_LAUNCH(k_win_maps, std::min<uint32_t>(ng, c->n_sm), WM_THREADS, WM_SMEM, c->stream, R);
-    LAUNCHED(c);
-    RRG_LAUNCH(k_win_bases, std::min<uint32_t>(nj, c->n_sm), WM_THREADS, WINDOW * 2, c->stream, R);
-    LAUNCHED(c);
-    RRG_LAUNCH(k_res_tails, tgrid, RES_THREADS, 0, c->stream, R);
-    LAUNCHED(c);
-    if (hs[nc]) {
-        RRG_LAUNCH(k_res_heads, hgrid, RES_THREADS, 0, c->stream, R);
-        LAUNCHED(c);
-    }
+    if (int rc = launch_resolve(c, R, c->stream, err)) return rc;
     kt.stop();
     uint32_t e4[4];
     unsigned long long nmk = 0;
@@ -1960,8 +2018,8 @@ namespace {
 struct PipeWave {
     uint32_t first = 0, n = 0;       // items
     uint32_t piece_off = 0, piece_cap = 0;
-    size_t grp_off = 0;              // offset of this wave's ResGroup/ResJob/chunk_group tables in the blob
-    uint32_t n_groups = 0;
+    size_t tab_off = 0;              // offset of this wave's resolve tables in the blob
+    ResTables tab;
 };
 
 int ensure_ring(rrg_ctx* c, size_t piece, uint32_t waves, rrg_error* err) {
@@ -2079,7 +2137,8 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
     std::vector<PipeWave> waves(Wn);
     std::vector<uint32_t> order(n);
     std::vector<uint8_t> tabs;  // ResGroup[], ResJob[1], chunk_group[] per wave, 8-byte aligned
-    uint32_t max_n = 0, max_g = 0, total_pieces = 0;
+    uint32_t max_n = 0, total_pieces = 0;
+    size_t max_win = 0;
     uint64_t out_bound = 0;
     for (uint32_t w = 0; w < Wn; w++) {
         PipeWave& pw = waves[w];
@@ -2096,30 +2155,19 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
         std::stable_sort(order.begin() + pw.first, order.begin() + pw.first + pw.n, [&](uint32_t a, uint32_t b) {
             return items[a].out_cap > items[b].out_cap;
         });
-        const uint32_t S = std::max<uint32_t>(1, (uint32_t)std::ceil(std::sqrt(0.7 * pw.n)));
-        pw.n_groups = (pw.n + S - 1) / S;
-        pw.grp_off = tabs.size();
-        std::vector<ResGroup> gr(pw.n_groups);
-        std::vector<uint32_t> cg(pw.n);
-        for (uint32_t g = 0; g < pw.n_groups; g++) {
-            gr[g] = ResGroup{g * S, std::min(S, pw.n - g * S)};
-            for (uint32_t q = gr[g].first; q < gr[g].first + gr[g].n; q++) cg[q] = g;
-        }
-        const ResJob jb{0, pw.n_groups};
-        const size_t o1 = round8(pw.n_groups * sizeof(ResGroup)), o2 = o1 + round8(sizeof(ResJob));
-        tabs.resize(pw.grp_off + o2 + round8(pw.n * 4));
-        std::memcpy(tabs.data() + pw.grp_off, gr.data(), pw.n_groups * sizeof(ResGroup));
-        std::memcpy(tabs.data() + pw.grp_off + o1, &jb, sizeof(jb));
-        std::memcpy(tabs.data() + pw.grp_off + o2, cg.data(), pw.n * 4);
+        build_res_tables({pw.n}, c->n_sm, pw.tab);
+        pw.tab_off = tabs.size();
+        tabs.resize(pw.tab_off + round8(pw.tab.bytes));
+        pw.tab.write(tabs.data() + pw.tab_off);
         max_n = std::max(max_n, pw.n);
-        max_g = std::max(max_g, pw.n_groups);
+        max_win = std::max(max_win, res_win_bytes(pw.tab, pw.n));
     }
     // ---- device memory
     // pipe layout: state | infos | live | n_pieces[W] | fin (exp/got/status/mpiece) |
-    //              chunks[max_n] | tail_tiles[max_n+1] | head_segs[max_n+1] | pieces | piece_crc | tabs
+    //              chunks[max_n] | head_segs[max_n+1] | pieces | piece_crc | tabs
     const size_t o_info = 64, o_live = o_info + round8(Wn * sizeof(WaveInfo)), o_np = o_live + 8,
                  o_fin = o_np + round8(Wn * 4), o_chunks = o_fin + 64,
-                 o_tt = o_chunks + round8((size_t)max_n * sizeof(ResolveChunk)), o_hs = o_tt + ((size_t)max_n + 1) * 8,
+                 o_hs = o_chunks + round8((size_t)max_n * sizeof(ResolveChunk)),
                  o_pc = o_hs + ((size_t)max_n + 1) * 8, o_pcrc = o_pc + (size_t)total_pieces * sizeof(CrcPiece),
                  o_tabs = o_pcrc + round8((size_t)total_pieces * 4), p_total = o_tabs + tabs.size();
     const uint64_t isize_hint = le32h(h_file + len - 4);
@@ -2134,7 +2182,7 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
     CK(dgrow(c->mbs, 4096 * sizeof(MemberRec)));
     CK(dgrow(c->mbcount, 16));
     CK(dgrow(c->cells, (arena + 8) * 2));
-    CK(dgrow(c->win, ((size_t)max_n + max_g) * WINDOW * 2));
+    CK(dgrow(c->win, max_win));
     CK(dgrow(c->rerr, 16));
     CK(dgrow(c->markers, 8));
     CK(dgrow(c->crc_table, sizeof(g_crc_tab) + sizeof(g_crc_z496)));
@@ -2208,7 +2256,6 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
         WA.info = h_info + w;  // mapped pinned memory: no copy queued behind the output
         WA.live = (uint32_t*)(P + o_live);
         WA.chunks = (ResolveChunk*)(P + o_chunks);
-        WA.tail_tiles = (uint64_t*)(P + o_tt);
         WA.head_segs = (uint64_t*)(P + o_hs);
         WA.pieces = (CrcPiece*)(P + o_pc) + pw.piece_off;
         WA.piece_cap = pw.piece_cap;
@@ -2225,29 +2272,13 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
         ResolveArgs R{};
         R.cells = (uint16_t*)c->cells.p;
         R.chunks = WA.chunks;
-        R.n_chunks = pw.n;
-        R.groups = (const ResGroup*)(P + o_tabs + pw.grp_off);
-        R.n_groups = pw.n_groups;
-        const size_t o1 = round8(pw.n_groups * sizeof(ResGroup)), o2 = o1 + round8(sizeof(ResJob));
-        R.jobs = (const ResJob*)(P + o_tabs + pw.grp_off + o1);
-        R.n_jobs = 1;
-        R.chunk_group = (const uint32_t*)(P + o_tabs + pw.grp_off + o2);
-        R.tail_tiles = WA.tail_tiles;
         R.head_segs = WA.head_segs;
-        R.maps = (uint16_t*)c->win.p;
-        R.bases = (uint16_t*)c->win.p + (size_t)max_n * WINDOW;
+        res_args(R, pw.tab, P + o_tabs + pw.tab_off, (uint16_t*)c->win.p, pw.n);
         R.out = tgt.p;
         R.err = (uint32_t*)c->rerr.p;
         R.markers = (unsigned long long*)c->markers.p;
         R.live = WA.live;
-        RRG_LAUNCH(k_win_maps, std::min<uint32_t>(pw.n_groups, c->n_sm), WM_THREADS, WM_SMEM, rs, R);
-        LAUNCHED(c);
-        RRG_LAUNCH(k_win_bases, 1, WM_THREADS, WINDOW * 2, rs, R);
-        LAUNCHED(c);
-        RRG_LAUNCH(k_res_tails, c->n_sm * 8, RES_THREADS, 0, rs, R);
-        LAUNCHED(c);
-        RRG_LAUNCH(k_res_heads, c->n_sm * 4, RES_THREADS, 0, rs, R);
-        LAUNCHED(c);
+        if (int rc = launch_resolve(c, R, rs, err)) return rc;
         CrcWideArgs CA{tgt.p, WA.pieces, pw.piece_cap, (uint32_t*)(P + o_pcrc) + pw.piece_off,
                        (const uint32_t*)c->crc_table.p, WA.n_pieces};
         RRG_LAUNCH(k_crc_pieces_wide, persistent_blocks(c, 8, pw.piece_cap, 1), CRCW_THREADS, 0, rs, CA);
@@ -3454,6 +3485,8 @@ rrg_ctx* rrg_gpu_create(const rrg_config* cfg, rrg_error* err) {
     cudaFuncSetAttribute(k_find_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(4 * sizeof(FindSmem)));
     cudaFuncSetAttribute(k_win_maps, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WM_SMEM);
     cudaFuncSetAttribute(k_win_bases, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(WINDOW * 2));
+    cudaFuncSetAttribute(k_win_supers, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(WINDOW * 2));
+    cudaFuncSetAttribute(k_res_tails, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(WINDOW * 2));
     cudaFuncSetAttribute(k_verify_heavy, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(4 * sizeof(FindSmem)));
     cudaFuncSetAttribute(k_inflate_lanes<uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(LANE_THREADS * sizeof(LaneTab)));

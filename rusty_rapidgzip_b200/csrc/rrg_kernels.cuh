@@ -6,7 +6,8 @@
 //   k_inflate      — rrg/src/pipeline.rs:1080-1185 decode_one_chunk with
 //                    rrg/src/deflate/fast_inflate.rs:1794-2234 (u16 marker cells), or a
 //                    whole member into final bytes (gzip.rs:197-249 decode_one_indexed_fast)
-//   k_win_maps / k_win_bases / k_res_tails / k_res_heads — rrg/src/deflate/speculative.rs:175-213
+//   k_win_maps / k_win_supers / k_win_bases / k_win_expand / k_res_tails / k_res_heads —
+//                    rrg/src/deflate/speculative.rs:175-213
 //                    resolve_markers together with the tail chain of rrg/src/pipeline.rs:1045-1078,
 //                    fused with the chunk compaction
 //   k_crc_pieces / k_crc_members — crc32fast hashing + combine (rrg/src/pipeline.rs:712-732, :885-916)
@@ -2171,50 +2172,62 @@ __global__ void __launch_bounds__(128) k_verify_heavy(VerifyArgs A) {
 // first occurrence of a frequent word may lie many chunks back), so the chain
 // is restated as composition of window maps. A window map describes each of
 // the 32768 bytes of a window as a literal, a position in an earlier base
-// window (WM_REF | index) or an unresolvable byte (WM_BAD). Four kernels:
-//   k_win_maps    one block per group of consecutive chunks of a job: R_k,
-//                 the map of W_{k+1} relative to the group's first window, is
-//                 built chunk after chunk in shared memory from chunk k's last
-//                 32 KiB of cells and R_{k-1} (one gather per byte);
-//   k_win_bases   one block per job: the groups' first windows as bytes, one
-//                 group after another (one gather per byte per group);
-//   k_res_tails   the last 32 KiB of every chunk: R_k through its group's
-//                 base window straight into the output;
+// window (WM_REF | index) or an unresolvable byte (WM_BAD). Chunks form groups
+// (consecutive chunks of a job), groups form supergroups. Six kernels:
+//   k_win_maps    one block per group: R_k, the map of W_{k+1} relative to the
+//                 group's first window, built chunk after chunk in shared
+//                 memory from chunk k's last 32 KiB of cells and R_{k-1};
+//   k_win_supers  one block per supergroup: each group's first window as a map
+//                 relative to the supergroup's first window, group after group,
+//                 and the supergroup's transfer map (the next supergroup's
+//                 first window relative to this one's);
+//   k_win_bases   one block per job: the supergroups' first windows as bytes,
+//                 one supergroup after another (one gather per byte each);
+//   k_win_expand  every group's first window as bytes, in parallel;
+//   k_res_tails   the last 32 KiB of every chunk, R_k through its group's first
+//                 window (staged in shared memory once per 8 chunks) straight
+//                 into the output;
 //   k_res_heads   every other cell with at most one gather from the 32 KiB of
 //                 output before its chunk, staged in shared memory once per
 //                 64 Ki-cell segment; cells read 16 bytes at a time, bytes
 //                 written as aligned 8-byte words.
+// The sequential steps are one 32 KiB gather each: chunks per group, groups
+// per supergroup and supergroups per job, about 24 + 12 + 12 for 3,552 chunks.
 // Device traffic: 2 bytes read and 1 written per cell, plus about 6 bytes per
 // window byte for the maps.
 constexpr int RES_THREADS = 256;
 constexpr int RES_CELLS = 8;                             // cells per thread per step (one 16-byte load)
-constexpr int RES_TAIL_TILE = RES_THREADS * RES_CELLS;   // window bytes per tail tile
+constexpr int RES_TAIL_TILE = RES_THREADS * RES_CELLS;   // window bytes per tail step
+constexpr uint32_t RES_TAIL_CHUNKS = 8;                  // chunks per tail unit (one base staging)
 constexpr uint64_t RES_HEAD_SEG = 65536;                 // head cells per window staging
 constexpr int WM_THREADS = 1024;
 constexpr uint32_t WM_REF = 0x8000u;  // | index into the base window
 constexpr uint32_t WM_BAD = 0x4000u;  // the byte lies before its member (or the output)
 
 struct ResGroup {
-    uint32_t first;  // first chunk
-    uint32_t n;      // consecutive chunks
+    uint32_t first;  // first chunk (of a group), first group (of a supergroup) or first supergroup (of a job)
+    uint32_t n;      // consecutive members
 };
-struct ResJob {
-    uint32_t first;  // first group
-    uint32_t n;      // consecutive groups
-};
+typedef ResGroup ResJob;
 
 struct ResolveArgs {
     uint16_t* cells;
     const ResolveChunk* chunks;
     uint32_t n_chunks;
-    const ResGroup* groups;
+    const ResGroup* groups;       // chunks of each group
     uint32_t n_groups;
-    const ResJob* jobs;
+    const ResGroup* supers;       // groups of each supergroup
+    uint32_t n_supers;
+    const ResJob* jobs;           // supergroups of each job
     uint32_t n_jobs;
     const uint32_t* chunk_group;  // n_chunks
-    const uint64_t* tail_tiles;   // n_chunks + 1: prefix of each chunk's tail tiles
+    const uint32_t* group_super;  // n_groups
+    const uint64_t* tail_units;   // n_groups + 1: prefix of each group's tail units (RES_TAIL_CHUNKS chunks each)
     const uint64_t* head_segs;    // n_chunks + 1: prefix of each chunk's head segments
     uint16_t* maps;               // n_chunks x WINDOW: R_k
+    uint16_t* gmaps;              // n_groups x WINDOW: each group's first window relative to its supergroup's
+    uint16_t* tmaps;              // n_supers x WINDOW: each supergroup's transfer map
+    uint16_t* sbases;             // n_supers x WINDOW: each supergroup's first window (byte or WM_BAD)
     uint16_t* bases;              // n_groups x WINDOW: each group's first window (byte or WM_BAD)
     uint8_t* out;
     uint32_t* err;                // [0] flag, [1] chunk, [2] cell lo, [3] cell hi
@@ -2368,94 +2381,144 @@ __global__ void __launch_bounds__(WM_THREADS, 1) k_win_maps(ResolveArgs A) {
     if ((threadIdx.x & 31) == 0 && nmk) atomicAdd(A.markers, (unsigned long long)nmk);
 }
 
-// Each job's groups in order: the first group's base window is the 32 KiB
+// One composition step of a sequential map chain held in shared memory:
+// cur[i] <- R[i] through cur (a literal or WM_BAD stays, WM_REF|j becomes
+// cur[j]), read first into registers so cur can be rewritten in place; the
+// result also goes to `out` when set. Block-wide, WM_THREADS threads.
+__device__ __forceinline__ void wm_step(uint16_t* cur, const uint16_t* R, uint16_t* out) {
+    uint4 nv[WM_VEC];
+#pragma unroll
+    for (uint32_t v = 0; v < WM_VEC; v++) nv[v] = reinterpret_cast<const uint4*>(R)[threadIdx.x + v * WM_THREADS];
+#pragma unroll
+    for (uint32_t v = 0; v < WM_VEC; v++) {
+        uint32_t r[8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            const uint32_t x = u16_of(nv[v], e);
+            r[e] = (x & WM_REF) ? (uint32_t)cur[x & 0x7fffu] : x;
+        }
+        nv[v] = pack_u16x8(r);
+    }
+    __syncthreads();  // every read of cur is done
+#pragma unroll
+    for (uint32_t v = 0; v < WM_VEC; v++) {
+        const uint32_t i0 = 8 * (threadIdx.x + v * WM_THREADS);
+        *reinterpret_cast<uint4*>(cur + i0) = nv[v];
+        if (out) *reinterpret_cast<uint4*>(out + i0) = nv[v];
+    }
+    __syncthreads();
+}
+
+// Each supergroup's groups in order: a group's first window relative to the
+// supergroup's first window (the identity for the first group), then the
+// transfer map after the last group.
+__global__ void __launch_bounds__(WM_THREADS, 1) k_win_supers(ResolveArgs A) {
+    if (A.live && *A.live == 0) return;
+    RRG_DYN_SMEM(sm);
+    uint16_t* cur = reinterpret_cast<uint16_t*>(sm);
+    for (uint32_t sg = blockIdx.x; sg < A.n_supers; sg += gridDim.x) {
+        const ResGroup SG = A.supers[sg];
+        for (uint32_t i = threadIdx.x; i < WINDOW; i += blockDim.x) {
+            cur[i] = (uint16_t)(WM_REF | i);
+            A.gmaps[(uint64_t)SG.first * WINDOW + i] = (uint16_t)(WM_REF | i);
+        }
+        __syncthreads();
+        for (uint32_t q = 0; q < SG.n; q++) {
+            const ResGroup G = A.groups[SG.first + q];
+            const uint16_t* R = A.maps + (uint64_t)(G.first + G.n - 1) * WINDOW;
+            uint16_t* dst = q + 1 < SG.n ? A.gmaps + (uint64_t)(SG.first + q + 1) * WINDOW
+                                         : A.tmaps + (uint64_t)sg * WINDOW;
+            wm_step(cur, R, dst);
+        }
+    }
+}
+
+// Each job's supergroups in order: the first one's first window is the 32 KiB
 // before the job (a stripe's prefix, already in the output, or WM_BAD); each
-// next base applies the previous group's last map to the previous base.
+// next one applies the previous supergroup's transfer map.
 __global__ void __launch_bounds__(WM_THREADS, 1) k_win_bases(ResolveArgs A) {
     if (A.live && *A.live == 0) return;
     RRG_DYN_SMEM(sm);
     uint16_t* cur = reinterpret_cast<uint16_t*>(sm);
     for (uint32_t jb = blockIdx.x; jb < A.n_jobs; jb += gridDim.x) {
         const ResJob J = A.jobs[jb];
-        for (uint32_t q = 0; q < J.n; q++) {
-            const uint32_t g = J.first + q;
-            uint16_t* B = A.bases + (uint64_t)g * WINDOW;
-            uint4 nv[WM_VEC];
-            if (q == 0) {
-                const ResolveChunk ck = A.chunks[A.groups[g].first];
-#pragma unroll
-                for (uint32_t v = 0; v < WM_VEC; v++) {
-                    const uint32_t i0 = 8 * (threadIdx.x + v * WM_THREADS);
-                    uint32_t r[8];
-#pragma unroll
-                    for (int e = 0; e < 8; e++) {
-                        const uint32_t i = i0 + e;
-                        r[e] = WM_BAD;
-                        if (ck.out_start >= (uint64_t)(WINDOW - i)) {
-                            const uint64_t pos = ck.out_start - WINDOW + i;
-                            if (pos >= ck.member_start && pos < ck.job_out) r[e] = A.out[pos];
-                        }
-                    }
-                    nv[v] = pack_u16x8(r);
-                }
-            } else {
-                const ResGroup P = A.groups[g - 1];
-                const uint4* R = reinterpret_cast<const uint4*>(A.maps + (uint64_t)(P.first + P.n - 1) * WINDOW);
-#pragma unroll
-                for (uint32_t v = 0; v < WM_VEC; v++) nv[v] = R[threadIdx.x + v * WM_THREADS];
-#pragma unroll
-                for (uint32_t v = 0; v < WM_VEC; v++) {
-                    uint32_t r[8];
-#pragma unroll
-                    for (int e = 0; e < 8; e++) {
-                        const uint32_t x = u16_of(nv[v], e);
-                        r[e] = (x & WM_REF) ? (uint32_t)cur[x & 0x7fffu] : x;
-                    }
-                    nv[v] = pack_u16x8(r);
-                }
+        const ResolveChunk ck = A.chunks[A.groups[A.supers[J.first].first].first];
+        for (uint32_t i = threadIdx.x; i < WINDOW; i += blockDim.x) {
+            uint32_t r = WM_BAD;
+            if (ck.out_start >= (uint64_t)(WINDOW - i)) {
+                const uint64_t pos = ck.out_start - WINDOW + i;
+                if (pos >= ck.member_start && pos < ck.job_out) r = A.out[pos];
             }
-            __syncthreads();  // every read of the previous base is done
-#pragma unroll
-            for (uint32_t v = 0; v < WM_VEC; v++) {
-                const uint32_t i0 = 8 * (threadIdx.x + v * WM_THREADS);
-                *reinterpret_cast<uint4*>(cur + i0) = nv[v];
-                *reinterpret_cast<uint4*>(B + i0) = nv[v];
-            }
-            __syncthreads();
+            cur[i] = (uint16_t)r;
+            A.sbases[(uint64_t)J.first * WINDOW + i] = (uint16_t)r;
         }
+        __syncthreads();
+        for (uint32_t q = 0; q + 1 < J.n; q++)
+            wm_step(cur, A.tmaps + (uint64_t)(J.first + q) * WINDOW, A.sbases + (uint64_t)(J.first + q + 1) * WINDOW);
     }
 }
 
+// Every group's first window as bytes: its map through its supergroup's first window.
+__global__ void __launch_bounds__(RES_THREADS) k_win_expand(ResolveArgs A) {
+    if (A.live && *A.live == 0) return;
+    const uint64_t total = (uint64_t)A.n_groups * (WINDOW / 8);
+    for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total;
+         x += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t g = (uint32_t)(x / (WINDOW / 8)), i0 = (uint32_t)(x % (WINDOW / 8)) * 8;
+        const uint16_t* sb = A.sbases + (uint64_t)A.group_super[g] * WINDOW;
+        const uint4 q = *reinterpret_cast<const uint4*>(A.gmaps + (uint64_t)g * WINDOW + i0);
+        uint32_t r[8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            const uint32_t v = u16_of(q, e);
+            r[e] = (v & WM_REF) ? (uint32_t)sb[v & 0x7fffu] : v;
+        }
+        *reinterpret_cast<uint4*>(A.bases + (uint64_t)g * WINDOW + i0) = pack_u16x8(r);
+    }
+}
+
+// Tails, one unit = up to RES_TAIL_CHUNKS chunks of one group: the group's
+// first window is staged in shared memory once, then each chunk's R_k is
+// read 16 bytes per lane and resolved through it.
 __global__ void __launch_bounds__(RES_THREADS) k_res_tails(ResolveArgs A) {
     if (A.live && *A.live == 0) return;
+    RRG_DYN_SMEM(sm);  // WINDOW u16: the group's first window
+    uint16_t* base = reinterpret_cast<uint16_t*>(sm);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint64_t n_tiles = A.tail_tiles[A.n_chunks];
-    for (uint64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
-        const uint32_t k = res_unit_chunk(A.tail_tiles, A.n_chunks, t);
-        const ResolveChunk ck = A.chunks[k];
-        const uint32_t i_lo = res_tail_lo(ck.n_cells);
-        // window index of this warp's first byte; tiles cover [i_lo & ~(TILE-1), WINDOW)
-        const uint32_t i0 = (i_lo & ~(uint32_t)(RES_TAIL_TILE - 1)) +
-                            (uint32_t)(t - A.tail_tiles[k]) * RES_TAIL_TILE + warp * (32 * RES_CELLS);
-        if (i0 + 32 * RES_CELLS <= i_lo) continue;  // warp-uniform: entirely before the chunk
-        const uint16_t* R = A.maps + (uint64_t)k * WINDOW;
-        const uint16_t* B = A.bases + (uint64_t)A.chunk_group[k] * WINDOW;
-        const uint4 q = reinterpret_cast<const uint4*>(R + i0)[lane];
-        const uint32_t w[4] = {q.x, q.y, q.z, q.w};
-        uint64_t v = 0;
-        bool bad = false;
+    const uint64_t n_units = A.tail_units[A.n_groups];
+    for (uint64_t u = blockIdx.x; u < n_units; u += gridDim.x) {
+        const uint32_t g = res_unit_chunk(A.tail_units, A.n_groups, u);
+        const ResGroup G = A.groups[g];
+        const uint32_t c0 = G.first + (uint32_t)(u - A.tail_units[g]) * RES_TAIL_CHUNKS;
+        const uint32_t c1 = c0 + RES_TAIL_CHUNKS < G.first + G.n ? c0 + RES_TAIL_CHUNKS : G.first + G.n;
+        __syncthreads();  // the previous unit's readers are done with base
+        const uint4* src = reinterpret_cast<const uint4*>(A.bases + (uint64_t)g * WINDOW);
+        for (uint32_t q = threadIdx.x; q < WINDOW / 8; q += blockDim.x) reinterpret_cast<uint4*>(base)[q] = src[q];
+        __syncthreads();
+        for (uint32_t k = c0; k < c1; k++) {
+            const ResolveChunk ck = A.chunks[k];
+            const uint32_t i_lo = res_tail_lo(ck.n_cells);
+            const uint16_t* R = A.maps + (uint64_t)k * WINDOW;
+            // window index i is output byte out_start + n - WINDOW + i
+            uint8_t* dst0 = A.out + (ck.out_start + ck.n_cells - WINDOW);
+            for (uint32_t i0 = (i_lo & ~(uint32_t)(32 * RES_CELLS - 1)) + warp * (32 * RES_CELLS); i0 < WINDOW;
+                 i0 += RES_THREADS * RES_CELLS) {
+                const uint4 q = reinterpret_cast<const uint4*>(R + i0)[lane];
+                uint32_t lo32 = 0, hi32 = 0;
+                bool bad = false;
 #pragma unroll
-        for (int e = 0; e < RES_CELLS; e++) {
-            const uint32_t i = i0 + RES_CELLS * lane + e;
-            uint32_t r = (w[e >> 1] >> (16 * (e & 1))) & 0xffffu;
-            if (r & WM_REF) r = B[r & 0x7fffu];
-            if (i >= i_lo) bad |= (r & WM_BAD) != 0;
-            v |= (uint64_t)(r & 0xffu) << (8 * e);
+                for (int e = 0; e < RES_CELLS; e++) {
+                    const uint32_t i = i0 + RES_CELLS * lane + e;
+                    uint32_t r = u16_of(q, e);
+                    r = (r & WM_REF) ? (uint32_t)base[r & 0x7fffu] : r;
+                    if (i >= i_lo) bad |= (r & WM_BAD) != 0;
+                    if (e < 4) lo32 |= (r & 0xffu) << (8 * e);
+                    else hi32 |= (r & 0xffu) << (8 * (e - 4));
+                }
+                if (bad) res_fail(A, k, i0);
+                warp_store8(dst0 + i0, ((uint64_t)hi32 << 32) | lo32, i_lo > i0 ? i_lo - i0 : 0u, 32u * RES_CELLS, lane);
+            }
         }
-        if (bad) res_fail(A, k, i0);
-        // window index i is output byte out_start + n - WINDOW + i
-        uint8_t* dst = A.out + (ck.out_start + ck.n_cells - WINDOW + i0);
-        warp_store8(dst, v, i_lo > i0 ? i_lo - i0 : 0u, 32u * RES_CELLS, lane);
     }
 }
 
@@ -2584,7 +2647,6 @@ struct WaveArgs {
     WaveInfo* info;
     uint32_t* live;            // gate of this wave's resolve and CRC launches
     ResolveChunk* chunks;      // n entries
-    uint64_t* tail_tiles;      // n + 1
     uint64_t* head_segs;       // n + 1
     CrcPiece* pieces;          // this wave's region of piece_cap pieces
     uint32_t piece_cap;
@@ -2634,7 +2696,7 @@ __global__ void __launch_bounds__(WAVE_THREADS, 1) k_wave_chain(WaveArgs A) {
     // each thread checks a contiguous run of sub-chunks
     const uint32_t per = (A.n + WAVE_THREADS - 1) / WAVE_THREADS;
     const uint32_t b = t * per < A.n ? t * per : A.n, e = b + per < A.n ? b + per : A.n;
-    uint64_t cells = 0, tiles = 0, segs = 0;
+    uint64_t cells = 0, segs = 0;
     for (uint32_t q = b; q < e; q++) {
         const uint32_t k = A.first + q;
         const ChunkItem it = A.items[k];
@@ -2654,13 +2716,11 @@ __global__ void __launch_bounds__(WAVE_THREADS, 1) k_wave_chain(WaveArgs A) {
             continue;
         }
         cells += r.n_cells;
-        tiles += (WINDOW - (res_tail_lo(r.n_cells) & ~(uint32_t)(RES_TAIL_TILE - 1))) / RES_TAIL_TILE;
         segs += (res_head_end(r.n_cells) + RES_HEAD_SEG - 1) / RES_HEAD_SEG;
     }
     __syncthreads();
-    uint64_t c_ex, t_ex, s_ex;
+    uint64_t c_ex, s_ex;
     const uint64_t total = block_scan(cells, sh, &c_ex);
-    const uint64_t n_tiles = block_scan(tiles, sh, &t_ex);
     const uint64_t n_segs = block_scan(segs, sh, &s_ex);
     const uint64_t out_begin = S.out_end, out_len = total;
     const uint32_t np = (uint32_t)((out_len + WAVE_PIECE - 1) / WAVE_PIECE);
@@ -2684,10 +2744,8 @@ __global__ void __launch_bounds__(WAVE_THREADS, 1) k_wave_chain(WaveArgs A) {
         const uint32_t k = A.first + q;
         const uint64_t n = A.results[k].n_cells;
         A.chunks[q] = ResolveChunk{out_begin + c_ex, A.items[k].out_off, n, 0, out_begin};
-        A.tail_tiles[q] = t_ex;
         A.head_segs[q] = s_ex;
         c_ex += n;
-        t_ex += (WINDOW - (res_tail_lo(n) & ~(uint32_t)(RES_TAIL_TILE - 1))) / RES_TAIL_TILE;
         s_ex += (res_head_end(n) + RES_HEAD_SEG - 1) / RES_HEAD_SEG;
     }
     for (uint32_t p = t; p < A.piece_cap; p += WAVE_THREADS) {
@@ -2699,7 +2757,6 @@ __global__ void __launch_bounds__(WAVE_THREADS, 1) k_wave_chain(WaveArgs A) {
     const bool has_last = A.first + lastq == A.last_item;
     uint64_t tb = 0;
     if (t == 0) {
-        A.tail_tiles[A.n] = n_tiles;
         A.head_segs[A.n] = n_segs;
         *A.n_pieces = A.piece_cap;
         if (has_last) {  // the trailer of the stream's only member
@@ -2912,9 +2969,15 @@ __global__ void k_crc_members(CrcMemberArgs A) {
         if (e > p1) e = p1;
         uint32_t c = 0;
         uint64_t len = 0;
+        uint64_t xl = 0;          // the length whose x^(8 len) is in xp: pieces mostly share
+        uint32_t xp = 0x80000000u;  // one length (256 KiB), so one multiply each
         for (uint32_t i = b; i < e; i++) {
-            uint64_t l = A.pieces[i].len;
-            c = (l ? gf2_mulmod(c, xpow8n(l)) : c) ^ A.piece_crc[i];
+            const uint64_t l = A.pieces[i].len;
+            if (l && l != xl) {
+                xp = xpow8n(l);
+                xl = l;
+            }
+            c = (l ? gf2_mulmod(c, xp) : c) ^ A.piece_crc[i];
             len += l;
         }
         for (int o = 1; o < 32; o <<= 1) {
