@@ -184,6 +184,47 @@ void rrg_index_free(rrg_index* idx);
 int rrg_gpu_decode_host(rrg_ctx* ctx, const uint8_t* data, size_t len, rrg_sink_fn sink,
                         void* user, rrg_stats* stats, rrg_error* err);
 
+/* One range of a single-member stream decoded on one of several GPUs (the
+ * reference's tail chain, pipeline.rs:1045-1078, spread over ranks: ranges
+ * decode in parallel and the only exchange is one 32 KiB window map per range).
+ * Phase 1, rrg_gpu_split_begin: `data` is the whole file in host memory and
+ * `body_off` its first member's deflate body. The range starts at the first
+ * dynamic block at or after body bit `start_target` (exactly there with
+ * RRG_SPLIT_EXACT_START; 0 is the body's start) and stops at the first block
+ * edge at or after the first dynamic block at or after `stop_target` (or at the
+ * member's end for ~0). It is decoded and its output laid out on the device;
+ * `end_map` (32768 entries) receives the range's last 32 KiB as a map of its
+ * first 32 KiB: a value below 0x100 is that byte, 0x8000|j is byte j of the
+ * window before the range, 0x4000 lies before the stream. `info` gets the exact
+ * start and end bits (a range is valid only if it starts where the previous
+ * non-empty one ended), its output length and the member trailer when it lies
+ * in this range. With no dynamic block after `start_target` the range is empty
+ * (start and end bits ~0, no output, identity map): the previous range, whose
+ * stop search finds the same nothing, decodes to the member's end.
+ * A range in which a member ends before its last block is refused
+ * (RRG_ERR_INVALID_ARGUMENT): split decoding takes one-member streams.
+ * Phase 2, rrg_gpu_split_finish: given the 32 KiB of output before the range
+ * (`window_len` < 32768 only near the stream's start; 0 for the first range),
+ * resolves the range, streams its bytes to `sink` and returns their CRC32 and
+ * length, which the ranks combine (crc32_combine) and compare with the trailer.
+ * One split range per context at a time. */
+#define RRG_SPLIT_EXACT_START 1u
+/* CRC32 of A||B from CRC32(A), CRC32(B) and |B| (crc32fast's combine, used by
+ * the reference's output stage, pipeline.rs:885-916), for joining the ranges'
+ * CRC32s. Host only. */
+uint32_t rrg_crc32_combine(uint32_t crc_a, uint32_t crc_b, uint64_t len_b);
+typedef struct rrg_split_info {
+    uint64_t start_bit, end_bit; /* body-relative */
+    uint64_t out_len;
+    uint32_t has_trailer, crc, isize, pad;
+    uint64_t trailer_byte;       /* file offset of the trailer (when has_trailer) */
+} rrg_split_info;
+int rrg_gpu_split_begin(rrg_ctx* ctx, const uint8_t* data, size_t len, uint64_t body_off,
+                        uint64_t start_target, uint64_t stop_target, uint32_t flags,
+                        uint16_t* end_map, rrg_split_info* info, rrg_error* err);
+int rrg_gpu_split_finish(rrg_ctx* ctx, const uint8_t* window, size_t window_len, rrg_sink_fn sink,
+                         void* user, uint32_t* crc_out, uint64_t* len_out, rrg_error* err);
+
 /* rrg_gpu_decode_host and rrg_gpu_read_gz with a destination provider (read_gz
  * with Config::recycle_rx/recycle_tx set, lib.rs:58-69): each piece of output
  * is copied from the device into a buffer `get` returns, and `sink` receives

@@ -86,6 +86,12 @@ _STAT_U64 = ["compressed_bytes", "uncompressed_bytes", "chunks_decoded", "specul
 _STAT_F64 = ["finder_ms", "inflate_ms", "resolve_ms", "crc_ms", "h2d_ms", "d2h_ms", "total_ms"]
 
 
+class _SplitInfo(C.Structure):
+    _fields_ = [("start_bit", C.c_uint64), ("end_bit", C.c_uint64), ("out_len", C.c_uint64),
+                ("has_trailer", C.c_uint32), ("crc", C.c_uint32), ("isize", C.c_uint32), ("pad", C.c_uint32),
+                ("trailer_byte", C.c_uint64)]
+
+
 class _Tuning(C.Structure):
     _fields_ = [("gpu_chunk_bytes", C.c_uint64), ("boundary_mode", C.c_int32), ("warps_per_member", C.c_int32),
                 ("finder_tile_bits", C.c_uint64), ("best_ms", C.c_double), ("default_ms", C.c_double),
@@ -253,6 +259,11 @@ def load_library(path: str | None = None):
         L.rrg_gpu_read_gz.argtypes = [vp, C.c_char_p, SINK_FN, vp, S, E]
         L.rrg_gpu_decode_host.argtypes = [vp, vp, sz, SINK_FN, vp, S, E]
         L.rrg_gpu_decode_host_into.argtypes = [vp, vp, sz, BUF_FN, SINK_FN, vp, S, E]
+        L.rrg_gpu_split_begin.argtypes = [vp, vp, sz, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint32,
+                                          C.POINTER(C.c_uint16), C.POINTER(_SplitInfo), E]
+        L.rrg_gpu_split_finish.argtypes = [vp, vp, sz, SINK_FN, vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), E]
+        L.rrg_crc32_combine.argtypes = [C.c_uint32, C.c_uint32, C.c_uint64]
+        L.rrg_crc32_combine.restype = C.c_uint32
         L.rrg_gpu_read_gz_into.argtypes = [vp, C.c_char_p, BUF_FN, SINK_FN, vp, S, E]
         L.rrg_gpu_read_stream.argtypes = [vp, READ_FN, vp, SINK_FN, vp, u64, S, E]
         L.rrg_gpu_index_build.argtypes = [vp, vp, sz, u64, C.POINTER(vp), S, E]
@@ -468,6 +479,47 @@ class Decoder:
             raise failure[0]
         _raise(e)
         return DecodeStats._from(st)
+
+    def crc32_combine(self, crc_a: int, crc_b: int, len_b: int) -> int:
+        """CRC32 of A||B from CRC32(A), CRC32(B) and |B| (rrg_crc32_combine)."""
+        return int(self._L.rrg_crc32_combine(crc_a, crc_b, len_b))
+
+    # ------------------------------------------------------- split member
+    def split_begin(self, data, body_off: int, start_target: int, stop_target: int, exact: bool = False):
+        """Phase 1 of one range of a member decoded on several GPUs
+        (rrg_gpu_split_begin): -> (info dict, end_map as a numpy uint16 array)."""
+        import numpy as np
+        addr, n, keep = _host_buffer(data)
+        m = np.empty(32768, dtype=np.uint16)
+        info, e = _SplitInfo(), _Error()
+        self._L.rrg_gpu_split_begin(self._ctx, addr, n, body_off, start_target, stop_target, 1 if exact else 0,
+                                    m.ctypes.data_as(C.POINTER(C.c_uint16)), C.byref(info), C.byref(e))
+        del keep
+        _raise(e)
+        return {f: int(getattr(info, f)) for f, _ in _SplitInfo._fields_ if f != "pad"}, m
+
+    def split_finish(self, window: bytes, sink) -> tuple[int, int]:
+        """Phase 2 (rrg_gpu_split_finish): resolve with the 32 KiB before the
+        range; the bytes go to `sink`; -> (CRC32, length) of the range."""
+        target = _as_sink(sink)
+        failure = []
+
+        def cb(_u, p, n):
+            try:
+                if target is not None:
+                    target(C.string_at(p, n))
+            except BaseException as ex:  # noqa: BLE001 - surfaced below
+                failure.append(ex)
+                return 1
+            return 0
+
+        crc, ln, e = C.c_uint32(), C.c_uint64(), _Error()
+        self._L.rrg_gpu_split_finish(self._ctx, window if window else None, len(window), SINK_FN(cb), None,
+                                     C.byref(crc), C.byref(ln), C.byref(e))
+        if failure:
+            raise failure[0]
+        _raise(e)
+        return int(crc.value), int(ln.value)
 
     def decode_host_into(self, data, recycle, sink) -> DecodeStats:
         """decode_host whose output pieces land in buffers from `recycle`."""
@@ -771,6 +823,11 @@ def crc32_noalloc(d_data, length: int, stream=None, lib: str | None = None) -> i
     load_library(lib).rrg_gpu_crc32_noalloc(_ptr(d_data), length, C.byref(out), _ptr(stream), C.byref(e))
     _raise(e)
     return int(out.value)
+
+
+def crc32_combine(crc_a: int, crc_b: int, len_b: int, lib: str | None = None) -> int:
+    """CRC32 of A||B from CRC32(A), CRC32(B) and |B| (rrg_crc32_combine)."""
+    return int(load_library(lib).rrg_crc32_combine(crc_a, crc_b, len_b))
 
 
 def kernel_launch_count(lib: str | None = None) -> int:

@@ -233,6 +233,18 @@ struct BgzfKey {
     uint64_t v[6];
 };
 
+// One range of a member split across GPUs, between its two phases: the
+// decoded cells stay in the context's slot arena, laid out from out + WINDOW.
+struct SplitState {
+    bool ready = false;
+    std::vector<ResolveChunk> rchunks;
+    uint64_t dst_off = 0, total = 0, end_bit = 0;
+    bool has_trailer = false;          // the member's trailer lies in this range
+    uint32_t crc = 0, isize = 0;       // that trailer
+    uint64_t trailer_byte = 0;
+    std::vector<uint16_t> end_map;     // WINDOW entries
+};
+
 // ====================================================================== ctx
 struct rrg_ctx {
     rrg_config cfg{};
@@ -278,6 +290,7 @@ struct rrg_ctx {
     uint8_t* h_wave = nullptr;       // pinned wave outcomes
     size_t h_wave_cap = 0;
     bool pipeline = true;            // take the pipelined path where it applies
+    SplitState* split = nullptr;     // a range of a split member between its phases
     // destination provider of the current *_into call (null: library staging)
     rrg_buffer_fn get_buf = nullptr;
     void* get_user = nullptr;
@@ -812,6 +825,54 @@ int run_resolve(rrg_ctx* c, const std::vector<ResolveChunk>& rchunks, uint8_t* d
     return 0;
 }
 
+// The window after the last chunk of `rchunks` (one job) as a map relative to
+// the job's first window, which is not known yet: the window kernels run with
+// an identity first window, and the map comes back to the host (WINDOW u16).
+int run_resolve_map(rrg_ctx* c, const std::vector<ResolveChunk>& rchunks, std::vector<uint16_t>& map,
+                    rrg_error* err) {
+    const uint32_t nc = (uint32_t)rchunks.size();
+    map.assign(WINDOW, 0);
+    if (!nc) {  // nothing decoded: the window is unchanged
+        for (uint32_t i = 0; i < WINDOW; i++) map[i] = (uint16_t)(WM_REF | i);
+        return 0;
+    }
+    ResTables T;
+    build_res_tables({nc}, c->n_sm, T);
+    const size_t o_t = round8(nc * sizeof(ResolveChunk)), total = o_t + T.bytes;
+    std::vector<uint8_t> blob(total);
+    std::memcpy(blob.data(), rchunks.data(), nc * sizeof(ResolveChunk));
+    T.write(blob.data() + o_t);
+    CK(dgrow(c->chunks, total));
+    CK(dgrow(c->win, res_win_bytes(T, nc) + WINDOW * 2));
+    CK(dgrow(c->markers, 8));
+    CK(cudaMemcpyAsync(c->chunks.p, blob.data(), total, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(c->markers.p, 0, 8, c->stream));
+    uint8_t* dev = (uint8_t*)c->chunks.p;
+    ResolveArgs R{};
+    R.cells = (uint16_t*)c->cells.p;
+    R.chunks = (const ResolveChunk*)dev;
+    res_args(R, T, dev + o_t, (uint16_t*)c->win.p, nc);
+    R.markers = (unsigned long long*)c->markers.p;
+    R.identity_base = 1;
+    uint16_t* d_map = (uint16_t*)((uint8_t*)c->win.p + res_win_bytes(T, nc));
+    const uint32_t nsm = c->n_sm;
+    RRG_LAUNCH(k_win_maps, std::min<uint32_t>(R.n_groups, nsm), WM_THREADS, WM_SMEM, c->stream, R);
+    LAUNCHED(c);
+    RRG_LAUNCH(k_win_supers, std::min<uint32_t>(R.n_supers, nsm), WM_THREADS, WINDOW * 2, c->stream, R);
+    LAUNCHED(c);
+    RRG_LAUNCH(k_win_bases, 1, WM_THREADS, WINDOW * 2, c->stream, R);
+    LAUNCHED(c);
+    const uint64_t ex = (uint64_t)R.n_groups * (WINDOW / 8);
+    RRG_LAUNCH(k_win_expand, (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((ex + 255) / 256, nsm * 8ull)),
+               RES_THREADS, 0, c->stream, R);
+    LAUNCHED(c);
+    RRG_LAUNCH(k_win_endmap, 32, 256, 0, c->stream, R, nc - 1, d_map);
+    LAUNCHED(c);
+    CK(cudaMemcpyAsync(map.data(), d_map, WINDOW * 2, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
 // ------------------------------------------------------------ boundary scan
 // Every bit offset of the body tested on the device; returns the sorted
 // offsets that pass the block finder's full strict verification.
@@ -1000,6 +1061,10 @@ struct MemberJob {
     // when set: every sub-chunk start the chain kept, as (bit relative to
     // body_off, output offset relative to dst_off), for a seek index
     std::vector<std::pair<uint64_t, uint64_t>>* capture = nullptr;
+    // when set: decode and lay out only, save what resolving needs here and
+    // compute the map of the job's last window relative to its first window
+    // (one range of a member split across GPUs)
+    struct SplitState* split = nullptr;
     uint64_t prefix_len = 0;
     uint32_t crc_prev = 0;
     uint64_t len_prev = 0;
@@ -1558,6 +1623,37 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
             span_member.push_back(j.member_base + nm);
             span_kind.push_back(nm == 0 && continued ? 3 : 2);  // 3: also the continued first member
         }
+    }
+    // ---- one range of a split member: stop before resolving
+    if (nj == 1 && jobs[0].split) {
+        MemberJob& j = jobs[0];
+        if (j.rc) return 0;
+        SplitState& S = *j.split;
+        size_t ends = 0, last = 0;
+        for (size_t m = 0; m < spans.size(); m++)
+            if (span_kind[m] <= 1) {
+                ends++;
+                last = m;
+            }
+        if (ends > 1 || (ends == 1 && !js[0].final_seen)) {
+            set_err(&j.err, RRG_ERR_INVALID_ARGUMENT, "a split decode takes a single-member stream");
+            j.rc = RRG_ERR_INVALID_ARGUMENT;
+            return 0;
+        }
+        S.rchunks = rchunks;
+        S.dst_off = j.dst_off;
+        S.total = j.out.total;
+        S.end_bit = js[0].expected;
+        S.has_trailer = ends == 1;
+        if (ends) {
+            S.crc = spans[last].crc;
+            S.isize = spans[last].isize;
+            S.trailer_byte = spans[last].trailer_byte;
+        }
+        S.ready = false;
+        if (int rm = run_resolve_map(c, rchunks, S.end_map, err)) return rm;
+        S.ready = true;
+        return 0;
     }
     // ---- resolve markers + compact; a failing chunk fails its job only
     int64_t bad = -1;
@@ -3517,6 +3613,7 @@ void rrg_gpu_destroy(rrg_ctx* c) {
     if (c->h_ring) cudaFreeHost(c->h_ring);
     if (c->h_wave) cudaFreeHost(c->h_wave);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c->split;
     delete c;
 }
 
@@ -3843,6 +3940,145 @@ int rrg_gpu_autotune(rrg_ctx* c, const uint8_t* d_in, const uint64_t* in_off, co
     int rc = autotune_impl(c, d_in, in_off, in_len, d_out, out_off, out_cap, n, result, err);
     c->stream = c->own_stream;
     return rc;
+}
+
+uint32_t rrg_crc32_combine(uint32_t crc_a, uint32_t crc_b, uint64_t len_b) {
+    std::call_once(g_tab_once, init_tables);
+    return host_crc_combine(crc_a, crc_b, len_b);
+}
+
+int rrg_gpu_split_begin(rrg_ctx* c, const uint8_t* data, size_t len, uint64_t body_off, uint64_t start_target,
+                        uint64_t stop_target, uint32_t flags, uint16_t* end_map, rrg_split_info* info,
+                        rrg_error* err) {
+    rrg_error local_err;
+    if (!err) err = &local_err;
+    std::memset(err, 0, sizeof(*err));
+    if (!c || !data || !end_map || !info || body_off + 8 > len || start_target >= (len - body_off) * 8 ||
+        (stop_target != ~0ull && stop_target <= start_target)) {
+        set_err(err, RRG_ERR_INVALID_ARGUMENT, "split range outside the member body");
+        return RRG_ERR_INVALID_ARGUMENT;
+    }
+    int rc = upload_tables(c, err);
+    if (rc) return rc;
+    if (!c->split) c->split = new SplitState;
+    SplitState& S = *c->split;
+    S.ready = false;
+    // the compressed bytes from the start target's byte to 16 MiB past the stop target
+    const uint64_t byte0 = body_off + start_target / 8;
+    const uint64_t end_byte =
+        stop_target == ~0ull ? len : std::min<uint64_t>(len, body_off + stop_target / 8 + (16u << 20));
+    const uint64_t clen = end_byte - byte0;
+    CK(dgrow(c->comp, clen + 16));
+    CK(cudaMemcpyAsync(c->comp.p, data + byte0, clen, cudaMemcpyHostToDevice, c->stream));
+    const uint8_t* d_span = (const uint8_t*)c->comp.p;
+    auto rel = [&](uint64_t body_bit) { return body_off * 8 + body_bit - byte0 * 8; };
+    // block starts from the targets (find_next_dynamic_block, block_finder.rs:109-141)
+    std::vector<uint64_t> targets, limits;
+    const bool search_start = start_target != 0 && !(flags & RRG_SPLIT_EXACT_START);
+    if (search_start) targets.push_back(rel(start_target));
+    if (stop_target != ~0ull) targets.push_back(rel(stop_target));
+    limits.assign(targets.size(), clen * 8);
+    std::vector<uint64_t> found(targets.size(), ~0ull);
+    if (!targets.empty()) {
+        const size_t n = targets.size();
+        CK(dgrow(c->targets, n * 8));
+        CK(dgrow(c->limits, n * 8));
+        CK(dgrow(c->found, n * 8));
+        CK(dgrow(c->queue, 16));
+        CK(cudaMemcpyAsync(c->targets.p, targets.data(), n * 8, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->limits.p, limits.data(), n * 8, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemsetAsync(c->queue.p, 0, 16, c->stream));
+        FindArgs F{d_span, clen, (const uint64_t*)c->targets.p, (const uint64_t*)c->limits.p,
+                   (uint64_t*)c->found.p, (uint32_t)n, (uint32_t*)c->queue.p, (const uint8_t*)c->next_lut.p,
+                   c->finder_tile};
+        RRG_LAUNCH(k_find_blocks, persistent_blocks(c, 4, n, 4), 128, 4 * sizeof(FindSmem), c->stream, F);
+        LAUNCHED(c);
+        CK(cudaMemcpyAsync(found.data(), c->found.p, n * 8, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    const uint64_t start_rel = search_start ? found[0] : rel(start_target);
+    const uint64_t stop_rel = stop_target == ~0ull ? ~0ull : found.back();
+    if (start_rel == ~0ull) {
+        // no dynamic block after the target: an empty range (the previous one,
+        // whose stop search meets the same nothing, decodes to the member's end)
+        S.rchunks.clear();
+        S.dst_off = WINDOW;
+        S.total = 0;
+        S.has_trailer = false;
+        S.end_map.resize(WINDOW);
+        for (uint32_t i = 0; i < WINDOW; i++) S.end_map[i] = (uint16_t)(WM_REF | i);
+        std::memset(info, 0, sizeof(*info));
+        info->start_bit = info->end_bit = ~0ull;
+        std::memcpy(end_map, S.end_map.data(), WINDOW * 2);
+        S.ready = true;
+        return 0;
+    }
+    OutTarget tgt{(uint8_t*)c->out.p, c->out.cap, true};
+    if ((rc = ensure_out(c, tgt, WINDOW + 4096, 0, err))) return rc;
+    const bool continued = byte0 * 8 + start_rel > body_off * 8;
+    std::vector<MemberJob> jobs(1);
+    MemberJob& j = jobs[0];
+    j.len = clen;
+    j.body_off = 0;
+    j.start_bit = start_rel;
+    j.stop_bit = stop_rel;
+    j.dst_off = WINDOW;
+    j.prefix_len = continued ? WINDOW : 0;  // the window is not known yet: all of it may be referenced
+    j.len_prev = continued ? 1 : 0;         // marks the first member as continued from earlier ranges
+    j.check_crc = false;
+    j.report_off = byte0;
+    j.split = &S;
+    if ((rc = members_route(c, d_span, jobs, tgt, err))) return rc;
+    if (j.rc) {
+        *err = j.err;
+        return j.rc;
+    }
+    const auto body_bit = [&](uint64_t r) { return r + byte0 * 8 - body_off * 8; };
+    info->start_bit = body_bit(start_rel);
+    info->end_bit = body_bit(S.end_bit);
+    info->out_len = S.total;
+    info->has_trailer = S.has_trailer ? 1u : 0u;
+    info->crc = S.crc;
+    info->isize = S.isize;
+    info->trailer_byte = S.trailer_byte;
+    std::memcpy(end_map, S.end_map.data(), WINDOW * 2);
+    return 0;
+}
+
+int rrg_gpu_split_finish(rrg_ctx* c, const uint8_t* window, size_t window_len, rrg_sink_fn sink, void* user,
+                         uint32_t* crc_out, uint64_t* len_out, rrg_error* err) {
+    rrg_error local_err;
+    if (!err) err = &local_err;
+    std::memset(err, 0, sizeof(*err));
+    if (!c || !c->split || !c->split->ready || window_len > WINDOW || (window_len && !window)) {
+        set_err(err, RRG_ERR_INVALID_ARGUMENT, "no split range awaits its window");
+        return RRG_ERR_INVALID_ARGUMENT;
+    }
+    SplitState& S = *c->split;
+    S.ready = false;
+    uint8_t* out = (uint8_t*)c->out.p;
+    if (window_len)
+        CK(cudaMemcpyAsync(out + S.dst_off - window_len, window, window_len, cudaMemcpyHostToDevice, c->stream));
+    // the continued first member now starts window_len bytes before the range
+    for (ResolveChunk& rc : S.rchunks)
+        if (rc.member_start == S.dst_off - WINDOW) rc.member_start = S.dst_off - window_len;
+    if (!S.total) {
+        if (crc_out) *crc_out = 0;
+        if (len_out) *len_out = 0;
+        return 0;
+    }
+    int rc = run_resolve(c, S.rchunks, out, err);
+    if (rc) return rc;
+    std::vector<int32_t> stv;
+    std::vector<uint32_t> got;
+    std::vector<uint64_t> glen;
+    const uint64_t members = c->st.members;
+    if ((rc = crc_spans(c, out, {MemberSpan{S.dst_off, S.total, 0, 0, 0}}, stv, got, glen, err))) return rc;
+    c->st.members = members;
+    if (crc_out) *crc_out = got.empty() ? 0u : got[0];
+    if (len_out) *len_out = S.total;
+    bool closed = false;
+    return deliver(c, out + S.dst_off, S.total, sink, user, &closed, err);
 }
 
 int rrg_gpu_find_blocks(rrg_ctx* c, const uint8_t* d_body, size_t body_len, const uint64_t* targets,

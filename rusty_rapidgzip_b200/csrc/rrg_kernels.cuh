@@ -2233,6 +2233,7 @@ struct ResolveArgs {
     uint32_t* err;                // [0] flag, [1] chunk, [2] cell lo, [3] cell hi
     unsigned long long* markers;  // count of marker cells resolved
     const uint32_t* live;         // when set and 0, the kernels do nothing (a failed pipeline wave)
+    uint32_t identity_base;       // the job's first window is unknown: maps stay relative to it
 };
 
 // Cells of a chunk that the head kernel resolves: all but the last 32 KiB.
@@ -2445,7 +2446,9 @@ __global__ void __launch_bounds__(WM_THREADS, 1) k_win_bases(ResolveArgs A) {
         const ResolveChunk ck = A.chunks[A.groups[A.supers[J.first].first].first];
         for (uint32_t i = threadIdx.x; i < WINDOW; i += blockDim.x) {
             uint32_t r = WM_BAD;
-            if (ck.out_start >= (uint64_t)(WINDOW - i)) {
+            if (A.identity_base) {
+                r = WM_REF | i;
+            } else if (ck.out_start >= (uint64_t)(WINDOW - i)) {
                 const uint64_t pos = ck.out_start - WINDOW + i;
                 if (pos >= ck.member_start && pos < ck.job_out) r = A.out[pos];
             }
@@ -2474,6 +2477,18 @@ __global__ void __launch_bounds__(RES_THREADS) k_win_expand(ResolveArgs A) {
             r[e] = (v & WM_REF) ? (uint32_t)sb[v & 0x7fffu] : v;
         }
         *reinterpret_cast<uint4*>(A.bases + (uint64_t)g * WINDOW + i0) = pack_u16x8(r);
+    }
+}
+
+// The window after chunk k (the last of its job) relative to the job's first
+// window: R_k through its group's first window (both maps when the job's base
+// is the identity).
+__global__ void k_win_endmap(ResolveArgs A, uint32_t k, uint16_t* out) {
+    const uint16_t* R = A.maps + (uint64_t)k * WINDOW;
+    const uint16_t* B = A.bases + (uint64_t)A.chunk_group[k] * WINDOW;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < WINDOW; i += gridDim.x * blockDim.x) {
+        const uint32_t r = R[i];
+        out[i] = (uint16_t)((r & WM_REF) ? (uint32_t)B[r & 0x7fffu] : r);
     }
 }
 

@@ -92,3 +92,98 @@ def decode_shard(decoder, blobs: Sequence[bytes], shard: range) -> list[tuple[in
             outs[k] = out[ooffs[q]:ooffs[q] + lens[q]].tobytes() if st[q] == 0 else None
         todo = retry
     return [(i, status[k] if status[k] is not None else ERR_CAPACITY, outs[k]) for k, i in enumerate(idx)]
+
+
+def gzip_body_offset(data: bytes) -> int:
+    """Byte offset of a gzip member's deflate body (RFC 1952 header: FEXTRA,
+    FNAME, FCOMMENT, FHCRC), as gzip.rs:252-300 parse_header reads it."""
+    if len(data) < 10 or data[0] != 0x1F or data[1] != 0x8B or data[2] != 8:
+        raise ValueError("not a deflate gzip member")
+    flg, p = data[3], 10
+    if flg & 4:
+        p += 2 + int.from_bytes(data[p:p + 2], "little")
+    for bit in (8, 16):
+        if flg & bit:
+            p = data.index(b"\0", p) + 1
+    if flg & 2:
+        p += 2
+    return p
+
+
+def decode_member_split(decoder, data: bytes, rank: int, world: int, sink=None, group=None) -> dict:
+    """Decode ONE gzip member on `world` GPUs, this rank's share: the body is cut
+    into `world` ranges at dynamic block starts near equal shares of its bits;
+    every rank decodes its range at once (phase 1), the ranks exchange their
+    ranges' end bits and 32 KiB window maps (the only exchange), each rank
+    composes the window before its range from the earlier ranges' maps and
+    resolves its range (phase 2), and the (CRC32, length) of every range are
+    combined and checked against the member trailer. A range whose start is not
+    where the previous range ended (a false block start) is decoded again from
+    that exact bit, so every rank takes the same rounds. This rank's bytes go to
+    `sink`. Returns {"ok", "total", "crc", "out_len", "rounds"}; raises on
+    corrupt data. Uses torch.distributed (NCCL on GPUs, gloo on CPUs)."""
+    import numpy as np
+    import torch.distributed as dist
+    body = gzip_body_offset(data)
+    nbits = (len(data) - body - 8) * 8
+    start_t = nbits * rank // world
+    stop_t = nbits * (rank + 1) // world if rank + 1 < world else (1 << 64) - 1
+    empty = (1 << 64) - 1  # start and end bit of a range with no block start after its target
+    failed = (1 << 64) - 2  # start bit of a range whose guessed start did not decode
+
+    def begin(start, exact):
+        # a guessed start may be false (a dynamic header inside stored data):
+        # its failure is a broken link the exchange repairs; a failure from an
+        # exact start is an error of the stream, raised on every rank together
+        try:
+            i, m = decoder.split_begin(data, body, start, stop_t, exact=exact)
+            return i, m, None
+        except Exception as ex:  # noqa: BLE001 - passed to every rank below
+            if not exact and start != 0:
+                return {"start_bit": failed, "end_bit": failed, "out_len": 0, "has_trailer": 0, "crc": 0,
+                        "isize": 0, "trailer_byte": 0}, np.zeros(32768, dtype=np.uint16), None
+            return None, None, ex
+
+    info, emap, error = begin(start_t, start_t == 0)
+    rounds = 1
+    for _ in range(world + 1):
+        ends = [None] * world
+        dist.all_gather_object(ends, (None, None, repr(error)) if error else
+                               (info["start_bit"], info["end_bit"], None), group=group)
+        errs = [e for _, _, e in ends if e]
+        if errs:
+            raise error if error else RuntimeError(f"split decode failed on another rank: {errs[0]}")
+        # every non-empty range must start where the previous non-empty one ended
+        live = [r for r in range(world) if ends[r][0] != empty]
+        broken = [b for a, b in zip(live, live[1:]) if ends[b][0] != ends[a][1] or ends[a][1] == failed]
+        if not broken:
+            break
+        first = broken[0]
+        prev = max(r for r in live if r < first)
+        if ends[prev][1] == failed:  # the previous range must be repaired first
+            first, prev = prev, max([r for r in live if r < prev], default=None)
+        if rank == first:  # from the previous range's exact end
+            info, emap, error = begin(ends[prev][1] if prev is not None else 0, True)
+        rounds += 1
+    else:
+        raise RuntimeError("split ranges did not chain")
+    maps = [None] * world
+    dist.all_gather_object(maps, (emap.tobytes(), info["out_len"]), group=group)
+    win = np.full(32768, 0x4000, dtype=np.uint16)  # before the stream: nothing
+    for r in range(rank):
+        m = np.frombuffer(maps[r][0], dtype=np.uint16)
+        win = np.where(m & 0x8000, win[m & 0x7FFF], m).astype(np.uint16)
+    wlen = min(32768, sum(maps[r][1] for r in range(rank)))
+    w = win[32768 - wlen:]
+    if (w >= 0x100).any():
+        raise ValueError("a back-reference reaches before the stream")
+    crc, n = decoder.split_finish(w.astype(np.uint8).tobytes(), sink)
+    parts = [None] * world
+    dist.all_gather_object(parts, (crc, n, info["has_trailer"], info["crc"], info["isize"]), group=group)
+    total_crc, total = parts[0][0], parts[0][1]
+    for c, ln, _, _, _ in parts[1:]:
+        total_crc = decoder.crc32_combine(total_crc, c, ln)
+        total += ln
+    last = [p for p in parts if p[2]]
+    ok = len(last) == 1 and total_crc == last[0][3] and (total & 0xFFFFFFFF) == last[0][4]
+    return {"ok": ok, "total": total, "crc": total_crc, "out_len": n, "rounds": rounds}

@@ -149,3 +149,37 @@ def test_serving_512mib_request_alone_and_in_the_mix(gpu_decoder_factory):
     assert {i: (s, sha(b) if b is not None else None) for i, (s, b) in got.items()} == want
     st = d.serve_stats()
     assert st["completed"] == len(reqs) and d.pending() == 0
+
+
+def test_member_split_in_four_ranges(gpu_decoder_factory):
+    """The member-split path on one GPU: 256 MiB of Zipf text in four ranges,
+    each decoded by its own context (phase 1), the windows composed from the
+    ranges' maps, then each range resolved (phase 2); the joined bytes and the
+    combined CRC32/ISIZE equal the member's."""
+    from rusty_rapidgzip_b200.sharding import gzip_body_offset
+    raw, gz = W.config1(256 << 20, seed=44)
+    body = gzip_body_offset(gz)
+    nbits = (len(gz) - body - 8) * 8
+    world = 4
+    decs = [gpu_decoder_factory() for _ in range(world)]
+    infos, maps = [], []
+    for r in range(world):
+        stop = nbits * (r + 1) // world if r + 1 < world else (1 << 64) - 1
+        info, m = decs[r].split_begin(gz, body, nbits * r // world, stop)
+        infos.append(info)
+        maps.append(m)
+    for a, b in zip(infos, infos[1:]):
+        assert b["start_bit"] == a["end_bit"]
+    win = np.full(32768, 0x4000, dtype=np.uint16)
+    h = hashlib.sha256()
+    crc, total = 0, 0
+    for r in range(world):
+        wlen = min(32768, sum(i["out_len"] for i in infos[:r]))
+        w = win[32768 - wlen:]
+        assert (w < 0x100).all()
+        c, n = decs[r].split_finish(w.astype(np.uint8).tobytes(), h.update)
+        crc = decs[0].crc32_combine(crc, c, n) if r else c
+        total += n
+        win = np.where(maps[r] & 0x8000, win[maps[r] & 0x7FFF], maps[r]).astype(np.uint16)
+    assert h.hexdigest() == sha(raw) and total == len(raw)
+    assert infos[-1]["has_trailer"] and crc == infos[-1]["crc"] and total & 0xFFFFFFFF == infos[-1]["isize"]
