@@ -254,6 +254,28 @@ def run_ours(args, raw, gz, desc):
         t = float(tt.item())
     value = world * len(raw) * args.steps / t / 1e9
 
+    # ---------------- BGZF: the plain per-member path on the file's first 4,096
+    # members (each a complete gzip file: one decode_device call per member)
+    plain = None
+    if args.workload == "bgzf":
+        offs, off = [], 0
+        while len(offs) < 4096 and off + 18 <= len(gz):
+            bs = int.from_bytes(gz[off + 16:off + 18], "little") + 1
+            offs.append((off, bs, int.from_bytes(gz[off + bs - 4:off + bs], "little")))
+            off += bs
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        u = 0
+        for o, bs, isz in offs:
+            m, _ = dec.decode_device(din[o:], bs, dout[u:], isz, stream=stream.cuda_stream)
+            assert m == isz
+            u += isz
+        p1.record(stream)
+        torch.cuda.synchronize()
+        plain = {"members": len(offs), "uncompressed_bytes": u,
+                 "gbs": round(u / (p0.elapsed_time(p1) / 1000.0) / 1e9, 3)}
+
     # ---------------- end to end through the C ABI with host buffers
     pinned = torch.empty(len(gz), dtype=torch.uint8, pin_memory=True)
     pinned.copy_(torch.frombuffer(bytearray(gz), dtype=torch.uint8))
@@ -310,7 +332,8 @@ def run_ours(args, raw, gz, desc):
                            inflate="lane-per-chunk" if args.warps_per_stream < 0 else "warp-per-chunk",
                            boundaries="per target" if args.boundary_mode == 1 else "every offset",
                            markers=ms.markers, speculation_failures=ms.speculation_failures,
-                           graph_launches=ms.graph_launches, autotuned=tuning),
+                           graph_launches=ms.graph_launches, autotuned=tuning,
+                           **({"plain_per_member": plain} if plain else {})),
             "e2e": {"value": round(e2e_value, 3), "unit": "GB/s", "h2d_bytes_per_step": C_,
                     "d2h_bytes_per_step": U_},
             "gpu_launches": int(launches),

@@ -84,7 +84,10 @@ typedef struct rrg_config {
     int32_t host_pipeline;       /* rrg_gpu_decode_host/read_gz: 0 = decode a large single-member stream
                                     in waves with the copy to the host overlapped (falls back to the
                                     checked path on any irregularity); -1 = always the checked path */
-    int32_t reserved;
+    int32_t batch_plan;          /* rrg_gpu_decode_batch: 0 = the member route planned and checked on the
+                                    device (sub-chunk starts, item list, anchored chain, resolve, CRC) as one
+                                    captured graph, with the jobs it cannot finish decoded on the checked
+                                    path; -1 = always the host-planned checked path */
 } rrg_config;
 
 /* Mirrors DecodeStats (lib.rs:103-108), plus device-path counters. */
@@ -98,7 +101,7 @@ typedef struct rrg_stats {
     uint64_t members;              /* gzip members verified */
     uint64_t kernel_launches;      /* kernels launched by this call */
     double finder_ms, inflate_ms, resolve_ms, crc_ms, h2d_ms, d2h_ms, total_ms;
-    uint64_t graph_launches;       /* captured decode graphs replayed by this call (BGZF route) */
+    uint64_t graph_launches;       /* captured decode graphs launched by this call (BGZF route, device-planned batch) */
     uint64_t pipeline_waves;       /* waves of the pipelined host path (0: not taken) */
     uint64_t pipeline_fallbacks;   /* 1 when the pipelined path handed the rest to the checked path */
 } rrg_stats;

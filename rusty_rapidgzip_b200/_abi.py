@@ -77,7 +77,7 @@ class _Config(C.Structure):
         ("boundary_mode", C.c_int32),
         ("hbm_budget_bytes", C.c_uint64),
         ("host_pipeline", C.c_int32),
-        ("reserved", C.c_int32),
+        ("batch_plan", C.c_int32),
     ]
 
 
@@ -130,6 +130,7 @@ class Config:
     boundary_mode: int = 0
     hbm_budget_bytes: int = 0
     host_pipeline: int = 0  # -1: the host path never decodes in overlapped waves
+    batch_plan: int = 0  # -1: decode_batch never takes the device-planned graph route
 
     def _c(self) -> _Config:
         c = _Config()
@@ -143,6 +144,7 @@ class Config:
         c.boundary_mode = self.boundary_mode
         c.hbm_budget_bytes = self.hbm_budget_bytes
         c.host_pipeline = self.host_pipeline
+        c.batch_plan = self.batch_plan
         return c
 
 

@@ -57,6 +57,7 @@ enum : uint32_t {
     ITEM_ONE_MEMBER = 2u,   // input is exactly one gzip member with its header (batch mode)
     ITEM_STORED_START = 4u, // host only: the start is a stored-block header byte of zeros
     ITEM_EMPTY_STORED = 8u, // host only: ... of an empty stored block (LEN = 0)
+    ITEM_SKIP = 16u,        // no work: an unused sub-chunk of a device-planned job (empty result)
 };
 
 struct ChunkResult {

@@ -232,6 +232,12 @@ struct BgzfKey {
     const void* p[24];
     uint64_t v[6];
 };
+// ... and a captured device-planned member batch
+struct BatchKey {
+    const void* p[20];
+    uint64_t v[20];
+};
+constexpr int BATCH_MARKS = 5;  // events between the stages: plan | inflate | chain + resolve | CRC
 
 // One range of a member split across GPUs, between its two phases: the
 // decoded cells stay in the context's slot arena, laid out from out + WINDOW.
@@ -303,6 +309,14 @@ struct rrg_ctx {
 #ifndef RRG_EMU
     cudaGraphExec_t bg_exec = nullptr;
     BgzfKey bg_key{};
+#endif
+    // device-planned member batch: plan and state, and its captured graph
+    DBuf bplan;
+    cudaEvent_t bt_marks[BATCH_MARKS] = {};  // stage boundaries, recorded by the graph
+#ifndef RRG_EMU
+    cudaGraphExec_t bt_exec = nullptr;
+    BatchKey bt_key{};
+    uint32_t bt_kernels = 0;
 #endif
 
     rrg_stats st{};
@@ -2259,10 +2273,11 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
         max_win = std::max(max_win, res_win_bytes(pw.tab, pw.n));
     }
     // ---- device memory
-    // pipe layout: state | infos | live | n_pieces[W] | fin (exp/got/status/mpiece) |
-    //              chunks[max_n] | head_segs[max_n+1] | pieces | piece_crc | tabs
+    // pipe layout: state | infos | live | n_pieces[W] | fin (exp/got/status/mpiece) | seg total |
+    //              wave jobs[W] | chunks[max_n] | head_segs[max_n+1] | pieces | piece_crc | tabs
     const size_t o_info = 64, o_live = o_info + round8(Wn * sizeof(WaveInfo)), o_np = o_live + 8,
-                 o_fin = o_np + round8(Wn * 4), o_chunks = o_fin + 64,
+                 o_fin = o_np + round8(Wn * 4), o_seg = o_fin + 64, o_wj = o_seg + 8,
+                 o_chunks = o_wj + round8(Wn * sizeof(WaveJob)),
                  o_hs = o_chunks + round8((size_t)max_n * sizeof(ResolveChunk)),
                  o_pc = o_hs + ((size_t)max_n + 1) * 8, o_pcrc = o_pc + (size_t)total_pieces * sizeof(CrcPiece),
                  o_tabs = o_pcrc + round8((size_t)total_pieces * 4), p_total = o_tabs + tabs.size();
@@ -2287,6 +2302,11 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
     uint8_t* P = (uint8_t*)c->pipe.p;
     WaveState st0{0, 0, 1, 0};
     CK(cudaMemcpyAsync(P, &st0, sizeof(st0), cudaMemcpyHostToDevice, c->stream));
+    std::vector<WaveJob> wj(Wn);
+    for (uint32_t w = 0; w < Wn; w++)
+        wj[w] = WaveJob{waves[w].first, waves[w].n, n - 1, waves[w].piece_off, waves[w].piece_cap, waves[w].n,
+                        tgt.cap, 0};
+    CK(cudaMemcpyAsync(P + o_wj, wj.data(), Wn * sizeof(WaveJob), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(P + o_tabs, tabs.data(), tabs.size(), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->items.p, items.data(), (size_t)n * sizeof(ChunkItem), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->order.p, order.data(), (size_t)n * 4, cudaMemcpyHostToDevice, c->stream));
@@ -2345,20 +2365,21 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
         WaveArgs WA{};
         WA.items = (const ChunkItem*)c->items.p;
         WA.results = (const ChunkResult*)c->results.p;
-        WA.first = pw.first;
-        WA.n = pw.n;
-        WA.last_item = n - 1;
+        WA.jobs = (const WaveJob*)(P + o_wj) + w;
+        WA.n_jobs = 1;
+        WA.item_base = pw.first;
+        WA.n_items = pw.n;
         WA.state = (WaveState*)P;
         WA.info = h_info + w;  // mapped pinned memory: no copy queued behind the output
         WA.live = (uint32_t*)(P + o_live);
         WA.chunks = (ResolveChunk*)(P + o_chunks);
         WA.head_segs = (uint64_t*)(P + o_hs);
-        WA.pieces = (CrcPiece*)(P + o_pc) + pw.piece_off;
-        WA.piece_cap = pw.piece_cap;
+        WA.pieces = (CrcPiece*)(P + o_pc);
         WA.n_pieces = (uint32_t*)(P + o_np) + w;
-        WA.out_cap = tgt.cap;
+        WA.seg_total = (uint64_t*)(P + o_seg);
         WA.mbs = (const MemberRec*)c->mbs.p;
         WA.mb_count = (const uint32_t*)c->mbcount.p;
+        WA.mb_cap = 4096;
         WA.exp_crc = (uint32_t*)(P + o_fin);
         WA.exp_isize = (uint32_t*)(P + o_fin) + 1;
         RRG_LAUNCH(k_wave_chain, 1, WAVE_THREADS, 0, rs, WA);
@@ -2375,7 +2396,7 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
         R.markers = (unsigned long long*)c->markers.p;
         R.live = WA.live;
         if (int rc = launch_resolve(c, R, rs, err)) return rc;
-        CrcWideArgs CA{tgt.p, WA.pieces, pw.piece_cap, (uint32_t*)(P + o_pcrc) + pw.piece_off,
+        CrcWideArgs CA{tgt.p, WA.pieces + pw.piece_off, pw.piece_cap, (uint32_t*)(P + o_pcrc) + pw.piece_off,
                        (const uint32_t*)c->crc_table.p, WA.n_pieces};
         RRG_LAUNCH(k_crc_pieces_wide, persistent_blocks(c, 8, pw.piece_cap, 1), CRCW_THREADS, 0, rs, CA);
         LAUNCHED(c);
@@ -3046,6 +3067,491 @@ int read_range_impl(rrg_ctx* c, const uint8_t* data, size_t len, const rrg_index
 // own output range. Headers are parsed on the device; BGZF files take the
 // BGZF route one by one; every other file is a job of the member route, in
 // waves whose reserved output cells fit the device budget.
+// ------------------------------------------------------------ device-planned member batch
+// The member route of a batch with every stage hand-off on the device (sub-
+// chunk starts from the scan's verified starts, the item list, the anchored
+// chain, resolve and CRC), so the decode after the header sniff is one
+// sequence of launches with no host round trip, captured once as a CUDA graph
+// and replayed while the batch's shape (sizes and buffers) stays the same. The
+// plan's contents (jobs, orders, tables) are uploaded before each launch, so a
+// new batch of the same shape replays the same graph. Jobs the device could not
+// take through (a false start, a full slot, a CRC piece region too small) come
+// back unfinished and go through the checked member route.
+struct BatchLaunch {
+    bool direct = false;           // no job split: every file decodes straight to its bytes
+    uint32_t nj = 0, n_items = 0, n_big = 0, total_pieces = 0, mb_cap = 0;
+    const uint8_t* scan_body = nullptr;
+    uint64_t scan_len = 0, n_tiles = 0;
+    uint32_t cap = 0, cap2 = 0, cap3 = 0, n_list = 0, sgrid = 0, igrid = 0;
+    ResTables tab;
+    // c->bplan layout: uploaded | device-written
+    size_t o_jobs = 0, o_bigbit = 0, o_bigjob = 0, o_order = 0, o_mp = 0, o_tabs = 0, o_state = 0, o_wj = 0,
+           up_end = 0;
+    size_t o_info = 0, o_ecrc = 0, o_eisz = 0, o_gcrc = 0, o_glen = 0, o_mst = 0, down_end = 0;
+    size_t o_np = 0, o_seg = 0, o_chunks = 0, o_hs = 0, o_pc = 0, o_pcrc = 0, o_keys = 0, total = 0;
+};
+
+int batch_enqueue(rrg_ctx* c, const uint8_t* d_in, uint8_t* d_out, const BatchLaunch& L, cudaEvent_t* marks,
+                  rrg_error* err) {
+    uint8_t* P = (uint8_t*)c->bplan.p;
+    cudaStream_t s = c->stream;
+    auto mark = [&](int i) -> int {
+        if (marks) CK(cudaEventRecord(marks[i], s));
+        return 0;
+    };
+    if (int r = mark(0)) return r;
+    CK(cudaMemsetAsync(c->queue.p, 0, 16, s));
+    CK(cudaMemsetAsync(c->mbcount.p, 0, 16, s));
+    CK(cudaMemsetAsync(c->rerr.p, 0, 16, s));
+    CK(cudaMemsetAsync(c->markers.p, 0, 8, s));
+    if (!L.direct) {
+        // ---- scan, verification, start selection and the item list
+        CK(cudaMemsetAsync(c->ncand.p, 0, 64, s));
+        CK(cudaMemsetAsync(P + L.o_keys, 0xff, (size_t)L.n_items * 8, s));
+        uint64_t* cand = (uint64_t*)c->cand.p;
+        uint64_t* surv = cand + L.cap;
+        uint64_t* stored = surv + L.cap2;
+        uint32_t* counts = (uint32_t*)c->ncand.p;
+        ScanArgs S{L.scan_body, L.scan_len, cand, counts, L.cap, stored, counts + 3, L.cap3, 0, L.n_tiles,
+                   L.n_list ? (const uint32_t*)c->tiles.p : nullptr, L.n_list};
+        const uint32_t st = c->scan_threads;
+        if (st == 64) RRG_LAUNCH(k_scan_candidates<64>, L.sgrid, 64, 0, s, S);
+        else if (st == 128) RRG_LAUNCH(k_scan_candidates<128>, L.sgrid, 128, 0, s, S);
+        else RRG_LAUNCH(k_scan_candidates<256>, L.sgrid, 256, 0, s, S);
+        LAUNCHED(c);
+        VerifyArgs V{L.scan_body, L.scan_len, cand, counts, L.cap, surv, counts + 1, L.cap2, nullptr, nullptr, counts + 4};
+        VerifyArgs H{L.scan_body, L.scan_len, surv, counts + 1, L.cap2, nullptr, nullptr, 0, (uint8_t*)c->vflag.p,
+                     counts + 2, nullptr};
+        RRG_LAUNCH(k_verify_light, c->n_sm * 8, 256, 0, s, V);
+        LAUNCHED(c);
+        RRG_LAUNCH(k_verify_heavy, c->n_sm * 4, 4 * 32, 4 * sizeof(FindSmem), s, H);
+        LAUNCHED(c);
+        BatchArgs B{};
+        B.jobs = (const BatchJob*)(P + L.o_jobs);
+        B.n_jobs = L.nj;
+        B.big_bit = (const uint64_t*)(P + L.o_bigbit);
+        B.big_job = (const uint32_t*)(P + L.o_bigjob);
+        B.n_big = L.n_big;
+        B.surv = surv;
+        B.vflag = (const uint8_t*)c->vflag.p;
+        B.counts = counts;
+        B.cap2 = L.cap2;
+        B.cap3 = L.cap3;
+        B.stored = stored;
+        B.keys = (unsigned long long*)(P + L.o_keys);
+        B.items = (ChunkItem*)c->items.p;
+        B.wjobs = (WaveJob*)(P + L.o_wj);
+        RRG_LAUNCH(k_batch_select, c->n_sm * 4, 256, 0, s, B);
+        LAUNCHED(c);
+        RRG_LAUNCH(k_batch_items, std::min<uint32_t>(L.nj, c->n_sm * 2), WAVE_THREADS, 0, s, B);
+        LAUNCHED(c);
+    }
+    if (int r = mark(1)) return r;
+    // ---- inflate
+    InflateArgs A{};
+    A.in = d_in;
+    A.items = (const ChunkItem*)c->items.p;
+    A.results = (ChunkResult*)c->results.p;
+    A.n_items = L.n_items;
+    A.order = (const uint32_t*)(P + L.o_order);
+    A.queue = (uint32_t*)c->queue.p;
+    A.out = L.direct ? (void*)d_out : c->cells.p;
+    A.mbs = (MemberRec*)c->mbs.p;
+    A.mb_count = (uint32_t*)c->mbcount.p;
+    A.mb_cap = L.mb_cap;
+    const uint32_t IW = c->inflate_warps;
+    if (L.direct) RRG_LAUNCH(k_inflate<uint8_t>, L.igrid, IW * 32, IW * sizeof(WarpSmem), s, A);
+    else RRG_LAUNCH(k_inflate<uint16_t>, L.igrid, IW * 32, IW * sizeof(WarpSmem), s, A);
+    LAUNCHED(c);
+    if (int r = mark(2)) return r;
+    // ---- anchored chains and layout, then resolve
+    WaveArgs WA{};
+    WA.items = (const ChunkItem*)c->items.p;
+    WA.results = (const ChunkResult*)c->results.p;
+    WA.jobs = (const WaveJob*)(P + L.o_wj);
+    WA.n_jobs = L.nj;
+    WA.item_base = 0;
+    WA.n_items = L.n_items;
+    WA.state = (WaveState*)(P + L.o_state);
+    WA.info = (WaveInfo*)(P + L.o_info);
+    WA.live = nullptr;
+    WA.chunks = (ResolveChunk*)(P + L.o_chunks);
+    WA.head_segs = (uint64_t*)(P + L.o_hs);
+    WA.pieces = (CrcPiece*)(P + L.o_pc);
+    WA.n_pieces = (uint32_t*)(P + L.o_np);
+    WA.seg_total = (uint64_t*)(P + L.o_seg);
+    WA.mbs = (const MemberRec*)c->mbs.p;
+    WA.mb_count = (const uint32_t*)c->mbcount.p;
+    WA.mb_cap = L.mb_cap;
+    WA.exp_crc = (uint32_t*)(P + L.o_ecrc);
+    WA.exp_isize = (uint32_t*)(P + L.o_eisz);
+    WA.direct = L.direct ? 1u : 0u;
+    RRG_LAUNCH(k_wave_chain, std::min<uint32_t>(L.nj, c->n_sm * 2), WAVE_THREADS, 0, s, WA);
+    LAUNCHED(c);
+    if (!L.direct) {
+        if (L.nj > 1) {
+            RRG_LAUNCH(k_wave_segs, 1, WAVE_THREADS, 0, s, WA);
+            LAUNCHED(c);
+            RRG_LAUNCH(k_wave_segs_add, std::min<uint32_t>(L.nj, c->n_sm * 4), 256, 0, s, WA);
+            LAUNCHED(c);
+        }
+        ResolveArgs R{};
+        R.cells = (uint16_t*)c->cells.p;
+        R.chunks = WA.chunks;
+        R.head_segs = WA.head_segs;
+        res_args(R, L.tab, P + L.o_tabs, (uint16_t*)c->win.p, L.n_items);
+        R.out = d_out;
+        R.err = (uint32_t*)c->rerr.p;
+        R.markers = (unsigned long long*)c->markers.p;
+        if (int rc = launch_resolve(c, R, s, err)) return rc;
+    }
+    if (int r = mark(3)) return r;
+    // ---- CRC32 and ISIZE of every member
+    CrcWideArgs CA{d_out, (const CrcPiece*)(P + L.o_pc), L.total_pieces, (uint32_t*)(P + L.o_pcrc),
+                   (const uint32_t*)c->crc_table.p, nullptr};
+    RRG_LAUNCH(k_crc_pieces_wide, persistent_blocks(c, 8, L.total_pieces, 1), CRCW_THREADS, 0, s, CA);
+    LAUNCHED(c);
+    CrcMemberArgs CB{(const CrcPiece*)(P + L.o_pc), (const uint32_t*)(P + L.o_pcrc), (const uint32_t*)(P + L.o_mp),
+                     L.nj, (const uint32_t*)(P + L.o_ecrc), (const uint32_t*)(P + L.o_eisz),
+                     (uint32_t*)(P + L.o_gcrc), (uint64_t*)(P + L.o_glen), (int32_t*)(P + L.o_mst), nullptr};
+    RRG_LAUNCH(k_crc_members, (L.nj * 32 + 255) / 256, 256, 0, s, CB);
+    LAUNCHED(c);
+    if (int r = mark(4)) return r;
+    return 0;
+}
+
+// Decodes the jobs (whole single-member streams with fixed destinations) on the
+// device-planned route. *taken is false when the route does not apply (the
+// caller then uses members_route); jobs it could not finish are decoded by
+// members_route here.
+int batch_device(rrg_ctx* c, const uint8_t* d_in, std::vector<MemberJob>& jobs, OutTarget& tgt, bool* taken,
+                 rrg_error* err) {
+    *taken = false;
+    const size_t nj = jobs.size();
+    if (!nj || tgt.grow || !c->scan_bounds || c->lanes || c->cfg.batch_plan < 0 || nj > (1u << 24)) return 0;
+    for (const MemberJob& j : jobs)
+        if (j.start_bit || j.stop_bit != ~0ull || j.dst_cap == ~0ull || j.capture || j.split || !j.check_crc) return 0;
+    if (int rc = upload_tables(c, err)) return rc;
+    // ---- plan: sub-chunks per job at the members_route spacing
+    uint64_t total_c = 0;
+    for (const MemberJob& j : jobs) total_c += j.len - j.body_off;
+    const uint64_t slots = inflate_slots(c);
+    const uint64_t G = c->gpu_chunk ? std::max<uint64_t>(c->gpu_chunk, 4096)
+                                    : std::max<uint64_t>(16ull << 10, (total_c + slots - 1) / slots);
+    BatchLaunch L;
+    L.nj = (uint32_t)nj;
+    std::vector<BatchJob> bj(nj);
+    uint64_t n_items = 0, arena = 0, pieces = 0;
+    bool any_split = false;
+    for (size_t i = 0; i < nj; i++) {
+        const MemberJob& j = jobs[i];
+        const uint64_t blen = j.len - j.body_off;
+        const uint64_t K = blen > G ? std::max<uint64_t>(1, (blen + G / 2) / G) : 1;
+        any_split |= K > 1;
+        BatchJob& b = bj[i];
+        b.in_off = j.file_off + j.body_off;
+        b.blen = blen;
+        b.expand = j.expand > 0 ? j.expand : c->expand;
+        b.dst_off = j.dst_off;
+        b.dst_cap = j.dst_cap;
+        b.K = (uint32_t)K;
+        b.item_first = (uint32_t)n_items;
+        b.arena = arena;
+        // every slot holds span x expand + 64 KiB (rounded to 8): the spans of
+        // the job's items add up to at most blen + K bytes
+        // (a multiple of 8 cells, so every slot starts 16-byte aligned)
+        const uint64_t slots_bound = round8((uint64_t)std::ceil((double)(blen + K) * b.expand) + K * (65536 + 16));
+        arena += slots_bound;
+        b.piece_off = (uint32_t)pieces;
+        b.piece_cap = (uint32_t)(std::min<uint64_t>(j.dst_cap, slots_bound) / WAVE_PIECE + 2);
+        pieces += b.piece_cap;
+        n_items += K;
+        if (n_items > (1u << 30) || pieces > (1u << 30)) return 0;
+    }
+    L.direct = !any_split;
+    L.n_items = (uint32_t)n_items;
+    L.total_pieces = (uint32_t)pieces;
+    L.mb_cap = L.n_items + 4096;
+    std::vector<ChunkItem> ditems;
+    std::vector<WaveJob> wj(nj);
+    if (L.direct) {  // one item per job, straight into its destination
+        ditems.resize(nj);
+        for (size_t i = 0; i < nj; i++) {
+            ChunkItem& it = ditems[i];
+            it = ChunkItem{};
+            it.in_off = bj[i].in_off;
+            it.in_len = bj[i].blen;
+            it.end_hint = ~0ull;
+            it.out_off = bj[i].dst_off;
+            it.out_cap = bj[i].dst_cap;
+            it.id = (uint32_t)i;
+            wj[i] = WaveJob{(uint32_t)i, 1, (uint32_t)i, bj[i].piece_off, bj[i].piece_cap, 1,
+                            bj[i].dst_off + bj[i].dst_cap, bj[i].dst_off};
+        }
+    }
+    // ---- scan region (every split job) and the tiles around the ideal starts
+    std::vector<uint64_t> big_bit;
+    std::vector<uint32_t> big_job, tiles;
+    if (!L.direct) {
+        std::vector<uint32_t> bigs;
+        for (size_t i = 0; i < nj; i++)
+            if (bj[i].K > 1) bigs.push_back((uint32_t)i);
+        std::sort(bigs.begin(), bigs.end(), [&](uint32_t a, uint32_t b) { return bj[a].in_off < bj[b].in_off; });
+        uint64_t lo = ~0ull, hi = 0;
+        for (uint32_t i : bigs) {
+            lo = std::min(lo, bj[i].in_off);
+            hi = std::max(hi, bj[i].in_off + bj[i].blen);
+        }
+        for (uint32_t i : bigs) {
+            bj[i].scan_bit = (bj[i].in_off - lo) * 8;
+            big_bit.push_back(bj[i].scan_bit);
+            big_job.push_back(i);
+        }
+        L.n_big = (uint32_t)bigs.size();
+        L.scan_body = d_in + lo;
+        L.scan_len = hi - lo;
+        const uint64_t tb = (uint64_t)c->scan_threads * 16, mis = (uintptr_t)(d_in + lo) & 15;
+        L.n_tiles = (mis + L.scan_len + tb - 1) / tb;
+        constexpr uint64_t NEAR = 16 << 10;
+        for (uint32_t i : bigs) {
+            const uint64_t nbits = bj[i].blen * 8;
+            for (uint32_t k = 1; k < bj[i].K; k++) {
+                const uint64_t byte = (bj[i].scan_bit + nbits * k / bj[i].K) / 8;
+                const uint64_t t0 = (mis + (byte > NEAR ? byte - NEAR : 0)) / tb;
+                const uint64_t t1 = std::min(L.n_tiles - 1, (mis + byte + NEAR) / tb);
+                for (uint64_t t = t0; t <= t1; t++) tiles.push_back((uint32_t)t);
+            }
+        }
+        std::sort(tiles.begin(), tiles.end());
+        tiles.erase(std::unique(tiles.begin(), tiles.end()), tiles.end());
+        if (L.n_tiles > 0xffffffffull || tiles.size() * 2 >= L.n_tiles) tiles.clear();  // scan everything
+        L.n_list = (uint32_t)tiles.size();
+        L.cap = (uint32_t)std::min<uint64_t>(L.scan_len / 64 + 65536, 1ull << 28);
+        L.cap2 = std::max<uint32_t>(L.cap / 16, 65536);
+        L.cap3 = (uint32_t)std::min<uint64_t>(L.scan_len / 1024 + 4096, 1ull << 26);
+        const uint64_t work = L.n_list ? L.n_list : L.n_tiles;
+        L.sgrid = (uint32_t)std::max<uint64_t>(
+            1, std::min<uint64_t>(work, (uint64_t)c->n_sm * (2048 / c->scan_threads)));
+        std::vector<uint32_t> jc(nj);
+        for (size_t i = 0; i < nj; i++) jc[i] = bj[i].K;
+        build_res_tables(jc, c->n_sm, L.tab);
+    }
+    // largest estimated spans first
+    std::vector<uint32_t> jorder(nj), order(L.n_items);
+    for (uint32_t i = 0; i < nj; i++) jorder[i] = i;
+    std::stable_sort(jorder.begin(), jorder.end(),
+                     [&](uint32_t a, uint32_t b) { return bj[a].blen / bj[a].K > bj[b].blen / bj[b].K; });
+    {
+        size_t q = 0;
+        for (uint32_t i : jorder)
+            for (uint32_t k = 0; k < bj[i].K; k++) order[q++] = bj[i].item_first + k;
+    }
+    std::vector<uint32_t> mp(nj + 1);
+    for (size_t i = 0; i < nj; i++) mp[i] = bj[i].piece_off;
+    mp[nj] = L.total_pieces;
+    std::vector<WaveState> st0(nj);
+    for (size_t i = 0; i < nj; i++) st0[i] = WaveState{0, bj[i].dst_off, 1, 0};
+    // ---- layout of c->bplan
+    size_t o = 0;
+    auto take = [&](size_t bytes) {
+        const size_t at = o;
+        o = round8(o + bytes);
+        return at;
+    };
+    L.o_jobs = take(nj * sizeof(BatchJob));
+    L.o_bigbit = take(big_bit.size() * 8);
+    L.o_bigjob = take(big_job.size() * 4);
+    L.o_order = take((size_t)L.n_items * 4);
+    L.o_mp = take((nj + 1) * 4);
+    L.o_tabs = take(L.direct ? 0 : L.tab.bytes);
+    L.o_state = take(nj * sizeof(WaveState));
+    L.o_wj = take(nj * sizeof(WaveJob));
+    L.up_end = o;
+    L.o_info = take(nj * sizeof(WaveInfo));
+    L.o_ecrc = take(nj * 4);
+    L.o_eisz = take(nj * 4);
+    L.o_gcrc = take(nj * 4);
+    L.o_glen = take(nj * 8);
+    L.o_mst = take(nj * 4);
+    L.down_end = o;
+    L.o_np = take(nj * 4);
+    L.o_seg = take(nj * 8);
+    L.o_chunks = take(L.direct ? 0 : (size_t)L.n_items * sizeof(ResolveChunk));
+    L.o_hs = take(L.direct ? 0 : ((size_t)L.n_items + 1) * 8);
+    L.o_pc = take((size_t)L.total_pieces * sizeof(CrcPiece));
+    L.o_pcrc = take((size_t)L.total_pieces * 4);
+    L.o_keys = take(L.direct ? 0 : (size_t)L.n_items * 8);
+    L.total = o;
+    std::vector<uint8_t> up(L.up_end);
+    std::memcpy(up.data() + L.o_jobs, bj.data(), nj * sizeof(BatchJob));
+    if (!big_bit.empty()) std::memcpy(up.data() + L.o_bigbit, big_bit.data(), big_bit.size() * 8);
+    if (!big_job.empty()) std::memcpy(up.data() + L.o_bigjob, big_job.data(), big_job.size() * 4);
+    std::memcpy(up.data() + L.o_order, order.data(), (size_t)L.n_items * 4);
+    std::memcpy(up.data() + L.o_mp, mp.data(), (nj + 1) * 4);
+    if (!L.direct) L.tab.write(up.data() + L.o_tabs);
+    std::memcpy(up.data() + L.o_state, st0.data(), nj * sizeof(WaveState));
+    std::memcpy(up.data() + L.o_wj, wj.data(), nj * sizeof(WaveJob));
+    // ---- device memory
+    CK(dgrow(c->bplan, L.total));
+    CK(dgrow(c->items, (size_t)L.n_items * sizeof(ChunkItem)));
+    CK(dgrow(c->results, (size_t)L.n_items * sizeof(ChunkResult)));
+    CK(dgrow(c->queue, 16));
+    CK(dgrow(c->mbs, (size_t)L.mb_cap * sizeof(MemberRec)));
+    CK(dgrow(c->mbcount, 16));
+    CK(dgrow(c->rerr, 16));
+    CK(dgrow(c->markers, 8));
+    if (!L.direct) {
+        CK(dgrow(c->cells, (arena + 8) * 2));
+        CK(dgrow(c->win, res_win_bytes(L.tab, L.n_items)));
+        CK(dgrow(c->cand, (size_t)L.cap * 8 + (size_t)L.cap2 * 8 + (size_t)L.cap3 * 8));
+        CK(dgrow(c->ncand, 64));
+        CK(dgrow(c->vflag, L.cap2));
+        if (L.n_list) CK(dgrow(c->tiles, (size_t)L.n_list * 4));
+    }
+    {
+        const uint32_t IW = c->inflate_warps;
+        int occ = 0;
+        if (L.direct) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_inflate<uint8_t>, IW * 32, IW * sizeof(WarpSmem));
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_inflate<uint16_t>, IW * 32, IW * sizeof(WarpSmem));
+        L.igrid = persistent_blocks(c, std::max(1, occ), L.n_items, IW);
+    }
+    if (int rw = wait_arrival(c, err)) return rw;
+    *taken = true;
+    // ---- uploads (outside the graph: the graph reads them from fixed buffers)
+    CK(cudaMemcpyAsync(c->bplan.p, up.data(), L.up_end, cudaMemcpyHostToDevice, c->stream));
+    if (L.direct)
+        CK(cudaMemcpyAsync(c->items.p, ditems.data(), nj * sizeof(ChunkItem), cudaMemcpyHostToDevice, c->stream));
+    if (L.n_list) CK(cudaMemcpyAsync(c->tiles.p, tiles.data(), (size_t)L.n_list * 4, cudaMemcpyHostToDevice, c->stream));
+    cudaEvent_t* marks = c->bt_marks;
+    bool timed = true;
+    for (int i = 0; i < BATCH_MARKS; i++)
+        if (!marks[i] && cudaEventCreate(&marks[i]) != cudaSuccess) {
+            marks[i] = nullptr;
+            timed = false;
+        }
+    cudaGetLastError();
+    bool ran = false;
+#ifndef RRG_EMU
+    if (c->use_graphs) {
+        BatchKey key{};
+        const DBuf* bs[] = {&c->bplan, &c->items, &c->results, &c->queue, &c->mbs,   &c->mbcount, &c->rerr,
+                            &c->markers, &c->cells, &c->win,   &c->cand,  &c->ncand, &c->vflag,   &c->tiles,
+                            &c->crc_table};
+        for (size_t i = 0; i < sizeof(bs) / sizeof(bs[0]); i++) key.p[i] = bs[i]->p;
+        key.p[15] = d_in;
+        key.p[16] = tgt.p;
+        key.p[17] = c->stream;
+        key.p[18] = L.scan_body;
+        key.p[19] = timed ? marks[0] : nullptr;
+        const uint64_t vals[] = {L.direct, L.nj, L.n_items, L.n_big, L.total_pieces, L.mb_cap, L.scan_len, L.n_tiles,
+                                 L.cap, L.cap2, L.cap3, L.n_list, L.sgrid, L.igrid, L.tab.groups.size(),
+                                 L.tab.supers.size(), L.tab.jobs.size(), L.total,
+                                 ((uint64_t)c->scan_threads << 32) | c->inflate_warps, L.o_tabs};
+        for (size_t i = 0; i < 20; i++) key.v[i] = vals[i];
+        if (!c->bt_exec || std::memcmp(&key, &c->bt_key, sizeof(key)) != 0) {
+            if (c->bt_exec) cudaGraphExecDestroy(c->bt_exec);
+            c->bt_exec = nullptr;
+            cudaGraph_t g = nullptr;
+            if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                const uint64_t l0 = c->launches;
+                int rc = batch_enqueue(c, d_in, tgt.p, L, timed ? marks : nullptr, err);
+                const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+                c->bt_kernels = (uint32_t)(c->launches - l0);
+                g_launches.fetch_sub(c->launches - l0);  // counted when the graph runs
+                c->launches = l0;
+                if (rc == 0 && e == cudaSuccess && g && cudaGraphInstantiate(&c->bt_exec, g, 0) == cudaSuccess)
+                    c->bt_key = key;
+                else
+                    c->bt_exec = nullptr;
+                if (g) cudaGraphDestroy(g);
+            }
+            cudaGetLastError();  // a failed capture leaves no sticky error; run directly below
+        }
+        if (c->bt_exec) {
+            CK(cudaGraphLaunch(c->bt_exec, c->stream));
+            g_launches.fetch_add(c->bt_kernels);
+            c->launches += c->bt_kernels;
+            c->st.graph_launches++;
+            ran = true;
+        }
+    }
+#endif
+    if (!ran) {
+        if (int rc = batch_enqueue(c, d_in, tgt.p, L, timed ? marks : nullptr, err)) return rc;
+    }
+    // ---- outcomes: one copy of the per-job words, one synchronisation
+    std::vector<uint8_t> down(L.down_end - L.o_info);
+    std::vector<WaveJob> wout(nj);
+    uint32_t e4[4] = {0, 0, 0, 0};
+    unsigned long long nmk = 0;
+    uint8_t* P = (uint8_t*)c->bplan.p;
+    CK(cudaMemcpyAsync(down.data(), P + L.o_info, down.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(wout.data(), P + L.o_wj, nj * sizeof(WaveJob), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(e4, c->rerr.p, 16, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(&nmk, c->markers.p, 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (timed) {
+        float f[4] = {0, 0, 0, 0};
+        for (int i = 0; i < 4; i++)
+            if (cudaEventElapsedTime(&f[i], marks[i], marks[i + 1]) != cudaSuccess) f[i] = 0;
+        cudaGetLastError();
+        c->st.finder_ms += f[0];
+        c->st.inflate_ms += f[1];
+        c->st.resolve_ms += f[2];
+        c->st.crc_ms += f[3];
+    }
+    c->st.markers += nmk;
+    auto at = [&](size_t off) { return down.data() + (off - L.o_info); };
+    const WaveInfo* info = (const WaveInfo*)at(L.o_info);
+    const uint32_t* ecrc = (const uint32_t*)at(L.o_ecrc);
+    const uint32_t* eisz = (const uint32_t*)at(L.o_eisz);
+    const uint32_t* gcrc = (const uint32_t*)at(L.o_gcrc);
+    const uint64_t* glen = (const uint64_t*)at(L.o_glen);
+    const int32_t* mst = (const int32_t*)at(L.o_mst);
+    int64_t bad_job = -1;
+    if (e4[0] && !L.direct) {  // the first chunk whose markers did not resolve
+        for (size_t i = 0; i < nj; i++)
+            if (e4[1] >= bj[i].item_first && e4[1] < bj[i].item_first + bj[i].K) bad_job = (int64_t)i;
+    }
+    std::vector<size_t> redo;
+    for (size_t i = 0; i < nj; i++) {
+        MemberJob& j = jobs[i];
+        c->st.gpu_chunks += wout[i].n;
+        if (!info[i].ok) {
+            redo.push_back(i);
+            continue;
+        }
+        j.out.total = info[i].out_len;
+        j.out.members = 1;
+        j.out.consumed = j.file_off + j.len;
+        c->st.members++;
+        if ((int64_t)i == bad_job) {
+            set_err(&j.err, RRG_ERR_DEFLATE_INVALID, "%s", msg_text(MSG_MARKER_WINDOW));
+            j.rc = RRG_ERR_DEFLATE_INVALID;
+            continue;
+        }
+        if (mst[i] == DS_CRC || mst[i] == DS_ISIZE) {
+            const MemberSpan m{j.dst_off, glen[i], ecrc[i], eisz[i],
+                               j.report_off + j.file_off + j.body_off + info[i].trailer_byte};
+            j.rc = member_error(&j.err, m, j.member_base, mst[i], gcrc[i], glen[i]);
+        }
+    }
+    // ---- jobs the device route did not finish: the checked route
+    if (!redo.empty()) {
+        std::vector<MemberJob> rj;
+        for (size_t i : redo) {
+            MemberJob j = jobs[i];
+            j.rc = 0;
+            j.err = rrg_error{};
+            j.out = Decoded{};
+            rj.push_back(j);
+        }
+        if (int rc = members_route(c, d_in, rj, tgt, err)) return rc;
+        for (size_t q = 0; q < redo.size(); q++) jobs[redo[q]] = rj[q];
+    }
+    return 0;
+}
+
 int batch_impl(rrg_ctx* c, const uint8_t* d_in, const uint64_t* in_off, const uint64_t* in_len, uint8_t* d_out,
                const uint64_t* out_off, const uint64_t* out_cap, uint64_t* out_len, int32_t* status, size_t n,
                rrg_error* err) {
@@ -3135,7 +3641,9 @@ int batch_impl(rrg_ctx* c, const uint8_t* d_in, const uint64_t* in_off, const ui
             b++;
         }
         std::vector<MemberJob> wave(jobs.begin() + a, jobs.begin() + b);
-        rc = members_route(c, d_in, wave, tgt, err);
+        bool taken = false;
+        rc = batch_device(c, d_in, wave, tgt, &taken, err);
+        if (!rc && !taken) rc = members_route(c, d_in, wave, tgt, err);
         if (rc) return rc;
         for (size_t q = 0; q < wave.size(); q++) {
             const size_t i = job_item[a + q];
@@ -3256,11 +3764,17 @@ void release_scratch(rrg_ctx* c) {
                     &c->out,    &c->targets, &c->limits,    &c->found,    &c->next_lut, &c->chunks,    &c->tiles,
                     &c->rerr,   &c->markers, &c->crc_table, &c->pieces,   &c->piece_crc, &c->mpiece,   &c->exp_crc,
                     &c->exp_isize, &c->got_crc, &c->got_len, &c->mstatus, &c->comp, &c->comp2, &c->pfx, &c->bg_bcount, &c->bg_bbase,
-                    &c->bg_coff, &c->bg_csize, &c->bg_small, &c->sniff, &c->pipe};
+                    &c->bg_coff, &c->bg_csize, &c->bg_small, &c->sniff, &c->pipe, &c->bplan};
 #ifndef RRG_EMU
     if (c->bg_exec) cudaGraphExecDestroy(c->bg_exec);
     c->bg_exec = nullptr;
+    if (c->bt_exec) cudaGraphExecDestroy(c->bt_exec);
+    c->bt_exec = nullptr;
 #endif
+    for (cudaEvent_t& e : c->bt_marks) {
+        if (e) cudaEventDestroy(e);
+        e = nullptr;
+    }
     for (DBuf* b : bufs) {
         if (b->p) cudaFree(b->p);
         b->p = nullptr;

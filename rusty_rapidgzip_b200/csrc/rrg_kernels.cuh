@@ -843,6 +843,11 @@ __device__ int dev_parse_header(const Src& s, uint64_t at, uint64_t* hl, int* ms
 template <typename CellT>
 __device__ void inflate_item(WarpSmem& S, const InflateArgs& A, uint32_t item_idx, int lane) {
     const ChunkItem it = A.items[item_idx];
+    if (it.flags & ITEM_SKIP) {
+        if (lane == 0) A.results[item_idx] = ChunkResult{0, it.start_bit, DS_OK, 0, 0, 0, 0, 0};
+        __syncwarp();
+        return;
+    }
     CellT* out = (CellT*)A.out + it.out_off;
     ItemState st;
     st.br.s = make_src(A.in + it.in_off, it.in_len);
@@ -1359,6 +1364,10 @@ __device__ void lane_stored(LaneState& st, CellT* out) {
 template <typename CellT>
 __device__ void lane_item(const InflateArgs& A, uint32_t item_idx, LaneTab& T, LaneScratch* scr, const LaneConsts& K) {
     const ChunkItem it = A.items[item_idx];
+    if (it.flags & ITEM_SKIP) {
+        A.results[item_idx] = ChunkResult{0, it.start_bit, DS_OK, 0, 0, 0, 0, 0};
+        return;
+    }
     CellT* out = (CellT*)A.out + it.out_off;
     LaneState st;
     st.br.s = make_src(A.in + it.in_off, it.in_len);
@@ -2629,57 +2638,68 @@ __global__ void k_resolve_list(uint8_t* bytes, uint64_t n_bytes, const uint32_t*
     }
 }
 
-// ------------------------------------------------------- pipelined member decode
-// A large single-member stream decodes in waves of sub-chunks, each wave one
-// resident set of decoders. k_wave_chain checks a wave's anchored chain on the
-// device (pipeline.rs:758-809: each sub-chunk starts where the previous one
-// stopped) and lays out its output, so the wave's resolve, CRC pieces and copy
-// to the host are queued behind its inflate with no host round trip. Any
-// irregularity (a false start, a full slot, a member ending before the last
-// sub-chunk, a full output buffer) stops the pipeline at that wave: the kernel
-// leaves the state of the last good wave for the host, which decodes the rest
-// from there on the checked path.
-struct WaveState {         // carried from wave to wave on the device
+// ------------------------------------------------------- anchored chain on the device
+// Jobs whose sub-chunks were inflated speculatively in one launch get their
+// anchored chain checked on the device (pipeline.rs:758-809: each sub-chunk
+// starts where the previous one stopped) and their output laid out, so resolve
+// and the CRC pieces queue behind the inflate with no host round trip: the
+// waves of the pipelined host path (one job per launch, carried from wave to
+// wave), and the member route of a batch (every job at once). A job with any
+// irregularity (a false start, a full slot, a member ending before its last
+// sub-chunk, a full output range) is left empty for the host, which decodes it
+// again on the checked path.
+struct WaveState {         // per job, carried from wave to wave on the device
     uint64_t expected;     // body-relative bit where the next sub-chunk must start
-    uint64_t out_end;      // output bytes laid out so far
-    uint32_t live;         // 0 once a wave failed
+    uint64_t out_end;      // output bytes laid out so far (absolute)
+    uint32_t live;         // 0 once the job failed
     uint32_t pad;
 };
-struct WaveInfo {          // one wave's outcome, copied to the host
+struct WaveInfo {          // a job's outcome in one launch, read by the host
     uint64_t out_begin, out_len;
-    uint64_t trailer_byte; // body-relative trailer offset (last wave)
+    uint64_t trailer_byte; // body-relative trailer offset (when its last sub-chunk is here)
     uint32_t ok;
-    int32_t fail_item;     // index in the wave of the first failing sub-chunk
+    int32_t fail_item;     // index among the job's items of the first failing sub-chunk
     int32_t fail_status;
     uint32_t final_seen;
 };
+struct WaveJob {
+    uint32_t first, n;     // global item indices of this launch's part of the job
+    uint32_t last_item;    // global index of the job's last sub-chunk (~0u: in a later launch)
+    uint32_t piece_off, piece_cap;  // the job's region of CRC pieces
+    uint32_t n_all;        // items [first, first + n_all) belong to the job; those past n are unused
+    uint64_t out_cap;      // the job's output may not pass this byte
+    uint64_t member_start; // output byte where the job's member begins
+};
 struct WaveArgs {
-    const ChunkItem* items;    // all waves' items; this wave's are [first, first + n)
+    const ChunkItem* items;
     const ChunkResult* results;
-    uint32_t first, n;
-    uint32_t last_item;        // global index of the stream's last sub-chunk
-    WaveState* state;
-    WaveInfo* info;
-    uint32_t* live;            // gate of this wave's resolve and CRC launches
-    ResolveChunk* chunks;      // n entries
-    uint64_t* head_segs;       // n + 1
-    CrcPiece* pieces;          // this wave's region of piece_cap pieces
-    uint32_t piece_cap;
-    uint32_t* n_pieces;        // pieces laid out (0 when the wave failed)
-    uint64_t out_cap;
+    const WaveJob* jobs;
+    uint32_t n_jobs;
+    uint32_t item_base;        // chunks[] and head_segs[] are indexed by item - item_base
+    uint32_t n_items;          // items of this launch; head_segs has n_items + 1 entries
+    WaveState* state;          // per job
+    WaveInfo* info;            // per job (may be mapped host memory)
+    uint32_t* live;            // when set: 1 if job 0 passed
+    ResolveChunk* chunks;      // per item (unless direct)
+    uint64_t* head_segs;       // per item + 1 (unless direct): job-local, then global after k_wave_segs
+    CrcPiece* pieces;
+    uint32_t* n_pieces;        // per job: pieces laid out
+    uint64_t* seg_total;       // per job: head segments; k_wave_segs turns it into each job's offset
     const MemberRec* mbs;
-    const uint32_t* mb_count;
-    uint32_t* exp_crc;         // the member trailer (last wave)
+    const uint32_t* mb_count;  // records written (those past mb_cap were dropped)
+    uint32_t mb_cap;
+    uint32_t* exp_crc;         // per job: the member trailer
     uint32_t* exp_isize;
+    uint32_t direct;           // the items decoded straight to bytes: nothing to resolve
 };
 constexpr int WAVE_THREADS = 1024;
+constexpr uint64_t WAVE_PIECE = 256 * 1024;  // CRC piece bytes
 
 // n status words to (mapped) host memory, so the host learns them without a
 // copy queued behind the output copies.
 __global__ void k_copy_words(const uint32_t* src, uint32_t* dst, uint32_t n) {
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
 }
-constexpr uint64_t WAVE_PIECE = 256 * 1024;  // CRC piece bytes
 
 // Exclusive block-wide prefix of one value per thread; returns the total.
 __device__ __forceinline__ uint64_t block_scan(uint64_t v, uint64_t* sh, uint64_t* excl) {
@@ -2698,101 +2718,361 @@ __device__ __forceinline__ uint64_t block_scan(uint64_t v, uint64_t* sh, uint64_
     return total;
 }
 
+__device__ __forceinline__ uint64_t head_segs_of(uint64_t n) { return (res_head_end(n) + RES_HEAD_SEG - 1) / RES_HEAD_SEG; }
+
+// One block per job.
 __global__ void __launch_bounds__(WAVE_THREADS, 1) k_wave_chain(WaveArgs A) {
     __shared__ uint64_t sh[WAVE_THREADS];
-    __shared__ int32_t s_fail, s_status;
+    __shared__ int32_t s_fail;
+    __shared__ uint32_t s_found, s_crc, s_isize;
+    __shared__ uint64_t s_tb;
     const int t = threadIdx.x;
-    const WaveState S = *A.state;
-    if (t == 0) {
-        s_fail = S.live ? 0x7fffffff : -1;
-        s_status = 0;
-    }
-    __syncthreads();
-    // each thread checks a contiguous run of sub-chunks
-    const uint32_t per = (A.n + WAVE_THREADS - 1) / WAVE_THREADS;
-    const uint32_t b = t * per < A.n ? t * per : A.n, e = b + per < A.n ? b + per : A.n;
-    uint64_t cells = 0, segs = 0;
-    for (uint32_t q = b; q < e; q++) {
-        const uint32_t k = A.first + q;
-        const ChunkItem it = A.items[k];
-        const ChunkResult r = A.results[k];
-        const uint64_t expected = q == 0 ? S.expected : A.results[k - 1].actual_end_bit;
-        // a start on a stored block's zero header byte decodes as the true start
-        // in the same byte's first 6 bits, or right after an empty block
-        const uint64_t d = expected - it.start_bit;
-        const bool same = it.start_bit == expected ||
-                          ((it.flags & ITEM_STORED_START) && expected > it.start_bit &&
-                           (d <= 5 || ((it.flags & ITEM_EMPTY_STORED) && d == 40)));
-        const bool last = k == A.last_item;
-        bool ok = same && r.status == DS_OK;
-        ok = ok && (last ? (r.final_block && r.n_members == 1) : (!r.final_block && r.n_members == 0));
-        if (!ok) {
-            atomicMin(reinterpret_cast<unsigned int*>(&s_fail), q);
-            continue;
-        }
-        cells += r.n_cells;
-        segs += (res_head_end(r.n_cells) + RES_HEAD_SEG - 1) / RES_HEAD_SEG;
-    }
-    __syncthreads();
-    uint64_t c_ex, s_ex;
-    const uint64_t total = block_scan(cells, sh, &c_ex);
-    const uint64_t n_segs = block_scan(segs, sh, &s_ex);
-    const uint64_t out_begin = S.out_end, out_len = total;
-    const uint32_t np = (uint32_t)((out_len + WAVE_PIECE - 1) / WAVE_PIECE);
-    if (t == 0 && s_fail == 0x7fffffff && (out_begin + out_len > A.out_cap || np > A.piece_cap)) s_fail = (int32_t)A.n;
-    __syncthreads();
-    if (s_fail != 0x7fffffff) {  // uniform: this wave and every later one do nothing
+    for (uint32_t jb = blockIdx.x; jb < A.n_jobs; jb += gridDim.x) {
+        const WaveJob J = A.jobs[jb];
+        const WaveState S = A.state[jb];
+        const bool has_last = J.n && J.first + J.n - 1 == J.last_item;
+        __syncthreads();  // the previous job's readers of the shared words are done
         if (t == 0) {
-            if (s_fail >= 0 && s_fail < (int32_t)A.n) s_status = A.results[A.first + s_fail].status;
-            A.state->live = 0;
-            *A.live = 0;
-            *A.n_pieces = 0;
-            A.info->ok = 0;
-            A.info->fail_item = s_fail;
-            A.info->fail_status = s_status;
-            A.info->out_begin = out_begin;
-            A.info->out_len = 0;
+            s_fail = S.live ? 0x7fffffff : -1;
+            s_found = 0;
         }
-        return;
-    }
-    for (uint32_t q = b; q < e; q++) {
-        const uint32_t k = A.first + q;
-        const uint64_t n = A.results[k].n_cells;
-        A.chunks[q] = ResolveChunk{out_begin + c_ex, A.items[k].out_off, n, 0, out_begin};
-        A.head_segs[q] = s_ex;
-        c_ex += n;
-        s_ex += (res_head_end(n) + RES_HEAD_SEG - 1) / RES_HEAD_SEG;
-    }
-    for (uint32_t p = t; p < A.piece_cap; p += WAVE_THREADS) {
-        const uint64_t o = (uint64_t)p * WAVE_PIECE;
-        A.pieces[p] = p < np ? CrcPiece{out_begin + o, out_len - o < WAVE_PIECE ? out_len - o : WAVE_PIECE}
-                             : CrcPiece{out_begin + out_len, 0};
-    }
-    const uint32_t lastq = A.n - 1;
-    const bool has_last = A.first + lastq == A.last_item;
-    uint64_t tb = 0;
-    if (t == 0) {
-        A.head_segs[A.n] = n_segs;
-        *A.n_pieces = A.piece_cap;
-        if (has_last) {  // the trailer of the stream's only member
-            const uint32_t id = A.items[A.last_item].id, nm = *A.mb_count;
-            for (uint32_t i = 0; i < nm; i++)
+        __syncthreads();
+        // each thread checks a contiguous run of sub-chunks
+        const uint32_t per = (J.n + WAVE_THREADS - 1) / WAVE_THREADS;
+        const uint32_t b = t * per < J.n ? t * per : J.n, e = b + per < J.n ? b + per : J.n;
+        uint64_t cells = 0, segs = 0;
+        for (uint32_t q = b; q < e; q++) {
+            const uint32_t k = J.first + q;
+            const ChunkItem it = A.items[k];
+            const ChunkResult r = A.results[k];
+            const uint64_t expected = q == 0 ? S.expected : A.results[k - 1].actual_end_bit;
+            // a start on a stored block's zero header byte decodes as the true start
+            // in the same byte's first 6 bits, or right after an empty block
+            const uint64_t d = expected - it.start_bit;
+            const bool same = it.start_bit == expected ||
+                              ((it.flags & ITEM_STORED_START) && expected > it.start_bit &&
+                               (d <= 5 || ((it.flags & ITEM_EMPTY_STORED) && d == 40)));
+            const bool last = k == J.last_item;
+            bool ok = same && r.status == DS_OK;
+            ok = ok && (last ? (r.final_block && r.n_members == 1) : (!r.final_block && r.n_members == 0));
+            if (!ok) {
+                atomicMin(reinterpret_cast<unsigned int*>(&s_fail), q);
+                continue;
+            }
+            cells += r.n_cells;
+            segs += A.direct ? 0 : head_segs_of(r.n_cells);
+        }
+        // the trailer of the job's only member, from the record of its last sub-chunk
+        if (has_last) {
+            const uint32_t id = A.items[J.last_item].id, nm = *A.mb_count < A.mb_cap ? *A.mb_count : A.mb_cap;
+            for (uint32_t i = t; i < nm; i += WAVE_THREADS)
                 if (A.mbs[i].item == id) {
-                    *A.exp_crc = A.mbs[i].crc;
-                    *A.exp_isize = A.mbs[i].isize;
-                    tb = A.mbs[i].trailer_byte;
+                    s_crc = A.mbs[i].crc;
+                    s_isize = A.mbs[i].isize;
+                    s_tb = A.mbs[i].trailer_byte;
+                    s_found = 1;
                 }
         }
-        A.state->expected = A.results[A.first + lastq].actual_end_bit;
-        A.state->out_end = out_begin + out_len;
-        *A.live = 1;
-        A.info->ok = 1;
-        A.info->fail_item = -1;
-        A.info->fail_status = 0;
-        A.info->out_begin = out_begin;
-        A.info->out_len = out_len;
-        A.info->trailer_byte = tb;
-        A.info->final_seen = has_last ? 1u : 0u;
+        __syncthreads();
+        uint64_t c_ex, s_ex;
+        const uint64_t total = block_scan(cells, sh, &c_ex);
+        const uint64_t n_segs = block_scan(segs, sh, &s_ex);
+        const uint64_t out_begin = S.out_end, out_len = total;
+        const uint32_t np = (uint32_t)((out_len + WAVE_PIECE - 1) / WAVE_PIECE);
+        if (t == 0 && s_fail == 0x7fffffff &&
+            (out_begin + out_len > J.out_cap || np > J.piece_cap || (has_last && !s_found)))
+            s_fail = (int32_t)J.n;
+        __syncthreads();
+        const bool failed = s_fail != 0x7fffffff;  // uniform
+        // a failed job's sub-chunks are laid out empty, so resolve and the CRC
+        // pieces do nothing for it; so are the unused ones past n
+        if (!A.direct) {
+            const uint32_t pa = (J.n_all + WAVE_THREADS - 1) / WAVE_THREADS;
+            const uint32_t ua = t * pa < J.n_all ? t * pa : J.n_all, va = ua + pa < J.n_all ? ua + pa : J.n_all;
+            const uint64_t empty_at = failed ? out_begin : out_begin + out_len;
+            for (uint32_t q = ua; q < va; q++) {
+                const uint32_t k = J.first + q;
+                if (q < J.n && !failed) continue;  // written below
+                A.chunks[k - A.item_base] = ResolveChunk{empty_at, A.items[k].out_off, 0, J.member_start, out_begin};
+                A.head_segs[k - A.item_base] = failed ? 0 : n_segs;
+            }
+            for (uint32_t q = b; q < e && !failed; q++) {
+                const uint32_t k = J.first + q;
+                const uint64_t n = A.results[k].n_cells;
+                A.chunks[k - A.item_base] =
+                    ResolveChunk{out_begin + c_ex, A.items[k].out_off, n, J.member_start, out_begin};
+                A.head_segs[k - A.item_base] = s_ex;
+                c_ex += n;
+                s_ex += head_segs_of(n);
+            }
+        }
+        for (uint32_t p = t; p < J.piece_cap; p += WAVE_THREADS) {
+            const uint64_t o = (uint64_t)p * WAVE_PIECE;
+            A.pieces[J.piece_off + p] =
+                (!failed && p < np) ? CrcPiece{out_begin + o, out_len - o < WAVE_PIECE ? out_len - o : WAVE_PIECE}
+                                    : CrcPiece{out_begin, 0};
+        }
+        if (t == 0) {
+            A.seg_total[jb] = failed ? 0 : n_segs;
+            A.n_pieces[jb] = failed ? 0 : J.piece_cap;
+            if (A.n_jobs == 1 && !A.direct) A.head_segs[A.n_items] = failed ? 0 : n_segs;
+            WaveInfo& I = A.info[jb];
+            I.out_begin = out_begin;
+            if (failed) {
+                int32_t st = 0;
+                if (s_fail >= 0 && s_fail < (int32_t)J.n) st = A.results[J.first + s_fail].status;
+                A.state[jb].live = 0;
+                if (A.live) *A.live = 0;
+                I.ok = 0;
+                I.fail_item = s_fail;
+                I.fail_status = st;
+                I.out_len = 0;
+                I.final_seen = 0;
+                I.trailer_byte = 0;
+            } else {
+                if (has_last) {
+                    A.exp_crc[jb] = s_crc;
+                    A.exp_isize[jb] = s_isize;
+                }
+                if (J.n) A.state[jb].expected = A.results[J.first + J.n - 1].actual_end_bit;
+                A.state[jb].out_end = out_begin + out_len;
+                if (A.live) *A.live = 1;
+                I.ok = 1;
+                I.fail_item = -1;
+                I.fail_status = 0;
+                I.out_len = out_len;
+                I.trailer_byte = has_last ? s_tb : 0;
+                I.final_seen = has_last ? 1u : 0u;
+            }
+        }
+    }
+}
+
+// Several jobs in one launch: each job's head-segment offset (one block), then
+// added to the job's items (one block per job).
+__global__ void __launch_bounds__(WAVE_THREADS) k_wave_segs(WaveArgs A) {
+    __shared__ uint64_t sh[WAVE_THREADS];
+    __shared__ uint64_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (uint32_t j0 = 0; j0 < A.n_jobs; j0 += WAVE_THREADS) {
+        const uint32_t j = j0 + threadIdx.x;
+        uint64_t ex;
+        const uint64_t tot = block_scan(j < A.n_jobs ? A.seg_total[j] : 0, sh, &ex);
+        if (j < A.n_jobs) A.seg_total[j] = carry + ex;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) A.head_segs[A.n_items] = carry;
+}
+__global__ void k_wave_segs_add(WaveArgs A) {
+    for (uint32_t j = blockIdx.x; j < A.n_jobs; j += gridDim.x) {
+        const WaveJob J = A.jobs[j];
+        const uint64_t o = A.seg_total[j];
+        for (uint32_t q = threadIdx.x; q < J.n_all; q += blockDim.x) A.head_segs[J.first + q - A.item_base] += o;
+    }
+}
+
+// ------------------------------------------------------- device-planned batch
+// The member route of a batch with every hand-off on the device, so the whole
+// decode is one captured graph: the boundary scan's verified starts pick each
+// job's sub-chunk starts (the verified start nearest each ideal position,
+// pipeline.rs:492-505 with the scan's starts), then the sub-chunk list with
+// end hints and slot sizes is built, inflated, chain-checked, resolved and
+// CRC-checked without the host.
+struct BatchJob {
+    uint64_t in_off;       // the body's first byte in the input buffer
+    uint64_t blen;         // body bytes
+    uint64_t scan_bit;     // the body's first bit relative to the scan base
+    uint64_t arena;        // the job's first cell in the slot arena
+    double expand;         // cells reserved per compressed byte
+    uint64_t dst_off, dst_cap;
+    uint32_t K;            // sub-chunks planned (ideal positions nbits*k/K, k >= 1)
+    uint32_t item_first;
+    uint32_t piece_off, piece_cap;
+};
+struct BatchArgs {
+    const BatchJob* jobs;
+    uint32_t n_jobs;
+    const uint64_t* big_bit;   // scan_bit of the jobs with K > 1, ascending
+    const uint32_t* big_job;   // their job indices
+    uint32_t n_big;
+    const uint64_t* surv;      // scan survivors and their verification flags
+    const uint8_t* vflag;
+    const uint32_t* counts;    // [1] survivors, [3] stored-block starts
+    uint32_t cap2, cap3;
+    const uint64_t* stored;    // stored-block starts (bit 0: an empty block)
+    unsigned long long* keys;  // per item: (distance << 4 | below << 3 | kind) of the best start, ~0 none
+    ChunkItem* items;
+    WaveJob* wjobs;
+};
+
+__device__ __forceinline__ uint64_t batch_ideal(uint64_t nbits, uint32_t k, uint32_t K) { return nbits * k / K; }
+
+// One thread per verified start (dynamic-block survivors, then stored-block
+// starts): the two ideal positions around it take it if it is the nearest.
+// kind: 1 a stored-block start, 3 an empty stored block.
+__global__ void k_batch_select(BatchArgs A) {
+    const uint32_t ns = A.counts[1] < A.cap2 ? A.counts[1] : A.cap2;
+    const uint32_t nst = A.counts[3] < A.cap3 ? A.counts[3] : A.cap3;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ns + nst; i += gridDim.x * blockDim.x) {
+        uint64_t v;
+        uint32_t kind = 0;
+        if (i < ns) {
+            if (!A.vflag[i]) continue;
+            v = A.surv[i];
+        } else {
+            const uint64_t x = A.stored[i - ns];
+            v = x & ~1ull;
+            kind = (x & 1) ? 3u : 1u;
+        }
+        // the job whose body holds v: the last big job starting at or before it
+        uint32_t lo = 0, hi = A.n_big;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (A.big_bit[mid] <= v) lo = mid + 1;
+            else hi = mid;
+        }
+        if (lo == 0) continue;
+        const BatchJob J = A.jobs[A.big_job[lo - 1]];
+        const uint64_t rel = v - J.scan_bit, nbits = J.blen * 8;
+        if (rel == 0 || rel >= nbits) continue;
+        uint32_t k = (uint32_t)(rel * J.K / nbits);  // rel < 2^36, K < 2^24
+        while (k + 1 < J.K && batch_ideal(nbits, k + 1, J.K) <= rel) k++;
+        while (k > 0 && batch_ideal(nbits, k, J.K) > rel) k--;
+        if (k >= 1) {  // above ideal k
+            const uint64_t d = rel - batch_ideal(nbits, k, J.K);
+            atomicMin(A.keys + J.item_first + k, (unsigned long long)((d << 4) | kind));
+        }
+        if (k + 1 < J.K) {  // below ideal k + 1
+            const uint64_t d = batch_ideal(nbits, k + 1, J.K) - rel;
+            atomicMin(A.keys + J.item_first + k + 1, (unsigned long long)((d << 4) | 8u | kind));
+        }
+    }
+}
+
+// One block per job: the chosen starts in order (repeats dropped), their end
+// hints, slot sizes and offsets; unused items at the job's end are skipped.
+__global__ void __launch_bounds__(WAVE_THREADS) k_batch_items(BatchArgs A) {
+    __shared__ uint64_t sh[WAVE_THREADS];
+    __shared__ uint64_t s_start[WAVE_THREADS + 1];
+    __shared__ uint32_t s_kind[WAVE_THREADS];
+    __shared__ uint64_t s_base, s_np;
+    const int t = threadIdx.x;
+    for (uint32_t jb = blockIdx.x; jb < A.n_jobs; jb += gridDim.x) {
+        const BatchJob J = A.jobs[jb];
+        const uint64_t nbits = J.blen * 8;
+        __syncthreads();
+        if (t == 0) {
+            s_base = 0;  // cells used so far
+            s_np = 0;    // items written so far
+        }
+        __syncthreads();
+        // the job's items WAVE_THREADS at a time; the start of a tile's first
+        // item after the previous tile is carried in s_start[WAVE_THREADS]
+        for (uint32_t q0 = 0; q0 < J.K; q0 += WAVE_THREADS) {
+            const uint32_t q = q0 + t;
+            uint64_t st = ~0ull;
+            uint32_t kind = 0;
+            if (q < J.K) {
+                if (q == 0) {
+                    st = 0;
+                } else {
+                    const unsigned long long key = A.keys[J.item_first + q];
+                    if (key != ~0ull) {
+                        const uint64_t d = key >> 4, x = batch_ideal(nbits, q, J.K);
+                        st = (key & 8u) ? x - d : x + d;
+                        kind = (uint32_t)(key & 7u);
+                        // the same start as the previous item's choice: dropped
+                        const unsigned long long pk = A.keys[J.item_first + q - 1];
+                        if (q > 1 && pk != ~0ull) {
+                            const uint64_t px = batch_ideal(nbits, q - 1, J.K);
+                            if (((pk & 8u) ? px - (pk >> 4) : px + (pk >> 4)) == st) st = ~0ull;
+                        }
+                    }
+                }
+            }
+            uint64_t ex;
+            const uint64_t n_here = block_scan(st != ~0ull ? 1 : 0, sh, &ex);
+            // compact the present starts of this tile into s_start
+            if (st != ~0ull) {
+                s_start[ex] = st;
+                s_kind[ex] = kind;
+            }
+            __syncthreads();
+            // the next present start after the tile: the first of the next tile,
+            // found by the next iteration; so write items one tile late, except
+            // the last present one of the job, which needs the following tile
+            // first. Simpler: defer each item until its successor is known.
+            const uint64_t np0 = s_np;
+            // items np0 .. np0 + n_here - 1 get their starts; the item before
+            // them (np0 - 1, held back) now learns its end hint
+            uint64_t cap = 0;
+            if ((uint64_t)t < n_here) {
+                const uint64_t my = s_start[t];
+                const uint64_t next = (uint64_t)t + 1 < n_here ? s_start[t + 1] : ~0ull;
+                ChunkItem it;
+                it.in_off = J.in_off;
+                it.in_len = J.blen;
+                it.start_bit = my;
+                it.end_hint = next;  // ~0: fixed below once the next tile is seen
+                const uint64_t span = ((next == ~0ull ? nbits : next) - my + 7) / 8;
+                cap = ((uint64_t)((double)span * J.expand) + 65536 + 7) & ~7ull;
+                it.out_cap = cap;
+                it.out_off = 0;
+                it.flags = ITEM_MARKERS | (s_kind[t] == 1 ? ITEM_STORED_START
+                                            : s_kind[t] == 3 ? (ITEM_STORED_START | ITEM_EMPTY_STORED) : 0u);
+                it.id = J.item_first + (uint32_t)(np0 + t);
+                A.items[J.item_first + np0 + t] = it;
+            }
+            __syncthreads();
+            // the held-back last item of the previous tile ends where this tile's first begins
+            if (t == 0 && np0 > 0 && n_here > 0) {
+                ChunkItem& pv = A.items[J.item_first + np0 - 1];
+                pv.end_hint = s_start[0];
+                const uint64_t span = (s_start[0] - pv.start_bit + 7) / 8;
+                pv.out_cap = ((uint64_t)((double)span * J.expand) + 65536 + 7) & ~7ull;
+            }
+            __syncthreads();
+            if (t == 0) s_np = np0 + n_here;
+            __syncthreads();
+        }
+        // slot offsets: a prefix of the caps over the job's present items
+        const uint64_t np = s_np;
+        for (uint64_t p0 = 0; p0 < np; p0 += WAVE_THREADS) {
+            const uint64_t p = p0 + t;
+            const uint64_t cap = p < np ? A.items[J.item_first + p].out_cap : 0;
+            uint64_t ex;
+            const uint64_t tot = block_scan(cap, sh, &ex);
+            if (p < np) A.items[J.item_first + p].out_off = J.arena + s_base + ex;
+            __syncthreads();
+            if (t == 0) s_base += tot;
+            __syncthreads();
+        }
+        for (uint32_t q = (uint32_t)np + t; q < J.K; q += WAVE_THREADS) {
+            ChunkItem it{};
+            it.in_off = J.in_off;
+            it.in_len = J.blen;
+            it.start_bit = nbits;
+            it.end_hint = ~0ull;
+            it.out_off = J.arena;
+            it.flags = ITEM_SKIP;
+            it.id = J.item_first + q;
+            A.items[J.item_first + q] = it;
+        }
+        if (t == 0) {
+            WaveJob W;
+            W.first = J.item_first;
+            W.n = (uint32_t)np;
+            W.last_item = J.item_first + (uint32_t)np - 1;
+            W.piece_off = J.piece_off;
+            W.piece_cap = J.piece_cap;
+            W.n_all = J.K;
+            W.out_cap = J.dst_off + J.dst_cap;
+            W.member_start = J.dst_off;
+            A.wjobs[jb] = W;
+        }
     }
 }
 

@@ -45,6 +45,10 @@ def dev(data, out_n):
 small = [(r, g, c) for r, g, c in batch_items() if len(g) < 100_000]
 b = Decoder(Config(device=-1, hbm_budget_bytes=1), lib=lib)  # several waves
 run_batch(b, small, dev)
+# one wave through the device-planned route, split files included
+b = Decoder(Config(device=-1, gpu_chunk_bytes=16384), lib=lib)
+outs, lens, status = run_batch(b, batch_items(), dev)
+assert status[:4] == [0, 0, 0, 0] and outs[0] == batch_items()[0][0]
 s = Decoder(Config(device=-1, hbm_budget_bytes=4 << 20), lib=lib)
 s.serve_start(engines=2, max_ready=2)
 got = run_serving(s, serve_requests(1, seed=5, hi=16 << 10), seed=3, gap_s=0.0)

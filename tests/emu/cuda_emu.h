@@ -304,6 +304,12 @@ inline unsigned atomicMin(unsigned* p, unsigned v) {
     }
     return cur;
 }
+inline unsigned long long atomicMin(unsigned long long* p, unsigned long long v) {
+    unsigned long long cur = __atomic_load_n(p, __ATOMIC_SEQ_CST);
+    while (v < cur && !__atomic_compare_exchange_n(p, &cur, v, false, __ATOMIC_SEQ_CST, __ATOMIC_SEQ_CST)) {
+    }
+    return cur;
+}
 inline unsigned atomicCAS(unsigned* p, unsigned cmp, unsigned v) {
     __atomic_compare_exchange_n(p, &cmp, v, false, __ATOMIC_SEQ_CST, __ATOMIC_SEQ_CST);
     return cmp;

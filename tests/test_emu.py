@@ -169,9 +169,12 @@ def expected_status(gz):
         return e.code
 
 
+@pytest.mark.parametrize("plan", [0, -1], ids=["device-planned", "host-planned"])
 @pytest.mark.parametrize("budget", [0, 1], ids=["one-wave", "waves"])
-def test_batch_mixed(emu_decoder_factory, budget):
-    """budget 1: the smallest wave size, so the files go through several waves."""
+def test_batch_mixed(emu_decoder_factory, budget, plan):
+    """budget 1: the smallest wave size, so the files go through several waves.
+    The device-planned route hands the two-member file and the one whose
+    destination is too small back to the checked route."""
     items = batch_items()
     keep = []
 
@@ -181,7 +184,7 @@ def test_batch_mixed(emu_decoder_factory, budget):
         keep.extend([a, o])
         return haddr(a), haddr(o), lambda: o.tobytes()
 
-    d = emu_decoder_factory(hbm_budget_bytes=budget)
+    d = emu_decoder_factory(hbm_budget_bytes=budget, batch_plan=plan)
     outs, lens, status = run_batch(d, items, dev)
     for (raw, gz, cap), got, n, stt in zip(items, outs, lens, status):
         want = expected_status(gz)
@@ -191,6 +194,44 @@ def test_batch_mixed(emu_decoder_factory, budget):
             assert stt == want
             if want == 0:
                 assert got == raw
+
+
+def test_batch_device_planned_routes(emu_decoder_factory):
+    """The device-planned batch: files split into sub-chunks at verified starts
+    picked on the device (Zipf text), a file with no dynamic-block start
+    (fixed-Huffman blocks only: every sub-chunk after the first is unused and
+    the first decodes it all), and a batch of small files only, which decode
+    straight to their bytes."""
+    keep = []
+
+    def run(pairs, **kw):
+        blobs = [g for _, g in pairs]
+        caps = [len(r) for r, _ in pairs]
+        offs = np.cumsum([0] + [len(b) for b in blobs])[:-1].tolist()
+        ooffs = np.cumsum([0] + caps)[:-1].tolist()
+        a = np.frombuffer(b"".join(blobs), dtype=np.uint8).copy()
+        o = np.zeros(sum(caps) + 64, dtype=np.uint8)
+        keep.extend([a, o])
+        d = emu_decoder_factory(**kw)
+        lens, status, st = d.decode_batch(haddr(a), offs, [len(b) for b in blobs], haddr(o), ooffs, caps)
+        out = o.tobytes()
+        return [out[x:x + n] for x, n in zip(ooffs, lens)], status, st
+
+    zipf_raw, zipf = W.config0(200_000, seed=11)
+    fixed_raw = W.config0(120_000, seed=12)[0]
+    co = zlib.compressobj(6, zlib.DEFLATED, -15, 9, zlib.Z_FIXED)
+    body = co.compress(fixed_raw) + co.flush()
+    fixed = (b"\x1f\x8b\x08\x00\x00\x00\x00\x00\x00\xff" + body +
+             struct.pack("<II", zlib.crc32(fixed_raw), len(fixed_raw)))
+    small = [(b"small %d " % i * (40 + 9 * i), None) for i in range(12)]
+    small = [(r, gzip_cli(r)) for r, _ in small]
+    pairs = [(zipf_raw, zipf), (fixed_raw, fixed)] + small[:3]
+    outs, status, st = run(pairs, gpu_chunk_bytes=16384)
+    assert status == [0] * len(pairs) and outs == [r for r, _ in pairs]
+    assert st.gpu_chunks > len(pairs) + 4 and st.members == len(pairs)
+    outs, status, st = run(small)
+    assert status == [0] * len(small) and outs == [r for r, _ in small]
+    assert st.markers == 0 and st.gpu_chunks == len(small)
 
 
 def test_autotune(emu_decoder_factory):

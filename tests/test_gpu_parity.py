@@ -339,11 +339,13 @@ def test_bgzf_device_walk(gpu_decoder_factory, case):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("plan", [0, -1], ids=["device-planned", "host-planned"])
 @pytest.mark.parametrize("budget", [0, 1], ids=["one-wave", "waves"])
-def test_batch_mixed(gpu_decoder_factory, budget):
+def test_batch_mixed(gpu_decoder_factory, budget, plan):
     """A batch mixing multi-chunk, single-chunk, multi-member and BGZF files, a
     corrupt file and a too-small output range; per-item status and bytes against
-    the oracle, in one wave and in several."""
+    the oracle, in one wave and in several, on the device-planned route (whose
+    unfinished jobs go the checked route) and on the host-planned one."""
     import torch
     from test_emu import batch_items, expected_status, run_batch
 
@@ -353,7 +355,7 @@ def test_batch_mixed(gpu_decoder_factory, budget):
         return din, dout, lambda: dout.cpu().numpy().tobytes()
 
     items = batch_items()
-    d = gpu_decoder_factory(hbm_budget_bytes=budget)
+    d = gpu_decoder_factory(hbm_budget_bytes=budget, batch_plan=plan)
     outs, lens, status = run_batch(d, items, devbuf)
     for (raw, gz, cap), got, n, stt in zip(items, outs, lens, status):
         want = expected_status(gz)
@@ -363,6 +365,38 @@ def test_batch_mixed(gpu_decoder_factory, budget):
             assert stt == want
             if want == 0:
                 assert got == raw
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("chunk", [0, 65536], ids=["auto-spacing", "64KiB"])
+def test_batch_graph_replay(gpu_decoder_factory, chunk):
+    """A batch of single-member files of uneven size on the device-planned
+    route: the first call captures its graph, the second replays it into a
+    zeroed output and every file's bytes come back again; the host-planned
+    route decodes the same bytes."""
+    import torch
+    files = W.config3_files(n_files=40, seed=21, lo=4 << 10, hi=6 << 20)
+    blobs = [gz for _, gz in files]
+    raws = [r for r, _ in files]
+    offs = np.cumsum([0] + [len(b) for b in blobs])[:-1].tolist()
+    ooffs = np.cumsum([0] + [len(r) for r in raws])[:-1].tolist()
+    din = dev(b"".join(blobs))
+    dout = torch.zeros(sum(len(r) for r in raws) + 16, dtype=torch.uint8, device="cuda")
+    d = gpu_decoder_factory(gpu_chunk_bytes=chunk)
+    for call in range(2):
+        dout.zero_()
+        lens, status, st = d.decode_batch(din, offs, [len(b) for b in blobs], dout, ooffs, [len(r) for r in raws])
+        assert status == [0] * len(files) and lens == [len(r) for r in raws]
+        assert st.graph_launches == 1 and st.members == len(files)
+        host = dout.cpu().numpy().tobytes()
+        for r, o in zip(raws, ooffs):
+            assert host[o:o + len(r)] == r
+    assert st.gpu_chunks > len(files)  # the larger files were split
+    h = gpu_decoder_factory(gpu_chunk_bytes=chunk, batch_plan=-1)
+    dout.zero_()
+    lens, status, st = h.decode_batch(din, offs, [len(b) for b in blobs], dout, ooffs, [len(r) for r in raws])
+    assert status == [0] * len(files) and st.graph_launches == 0
+    assert dout.cpu().numpy().tobytes()[:sum(len(r) for r in raws)] == b"".join(raws)
 
 
 @pytest.mark.gpu
