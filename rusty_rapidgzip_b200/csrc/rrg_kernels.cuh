@@ -2562,23 +2562,26 @@ __global__ void __launch_bounds__(RES_THREADS, 4) k_res_heads(ResolveArgs A) {
         // markers of this chunk may name positions [out_start - lim, out_start)
         const uint64_t lim = ck.out_start - ck.member_start;
         // stage the 32 KiB before the chunk: whole aligned 16-byte words inside
-        // [w_lo, out_start), bytes at the edges; win[i] holds output byte wa + i
+        // [w_lo, out_start), bytes at the edges; win[i] holds the byte at
+        // address a_lo + i (addresses, not offsets from A.out: the aligned start
+        // may lie before A.out itself when the window starts at the output's
+        // first byte)
         const uint64_t w_lo = ck.out_start > WINDOW ? ck.out_start - WINDOW : 0;
-        const uintptr_t a_lo = (uintptr_t)(A.out + w_lo) & ~(uintptr_t)15;
-        const uint64_t wa = (uint64_t)(a_lo - (uintptr_t)A.out);  // may sit up to 15 bytes before w_lo
+        const uintptr_t lo_addr = (uintptr_t)(A.out + w_lo), end_addr = (uintptr_t)(A.out + ck.out_start);
+        const uintptr_t a_lo = lo_addr & ~(uintptr_t)15;  // up to 15 bytes before lo_addr
         __syncthreads();  // the previous segment's readers are done with win
         for (uint64_t q = threadIdx.x; 16 * q < WINDOW + 16; q += blockDim.x) {
-            const uint64_t p = wa + 16 * q;  // relative to A.out, p + 16 > w_lo
-            if (p >= ck.out_start) break;
-            if (p >= w_lo && p + 16 <= ck.out_start) {
-                *reinterpret_cast<uint4*>(win + 16 * q) = *reinterpret_cast<const uint4*>(A.out + p);
+            const uintptr_t p = a_lo + 16 * q;  // p + 16 > lo_addr
+            if (p >= end_addr) break;
+            if (p >= lo_addr && p + 16 <= end_addr) {
+                *reinterpret_cast<uint4*>(win + 16 * q) = *reinterpret_cast<const uint4*>(p);
             } else {
                 for (int b = 0; b < 16; b++)
-                    if (p + b >= w_lo && p + b < ck.out_start) win[16 * q + b] = A.out[p + b];
+                    if (p + b >= lo_addr && p + b < end_addr) win[16 * q + b] = *reinterpret_cast<const uint8_t*>(p + b);
             }
         }
         __syncthreads();
-        const uint64_t wbase = ck.out_start - 1 - wa;  // win index of the byte before the chunk
+        const uint64_t wbase = (uint64_t)(end_addr - 1 - a_lo);  // win index of the byte before the chunk
         const uint16_t* cells = A.cells + ck.slot_off;
         constexpr uint64_t STEP = RES_THREADS * RES_CELLS;
         // the next step's cells are loaded before this step's are processed

@@ -401,7 +401,10 @@ inline cudaError_t cudaGetDevice(int* d) {
 }
 inline cudaError_t cudaSetDevice(int) { return cudaSuccess; }
 inline cudaError_t cudaDeviceGetAttribute(int* v, cudaDeviceAttr a, int) {
-    *v = a == cudaDevAttrMultiProcessorCount ? 2 : 232448;
+    // RRG_EMU_SMS: the SM count to report (default 2), so the CPU build can
+    // lay out work as a full-size device would
+    static const int sms = getenv("RRG_EMU_SMS") ? atoi(getenv("RRG_EMU_SMS")) : 2;
+    *v = a == cudaDevAttrMultiProcessorCount ? sms : 232448;
     return cudaSuccess;
 }
 template <class F>

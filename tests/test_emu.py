@@ -557,6 +557,22 @@ def test_resolve_long_chunks_and_unaligned_output(emu_decoder_factory):
         assert (dst[:shift] == 0xA5).all() and (dst[shift + n:] == 0xA5).all()
 
 
+def test_resolve_window_at_an_unaligned_output_start(emu_decoder_factory):
+    """Sub-chunks shorter than the window: the second one's 32 KiB window
+    begins at the output's first byte, whose 16-byte-aligned word lies before
+    the output when it starts at an odd address. Every staged word must still
+    be read (a start before the buffer once skipped a thread's words)."""
+    raw, gz = W.config0(90_000, seed=23)
+    d = emu_decoder_factory(gpu_chunk_bytes=8 << 10)
+    src = np.frombuffer(gz, dtype=np.uint8).copy()
+    for shift in (0, 1, 7, 8, 9, 15):
+        dst = np.full(len(raw) + 32, 0xA5, dtype=np.uint8)
+        n, st = d.decode_device(haddr(src), len(gz), haddr(dst) + shift, len(raw))
+        assert n == len(raw) and dst[shift:shift + n].tobytes() == raw, shift
+        assert st.gpu_chunks >= 2 and st.markers > 0
+        assert (dst[:shift] == 0xA5).all() and (dst[shift + n:] == 0xA5).all()
+
+
 def test_pipelined_host_path(emu_decoder_factory):
     """A member stream large enough for several waves takes the pipelined host
     path: its output equals the generator's and the checked path's, the sink
