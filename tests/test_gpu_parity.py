@@ -93,6 +93,23 @@ def test_device_resident_matches_host(gpu_decoder_factory):
     assert e.value.required == len(raw)
 
 
+def test_resolve_window_at_an_unaligned_output_start(gpu_decoder_factory):
+    """Short sub-chunks into outputs at every alignment: the second sub-chunk's
+    window begins at the output's first byte, whose aligned 16-byte word lies
+    before the output."""
+    import torch
+    raw, gz = W.config0(90_000, seed=23)
+    d = gpu_decoder_factory(gpu_chunk_bytes=8 << 10)
+    din = dev(gz)
+    for shift in range(16):
+        dout = torch.full((len(raw) + 32,), 0xA5, dtype=torch.uint8, device="cuda")
+        n, st = d.decode_device(din, len(gz), dout[shift:], len(raw))
+        host = dout.cpu().numpy()
+        assert n == len(raw) and host[shift:shift + n].tobytes() == raw, shift
+        assert (host[:shift] == 0xA5).all() and (host[shift + n:] == 0xA5).all()
+        assert st.gpu_chunks >= 2 and st.markers > 0
+
+
 def test_block_finder_parity(gpu_decoder_factory):
     raw, gz = W.config0(4 << 20, seed=9)
     body = gz[10:]
