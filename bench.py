@@ -610,16 +610,18 @@ def run_files(args):
         U_all = int(uu.item())
     value = U_all * args.steps / t / 1e9
     # ---- plain path: one device-resident decode per file, same buffers
-    torch.cuda.synchronize()
-    p0 = torch.cuda.Event(enable_timing=True)
-    p1 = torch.cuda.Event(enable_timing=True)
-    p0.record(stream)
-    for o, n, io, il in zip(out_off, lens, in_off, in_len):
-        m, _ = dec.decode_device(din[io:], il, dout[o:], n, stream=stream.cuda_stream)
-        assert m == n
-    p1.record(stream)
-    torch.cuda.synchronize()
-    plain = U_ / (p0.elapsed_time(p1) / 1000.0) / 1e9
+    plain = None
+    if not args.no_plain:
+        torch.cuda.synchronize()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for o, n, io, il in zip(out_off, lens, in_off, in_len):
+            m, _ = dec.decode_device(din[io:], il, dout[o:], n, stream=stream.cuda_stream)
+            assert m == n
+        p1.record(stream)
+        torch.cuda.synchronize()
+        plain = round(U_ / (p0.elapsed_time(p1) / 1000.0) / 1e9, 3)
     # ---- end to end: pinned host input -> batch -> pinned host output, every step
     e2e = None
     try:
@@ -665,7 +667,7 @@ def run_files(args):
                        "files": n_files_all, "uncompressed_bytes": U_all, "rank0_files": n_files,
                        "rank0_compressed_bytes": C_,
                        "parallelism": f"file shards x{world} (byte-balanced)", "l2": "inputs larger than L2; no flush",
-                       "plain_per_file_gbs": round(plain, 3), "autotuned": tuning,
+                       "plain_per_file_gbs": plain, "autotuned": tuning,
                        "gpu_chunks": st.gpu_chunks, "generation_s": round(t_gen, 1)},
             "e2e": e2e, "gpu_launches": int(launches), "kernels_ms": kern,
             "clocks": clk.summary(), "cpu_baseline": cpu,
@@ -745,6 +747,7 @@ def main():
     ap.add_argument("--warps-per-stream", type=int, default=0, help="-1: one decoder per lane")
     ap.add_argument("--boundary-mode", type=int, default=0, help="1: one finder search per target")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="files: leave out the plain per-file comparison arm")
     ap.add_argument("--stripe", type=int, default=0, help="stream: compressed bytes per stripe (0: 256 MiB)")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -3095,8 +3095,10 @@ int batch_enqueue(rrg_ctx* c, const uint8_t* d_in, uint8_t* d_out, const BatchLa
                   rrg_error* err) {
     uint8_t* P = (uint8_t*)c->bplan.p;
     cudaStream_t s = c->stream;
+    // external records: under stream capture they become event-record nodes
+    // of the graph (a plain record would only order the captured work)
     auto mark = [&](int i) -> int {
-        if (marks) CK(cudaEventRecord(marks[i], s));
+        if (marks) CK(cudaEventRecordWithFlags(marks[i], s, cudaEventRecordExternal));
         return 0;
     };
     if (int r = mark(0)) return r;

@@ -385,6 +385,8 @@ inline cudaError_t cudaEventCreate(cudaEvent_t* e) {
     return cudaSuccess;
 }
 inline cudaError_t cudaEventRecord(cudaEvent_t, cudaStream_t = nullptr) { return cudaSuccess; }
+enum { cudaEventRecordDefault = 0, cudaEventRecordExternal = 1 };
+inline cudaError_t cudaEventRecordWithFlags(cudaEvent_t, cudaStream_t = nullptr, unsigned = 0) { return cudaSuccess; }
 inline cudaError_t cudaStreamWaitEvent(cudaStream_t, cudaEvent_t, unsigned = 0) { return cudaSuccess; }
 inline cudaError_t cudaEventElapsedTime(float* ms, cudaEvent_t, cudaEvent_t) {
     *ms = 0.f;
