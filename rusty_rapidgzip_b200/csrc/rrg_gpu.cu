@@ -239,6 +239,57 @@ struct BatchKey {
 };
 constexpr int BATCH_MARKS = 5;  // events between the stages: plan | inflate | chain + resolve | CRC
 
+#ifndef RRG_EMU
+// Captured graphs by shape. A shape is captured the second time it runs (a
+// one-off shape, such as one small file, runs its launches directly: an
+// instantiation costs more than it saves), and the most recent few stay
+// instantiated, so the waves of a repeated multi-wave batch all replay.
+template <class Key>
+struct GraphCache {
+    struct Ent {
+        Key k;
+        cudaGraphExec_t e;
+        uint32_t kernels;
+    };
+    static constexpr size_t CAP = 8, SEEN = 32;
+    std::vector<Ent> ents;  // most recent first
+    std::vector<Key> seen;  // shapes run once without a graph, most recent first
+    static bool same(const Key& a, const Key& b) { return std::memcmp(&a, &b, sizeof(Key)) == 0; }
+    Ent* find(const Key& k) {
+        for (size_t i = 0; i < ents.size(); i++)
+            if (same(ents[i].k, k)) {
+                std::rotate(ents.begin(), ents.begin() + i, ents.begin() + i + 1);
+                return &ents[0];
+            }
+        return nullptr;
+    }
+    // true when the shape ran before (capture it now); else remembers it
+    bool repeat(const Key& k) {
+        for (size_t i = 0; i < seen.size(); i++)
+            if (same(seen[i], k)) {
+                seen.erase(seen.begin() + i);
+                return true;
+            }
+        seen.insert(seen.begin(), k);
+        if (seen.size() > SEEN) seen.pop_back();
+        return false;
+    }
+    Ent* add(const Key& k, cudaGraphExec_t e, uint32_t kernels) {
+        if (ents.size() >= CAP) {
+            cudaGraphExecDestroy(ents.back().e);
+            ents.pop_back();
+        }
+        ents.insert(ents.begin(), Ent{k, e, kernels});
+        return &ents[0];
+    }
+    void clear() {
+        for (Ent& x : ents) cudaGraphExecDestroy(x.e);
+        ents.clear();
+        seen.clear();
+    }
+};
+#endif
+
 // One range of a member split across GPUs, between its two phases: the
 // decoded cells stay in the context's slot arena, laid out from out + WINDOW.
 struct SplitState {
@@ -307,16 +358,13 @@ struct rrg_ctx {
     uint32_t bg_cap = 0;
     bool use_graphs = true;
 #ifndef RRG_EMU
-    cudaGraphExec_t bg_exec = nullptr;
-    BgzfKey bg_key{};
+    GraphCache<BgzfKey> bg_graphs;
 #endif
     // device-planned member batch: plan and state, and its captured graph
     DBuf bplan;
     cudaEvent_t bt_marks[BATCH_MARKS] = {};  // stage boundaries, recorded by the graph
 #ifndef RRG_EMU
-    cudaGraphExec_t bt_exec = nullptr;
-    BatchKey bt_key{};
-    uint32_t bt_kernels = 0;
+    GraphCache<BatchKey> bt_graphs;
 #endif
 
     rrg_stats st{};
@@ -1063,6 +1111,7 @@ struct MemberJob {
     uint64_t dst_cap = ~0ull; // output bytes available at dst_off (~0: the target grows)
     uint32_t member_base = 0; // index of the first member, for error reports
     double expand = 0;        // output cells per compressed byte to reserve (0: the context's estimate)
+    uint64_t isize_hint = 0;  // the trailer's ISIZE (0: unknown), for balancing sub-chunks
     // A stripe of a non-seekable stream: decoding starts at start_bit (relative
     // to body_off) inside a member whose earlier bytes have been delivered,
     // and stops at the first block edge at or after stop_bit. The last
@@ -1862,10 +1911,10 @@ int bgzf_route(rrg_ctx* c, const uint8_t* d_file, uint64_t len, OutTarget& tgt, 
         key.v[4] = c->lanes;
         key.v[5] = c->inflate_warps;
         if (c->use_graphs) {
-            if (!c->bg_exec || std::memcmp(&key, &c->bg_key, sizeof(key)) != 0) {
-                if (c->bg_exec) cudaGraphExecDestroy(c->bg_exec);
-                c->bg_exec = nullptr;
+            auto* ent = c->bg_graphs.find(key);
+            if (!ent && c->bg_graphs.repeat(key)) {
                 cudaGraph_t g = nullptr;
+                cudaGraphExec_t ex = nullptr;
                 if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
                     const uint64_t l0 = c->launches;
                     int rc = bgzf_enqueue(c, d_file, len, tgt.p, tgt.cap, sgrid, per_block, cap, err);
@@ -1873,20 +1922,16 @@ int bgzf_route(rrg_ctx* c, const uint8_t* d_file, uint64_t len, OutTarget& tgt, 
                     // kernels recorded into the graph are counted when it runs
                     g_launches.fetch_sub(c->launches - l0);
                     c->launches = l0;
-                    if (rc == 0 && e == cudaSuccess && g &&
-                        cudaGraphInstantiate(&c->bg_exec, g, 0) == cudaSuccess) {
-                        c->bg_key = key;
-                    } else {
-                        c->bg_exec = nullptr;
-                    }
+                    if (rc == 0 && e == cudaSuccess && g && cudaGraphInstantiate(&ex, g, 0) == cudaSuccess)
+                        ent = c->bg_graphs.add(key, ex, BGK_KERNELS);
                     if (g) cudaGraphDestroy(g);
                 }
                 cudaGetLastError();  // a failed capture leaves no sticky error; run directly below
             }
-            if (c->bg_exec) {
-                CK(cudaGraphLaunch(c->bg_exec, c->stream));
-                g_launches.fetch_add(BGK_KERNELS);
-                c->launches += BGK_KERNELS;
+            if (ent) {
+                CK(cudaGraphLaunch(ent->e, c->stream));
+                g_launches.fetch_add(ent->kernels);
+                c->launches += ent->kernels;
                 c->st.graph_launches++;
                 ran = true;
             }
@@ -3234,12 +3279,22 @@ int batch_device(rrg_ctx* c, const uint8_t* d_in, std::vector<MemberJob>& jobs, 
     for (const MemberJob& j : jobs)
         if (j.start_bit || j.stop_bit != ~0ull || j.dst_cap == ~0ull || j.capture || j.split || !j.check_crc) return 0;
     if (int rc = upload_tables(c, err)) return rc;
-    // ---- plan: sub-chunks per job at the members_route spacing
-    uint64_t total_c = 0;
-    for (const MemberJob& j : jobs) total_c += j.len - j.body_off;
+    // ---- plan: sub-chunks per job. A sub-chunk's decode time grows with its
+    // compressed bytes (symbols) and its output bytes (cells written), so with
+    // automatic spacing every job gets sub-chunks in proportion to
+    // C + U/3 (U from the trailer's ISIZE), spreading one wave of resident
+    // decoders evenly over text, low-entropy and stored content alike; none is
+    // smaller than 16 KiB of input. A fixed gpu_chunk_bytes spaces by input.
     const uint64_t slots = inflate_slots(c);
-    const uint64_t G = c->gpu_chunk ? std::max<uint64_t>(c->gpu_chunk, 4096)
-                                    : std::max<uint64_t>(16ull << 10, (total_c + slots - 1) / slots);
+    auto cost_of = [&](const MemberJob& j) -> uint64_t {
+        const uint64_t blen = j.len - j.body_off;
+        const uint64_t u = j.isize_hint >= blen / 4 ? j.isize_hint : blen * 3;  // a wrapped or absent ISIZE
+        return blen + u / 3;
+    };
+    uint64_t total_cost = 0;
+    for (const MemberJob& j : jobs) total_cost += cost_of(j);
+    const uint64_t G = c->gpu_chunk ? std::max<uint64_t>(c->gpu_chunk, 4096) : 0;
+    const uint64_t Gc = std::max<uint64_t>(16ull << 10, (total_cost + slots - 1) / slots);
     BatchLaunch L;
     L.nj = (uint32_t)nj;
     std::vector<BatchJob> bj(nj);
@@ -3248,7 +3303,14 @@ int batch_device(rrg_ctx* c, const uint8_t* d_in, std::vector<MemberJob>& jobs, 
     for (size_t i = 0; i < nj; i++) {
         const MemberJob& j = jobs[i];
         const uint64_t blen = j.len - j.body_off;
-        const uint64_t K = blen > G ? std::max<uint64_t>(1, (blen + G / 2) / G) : 1;
+        uint64_t K = 1;
+        if (G) {
+            K = blen > G ? std::max<uint64_t>(1, (blen + G / 2) / G) : 1;
+        } else {
+            const uint64_t cj = cost_of(j);
+            K = cj > Gc ? std::max<uint64_t>(1, (cj + Gc / 2) / Gc) : 1;
+            K = std::min<uint64_t>(K, std::max<uint64_t>(1, blen / (16ull << 10)));
+        }
         any_split |= K > 1;
         BatchJob& b = bj[i];
         b.in_off = j.file_off + j.body_off;
@@ -3338,11 +3400,14 @@ int batch_device(rrg_ctx* c, const uint8_t* d_in, std::vector<MemberJob>& jobs, 
         for (size_t i = 0; i < nj; i++) jc[i] = bj[i].K;
         build_res_tables(jc, c->n_sm, L.tab);
     }
-    // largest estimated spans first
+    // the costliest sub-chunks first
     std::vector<uint32_t> jorder(nj), order(L.n_items);
-    for (uint32_t i = 0; i < nj; i++) jorder[i] = i;
-    std::stable_sort(jorder.begin(), jorder.end(),
-                     [&](uint32_t a, uint32_t b) { return bj[a].blen / bj[a].K > bj[b].blen / bj[b].K; });
+    std::vector<uint64_t> per(nj);
+    for (uint32_t i = 0; i < nj; i++) {
+        jorder[i] = i;
+        per[i] = cost_of(jobs[i]) / bj[i].K;
+    }
+    std::stable_sort(jorder.begin(), jorder.end(), [&](uint32_t a, uint32_t b) { return per[a] > per[b]; });
     {
         size_t q = 0;
         for (uint32_t i : jorder)
@@ -3450,29 +3515,27 @@ int batch_device(rrg_ctx* c, const uint8_t* d_in, std::vector<MemberJob>& jobs, 
                                  L.tab.supers.size(), L.tab.jobs.size(), L.total,
                                  ((uint64_t)c->scan_threads << 32) | c->inflate_warps, L.o_tabs};
         for (size_t i = 0; i < 20; i++) key.v[i] = vals[i];
-        if (!c->bt_exec || std::memcmp(&key, &c->bt_key, sizeof(key)) != 0) {
-            if (c->bt_exec) cudaGraphExecDestroy(c->bt_exec);
-            c->bt_exec = nullptr;
+        auto* ent = c->bt_graphs.find(key);
+        if (!ent && c->bt_graphs.repeat(key)) {
             cudaGraph_t g = nullptr;
+            cudaGraphExec_t ex = nullptr;
             if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
                 const uint64_t l0 = c->launches;
                 int rc = batch_enqueue(c, d_in, tgt.p, L, timed ? marks : nullptr, err);
                 const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
-                c->bt_kernels = (uint32_t)(c->launches - l0);
+                const uint32_t kernels = (uint32_t)(c->launches - l0);
                 g_launches.fetch_sub(c->launches - l0);  // counted when the graph runs
                 c->launches = l0;
-                if (rc == 0 && e == cudaSuccess && g && cudaGraphInstantiate(&c->bt_exec, g, 0) == cudaSuccess)
-                    c->bt_key = key;
-                else
-                    c->bt_exec = nullptr;
+                if (rc == 0 && e == cudaSuccess && g && cudaGraphInstantiate(&ex, g, 0) == cudaSuccess)
+                    ent = c->bt_graphs.add(key, ex, kernels);
                 if (g) cudaGraphDestroy(g);
             }
             cudaGetLastError();  // a failed capture leaves no sticky error; run directly below
         }
-        if (c->bt_exec) {
-            CK(cudaGraphLaunch(c->bt_exec, c->stream));
-            g_launches.fetch_add(c->bt_kernels);
-            c->launches += c->bt_kernels;
+        if (ent) {
+            CK(cudaGraphLaunch(ent->e, c->stream));
+            g_launches.fetch_add(ent->kernels);
+            c->launches += ent->kernels;
             c->st.graph_launches++;
             ran = true;
         }
@@ -3622,6 +3685,7 @@ int batch_impl(rrg_ctx* c, const uint8_t* d_in, const uint64_t* in_off, const ui
         // ISIZE of the (last) member: a size hint for the reserved cells
         if (isz[i] && blen)
             j.expand = std::min(1100.0, std::max(1.05, 1.25 * (double)isz[i] / (double)blen + 0.05));
+        j.isize_hint = isz[i];
         jobs.push_back(j);
         job_item.push_back(i);
     }
@@ -3768,10 +3832,8 @@ void release_scratch(rrg_ctx* c) {
                     &c->exp_isize, &c->got_crc, &c->got_len, &c->mstatus, &c->comp, &c->comp2, &c->pfx, &c->bg_bcount, &c->bg_bbase,
                     &c->bg_coff, &c->bg_csize, &c->bg_small, &c->sniff, &c->pipe, &c->bplan};
 #ifndef RRG_EMU
-    if (c->bg_exec) cudaGraphExecDestroy(c->bg_exec);
-    c->bg_exec = nullptr;
-    if (c->bt_exec) cudaGraphExecDestroy(c->bt_exec);
-    c->bt_exec = nullptr;
+    c->bg_graphs.clear();
+    c->bt_graphs.clear();
 #endif
     for (cudaEvent_t& e : c->bt_marks) {
         if (e) cudaEventDestroy(e);
