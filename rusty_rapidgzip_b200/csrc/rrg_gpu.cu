@@ -3140,10 +3140,16 @@ int batch_enqueue(rrg_ctx* c, const uint8_t* d_in, uint8_t* d_out, const BatchLa
                   rrg_error* err) {
     uint8_t* P = (uint8_t*)c->bplan.p;
     cudaStream_t s = c->stream;
-    // external records: under stream capture they become event-record nodes
-    // of the graph (a plain record would only order the captured work)
+    // under stream capture the records are external, so they become
+    // event-record nodes of the graph (a plain record would only order the
+    // captured work); outside a capture they are plain records
+    cudaStreamCaptureStatus cap_st = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(s, &cap_st));
+    const bool capturing = cap_st == cudaStreamCaptureStatusActive;
     auto mark = [&](int i) -> int {
-        if (marks) CK(cudaEventRecordWithFlags(marks[i], s, cudaEventRecordExternal));
+        if (!marks) return 0;
+        if (capturing) CK(cudaEventRecordWithFlags(marks[i], s, cudaEventRecordExternal));
+        else CK(cudaEventRecord(marks[i], s));
         return 0;
     };
     if (int r = mark(0)) return r;

@@ -386,6 +386,11 @@ inline cudaError_t cudaEventCreate(cudaEvent_t* e) {
 }
 inline cudaError_t cudaEventRecord(cudaEvent_t, cudaStream_t = nullptr) { return cudaSuccess; }
 enum { cudaEventRecordDefault = 0, cudaEventRecordExternal = 1 };
+enum cudaStreamCaptureStatus { cudaStreamCaptureStatusNone = 0, cudaStreamCaptureStatusActive = 1 };
+inline cudaError_t cudaStreamIsCapturing(cudaStream_t, cudaStreamCaptureStatus* st) {
+    *st = cudaStreamCaptureStatusNone;
+    return cudaSuccess;
+}
 inline cudaError_t cudaEventRecordWithFlags(cudaEvent_t, cudaStream_t = nullptr, unsigned = 0) { return cudaSuccess; }
 inline cudaError_t cudaStreamWaitEvent(cudaStream_t, cudaEvent_t, unsigned = 0) { return cudaSuccess; }
 inline cudaError_t cudaEventElapsedTime(float* ms, cudaEvent_t, cudaEvent_t) {
