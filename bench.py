@@ -205,7 +205,7 @@ def run_ours(args, raw, gz, desc):
     dout = torch.empty(len(raw) + 64, dtype=torch.uint8, device="cuda")
     torch.cuda.synchronize()
     tuning = None
-    if args.workload == "bgzf" and args.warps_per_stream == 0:
+    if args.workload == "bgzf" and args.warps_per_stream == 0 and not args.no_autotune:
         # autotune (untimed) on the file's first 2048 members
         off, k = 0, 0
         while k < 2048 and off + 18 <= len(gz):
@@ -566,14 +566,17 @@ def run_files(args):
     dout = torch.empty(U_ + 64, dtype=torch.uint8, device="cuda")
     dec = Decoder(Config(device=local))
     stream = torch.cuda.Stream()
-    # ---- autotune on a sample (untimed)
-    s_gz = [g for _, g in sample]
-    s_raw = [r for r, _ in sample]
-    s_in = torch.from_numpy(np.frombuffer(b"".join(s_gz), dtype=np.uint8).copy()).cuda()
-    s_out = torch.empty(sum(len(r) for r in s_raw) + 64, dtype=torch.uint8, device="cuda")
-    tuning = dec.autotune(s_in, np.cumsum([0] + [len(g) for g in s_gz])[:-1].tolist(), [len(g) for g in s_gz],
-                          s_out, np.cumsum([0] + [len(r) for r in s_raw])[:-1].tolist(), [len(r) for r in s_raw])
-    del s_in, s_out
+    # ---- autotune on a sample (untimed; --no-autotune keeps the defaults, for
+    # profiler runs whose own slowdown would steer the sweep)
+    tuning = None
+    if not args.no_autotune:
+        s_gz = [g for _, g in sample]
+        s_raw = [r for r, _ in sample]
+        s_in = torch.from_numpy(np.frombuffer(b"".join(s_gz), dtype=np.uint8).copy()).cuda()
+        s_out = torch.empty(sum(len(r) for r in s_raw) + 64, dtype=torch.uint8, device="cuda")
+        tuning = dec.autotune(s_in, np.cumsum([0] + [len(g) for g in s_gz])[:-1].tolist(), [len(g) for g in s_gz],
+                              s_out, np.cumsum([0] + [len(r) for r in s_raw])[:-1].tolist(), [len(r) for r in s_raw])
+        del s_in, s_out
 
     def step():
         got, status, st = dec.decode_batch(din, in_off, in_len, dout, out_off, lens, stream=stream.cuda_stream)
@@ -748,6 +751,7 @@ def main():
     ap.add_argument("--boundary-mode", type=int, default=0, help="1: one finder search per target")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="files: leave out the plain per-file comparison arm")
+    ap.add_argument("--no-autotune", action="store_true", help="files, bgzf: keep the default tunables")
     ap.add_argument("--stripe", type=int, default=0, help="stream: compressed bytes per stripe (0: 256 MiB)")
     args = ap.parse_args()
     if args.warmup < 3:
