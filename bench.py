@@ -198,7 +198,7 @@ def run_ours(args, raw, gz, desc):
     if world > 1:
         dist.init_process_group("nccl", device_id=torch.device("cuda", local))
     dec = Decoder(Config(device=local, gpu_chunk_bytes=args.gpu_chunk, warps_per_stream=args.warps_per_stream,
-                         boundary_mode=args.boundary_mode, verbose=False))
+                         boundary_mode=args.boundary_mode, host_pipeline=args.pipeline_waves, verbose=False))
     stream = torch.cuda.Stream()
     din = torch.empty(len(gz), dtype=torch.uint8, device="cuda")
     din.copy_(torch.frombuffer(bytearray(gz), dtype=torch.uint8))
@@ -284,10 +284,11 @@ def run_ours(args, raw, gz, desc):
     assert n == len(raw)
     barrier()
     e2e_times = []
+    e2e_st = None
     for _ in range(args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        n, _ = dec.count(buf)
+        n, e2e_st = dec.count(buf)
         e2e_times.append(time.perf_counter() - t0)
         assert n == len(raw)
     te = sum(e2e_times)
@@ -335,7 +336,7 @@ def run_ours(args, raw, gz, desc):
                            graph_launches=ms.graph_launches, autotuned=tuning,
                            **({"plain_per_member": plain} if plain else {})),
             "e2e": {"value": round(e2e_value, 3), "unit": "GB/s", "h2d_bytes_per_step": C_,
-                    "d2h_bytes_per_step": U_},
+                    "d2h_bytes_per_step": U_, "pipeline_waves": e2e_st.pipeline_waves if e2e_st else None},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 2), "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
@@ -752,6 +753,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="files: leave out the plain per-file comparison arm")
     ap.add_argument("--no-autotune", action="store_true", help="files, bgzf: keep the default tunables")
+    ap.add_argument("--pipeline-waves", type=int, default=0,
+                    help="end-to-end leg: waves of the pipelined host path (0: automatic, -1: off)")
     ap.add_argument("--stripe", type=int, default=0, help="stream: compressed bytes per stripe (0: 256 MiB)")
     args = ap.parse_args()
     if args.warmup < 3:

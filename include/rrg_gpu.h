@@ -83,7 +83,9 @@ typedef struct rrg_config {
     uint64_t hbm_budget_bytes;   /* serving admission budget; 0 = 120 GB */
     int32_t host_pipeline;       /* rrg_gpu_decode_host/read_gz: 0 = decode a large single-member stream
                                     in waves with the copy to the host overlapped (falls back to the
-                                    checked path on any irregularity); -1 = always the checked path */
+                                    checked path on any irregularity), up to 4 waves; N >= 2 = N waves
+                                    where every sub-chunk keeps at least 8 KiB; -1 = always the
+                                    checked path */
     int32_t batch_plan;          /* rrg_gpu_decode_batch: 0 = the member route planned and checked on the
                                     device (sub-chunk starts, item list, anchored chain, resolve, CRC) as one
                                     captured graph, with the jobs it cannot finish decoded on the checked

@@ -129,7 +129,7 @@ class Config:
     warps_per_stream: int = 0
     boundary_mode: int = 0
     hbm_budget_bytes: int = 0
-    host_pipeline: int = 0  # -1: the host path never decodes in overlapped waves
+    host_pipeline: int = 0  # -1: the host path never decodes in overlapped waves; N >= 2: N waves
     batch_plan: int = 0  # -1: decode_batch never takes the device-planned graph route
 
     def _c(self) -> _Config:

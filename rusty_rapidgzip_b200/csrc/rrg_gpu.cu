@@ -2198,11 +2198,15 @@ int ensure_ring(rrg_ctx* c, size_t piece, uint32_t waves, rrg_error* err) {
 }
 
 // Waves the pipelined path would use for a body of `blen` compressed bytes:
-// each wave needs one sub-chunk of at least 32 KiB per resident decoder.
+// each wave needs one sub-chunk of at least 32 KiB per resident decoder (at
+// most 4 waves), or the configured count, as long as each sub-chunk keeps at
+// least 8 KiB.
 uint32_t pipeline_waves(rrg_ctx* c, uint64_t blen) {
     if (!c->pipeline || !c->scan_bounds || c->lanes || c->gpu_chunk) return 0;
-    const uint64_t per_wave = inflate_slots(c) * (32ull << 10);
-    return (uint32_t)std::min<uint64_t>(4, blen / per_wave);
+    const uint64_t slots = inflate_slots(c);
+    if (c->cfg.host_pipeline >= 2)
+        return (uint32_t)std::min<uint64_t>(c->cfg.host_pipeline, blen / (slots * (8ull << 10)));
+    return (uint32_t)std::min<uint64_t>(4, blen / (slots * (32ull << 10)));
 }
 
 // Returns 0 with *taken = false when the file does not suit the pipeline
