@@ -1076,6 +1076,53 @@ int scan_boundaries(rrg_ctx* c, const uint8_t* body, uint64_t blen, std::vector<
     return 0;
 }
 
+// Targets (bits from `body`) that have no start in `verified` within `half`
+// bits on either side.
+std::vector<uint64_t> lone_targets(const std::vector<uint64_t>& targets, const std::vector<uint64_t>& verified,
+                                   uint64_t half) {
+    std::vector<uint64_t> lone;
+    for (uint64_t x : targets) {
+        auto it = std::lower_bound(verified.begin(), verified.end(), x > half ? x - half : 0);
+        if (it == verified.end() || *it > x + half) lone.push_back(x);
+    }
+    return lone;
+}
+
+// Block starts found by walking the fixed Huffman code forward from each
+// target (k_fixed_walk), for targets the candidate scan left without a start,
+// as in a stream of fixed-Huffman blocks. They join `verified`, which stays
+// sorted and free of duplicates. A walk gives up 256 KiB past its target.
+int fixed_walk_starts(rrg_ctx* c, const uint8_t* body, uint64_t blen, const std::vector<uint64_t>& from,
+                      std::vector<uint64_t>& verified, rrg_error* err) {
+    if (from.empty() || blen < 8) return 0;
+    const uint32_t n = (uint32_t)from.size();
+    KTimer kt(c->stream);
+    CK(dgrow(c->targets, (size_t)n * 8));
+    CK(dgrow(c->found, (size_t)n * 8));
+    CK(cudaMemcpyAsync(c->targets.p, from.data(), (size_t)n * 8, cudaMemcpyHostToDevice, c->stream));
+    FixedWalkArgs F{body, blen, (const uint64_t*)c->targets.p, (uint64_t*)c->found.p, n, (256ull << 10) * 8};
+    RRG_LAUNCH(k_fixed_walk, (n + FW_THREADS - 1) / FW_THREADS, FW_THREADS, 0, c->stream, F);
+    LAUNCHED(c);
+    kt.stop();
+    std::vector<uint64_t> found(n);
+    CK(cudaMemcpyAsync(found.data(), c->found.p, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->st.finder_ms += kt.ms();
+    size_t added = 0;
+    for (uint64_t f : found)
+        if (f != ~0ull) {
+            verified.push_back(f);
+            added++;
+        }
+    if (c->cfg.verbose >= 2)
+        std::fprintf(stderr, "[rrg-gpu] fixed-code walk from %u targets: %zu block starts\n", n, added);
+    if (added) {
+        std::sort(verified.begin(), verified.end());
+        verified.erase(std::unique(verified.begin(), verified.end()), verified.end());
+    }
+    return 0;
+}
+
 // ------------------------------------------------------------ member route
 // Decoders resident at once on the device: warps (or lanes) of one full wave
 // of the inflate kernel.
@@ -1262,6 +1309,10 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
                     }
                 }
             }
+            // targets with no start within 256 KiB: fixed-Huffman blocks
+            if (int rf = fixed_walk_starts(c, d_base + lo, hi - lo, lone_targets(ideal, verified, WIDE * 8), verified,
+                                           err))
+                return rf;
             // verified offsets are sorted bit offsets from `lo`
             for (size_t q = a; q < b; q++) {
                 MemberJob& j = jobs[big[q]];
@@ -2226,6 +2277,14 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
     if (int rc = scan_boundaries(c, body, blen, verified, &stored, err)) return rc;
     const uint64_t slots = inflate_slots(c);
     const uint64_t nbits = blen * 8;
+    {  // sub-chunk targets with no start within 256 KiB: fixed-Huffman blocks
+        std::vector<uint64_t> ideal;
+        const uint64_t K = slots * W;
+        for (uint64_t k = 1; k < K; k++) ideal.push_back(nbits * k / K);
+        if (int rf = fixed_walk_starts(c, body, blen, lone_targets(ideal, verified, (256ull << 10) * 8), verified,
+                                       err))
+            return rf;
+    }
     // block starts the chunks may begin at, and wave edges among them nearest
     // to equal shares of the input
     std::vector<uint64_t> cand{0};

@@ -2171,6 +2171,136 @@ __global__ void __launch_bounds__(128) k_verify_heavy(VerifyArgs A) {
     }
 }
 
+// ------------------------------------------------------- fixed-Huffman block starts
+// A fixed-Huffman block (BTYPE=01, RFC 1951 §3.2.6) has no code-length header
+// to test, so the candidate scan cannot see where one starts. The reference's
+// finder looks for dynamic blocks only (block_finder.rs:60-78), and a stream of
+// fixed blocks (zlib's Z_FIXED strategy, or short or low-entropy blocks at low
+// levels) would decode as one sub-chunk. Instead of testing offsets, one thread
+// walks the fixed code from a target bit: a prefix code resynchronises with
+// the true symbol boundaries within a few symbols, so after FW_WARM symbols
+// without an end-of-block or invalid code the walk is on the real symbol path
+// and the next end-of-block code it meets ends a real block. The bit after it
+// counts as a block start when the block there parses: a stored header with
+// LEN = ~NLEN, a dynamic header that passes verify_light, or a fixed block
+// whose first FW_MINSYM symbols decode without an end-of-block or invalid code
+// (random bits meet one of those within about 36 symbols on average, so a walk
+// over non-fixed data, where end-of-block codes are chance matches, essentially
+// never passes). Any start this returns is checked again by the anchored chain.
+
+constexpr uint32_t FW_THREADS = 32;
+constexpr uint32_t FW_WARM = 256;     // symbols since the last end-of-block or invalid code before one is trusted
+constexpr uint32_t FW_MINSYM = 1024;  // symbols a fixed block after the start must decode cleanly
+
+struct FixedWalkArgs {
+    const uint8_t* body;
+    uint64_t body_len;
+    const uint64_t* from;  // bit offsets to walk from (relative to body)
+    uint64_t* found;       // per target: the first block start the walk proves, or ~0
+    uint32_t n;
+    uint64_t limit_bits;   // how far past its target a walk may go
+};
+
+// One fixed-code symbol from `buf` (at least 32 bits buffered): 0 literal or
+// length/distance pair, 1 end of block, 2 invalid code (286/287, distance
+// 30/31). *used = bits taken (codes are stored MSB first, RFC 1951 §3.1.1).
+__device__ __forceinline__ uint32_t fixed_step(uint64_t buf, uint32_t* used) {
+    const uint32_t r = __brev((uint32_t)buf & 511u) >> 23;  // the next 9 code bits, MSB first
+    const uint32_t t8 = r >> 1;
+    uint32_t sym, cl;
+    if (t8 < 0x30u) {  // 7-bit codes 0000000-0010111: symbols 256-279
+        sym = 256u + (r >> 2);
+        cl = 7;
+    } else if (t8 < 0xc0u) {  // 8-bit codes 00110000-10111111: literals 0-143
+        *used = 8;
+        return 0;
+    } else if (t8 < 0xc8u) {  // 8-bit codes 11000000-11000111: symbols 280-287
+        sym = 280u + (t8 - 0xc0u);
+        cl = 8;
+    } else {  // 9-bit codes 110010000-111111111: literals 144-255
+        *used = 9;
+        return 0;
+    }
+    if (sym == 256u) {
+        *used = 7;
+        return 1;
+    }
+    if (sym > 285u) {
+        *used = cl;
+        return 2;
+    }
+    const uint32_t p = cl + c_len_extra[sym - 257u];
+    const uint32_t dc = __brev((uint32_t)(buf >> p) & 31u) >> 27;  // 5-bit distance code
+    if (dc >= 30u) {
+        *used = p + 5;
+        return 2;
+    }
+    *used = p + 5 + c_dist_extra[dc];
+    return 0;
+}
+
+// Does a block start at bit e? (the tests the walk applies, see above)
+__device__ bool fixed_start_ok(const Src& s, uint64_t total_bits, uint64_t e, uint8_t* lut) {
+    if (e + 3 > total_bits) return false;
+    const uint32_t btype = peek_at(s, e, 3) >> 1;
+    if (btype == 3) return false;
+    if (btype == 2) return verify_light(s, total_bits, e, lut);
+    if (btype == 0) {
+        const uint64_t q = (e + 3 + 7) & ~7ull;  // LEN and NLEN start at the next byte
+        if (q + 32 > total_bits) return false;
+        const uint32_t len = peek_at(s, q, 16), nlen = peek_at(s, q + 16, 16);
+        if ((len ^ nlen) != 0xffffu) return false;
+        const uint64_t nx = q + 32 + 8ull * len;  // the next block's header
+        return nx + 3 <= total_bits && (peek_at(s, nx, 3) >> 1) != 3u;
+    }
+    BR b{s, 0, 0, 0};
+    br_seek(b, e + 3);
+    for (uint32_t k = 0; k < FW_MINSYM; k++) {
+        br_refill(b);
+        uint32_t used = 0;
+        if (fixed_step(b.buf, &used) != 0) return false;
+        br_consume(b, used);
+        if (br_tell(b) > total_bits) return false;
+    }
+    return true;
+}
+
+// One thread per target.
+__global__ void __launch_bounds__(FW_THREADS) k_fixed_walk(FixedWalkArgs A) {
+    __shared__ __align__(16) uint8_t s_lut[FW_THREADS * 128];  // verify_light's precode table, one per thread
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    const Src s = make_src(A.body, A.body_len);
+    const uint64_t total_bits = A.body_len * 8;
+    const uint64_t p0 = A.from[i];
+    uint64_t found = ~0ull;
+    if (p0 < total_bits) {
+        const uint64_t stop = total_bits - p0 > A.limit_bits ? p0 + A.limit_bits : total_bits;
+        BR b{s, 0, 0, 0};
+        br_seek(b, p0);
+        uint32_t run = 0;
+        while (br_tell(b) < stop) {
+            br_refill(b);
+            uint32_t used = 0;
+            const uint32_t k = fixed_step(b.buf, &used);
+            br_consume(b, used);
+            if (k == 0) {
+                run++;
+                continue;
+            }
+            if (k == 1 && run >= FW_WARM) {
+                const uint64_t e = br_tell(b);
+                if (e < total_bits && fixed_start_ok(s, total_bits, e, s_lut + threadIdx.x * 128)) {
+                    found = e;
+                    break;
+                }
+            }
+            run = 0;
+        }
+    }
+    A.found[i] = found;
+}
+
 // ------------------------------------------------------- marker resolution
 // A marker cell 0x8000|m of chunk k names the output byte m + 1 positions
 // before chunk k's first byte (speculative.rs:12-17, :41), so every marker

@@ -199,11 +199,13 @@ def _crc32(data: bytes) -> int:
 
 
 def gzip_member(data: bytes, level: int = 6, parallel_threshold: int = 64 << 20,
-                piece: int = 32 << 20, threads: int | None = None) -> bytes:
-    """One gzip member (RFC 1952) of ``data`` at zlib ``level``."""
+                piece: int = 32 << 20, threads: int | None = None,
+                strategy: int = zlib.Z_DEFAULT_STRATEGY) -> bytes:
+    """One gzip member (RFC 1952) of ``data`` at zlib ``level`` and ``strategy``
+    (``zlib.Z_FIXED``: every block fixed-Huffman)."""
     mv = memoryview(data)
     if len(data) <= parallel_threshold:
-        c = zlib.compressobj(level, zlib.DEFLATED, -15, 8)
+        c = zlib.compressobj(level, zlib.DEFLATED, -15, 8, strategy)
         body = c.compress(mv) + c.flush(zlib.Z_FINISH)
     else:
         starts = list(range(0, len(data), piece))
@@ -212,9 +214,9 @@ def gzip_member(data: bytes, level: int = 6, parallel_threshold: int = 64 << 20,
             s = starts[i]
             e = min(len(data), s + piece)
             if i == 0:
-                c = zlib.compressobj(level, zlib.DEFLATED, -15, 8)
+                c = zlib.compressobj(level, zlib.DEFLATED, -15, 8, strategy)
             else:
-                c = zlib.compressobj(level, zlib.DEFLATED, -15, 8,
+                c = zlib.compressobj(level, zlib.DEFLATED, -15, 8, strategy,
                                      zdict=bytes(mv[max(0, s - 32768):s]))
             last = e == len(data)
             return c.compress(mv[s:e]) + c.flush(zlib.Z_FINISH if last else zlib.Z_SYNC_FLUSH)
@@ -256,6 +258,14 @@ def config1(n_bytes: int = 1 << 30, seed: int = 1):
     """Zipf text, zlib level 9, one gzip member."""
     raw = zipf_text(n_bytes, seed)
     return raw, gzip_member(raw, 9)
+
+
+def fixed_blocks(n_bytes: int = 64 << 20, seed: int = 1):
+    """Zipf text, zlib level 1 with the Z_FIXED strategy: one gzip member made
+    of fixed-Huffman blocks only (16,383 symbols each), which no dynamic-block
+    finder can split."""
+    raw = zipf_text(n_bytes, seed)
+    return raw, gzip_member(raw, 1, strategy=zlib.Z_FIXED)
 
 
 def config2(n_bytes: int = 4 << 30, seed: int = 0):

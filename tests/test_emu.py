@@ -677,3 +677,20 @@ def test_destination_provider(emu_decoder_factory, tmp_path, pipelined):
     out.clear()
     st = d.decode_host_into(gz, recycle, sink)
     assert b"".join(out) == raw
+
+
+def test_fixed_huffman_blocks_split(emu_decoder_factory):
+    """A member of fixed-Huffman blocks only (zlib Z_FIXED) splits into
+    sub-chunks at block starts found by walking the fixed code, on the
+    pipelined host path and on the member route, with no re-decode."""
+    raw, gz = W.fixed_blocks(1 << 20, seed=11)
+    assert oracle.read_gz(gz, 2, 1 << 20) == raw
+    d = emu_decoder_factory()
+    n, st = d.count(gz)
+    assert n == len(raw)
+    assert st.gpu_chunks >= 8 and st.speculation_failures == 0
+    src = np.frombuffer(gz, dtype=np.uint8).copy()
+    dst = np.zeros(len(raw) + 65536, dtype=np.uint8)
+    m, st2 = d.decode_device(haddr(src), src.size, haddr(dst), dst.size)
+    assert m == len(raw) and dst[:m].tobytes() == raw
+    assert st2.gpu_chunks >= 4 and st2.speculation_failures == 0

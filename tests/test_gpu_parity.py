@@ -554,3 +554,27 @@ def test_seek_index_gpu(gpu_decoder_factory):
     for off, n in cases:
         n = min(n, len(whole) - off)
         assert d.read_range(data, idx, off, n) == whole[off:off + n], (off, n)
+
+
+@pytest.mark.parametrize("size", [4 << 20, 128 << 20])
+def test_fixed_huffman_blocks(gpu_decoder_factory, size):
+    """Fixed-Huffman blocks only (zlib level 1, Z_FIXED): block starts come
+    from the fixed-code walk, so the member splits into many sub-chunks with
+    no re-decode, device-resident and through the pipelined host path."""
+    import torch
+    raw, gz = W.fixed_blocks(size, seed=21)
+    if size <= 4 << 20:
+        assert oracle.read_gz(gz, 4, 1 << 20) == raw
+    d = gpu_decoder_factory()
+    src = dev(gz)
+    out = torch.empty(len(raw) + (1 << 20), dtype=torch.uint8, device="cuda")
+    n, st = d.decode_device(src.data_ptr(), len(gz), out.data_ptr(), out.numel())
+    assert n == len(raw)
+    assert hashlib.sha256(out[:n].cpu().numpy().tobytes()).hexdigest() == sha256(raw)
+    assert st.gpu_chunks >= 32 and st.speculation_failures == 0
+    got = []
+    d2 = gpu_decoder_factory(host_pipeline=2)  # two overlapped waves where the input is large enough
+    st2 = d2.decode_host(gz, got.append)
+    assert b"".join(got) == raw
+    assert st2.gpu_chunks >= 32 and st2.speculation_failures == 0
+    assert st2.pipeline_waves == (2 if size > 64 << 20 else 0)
