@@ -2272,142 +2272,186 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
     *taken = true;
     c->st.pipeline_waves = W;
     const uint8_t* body = d_file + hl;
+    const double t_enter = now_ms();
+    double t_mark[4] = {0, 0, 0, 0};  // host timeline (verbose)
+    const uint64_t slots = inflate_slots(c);
+    const uint64_t nbits = blen * 8;
+    // Wave shares of the input. The last wave's output copy is the one that
+    // nothing overlaps, so it gets 0.4 of the others' share (measured on a
+    // 1 GiB level-9 member with three waves: 48.6 -> 43.0 ms end to end).
+    std::vector<double> cum(W + 1, 0.0);
+    for (uint32_t w = 0; w < W; w++) cum[w + 1] = cum[w] + (w + 1 == W && W <= 4 ? 0.4 : 1.0);
+    auto wave_ideal = [&](uint32_t w) { return (uint64_t)((double)nbits * cum[w] / cum[W]); };
+    // sub-chunk targets (one per resident decoder and wave), for the fixed-code walk
+    const uint64_t K = slots * W;
+    auto targets_in = [&](uint64_t lo, uint64_t hi) {
+        std::vector<uint64_t> t;
+        for (uint64_t k = 1; k < K; k++) {
+            const uint64_t x = nbits * k / K;
+            if (x >= lo && x < hi) t.push_back(x);
+        }
+        return t;
+    };
+    constexpr uint64_t WALK_WIDE = (256ull << 10) * 8;
+    // ---- planning state of both phases
+    std::vector<uint64_t> cand{0};  // block starts a sub-chunk may begin at
+    std::vector<uint64_t> st;       // sub-chunk starts
+    std::vector<uint32_t> wfirst;   // first sub-chunk of each wave
+    std::vector<ChunkItem> items;
+    std::vector<PipeWave> waves;
+    std::vector<uint32_t> order;
+    std::vector<uint8_t> tabs;  // ResGroup[], ResJob[1], chunk_group[] per wave, 8-byte aligned
+    uint64_t arena = 0;
+    uint32_t total_pieces = 0;
+    auto set_cand = [&](const std::vector<uint64_t>& v) {
+        cand.assign(1, 0);
+        for (uint64_t x : v)
+            if (x > cand.back() && x < nbits) cand.push_back(x);
+    };
+    auto end_of = [&](size_t i) { return i < cand.size() ? cand[i] : nbits; };
+    auto nearest = [&](uint64_t x, size_t i_lo) {  // index of the candidate nearest x, at or after i_lo
+        size_t i = (size_t)(std::lower_bound(cand.begin() + i_lo, cand.end(), x) - cand.begin());
+        if (i == cand.size() || (i > i_lo && x - cand[i - 1] < cand[i] - x)) i--;
+        return i;
+    };
+    // Waves [w_from, w_to) over the candidates [i_from, i_end): wave edges are
+    // the block starts nearest each wave's share; within a wave (one item per
+    // resident decoder), runs of consecutive blocks whose largest span is as
+    // small as possible (the wave ends with its largest sub-chunk, and a block
+    // is the finest unit a sub-chunk can take).
+    auto plan_starts = [&](uint32_t w_from, uint32_t w_to, size_t i_from, size_t i_end) {
+        std::vector<size_t> wedge{i_from};
+        for (uint32_t w = w_from + 1; w < w_to; w++) {
+            const size_t i = std::min(nearest(wave_ideal(w), i_from), i_end);
+            if (i > wedge.back() && i < i_end) wedge.push_back(i);
+        }
+        wedge.push_back(i_end);
+        for (size_t w = 0; w + 1 < wedge.size(); w++) {
+            const size_t a = wedge[w], b = wedge[w + 1];
+            auto runs = [&](uint64_t B, std::vector<uint64_t>* out) {
+                uint64_t cnt = 0;
+                for (size_t i = a; i < b;) {
+                    size_t j = i + 1;
+                    while (j < b && end_of(j + 1) - cand[i] <= B) j++;
+                    if (out) out->push_back(cand[i]);
+                    cnt++;
+                    i = j;
+                }
+                return cnt;
+            };
+            // the answer lies between an even split and an even split plus the widest block
+            uint64_t gap = 0;
+            for (size_t i = a; i < b; i++) gap = std::max(gap, end_of(i + 1) - cand[i]);
+            const uint64_t range = end_of(b) - cand[a];
+            uint64_t lo = std::max<uint64_t>(1, range / slots), hi = std::min(range, range / slots + gap);
+            while (lo < hi) {  // the smallest largest span that fits one wave
+                const uint64_t mid = lo + (hi - lo) / 2;
+                if (runs(mid, nullptr) <= slots) hi = mid;
+                else lo = mid + 1;
+            }
+            wfirst.push_back((uint32_t)st.size());
+            runs(lo, &st);
+        }
+    };
+    // items [k_from, st.size()): the last one ends at next_start (~0: the member's end)
+    auto make_items = [&](uint32_t k_from, uint64_t next_start, const std::vector<uint64_t>& stored) {
+        const uint32_t k_to = (uint32_t)st.size();
+        for (uint32_t k = k_from; k < k_to; k++) {
+            ChunkItem it{};
+            it.in_off = hl;
+            it.in_len = blen;
+            it.start_bit = st[k];
+            it.end_hint = k + 1 < k_to ? st[k + 1] : next_start;
+            const uint64_t span = ((it.end_hint == ~0ull ? nbits : it.end_hint) - st[k] + 7) / 8;
+            it.out_cap = round8((uint64_t)(span * c->expand) + 65536);
+            it.out_off = arena;
+            it.flags = ITEM_MARKERS;
+            if (k) {
+                if (std::binary_search(stored.begin(), stored.end(), st[k])) it.flags |= ITEM_STORED_START;
+                else if (std::binary_search(stored.begin(), stored.end(), st[k] | 1))
+                    it.flags |= ITEM_STORED_START | ITEM_EMPTY_STORED;
+            }
+            it.id = k;
+            arena += it.out_cap;
+            items.push_back(it);
+        }
+    };
+    // waves [waves.size(), wfirst.size()) (the last one ends at the last item):
+    // each wave's resolve tables and a CRC piece region large enough for any
+    // output its slots can hold
+    auto make_waves = [&]() {
+        order.resize(items.size());
+        for (uint32_t w = (uint32_t)waves.size(); w < wfirst.size(); w++) {
+            PipeWave pw;
+            pw.first = wfirst[w];
+            pw.n = (w + 1 < wfirst.size() ? wfirst[w + 1] : (uint32_t)st.size()) - wfirst[w];
+            uint64_t cap = 0;
+            for (uint32_t q = 0; q < pw.n; q++) cap += items[pw.first + q].out_cap;
+            pw.piece_off = total_pieces;
+            pw.piece_cap = (uint32_t)(cap / WAVE_PIECE + 2);
+            total_pieces += pw.piece_cap;
+            // largest spans first within the wave
+            for (uint32_t q = 0; q < pw.n; q++) order[pw.first + q] = pw.first + q;
+            std::stable_sort(order.begin() + pw.first, order.begin() + pw.first + pw.n,
+                             [&](uint32_t a, uint32_t b) { return items[a].out_cap > items[b].out_cap; });
+            build_res_tables({pw.n}, c->n_sm, pw.tab);
+            pw.tab_off = tabs.size();
+            tabs.resize(pw.tab_off + round8(pw.tab.bytes));
+            pw.tab.write(tabs.data() + pw.tab_off);
+            waves.push_back(std::move(pw));
+        }
+    };
     // ---- boundaries (the scan overlaps the input's arrival) and sub-chunk starts
     std::vector<uint64_t> verified, stored;
     if (int rc = scan_boundaries(c, body, blen, verified, &stored, err)) return rc;
-    const uint64_t slots = inflate_slots(c);
-    const uint64_t nbits = blen * 8;
-    {  // sub-chunk targets with no start within 256 KiB: fixed-Huffman blocks
-        std::vector<uint64_t> ideal;
-        const uint64_t K = slots * W;
-        for (uint64_t k = 1; k < K; k++) ideal.push_back(nbits * k / K);
-        if (int rf = fixed_walk_starts(c, body, blen, lone_targets(ideal, verified, (256ull << 10) * 8), verified,
-                                       err))
-            return rf;
-    }
-    // block starts the chunks may begin at, and wave edges among them nearest
-    // to equal shares of the input
-    std::vector<uint64_t> cand{0};
-    for (uint64_t v : verified)
-        if (v > cand.back() && v < nbits) cand.push_back(v);
-    std::vector<size_t> wedge{0};
-    for (uint32_t w = 1; w < W; w++) {
-        const uint64_t ideal = nbits * w / W;
-        size_t i = (size_t)(std::lower_bound(cand.begin(), cand.end(), ideal) - cand.begin());
-        if (i == cand.size() || (i > 0 && ideal - cand[i - 1] < cand[i] - ideal)) i--;
-        if (i > wedge.back()) wedge.push_back(i);
-    }
-    wedge.push_back(cand.size());
-    auto end_of = [&](size_t i) { return i < cand.size() ? cand[i] : nbits; };
-    // within a wave (one item per resident decoder), runs of consecutive blocks
-    // whose largest span is as small as possible: the wave ends with its
-    // largest sub-chunk, and a block is the finest unit a sub-chunk can take
-    std::vector<uint64_t> st;
-    std::vector<uint32_t> wfirst;
-    for (size_t w = 0; w + 1 < wedge.size(); w++) {
-        const size_t a = wedge[w], b = wedge[w + 1];
-        auto runs = [&](uint64_t B, std::vector<uint64_t>* out) {
-            uint64_t cnt = 0;
-            for (size_t i = a; i < b;) {
-                size_t j = i + 1;
-                while (j < b && end_of(j + 1) - cand[i] <= B) j++;
-                if (out) out->push_back(cand[i]);
-                cnt++;
-                i = j;
-            }
-            return cnt;
-        };
-        uint64_t lo = 1, hi = end_of(b) - cand[a];
-        while (lo < hi) {  // the smallest largest span that fits one wave
-            const uint64_t mid = lo + (hi - lo) / 2;
-            if (runs(mid, nullptr) <= slots) hi = mid;
-            else lo = mid + 1;
-        }
-        wfirst.push_back((uint32_t)st.size());
-        runs(lo, &st);
-    }
-    wfirst.push_back((uint32_t)st.size());
-    const uint32_t n = (uint32_t)st.size();
-    // ---- items and the slot arena
-    std::vector<ChunkItem> items(n);
-    uint64_t arena = 0;
-    for (uint32_t k = 0; k < n; k++) {
-        ChunkItem& it = items[k];
-        it.in_off = hl;
-        it.in_len = blen;
-        it.start_bit = st[k];
-        it.end_hint = k + 1 < n ? st[k + 1] : ~0ull;
-        const uint64_t span = ((k + 1 < n ? st[k + 1] : nbits) - st[k] + 7) / 8;
-        it.out_cap = round8((uint64_t)(span * c->expand) + 65536);
-        it.out_off = arena;
-        it.flags = ITEM_MARKERS;
-        if (k) {
-            if (std::binary_search(stored.begin(), stored.end(), st[k])) it.flags |= ITEM_STORED_START;
-            else if (std::binary_search(stored.begin(), stored.end(), st[k] | 1))
-                it.flags |= ITEM_STORED_START | ITEM_EMPTY_STORED;
-        }
-        it.id = k;
-        arena += it.out_cap;
-    }
-    // ---- waves: contiguous runs of items; per wave the resolve tables and a
-    // CRC piece region large enough for any output its slots can hold
-    const uint32_t Wn = (uint32_t)wfirst.size() - 1;
-    std::vector<PipeWave> waves(Wn);
-    std::vector<uint32_t> order(n);
-    std::vector<uint8_t> tabs;  // ResGroup[], ResJob[1], chunk_group[] per wave, 8-byte aligned
-    uint32_t max_n = 0, total_pieces = 0;
-    size_t max_win = 0;
-    uint64_t out_bound = 0;
-    for (uint32_t w = 0; w < Wn; w++) {
-        PipeWave& pw = waves[w];
-        pw.first = wfirst[w];
-        pw.n = wfirst[w + 1] - wfirst[w];
-        uint64_t cap = 0;
-        for (uint32_t q = 0; q < pw.n; q++) cap += items[pw.first + q].out_cap;
-        out_bound += cap;
-        pw.piece_off = total_pieces;
-        pw.piece_cap = (uint32_t)(cap / WAVE_PIECE + 2);
-        total_pieces += pw.piece_cap;
-        // largest spans first within the wave
-        for (uint32_t q = 0; q < pw.n; q++) order[pw.first + q] = pw.first + q;
-        std::stable_sort(order.begin() + pw.first, order.begin() + pw.first + pw.n, [&](uint32_t a, uint32_t b) {
-            return items[a].out_cap > items[b].out_cap;
-        });
-        build_res_tables({pw.n}, c->n_sm, pw.tab);
-        pw.tab_off = tabs.size();
-        tabs.resize(pw.tab_off + round8(pw.tab.bytes));
-        pw.tab.write(tabs.data() + pw.tab_off);
-        max_n = std::max(max_n, pw.n);
-        max_win = std::max(max_win, res_win_bytes(pw.tab, pw.n));
-    }
-    // ---- device memory
+    if (int rf = fixed_walk_starts(c, body, blen, lone_targets(targets_in(0, nbits), verified, WALK_WIDE), verified,
+                                   err))
+        return rf;
+    const double t_scanned = now_ms();
+    set_cand(verified);
+    plan_starts(0, W, 0, cand.size());
+    make_items(0, ~0ull, stored);
+    make_waves();
+    t_mark[0] = now_ms();
+    // ---- device memory, sized for every wave (nothing is allocated once the first wave runs)
+    const uint64_t n_max = slots * W;
+    const uint64_t arena_max = (uint64_t)((double)(blen + n_max) * c->expand) + n_max * (65536 + 8) + 64;
+    const uint32_t pieces_max = (uint32_t)(arena_max / WAVE_PIECE + 2 * W);
+    ResTables full;
+    build_res_tables({(uint32_t)slots}, c->n_sm, full);
+    const size_t tabs_max = (size_t)W * round8(full.bytes);
+    const size_t max_win = res_win_bytes(full, (uint32_t)slots);
+    const uint32_t max_n = (uint32_t)slots;
     // pipe layout: state | infos | live | n_pieces[W] | fin (exp/got/status/mpiece) | seg total |
     //              wave jobs[W] | chunks[max_n] | head_segs[max_n+1] | pieces | piece_crc | tabs
-    const size_t o_info = 64, o_live = o_info + round8(Wn * sizeof(WaveInfo)), o_np = o_live + 8,
-                 o_fin = o_np + round8(Wn * 4), o_seg = o_fin + 64, o_wj = o_seg + 8,
-                 o_chunks = o_wj + round8(Wn * sizeof(WaveJob)),
+    const size_t o_info = 64, o_live = o_info + round8(W * sizeof(WaveInfo)), o_np = o_live + 8,
+                 o_fin = o_np + round8(W * 4), o_seg = o_fin + 64, o_wj = o_seg + 8,
+                 o_chunks = o_wj + round8(W * sizeof(WaveJob)),
                  o_hs = o_chunks + round8((size_t)max_n * sizeof(ResolveChunk)),
-                 o_pc = o_hs + ((size_t)max_n + 1) * 8, o_pcrc = o_pc + (size_t)total_pieces * sizeof(CrcPiece),
-                 o_tabs = o_pcrc + round8((size_t)total_pieces * 4), p_total = o_tabs + tabs.size();
+                 o_pc = o_hs + ((size_t)max_n + 1) * 8, o_pcrc = o_pc + (size_t)pieces_max * sizeof(CrcPiece),
+                 o_tabs = o_pcrc + round8((size_t)pieces_max * 4), p_total = o_tabs + tabs_max;
     const uint64_t isize_hint = le32h(h_file + len - 4);
     OutTarget tgt{(uint8_t*)c->out.p, c->out.cap, true};
-    const uint64_t out_cap = std::min<uint64_t>(out_bound, std::max<uint64_t>(isize_hint, 2 * len) + (1u << 20));
+    const uint64_t out_cap = std::min<uint64_t>(arena_max, std::max<uint64_t>(isize_hint, 2 * len) + (1u << 20));
     if (int rc = ensure_out(c, tgt, out_cap, 0, err)) return rc;
     CK(dgrow(c->pipe, p_total));
-    CK(dgrow(c->items, (size_t)n * sizeof(ChunkItem)));
-    CK(dgrow(c->results, (size_t)n * sizeof(ChunkResult)));
-    CK(dgrow(c->order, (size_t)n * 4));
-    CK(dgrow(c->queue, (size_t)Wn * 16));
+    CK(dgrow(c->items, (size_t)n_max * sizeof(ChunkItem)));
+    CK(dgrow(c->results, (size_t)n_max * sizeof(ChunkResult)));
+    CK(dgrow(c->order, (size_t)n_max * 4));
+    CK(dgrow(c->queue, (size_t)W * 16));
     CK(dgrow(c->mbs, 4096 * sizeof(MemberRec)));
     CK(dgrow(c->mbcount, 16));
-    CK(dgrow(c->cells, (arena + 8) * 2));
+    CK(dgrow(c->cells, (arena_max + 8) * 2));
     CK(dgrow(c->win, max_win));
     CK(dgrow(c->rerr, 16));
     CK(dgrow(c->markers, 8));
     CK(dgrow(c->crc_table, sizeof(g_crc_tab) + sizeof(g_crc_z496)));
-    if (int rc = ensure_ring(c, 16u << 20, Wn, err)) return rc;
+    if (int rc = ensure_ring(c, 16u << 20, W, err)) return rc;
     if (!c->copy_stream) CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    t_mark[1] = now_ms();
     uint8_t* P = (uint8_t*)c->pipe.p;
+    const uint32_t Wn = (uint32_t)waves.size();
+    const uint32_t n = (uint32_t)items.size();
     WaveState st0{0, 0, 1, 0};
     CK(cudaMemcpyAsync(P, &st0, sizeof(st0), cudaMemcpyHostToDevice, c->stream));
     std::vector<WaveJob> wj(Wn);
@@ -2418,13 +2462,14 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
     CK(cudaMemcpyAsync(P + o_tabs, tabs.data(), tabs.size(), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->items.p, items.data(), (size_t)n * sizeof(ChunkItem), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->order.p, order.data(), (size_t)n * 4, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemsetAsync(c->queue.p, 0, (size_t)Wn * 16, c->stream));
+    CK(cudaMemsetAsync(c->queue.p, 0, (size_t)W * 16, c->stream));
     CK(cudaMemsetAsync(c->mbcount.p, 0, 16, c->stream));
     CK(cudaMemsetAsync(c->rerr.p, 0, 16, c->stream));
     CK(cudaMemsetAsync(c->markers.p, 0, 8, c->stream));
     // the final member check: one member over every wave's piece region
     const uint32_t mps[2] = {0, total_pieces};
     CK(cudaMemcpyAsync(P + o_fin + 48, mps, 8, cudaMemcpyHostToDevice, c->stream));
+    t_mark[2] = now_ms();
     // every stream starts after the input, the scan and these uploads
     cudaEvent_t ev0 = nullptr;
     std::vector<cudaEvent_t> evs;  // destroyed on every return
@@ -2442,18 +2487,17 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
     CK(mkev(&ev0, true));
     CK(cudaEventRecord(ev0, c->stream));
     CK(cudaStreamWaitEvent(c->copy_stream, ev0, 0));
-    // ---- enqueue every wave: inflate | chain check, resolve, CRC pieces
+    // ---- per wave: inflate | chain check, resolve, CRC pieces
     const uint32_t IW = c->inflate_warps;
     const size_t ismem = IW * sizeof(WarpSmem);
     int occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_inflate<uint16_t>, IW * 32, ismem);
-    std::vector<cudaEvent_t> e_chain(Wn), e_res(Wn), e_inf(Wn);
+    std::vector<cudaEvent_t> e_chain(W), e_res(W), e_inf(W);
     WaveInfo* h_info = (WaveInfo*)c->h_wave;
-    uint32_t* h_err = (uint32_t*)(c->h_wave + Wn * sizeof(WaveInfo));  // resolve error word per wave
-    uint32_t* h_fin = h_err + Wn + 1;                                    // status, got_crc, got_len lo/hi
-    for (uint32_t w = 0; w < Wn; w++) {
+    uint32_t* h_err = (uint32_t*)(c->h_wave + W * sizeof(WaveInfo));  // resolve error word per wave
+    uint32_t* h_fin = h_err + W + 1;                                    // status, got_crc, got_len lo/hi
+    auto enqueue_inflate = [&](uint32_t w) -> int {
         const PipeWave& pw = waves[w];
-        cudaStream_t ws = c->stream;
         InflateArgs A{};
         A.in = d_file;
         A.items = (const ChunkItem*)c->items.p;
@@ -2465,10 +2509,15 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
         A.mbs = (MemberRec*)c->mbs.p;
         A.mb_count = (uint32_t*)c->mbcount.p;
         A.mb_cap = 4096;
-        RRG_LAUNCH(k_inflate<uint16_t>, persistent_blocks(c, std::max(1, occ), pw.n, IW), IW * 32, ismem, ws, A);
+        RRG_LAUNCH(k_inflate<uint16_t>, persistent_blocks(c, std::max(1, occ), pw.n, IW), IW * 32, ismem, c->stream,
+                   A);
         LAUNCHED(c);
         CK(mkev(&e_inf[w], true));
-        CK(cudaEventRecord(e_inf[w], ws));
+        CK(cudaEventRecord(e_inf[w], c->stream));
+        return 0;
+    };
+    auto enqueue_rest = [&](uint32_t w) -> int {
+        const PipeWave& pw = waves[w];
         cudaStream_t rs = c->stream;
         WaveArgs WA{};
         WA.items = (const ChunkItem*)c->items.p;
@@ -2494,16 +2543,16 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
         LAUNCHED(c);
         CK(mkev(&e_chain[w], true));
         CK(cudaEventRecord(e_chain[w], rs));
-        ResolveArgs R{};
-        R.cells = (uint16_t*)c->cells.p;
-        R.chunks = WA.chunks;
-        R.head_segs = WA.head_segs;
-        res_args(R, pw.tab, P + o_tabs + pw.tab_off, (uint16_t*)c->win.p, pw.n);
-        R.out = tgt.p;
-        R.err = (uint32_t*)c->rerr.p;
-        R.markers = (unsigned long long*)c->markers.p;
-        R.live = WA.live;
-        if (int rc = launch_resolve(c, R, rs, err)) return rc;
+        ResolveArgs RA{};
+        RA.cells = (uint16_t*)c->cells.p;
+        RA.chunks = WA.chunks;
+        RA.head_segs = WA.head_segs;
+        res_args(RA, pw.tab, P + o_tabs + pw.tab_off, (uint16_t*)c->win.p, pw.n);
+        RA.out = tgt.p;
+        RA.err = (uint32_t*)c->rerr.p;
+        RA.markers = (unsigned long long*)c->markers.p;
+        RA.live = WA.live;
+        if (int rc = launch_resolve(c, RA, rs, err)) return rc;
         CrcWideArgs CA{tgt.p, WA.pieces + pw.piece_off, pw.piece_cap, (uint32_t*)(P + o_pcrc) + pw.piece_off,
                        (const uint32_t*)c->crc_table.p, WA.n_pieces};
         RRG_LAUNCH(k_crc_pieces_wide, persistent_blocks(c, 8, pw.piece_cap, 1), CRCW_THREADS, 0, rs, CA);
@@ -2512,7 +2561,17 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
         LAUNCHED(c);
         CK(mkev(&e_res[w], true));
         CK(cudaEventRecord(e_res[w], rs));
+        return 0;
+    };
+    for (uint32_t w = 0; w < (uint32_t)waves.size(); w++) {
+        if (int rc = enqueue_inflate(w)) return rc;
+        if (int rc = enqueue_rest(w)) return rc;
     }
+    t_mark[3] = now_ms();
+    if (c->cfg.verbose >= 2)
+        std::fprintf(stderr, "[rrg-gpu] host: scan results %.3f ms, plan %.3f, memory %.3f, uploads %.3f, "
+                     "waves enqueued %.3f ms after the call\n", t_scanned - t_enter, t_mark[0] - t_enter,
+                     t_mark[1] - t_enter, t_mark[2] - t_enter, t_mark[3] - t_enter);
     // the member's CRC32/ISIZE over all pieces (meaningful when every wave passed)
     {
         uint32_t* fin = (uint32_t*)(P + o_fin);
@@ -2566,6 +2625,10 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
         if (issued == pcs.size() && known < Wn && failed_wave < 0) {
             CK(cudaEventSynchronize(e_chain[known]));
             const WaveInfo wi = h_info[known];
+            if (c->cfg.verbose >= 3)
+                std::fprintf(stderr, "[rrg-gpu] wave %u of %u: ok %u, output [%llu, +%llu), trailer %llu, items %u\n",
+                             known, Wn, wi.ok, (unsigned long long)wi.out_begin, (unsigned long long)wi.out_len,
+                             (unsigned long long)wi.trailer_byte, waves[known].n);
             if (!wi.ok) {
                 failed_wave = (int)known;
             } else {
