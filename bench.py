@@ -7,7 +7,7 @@ decoded on one GPU (input resident in HBM, output to HBM). A step is one
 whole-file decode through rrg_gpu_decode_device.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload zipf1g|fastq64m|bgzf|files]
+                    [--workload zipf1g|zipf_plain|fixed|fastq64m|bgzf|files|serve|stream]
 
 With N > 1 (torchrun, one rank per GPU) every rank decodes its own copy of the
 workload (independent files: weak scaling, no collective on the data path);
@@ -57,6 +57,13 @@ def workload(name: str, size: int | None):
         key = f"zipfplain_{n}_s1_v{GEN_VERSION}"
         desc = {"workload": "zipf_text_level9_single_member_one_zlib_stream", "uncompressed_bytes": n,
                 "zlib_level": 9, "vocabulary": 50000, "zipf_exponent": 1.1}
+    elif name == "fixed":
+        # one member of fixed-Huffman blocks only (zlib level 1, Z_FIXED): its
+        # sub-chunk starts come from the fixed-code walk
+        n = size or (256 << 20)
+        key, make = f"fixed_{n}_s1_v{GEN_VERSION}", lambda: W.fixed_blocks(n, seed=1)
+        desc = {"workload": "zipf_text_level1_fixed_huffman_single_member", "uncompressed_bytes": n,
+                "zlib_level": 1, "zlib_strategy": "Z_FIXED", "vocabulary": 50000, "zipf_exponent": 1.1}
     elif name == "fastq64m":
         n = size or (64 << 20)
         key, make = f"fastq_{n}_s0_v{GEN_VERSION}", lambda: W.config0(n, seed=0)
@@ -741,7 +748,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="zipf1g",
-                    choices=["zipf1g", "zipf_plain", "fastq64m", "bgzf", "files", "serve", "stream"])
+                    choices=["zipf1g", "zipf_plain", "fixed", "fastq64m", "bgzf", "files", "serve", "stream"])
     ap.add_argument("--rates", default="10,50,200", help="serve: request rates (req/s)")
     ap.add_argument("--duration", type=float, default=20.0, help="serve: seconds of arrivals per rate")
     ap.add_argument("--max-outstanding", type=int, default=32, help="serve: waiting requests before rejecting")

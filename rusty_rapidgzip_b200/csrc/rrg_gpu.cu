@@ -1088,6 +1088,17 @@ std::vector<uint64_t> lone_targets(const std::vector<uint64_t>& targets, const s
     return lone;
 }
 
+// Targets for the fixed-code walk. A target with no start within 256 KiB shows
+// fixed-Huffman blocks nearby (zlib's dynamic and stored blocks are at most a
+// few tens of KiB apart); then every target with no start within 16 KiB is
+// walked, so that one false dynamic-header match among fixed blocks does not
+// leave a wide span to a single sub-chunk. A stream without such a target
+// walks nothing.
+std::vector<uint64_t> walk_targets(const std::vector<uint64_t>& targets, const std::vector<uint64_t>& verified) {
+    if (lone_targets(targets, verified, (256ull << 10) * 8).empty()) return {};
+    return lone_targets(targets, verified, (16ull << 10) * 8);
+}
+
 // Block starts found by walking the fixed Huffman code forward from each
 // target (k_fixed_walk), for targets the candidate scan left without a start,
 // as in a stream of fixed-Huffman blocks. They join `verified`, which stays
@@ -1101,7 +1112,7 @@ int fixed_walk_starts(rrg_ctx* c, const uint8_t* body, uint64_t blen, const std:
     CK(dgrow(c->found, (size_t)n * 8));
     CK(cudaMemcpyAsync(c->targets.p, from.data(), (size_t)n * 8, cudaMemcpyHostToDevice, c->stream));
     FixedWalkArgs F{body, blen, (const uint64_t*)c->targets.p, (uint64_t*)c->found.p, n, (256ull << 10) * 8};
-    RRG_LAUNCH(k_fixed_walk, (n + FW_THREADS - 1) / FW_THREADS, FW_THREADS, 0, c->stream, F);
+    RRG_LAUNCH(k_fixed_walk, (n + FW_THREADS / 32 - 1) / (FW_THREADS / 32), FW_THREADS, 0, c->stream, F);
     LAUNCHED(c);
     kt.stop();
     std::vector<uint64_t> found(n);
@@ -1309,8 +1320,8 @@ int members_route(rrg_ctx* c, const uint8_t* d_base, std::vector<MemberJob>& job
                     }
                 }
             }
-            // targets with no start within 256 KiB: fixed-Huffman blocks
-            if (int rf = fixed_walk_starts(c, d_base + lo, hi - lo, lone_targets(ideal, verified, WIDE * 8), verified,
+            // fixed-Huffman blocks: starts found by walking the fixed code
+            if (int rf = fixed_walk_starts(c, d_base + lo, hi - lo, walk_targets(ideal, verified), verified,
                                            err))
                 return rf;
             // verified offsets are sorted bit offsets from `lo`
@@ -2292,7 +2303,6 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
         }
         return t;
     };
-    constexpr uint64_t WALK_WIDE = (256ull << 10) * 8;
     // ---- planning state of both phases
     std::vector<uint64_t> cand{0};  // block starts a sub-chunk may begin at
     std::vector<uint64_t> st;       // sub-chunk starts
@@ -2404,7 +2414,7 @@ int pipelined_host(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_
     // ---- boundaries (the scan overlaps the input's arrival) and sub-chunk starts
     std::vector<uint64_t> verified, stored;
     if (int rc = scan_boundaries(c, body, blen, verified, &stored, err)) return rc;
-    if (int rf = fixed_walk_starts(c, body, blen, lone_targets(targets_in(0, nbits), verified, WALK_WIDE), verified,
+    if (int rf = fixed_walk_starts(c, body, blen, walk_targets(targets_in(0, nbits), verified), verified,
                                    err))
         return rf;
     const double t_scanned = now_ms();

@@ -2188,9 +2188,11 @@ __global__ void __launch_bounds__(128) k_verify_heavy(VerifyArgs A) {
 // over non-fixed data, where end-of-block codes are chance matches, essentially
 // never passes). Any start this returns is checked again by the anchored chain.
 
-constexpr uint32_t FW_THREADS = 32;
-constexpr uint32_t FW_WARM = 256;     // symbols since the last end-of-block or invalid code before one is trusted
-constexpr uint32_t FW_MINSYM = 1024;  // symbols a fixed block after the start must decode cleanly
+constexpr uint32_t FW_THREADS = 128;     // four targets per block, one warp each
+constexpr uint32_t FW_WARM = 256;        // symbols since the last end-of-block or invalid code before one is trusted
+constexpr uint32_t FW_MINSYM = 1024;     // symbols a fixed block after the start must decode cleanly
+constexpr uint32_t FW_SEG_BITS = 8192;   // bits of a round each lane starts in
+constexpr uint32_t FW_OVER_BITS = 8192;  // a lane walks on this far past its segment: FW_WARM symbols of <= 32 bits
 
 struct FixedWalkArgs {
     const uint8_t* body;
@@ -2204,39 +2206,27 @@ struct FixedWalkArgs {
 // One fixed-code symbol from `buf` (at least 32 bits buffered): 0 literal or
 // length/distance pair, 1 end of block, 2 invalid code (286/287, distance
 // 30/31). *used = bits taken (codes are stored MSB first, RFC 1951 §3.1.1).
+// Written with selects rather than branches, so that the lanes of a warp, each
+// on its own stream, stay in step; the extra-bit counts come from the codes
+// (RFC 1951 §3.2.5), not from the tables in constant memory, whose divergent
+// reads would be serialised.
 __device__ __forceinline__ uint32_t fixed_step(uint64_t buf, uint32_t* used) {
     const uint32_t r = __brev((uint32_t)buf & 511u) >> 23;  // the next 9 code bits, MSB first
     const uint32_t t8 = r >> 1;
-    uint32_t sym, cl;
-    if (t8 < 0x30u) {  // 7-bit codes 0000000-0010111: symbols 256-279
-        sym = 256u + (r >> 2);
-        cl = 7;
-    } else if (t8 < 0xc0u) {  // 8-bit codes 00110000-10111111: literals 0-143
-        *used = 8;
-        return 0;
-    } else if (t8 < 0xc8u) {  // 8-bit codes 11000000-11000111: symbols 280-287
-        sym = 280u + (t8 - 0xc0u);
-        cl = 8;
-    } else {  // 9-bit codes 110010000-111111111: literals 144-255
-        *used = 9;
-        return 0;
-    }
-    if (sym == 256u) {
-        *used = 7;
-        return 1;
-    }
-    if (sym > 285u) {
-        *used = cl;
-        return 2;
-    }
-    const uint32_t p = cl + c_len_extra[sym - 257u];
-    const uint32_t dc = __brev((uint32_t)(buf >> p) & 31u) >> 27;  // 5-bit distance code
-    if (dc >= 30u) {
-        *used = p + 5;
-        return 2;
-    }
-    *used = p + 5 + c_dist_extra[dc];
-    return 0;
+    const bool c7 = t8 < 0x30u;                 // 7-bit codes 0000000-0010111: symbols 256-279
+    const bool c8h = t8 >= 0xc0u && t8 < 0xc8u;  // 8-bit codes 11000000-11000111: symbols 280-287
+    const bool c9 = t8 >= 0xc8u;                // 9-bit codes: literals 144-255 (8-bit: literals 0-143)
+    const uint32_t cl = c7 ? 7u : (c9 ? 9u : 8u);
+    const uint32_t sym = c7 ? 256u + (r >> 2) : 280u + (t8 - 0xc0u);  // meaningful when c7 or c8h
+    const bool eob = c7 && sym == 256u;
+    const bool len_code = (c7 && sym != 256u) || (c8h && sym <= 285u);
+    const bool bad_len = c8h && sym > 285u;
+    const uint32_t li = sym - 257u;
+    const uint32_t p = cl + (li >= 8u && li < 28u ? (li - 4u) >> 2 : 0u);
+    const uint32_t dc = __brev((uint32_t)(buf >> (p & 63u)) & 31u) >> 27;  // 5-bit distance code
+    const bool bad_dist = dc >= 30u;
+    *used = len_code ? p + 5u + (!bad_dist && dc >= 4u ? (dc - 2u) >> 1 : 0u) : cl;
+    return eob ? 1u : ((bad_len || (len_code && bad_dist)) ? 2u : 0u);
 }
 
 // Does a block start at bit e? (the tests the walk applies, see above)
@@ -2265,40 +2255,63 @@ __device__ bool fixed_start_ok(const Src& s, uint64_t total_bits, uint64_t e, ui
     return true;
 }
 
-// One thread per target.
+// One warp per target. A walk from the target alone would be serial over the
+// rest of its block (16,383 symbols for zlib's fixed blocks); instead, in each
+// round of 32 segments, lane l walks from the start of segment l to
+// FW_OVER_BITS past its end. Where lane l + 1 is still in its first FW_WARM
+// symbols, lane l is already on the real symbol path, so every end-of-block
+// code past the target's own first FW_WARM symbols is judged by some lane.
+// The warp keeps the lowest block start any lane proves.
 __global__ void __launch_bounds__(FW_THREADS) k_fixed_walk(FixedWalkArgs A) {
     __shared__ __align__(16) uint8_t s_lut[FW_THREADS * 128];  // verify_light's precode table, one per thread
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.n) return;
+    const int lane = threadIdx.x & 31;
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= A.n) return;  // uniform over the warp
     const Src s = make_src(A.body, A.body_len);
     const uint64_t total_bits = A.body_len * 8;
     const uint64_t p0 = A.from[i];
     uint64_t found = ~0ull;
     if (p0 < total_bits) {
         const uint64_t stop = total_bits - p0 > A.limit_bits ? p0 + A.limit_bits : total_bits;
-        BR b{s, 0, 0, 0};
-        br_seek(b, p0);
-        uint32_t run = 0;
-        while (br_tell(b) < stop) {
-            br_refill(b);
-            uint32_t used = 0;
-            const uint32_t k = fixed_step(b.buf, &used);
-            br_consume(b, used);
-            if (k == 0) {
-                run++;
-                continue;
-            }
-            if (k == 1 && run >= FW_WARM) {
-                const uint64_t e = br_tell(b);
-                if (e < total_bits && fixed_start_ok(s, total_bits, e, s_lut + threadIdx.x * 128)) {
-                    found = e;
-                    break;
+        for (uint64_t base = p0; base < stop && found == ~0ull; base += 32ull * FW_SEG_BITS) {
+            const uint64_t s0 = base + (uint64_t)lane * FW_SEG_BITS;
+            const uint64_t s1 = s0 + FW_SEG_BITS + FW_OVER_BITS < stop ? s0 + FW_SEG_BITS + FW_OVER_BITS : stop;
+            uint64_t mine = ~0ull;
+            bool walking = s0 < stop;
+            BR b{s, 0, 0, 0};
+            br_seek(b, walking ? s0 : p0);
+            uint32_t run = 0;
+            // one symbol per lane per step, the warp in step
+            while (__any_sync(FULLMASK, walking)) {
+                uint32_t k = 0;
+                if (walking) {
+                    br_refill(b);
+                    uint32_t used = 0;
+                    k = fixed_step(b.buf, &used);
+                    br_consume(b, used);
                 }
+                const bool probe = walking && k == 1u && run >= FW_WARM;
+                run = k == 0u ? run + 1u : 0u;
+                __syncwarp();
+                if (__any_sync(FULLMASK, probe)) {  // rare: the start after an end-of-block
+                    if (probe) {
+                        const uint64_t e = br_tell(b);
+                        if (e < total_bits && fixed_start_ok(s, total_bits, e, s_lut + threadIdx.x * 128)) {
+                            mine = e;
+                            walking = false;
+                        }
+                    }
+                    __syncwarp();
+                }
+                if (walking && br_tell(b) >= s1) walking = false;
             }
-            run = 0;
+            // lowest proven start of the round (offsets from base fit 32 bits)
+            const uint32_t rel = mine == ~0ull ? 0xffffffffu : (uint32_t)(mine - base);
+            const uint32_t best = __reduce_min_sync(FULLMASK, rel);
+            if (best != 0xffffffffu) found = base + best;
         }
     }
-    A.found[i] = found;
+    if (lane == 0) A.found[i] = found;
 }
 
 // ------------------------------------------------------- marker resolution

@@ -263,6 +263,17 @@ inline unsigned __reduce_or_sync(unsigned, unsigned v) {
     w->bar.arrive_and_wait();
     return m;
 }
+inline int __any_sync(unsigned m, int pred) { return __ballot_sync(m, pred) != 0; }
+inline unsigned __reduce_min_sync(unsigned, unsigned v) {
+    emu::Warp* w = emu::t_warp;
+    int lane = emu::t_tid.x & 31;
+    w->slot[lane] = v;
+    w->bar.arrive_and_wait();
+    unsigned m = 0xffffffffu;
+    for (int i = 0; i < 32; i++) m = (unsigned)w->slot[i] < m ? (unsigned)w->slot[i] : m;
+    w->bar.arrive_and_wait();
+    return m;
+}
 inline int __popc(unsigned v) { return __builtin_popcount(v); }
 inline unsigned __byte_perm(unsigned x, unsigned y, unsigned s) {  // PTX prmt, default mode
     const uint64_t v = ((uint64_t)y << 32) | x;
