@@ -383,6 +383,15 @@ def run_serve(args):
         sums.append(hashlib.sha256(raw).digest())
         lens.append(len(raw))
     t_gen = time.perf_counter() - t_gen
+    # the requests sit in page-locked host memory, as a server's receive
+    # buffers would, and are submitted in place: a read-only bytes object
+    # would be copied by the Python binding on every submit
+    pinned = []
+    for i, gz in enumerate(pool):
+        t = torch.empty(len(gz), dtype=torch.uint8, pin_memory=True)
+        t.numpy()[:] = np.frombuffer(gz, dtype=np.uint8)
+        pinned.append(t)
+        pool[i] = t.numpy()
     rates = [float(x) for x in args.rates.split(",")]
     dec = Decoder(Config(device=0))
     dec.serve_start(engines=args.engines, max_ready=16)
@@ -393,7 +402,10 @@ def run_serve(args):
         while dec.poll(timeout_ms=1000) is None:
             pass
     per_rate = []
-    hasher = ThreadPoolExecutor(max_workers=4)
+    # every result is checked against its SHA-256 before it is freed: enough
+    # threads that the checks keep up with the decoder (held results would
+    # make the library allocate more page-locked result buffers)
+    hasher = ThreadPoolExecutor(max_workers=max(4, min(8, (os.cpu_count() or 8) // 2)))
     for rate in rates:
         rng = random.Random(int(rate * 1000))
         sched, lock = {}, threading.Lock()

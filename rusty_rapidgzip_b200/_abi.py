@@ -323,13 +323,20 @@ def _ptr(x) -> int:
 
 
 def _host_buffer(data):
-    """(address, length, keepalive) of a host bytes-like object."""
+    """(address, length, keepalive) of a host bytes-like object, in place: the
+    library only reads it. A read-only object (bytes, a read-only mmap) is not
+    copied either; the keepalive holds it for as long as the call needs it."""
+    if isinstance(data, bytes):
+        return (C.cast(C.c_char_p(data), C.c_void_p).value if data else None), len(data), (data,)
     mv = memoryview(data).cast("B")
+    if not len(mv):
+        return None, 0, (mv,)
     if mv.readonly:
-        buf = (C.c_char * len(mv)).from_buffer_copy(mv) if len(mv) else None
-    else:
-        buf = (C.c_char * len(mv)).from_buffer(mv) if len(mv) else None
-    return (C.addressof(buf) if buf is not None else None), len(mv), (buf, mv)
+        import numpy as np  # exposes a read-only buffer's address without a copy
+        arr = np.frombuffer(mv, dtype=np.uint8)
+        return arr.ctypes.data, len(mv), (arr, mv)
+    buf = (C.c_char * len(mv)).from_buffer(mv)
+    return C.addressof(buf), len(mv), (buf, mv)
 
 
 def _as_sink(sink):
