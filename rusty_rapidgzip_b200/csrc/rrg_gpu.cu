@@ -235,7 +235,7 @@ struct BgzfKey {
 // ... and a captured device-planned member batch
 struct BatchKey {
     const void* p[20];
-    uint64_t v[20];
+    uint64_t v[21];
 };
 constexpr int BATCH_MARKS = 5;  // events between the stages: plan | inflate | chain + resolve | CRC
 
@@ -2072,6 +2072,9 @@ int bgzf_route(rrg_ctx* c, const uint8_t* d_file, uint64_t len, OutTarget& tgt, 
 // ------------------------------------------------------------ whole file
 // Decode a whole gzip file at d_file (device) into d_dst. `h_file` (optional)
 // is the same bytes in host memory, used for header parsing.
+int batch_device(rrg_ctx* c, const uint8_t* d_in, std::vector<MemberJob>& jobs, OutTarget& tgt, bool* taken,
+                 rrg_error* err);
+
 int decode_file(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_t* h_file, OutTarget& tgt, Decoded* out,
                 rrg_error* err) {
     *out = Decoded{};
@@ -2153,6 +2156,30 @@ int decode_file(rrg_ctx* c, const uint8_t* d_file, uint64_t len, const uint8_t* 
         st = host_parse_header(head.data(), len, &hl, &detail);
     }
     if (st) return status_err(err, st, detail, 0);
+    // A large member stream into a fixed destination takes the device-planned
+    // route of the batch path: sub-chunk starts, the anchored chain, resolve
+    // and CRC are planned and checked on the device with no host round trip,
+    // and a repeated shape replays as one captured graph. What that route
+    // cannot finish (more than one member, trailing bytes, a false start) is
+    // decoded on the checked member route.
+#ifdef RRG_EMU
+    constexpr uint64_t PLANNED_MIN = 256u << 10;  // small inputs exercise the route in the CPU emulation
+#else
+    constexpr uint64_t PLANNED_MIN = 16ull << 20;
+#endif
+    if (!tgt.grow && len - hl >= PLANNED_MIN) {
+        std::vector<MemberJob> jobs(1);
+        jobs[0].len = len;
+        jobs[0].body_off = hl;
+        jobs[0].dst_cap = tgt.cap;
+        bool taken = false;
+        if (int rc0 = batch_device(c, d_file, jobs, tgt, &taken, err)) return rc0;
+        if (taken) {
+            *out = jobs[0].out;
+            if (jobs[0].rc && err) *err = jobs[0].err;
+            return jobs[0].rc;
+        }
+    }
     return member_route(c, d_file, len, hl, tgt, 0, 0, out, err);
 }
 
@@ -3264,6 +3291,7 @@ struct BatchLaunch {
     const uint8_t* scan_body = nullptr;
     uint64_t scan_len = 0, n_tiles = 0;
     uint32_t cap = 0, cap2 = 0, cap3 = 0, n_list = 0, sgrid = 0, igrid = 0;
+    uint32_t walk_kb = 1;          // k_batch_walk: blocks per big job (4 ideals each)
     ResTables tab;
     // c->bplan layout: uploaded | device-written
     size_t o_jobs = 0, o_bigbit = 0, o_bigjob = 0, o_order = 0, o_mp = 0, o_tabs = 0, o_state = 0, o_wj = 0,
@@ -3330,8 +3358,14 @@ int batch_enqueue(rrg_ctx* c, const uint8_t* d_in, uint8_t* d_out, const BatchLa
         B.keys = (unsigned long long*)(P + L.o_keys);
         B.items = (ChunkItem*)c->items.p;
         B.wjobs = (WaveJob*)(P + L.o_wj);
+        B.scan_body = L.scan_body;
+        B.walk_kb = L.walk_kb;
         RRG_LAUNCH(k_batch_select, c->n_sm * 4, 256, 0, s, B);
         LAUNCHED(c);
+        if (L.n_big) {  // ideal starts with no candidate in jobs of fixed-Huffman blocks
+            RRG_LAUNCH(k_batch_walk, L.walk_kb * std::min<uint32_t>(L.n_big, 4096), FW_THREADS, 0, s, B);
+            LAUNCHED(c);
+        }
         RRG_LAUNCH(k_batch_items, std::min<uint32_t>(L.nj, c->n_sm * 2), WAVE_THREADS, 0, s, B);
         LAUNCHED(c);
     }
@@ -3508,11 +3542,14 @@ int batch_device(rrg_ctx* c, const uint8_t* d_in, std::vector<MemberJob>& jobs, 
             lo = std::min(lo, bj[i].in_off);
             hi = std::max(hi, bj[i].in_off + bj[i].blen);
         }
+        uint32_t max_k = 0;
         for (uint32_t i : bigs) {
             bj[i].scan_bit = (bj[i].in_off - lo) * 8;
             big_bit.push_back(bj[i].scan_bit);
             big_job.push_back(i);
+            max_k = std::max(max_k, bj[i].K);
         }
+        L.walk_kb = std::max<uint32_t>(1, (max_k + FW_THREADS / 32 - 1) / (FW_THREADS / 32));
         L.n_big = (uint32_t)bigs.size();
         L.scan_body = d_in + lo;
         L.scan_len = hi - lo;
@@ -3655,8 +3692,8 @@ int batch_device(rrg_ctx* c, const uint8_t* d_in, std::vector<MemberJob>& jobs, 
         const uint64_t vals[] = {L.direct, L.nj, L.n_items, L.n_big, L.total_pieces, L.mb_cap, L.scan_len, L.n_tiles,
                                  L.cap, L.cap2, L.cap3, L.n_list, L.sgrid, L.igrid, L.tab.groups.size(),
                                  L.tab.supers.size(), L.tab.jobs.size(), L.total,
-                                 ((uint64_t)c->scan_threads << 32) | c->inflate_warps, L.o_tabs};
-        for (size_t i = 0; i < 20; i++) key.v[i] = vals[i];
+                                 ((uint64_t)c->scan_threads << 32) | c->inflate_warps, L.o_tabs, L.walk_kb};
+        for (size_t i = 0; i < sizeof(vals) / sizeof(vals[0]); i++) key.v[i] = vals[i];
         auto* ent = c->bt_graphs.find(key);
         if (!ent && c->bt_graphs.repeat(key)) {
             cudaGraph_t g = nullptr;

@@ -2262,6 +2262,51 @@ __device__ bool fixed_start_ok(const Src& s, uint64_t total_bits, uint64_t e, ui
 // symbols, lane l is already on the real symbol path, so every end-of-block
 // code past the target's own first FW_WARM symbols is judged by some lane.
 // The warp keeps the lowest block start any lane proves.
+// The lowest block start the warp proves in [p0, stop) (~0: none); uniform
+// over the warp, which calls it together.
+__device__ uint64_t fixed_walk_warp(const Src& s, uint64_t total_bits, uint64_t p0, uint64_t stop, uint8_t* lut,
+                                    int lane) {
+    uint64_t found = ~0ull;
+    for (uint64_t base = p0; base < stop && found == ~0ull; base += 32ull * FW_SEG_BITS) {
+        const uint64_t s0 = base + (uint64_t)lane * FW_SEG_BITS;
+        const uint64_t s1 = s0 + FW_SEG_BITS + FW_OVER_BITS < stop ? s0 + FW_SEG_BITS + FW_OVER_BITS : stop;
+        uint64_t mine = ~0ull;
+        bool walking = s0 < stop;
+        BR b{s, 0, 0, 0};
+        br_seek(b, walking ? s0 : p0);
+        uint32_t run = 0;
+        // one symbol per lane per step, the warp in step
+        while (__any_sync(FULLMASK, walking)) {
+            uint32_t k = 0;
+            if (walking) {
+                br_refill(b);
+                uint32_t used = 0;
+                k = fixed_step(b.buf, &used);
+                br_consume(b, used);
+            }
+            const bool probe = walking && k == 1u && run >= FW_WARM;
+            run = k == 0u ? run + 1u : 0u;
+            __syncwarp();
+            if (__any_sync(FULLMASK, probe)) {  // rare: the start after an end-of-block
+                if (probe) {
+                    const uint64_t e = br_tell(b);
+                    if (e < total_bits && fixed_start_ok(s, total_bits, e, lut)) {
+                        mine = e;
+                        walking = false;
+                    }
+                }
+                __syncwarp();
+            }
+            if (walking && br_tell(b) >= s1) walking = false;
+        }
+        // lowest proven start of the round (offsets from base fit 32 bits)
+        const uint32_t rel = mine == ~0ull ? 0xffffffffu : (uint32_t)(mine - base);
+        const uint32_t best = __reduce_min_sync(FULLMASK, rel);
+        if (best != 0xffffffffu) found = base + best;
+    }
+    return found;
+}
+
 __global__ void __launch_bounds__(FW_THREADS) k_fixed_walk(FixedWalkArgs A) {
     __shared__ __align__(16) uint8_t s_lut[FW_THREADS * 128];  // verify_light's precode table, one per thread
     const int lane = threadIdx.x & 31;
@@ -2273,43 +2318,7 @@ __global__ void __launch_bounds__(FW_THREADS) k_fixed_walk(FixedWalkArgs A) {
     uint64_t found = ~0ull;
     if (p0 < total_bits) {
         const uint64_t stop = total_bits - p0 > A.limit_bits ? p0 + A.limit_bits : total_bits;
-        for (uint64_t base = p0; base < stop && found == ~0ull; base += 32ull * FW_SEG_BITS) {
-            const uint64_t s0 = base + (uint64_t)lane * FW_SEG_BITS;
-            const uint64_t s1 = s0 + FW_SEG_BITS + FW_OVER_BITS < stop ? s0 + FW_SEG_BITS + FW_OVER_BITS : stop;
-            uint64_t mine = ~0ull;
-            bool walking = s0 < stop;
-            BR b{s, 0, 0, 0};
-            br_seek(b, walking ? s0 : p0);
-            uint32_t run = 0;
-            // one symbol per lane per step, the warp in step
-            while (__any_sync(FULLMASK, walking)) {
-                uint32_t k = 0;
-                if (walking) {
-                    br_refill(b);
-                    uint32_t used = 0;
-                    k = fixed_step(b.buf, &used);
-                    br_consume(b, used);
-                }
-                const bool probe = walking && k == 1u && run >= FW_WARM;
-                run = k == 0u ? run + 1u : 0u;
-                __syncwarp();
-                if (__any_sync(FULLMASK, probe)) {  // rare: the start after an end-of-block
-                    if (probe) {
-                        const uint64_t e = br_tell(b);
-                        if (e < total_bits && fixed_start_ok(s, total_bits, e, s_lut + threadIdx.x * 128)) {
-                            mine = e;
-                            walking = false;
-                        }
-                    }
-                    __syncwarp();
-                }
-                if (walking && br_tell(b) >= s1) walking = false;
-            }
-            // lowest proven start of the round (offsets from base fit 32 bits)
-            const uint32_t rel = mine == ~0ull ? 0xffffffffu : (uint32_t)(mine - base);
-            const uint32_t best = __reduce_min_sync(FULLMASK, rel);
-            if (best != 0xffffffffu) found = base + best;
-        }
+        found = fixed_walk_warp(s, total_bits, p0, stop, s_lut + threadIdx.x * 128, lane);
     }
     if (lane == 0) A.found[i] = found;
 }
@@ -3052,6 +3061,8 @@ struct BatchArgs {
     unsigned long long* keys;  // per item: (distance << 4 | below << 3 | kind) of the best start, ~0 none
     ChunkItem* items;
     WaveJob* wjobs;
+    const uint8_t* scan_body;  // the scanned region: job J's body starts at byte J.scan_bit / 8
+    uint32_t walk_kb;          // k_batch_walk: blocks per big job (4 ideals each); the grid is a multiple
 };
 
 __device__ __forceinline__ uint64_t batch_ideal(uint64_t nbits, uint32_t k, uint32_t K) { return nbits * k / K; }
@@ -3095,6 +3106,41 @@ __global__ void k_batch_select(BatchArgs A) {
             const uint64_t d = batch_ideal(nbits, k + 1, J.K) - rel;
             atomicMin(A.keys + J.item_first + k + 1, (unsigned long long)((d << 4) | 8u | kind));
         }
+    }
+}
+
+// Fixed-Huffman blocks in the batch (the walk of k_fixed_walk): a job more
+// than half of whose ideal starts found no candidate shows fixed blocks, and
+// each of its ideals walks the fixed code up to the next ideal (at most
+// 256 KiB). Block b serves big jobs b / walk_kb (striding by the
+// grid) and their ideals (b % walk_kb) * 4 + warp.
+__global__ void __launch_bounds__(FW_THREADS) k_batch_walk(BatchArgs A) {
+    __shared__ __align__(16) uint8_t s_lut[FW_THREADS * 128];
+    __shared__ uint32_t s_missing;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t kb = blockIdx.x % A.walk_kb;
+    for (uint32_t m = blockIdx.x / A.walk_kb; m < A.n_big; m += gridDim.x / A.walk_kb) {
+        const BatchJob J = A.jobs[A.big_job[m]];
+        const uint32_t k = kb * (FW_THREADS / 32) + warp;
+        __syncthreads();
+        if (threadIdx.x == 0) s_missing = 0;
+        __syncthreads();
+        if (kb * (FW_THREADS / 32) >= J.K) continue;  // uniform over the block
+        uint32_t miss = 0;
+        for (uint32_t q = 1 + threadIdx.x; q < J.K; q += blockDim.x) miss += A.keys[J.item_first + q] == ~0ull;
+        atomicAdd(&s_missing, miss);
+        __syncthreads();
+        if (2 * s_missing <= J.K - 1) continue;  // uniform: dynamic or stored blocks
+        // A job of fixed blocks walks every ideal and keeps the walk's start:
+        // there a dynamic-header candidate is more likely a chance match than
+        // a block start (one false start sends the whole job to the checked route).
+        if (k == 0 || k >= J.K) continue;  // uniform over the warp
+        const uint64_t nbits = J.blen * 8, x = batch_ideal(nbits, k, J.K);
+        const uint64_t nx = batch_ideal(nbits, k + 1, J.K);
+        const uint64_t stop = nx - x > (256ull << 13) ? x + (256ull << 13) : nx;
+        const Src s = make_src(A.scan_body + J.scan_bit / 8, J.blen);
+        const uint64_t f = fixed_walk_warp(s, nbits, x, stop, s_lut + threadIdx.x * 128, lane);
+        if (lane == 0 && f != ~0ull && f < nbits) A.keys[J.item_first + k] = (unsigned long long)((f - x) << 4);
     }
 }
 
