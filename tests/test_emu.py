@@ -694,3 +694,31 @@ def test_fixed_huffman_blocks_split(emu_decoder_factory):
     m, st2 = d.decode_device(haddr(src), src.size, haddr(dst), dst.size)
     assert m == len(raw) and dst[:m].tobytes() == raw
     assert st2.gpu_chunks >= 4 and st2.speculation_failures == 0
+
+
+def test_fixed_huffman_blocks_in_a_batch(emu_decoder_factory):
+    """A member of fixed-Huffman blocks in a device-planned batch, next to a
+    dynamic one: the batch route walks the fixed code for its sub-chunk starts
+    (k_batch_walk), so it splits with no re-decode, and both outputs equal the
+    generator's."""
+    r1, g1 = W.fixed_blocks(1 << 20, seed=11)
+    r2, g2 = W.config1(300 << 10, seed=12)
+    blobs, raws = [g1, g2], [r1, r2]
+    offs, o = [], 0
+    for b in blobs:
+        offs.append(o)
+        o += (len(b) + 255) & ~255
+    src = np.zeros(o + 256, dtype=np.uint8)
+    for off, b in zip(offs, blobs):
+        src[off:off + len(b)] = np.frombuffer(b, dtype=np.uint8)
+    caps = [len(r) + 4096 for r in raws]
+    ooffs, q = [], 0
+    for cp in caps:
+        ooffs.append(q)
+        q += (cp + 255) & ~255
+    dst = np.zeros(q + 256, dtype=np.uint8)
+    d = emu_decoder_factory()
+    lens, status, st = d.decode_batch(haddr(src), offs, [len(b) for b in blobs], haddr(dst), ooffs, caps)
+    assert status == [0, 0]
+    assert [dst[oo:oo + n].tobytes() for oo, n in zip(ooffs, lens)] == raws
+    assert st.gpu_chunks >= 4 and st.speculation_failures == 0  # one sub-chunk for the fixed member without the walk
