@@ -86,8 +86,9 @@ typedef struct rrg_config {
                                     checked path on any irregularity), up to 4 waves; N >= 2 = N waves
                                     where every sub-chunk keeps at least 8 KiB; -1 = always the
                                     checked path */
-    int32_t batch_plan;          /* rrg_gpu_decode_batch: 0 = the member route planned and checked on the
-                                    device (sub-chunk starts, item list, anchored chain, resolve, CRC) as one
+    int32_t batch_plan;          /* rrg_gpu_decode_batch, and rrg_gpu_decode_device for member streams of
+                                    16 MiB or more: 0 = the member route planned and checked on the device
+                                    (sub-chunk starts, item list, anchored chain, resolve, CRC) as one
                                     captured graph, with the jobs it cannot finish decoded on the checked
                                     path; -1 = always the host-planned checked path */
 } rrg_config;
