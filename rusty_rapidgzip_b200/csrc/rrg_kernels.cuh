@@ -2260,7 +2260,7 @@ __device__ bool fixed_start_ok(const Src& s, uint64_t total_bits, uint64_t e, ui
 // round of 32 segments, lane l walks from the start of segment l to
 // FW_OVER_BITS past its end. Where lane l + 1 is still in its first FW_WARM
 // symbols, lane l is already on the real symbol path, so every end-of-block
-// code past the target's own first FW_WARM symbols is judged by some lane.
+// code past the target's own first FW_WARM symbols is tested by some lane.
 // The warp keeps the lowest block start any lane proves.
 // The lowest block start the warp proves in [p0, stop) (~0: none); uniform
 // over the warp, which calls it together.
