@@ -2255,15 +2255,14 @@ __device__ bool fixed_start_ok(const Src& s, uint64_t total_bits, uint64_t e, ui
     return true;
 }
 
-// One warp per target. A walk from the target alone would be serial over the
-// rest of its block (16,383 symbols for zlib's fixed blocks); instead, in each
-// round of 32 segments, lane l walks from the start of segment l to
-// FW_OVER_BITS past its end. Where lane l + 1 is still in its first FW_WARM
-// symbols, lane l is already on the real symbol path, so every end-of-block
-// code past the target's own first FW_WARM symbols is tested by some lane.
-// The warp keeps the lowest block start any lane proves.
-// The lowest block start the warp proves in [p0, stop) (~0: none); uniform
-// over the warp, which calls it together.
+// The lowest block start a warp proves in [p0, stop) (~0: none); uniform over
+// the warp, which calls it together. A walk from p0 alone would be serial
+// over the rest of its block (16,383 symbols for zlib's fixed blocks);
+// instead, in each round of 32 segments, lane l walks from the start of
+// segment l to FW_OVER_BITS past its end. Where lane l + 1 is still in its
+// first FW_WARM symbols, lane l is already on the real symbol path, so every
+// end-of-block code past the first FW_WARM symbols after p0 is tested by some
+// lane. The warp keeps the lowest block start any lane proves.
 __device__ uint64_t fixed_walk_warp(const Src& s, uint64_t total_bits, uint64_t p0, uint64_t stop, uint8_t* lut,
                                     int lane) {
     uint64_t found = ~0ull;
@@ -2307,6 +2306,7 @@ __device__ uint64_t fixed_walk_warp(const Src& s, uint64_t total_bits, uint64_t 
     return found;
 }
 
+// One warp per target.
 __global__ void __launch_bounds__(FW_THREADS) k_fixed_walk(FixedWalkArgs A) {
     __shared__ __align__(16) uint8_t s_lut[FW_THREADS * 128];  // verify_light's precode table, one per thread
     const int lane = threadIdx.x & 31;
