@@ -722,3 +722,31 @@ def test_fixed_huffman_blocks_in_a_batch(emu_decoder_factory):
     assert status == [0, 0]
     assert [dst[oo:oo + n].tobytes() for oo, n in zip(ooffs, lens)] == raws
     assert st.gpu_chunks >= 4 and st.speculation_failures == 0  # one sub-chunk for the fixed member without the walk
+
+
+def test_device_planned_member_falls_back(emu_decoder_factory):
+    """decode_device sends a large member stream through the device-planned
+    route; a file that route cannot finish (two members, or trailing bytes)
+    is decoded again on the checked route: the bytes and the error are the
+    oracle's."""
+    from rusty_rapidgzip_b200 import RrgError
+    r1, g1 = W.config1(700 << 10, seed=31)
+    r2, g2 = W.config1(500 << 10, seed=32)
+    d = emu_decoder_factory()
+
+    def device(gz, cap):
+        src = np.frombuffer(gz, dtype=np.uint8).copy()
+        dst = np.zeros(cap + 64, dtype=np.uint8)
+        n, st = d.decode_device(haddr(src), src.size, haddr(dst), dst.size)
+        return dst[:n].tobytes(), st
+
+    got, st = device(g1, len(r1))
+    assert got == r1 and st.graph_launches == 0 and st.members == 1
+    got, st = device(g1 + g2, len(r1) + len(r2))
+    assert got == r1 + r2 and st.members == 2
+    bad = g1 + b"\x1f\x8b\x08\x00garbage"
+    with pytest.raises(oracle.OracleError) as oe:
+        oracle.read_gz(bad, 2)
+    with pytest.raises(RrgError) as ge:
+        device(bad, len(r1))
+    assert ge.value.code == oe.value.code

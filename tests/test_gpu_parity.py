@@ -578,3 +578,37 @@ def test_fixed_huffman_blocks(gpu_decoder_factory, size):
     assert b"".join(got) == raw
     assert st2.gpu_chunks >= 32 and st2.speculation_failures == 0
     assert st2.pipeline_waves == (2 if size > 64 << 20 else 0)
+
+
+def test_device_planned_member_falls_back_gpu(gpu_decoder_factory):
+    """decode_device takes the device-planned route for members of 16 MiB or
+    more and replays it as a graph when the call repeats; two concatenated
+    members and trailing bytes fall back to the checked route, with the
+    oracle's bytes and error code."""
+    import torch
+    from rusty_rapidgzip_b200 import RrgError
+    r1, g1 = W.config0(48 << 20, seed=41)
+    r2 = b"second member " * 4096
+    g2 = gzip_cli(r2, 6)
+    d = gpu_decoder_factory()
+
+    def device(gz, cap, reuse=None):
+        src = reuse[0] if reuse else dev(gz)
+        out = reuse[1] if reuse else torch.empty(cap + 64, dtype=torch.uint8, device="cuda")
+        n, st = d.decode_device(src.data_ptr(), len(gz), out.data_ptr(), out.numel())
+        return out[:n].cpu().numpy().tobytes(), st, (src, out)
+
+    got, st, bufs = device(g1, len(r1))
+    assert got == r1 and st.members == 1 and st.speculation_failures == 0
+    for _ in range(2):
+        got, st, _ = device(g1, len(r1), reuse=bufs)
+        assert got == r1
+    assert st.graph_launches == 1
+    got, st, _ = device(g1 + g2, len(r1) + len(r2))
+    assert got == r1 + r2 and st.members == 2
+    bad = g1 + b"\x1f\x8b\x08\x00garbage"
+    with pytest.raises(RrgError) as ge:
+        device(bad, len(r1))
+    with pytest.raises(oracle.OracleError) as oe:
+        oracle.read_gz(bad, 4, 1 << 20)
+    assert ge.value.code == oe.value.code
